@@ -1,0 +1,339 @@
+#!/usr/bin/env python
+"""Throughput of the CubeSphere per-stage volume update on B200.
+
+One step = one full RK time step (all stages, the CFL reduction and its
+read-back) of a resident solve.  The metric is zone-updates/s: interior
+zones x steps / device seconds, summed over ranks (each rank runs its own
+replica of the solve: the path does not shard).
+
+Default workload ``shell128``: 6 panels x 128^2 angular x 64 radial zones,
+radii 1..2 with geometric stretch 1.02, 4 ghost layers, FP64, hydrostatic
+1/r^2 shell with seeded density / field perturbations (amplitude 0.05)
+under point-mass gravity, two-stage RK.  The state (0.8 GB) and the
+per-stage work arrays are far larger than L2, so no L2 flush is needed.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+``--impl reference`` times the CPU oracle port of the same path (all host
+threads) on a bounded sample of the workload instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+# Algorithmic DRAM bytes per unit for the kernels that can dominate a stage:
+# unique words each kernel must read and write once (state, work arrays and
+# geometry it touches), 8 bytes each.  Units: zones of the kernel's range.
+ALGO_WORDS_PER_UNIT = {
+    # 8 prims x 4 one-sided stencils' neighbours are re-reads; compulsory: 9
+    # comps of V/ent mode 1 + 3 centroid + scale + 9 x 3 gradient modes out
+    "k_weno7a": 9 + 4 + 27,
+    # 8 comps x 10 modes in/out of V, flattener, 18-zone centroids (re-reads
+    # excluded), coefficients 10
+    "k_weno7b": 80 + 1 + 4 + 10 + 72,
+    # face-B quadrature values of 6 faces (30), V B-modes out (30), U(6:8), E
+    # mode 1, geometry of 6 faces (3 normals + 5 weights + 15 points each)
+    "k_adp": 30 + 30 + 4 + 6 * 23 + 14,
+    # 3 faces per zone: 2 x 80 modes of the two zones amortised to 80 per
+    # zone, 3 x (15 + 5 + 3 + 1 + 3) geometry, 16 outputs + 3 speeds
+    "k_flux": 80 + 27 + 2 * 8 + 3 + 1,
+    "k_efield_c": 30 + 8 + 10 + 30,
+    "k_positivity": 80 + 4 + 80,
+    "k_faceB": 80 + 1 + 20 + 5,
+}
+
+WORKLOAD_DOC = {
+    "shell128": "FP64 ideal-MHD hydrostatic shell, 6x128^2x64 zones, r 1..2 stretch 1.02, 4 ghosts, RK2, "
+                "P12 WENO-AO/MRWENO + ADP, HLL fluxes, LLF multi-D EMFs, CT",
+    "shell32": "FP64 ideal-MHD hydrostatic shell, 6x32^2x16 zones, 4 ghosts, RK2",
+    "surface32": "FP64 ideal-MHD surface, 6x32^2x1 zones, 3 ghosts, SSP-RK3",
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="cubesphere_b200", choices=["cubesphere_b200", "reference"])
+    ap.add_argument("--workload", default="shell128")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-json", default="", help="also write the per-kernel device times here")
+    return ap.parse_args()
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in Path(self.path).read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_baseline_sample(threads: int, steps: int = 1) -> dict:
+    """The oracle (CPU port) on a bounded sample of the workload: the same
+    shell physics on 6 x 16^2 x 8 zones, ``steps`` RK2 steps."""
+    import cubesphere_b200 as cs
+    from oracle import Oracle
+
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    pr = cs.preset("shell16")
+    s = cs.Solve(**pr["params"])
+    s.mesh_build(device=False)
+    st = s.init_problem_host(**pr["init"])
+    o = Oracle(s)
+    o.put_state(st)
+    dt = o.evaluate_timestep(1e30)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        dt = o.step(dt)
+    sec = time.perf_counter() - t0
+    zones = 6 * s.N * s.N * s.nr
+    return {"value": zones * steps / sec, "unit": "zone-updates/s", "cores": threads, "kind": "port",
+            "sample": f"oracle C++ port, shell 6x{s.N}^2x{s.nr} zones (same physics as the workload), "
+                      f"{steps} RK2 step(s), {sec:.2f} s"}
+
+
+def run_reference(args):
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return 0
+    threads = min(6, os.cpu_count() or 1)  # the oracle parallelises over the 6 panels
+    vals = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline_sample(threads, steps=1)
+        if i >= args.warmup:
+            vals.append(r["value"])
+    v = statistics.mean(vals)
+    out = {
+        "metric": "zone-updates/s", "value": v, "unit": "zone-updates/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded harmonic perturbations)",
+        "config": {"workload": args.workload, "sample": "6x16^2x8 shell per step"},
+        "impl": "reference",
+        "cpu_baseline": {"value": v, "unit": "zone-updates/s", "cores": threads, "kind": "port",
+                         "sample": r["sample"]},
+        "e2e": {"value": v, "unit": "zone-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+def run_gpu(args):
+    import numpy as np
+    import torch
+
+    import cubesphere_b200 as cs
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def allmax(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    pr = cs.preset(args.workload)
+    s = cs.Solve(**pr["params"])
+    s.mesh_build()
+    s.init_problem(**pr["init"])
+    zones = 6 * s.N * s.N * s.nr
+    stream = torch.cuda.ExternalStream(s.stream_ptr())
+    dt = s.evaluate_timestep(1e30)
+    for _ in range(max(args.warmup, 3)):
+        dt = s.step(dt)
+
+    # ---- device-resident timing
+    clocks = Clocks(local)
+    barrier()
+    torch.cuda.synchronize()
+    s.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    l0 = s.launch_count()
+    s.profile_begin()
+    clocks.start()
+    e0.record(stream)
+    for _ in range(args.steps):
+        dt = s.step(dt)
+    e1.record(stream)
+    e1.synchronize()
+    clk = clocks.stop()
+    prof = s.profile_end()
+    launches = s.launch_count() - l0
+    ms = allmax(e0.elapsed_time(e1))
+    barrier()
+    value = zones * args.steps * world / (ms / 1e3)
+
+    # ---- end to end through the C ABI with pinned host buffers
+    host = {}
+    for k in ("U", "ent", "bxf", "byf", "bzf"):
+        nc = 8 if k == "U" else 1
+        host[k] = torch.empty(s.shape(nc), dtype=torch.float64, pin_memory=True).numpy()
+    s.get_state(host)
+    h2d = sum(a.nbytes for a in host.values())
+    d2h = h2d
+    barrier()
+    torch.cuda.synchronize()
+    s.synchronize()
+    k_e2e = max(1, min(args.steps, 5))
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(k_e2e):
+        s.put_state(host)
+        dt = s.step(dt)
+        s.get_state(host)
+    f1.record(stream)
+    f1.synchronize()
+    ms_e2e = allmax(f0.elapsed_time(f1))
+    e2e = zones * k_e2e * world / (ms_e2e / 1e3)
+    finite = bool(np.isfinite(host["U"]).all())
+
+    # ---- roofline of the dominant kernel (by device time in the timed region)
+    import json as _json
+
+    peaks = {}
+    pk = ROOT / "MEASURED_PEAKS.json"
+    if pk.exists():
+        peaks = _json.loads(pk.read_text())
+    hbm_peak = None
+    peak_note = "measured"
+    for key in ("hbm_gbs", "hbm_GBs", "hbm_gb_s"):
+        if key in peaks:
+            hbm_peak = float(peaks[key])
+    if hbm_peak is None:
+        hbm_peak, peak_note = 6650.0, "fallback"
+    dom = max(prof.items(), key=lambda kv: kv[1][0])
+    dname, (dms, dcount) = dom
+    G, N, nr = s.G, s.N, s.nr
+    units = 6 * (N + 2 * G - 2) ** 2 * (nr + 2 * G - 2)  # zones of the shrink-1 range (7.a / 8.d / 9.b)
+    if dname in ("k_weno7b", "k_efield_c"):
+        units = 6 * (N + 2 * G - 4) ** 2 * (nr + 2 * G - 4)
+    words = ALGO_WORDS_PER_UNIT.get(dname)
+    roof = None
+    if words is not None:
+        per_launch = words * 8.0 * units
+        if dname in ("k_flux", "k_faceB"):
+            per_launch /= 3.0  # one launch per face direction
+        achieved = per_launch / (dms / dcount / 1e3) / 1e9
+        roof = {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                "frac": achieved / hbm_peak, "traffic": None, "peak_source": peak_note,
+                "algorithmic_bytes_per_launch": per_launch, "avg_launch_ms": dms / dcount,
+                "share_of_step": dms / sum(v[0] for v in prof.values())}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample(min(6, os.cpu_count() or 1), steps=1)
+
+    if args.profile_json and rank == 0:
+        Path(args.profile_json).write_text(_json.dumps(
+            {k: {"ms": v[0], "launches": v[1]} for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},
+            indent=1))
+
+    out = {
+        "metric": "zone-updates/s", "value": value, "unit": "zone-updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded harmonic density / vector-potential perturbations)",
+        "config": {"workload": args.workload, "desc": WORKLOAD_DOC.get(args.workload, ""),
+                   "zones": zones, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (state and work arrays >> 126 MB), no flush"},
+        "e2e": {"value": e2e, "unit": "zone-updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "steps": k_e2e},
+        "roofline": roof, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches,
+        "top_kernels": {k: round(v[0] / args.steps, 3) for k, v in
+                        sorted(prof.items(), key=lambda kv: -kv[1][0])[:8]},
+        "finite": finite, "dt_last": dt,
+    }
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    s.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_gpu(args)
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -1,0 +1,743 @@
+// C ABI of the B200 stage update (include/cubesphere_b200.h): context
+// lifecycle, mesh build and upload, ghost-exchange map construction, state
+// transfer, the stage / step sequence and the per-routine entry points.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "cs_solve.h"
+
+struct cs_ctx {
+  cs::Solve sv;
+};
+
+namespace cs {
+namespace {
+
+const int kNbr[6][4] = {{3, 6, 2, 5}, {1, 4, 3, 6}, {2, 5, 1, 4}, {5, 2, 6, 3}, {6, 3, 4, 1}, {4, 1, 5, 2}};
+
+int fail(Solve& sv, int code, const std::string& msg) {
+  sv.err = msg;
+  return code;
+}
+
+int cuda_fail(Solve& sv, cudaError_t e, const char* what) {
+  return fail(sv, CS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CS_CUDA(sv, call)                                   \
+  do {                                                      \
+    cudaError_t e_ = (call);                                \
+    if (e_ != cudaSuccess) return cs::cuda_fail(sv, e_, #call); \
+  } while (0)
+
+void* dalloc(Solve& sv, size_t bytes, cudaError_t& e) {
+  void* p = nullptr;
+  e = cudaMalloc(&p, bytes);
+  if (e != cudaSuccess) return nullptr;
+  sv.allocs.push_back(p);
+  e = cudaMemsetAsync(p, 0, bytes, sv.stream);
+  return p;
+}
+
+void free_all(Solve& sv) {
+  if (sv.stream) cudaStreamSynchronize(sv.stream);
+  for (cudaEvent_t e : sv.prof.ev) cudaEventDestroy(e);
+  sv.prof.ev.clear();
+  sv.prof.name.clear();
+  for (void* p : sv.allocs) cudaFree(p);
+  sv.allocs.clear();
+  if (sv.stream) cudaStreamDestroy(sv.stream);
+  sv.stream = nullptr;
+}
+
+// Host construction of the ghost-exchange map.  The strips are visited in
+// the order of the reference's fill (x strips of every panel, then y
+// strips), a later write to the same destination replaces the earlier
+// one, and all sources are read before any destination is written.
+struct MapEntry {
+  int32_t src, dst;
+  uint8_t meta;
+};
+
+std::string build_fill_map(const Solve& sv, std::vector<MapEntry>& out) {
+  const GeomHost& g = sv.host;
+  const Box& b = g.box;
+  const int N = b.N, G = b.G, nr = b.nr;
+  const long long S = (long long)b.size();
+  const long long S6 = 6 * S;
+  if (8 * S6 >= (1LL << 31)) return "solve too large for 32-bit ghost-map offsets";
+  std::vector<int32_t> slot[5];
+  for (int f = 0; f < 5; ++f) slot[f].assign((size_t)S6, -1);
+  std::vector<MapEntry> e;
+  std::string err;
+  auto off = [&](int p, int i, int j, int k) { return (long long)p * S + (long long)b.idx(i, j, k); };
+  // fd / fs: destination / source field (0 U, 1 ent, 2 Bxf, 3 Byf, 4 Bzf).
+  auto emit = [&](int fd, int fs, int pd, int i, int j, int k, int ps, int si, int sj, int sk, bool neg, bool avg) {
+    const long long d = off(pd, i, j, k), s = off(ps, si, sj, sk);
+    const int ncomp = (fd == 0) ? NVAR : 1;
+    int32_t& sl = slot[fd][(size_t)d];
+    if (sl >= 0 && avg) err = "averaged panel-edge face written twice";
+    if (sl < 0) {
+      sl = (int32_t)e.size();
+      e.resize(e.size() + ncomp);
+    }
+    for (int c = 0; c < ncomp; ++c) {
+      MapEntry& m = e[(size_t)sl + c];
+      m.src = (int32_t)(c * S6 + s);
+      m.dst = (int32_t)(c * S6 + d);
+      m.meta = (uint8_t)(fd | (neg ? 8 : 0) | (avg ? 16 : 0) | (fs << 5));
+    }
+  };
+  auto zone = [&](int pd, int i, int j, int k, int ps, int si, int sj, int sk) {
+    emit(0, 0, pd, i, j, k, ps, si, sj, sk, false, false);
+    emit(1, 1, pd, i, j, k, ps, si, sj, sk, false, false);
+  };
+  auto mk = [&](int p, int i, int j) { return g.mask[(size_t)p * S + b.idx(i, j, 0)]; };
+  auto xmask = [&](int p, int i, int j) { return mk(p, std::max(i, 1 - G), j) * mk(p, std::min(i + 1, N + G), j); };
+  auto ymask = [&](int p, int i, int j) { return mk(p, i, std::max(j, 1 - G)) * mk(p, i, std::min(j + 1, N + G)); };
+  // x direction (330fetch_buffers_fill_in_ux.f:220-714 with the index maps of 203:104-163).
+  for (int pn = 0; pn < 6; ++pn) {
+    const int rt = kNbr[pn][0] - 1, lf = kNbr[pn][1] - 1;
+    auto inner = [&](int j, int k) { return j >= 1 && j <= N && k >= 1 && k <= nr; };
+    for (int k = 1 - G; k <= nr + G; ++k)
+      for (int j = 1 - G; j <= N + G; ++j)
+        for (int i = N + 1; i <= N + G; ++i) zone(pn, i, j, k, rt, j, 2 * N + 1 - i, k);
+    for (int k = 1 - G; k <= nr + G; ++k)
+      for (int j = 1 - G; j <= N + G; ++j)
+        for (int i = N; i <= N + G; ++i)
+          if (xmask(pn, i, j) == 1) emit(2, 3, pn, i, j, k, rt, j, 2 * N - i, k, true, i == N && inner(j, k));
+    for (int k = 1 - G; k <= nr + G; ++k)
+      for (int j = -G; j <= N + G; ++j)
+        for (int i = N + 1; i <= N + G; ++i) emit(3, 2, pn, i, j, k, rt, j, 2 * N + 1 - i, k, false, false);
+    for (int k = -G; k <= nr + G; ++k)
+      for (int j = 1 - G; j <= N + G; ++j)
+        for (int i = N + 1; i <= N + G; ++i) emit(4, 4, pn, i, j, k, rt, j, 2 * N + 1 - i, k, false, false);
+    for (int k = 1 - G; k <= nr + G; ++k)
+      for (int j = 1 - G; j <= N + G; ++j)
+        for (int i = 1 - G; i <= 0; ++i) zone(pn, i, j, k, lf, 1 - i, N + 1 - j, k);
+    for (int k = 1 - G; k <= nr + G; ++k)
+      for (int j = 1 - G; j <= N + G; ++j)
+        for (int i = -G; i <= 0; ++i)
+          if (xmask(pn, i, j) == 1) emit(2, 2, pn, i, j, k, lf, -i, N + 1 - j, k, true, i == 0 && inner(j, k));
+    for (int k = 1 - G; k <= nr + G; ++k)
+      for (int j = -G; j <= N + G; ++j)
+        for (int i = 1 - G; i <= 0; ++i) emit(3, 3, pn, i, j, k, lf, 1 - i, N - j, k, true, false);
+    for (int k = -G; k <= nr + G; ++k)
+      for (int j = 1 - G; j <= N + G; ++j)
+        for (int i = 1 - G; i <= 0; ++i) emit(4, 4, pn, i, j, k, lf, 1 - i, N + 1 - j, k, false, false);
+  }
+  // y direction (331fetch_buffers_fill_in_uy.f, 332fetch_buffers_fill_in_uy_top.f).
+  for (int pn = 0; pn < 6; ++pn) {
+    const int up = kNbr[pn][2] - 1, dn = kNbr[pn][3] - 1;
+    auto inner = [&](int i, int k) { return i >= 1 && i <= N && k >= 1 && k <= nr; };
+    for (int k = 1 - G; k <= nr + G; ++k)
+      for (int j = 1 - G; j <= 0; ++j)
+        for (int i = 1 - G; i <= N + G; ++i) zone(pn, i, j, k, dn, N + 1 - i, 1 - j, k);
+    for (int k = 1 - G; k <= nr + G; ++k)
+      for (int j = -G; j <= 0; ++j)
+        for (int i = 1 - G; i <= N + G; ++i)
+          if (ymask(pn, i, j) == 1) emit(3, 3, pn, i, j, k, dn, N + 1 - i, -j, k, true, j == 0 && inner(i, k));
+    for (int k = 1 - G; k <= nr + G; ++k)
+      for (int j = 1 - G; j <= 0; ++j)
+        for (int i = -G; i <= N + G; ++i) emit(2, 2, pn, i, j, k, dn, N - i, 1 - j, k, true, false);
+    for (int k = -G; k <= nr + G; ++k)
+      for (int j = 1 - G; j <= 0; ++j)
+        for (int i = 1 - G; i <= N + G; ++i) emit(4, 4, pn, i, j, k, dn, N + 1 - i, 1 - j, k, false, false);
+    for (int k = 1 - G; k <= nr + G; ++k)
+      for (int j = N + 1; j <= N + G; ++j)
+        for (int i = 1 - G; i <= N + G; ++i) zone(pn, i, j, k, up, 2 * N + 1 - j, i, k);
+    for (int k = 1 - G; k <= nr + G; ++k)
+      for (int j = N; j <= N + G; ++j)
+        for (int i = 1 - G; i <= N + G; ++i)
+          if (ymask(pn, i, j) == 1) emit(3, 2, pn, i, j, k, up, 2 * N - j, i, k, true, j == N && inner(i, k));
+    for (int k = 1 - G; k <= nr + G; ++k)
+      for (int j = N + 1; j <= N + G; ++j)
+        for (int i = -G; i <= N + G; ++i) emit(2, 3, pn, i, j, k, up, 2 * N + 1 - j, i, k, false, false);
+    for (int k = -G; k <= nr + G; ++k)
+      for (int j = N + 1; j <= N + G; ++j)
+        for (int i = 1 - G; i <= N + G; ++i) emit(4, 4, pn, i, j, k, up, 2 * N + 1 - j, i, k, false, false);
+  }
+  if (!err.empty()) return err;
+  out.swap(e);
+  return "";
+}
+
+}  // namespace
+}  // namespace cs
+
+namespace cs {
+
+void mark(Solve& sv, const char* name, bool kernel) {
+  if (kernel) ++sv.launches;
+  Prof& pf = sv.prof;
+  if (!pf.on) return;
+  if (pf.n == 0) return;  // no start event: launch outside a profiled sequence
+  if ((size_t)pf.n >= pf.ev.size()) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return;
+    pf.ev.push_back(e);
+    pf.name.push_back(nullptr);
+  }
+  cudaEventRecord(pf.ev[pf.n], sv.stream);
+  pf.name[pf.n] = name;
+  ++pf.n;
+}
+
+void prof_start(Solve& sv) {
+  Prof& pf = sv.prof;
+  if (!pf.on || pf.n > 0) return;
+  if (pf.ev.empty()) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return;
+    pf.ev.push_back(e);
+    pf.name.push_back(nullptr);
+  }
+  cudaEventRecord(pf.ev[0], sv.stream);
+  pf.n = 1;
+}
+
+namespace {
+
+// Adds the recorded intervals to the per-kernel totals (stream must be idle).
+void prof_harvest(Solve& sv) {
+  Prof& pf = sv.prof;
+  for (int i = 1; i < pf.n; ++i) {
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, pf.ev[i - 1], pf.ev[i]) != cudaSuccess) continue;
+    const std::string key = pf.name[i];
+    size_t q = 0;
+    while (q < pf.keys.size() && pf.keys[q] != key) ++q;
+    if (q == pf.keys.size()) {
+      pf.keys.push_back(key);
+      pf.ms.push_back(0.0);
+      pf.count.push_back(0);
+    }
+    pf.ms[q] += ms;
+    pf.count[q] += 1;
+  }
+  pf.n = 0;
+}
+
+bool check_params(const cs_params& p, std::string& why) {
+  if (p.ntp < 2 || p.nr < 1) { why = "ntp must be >= 2 and nr >= 1"; return false; }
+  if (p.nghost < 3 || p.nghost > p.ntp - 1) { why = "nghost must be in [3, ntp-1]"; return false; }
+  if (!(p.gamma > 1.0)) { why = "gamma must be > 1"; return false; }
+  if (!(p.rmax > p.rmin) || !(p.rmin > 0.0)) { why = "need 0 < rmin < rmax"; return false; }
+  if (p.radial_mesh < 0 || p.radial_mesh > 2) { why = "radial_mesh must be 0, 1 or 2"; return false; }
+  if (p.rk_scheme != CS_RK2 && p.rk_scheme != CS_SSPRK3) {
+    why = "rk_scheme must be CS_RK2 or CS_SSPRK3";
+    return false;
+  }
+  if (!(p.smallnum > 0.0) || !(p.rhofloor > 0.0) || !(p.prsfloor > 0.0)) {
+    why = "smallnum, rhofloor and prsfloor must be > 0";
+    return false;
+  }
+  if ((p.bc_lower != 2 && p.bc_lower != 0) || (p.bc_upper != 2 && p.bc_upper != 0)) {
+    why = "radial boundary codes must be 2 (outflow) or 0 (none)";
+    return false;
+  }
+  return true;
+}
+
+PhysC make_phys(const cs_params& p) {
+  PhysC ph;
+  const double pi = 4.0 * std::atan(1.0);
+  ph.gamma = p.gamma;
+  ph.rhofloor = p.rhofloor;
+  ph.prsfloor = p.prsfloor;
+  ph.smallnum = p.smallnum;
+  ph.ob4pi = 1.0 / (4.0 * pi);
+  ph.ob8pi = 1.0 / (8.0 * pi);
+  ph.fourpi = 4.0 * pi;
+  ph.cfl = p.cfl_coef;
+  ph.flatten_coef = p.flatten_coef;
+  ph.prs_flatten_coef = p.prs_flatten_coef;
+  ph.gm = p.gm;
+  return ph;
+}
+
+int ensure_host_mesh(Solve& sv) {
+  if (!sv.host.f[0].empty()) return CS_OK;
+  std::string e = build_geometry(sv.p, sv.host);
+  if (!e.empty()) return fail(sv, CS_ERR_ARG, e);
+  return CS_OK;
+}
+
+int upload_mesh(Solve& sv) {
+  const Box& b = sv.host.box;
+  Dims& d = sv.d;
+  d.N = b.N; d.nr = b.nr; d.G = b.G; d.NI = b.NI; d.NJ = b.NJ; d.NK = b.NK;
+  d.S = (long long)b.size();
+  CS_CUDA(sv, cudaGetDevice(&sv.device));
+  CS_CUDA(sv, cudaDeviceGetAttribute(&sv.sm_count, cudaDevAttrMultiProcessorCount, sv.device));
+  CS_CUDA(sv, cudaStreamCreateWithFlags(&sv.stream, cudaStreamNonBlocking));
+  cudaError_t e = cudaSuccess;
+  const size_t S6 = (size_t)6 * d.S;
+  for (int f = 0; f < CS_G_NFIELDS; ++f) {
+    const size_t bytes = sv.host.f[f].size() * sizeof(double);
+    double* p = (double*)dalloc(sv, bytes, e);
+    if (!p) return cuda_fail(sv, e, "cudaMalloc(geometry)");
+    CS_CUDA(sv, cudaMemcpyAsync(p, sv.host.f[f].data(), bytes, cudaMemcpyHostToDevice, sv.stream));
+    sv.g.f[f] = p;
+  }
+  int32_t* m = (int32_t*)dalloc(sv, sv.host.mask.size() * sizeof(int32_t), e);
+  if (!m) return cuda_fail(sv, e, "cudaMalloc(mask)");
+  CS_CUDA(sv, cudaMemcpyAsync(m, sv.host.mask.data(), sv.host.mask.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                              sv.stream));
+  sv.g.mask = m;
+  int32_t* st = (int32_t*)dalloc(sv, sv.host.stencil.size() * sizeof(int32_t), e);
+  if (!st) return cuda_fail(sv, e, "cudaMalloc(stencil)");
+  CS_CUDA(sv, cudaMemcpyAsync(st, sv.host.stencil.data(), sv.host.stencil.size() * sizeof(int32_t),
+                              cudaMemcpyHostToDevice, sv.stream));
+  sv.g.st = st;
+  // State and work arrays.
+  auto A = [&](int ncomp) -> double* { return (double*)dalloc(sv, (size_t)ncomp * S6 * sizeof(double), e); };
+  DState& s = sv.st;
+  s.U = A(NVAR); s.ent = A(4); s.Bxf = A(1); s.Byf = A(1); s.Bzf = A(1);
+  s.V = A(NVAR * NMODE); s.E = A(3 * NMODE); s.Esnap = A(3);
+  s.msonic = A(1); s.flatA = A(1); s.flatB = A(1);
+  for (int q = 0; q < 3; ++q) { s.Bq[q] = A(NQ); s.fcon[q] = A(2 * NVAR); s.EF[q] = A(1); s.Ef[q] = A(1); s.B0[q] = A(1); }
+  for (int q = 0; q < 6; ++q) s.S[q] = A(1);
+  s.dUdt = A(NVAR); s.U0 = A(NVAR); s.ent0 = A(1);
+  s.giveup = (int32_t*)dalloc(sv, S6 * sizeof(int32_t), e);
+  s.dtmin = (unsigned long long*)dalloc(sv, 64, e);
+  if (e != cudaSuccess || !s.U || !s.V || !s.E || !s.dtmin) return cuda_fail(sv, e, "cudaMalloc(state)");
+  for (int q = 0; q < 3; ++q)
+    if (!s.Bq[q] || !s.fcon[q] || !s.EF[q] || !s.Ef[q] || !s.B0[q]) return fail(sv, CS_ERR_NOMEM, "cudaMalloc(work)");
+  // Ghost-exchange map.
+  std::vector<MapEntry> map;
+  std::string why = build_fill_map(sv, map);
+  if (!why.empty()) return fail(sv, CS_ERR_ARG, why);
+  std::sort(map.begin(), map.end(), [](const MapEntry& a, const MapEntry& b2) {
+    if ((a.meta & 7) != (b2.meta & 7)) return (a.meta & 7) < (b2.meta & 7);
+    return a.dst < b2.dst;
+  });
+  const size_t n = map.size();
+  std::vector<int32_t> hs(n), hd(n);
+  std::vector<uint8_t> hm(n);
+  for (size_t t = 0; t < n; ++t) { hs[t] = map[t].src; hd[t] = map[t].dst; hm[t] = map[t].meta; }
+  FillMap& f = sv.fill;
+  f.n = (long long)n;
+  f.d_src = (int32_t*)dalloc(sv, n * sizeof(int32_t) + 16, e);
+  f.d_dst = (int32_t*)dalloc(sv, n * sizeof(int32_t) + 16, e);
+  f.d_meta = (uint8_t*)dalloc(sv, n + 16, e);
+  f.d_tmp = (double*)dalloc(sv, n * sizeof(double) + 16, e);
+  if (!f.d_src || !f.d_dst || !f.d_meta || !f.d_tmp) return cuda_fail(sv, e, "cudaMalloc(ghost map)");
+  CS_CUDA(sv, cudaMemcpyAsync(f.d_src, hs.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, sv.stream));
+  CS_CUDA(sv, cudaMemcpyAsync(f.d_dst, hd.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, sv.stream));
+  CS_CUDA(sv, cudaMemcpyAsync(f.d_meta, hm.data(), n, cudaMemcpyHostToDevice, sv.stream));
+  CS_CUDA(sv, cudaStreamSynchronize(sv.stream));
+  return CS_OK;
+}
+
+int launch_check(Solve& sv, const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(sv, e, what);
+  return CS_OK;
+}
+
+int need(Solve& sv, bool state) {
+  if (!sv.has_mesh) return fail(sv, CS_ERR_STATE, "cs_mesh_build has not run");
+  if (state && !sv.has_state) return fail(sv, CS_ERR_STATE, "no state: call cs_init_problem or cs_state_put");
+  return CS_OK;
+}
+
+void limit_all(Solve& sv) {
+  launch_prim_and_masks(sv);
+  launch_flattener(sv);
+  launch_weno(sv);
+  launch_positivity(sv);
+  launch_faceB_adp(sv);
+  launch_efield(sv);
+}
+
+int run_stage(Solve& sv, int irk, double dtcur) {
+  const int ns = sv.p.rk_scheme == CS_SSPRK3 ? 3 : 2;
+  if (irk < 1 || irk > ns) return fail(sv, CS_ERR_ARG, "irk out of range for the RK scheme");
+  double dtmove = dtcur, a0 = 0.0;
+  int kind = 0;
+  if (sv.p.rk_scheme == CS_SSPRK3) {
+    kind = 1;
+    if (irk == 2) { a0 = 0.75; dtmove = 0.25 * dtcur; }
+    if (irk == 3) { a0 = 1.0 / 3.0; dtmove = (2.0 / 3.0) * dtcur; }
+  } else if (irk == 2) {
+    dtmove = 0.5 * dtcur;
+  }
+  prof_start(sv);
+  launch_fill_ghosts(sv);
+  limit_all(sv);
+  launch_fluxes(sv);
+  launch_edges(sv);
+  launch_sources(sv);
+  if (irk == 1) launch_save_stage0(sv);
+  else launch_combine(sv, a0, kind);
+  launch_update(sv, dtmove);
+  launch_cleanup(sv);
+  return launch_check(sv, "stage launch");
+}
+
+int read_dt(Solve& sv, double* out) {
+  unsigned long long bits = 0;
+  CS_CUDA(sv, cudaMemcpyAsync(&bits, sv.st.dtmin, sizeof(bits), cudaMemcpyDeviceToHost, sv.stream));
+  CS_CUDA(sv, cudaStreamSynchronize(sv.stream));
+  if (sv.prof.on) prof_harvest(sv);
+  std::memcpy(out, &bits, sizeof(bits));
+  return CS_OK;
+}
+
+size_t field_ncomp_debug(int which) {
+  static const int nc[13] = {NVAR * NMODE, 4, 1, NVAR, 1, 1, 1, NQ, NQ, NQ, 3, 6, 3};
+  return (which < 0 || which > 12) ? 0 : (size_t)nc[which];
+}
+
+}  // namespace
+}  // namespace cs
+
+using cs::Solve;
+
+extern "C" {
+
+int cs_geom_ncomp(int field) { return cs::geom_ncomp(field); }
+
+int cs_create(const cs_params* p, cs_ctx** out) {
+  if (!p || !out) return CS_ERR_ARG;
+  *out = nullptr;
+  cs_ctx* c = new (std::nothrow) cs_ctx();
+  if (!c) return CS_ERR_NOMEM;
+  std::string why;
+  if (!cs::check_params(*p, why)) {
+    delete c;
+    return CS_ERR_ARG;
+  }
+  c->sv.p = *p;
+  c->sv.ph = cs::make_phys(*p);
+  const cs::Box b(p->ntp, p->nr, p->nghost);
+  c->sv.d.N = b.N; c->sv.d.nr = b.nr; c->sv.d.G = b.G; c->sv.d.NI = b.NI; c->sv.d.NJ = b.NJ; c->sv.d.NK = b.NK;
+  c->sv.d.S = (long long)b.size();
+  *out = c;
+  return CS_OK;
+}
+
+const char* cs_params_check(const cs_params* p) {
+  static thread_local std::string why;
+  why.clear();
+  if (!p) return "null params";
+  cs::check_params(*p, why);
+  return why.c_str();
+}
+
+int cs_destroy(cs_ctx* ctx) {
+  if (!ctx) return CS_OK;
+  cs::free_all(ctx->sv);
+  delete ctx;
+  return CS_OK;
+}
+
+const char* cs_last_error(const cs_ctx* ctx) { return ctx ? ctx->sv.err.c_str() : "null context"; }
+
+int cs_box_dims(const cs_ctx* ctx, int32_t* ni, int32_t* nj, int32_t* nk) {
+  if (!ctx || !ni || !nj || !nk) return CS_ERR_ARG;
+  *ni = ctx->sv.d.NI;
+  *nj = ctx->sv.d.NJ;
+  *nk = ctx->sv.d.NK;
+  return CS_OK;
+}
+
+int cs_mesh_build_host(cs_ctx* ctx) {
+  if (!ctx) return CS_ERR_ARG;
+  return cs::ensure_host_mesh(ctx->sv);
+}
+
+int cs_mesh_build(cs_ctx* ctx) {
+  if (!ctx) return CS_ERR_ARG;
+  Solve& sv = ctx->sv;
+  if (sv.has_mesh) return cs::fail(sv, CS_ERR_STATE, "mesh already built on this context");
+  int rc = cs::ensure_host_mesh(sv);
+  if (rc) return rc;
+  rc = cs::upload_mesh(sv);
+  if (rc) {
+    cs::free_all(sv);
+    return rc;
+  }
+  sv.has_mesh = true;
+  return CS_OK;
+}
+
+int cs_geometry_get(cs_ctx* ctx, int field, double* host_out, size_t n) {
+  if (!ctx || !host_out || field < 0 || field >= CS_G_NFIELDS) return CS_ERR_ARG;
+  Solve& sv = ctx->sv;
+  if (sv.host.f[0].empty()) return cs::fail(sv, CS_ERR_STATE, "no mesh: call cs_mesh_build or cs_mesh_build_host");
+  const std::vector<double>& v = sv.host.f[field];
+  if (n != v.size()) return cs::fail(sv, CS_ERR_ARG, "geometry buffer size mismatch");
+  std::memcpy(host_out, v.data(), n * sizeof(double));
+  return CS_OK;
+}
+
+int cs_mask_get(cs_ctx* ctx, int32_t* host_out, size_t n) {
+  if (!ctx || !host_out) return CS_ERR_ARG;
+  Solve& sv = ctx->sv;
+  if (sv.host.mask.empty()) return cs::fail(sv, CS_ERR_STATE, "no mesh");
+  if (n != sv.host.mask.size()) return cs::fail(sv, CS_ERR_ARG, "mask buffer size mismatch");
+  std::memcpy(host_out, sv.host.mask.data(), n * sizeof(int32_t));
+  return CS_OK;
+}
+
+int cs_stencil_get(cs_ctx* ctx, int32_t* host_out, size_t n) {
+  if (!ctx || !host_out) return CS_ERR_ARG;
+  Solve& sv = ctx->sv;
+  if (sv.host.stencil.empty()) return cs::fail(sv, CS_ERR_STATE, "no mesh");
+  if (n != sv.host.stencil.size()) return cs::fail(sv, CS_ERR_ARG, "stencil buffer size mismatch");
+  std::memcpy(host_out, sv.host.stencil.data(), n * sizeof(int32_t));
+  return CS_OK;
+}
+
+int cs_geometry_single_zone(int32_t isector, int32_t ntp_global, int32_t nr_global, int32_t iscale, double rmin,
+                            double rmax, int32_t radial_mesh, int32_t field, double* host_out, size_t n) {
+  if (!host_out || field < 0 || field >= CS_G_NFIELDS || isector < 1 || isector > 6 || iscale < 1 ||
+      ntp_global < 1 || nr_global < 1 || ntp_global % iscale || nr_global % iscale)
+    return CS_ERR_ARG;
+  cs::GeomHost g;
+  std::string e = cs::build_geometry_single_zone(isector, ntp_global, nr_global, iscale, rmin, rmax, radial_mesh, g);
+  if (!e.empty()) return CS_ERR_ARG;
+  const std::vector<double>& v = g.f[field];
+  if (n != v.size()) return CS_ERR_ARG;
+  std::memcpy(host_out, v.data(), n * sizeof(double));
+  return CS_OK;
+}
+
+int cs_init_problem_host(cs_ctx* ctx, const cs_init_desc* d, double* U, double* ent, double* bxf, double* byf,
+                         double* bzf) {
+  if (!ctx || !d || !U || !ent || !bxf || !byf || !bzf) return CS_ERR_ARG;
+  Solve& sv = ctx->sv;
+  int rc = cs::ensure_host_mesh(sv);
+  if (rc) return rc;
+  std::string e = cs::init_problem_host(sv.p, *d, sv.host, U, ent, bxf, byf, bzf);
+  if (!e.empty()) return cs::fail(sv, CS_ERR_ARG, e);
+  return CS_OK;
+}
+
+int cs_state_put(cs_ctx* ctx, const double* U, const double* ent, const double* bxf, const double* byf,
+                 const double* bzf) {
+  if (!ctx || !U || !ent || !bxf || !byf || !bzf) return CS_ERR_ARG;
+  Solve& sv = ctx->sv;
+  if (int rc = cs::need(sv, false)) return rc;
+  const size_t S6 = (size_t)6 * sv.d.S * sizeof(double);
+  CS_CUDA(sv, cudaMemcpyAsync(sv.st.U, U, cs::NVAR * S6, cudaMemcpyHostToDevice, sv.stream));
+  CS_CUDA(sv, cudaMemcpyAsync(sv.st.ent, ent, S6, cudaMemcpyHostToDevice, sv.stream));
+  CS_CUDA(sv, cudaMemcpyAsync(sv.st.Bxf, bxf, S6, cudaMemcpyHostToDevice, sv.stream));
+  CS_CUDA(sv, cudaMemcpyAsync(sv.st.Byf, byf, S6, cudaMemcpyHostToDevice, sv.stream));
+  CS_CUDA(sv, cudaMemcpyAsync(sv.st.Bzf, bzf, S6, cudaMemcpyHostToDevice, sv.stream));
+  CS_CUDA(sv, cudaStreamSynchronize(sv.stream));
+  sv.has_state = true;
+  return CS_OK;
+}
+
+int cs_state_get(cs_ctx* ctx, double* U, double* ent, double* bxf, double* byf, double* bzf) {
+  if (!ctx || !U || !ent || !bxf || !byf || !bzf) return CS_ERR_ARG;
+  Solve& sv = ctx->sv;
+  if (int rc = cs::need(sv, true)) return rc;
+  const size_t S6 = (size_t)6 * sv.d.S * sizeof(double);
+  CS_CUDA(sv, cudaMemcpyAsync(U, sv.st.U, cs::NVAR * S6, cudaMemcpyDeviceToHost, sv.stream));
+  CS_CUDA(sv, cudaMemcpyAsync(ent, sv.st.ent, S6, cudaMemcpyDeviceToHost, sv.stream));
+  CS_CUDA(sv, cudaMemcpyAsync(bxf, sv.st.Bxf, S6, cudaMemcpyDeviceToHost, sv.stream));
+  CS_CUDA(sv, cudaMemcpyAsync(byf, sv.st.Byf, S6, cudaMemcpyDeviceToHost, sv.stream));
+  CS_CUDA(sv, cudaMemcpyAsync(bzf, sv.st.Bzf, S6, cudaMemcpyDeviceToHost, sv.stream));
+  CS_CUDA(sv, cudaStreamSynchronize(sv.stream));
+  return CS_OK;
+}
+
+int cs_init_problem(cs_ctx* ctx, const cs_init_desc* d) {
+  if (!ctx || !d) return CS_ERR_ARG;
+  Solve& sv = ctx->sv;
+  if (int rc = cs::need(sv, false)) return rc;
+  const size_t S6 = (size_t)6 * sv.d.S;
+  std::vector<double> U(cs::NVAR * S6), ent(S6), bx(S6), by(S6), bz(S6);
+  std::string e = cs::init_problem_host(sv.p, *d, sv.host, U.data(), ent.data(), bx.data(), by.data(), bz.data());
+  if (!e.empty()) return cs::fail(sv, CS_ERR_ARG, e);
+  return cs_state_put(ctx, U.data(), ent.data(), bx.data(), by.data(), bz.data());
+}
+
+int cs_stage(cs_ctx* ctx, int32_t irk, double dtcur) {
+  if (!ctx) return CS_ERR_ARG;
+  Solve& sv = ctx->sv;
+  if (int rc = cs::need(sv, true)) return rc;
+  if (!(dtcur > 0.0)) return cs::fail(sv, CS_ERR_ARG, "dtcur must be > 0");
+  return cs::run_stage(sv, irk, dtcur);
+}
+
+int cs_evaluate_timestep(cs_ctx* ctx, double dtcur, double* dtcurp1) {
+  if (!ctx || !dtcurp1) return CS_ERR_ARG;
+  Solve& sv = ctx->sv;
+  if (int rc = cs::need(sv, true)) return rc;
+  if (!(dtcur > 0.0)) return cs::fail(sv, CS_ERR_ARG, "dtcur must be > 0");
+  cs::prof_start(sv);
+  cs::launch_timestep(sv, dtcur);
+  if (int rc = cs::launch_check(sv, "timestep launch")) return rc;
+  return cs::read_dt(sv, dtcurp1);
+}
+
+int cs_step(cs_ctx* ctx, double dtcur, double* dtcurp1) {
+  if (!ctx || !dtcurp1) return CS_ERR_ARG;
+  Solve& sv = ctx->sv;
+  if (int rc = cs::need(sv, true)) return rc;
+  if (!(dtcur > 0.0)) return cs::fail(sv, CS_ERR_ARG, "dtcur must be > 0");
+  const int ns = sv.p.rk_scheme == CS_SSPRK3 ? 3 : 2;
+  for (int irk = 1; irk <= ns; ++irk)
+    if (int rc = cs::run_stage(sv, irk, dtcur)) return rc;
+  cs::prof_start(sv);
+  cs::launch_timestep(sv, dtcur);
+  if (int rc = cs::launch_check(sv, "timestep launch")) return rc;
+  return cs::read_dt(sv, dtcurp1);
+}
+
+int cs_synchronize(cs_ctx* ctx) {
+  if (!ctx) return CS_ERR_ARG;
+  Solve& sv = ctx->sv;
+  if (!sv.stream) return CS_OK;
+  CS_CUDA(sv, cudaStreamSynchronize(sv.stream));
+  if (sv.prof.on) cs::prof_harvest(sv);
+  return CS_OK;
+}
+
+int cs_get_stream(cs_ctx* ctx, void** stream) {
+  if (!ctx || !stream) return CS_ERR_ARG;
+  if (int rc = cs::need(ctx->sv, false)) return rc;
+  *stream = (void*)ctx->sv.stream;
+  return CS_OK;
+}
+
+int cs_launch_count(cs_ctx* ctx, int64_t* n) {
+  if (!ctx || !n) return CS_ERR_ARG;
+  *n = ctx->sv.launches;
+  return CS_OK;
+}
+
+int cs_profile_begin(cs_ctx* ctx) {
+  if (!ctx) return CS_ERR_ARG;
+  Solve& sv = ctx->sv;
+  if (int rc = cs::need(sv, false)) return rc;
+  CS_CUDA(sv, cudaStreamSynchronize(sv.stream));
+  sv.prof.keys.clear();
+  sv.prof.ms.clear();
+  sv.prof.count.clear();
+  sv.prof.n = 0;
+  sv.prof.on = true;
+  return CS_OK;
+}
+
+int cs_profile_end(cs_ctx* ctx, int32_t max_kernels, char* names, double* total_ms, int64_t* launches,
+                   int32_t* n_kernels) {
+  if (!ctx || !names || !total_ms || !launches || !n_kernels || max_kernels < 0) return CS_ERR_ARG;
+  Solve& sv = ctx->sv;
+  if (int rc = cs::need(sv, false)) return rc;
+  CS_CUDA(sv, cudaStreamSynchronize(sv.stream));
+  cs::prof_harvest(sv);
+  sv.prof.on = false;
+  const int n = (int)sv.prof.keys.size();
+  *n_kernels = n;
+  for (int q = 0; q < n && q < max_kernels; ++q) {
+    std::memset(names + 32 * q, 0, 32);
+    std::strncpy(names + 32 * q, sv.prof.keys[q].c_str(), 31);
+    total_ms[q] = sv.prof.ms[q];
+    launches[q] = sv.prof.count[q];
+  }
+  return n > max_kernels ? cs::fail(sv, CS_ERR_ARG, "more kernels than max_kernels") : CS_OK;
+}
+
+#define CS_ROUTINE(name, body)                       \
+  int name(cs_ctx* ctx) {                            \
+    if (!ctx) return CS_ERR_ARG;                     \
+    Solve& sv = ctx->sv;                             \
+    if (int rc = cs::need(sv, true)) return rc;      \
+    body;                                            \
+    return cs::launch_check(sv, #name);              \
+  }
+
+CS_ROUTINE(cs_fill_ghosts, cs::launch_fill_ghosts(sv))
+CS_ROUTINE(cs_limit_all_slopes_p12, cs::limit_all(sv))
+CS_ROUTINE(cs_make_facial_fluxes, cs::launch_fluxes(sv))
+CS_ROUTINE(cs_make_edge_efields_p1, cs::launch_edges(sv))
+CS_ROUTINE(cs_build_non_stiff_sources, cs::launch_sources(sv))
+CS_ROUTINE(cs_cleanup_after_update, cs::launch_cleanup(sv))
+
+int cs_update_imex_rk_step_p1(cs_ctx* ctx, double dtmove) {
+  if (!ctx) return CS_ERR_ARG;
+  Solve& sv = ctx->sv;
+  if (int rc = cs::need(sv, true)) return rc;
+  cs::launch_update(sv, dtmove);
+  return cs::launch_check(sv, "cs_update_imex_rk_step_p1");
+}
+
+int cs_debug_get(cs_ctx* ctx, int32_t which, double* host_out, size_t n) {
+  if (!ctx || !host_out) return CS_ERR_ARG;
+  Solve& sv = ctx->sv;
+  if (int rc = cs::need(sv, true)) return rc;
+  const size_t nc = cs::field_ncomp_debug(which);
+  const size_t S6 = (size_t)6 * sv.d.S;
+  if (nc == 0) return cs::fail(sv, CS_ERR_ARG, "unknown debug array");
+  if (n != nc * S6) return cs::fail(sv, CS_ERR_ARG, "debug buffer size mismatch");
+  const cs::DState& s = sv.st;
+  const size_t B = S6 * sizeof(double);
+  auto cp = [&](double* dst, const double* src, size_t bytes) {
+    return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, sv.stream);
+  };
+  cudaError_t e = cudaSuccess;
+  switch (which) {
+    case 0: e = cp(host_out, s.V, nc * B); break;
+    case 1: e = cp(host_out, s.ent, nc * B); break;
+    case 2: e = cp(host_out, s.flatA, B); break;
+    case 3: e = cp(host_out, s.dUdt, nc * B); break;
+    case 4: case 5: case 6: e = cp(host_out, s.Ef[which - 4], B); break;
+    case 7: case 8: case 9: e = cp(host_out, s.Bq[which - 7], nc * B); break;
+    case 10: e = cp(host_out, s.E, 3 * B); break;
+    case 11:
+      for (int q = 0; q < 6 && e == cudaSuccess; ++q) e = cp(host_out + q * S6, s.S[q], B);
+      break;
+    case 12:
+      for (int q = 0; q < 3 && e == cudaSuccess; ++q) e = cp(host_out + q * S6, s.EF[q], B);
+      break;
+  }
+  if (e != cudaSuccess) return cs::cuda_fail(sv, e, "cs_debug_get copy");
+  CS_CUDA(sv, cudaStreamSynchronize(sv.stream));
+  return CS_OK;
+}
+
+int cs_diag(cs_ctx* ctx, double* mass, double* energy, double* max_divb) {
+  if (!ctx || !mass || !energy || !max_divb) return CS_ERR_ARG;
+  Solve& sv = ctx->sv;
+  if (int rc = cs::need(sv, true)) return rc;
+  const size_t S6 = (size_t)6 * sv.d.S;
+  std::vector<double> U(cs::NVAR * S6), ent(S6), bx(S6), by(S6), bz(S6);
+  if (int rc = cs_state_get(ctx, U.data(), ent.data(), bx.data(), by.data(), bz.data())) return rc;
+  const cs::Box& b = sv.host.box;
+  const auto& G = sv.host.f;
+  double m = 0.0, en = 0.0, dv = 0.0;
+  for (int p = 0; p < 6; ++p)
+    for (int k = 1; k <= b.nr; ++k)
+      for (int j = 1; j <= b.N; ++j)
+        for (int i = 1; i <= b.N; ++i) {
+          const size_t o = (size_t)p * b.size() + b.idx(i, j, k);
+          const double vol = G[CS_G_V_VOL][o];
+          m += U[o] * vol;
+          en += U[4 * S6 + o] * vol;
+          auto at = [&](int a, int c, int e2) { return (size_t)p * b.size() + b.idx(a, c, e2); };
+          const double flux = G[CS_G_XF_AREA][at(i, j, k)] * bx[at(i, j, k)] -
+                              G[CS_G_XF_AREA][at(i - 1, j, k)] * bx[at(i - 1, j, k)] +
+                              G[CS_G_YF_AREA][at(i, j, k)] * by[at(i, j, k)] -
+                              G[CS_G_YF_AREA][at(i, j - 1, k)] * by[at(i, j - 1, k)] +
+                              G[CS_G_ZF_AREA][at(i, j, k)] * bz[at(i, j, k)] -
+                              G[CS_G_ZF_AREA][at(i, j, k - 1)] * bz[at(i, j, k - 1)];
+          dv = std::fmax(dv, std::fabs(flux) / vol);
+        }
+  *mass = m;
+  *energy = en;
+  *max_divb = dv;
+  return CS_OK;
+}
+
+}  // extern "C"

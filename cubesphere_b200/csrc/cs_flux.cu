@@ -1,0 +1,292 @@
+// Face fluxes of the stage: five-point quadrature per face, rotation to
+// the face frame, HLL solve, rotation back, and the race-free gather of
+// the per-face contributions into the zone time derivative; plus the
+// explicit point-mass gravity source.
+//
+// Follows MAKE_FACIAL_FLUXES (pkg/inc/cubesphere/400riemann_integrate/
+// 450make_facial_fluxes.f:405-2933), OneD_RS_MHD_Ptwise
+// (600riemann_1d/610_1d_rs_oned_rs_mhd_ptwise.f) and
+// BUILD_NON_STIFF_SOURCES (470build_non_stiff_sources.f:147-244).
+// The reference scatters each face into both neighbours inside one
+// parallel loop; here each face writes its two one-sided contributions and
+// each zone sums its own six faces in a fixed order.
+#include "cs_solve.h"
+
+namespace cs {
+
+namespace {
+
+constexpr int TPB = 128;
+
+__device__ __forceinline__ double Vm(const DState& s, const Dims& d, int comp, int mode, int p, long long o) {
+  return s.V[((long long)(mode * NVAR + comp) * NPANEL + p) * d.S + o];
+}
+
+__global__ void __launch_bounds__(TPB) k_flux(Dims d, PhysC ph, DGeom g, DState s, Range3 r, int dir) {
+  const int QP = dir == 0 ? CS_G_XF_QP : (dir == 1 ? CS_G_YF_QP : CS_G_ZF_QP);
+  const int QW = dir == 0 ? CS_G_XF_QW : (dir == 1 ? CS_G_YF_QW : CS_G_ZF_QW);
+  const int AR = dir == 0 ? CS_G_XF_AREA : (dir == 1 ? CS_G_YF_AREA : CS_G_ZF_AREA);
+  double* F = s.fcon[dir];
+  double* SLo = s.S[2 * dir];
+  double* SHi = s.S[2 * dir + 1];
+  double* EF = s.EF[dir];
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
+    int p, i, j, k;
+    r.decode(t, p, i, j, k);
+    int lx = i, ly = j, lz = k, rx = i, ry = j, rz = k;
+    bool skip = false;
+    if (dir == 0) {
+      const int mL = mask_at(g, d, p, i, j), mR = mask_at(g, d, p, i + 1, j);
+      rx = i + 1;
+      if (mL == 0 && mR == 1) { lx = sten(g, d, p, rx, ry, 1, 0); ly = sten(g, d, p, rx, ry, 1, 1); }
+      else if (mL == 1 && mR == 0) { rx = sten(g, d, p, lx, ly, 0, 0); ry = sten(g, d, p, lx, ly, 0, 1); }
+      else if (mL == 0 && mR == 0) skip = true;
+    } else if (dir == 1) {
+      const int mL = mask_at(g, d, p, i, j), mR = mask_at(g, d, p, i, j + 1);
+      ry = j + 1;
+      if (mL == 0 && mR == 1) { lx = sten(g, d, p, rx, ry, 3, 0); ly = sten(g, d, p, rx, ry, 3, 1); }
+      else if (mL == 1 && mR == 0) { rx = sten(g, d, p, lx, ly, 2, 0); ry = sten(g, d, p, lx, ly, 2, 1); }
+      else if (mL == 0 && mR == 0) skip = true;
+    } else {
+      if (mask_at(g, d, p, i, j) == 0) skip = true;
+      rz = k + 1;
+    }
+    const long long fo = d.idx(i, j, k);
+    if (skip) {
+#pragma unroll
+      for (int c = 0; c < 16; ++c) F[((long long)c * NPANEL + p) * d.S + fo] = 0.0;
+      continue;
+    }
+    const long long oL = d.idx(lx, ly, lz), oR = d.idx(rx, ry, rz);
+    const double obl0 = 1.0 / fmax(geo(g, d, CS_G_V_SCALE, 0, p, lx, ly, lz), ph.smallnum);
+    const double obl02 = 1.0 / fmax(geo(g, d, CS_G_V_SCALE, 0, p, rx, ry, rz), ph.smallnum);
+    const double lcx = geo(g, d, CS_G_V_CEN, 0, p, lx, ly, lz), lcy = geo(g, d, CS_G_V_CEN, 1, p, lx, ly, lz),
+                 lcz = geo(g, d, CS_G_V_CEN, 2, p, lx, ly, lz);
+    const double rcx = geo(g, d, CS_G_V_CEN, 0, p, rx, ry, rz), rcy = geo(g, d, CS_G_V_CEN, 1, p, rx, ry, rz),
+                 rcz = geo(g, d, CS_G_V_CEN, 2, p, rx, ry, rz);
+    double cL[10], cR[10];
+#pragma unroll
+    for (int m = 0; m < 10; ++m) {
+      cL[m] = geo(g, d, CS_G_COEF, m, p, lx, ly, lz);
+      cR[m] = geo(g, d, CS_G_COEF, m, p, rx, ry, rz);
+    }
+    const double area = geo(g, d, AR, 0, p, i, j, k);
+    const double volL = geo(g, d, CS_G_V_VOL, 0, p, lx, ly, lz), volR = geo(g, d, CS_G_V_VOL, 0, p, rx, ry, rz);
+    double accL[8], accR[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) accL[c] = accR[c] = 0.0;
+    // Frame pieces that do not depend on the quadrature point.
+    double Ax = 0, Ay = 0, Az = 0, Bx = 0, By = 0, Bz = 0, Cx = 0, Cy = 0, Cz = 0, vbx = 0, vby = 0, vbz = 0;
+    if (dir == 0) {
+      Ax = geo(g, d, CS_G_XF_N, 0, p, i, j, k);
+      Ay = geo(g, d, CS_G_XF_N, 1, p, i, j, k);
+      Az = geo(g, d, CS_G_XF_N, 2, p, i, j, k);
+      Cx = geo(g, d, CS_G_XF_CEN, 0, p, i, j, k);
+      Cy = geo(g, d, CS_G_XF_CEN, 1, p, i, j, k);
+      Cz = geo(g, d, CS_G_XF_CEN, 2, p, i, j, k);
+      const double tt = 1.0 / fmax(sqrt(Cx * Cx + Cy * Cy + Cz * Cz), ph.smallnum);
+      Cx = Cx * tt;
+      Cy = Cy * tt;
+      Cz = Cz * tt;
+      Bx = Cy * Az - Cz * Ay;
+      By = Cz * Ax - Cx * Az;
+      Bz = Cx * Ay - Cy * Ax;
+    } else if (dir == 1) {
+      Ax = geo(g, d, CS_G_YF_N, 0, p, i, j, k);
+      Ay = geo(g, d, CS_G_YF_N, 1, p, i, j, k);
+      Az = geo(g, d, CS_G_YF_N, 2, p, i, j, k);
+      Bx = geo(g, d, CS_G_YF_CEN, 0, p, i, j, k);
+      By = geo(g, d, CS_G_YF_CEN, 1, p, i, j, k);
+      Bz = geo(g, d, CS_G_YF_CEN, 2, p, i, j, k);
+      const double tt = 1.0 / fmax(sqrt(Bx * Bx + By * By + Bz * Bz), ph.smallnum);
+      Bx = Bx * tt;
+      By = By * tt;
+      Bz = Bz * tt;
+      Cx = Ay * Bz - Az * By;
+      Cy = Az * Bx - Ax * Bz;
+      Cz = Ax * By - Ay * Bx;
+    } else {
+      auto vt = [&](int q, int x, int y) { return geo(g, d, CS_G_VERT, q, p, x, y, k); };
+      vbx = vt(0, i, j) + vt(0, i, j - 1) - vt(0, i - 1, j) - vt(0, i - 1, j - 1);
+      vby = vt(1, i, j) + vt(1, i, j - 1) - vt(1, i - 1, j) - vt(1, i - 1, j - 1);
+      vbz = vt(2, i, j) + vt(2, i, j - 1) - vt(2, i - 1, j) - vt(2, i - 1, j - 1);
+    }
+    for (int jq = 0; jq < 5; ++jq) {
+      if (dir == 2) {
+        Ax = geo(g, d, CS_G_ZF_N, jq, p, i, j, k);
+        Ay = geo(g, d, CS_G_ZF_N, 5 + jq, p, i, j, k);
+        Az = geo(g, d, CS_G_ZF_N, 10 + jq, p, i, j, k);
+        double tt = 1.0 / fmax(sqrt(Ax * Ax + Ay * Ay + Az * Az), ph.smallnum);
+        Ax = Ax * tt;
+        Ay = Ay * tt;
+        Az = Az * tt;
+        Bx = vbx;
+        By = vby;
+        Bz = vbz;
+        tt = Bx * Ax + By * Ay + Bz * Az;
+        Bx = Bx - tt * Ax;
+        By = By - tt * Ay;
+        Bz = Bz - tt * Az;
+        tt = 1.0 / fmax(sqrt(Bx * Bx + By * By + Bz * Bz), ph.smallnum);
+        Bx = Bx * tt;
+        By = By * tt;
+        Bz = Bz * tt;
+        Cx = Ay * Bz - Az * By;
+        Cy = Az * Bx - Ax * Bz;
+        Cz = Ax * By - Ay * Bx;
+        tt = 1.0 / fmax(sqrt(Cx * Cx + Cy * Cy + Cz * Cz), ph.smallnum);
+        Cx = Cx * tt;
+        Cy = Cy * tt;
+        Cz = Cz * tt;
+      }
+      const double px = geo(g, d, QP, jq, p, i, j, k), py = geo(g, d, QP, 5 + jq, p, i, j, k),
+                   pz = geo(g, d, QP, 10 + jq, p, i, j, k);
+      const double x = (px - lcx) * obl0, y = (py - lcy) * obl0, z = (pz - lcz) * obl0;
+      const double x2 = (px - rcx) * obl02, y2 = (py - rcy) * obl02, z2 = (pz - rcz) * obl02;
+      const double wt = geo(g, d, QW, jq, p, i, j, k);
+      double VL[8], VR[8];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        double vl[10], vr[10];
+#pragma unroll
+        for (int m = 0; m < 10; ++m) {
+          vl[m] = Vm(s, d, c, m, p, oL);
+          vr[m] = Vm(s, d, c, m, p, oR);
+        }
+        VL[c] = d_poly10(vl, cL, x, y, z);
+        VR[c] = d_poly10(vr, cR, x2, y2, z2);
+      }
+      const double* E = s.ent;
+      const double entL = E[((long long)0 * NPANEL + p) * d.S + oL] + E[((long long)1 * NPANEL + p) * d.S + oL] * x +
+                          E[((long long)2 * NPANEL + p) * d.S + oL] * y + E[((long long)3 * NPANEL + p) * d.S + oL] * z;
+      const double entR = E[((long long)0 * NPANEL + p) * d.S + oR] + E[((long long)1 * NPANEL + p) * d.S + oR] * x2 +
+                          E[((long long)2 * NPANEL + p) * d.S + oR] * y2 + E[((long long)3 * NPANEL + p) * d.S + oR] * z2;
+#pragma unroll
+      for (int o = 1; o <= 5; o += 4) {
+        double a1 = Ax * VL[o] + Ay * VL[o + 1] + Az * VL[o + 2];
+        double b1 = Bx * VL[o] + By * VL[o + 1] + Bz * VL[o + 2];
+        double c1 = Cx * VL[o] + Cy * VL[o + 1] + Cz * VL[o + 2];
+        VL[o] = a1;
+        VL[o + 1] = b1;
+        VL[o + 2] = c1;
+        a1 = Ax * VR[o] + Ay * VR[o + 1] + Az * VR[o + 2];
+        b1 = Bx * VR[o] + By * VR[o + 1] + Bz * VR[o + 2];
+        c1 = Cx * VR[o] + Cy * VR[o + 1] + Cz * VR[o + 2];
+        VR[o] = a1;
+        VR[o + 1] = b1;
+        VR[o + 2] = c1;
+      }
+      double FlL[8], FlR[8], FL[8], FR[8], SL, SR, entF;
+      d_hll(ph, VL, VR, entL, entR, FlL, FlR, FL, FR, SL, SR, entF);
+      if (jq == 0) {
+        SLo[((long long)p) * d.S + fo] = SL;
+        SHi[((long long)p) * d.S + fo] = SR;
+        EF[((long long)p) * d.S + fo] = entF;
+      }
+      // rotate back to global components and accumulate both sides
+      auto back = [&](const double* W, double* O) {
+        O[0] = W[0];
+        O[1] = Ax * W[1] + Bx * W[2] + Cx * W[3];
+        O[2] = Ay * W[1] + By * W[2] + Cy * W[3];
+        O[3] = Az * W[1] + Bz * W[2] + Cz * W[3];
+        O[4] = W[4];
+        O[5] = Ax * W[5] + Bx * W[6] + Cx * W[7];
+        O[6] = Ay * W[5] + By * W[6] + Cy * W[7];
+        O[7] = Az * W[5] + Bz * W[6] + Cz * W[7];
+      };
+      double Fm[8], Fp[8], FLL[8], FRR[8];
+      back(FlL, Fm);
+      back(FlR, Fp);
+      back(FL, FLL);
+      back(FR, FRR);
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        accL[c] = accL[c] + wt * (Fm[c] + FLL[c]) * area / volL;
+        accR[c] = accR[c] + wt * (Fp[c] - FRR[c]) * area / volR;
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      F[((long long)c * NPANEL + p) * d.S + fo] = accL[c];
+      F[((long long)(8 + c) * NPANEL + p) * d.S + fo] = accR[c];
+    }
+  }
+}
+
+// dU/dt of each zone from its six faces (x, then y, then z; lower face,
+// upper face) for the zones whose faces were all computed.
+__global__ void k_gather(Dims d, DGeom g, DState s, Range3 r) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
+    int p, i, j, k;
+    r.decode(t, p, i, j, k);
+    double acc[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) acc[c] = 0.0;
+    if (mask_at(g, d, p, i, j) == 1) {
+      const long long ox[2] = {d.idx(i - 1, j, k), d.idx(i, j, k)};
+      const long long oy[2] = {d.idx(i, j - 1, k), d.idx(i, j, k)};
+      const long long oz[2] = {d.idx(i, j, k - 1), d.idx(i, j, k)};
+      const long long* os[3] = {ox, oy, oz};
+      for (int dir = 0; dir < 3; ++dir) {
+        const double* F = s.fcon[dir];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+          acc[c] = acc[c] - F[((long long)(8 + c) * NPANEL + p) * d.S + os[dir][0]];
+          acc[c] = acc[c] - F[((long long)c * NPANEL + p) * d.S + os[dir][1]];
+        }
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 8; ++c) s.dUdt[d.at(c, p, i, j, k)] = acc[c];
+  }
+}
+
+// Point-mass gravity on zones 0..N+1 (470:147-244).
+__global__ void k_sources(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
+    int p, i, j, k;
+    r.decode(t, p, i, j, k);
+    if (mask_at(g, d, p, i, j) != 1) continue;
+    const double x = geo(g, d, CS_G_V_CEN, 0, p, i, j, k), y = geo(g, d, CS_G_V_CEN, 1, p, i, j, k),
+                 z = geo(g, d, CS_G_V_CEN, 2, p, i, j, k);
+    const double rho = s.V[d.at(0, p, i, j, k)], vx = s.V[d.at(1, p, i, j, k)], vy = s.V[d.at(2, p, i, j, k)],
+                 vz = s.V[d.at(3, p, i, j, k)];
+    const double rad = sqrt(x * x + y * y + z * z);
+    const double gmb = ph.gm * (1.0 / (rad * rad * rad));
+    const double S2 = -(gmb * x * rho), S3 = -(gmb * y * rho), S4 = -(gmb * z * rho);
+    const double S5 = vx * S2 + vy * S3 + vz * S4;
+    s.dUdt[d.at(1, p, i, j, k)] += S2;
+    s.dUdt[d.at(2, p, i, j, k)] += S3;
+    s.dUdt[d.at(3, p, i, j, k)] += S4;
+    s.dUdt[d.at(4, p, i, j, k)] += S5;
+  }
+}
+
+}  // namespace
+
+void launch_fluxes(Solve& sv) {
+  const Dims& d = sv.d;
+  const int N = d.N, nr = d.nr;
+  Range3 fx = {-1, N + 1, 0, N + 1, 0, nr + 1};
+  Range3 fy = {0, N + 1, -1, N + 1, 0, nr + 1};
+  Range3 fz = {0, N + 1, 0, N + 1, -1, nr + 1};
+  k_flux<<<blocks_for(fx.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, fx, 0);
+  mark(sv, "k_flux");
+  k_flux<<<blocks_for(fy.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, fy, 1);
+  mark(sv, "k_flux");
+  k_flux<<<blocks_for(fz.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, fz, 2);
+  mark(sv, "k_flux");
+  Range3 z = {0, N + 1, 0, N + 1, 0, nr + 1};
+  k_gather<<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, sv.st, z);
+  mark(sv, "k_gather");
+}
+
+void launch_sources(Solve& sv) {
+  if (!(sv.ph.gm > sv.p.smallnum)) return;
+  const Dims& d = sv.d;
+  Range3 z = {0, d.N + 1, 0, d.N + 1, 0, d.nr + 1};
+  k_sources<<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, z);
+  mark(sv, "k_sources");
+}
+
+}  // namespace cs

@@ -1,0 +1,1031 @@
+// Reconstruction kernels of the stage: primitive variables, flattener,
+// WENO-AO / MRWENO (P12) slopes, positivity limiting, face-B quadrature
+// values, the ADP constrained least-squares magnetic reconstruction and the
+// zone-centred electric field with its WENO limiting.
+//
+// Follows LIMIT_ALL_SLOPES_P12
+// (pkg/inc/cubesphere/400riemann_integrate/421limit_all_slopes_p12.f) and
+// ENFORCE_PRESSURE_POSITIVITY_PRIM (440enforce_pressure_positivity_prim.f);
+// each kernel names the reference step it implements.  One thread per zone
+// or face; the ADP solve uses one warp per zone with the 36x36 KKT system
+// in shared memory.
+#include "cs_solve.h"
+
+namespace cs {
+
+namespace {
+
+constexpr int TPB = 128;
+
+__device__ __forceinline__ double& Vat(const DState& s, const Dims& d, int comp, int mode, int p, int i, int j, int k) {
+  return s.V[d.at(mode * NVAR + comp, p, i, j, k)];
+}
+
+// STEP 2 (zone part, 421:597-635) and STEP 5 (421:1497-1628).
+__global__ void k_prim(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
+    int p, i, j, k;
+    r.decode(t, p, i, j, k);
+    const int m = mask_at(g, d, p, i, j);
+    double U[8], V[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) U[c] = s.U[d.at(c, p, i, j, k)];
+    if (m == 0) {
+#pragma unroll
+      for (int c = 0; c < 8; ++c) U[c] = 0.0;
+      U[0] = ph.rhofloor;
+      U[4] = ph.prsfloor / (ph.gamma - 1.0);
+    }
+    double en = s.ent[d.at(0, p, i, j, k)];
+    d_cons_to_prim(ph, en, U, V);
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      s.U[d.at(c, p, i, j, k)] = U[c];
+      s.V[d.at(c, p, i, j, k)] = V[c];
+    }
+    s.ent[d.at(0, p, i, j, k)] = en;
+    s.ent[d.at(1, p, i, j, k)] = 0.0;
+    s.ent[d.at(2, p, i, j, k)] = 0.0;
+    s.ent[d.at(3, p, i, j, k)] = 0.0;
+    // Modes 2..10 stay zero wherever the P12 steps do not write them.
+    const int lo = 3 - d.G, hx = d.N + d.G - 2, hz = d.nr + d.G - 2;
+    const bool full = m == 1 && i >= lo && i <= hx && j >= lo && j <= hx && k >= lo && k <= hz;
+    if (!full)
+      for (int q = NVAR; q < NVAR * NMODE; ++q) s.V[d.at(q, p, i, j, k)] = 0.0;
+    const double a12 = (V[5] * V[5] + V[6] * V[6] + V[7] * V[7]) * ph.ob4pi;
+    s.msonic[d.at(0, p, i, j, k)] = sqrt((ph.gamma * V[4] + a12) / V[0]);
+  }
+}
+
+// Masked-face zeroing (421:658-759; 485:383-484).
+__global__ void k_zero_masked_faces(Dims d, DGeom g, DState s, Range3 r) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
+    int p, i, j, k;
+    r.decode(t, p, i, j, k);
+    const int lo = 1 - d.G, hi = d.N + d.G;
+    if (k >= lo && j >= lo && mask_at(g, d, p, max(i, lo), j) == 0 && mask_at(g, d, p, min(i + 1, hi), j) == 0)
+      s.Bxf[d.at(0, p, i, j, k)] = 0.0;
+    if (k >= lo && i >= lo && mask_at(g, d, p, i, max(j, lo)) == 0 && mask_at(g, d, p, i, min(j + 1, hi)) == 0)
+      s.Byf[d.at(0, p, i, j, k)] = 0.0;
+    if (i >= lo && j >= lo && mask_at(g, d, p, i, j) == 0) s.Bzf[d.at(0, p, i, j, k)] = 0.0;
+  }
+}
+
+// Tri-corner face-B synchronisation (421:779-962; 485:504-687).  One
+// thread per (panel, corner, ghost column, k).
+__global__ void k_tricorner(Dims d, DGeom g, DState s) {
+  const long long n = 6LL * 4 * d.G * (d.NK - 1);
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    long long u = t;
+    const int k = (int)(u % (d.NK - 1)) + 1 - d.G;
+    u /= (d.NK - 1);
+    const int col = (int)(u % d.G);
+    u /= d.G;
+    const int corner = (int)(u % 4);
+    const int p = (int)(u / 4);
+    const int N = d.N;
+    if (corner == 0) {  // LD
+      const int i = 1 - d.G + col;
+      const int xd = sten(g, d, p, i, 1, 3, 0), yd = sten(g, d, p, i, 1, 3, 1);
+      double& a = s.Byf[d.at(0, p, i, 0, k)];
+      double& b = s.Bxf[d.at(0, p, xd - 1, yd, k)];
+      const double a11 = 0.5 * (a - b);
+      a = a11;
+      b = -a11;
+    } else if (corner == 1) {  // RD
+      const int i = N + 1 + col;
+      const int xd = sten(g, d, p, i, 1, 3, 0), yd = sten(g, d, p, i, 1, 3, 1);
+      double& a = s.Byf[d.at(0, p, i, 0, k)];
+      double& b = s.Bxf[d.at(0, p, xd, yd, k)];
+      const double a11 = 0.5 * (a + b);
+      a = a11;
+      b = a11;
+    } else if (corner == 2) {  // RU
+      const int i = N + 1 + col;
+      const int xu = sten(g, d, p, i, N, 2, 0), yu = sten(g, d, p, i, N, 2, 1);
+      double& a = s.Byf[d.at(0, p, i, N, k)];
+      double& b = s.Bxf[d.at(0, p, xu, yu, k)];
+      const double a11 = 0.5 * (a - b);
+      a = a11;
+      b = -a11;
+    } else {  // LU
+      const int i = 1 - d.G + col;
+      const int xu = sten(g, d, p, i, N, 2, 0), yu = sten(g, d, p, i, N, 2, 1);
+      double& a = s.Byf[d.at(0, p, i, N, k)];
+      double& b = s.Bxf[d.at(0, p, xu - 1, yu, k)];
+      const double a11 = 0.5 * (a + b);
+      a = a11;
+      b = a11;
+    }
+  }
+}
+
+// STEP 6.a (421:1837-2131): velocity divergence and the divergence flattener.
+__global__ void k_flat_a(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
+    int p, i, j, k;
+    r.decode(t, p, i, j, k);
+    const int lo = 2 - d.G, hx = d.N + d.G - 1, hz = d.nr + d.G - 1;
+    double fl = 0.0;
+    if (i >= lo && i <= hx && j >= lo && j <= hx && k >= lo && k <= hz) {
+      const int xr = sten(g, d, p, i, j, 0, 0), yr = sten(g, d, p, i, j, 0, 1);
+      const int xl = sten(g, d, p, i, j, 1, 0), yl = sten(g, d, p, i, j, 1, 1);
+      const int xu = sten(g, d, p, i, j, 2, 0), yu = sten(g, d, p, i, j, 2, 1);
+      const int xd = sten(g, d, p, i, j, 3, 0), yd = sten(g, d, p, i, j, 3, 1);
+      const double obl0 = 1.0 / fmax(geo(g, d, CS_G_V_SCALE, 0, p, i, j, k), ph.smallnum);
+      const double* ms = s.msonic;
+      double w = ms[d.at(0, p, i, j, k)];
+      w = fmin(w, ms[d.at(0, p, xr, yr, k)]);
+      w = fmin(w, ms[d.at(0, p, xl, yl, k)]);
+      w = fmin(w, ms[d.at(0, p, xu, yu, k)]);
+      w = fmin(w, ms[d.at(0, p, xd, yd, k)]);
+      w = fmin(w, ms[d.at(0, p, i, j, k + 1)]);
+      w = fmin(w, ms[d.at(0, p, i, j, k - 1)]);
+      double dv = 0.0;
+      auto term = [&](int ax, int ay, int az, int bx, int by, int bz, double nx, double ny, double nz) {
+        const double x = (geo(g, d, CS_G_V_CEN, 0, p, bx, by, bz) - geo(g, d, CS_G_V_CEN, 0, p, ax, ay, az)) * obl0;
+        const double y = (geo(g, d, CS_G_V_CEN, 1, p, bx, by, bz) - geo(g, d, CS_G_V_CEN, 1, p, ax, ay, az)) * obl0;
+        const double z = (geo(g, d, CS_G_V_CEN, 2, p, bx, by, bz) - geo(g, d, CS_G_V_CEN, 2, p, ax, ay, az)) * obl0;
+        const double a11 = 0.5 / fmax(sqrt(x * x + y * y + z * z), ph.smallnum);
+        dv = dv + nx * a11 * (Vat(s, d, 1, 0, p, bx, by, bz) - Vat(s, d, 1, 0, p, ax, ay, az)) +
+             ny * a11 * (Vat(s, d, 2, 0, p, bx, by, bz) - Vat(s, d, 2, 0, p, ax, ay, az)) +
+             nz * a11 * (Vat(s, d, 3, 0, p, bx, by, bz) - Vat(s, d, 3, 0, p, ax, ay, az));
+      };
+      term(i, j, k, xr, yr, k, geo(g, d, CS_G_XF_N, 0, p, i, j, k), geo(g, d, CS_G_XF_N, 1, p, i, j, k),
+           geo(g, d, CS_G_XF_N, 2, p, i, j, k));
+      term(xl, yl, k, i, j, k, geo(g, d, CS_G_XF_N, 0, p, i - 1, j, k), geo(g, d, CS_G_XF_N, 1, p, i - 1, j, k),
+           geo(g, d, CS_G_XF_N, 2, p, i - 1, j, k));
+      term(i, j, k, xu, yu, k, geo(g, d, CS_G_YF_N, 0, p, i, j, k), geo(g, d, CS_G_YF_N, 1, p, i, j, k),
+           geo(g, d, CS_G_YF_N, 2, p, i, j, k));
+      term(xd, yd, k, i, j, k, geo(g, d, CS_G_YF_N, 0, p, i, j - 1, k), geo(g, d, CS_G_YF_N, 1, p, i, j - 1, k),
+           geo(g, d, CS_G_YF_N, 2, p, i, j - 1, k));
+      double nx = geo(g, d, CS_G_ZF_CEN, 0, p, i, j, k), ny = geo(g, d, CS_G_ZF_CEN, 1, p, i, j, k),
+             nz = geo(g, d, CS_G_ZF_CEN, 2, p, i, j, k);
+      const double a12 = 1.0 / fmax(sqrt(nx * nx + ny * ny + nz * nz), ph.smallnum);
+      nx = nx * a12;
+      ny = ny * a12;
+      nz = nz * a12;
+      term(i, j, k, i, j, k + 1, nx, ny, nz);
+      term(i, j, k - 1, i, j, k, nx, ny, nz);
+      double a13 = fabs(dv) / (ph.flatten_coef * w);
+      a13 = a13 - 1.0;
+      fl = (a13 <= 0.0) ? 0.0 : fmin(1.0, a13);
+      if (mask_at(g, d, p, i, j) != 1) fl = 0.0;
+    }
+    s.flatA[d.at(0, p, i, j, k)] = fl;
+  }
+}
+
+// STEP 6.b (pressure-ratio raise, pass 0) and 6.c (upwinding, pass 1),
+// 421:2150-2458: dst(self) = max over the six neighbours of src.
+__global__ void k_flat_bc(Dims d, PhysC ph, DGeom g, DState s, Range3 r, const double* src, double* dst, int pass) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
+    int p, i, j, k;
+    r.decode(t, p, i, j, k);
+    const int lo = 2 - d.G, hx = d.N + d.G - 1, hz = d.nr + d.G - 1;
+    double fl = src[d.at(0, p, i, j, k)];
+    if (i >= lo && i <= hx && j >= lo && j <= hx && k >= lo && k <= hz) {
+      int xs[6], ys[6];
+#pragma unroll
+      for (int w = 0; w < 4; ++w) {
+        xs[w] = sten(g, d, p, i, j, w, 0);
+        ys[w] = sten(g, d, p, i, j, w, 1);
+      }
+      xs[4] = xs[5] = i;
+      ys[4] = ys[5] = j;
+      const int zs[6] = {k, k, k, k, k + 1, k - 1};
+      const double p0 = Vat(s, d, 4, 0, p, i, j, k);
+#pragma unroll
+      for (int w = 0; w < 6; ++w) {
+        const bool take = pass == 1 || (Vat(s, d, 4, 0, p, xs[w], ys[w], zs[w]) > ph.prs_flatten_coef * p0);
+        if (take) fl = fmax(fl, src[d.at(0, p, xs[w], ys[w], zs[w])]);
+      }
+    }
+    dst[d.at(0, p, i, j, k)] = fl;
+  }
+}
+
+// Stencils of STEP 7.a: (neighbour in plane, neighbour in plane, dz).
+__constant__ int c_st8[8][3] = {{0, 2, 1}, {0, 2, -1}, {1, 2, 1}, {1, 2, -1}, {0, 3, 1}, {0, 3, -1}, {1, 3, 1}, {1, 3, -1}};
+// Central 18-zone stencil of STEP 7.b / 9.c: (neighbour w or -1 for self, dz).
+__constant__ int c_n18[18][2] = {{0, 0},  {1, 0},  {2, 0},  {3, 0},  {-1, 1}, {-1, -1}, {8, 0}, {9, 0},  {10, 0},
+                                 {11, 0}, {0, 1},  {1, 1},  {0, -1}, {1, -1}, {2, 1},   {3, 1}, {2, -1}, {3, -1}};
+
+struct Nbr12 {
+  int x[12], y[12];
+};
+__device__ __forceinline__ Nbr12 load_nbr(const DGeom& g, const Dims& d, int p, int i, int j) {
+  Nbr12 n;
+#pragma unroll
+  for (int w = 0; w < 12; ++w) {
+    n.x[w] = sten(g, d, p, i, j, w, 0);
+    n.y[w] = sten(g, d, p, i, j, w, 1);
+  }
+  return n;
+}
+
+__device__ void stencil_inv(const Dims& d, const PhysC& ph, const DGeom& g, int p, int i, int j, int k, const Nbr12& n,
+                            double Ai[8][9]) {
+  const double obl0 = 1.0 / fmax(geo(g, d, CS_G_V_SCALE, 0, p, i, j, k), ph.smallnum);
+  const double cx = geo(g, d, CS_G_V_CEN, 0, p, i, j, k), cy = geo(g, d, CS_G_V_CEN, 1, p, i, j, k),
+               cz = geo(g, d, CS_G_V_CEN, 2, p, i, j, k);
+#pragma unroll
+  for (int st = 0; st < 8; ++st) {
+    const int w1 = c_st8[st][0], w2 = c_st8[st][1], dz = c_st8[st][2];
+    const double a11 = (geo(g, d, CS_G_V_CEN, 0, p, n.x[w1], n.y[w1], k) - cx) * obl0;
+    const double a12 = (geo(g, d, CS_G_V_CEN, 1, p, n.x[w1], n.y[w1], k) - cy) * obl0;
+    const double a13 = (geo(g, d, CS_G_V_CEN, 2, p, n.x[w1], n.y[w1], k) - cz) * obl0;
+    const double a21 = (geo(g, d, CS_G_V_CEN, 0, p, n.x[w2], n.y[w2], k) - cx) * obl0;
+    const double a22 = (geo(g, d, CS_G_V_CEN, 1, p, n.x[w2], n.y[w2], k) - cy) * obl0;
+    const double a23 = (geo(g, d, CS_G_V_CEN, 2, p, n.x[w2], n.y[w2], k) - cz) * obl0;
+    const double a31 = (geo(g, d, CS_G_V_CEN, 0, p, i, j, k + dz) - cx) * obl0;
+    const double a32 = (geo(g, d, CS_G_V_CEN, 1, p, i, j, k + dz) - cy) * obl0;
+    const double a33 = (geo(g, d, CS_G_V_CEN, 2, p, i, j, k + dz) - cz) * obl0;
+    double ob = (-a13 * a22 * a31 + a12 * a23 * a31 + a13 * a21 * a32 - a11 * a23 * a32 - a12 * a21 * a33 + a11 * a22 * a33);
+    ob = copysign(1.0, ob) / fmax(1.0e-32, fabs(ob));
+    Ai[st][0] = (-a23 * a32 + a22 * a33) * ob;
+    Ai[st][1] = (a13 * a32 - a12 * a33) * ob;
+    Ai[st][2] = (-a13 * a22 + a12 * a23) * ob;
+    Ai[st][3] = (a23 * a31 - a21 * a33) * ob;
+    Ai[st][4] = (-a13 * a31 + a11 * a33) * ob;
+    Ai[st][5] = (a13 * a21 - a11 * a23) * ob;
+    Ai[st][6] = (-a22 * a31 + a21 * a32) * ob;
+    Ai[st][7] = (a12 * a31 - a11 * a32) * ob;
+    Ai[st][8] = (-a12 * a21 + a11 * a22) * ob;
+  }
+}
+
+// WENO of the eight linear stencils plus their mean (weight 100).
+__device__ void weno8(const Dims& d, const PhysC& ph, int p, int i, int j, int k, const Nbr12& n, const double Ai[8][9],
+                      const double* f, long long cstride_off, double gr[3]) {
+  const double f0 = f[cstride_off + d.idx(i, j, k)];
+  double X[3][9];
+#pragma unroll
+  for (int st = 0; st < 8; ++st) {
+    const int w1 = c_st8[st][0], w2 = c_st8[st][1], dz = c_st8[st][2];
+    const double R0 = f[cstride_off + d.idx(n.x[w1], n.y[w1], k)] - f0;
+    const double R1 = f[cstride_off + d.idx(n.x[w2], n.y[w2], k)] - f0;
+    const double R2 = f[cstride_off + d.idx(i, j, k + dz)] - f0;
+#pragma unroll
+    for (int rr = 0; rr < 3; ++rr) X[rr][st] = Ai[st][rr * 3 + 0] * R0 + Ai[st][rr * 3 + 1] * R1 + Ai[st][rr * 3 + 2] * R2;
+  }
+#pragma unroll
+  for (int rr = 0; rr < 3; ++rr)
+    X[rr][8] = 0.125 * (X[rr][0] + X[rr][1] + X[rr][2] + X[rr][3] + X[rr][4] + X[rr][5] + X[rr][6] + X[rr][7]);
+  double W[9];
+#pragma unroll
+  for (int st = 0; st < 9; ++st) {
+    const double IS = X[0][st] * X[0][st] + X[1][st] * X[1][st] + X[2][st] * X[2][st];
+    const double t = IS + ph.smallnum;
+    const double t2 = t * t;
+    W[st] = (st < 8 ? 1.0 : 100.0) / (t2 * t2);
+  }
+  const double a11 = 1.0 / (W[0] + W[1] + W[2] + W[3] + W[4] + W[5] + W[6] + W[7] + W[8]);
+#pragma unroll
+  for (int st = 0; st < 9; ++st) W[st] = W[st] * a11;
+#pragma unroll
+  for (int rr = 0; rr < 3; ++rr) {
+    double t = W[0] * X[rr][0];
+#pragma unroll
+    for (int st = 1; st < 9; ++st) t = t + W[st] * X[rr][st];
+    gr[rr] = t;
+  }
+}
+
+// STEP 7.a (421:2515-3804): linear WENO slopes of the 8 primitives and the entropy.
+__global__ void k_weno7a(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
+    int p, i, j, k;
+    r.decode(t, p, i, j, k);
+    if (mask_at(g, d, p, i, j) != 1) continue;
+    const Nbr12 n = load_nbr(g, d, p, i, j);
+    double Ai[8][9];
+    stencil_inv(d, ph, g, p, i, j, k, n, Ai);
+    for (int q = 0; q < NVAR; ++q) {
+      double gr[3];
+      weno8(d, ph, p, i, j, k, n, Ai, s.V, ((long long)(0 * NVAR + q) * NPANEL + p) * d.S, gr);
+      Vat(s, d, q, 1, p, i, j, k) = gr[0];
+      Vat(s, d, q, 2, p, i, j, k) = gr[1];
+      Vat(s, d, q, 3, p, i, j, k) = gr[2];
+    }
+    double gr[3];
+    weno8(d, ph, p, i, j, k, n, Ai, s.ent, (long long)p * d.S, gr);
+    const double om = 1.0 - s.flatA[d.at(0, p, i, j, k)];
+    s.ent[d.at(1, p, i, j, k)] = gr[0] * om;
+    s.ent[d.at(2, p, i, j, k)] = gr[1] * om;
+    s.ent[d.at(3, p, i, j, k)] = gr[2] * om;
+  }
+}
+
+__device__ __forceinline__ void coef10(const DGeom& g, const Dims& d, int p, int i, int j, int k, double* c) {
+#pragma unroll
+  for (int t = 0; t < 10; ++t) c[t] = geo(g, d, CS_G_COEF, t, p, i, j, k);
+}
+
+// STEP 7.b (421:3869-4551): 18-zone quadratic least squares hybridised
+// with the linear WENO slopes (MRWENO weights, flattener damping).
+__global__ void __launch_bounds__(TPB) k_weno7b(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
+  const double ob12 = 1.0 / 12.0, ob180 = 1.0 / 180.0, ob144 = 1.0 / 144.0;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
+    int p, i, j, k;
+    r.decode(t, p, i, j, k);
+    if (mask_at(g, d, p, i, j) != 1) continue;
+    const Nbr12 n = load_nbr(g, d, p, i, j);
+    const double l0 = fmax(geo(g, d, CS_G_V_SCALE, 0, p, i, j, k), ph.smallnum), obl0 = 1.0 / l0;
+    double c0[10];
+    coef10(g, d, p, i, j, k, c0);
+    const double cx = geo(g, d, CS_G_V_CEN, 0, p, i, j, k), cy = geo(g, d, CS_G_V_CEN, 1, p, i, j, k),
+                 cz = geo(g, d, CS_G_V_CEN, 2, p, i, j, k);
+    double A[18][9];
+    long long off[18];
+    for (int rr = 0; rr < 18; ++rr) {
+      const int w = c_n18[rr][0], dz = c_n18[rr][1];
+      const int zx = w < 0 ? i : n.x[w], zy = w < 0 ? j : n.y[w], zz = k + dz;
+      off[rr] = d.idx(zx, zy, zz);
+      const double x = (geo(g, d, CS_G_V_CEN, 0, p, zx, zy, zz) - cx) * obl0;
+      const double y = (geo(g, d, CS_G_V_CEN, 1, p, zx, zy, zz) - cy) * obl0;
+      const double z = (geo(g, d, CS_G_V_CEN, 2, p, zx, zy, zz) - cz) * obl0;
+      const double lj = fmax(geo(g, d, CS_G_V_SCALE, 0, p, zx, zy, zz), ph.smallnum);
+      const double rt = lj / l0, r2 = rt * rt;
+      A[rr][0] = x;
+      A[rr][1] = y;
+      A[rr][2] = z;
+      A[rr][3] = x * x - c0[4] + geo(g, d, CS_G_COEF, 4, p, zx, zy, zz) * r2;
+      A[rr][4] = y * y - c0[5] + geo(g, d, CS_G_COEF, 5, p, zx, zy, zz) * r2;
+      A[rr][5] = z * z - c0[6] + geo(g, d, CS_G_COEF, 6, p, zx, zy, zz) * r2;
+      A[rr][6] = x * y - c0[7] + geo(g, d, CS_G_COEF, 7, p, zx, zy, zz) * r2;
+      A[rr][7] = y * z - c0[8] + geo(g, d, CS_G_COEF, 8, p, zx, zy, zz) * r2;
+      A[rr][8] = x * z - c0[9] + geo(g, d, CS_G_COEF, 9, p, zx, zy, zz) * r2;
+    }
+    double M[81], Minv[81];
+#pragma unroll
+    for (int a = 0; a < 9; ++a)
+#pragma unroll
+      for (int b = 0; b < 9; ++b) {
+        double sacc = 0.0;
+#pragma unroll
+        for (int rr = 0; rr < 18; ++rr) sacc = sacc + A[rr][a] * A[rr][b];
+        M[a * 9 + b] = sacc;
+      }
+    d_matinv<9>(M, Minv);
+    const double f = s.flatA[d.at(0, p, i, j, k)];
+    const double betalo = f + (1.0 - f) * 2.0;
+    const double ghi = f * 0.6 + (1.0 - f) * 0.95, glo = 1.0 - ghi, obghi = 1.0 / ghi, grat = glo / ghi;
+    for (int q = 0; q < NVAR; ++q) {
+      const double* Vq = s.V + ((long long)q * NPANEL + p) * d.S;
+      const double v0 = Vq[d.idx(i, j, k)];
+      double Y[9];
+#pragma unroll
+      for (int a = 0; a < 9; ++a) Y[a] = 0.0;
+#pragma unroll
+      for (int rr = 0; rr < 18; ++rr) {
+        const double R = Vq[off[rr]] - v0;
+#pragma unroll
+        for (int a = 0; a < 9; ++a) Y[a] = Y[a] + A[rr][a] * R;
+      }
+      double X[9];
+#pragma unroll
+      for (int a = 0; a < 9; ++a) {
+        double sacc = 0.0;
+#pragma unroll
+        for (int b = 0; b < 9; ++b) sacc = sacc + Minv[a * 9 + b] * Y[b];
+        X[a] = sacc;
+      }
+      const double v2 = Vat(s, d, q, 1, p, i, j, k), v3 = Vat(s, d, q, 2, p, i, j, k), v4 = Vat(s, d, q, 3, p, i, j, k);
+      const double ISlo = betalo * (v2 * v2 + v3 * v3 + v4 * v4) * ob12;
+      double Phi[9];
+      Phi[0] = X[0] * obghi - v2 * grat;
+      Phi[1] = X[1] * obghi - v3 * grat;
+      Phi[2] = X[2] * obghi - v4 * grat;
+#pragma unroll
+      for (int a = 3; a < 9; ++a) Phi[a] = X[a] * obghi;
+      const double IShi = (Phi[0] * Phi[0] + Phi[1] * Phi[1] + Phi[2] * Phi[2]) * ob12 +
+                          (Phi[3] * Phi[3]) * (sqr(c0[4] - ob12) + ob180) + (Phi[4] * Phi[4]) * (sqr(c0[5] - ob12) + ob180) +
+                          (Phi[5] * Phi[5]) * (sqr(c0[6] - ob12) + ob180) + (Phi[6] * Phi[6]) * (c0[7] * c0[7] + ob144) +
+                          (Phi[7] * Phi[7]) * (c0[8] * c0[8] + ob144) + (Phi[8] * Phi[8]) * (c0[9] * c0[9] + ob144);
+      const double tau = fabs(IShi - ISlo);
+      double Wlo = glo * (1.0 + tau / (ISlo + ph.smallnum)), Whi = ghi * (1.0 + tau / (IShi + ph.smallnum));
+      const double aa = 1.0 / (Wlo + Whi);
+      Wlo = Wlo * aa;
+      Whi = Whi * aa;
+      const double x = 1.0 - f;
+      Vat(s, d, q, 1, p, i, j, k) = (Whi * Phi[0] + Wlo * v2) * x;
+      Vat(s, d, q, 2, p, i, j, k) = (Whi * Phi[1] + Wlo * v3) * x;
+      Vat(s, d, q, 3, p, i, j, k) = (Whi * Phi[2] + Wlo * v4) * x;
+#pragma unroll
+      for (int m = 4; m < 10; ++m) Vat(s, d, q, m, p, i, j, k) = (Whi * Phi[m - 1]) * x;
+    }
+  }
+}
+
+// STEP 7.c (440:204-829): shrink the higher modes until the 27 nodal
+// values of density, pressure and entropy lie in the expanded local range.
+__global__ void __launch_bounds__(TPB) k_positivity(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
+    int p, i, j, k;
+    r.decode(t, p, i, j, k);
+    const int lo = 2 - d.G, hx = d.N + d.G - 1, hz = d.nr + d.G - 1;
+    if (!(i >= lo && i <= hx && j >= lo && j <= hx && k >= lo && k <= hz)) {
+      s.giveup[d.at(0, p, i, j, k)] = 0;
+      continue;
+    }
+    const Nbr12 n = load_nbr(g, d, p, i, j);
+    const int px[9] = {i, n.x[0], n.x[1], n.x[2], n.x[3], n.x[8], n.x[9], n.x[10], n.x[11]};
+    const int py[9] = {j, n.y[0], n.y[1], n.y[2], n.y[3], n.y[8], n.y[9], n.y[10], n.y[11]};
+    double mn0 = 1e300, mx0 = -1e300, mn4 = 1e300, mx4 = -1e300, emin = 1e300, emax = -1e300;
+    for (int a = 0; a < 9; ++a)
+      for (int dz = -1; dz <= 1; ++dz) {
+        const long long o = d.idx(px[a], py[a], k + dz);
+        const double v0 = s.V[((long long)0 * NPANEL + p) * d.S + o], v4 = s.V[((long long)4 * NPANEL + p) * d.S + o];
+        const double e = s.ent[(long long)p * d.S + o];
+        mn0 = fmin(mn0, v0);
+        mx0 = fmax(mx0, v0);
+        mn4 = fmin(mn4, v4);
+        mx4 = fmax(mx4, v4);
+        emin = fmin(emin, e);
+        emax = fmax(emax, e);
+      }
+    const double ef = 0.2;
+    const double ff = fmax(fmin((s.flatA[d.at(0, p, i, j, k)] - 0.1) / 0.4, 1.0), 0.0), omff = 1.0 - ff;
+    mn0 = fmax(mn0 * (1.0 - ef * omff), ph.rhofloor);
+    mx0 = fmax(mx0 * (1.0 + ef * omff), ph.rhofloor);
+    mn4 = fmax(mn4 * (1.0 - ef * omff), ph.prsfloor);
+    mx4 = fmax(mx4 * (1.0 + ef * omff), ph.prsfloor);
+    emin = emin * (1.0 - ef * omff);
+    emax = emax * (1.0 + ef * omff);
+    const double obl0 = 1.0 / fmax(geo(g, d, CS_G_V_SCALE, 0, p, i, j, k), ph.smallnum);
+    const double vc[3] = {geo(g, d, CS_G_V_CEN, 0, p, i, j, k), geo(g, d, CS_G_V_CEN, 1, p, i, j, k),
+                          geo(g, d, CS_G_V_CEN, 2, p, i, j, k)};
+    double c0[10];
+    coef10(g, d, p, i, j, k, c0);
+    double vr[10], vp[10], ep[4];
+#pragma unroll
+    for (int m = 0; m < 10; ++m) {
+      vr[m] = Vat(s, d, 0, m, p, i, j, k);
+      vp[m] = Vat(s, d, 4, m, p, i, j, k);
+    }
+#pragma unroll
+    for (int m = 0; m < 4; ++m) ep[m] = s.ent[d.at(m, p, i, j, k)];
+    // the 27 nodes: 8 vertices, 6 face centroids, 12 edge midpoints, centroid
+    double xyz[27][3];
+    {
+      double v8[8][3];
+      const int vi[8] = {i - 1, i, i - 1, i, i - 1, i, i - 1, i}, vj[8] = {j - 1, j - 1, j, j, j - 1, j - 1, j, j},
+                vk[8] = {k - 1, k - 1, k - 1, k - 1, k, k, k, k};
+      for (int a = 0; a < 8; ++a)
+        for (int q = 0; q < 3; ++q) v8[a][q] = geo(g, d, CS_G_VERT, q, p, vi[a], vj[a], vk[a]);
+      for (int a = 0; a < 8; ++a)
+        for (int q = 0; q < 3; ++q) xyz[a][q] = v8[a][q];
+      for (int q = 0; q < 3; ++q) {
+        xyz[8][q] = geo(g, d, CS_G_XF_CEN, q, p, i, j, k);
+        xyz[9][q] = geo(g, d, CS_G_XF_CEN, q, p, i - 1, j, k);
+        xyz[10][q] = geo(g, d, CS_G_YF_CEN, q, p, i, j, k);
+        xyz[11][q] = geo(g, d, CS_G_YF_CEN, q, p, i, j - 1, k);
+        xyz[12][q] = geo(g, d, CS_G_ZF_CEN, q, p, i, j, k);
+        xyz[13][q] = geo(g, d, CS_G_ZF_CEN, q, p, i, j, k - 1);
+      }
+      const int pr[12][2] = {{0, 1}, {2, 3}, {4, 5}, {6, 7}, {0, 2}, {1, 3}, {4, 6}, {5, 7}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
+      for (int e = 0; e < 12; ++e)
+        for (int q = 0; q < 3; ++q) xyz[14 + e][q] = (v8[pr[e][0]][q] + v8[pr[e][1]][q]) * 0.5;
+      for (int q = 0; q < 3; ++q) xyz[26][q] = vc[q];
+      for (int a = 0; a < 27; ++a)
+        for (int q = 0; q < 3; ++q) xyz[a][q] = (xyz[a][q] - vc[q]) * obl0;
+    }
+    const int niter = 15;
+    const double ratio = pow(0.10, 1.0 / (double)niter);
+    double scale = 1.0;  // cumulative shrink of the higher modes
+    int gave_up = 0;
+    for (int iter = 1; iter <= niter + 1; ++iter) {
+      if (iter == niter + 1) {
+        gave_up = 1;
+        break;
+      }
+      bool pass = true;
+      for (int a = 0; a < 27 && pass; ++a) {
+        const double x = xyz[a][0], y = xyz[a][1], z = xyz[a][2];
+        const double v1 = d_poly10(vr, c0, x, y, z), v5 = d_poly10(vp, c0, x, y, z);
+        const double en = ep[0] + ep[1] * x + ep[2] * y + ep[3] * z;
+        if (v1 < mn0 || v1 > mx0 || v5 < mn4 || v5 > mx4 || en < emin || en > emax) pass = false;
+      }
+      if (pass) break;
+#pragma unroll
+      for (int m = 1; m < 10; ++m) {
+        vr[m] = ratio * vr[m];
+        vp[m] = ratio * vp[m];
+      }
+#pragma unroll
+      for (int m = 1; m < 4; ++m) ep[m] = ratio * ep[m];
+      scale = scale + 1.0;  // counts the shrinks applied
+    }
+    const int nshrink = (int)(scale - 1.0);
+    if (gave_up || nshrink > 0) {
+      for (int q = 0; q < NVAR; ++q)
+        for (int m = 1; m < 10; ++m) {
+          double v = Vat(s, d, q, m, p, i, j, k);
+          if (gave_up) {
+            v = 0.0;
+          } else {
+            for (int it = 0; it < nshrink; ++it) v = ratio * v;
+          }
+          Vat(s, d, q, m, p, i, j, k) = v;
+        }
+      for (int m = 1; m < 4; ++m) s.ent[d.at(m, p, i, j, k)] = gave_up ? 0.0 : ep[m];
+    }
+    s.giveup[d.at(0, p, i, j, k)] = gave_up;
+  }
+}
+
+// A zone that exhausted the shrink passes also zeroes its entropy value
+// (440:569-575); applied after every zone has read its neighbours.
+__global__ void k_apply_giveup(Dims d, DState s, Range3 r) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
+    int p, i, j, k;
+    r.decode(t, p, i, j, k);
+    if (s.giveup[d.at(0, p, i, j, k)]) s.ent[d.at(0, p, i, j, k)] = 0.0;
+  }
+}
+
+// STEP 8.a-c (421:4686-5567): B at the five quadrature points of each face,
+// averaged from both sides and shifted to the facial mean.
+__global__ void __launch_bounds__(TPB) k_faceB(Dims d, PhysC ph, DGeom g, DState s, Range3 r, int dir) {
+  const int QP = dir == 0 ? CS_G_XF_QP : (dir == 1 ? CS_G_YF_QP : CS_G_ZF_QP);
+  const int BW = dir == 0 ? CS_G_XB_QW : (dir == 1 ? CS_G_YB_QW : CS_G_ZB_QW);
+  const int NF = dir == 0 ? CS_G_XF_N : (dir == 1 ? CS_G_YF_N : CS_G_ZF_N);
+  double* Bq = s.Bq[dir];
+  const double* Bf = dir == 0 ? s.Bxf : (dir == 1 ? s.Byf : s.Bzf);
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
+    int p, i, j, k;
+    r.decode(t, p, i, j, k);
+    int lx = i, ly = j, lz = k, rx = i, ry = j, rz = k;
+    bool skip = false;
+    if (dir == 0) {
+      const int mL = mask_at(g, d, p, i, j), mR = mask_at(g, d, p, i + 1, j);
+      rx = i + 1;
+      if (mL == 0 && mR == 1) { lx = sten(g, d, p, rx, ry, 1, 0); ly = sten(g, d, p, rx, ry, 1, 1); }
+      else if (mL == 1 && mR == 0) { rx = sten(g, d, p, lx, ly, 0, 0); ry = sten(g, d, p, lx, ly, 0, 1); }
+      else if (mL == 0 && mR == 0) skip = true;
+    } else if (dir == 1) {
+      const int mL = mask_at(g, d, p, i, j), mR = mask_at(g, d, p, i, j + 1);
+      ry = j + 1;
+      if (mL == 0 && mR == 1) { lx = sten(g, d, p, rx, ry, 3, 0); ly = sten(g, d, p, rx, ry, 3, 1); }
+      else if (mL == 1 && mR == 0) { rx = sten(g, d, p, lx, ly, 2, 0); ry = sten(g, d, p, lx, ly, 2, 1); }
+      else if (mL == 0 && mR == 0) skip = true;
+    } else {
+      if (mask_at(g, d, p, i, j) == 0) skip = true;
+      rz = k + 1;
+    }
+    double bq[5] = {0, 0, 0, 0, 0};
+    if (!skip) {
+      const double obl0 = 1.0 / fmax(geo(g, d, CS_G_V_SCALE, 0, p, lx, ly, lz), ph.smallnum);
+      const double obl02 = 1.0 / fmax(geo(g, d, CS_G_V_SCALE, 0, p, rx, ry, rz), ph.smallnum);
+      double cL[10], cR[10], vL[3][10], vR[3][10];
+      coef10(g, d, p, lx, ly, lz, cL);
+      coef10(g, d, p, rx, ry, rz, cR);
+#pragma unroll
+      for (int b = 0; b < 3; ++b)
+#pragma unroll
+        for (int m = 0; m < 10; ++m) {
+          vL[b][m] = Vat(s, d, 5 + b, m, p, lx, ly, lz);
+          vR[b][m] = Vat(s, d, 5 + b, m, p, rx, ry, rz);
+        }
+      const double lcx = geo(g, d, CS_G_V_CEN, 0, p, lx, ly, lz), lcy = geo(g, d, CS_G_V_CEN, 1, p, lx, ly, lz),
+                   lcz = geo(g, d, CS_G_V_CEN, 2, p, lx, ly, lz);
+      const double rcx = geo(g, d, CS_G_V_CEN, 0, p, rx, ry, rz), rcy = geo(g, d, CS_G_V_CEN, 1, p, rx, ry, rz),
+                   rcz = geo(g, d, CS_G_V_CEN, 2, p, rx, ry, rz);
+#pragma unroll
+      for (int q = 0; q < 5; ++q) {
+        const int nq = dir == 2 ? q : 0, ns = dir == 2 ? 5 : 1;
+        const double nx = geo(g, d, NF, 0 * ns + nq, p, i, j, k), ny = geo(g, d, NF, 1 * ns + nq, p, i, j, k),
+                     nz = geo(g, d, NF, 2 * ns + nq, p, i, j, k);
+        const double px = geo(g, d, QP, q, p, i, j, k), py = geo(g, d, QP, 5 + q, p, i, j, k),
+                     pz = geo(g, d, QP, 10 + q, p, i, j, k);
+        const double x = (px - lcx) * obl0, y = (py - lcy) * obl0, z = (pz - lcz) * obl0;
+        const double x2 = (px - rcx) * obl02, y2 = (py - rcy) * obl02, z2 = (pz - rcz) * obl02;
+        const double bx = d_poly10(vL[0], cL, x, y, z), by = d_poly10(vL[1], cL, x, y, z), bz = d_poly10(vL[2], cL, x, y, z);
+        const double bx2 = d_poly10(vR[0], cR, x2, y2, z2), by2 = d_poly10(vR[1], cR, x2, y2, z2),
+                     bz2 = d_poly10(vR[2], cR, x2, y2, z2);
+        bq[q] = 0.5 * (nx * (bx + bx2) + ny * (by + by2) + nz * (bz + bz2));
+      }
+    }
+    double bd = Bf[d.at(0, p, i, j, k)];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) bd = bd - geo(g, d, BW, q, p, i, j, k) * bq[q];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) Bq[d.at(q, p, i, j, k)] = bq[q] + bd;
+  }
+}
+
+// STEP 8.d ADP (421:5617-6677): constrained least squares for the 30
+// quadratic B modes matching the 6 face means exactly, solved per zone as
+// the 36x36 KKT system by one warp with Gaussian elimination (scaled
+// partial pivoting) in shared memory.
+constexpr int ADP_WARPS = 4;
+struct AdpSmem {
+  double K[36][37];
+  double Q[30][31];
+  double bq[30], wt[30], C[6][30], D[6], rhs[36], sol[36], sc[36], vB[30];
+  int piv[36];
+};
+
+__global__ void __launch_bounds__(32 * ADP_WARPS) k_adp(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
+  extern __shared__ unsigned char smem_raw[];
+  AdpSmem& S = reinterpret_cast<AdpSmem*>(smem_raw)[threadIdx.x / 32];
+  const int lane = threadIdx.x & 31;
+  const long long nw = (long long)gridDim.x * ADP_WARPS;
+  for (long long t = blockIdx.x * (long long)ADP_WARPS + threadIdx.x / 32; t < r.count(); t += nw) {
+    int p, i, j, k;
+    r.decode(t, p, i, j, k);
+    if (mask_at(g, d, p, i, j) == 0) continue;
+    const double obl0 = 1.0 / fmax(geo(g, d, CS_G_V_SCALE, 0, p, i, j, k), ph.smallnum);
+    const double vc0 = geo(g, d, CS_G_V_CEN, 0, p, i, j, k), vc1 = geo(g, d, CS_G_V_CEN, 1, p, i, j, k),
+                 vc2 = geo(g, d, CS_G_V_CEN, 2, p, i, j, k);
+    double c0[10];
+    coef10(g, d, p, i, j, k, c0);
+    // 1. the 30 quadrature rows, one per lane
+    if (lane < 30) {
+      const int f = lane / 5, q = lane % 5, dir = f / 2;
+      const int fx = (f == 1) ? i - 1 : i, fy = (f == 3) ? j - 1 : j, fz = (f == 5) ? k - 1 : k;
+      const int QP = dir == 0 ? CS_G_XF_QP : (dir == 1 ? CS_G_YF_QP : CS_G_ZF_QP);
+      const int BW = dir == 0 ? CS_G_XB_QW : (dir == 1 ? CS_G_YB_QW : CS_G_ZB_QW);
+      const int NF = dir == 0 ? CS_G_XF_N : (dir == 1 ? CS_G_YF_N : CS_G_ZF_N);
+      const int nq = dir == 2 ? q : 0, ns = dir == 2 ? 5 : 1;
+      const double nx = geo(g, d, NF, nq, p, fx, fy, fz), ny = geo(g, d, NF, ns + nq, p, fx, fy, fz),
+                   nz = geo(g, d, NF, 2 * ns + nq, p, fx, fy, fz);
+      const double x = (geo(g, d, QP, q, p, fx, fy, fz) - vc0) * obl0;
+      const double y = (geo(g, d, QP, 5 + q, p, fx, fy, fz) - vc1) * obl0;
+      const double z = (geo(g, d, QP, 10 + q, p, fx, fy, fz) - vc2) * obl0;
+      const double bfn[10] = {1.0, x, y, z, x * x - c0[4], y * y - c0[5], z * z - c0[6], x * y - c0[7], y * z - c0[8], x * z - c0[9]};
+#pragma unroll
+      for (int m = 0; m < 10; ++m) {
+        S.Q[lane][m] = m == 0 ? nx : nx * bfn[m];
+        S.Q[lane][10 + m] = m == 0 ? ny : ny * bfn[m];
+        S.Q[lane][20 + m] = m == 0 ? nz : nz * bfn[m];
+      }
+      S.wt[lane] = geo(g, d, BW, q, p, fx, fy, fz);
+      S.bq[lane] = s.Bq[dir][d.at(q, p, fx, fy, fz)];
+      S.vB[lane] = Vat(s, d, 5 + lane / 10, lane % 10, p, i, j, k);
+    }
+    __syncwarp();
+    // 2. constraint rows C, D and the KKT matrix
+    for (int e = lane; e < 180; e += 32) {
+      const int f = e / 30, m = e % 30;
+      double acc = 0.0;
+#pragma unroll
+      for (int q = 0; q < 5; ++q) acc = acc + S.wt[f * 5 + q] * S.Q[f * 5 + q][m];
+      S.C[f][m] = acc;
+    }
+    if (lane < 6) {
+      double acc = 0.0;
+#pragma unroll
+      for (int q = 0; q < 5; ++q) acc = acc + S.wt[lane * 5 + q] * S.bq[lane * 5 + q];
+      S.D[lane] = acc;
+    }
+    __syncwarp();
+    // divergence-free rows (421:6586-6600) as (column, value) pairs
+    const int dcol[4][3] = {{1, 12, 23}, {4, 17, 29}, {7, 15, 28}, {9, 18, 26}};
+    const double dval[4][3] = {{1.0, 1.0, 1.0}, {2.0, 1.0, 1.0}, {1.0, 2.0, 1.0}, {1.0, 1.0, 2.0}};
+    for (int e = lane; e < 900; e += 32) {
+      const int a = e / 30, b = e % 30;
+      double acc = 0.0;
+      for (int q = 0; q < 30; ++q) acc = acc + S.Q[q][a] * S.Q[q][b];
+      if (a == b) acc = acc + 1.0;
+      for (int rr = 0; rr < 4; ++rr) {
+        double va = 0.0, vb = 0.0;
+        for (int c = 0; c < 3; ++c) {
+          if (dcol[rr][c] == a) va = dval[rr][c];
+          if (dcol[rr][c] == b) vb = dval[rr][c];
+        }
+        acc = acc + va * vb;
+      }
+      S.K[a][b] = acc;
+    }
+    for (int e = lane; e < 180; e += 32) {
+      const int f = e / 30, m = e % 30;
+      S.K[m][30 + f] = S.C[f][m];
+      S.K[30 + f][m] = S.C[f][m];
+    }
+    for (int e = lane; e < 36; e += 32) {
+      S.K[30 + e / 6][30 + e % 6] = 0.0;
+    }
+    if (lane < 30) {
+      double acc = 0.0;
+      for (int q = 0; q < 30; ++q) acc = acc + S.Q[q][lane] * S.bq[q];
+      S.rhs[lane] = acc + S.vB[lane];
+    } else {
+      for (int f = lane - 30; f < 6; f += 2) S.rhs[30 + f] = S.D[f];
+    }
+    __syncwarp();
+    // 3. elimination with scaled partial pivoting
+    for (int row = lane; row < 36; row += 32) {
+      double m = 0.0;
+      for (int c = 0; c < 36; ++c) m = fmax(m, fabs(S.K[row][c]));
+      S.sc[row] = (m == 0.0) ? 0.0 : 1.0 / m;
+      S.piv[row] = row;
+    }
+    __syncwarp();
+    for (int kk = 0; kk < 36; ++kk) {
+      double best = -1.0;
+      int bi = kk;
+      for (int row = kk + lane; row < 36; row += 32) {
+        const double v = fabs(S.K[row][kk]) * S.sc[row];
+        if (v > best) {
+          best = v;
+          bi = row;
+        }
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const double ob = __shfl_xor_sync(0xffffffffu, best, off);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+        if (ob > best || (ob == best && oi < bi)) {
+          best = ob;
+          bi = oi;
+        }
+      }
+      if (bi != kk) {
+        for (int c = lane; c < 36; c += 32) {
+          const double tmp = S.K[kk][c];
+          S.K[kk][c] = S.K[bi][c];
+          S.K[bi][c] = tmp;
+        }
+        if (lane == 0) {
+          const double ts = S.sc[kk];
+          S.sc[kk] = S.sc[bi];
+          S.sc[bi] = ts;
+          const int tp = S.piv[kk];
+          S.piv[kk] = S.piv[bi];
+          S.piv[bi] = tp;
+        }
+      }
+      __syncwarp();
+      if (lane == 0 && S.K[kk][kk] == 0.0) S.K[kk][kk] = 1.0e-20;
+      __syncwarp();
+      const double inv = 1.0 / S.K[kk][kk];
+      for (int row = kk + 1 + lane; row < 36; row += 32) {
+        const double l = S.K[row][kk] * inv;
+        S.K[row][kk] = l;
+        for (int c = kk + 1; c < 36; ++c) S.K[row][c] -= l * S.K[kk][c];
+      }
+      __syncwarp();
+    }
+    // 4. substitution (one lane, reference order)
+    if (lane == 0) {
+      double y[36];
+      for (int a = 0; a < 36; ++a) {
+        double acc = S.rhs[S.piv[a]];
+        for (int b = 0; b < a; ++b) acc -= S.K[a][b] * y[b];
+        y[a] = acc;
+      }
+      for (int a = 35; a >= 0; --a) {
+        double acc = y[a];
+        for (int b = a + 1; b < 36; ++b) acc -= S.K[a][b] * S.sol[b];
+        S.sol[a] = acc / S.K[a][a];
+      }
+    }
+    __syncwarp();
+    // 5. write back the modes, zone B and the energy adjustment
+    if (lane < 30) Vat(s, d, 5 + lane / 10, lane % 10, p, i, j, k) = S.sol[lane];
+    if (lane == 0) {
+      double* U = s.U;
+      const long long o5 = d.at(4, p, i, j, k);
+      const double u6 = U[d.at(5, p, i, j, k)], u7 = U[d.at(6, p, i, j, k)], u8 = U[d.at(7, p, i, j, k)];
+      const double aa = (u6 * u6 + u7 * u7 + u8 * u8) * ph.ob8pi;
+      const double n6 = S.sol[0], n7 = S.sol[10], n8 = S.sol[20];
+      U[d.at(5, p, i, j, k)] = n6;
+      U[d.at(6, p, i, j, k)] = n7;
+      U[d.at(7, p, i, j, k)] = n8;
+      const double bb = (n6 * n6 + n7 * n7 + n8 * n8) * ph.ob8pi;
+      U[o5] = U[o5] - aa + bb;
+    }
+    __syncwarp();
+  }
+}
+
+// STEP 9.a (421:6700-6790): zone-centred E = -v x B from the point values.
+__global__ void k_efield_a(Dims d, DGeom g, DState s, Range3 r) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
+    int p, i, j, k;
+    r.decode(t, p, i, j, k);
+    double co[10];
+    coef10(g, d, p, i, j, k, co);
+    double pv[8];
+    for (int q = 1; q < 8; ++q) {
+      if (q == 4) continue;
+      double acc = Vat(s, d, q, 0, p, i, j, k);
+      for (int m = 4; m < 10; ++m) acc = acc - Vat(s, d, q, m, p, i, j, k) * co[m];
+      pv[q] = acc;
+    }
+    const double vx = pv[1], vy = pv[2], vz = pv[3], Bx = pv[5], By = pv[6], Bz = pv[7];
+    const double ex = -(vy * Bz - vz * By), ey = -(vz * Bx - vx * Bz), ez = -(vx * By - vy * Bx);
+    s.E[d.at(0, p, i, j, k)] = ex;
+    s.E[d.at(1, p, i, j, k)] = ey;
+    s.E[d.at(2, p, i, j, k)] = ez;
+    s.Esnap[d.at(0, p, i, j, k)] = ex;
+    s.Esnap[d.at(1, p, i, j, k)] = ey;
+    s.Esnap[d.at(2, p, i, j, k)] = ez;
+  }
+}
+
+// STEP 9.b (421:6840-8400): linear WENO slopes of the E point values.
+__global__ void k_efield_b(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
+    int p, i, j, k;
+    r.decode(t, p, i, j, k);
+    if (mask_at(g, d, p, i, j) != 1) continue;
+    const Nbr12 n = load_nbr(g, d, p, i, j);
+    double Ai[8][9];
+    stencil_inv(d, ph, g, p, i, j, k, n, Ai);
+    for (int q = 0; q < 3; ++q) {
+      double gr[3];
+      weno8(d, ph, p, i, j, k, n, Ai, s.Esnap, ((long long)q * NPANEL + p) * d.S, gr);
+      s.E[d.at(3 + q, p, i, j, k)] = gr[0];
+      s.E[d.at(6 + q, p, i, j, k)] = gr[1];
+      s.E[d.at(9 + q, p, i, j, k)] = gr[2];
+    }
+  }
+}
+
+// STEP 9.c (421:8464-9350): 19-point interpolation least squares
+// hybridised with the slopes; the point value is flattened toward E_pt.
+__global__ void __launch_bounds__(TPB) k_efield_c(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
+  const double ob12 = 1.0 / 12.0, ob180 = 1.0 / 180.0, ob144 = 1.0 / 144.0;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
+    int p, i, j, k;
+    r.decode(t, p, i, j, k);
+    if (mask_at(g, d, p, i, j) != 1) continue;
+    const Nbr12 n = load_nbr(g, d, p, i, j);
+    const double obl0 = 1.0 / fmax(geo(g, d, CS_G_V_SCALE, 0, p, i, j, k), ph.smallnum);
+    double c0[10];
+    coef10(g, d, p, i, j, k, c0);
+    const double cx = geo(g, d, CS_G_V_CEN, 0, p, i, j, k), cy = geo(g, d, CS_G_V_CEN, 1, p, i, j, k),
+                 cz = geo(g, d, CS_G_V_CEN, 2, p, i, j, k);
+    double A[19][10];
+    long long off[19];
+    off[0] = d.idx(i, j, k);
+    {
+      const double row0[10] = {1.0, 0.0, 0.0, 0.0, 0.0 * 0.0 - c0[4], 0.0 * 0.0 - c0[5], 0.0 * 0.0 - c0[6],
+                               0.0 * 0.0 - c0[7], 0.0 * 0.0 - c0[8], 0.0 * 0.0 - c0[9]};
+      for (int m = 0; m < 10; ++m) A[0][m] = row0[m];
+    }
+    for (int rr = 0; rr < 18; ++rr) {
+      const int w = c_n18[rr][0], dz = c_n18[rr][1];
+      const int zx = w < 0 ? i : n.x[w], zy = w < 0 ? j : n.y[w], zz = k + dz;
+      off[rr + 1] = d.idx(zx, zy, zz);
+      const double x = (geo(g, d, CS_G_V_CEN, 0, p, zx, zy, zz) - cx) * obl0;
+      const double y = (geo(g, d, CS_G_V_CEN, 1, p, zx, zy, zz) - cy) * obl0;
+      const double z = (geo(g, d, CS_G_V_CEN, 2, p, zx, zy, zz) - cz) * obl0;
+      A[rr + 1][0] = 1.0;
+      A[rr + 1][1] = x;
+      A[rr + 1][2] = y;
+      A[rr + 1][3] = z;
+      A[rr + 1][4] = x * x - c0[4];
+      A[rr + 1][5] = y * y - c0[5];
+      A[rr + 1][6] = z * z - c0[6];
+      A[rr + 1][7] = x * y - c0[7];
+      A[rr + 1][8] = y * z - c0[8];
+      A[rr + 1][9] = x * z - c0[9];
+    }
+    double M[100], Minv[100];
+    for (int a = 0; a < 10; ++a)
+      for (int b = 0; b < 10; ++b) {
+        double acc = 0.0;
+        for (int rr = 0; rr < 19; ++rr) acc = acc + A[rr][a] * A[rr][b];
+        M[a * 10 + b] = acc;
+      }
+    d_matinv<10>(M, Minv);
+    const double f = s.flatA[d.at(0, p, i, j, k)];
+    const double betalo = f + (1.0 - f) * 2.0;
+    const double ghi = f * 0.6 + (1.0 - f) * 0.95, glo = 1.0 - ghi, obghi = 1.0 / ghi, grat = glo / ghi;
+    for (int q = 0; q < 3; ++q) {
+      const double* Eq = s.Esnap + ((long long)q * NPANEL + p) * d.S;
+      const double Ept = Eq[off[0]];
+      double Y[10];
+      for (int a = 0; a < 10; ++a) Y[a] = 0.0;
+      for (int rr = 0; rr < 19; ++rr) {
+        const double R = Eq[off[rr]];
+        for (int a = 0; a < 10; ++a) Y[a] = Y[a] + A[rr][a] * R;
+      }
+      double X[10];
+      for (int a = 0; a < 10; ++a) {
+        double acc = 0.0;
+        for (int b = 0; b < 10; ++b) acc = acc + Minv[a * 10 + b] * Y[b];
+        X[a] = acc;
+      }
+      double e[4];
+      e[0] = Ept;
+      for (int m = 1; m < 4; ++m) e[m] = s.E[d.at(m * 3 + q, p, i, j, k)];
+      const double ISlo = betalo * (e[1] * e[1] + e[2] * e[2] + e[3] * e[3]) * ob12;
+      double Phi[10];
+      for (int m = 0; m < 4; ++m) Phi[m] = X[m] * obghi - e[m] * grat;
+      for (int m = 4; m < 10; ++m) Phi[m] = X[m] * obghi;
+      const double IShi = (Phi[1] * Phi[1] + Phi[2] * Phi[2] + Phi[3] * Phi[3]) * ob12 +
+                          (Phi[4] * Phi[4]) * (sqr(c0[4] - ob12) + ob180) + (Phi[5] * Phi[5]) * (sqr(c0[5] - ob12) + ob180) +
+                          (Phi[6] * Phi[6]) * (sqr(c0[6] - ob12) + ob180) + (Phi[7] * Phi[7]) * (c0[7] * c0[7] + ob144) +
+                          (Phi[8] * Phi[8]) * (c0[8] * c0[8] + ob144) + (Phi[9] * Phi[9]) * (c0[9] * c0[9] + ob144);
+      const double tau = fabs(IShi - ISlo);
+      double Wlo = glo * (1.0 + tau / (ISlo + ph.smallnum)), Whi = ghi * (1.0 + tau / (IShi + ph.smallnum));
+      const double aa = 1.0 / (Wlo + Whi);
+      Wlo = Wlo * aa;
+      Whi = Whi * aa;
+      const double x = 1.0 - f;
+      const double e0 = Whi * Phi[0] + Wlo * e[0];
+      s.E[d.at(q, p, i, j, k)] = Ept * f + e0 * x;
+      for (int m = 1; m < 4; ++m) s.E[d.at(m * 3 + q, p, i, j, k)] = (Whi * Phi[m] + Wlo * e[m]) * x;
+      for (int m = 4; m < 10; ++m) s.E[d.at(m * 3 + q, p, i, j, k)] = (Whi * Phi[m]) * x;
+    }
+  }
+}
+
+inline Range3 zones_all(const Dims& d) { return {1 - d.G, d.N + d.G, 1 - d.G, d.N + d.G, 1 - d.G, d.nr + d.G}; }
+inline Range3 shrink(const Dims& d, int s) {
+  return {1 - d.G + s, d.N + d.G - s, 1 - d.G + s, d.N + d.G - s, 1 - d.G + s, d.nr + d.G - s};
+}
+
+}  // namespace
+
+void launch_prim_and_masks(Solve& sv) {
+  const Dims& d = sv.d;
+  Range3 z = zones_all(d);
+  k_prim<<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, z);
+  mark(sv, "k_prim");
+  launch_face_masks(sv);
+}
+
+void launch_face_masks(Solve& sv) {
+  const Dims& d = sv.d;
+  Range3 f = {-d.G, d.N + d.G, -d.G, d.N + d.G, -d.G, d.nr + d.G};
+  k_zero_masked_faces<<<blocks_for(f.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, sv.st, f);
+  mark(sv, "k_zero_masked_faces");
+  k_tricorner<<<blocks_for(6LL * 4 * d.G * (d.NK - 1), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, sv.st);
+  mark(sv, "k_tricorner");
+}
+
+void launch_flattener(Solve& sv) {
+  const Dims& d = sv.d;
+  Range3 z = zones_all(d);
+  const int nb = blocks_for(z.count(), TPB, sv.sm_count);
+  k_flat_a<<<nb, TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, z);
+  mark(sv, "k_flat_a");
+  k_flat_bc<<<nb, TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, z, sv.st.flatA, sv.st.flatB, 0);
+  mark(sv, "k_flat_bc");
+  k_flat_bc<<<nb, TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, z, sv.st.flatB, sv.st.flatA, 1);
+  mark(sv, "k_flat_bc");
+}
+
+void launch_weno(Solve& sv) {
+  const Dims& d = sv.d;
+  Range3 a = shrink(d, 1), b = shrink(d, 2);
+  k_weno7a<<<blocks_for(a.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, a);
+  mark(sv, "k_weno7a");
+  k_weno7b<<<blocks_for(b.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, b);
+  mark(sv, "k_weno7b");
+}
+
+void launch_positivity(Solve& sv) {
+  const Dims& d = sv.d;
+  Range3 z = zones_all(d);
+  k_positivity<<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, z);
+  mark(sv, "k_positivity");
+  k_apply_giveup<<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.st, z);
+  mark(sv, "k_apply_giveup");
+}
+
+void launch_faceB_adp(Solve& sv) {
+  const Dims& d = sv.d;
+  const int G = d.G, N = d.N, nr = d.nr;
+  Range3 fx = {1 - G, N + G - 1, 2 - G, N + G - 1, 2 - G, nr + G - 1};
+  Range3 fy = {2 - G, N + G - 1, 1 - G, N + G - 1, 2 - G, nr + G - 1};
+  Range3 fz = {2 - G, N + G - 1, 2 - G, N + G - 1, 1 - G, nr + G - 1};
+  k_faceB<<<blocks_for(fx.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, fx, 0);
+  mark(sv, "k_faceB");
+  k_faceB<<<blocks_for(fy.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, fy, 1);
+  mark(sv, "k_faceB");
+  k_faceB<<<blocks_for(fz.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, fz, 2);
+  mark(sv, "k_faceB");
+  Range3 a = shrink(d, 1);
+  const size_t smem = sizeof(AdpSmem) * ADP_WARPS;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(k_adp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr_set = true;
+  }
+  long long nwarps = a.count();
+  long long nblk = (nwarps + ADP_WARPS - 1) / ADP_WARPS;
+  long long cap = (long long)sv.sm_count * 16;
+  if (nblk > cap) nblk = cap;
+  k_adp<<<(int)nblk, 32 * ADP_WARPS, smem, sv.stream>>>(d, sv.ph, sv.g, sv.st, a);
+  mark(sv, "k_adp");
+}
+
+void launch_efield(Solve& sv) {
+  const Dims& d = sv.d;
+  Range3 z = zones_all(d), a = shrink(d, 1), b = shrink(d, 2);
+  k_efield_a<<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, sv.st, z);
+  mark(sv, "k_efield_a");
+  k_efield_b<<<blocks_for(a.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, a);
+  mark(sv, "k_efield_b");
+  k_efield_c<<<blocks_for(b.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, b);
+  mark(sv, "k_efield_c");
+}
+
+}  // namespace cs

@@ -1,0 +1,374 @@
+// Ghost exchange across the panel edges, radial padding, the RK stage
+// combine, the conservative update with the constrained-transport face-B
+// update, the post-update clean-up and the CFL reduction.
+//
+// Follows FETCH_BUFFERS_FILL_IN_UX / _UY (300riemann_module/330-332),
+// PAD_BOUNDARY_R (800applications_cs/826pad_boundary_r.f:190-420),
+// UPDATE_IMEX_RK_STEP_P1 (400riemann_integrate/484update_imex_rk_step_p1.f:212-906),
+// CLEANUP_AFTER_UPDATE (485cleanup_after_update.f:383-1273),
+// EVALUATE_TIMESTEP (490evaluate_timestep.f:121-286) and the RK combine of
+// the driver (_I/_1000riemann_geomesh_cs_mhd/1000riemann_geomesh_cs_mhd.f:2661-2773).
+#include "cs_solve.h"
+
+namespace cs {
+
+namespace {
+
+constexpr int TPB = 128;
+
+__device__ __forceinline__ double* fill_base(const DState& s, int f) {
+  switch (f) {
+    case 0: return s.U;
+    case 1: return s.ent;
+    case 2: return s.Bxf;
+    case 3: return s.Byf;
+    default: return s.Bzf;
+  }
+}
+
+// Phase 1 of the exchange: every destination value is computed from the
+// pre-exchange arrays (the reference reads all sources from buffers packed
+// before any ghost is written).
+__global__ void k_fill_gather(DState s, const int32_t* __restrict__ src, const int32_t* __restrict__ dst,
+                              const uint8_t* __restrict__ meta, double* __restrict__ tmp, long long n) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int m = meta[t];
+    double v = fill_base(s, (m >> 5) & 7)[src[t]];
+    if (m & 8) v = -v;
+    if (m & 16) v = (fill_base(s, m & 7)[dst[t]] + v) * 0.5;
+    tmp[t] = v;
+  }
+}
+
+__global__ void k_fill_scatter(DState s, const int32_t* __restrict__ dst, const uint8_t* __restrict__ meta,
+                               const double* __restrict__ tmp, long long n) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    double* b = fill_base(s, meta[t] & 7);
+    b[dst[t]] = tmp[t];
+  }
+}
+
+// Radial outflow padding below k = 1 and above k = nr (826:190-420).  Two
+// columns that share an x- or y-face copy the same value into it.
+__global__ void k_pad_radial(Dims d, DGeom g, DState s, int bc_lower, int bc_upper) {
+  const int n1 = d.N + 2 * d.G;
+  const long long n = 6LL * n1 * n1;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % n1) + 1 - d.G;
+    const int j = (int)((t / n1) % n1) + 1 - d.G;
+    const int p = (int)(t / ((long long)n1 * n1));
+    if (mask_at(g, d, p, i, j) != 1) continue;
+    if (bc_lower == 2) {
+      for (int kk = 1; kk <= d.G; ++kk) {
+        const int l = 1 - kk, r = 1;
+        for (int q = 0; q < NVAR; ++q) s.U[d.at(q, p, i, j, l)] = s.U[d.at(q, p, i, j, r)];
+        s.Bxf[d.at(0, p, i, j, l)] = s.Bxf[d.at(0, p, i, j, r)];
+        s.Bxf[d.at(0, p, i - 1, j, l)] = s.Bxf[d.at(0, p, i - 1, j, r)];
+        s.Byf[d.at(0, p, i, j, l)] = s.Byf[d.at(0, p, i, j, r)];
+        s.Byf[d.at(0, p, i, j - 1, l)] = s.Byf[d.at(0, p, i, j - 1, r)];
+        s.Bzf[d.at(0, p, i, j, l - 1)] = s.Bzf[d.at(0, p, i, j, r - 1)];
+      }
+    }
+    if (bc_upper == 2) {
+      const int r = d.nr;
+      for (int kk = 1; kk <= d.G; ++kk) {
+        const int l = d.nr + kk;
+        const double vr = geo(g, d, CS_G_V_VOL, 0, p, i, j, r), vl = geo(g, d, CS_G_V_VOL, 0, p, i, j, l);
+        for (int q = 0; q < NVAR; ++q) s.U[d.at(q, p, i, j, l)] = s.U[d.at(q, p, i, j, r)] * vr / vl;
+        s.Bzf[d.at(0, p, i, j, l)] =
+            s.Bzf[d.at(0, p, i, j, r)] * geo(g, d, CS_G_ZF_AREA, 0, p, i, j, r) / geo(g, d, CS_G_ZF_AREA, 0, p, i, j, l);
+        s.Bxf[d.at(0, p, i, j, l)] =
+            s.Bxf[d.at(0, p, i, j, r)] * geo(g, d, CS_G_XF_AREA, 0, p, i, j, r) / geo(g, d, CS_G_XF_AREA, 0, p, i, j, l);
+        s.Byf[d.at(0, p, i, j, l)] =
+            s.Byf[d.at(0, p, i, j, r)] * geo(g, d, CS_G_YF_AREA, 0, p, i, j, r) / geo(g, d, CS_G_YF_AREA, 0, p, i, j, l);
+        s.Bxf[d.at(0, p, i - 1, j, l)] = s.Bxf[d.at(0, p, i - 1, j, r)] * geo(g, d, CS_G_XF_AREA, 0, p, i - 1, j, r) /
+                                          geo(g, d, CS_G_XF_AREA, 0, p, i - 1, j, l);
+        s.Byf[d.at(0, p, i, j - 1, l)] = s.Byf[d.at(0, p, i, j - 1, r)] * geo(g, d, CS_G_YF_AREA, 0, p, i, j - 1, r) /
+                                          geo(g, d, CS_G_YF_AREA, 0, p, i, j - 1, l);
+      }
+    }
+  }
+}
+
+// RK stage combine on the whole box: kind 0 is the two-stage average
+// (x + x0) / 2, kind 1 the Shu-Osher form a0 x0 + (1 - a0) x.
+struct CombineSeg {
+  double* x[5];
+  const double* x0[5];
+  long long n[5];
+};
+__global__ void k_combine(CombineSeg sg, long long total, double a0, int kind) {
+  const double a1 = 1.0 - a0;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    long long u = t;
+    int q = 0;
+    while (q < 4 && u >= sg.n[q]) {
+      u -= sg.n[q];
+      ++q;
+    }
+    const double x = sg.x[q][u], x0 = sg.x0[q][u];
+    sg.x[q][u] = kind == 1 ? a0 * x0 + a1 * x : (x + x0) * 0.5;
+  }
+}
+
+// Zone update (484:212-372): U += dt dU/dt on every zone, then on the
+// interior the entropy update and the conserved->primitive repair.
+__global__ void k_update_zones(Dims d, PhysC ph, DGeom g, DState s, Range3 r, double dt) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
+    int p, i, j, k;
+    r.decode(t, p, i, j, k);
+    double U[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) U[q] = s.U[d.at(q, p, i, j, k)] + dt * s.dUdt[d.at(q, p, i, j, k)];
+    if (i >= 1 && i <= d.N && j >= 1 && j <= d.N && k >= 1 && k <= d.nr) {
+      const double div = geo(g, d, CS_G_XF_AREA, 0, p, i, j, k) * s.EF[0][d.at(0, p, i, j, k)] -
+                         geo(g, d, CS_G_XF_AREA, 0, p, i - 1, j, k) * s.EF[0][d.at(0, p, i - 1, j, k)] +
+                         geo(g, d, CS_G_YF_AREA, 0, p, i, j, k) * s.EF[1][d.at(0, p, i, j, k)] -
+                         geo(g, d, CS_G_YF_AREA, 0, p, i, j - 1, k) * s.EF[1][d.at(0, p, i, j - 1, k)] +
+                         geo(g, d, CS_G_ZF_AREA, 0, p, i, j, k) * s.EF[2][d.at(0, p, i, j, k)] -
+                         geo(g, d, CS_G_ZF_AREA, 0, p, i, j, k - 1) * s.EF[2][d.at(0, p, i, j, k - 1)];
+      double en = s.ent[d.at(0, p, i, j, k)] - dt * div / geo(g, d, CS_G_V_VOL, 0, p, i, j, k);
+      double V[8];
+      d_cons_to_prim(ph, en, U, V);
+      s.ent[d.at(0, p, i, j, k)] = en;
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) s.U[d.at(q, p, i, j, k)] = U[q];
+  }
+}
+
+__device__ __forceinline__ double vrad(const DGeom& g, const Dims& d, int p, int i, int j, int k) {
+  const double x = geo(g, d, CS_G_VERT, 0, p, i, j, k), y = geo(g, d, CS_G_VERT, 1, p, i, j, k),
+               z = geo(g, d, CS_G_VERT, 2, p, i, j, k);
+  return sqrt(x * x + y * y + z * z);
+}
+// Angle between the vertices a and b on the sphere of radius 1/inv.
+__device__ __forceinline__ double vang(const DGeom& g, const Dims& d, int p, int ax, int ay, int bx, int by, int k,
+                                       double inv) {
+  const double c = (geo(g, d, CS_G_VERT, 0, p, ax, ay, k) * inv) * (geo(g, d, CS_G_VERT, 0, p, bx, by, k) * inv) +
+                   (geo(g, d, CS_G_VERT, 1, p, ax, ay, k) * inv) * (geo(g, d, CS_G_VERT, 1, p, bx, by, k) * inv) +
+                   (geo(g, d, CS_G_VERT, 2, p, ax, ay, k) * inv) * (geo(g, d, CS_G_VERT, 2, p, bx, by, k) * inv);
+  return acos(c);
+}
+
+// Constrained-transport face update (484:376-906): Stokes circulation of
+// the edge EMFs with spherical arc lengths for the angular edges.
+__global__ void k_ct(Dims d, DGeom g, DState s, Range3 r, int dir, double dt) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
+    int p, i, j, k;
+    r.decode(t, p, i, j, k);
+    const double* Ex = s.Ef[0];
+    const double* Ey = s.Ef[1];
+    const double* Ez = s.Ef[2];
+    if (dir == 0) {
+      const double rout = vrad(g, d, p, i, j, k), rin = vrad(g, d, p, i, j, k - 1), dr = rout - rin;
+      const double th = vang(g, d, p, i, j, i, j - 1, k, 1.0 / rout);
+      const double lin = rin * th, lout = rout * th;
+      const double c = dr * Ez[d.at(0, p, i, j, k)] - dr * Ez[d.at(0, p, i, j - 1, k)] - lout * Ey[d.at(0, p, i, j, k)] +
+                       lin * Ey[d.at(0, p, i, j, k - 1)];
+      double& b = s.Bxf[d.at(0, p, i, j, k)];
+      b = b - dt * c / geo(g, d, CS_G_XF_AREA, 0, p, i, j, k);
+    } else if (dir == 1) {
+      const double rout = vrad(g, d, p, i, j, k), rin = vrad(g, d, p, i, j, k - 1), dr = rout - rin;
+      const double th = vang(g, d, p, i, j, i - 1, j, k, 1.0 / rout);
+      const double lin = rin * th, lout = rout * th;
+      const double c = -dr * Ez[d.at(0, p, i, j, k)] + dr * Ez[d.at(0, p, i - 1, j, k)] + lout * Ex[d.at(0, p, i, j, k)] -
+                       lin * Ex[d.at(0, p, i, j, k - 1)];
+      double& b = s.Byf[d.at(0, p, i, j, k)];
+      b = b - dt * c / geo(g, d, CS_G_YF_AREA, 0, p, i, j, k);
+    } else {
+      const double rout = vrad(g, d, p, i, j, k), inv = 1.0 / rout;
+      const double lxp = rout * vang(g, d, p, i, j, i - 1, j, k, inv);
+      const double lxm = rout * vang(g, d, p, i, j - 1, i - 1, j - 1, k, inv);
+      const double lyp = rout * vang(g, d, p, i, j, i, j - 1, k, inv);
+      const double lym = rout * vang(g, d, p, i - 1, j, i - 1, j - 1, k, inv);
+      const double c = lyp * Ey[d.at(0, p, i, j, k)] - lym * Ey[d.at(0, p, i - 1, j, k)] - lxp * Ex[d.at(0, p, i, j, k)] +
+                       lxm * Ex[d.at(0, p, i, j - 1, k)];
+      double& b = s.Bzf[d.at(0, p, i, j, k)];
+      b = b - dt * c / geo(g, d, CS_G_ZF_AREA, 0, p, i, j, k);
+    }
+  }
+}
+
+// Clean-up zone pass (485:688-1273): least-squares zone-centred B from the
+// six face values on active zones with the matching total-energy fix, then
+// the conserved->primitive repair on every zone.
+__global__ void k_cleanup_zones(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
+    int p, i, j, k;
+    r.decode(t, p, i, j, k);
+    double U[8], V[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) U[q] = s.U[d.at(q, p, i, j, k)];
+    if (mask_at(g, d, p, i, j) == 1) {
+      double nv[3] = {geo(g, d, CS_G_ZF_CEN, 0, p, i, j, k), geo(g, d, CS_G_ZF_CEN, 1, p, i, j, k),
+                      geo(g, d, CS_G_ZF_CEN, 2, p, i, j, k)};
+      const double a = 1.0 / fmax(ph.smallnum, sqrt(nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2]));
+      nv[0] = nv[0] * a;
+      nv[1] = nv[1] * a;
+      nv[2] = nv[2] * a;
+      double Am[6][3];
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        Am[0][q] = geo(g, d, CS_G_XF_N, q, p, i, j, k);
+        Am[1][q] = geo(g, d, CS_G_XF_N, q, p, i - 1, j, k);
+        Am[2][q] = geo(g, d, CS_G_YF_N, q, p, i, j, k);
+        Am[3][q] = geo(g, d, CS_G_YF_N, q, p, i, j - 1, k);
+        Am[4][q] = nv[q];
+        Am[5][q] = nv[q];
+      }
+      const double Rm[6] = {s.Bxf[d.at(0, p, i, j, k)], s.Bxf[d.at(0, p, i - 1, j, k)], s.Byf[d.at(0, p, i, j, k)],
+                            s.Byf[d.at(0, p, i, j - 1, k)], s.Bzf[d.at(0, p, i, j, k)], s.Bzf[d.at(0, p, i, j, k - 1)]};
+      double M[3][3], R[3];
+#pragma unroll
+      for (int a1 = 0; a1 < 3; ++a1) {
+#pragma unroll
+        for (int a2 = 0; a2 < 3; ++a2) {
+          double sm = 0.0;
+#pragma unroll
+          for (int q = 0; q < 6; ++q) sm = sm + Am[q][a1] * Am[q][a2];
+          M[a1][a2] = sm;
+        }
+        double sm = 0.0;
+#pragma unroll
+        for (int q = 0; q < 6; ++q) sm = sm + Am[q][a1] * Rm[q];
+        R[a1] = sm;
+      }
+      const double a11 = M[0][0], a12 = M[0][1], a13 = M[0][2], a21 = M[1][0], a22 = M[1][1], a23 = M[1][2],
+                   a31 = M[2][0], a32 = M[2][1], a33 = M[2][2];
+      const double det = a11 * (a22 * a33 - a32 * a23) - a12 * (a21 * a33 - a31 * a23) + a13 * (a21 * a32 - a31 * a22);
+      const double ob = copysign(1.0, det) / fmax(1.0e-32, fabs(det));
+      const double b11 = (a22 * a33 - a23 * a32) * ob, b12 = (a13 * a32 - a12 * a33) * ob, b13 = (a12 * a23 - a22 * a13) * ob;
+      const double b21 = (a23 * a31 - a21 * a33) * ob, b22 = (a11 * a33 - a13 * a31) * ob, b23 = (a13 * a21 - a11 * a23) * ob;
+      const double b31 = (a21 * a32 - a22 * a31) * ob, b32 = (a12 * a31 - a11 * a32) * ob, b33 = (a11 * a22 - a12 * a21) * ob;
+      const double nb0 = b11 * R[0] + b12 * R[1] + b13 * R[2];
+      const double nb1 = b21 * R[0] + b22 * R[1] + b23 * R[2];
+      const double nb2 = b31 * R[0] + b32 * R[1] + b33 * R[2];
+      const double Bx = U[5], By = U[6], Bz = U[7];
+      U[5] = nb0;
+      U[6] = nb1;
+      U[7] = nb2;
+      U[4] = U[4] - (Bx * Bx + By * By + Bz * Bz) * ph.ob8pi + (nb0 * nb0 + nb1 * nb1 + nb2 * nb2) * ph.ob8pi;
+    }
+    double en = s.ent[d.at(0, p, i, j, k)];
+    d_cons_to_prim(ph, en, U, V);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      s.U[d.at(q, p, i, j, k)] = U[q];
+      s.V[d.at(q, p, i, j, k)] = V[q];
+    }
+    s.ent[d.at(0, p, i, j, k)] = en;
+  }
+}
+
+__global__ void k_set_u64(unsigned long long* p, unsigned long long v) { *p = v; }
+
+// CFL limit over the active interior zones; the minimum positive double is
+// found with an integer atomicMin on its bit pattern (positive IEEE doubles
+// order like their bit patterns).
+__global__ void k_timestep(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
+  double dtl = 1.0e300;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
+    int p, i, j, k;
+    r.decode(t, p, i, j, k);
+    if (mask_at(g, d, p, i, j) == 0) continue;
+    double U[8], V[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) U[q] = s.U[d.at(q, p, i, j, k)];
+    double en = s.ent[d.at(0, p, i, j, k)];
+    d_cons_to_prim(ph, en, U, V);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      s.U[d.at(q, p, i, j, k)] = U[q];
+      s.V[d.at(q, p, i, j, k)] = V[q];
+    }
+    s.ent[d.at(0, p, i, j, k)] = en;
+    const double b2 = V[5] * V[5] + V[6] * V[6] + V[7] * V[7];
+    const double ms = sqrt((ph.gamma * V[4] + ph.ob4pi * b2) / V[0]);
+    s.msonic[d.at(0, p, i, j, k)] = ms;
+    const double a21 = sqrt(V[1] * V[1] + V[2] * V[2] + V[3] * V[3]) + ms;
+    dtl = fmin(dtl, ph.cfl * geo(g, d, CS_G_V_SCALE, 0, p, i, j, k) / a21);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) dtl = fmin(dtl, __shfl_down_sync(0xffffffffu, dtl, o));
+  if ((threadIdx.x & 31) == 0 && dtl < 1.0e300 && dtl > 0.0)
+    atomicMin(s.dtmin, (unsigned long long)__double_as_longlong(dtl));
+}
+
+inline Range3 zones_all(const Dims& d) { return {1 - d.G, d.N + d.G, 1 - d.G, d.N + d.G, 1 - d.G, d.nr + d.G}; }
+
+}  // namespace
+
+void launch_fill_ghosts(Solve& sv) {
+  const FillMap& f = sv.fill;
+  if (f.n > 0) {
+    const int nb = blocks_for(f.n, 256, sv.sm_count);
+    k_fill_gather<<<nb, 256, 0, sv.stream>>>(sv.st, f.d_src, f.d_dst, f.d_meta, f.d_tmp, f.n);
+    mark(sv, "k_fill_gather");
+    k_fill_scatter<<<nb, 256, 0, sv.stream>>>(sv.st, f.d_dst, f.d_meta, f.d_tmp, f.n);
+    mark(sv, "k_fill_scatter");
+  }
+  const int n1 = sv.d.N + 2 * sv.d.G;
+  k_pad_radial<<<blocks_for(6LL * n1 * n1, TPB, sv.sm_count), TPB, 0, sv.stream>>>(sv.d, sv.g, sv.st, sv.p.bc_lower,
+                                                                                   sv.p.bc_upper);
+  mark(sv, "k_pad_radial");
+}
+
+void launch_save_stage0(Solve& sv) {
+  const size_t S6 = (size_t)6 * sv.d.S * sizeof(double);
+  cudaMemcpyAsync(sv.st.U0, sv.st.U, NVAR * S6, cudaMemcpyDeviceToDevice, sv.stream);
+  cudaMemcpyAsync(sv.st.ent0, sv.st.ent, S6, cudaMemcpyDeviceToDevice, sv.stream);
+  cudaMemcpyAsync(sv.st.B0[0], sv.st.Bxf, S6, cudaMemcpyDeviceToDevice, sv.stream);
+  cudaMemcpyAsync(sv.st.B0[1], sv.st.Byf, S6, cudaMemcpyDeviceToDevice, sv.stream);
+  cudaMemcpyAsync(sv.st.B0[2], sv.st.Bzf, S6, cudaMemcpyDeviceToDevice, sv.stream);
+  mark(sv, "copy_stage0", false);
+}
+
+void launch_combine(Solve& sv, double a0, int kind) {
+  const long long S6 = 6LL * sv.d.S;
+  CombineSeg sg;
+  sg.x[0] = sv.st.U;   sg.x0[0] = sv.st.U0;    sg.n[0] = NVAR * S6;
+  sg.x[1] = sv.st.ent; sg.x0[1] = sv.st.ent0;  sg.n[1] = S6;
+  sg.x[2] = sv.st.Bxf; sg.x0[2] = sv.st.B0[0]; sg.n[2] = S6;
+  sg.x[3] = sv.st.Byf; sg.x0[3] = sv.st.B0[1]; sg.n[3] = S6;
+  sg.x[4] = sv.st.Bzf; sg.x0[4] = sv.st.B0[2]; sg.n[4] = S6;
+  const long long total = (NVAR + 4) * S6;
+  k_combine<<<blocks_for(total, 256, sv.sm_count), 256, 0, sv.stream>>>(sg, total, a0, kind);
+  mark(sv, "k_combine");
+}
+
+void launch_update(Solve& sv, double dtmove) {
+  const Dims& d = sv.d;
+  Range3 z = zones_all(d);
+  k_update_zones<<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, z, dtmove);
+  mark(sv, "k_update_zones");
+  const int N = d.N, nr = d.nr;
+  Range3 fx = {0, N, 1, N, 1, nr}, fy = {1, N, 0, N, 1, nr}, fz = {1, N, 1, N, 0, nr};
+  k_ct<<<blocks_for(fx.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, sv.st, fx, 0, dtmove);
+  mark(sv, "k_ct");
+  k_ct<<<blocks_for(fy.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, sv.st, fy, 1, dtmove);
+  mark(sv, "k_ct");
+  k_ct<<<blocks_for(fz.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, sv.st, fz, 2, dtmove);
+  mark(sv, "k_ct");
+}
+
+void launch_cleanup(Solve& sv) {
+  launch_face_masks(sv);
+  Range3 z = zones_all(sv.d);
+  k_cleanup_zones<<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(sv.d, sv.ph, sv.g, sv.st, z);
+  mark(sv, "k_cleanup_zones");
+}
+
+void launch_timestep(Solve& sv, double dtcur) {
+  const double start = 1.1 * dtcur;
+  unsigned long long bits;
+  static_assert(sizeof(bits) == sizeof(start), "double is 64-bit");
+  std::memcpy(&bits, &start, sizeof(bits));
+  k_set_u64<<<1, 1, 0, sv.stream>>>(sv.st.dtmin, bits);
+  mark(sv, "k_set_u64");
+  Range3 r = {1, sv.d.N, 1, sv.d.N, 1, sv.d.nr};
+  k_timestep<<<blocks_for(r.count(), 256, sv.sm_count), 256, 0, sv.stream>>>(sv.d, sv.ph, sv.g, sv.st, r);
+  mark(sv, "k_timestep");
+}
+
+}  // namespace cs

@@ -1,0 +1,205 @@
+/*
+ * cubesphere_b200.h -- C ABI of the B200 per-stage volume update of the
+ * CubeSphere cubed-sphere MHD code.
+ *
+ * Every entry point returns 0 on success and a nonzero cs_status otherwise;
+ * nothing aborts.  cs_last_error() returns a one-line reason for the last
+ * failure on a context.  One host thread and one CUDA stream per context;
+ * contexts are independent.
+ *
+ * Array layout shared by every host<->device entry point ("panel box"):
+ *   each of the 6 panels (sectors) is a box of NI x NJ x NK points with
+ *   NI = NJ = ntp + 2*nghost + 1, NK = nr + 2*nghost + 1; the point (i,j,k),
+ *   i,j in [-nghost, ntp+nghost], k in [-nghost, nr+nghost], sits at offset
+ *     ((k+nghost)*NJ + (j+nghost))*NI + (i+nghost)
+ *   (i fastest, like the reference's column-major patch arrays).  Zone (cell)
+ *   arrays use i,j,k >= 1-nghost; x-face arrays use i >= -nghost (the
+ *   reference's 0-NGhost lower bound), y- and z-faces likewise in j and k.
+ *   A field with C components is stored component-major:
+ *     field[(c*6 + panel)*box + offset].
+ *
+ * Reference interfaces replaced (paths inside SPGEOMESH/CubeSphere):
+ *   cs_mesh_build        _I/_1000riemann_geomesh_cs_mhd/1000riemann_geomesh_cs_mhd.f:860-1341
+ *                        (BUILD_BASE_PATCHES, GENERATE_GLOBAL_RADIAL_*, Mesh_Sector_General,
+ *                         FILL_GHOST2D_GLOBAL, EXTRACT_VERT_COORDS_PATCH,
+ *                         STENCIL_INDEXING_TRICORNERS, COORDS_TO_WT_QUADPTS_{FACES,BFLD,VOLUME}_ISO2,
+ *                         INIT_BASIS_FUNCTION_COEFS)
+ *   cs_init_problem      pkg/inc/cubesphere/800applications_cs/820init_patch_cube_sphere.f:8
+ *   cs_state_put/get     the !$acc update device/host copies of the driver
+ *                        (1000riemann_geomesh_cs_mhd.f:2160-2198, :3051-3073)
+ *   cs_fill_ghosts       pkg/inc/cubesphere/300riemann_module/320-333 (LOAD_LOCAL_BUFFERS_UXY/UZ,
+ *                        FETCH_BUFFERS_FILL_IN_{UX,UY,UY_TOP,UZ}) and
+ *                        pkg/inc/cubesphere/800applications_cs/826pad_boundary_r.f:11
+ *   cs_limit_all_slopes_p12  pkg/inc/cubesphere/400riemann_integrate/421limit_all_slopes_p12.f:9
+ *   cs_make_facial_fluxes    pkg/inc/cubesphere/400riemann_integrate/450make_facial_fluxes.f:5
+ *   cs_make_edge_efields_p1  pkg/inc/cubesphere/400riemann_integrate/460make_edge_fields_p1.f:1
+ *   cs_build_non_stiff_sources pkg/inc/cubesphere/400riemann_integrate/470build_non_stiff_sources.f:6
+ *   cs_update_imex_rk_step_p1 pkg/inc/cubesphere/400riemann_integrate/484update_imex_rk_step_p1.f:7
+ *   cs_cleanup_after_update   pkg/inc/cubesphere/400riemann_integrate/485cleanup_after_update.f:4
+ *   cs_evaluate_timestep      pkg/inc/cubesphere/400riemann_integrate/490evaluate_timestep.f:7
+ *   cs_stage / cs_step        the per-stage call sequence and RK combine of
+ *                             1000riemann_geomesh_cs_mhd.f:1738-2908
+ */
+#ifndef CUBESPHERE_B200_H
+#define CUBESPHERE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum cs_status {
+  CS_OK = 0,
+  CS_ERR_ARG = 1,      /* bad argument / size */
+  CS_ERR_CUDA = 2,     /* a CUDA call failed */
+  CS_ERR_STATE = 3,    /* called out of order (e.g. stage before mesh build) */
+  CS_ERR_NOMEM = 4,    /* device allocation failed */
+  CS_ERR_NUMERIC = 5   /* non-finite value detected by a checking entry point */
+};
+
+/* Radial mesh choices (reference CHOOSE_RADIAL_MESH values). */
+enum cs_radial_mesh { CS_RADIAL_UNIFORM = 0, CS_RADIAL_LOG = 1, CS_RADIAL_STRETCHED = 2 };
+
+/* Time integrators.  CS_RK2 is the reference's two-stage combine
+ * (1000riemann_geomesh_cs_mhd.f:2661-2773); CS_SSPRK3 the three-stage
+ * Shu-Osher scheme in the same combine form; CS_IMEX_RK2 the two-stage
+ * scheme with the radial gravity source taken implicitly. */
+enum cs_rk_scheme { CS_RK2 = 2, CS_SSPRK3 = 3, CS_IMEX_RK2 = 4 };
+
+/* Runtime parameters: the reference's compile-time directives, module
+ * sizes and COMMON /RIEMANN_COM/ constants (pkg/inc/cubesphere/000com/riemann.com:42-74). */
+typedef struct cs_params {
+  int32_t ntp;          /* zones along each panel edge (ntp_zones) */
+  int32_t nr;           /* radial zones (nr_zones) */
+  int32_t nghost;       /* ghost layers (NGhost); 4 in the reference */
+  int32_t radial_mesh;  /* enum cs_radial_mesh */
+  double rmin, rmax;    /* radial extent */
+  double radial_ratio;  /* geometric stretch ratio (CS_RADIAL_STRETCHED) */
+  double gamma;         /* ratio of specific heats */
+  double rhofloor, prsfloor, smallnum;
+  double cfl_coef, flatten_coef, prs_flatten_coef;
+  double gm;            /* newtonsc * Mstar for the point-mass gravity source */
+  int32_t bc_lower, bc_upper; /* radial boundary codes: 2 = outflow */
+  int32_t rk_scheme;    /* enum cs_rk_scheme */
+  int32_t reserved;
+} cs_params;
+
+/* Seeded initial-state description (new generator cases of the problem
+ * library, built with the reference mechanism of 820init_patch_cube_sphere.f). */
+typedef struct cs_init_desc {
+  uint64_t seed;
+  int32_t kind;         /* 0: surface (config 0), 1: hydrostatic shell (configs 1-2) */
+  int32_t lmax;         /* harmonic degree of the seeded sums */
+  double rho_amp;       /* density perturbation amplitude */
+  double a_amp;         /* vector-potential amplitude */
+  double v_amp;         /* solid-body rotation amplitude */
+  double p0;            /* background pressure (kind 0) / p_inf (kind 1) */
+} cs_init_desc;
+
+typedef struct cs_ctx cs_ctx;
+
+/* Geometry fields readable through cs_geometry_get (component count in ()). */
+enum cs_geom_field {
+  CS_G_VERT = 0,   /* (3) vertex coordinates            */
+  CS_G_XF_QP,      /* (15) x-face quadrature points [c*5+q] (also the B points) */
+  CS_G_XF_QW,      /* (5)  x-face area weights (sum 1)  */
+  CS_G_XF_N,       /* (3)  x-face unit normal           */
+  CS_G_XF_AREA,    /* (1) */
+  CS_G_XF_CEN,     /* (3) */
+  CS_G_YF_QP, CS_G_YF_QW, CS_G_YF_N, CS_G_YF_AREA, CS_G_YF_CEN,
+  CS_G_ZF_QP, CS_G_ZF_QW,
+  CS_G_ZF_N,       /* (15) z-face normal per quadrature point [c*5+q] */
+  CS_G_ZF_AREA, CS_G_ZF_CEN,
+  CS_G_XB_QW, CS_G_YB_QW, CS_G_ZB_QW, /* (5) B-field quadrature weights */
+  CS_G_V_SCALE,    /* (1) v_scale_length */
+  CS_G_V_VOL,      /* (1) */
+  CS_G_V_CEN,      /* (3) */
+  CS_G_COEF,       /* (10) Coef_Basis_Moments */
+  CS_G_NFIELDS
+};
+
+int cs_geom_ncomp(int field);
+
+/* Lifecycle. */
+int cs_create(const cs_params* p, cs_ctx** out);
+int cs_destroy(cs_ctx* ctx);
+const char* cs_last_error(const cs_ctx* ctx);
+int cs_box_dims(const cs_ctx* ctx, int32_t* ni, int32_t* nj, int32_t* nk);
+
+/* One-line reason why p is rejected by cs_create, or "" when it is valid. */
+const char* cs_params_check(const cs_params* p);
+
+/* Mesh: builds the 6-panel geometry on the host and keeps it resident on the device. */
+int cs_mesh_build(cs_ctx* ctx);
+/* Host-only mesh build (no device is touched); the geometry, mask and
+ * stencil getters below then work without a GPU. */
+int cs_mesh_build_host(cs_ctx* ctx);
+int cs_geometry_get(cs_ctx* ctx, int field, double* host_out, size_t n_doubles);
+int cs_mask_get(cs_ctx* ctx, int32_t* host_out, size_t n);            /* imask_active, per box */
+int cs_stencil_get(cs_ctx* ctx, int32_t* host_out, size_t n);         /* istencil, [6][12][2][NJ][NI] */
+
+/* Geometry of one coarse zone cut with stride iscale out of sector isector
+ * (1..6) of a ntp_global x ntp_global x nr_global mesh without ghosts: the
+ * setting of the reference's quadrature-point test program
+ * (_T/_200mesh/004test_quadpoints.f:42-246).  Host only; field as in
+ * cs_geometry_get with a box of (ntp_global/iscale + 1)^2 x (nr_global/iscale + 1). */
+int cs_geometry_single_zone(int32_t isector, int32_t ntp_global, int32_t nr_global, int32_t iscale,
+                            double rmin, double rmax, int32_t radial_mesh, int32_t field,
+                            double* host_out, size_t n_doubles);
+
+/* State.  U: 8 components; ent: 1; bxf/byf/bzf: 1 each; all FP64 panel boxes. */
+int cs_init_problem(cs_ctx* ctx, const cs_init_desc* d);
+/* The same seeded initial state written into host arrays (no device). */
+int cs_init_problem_host(cs_ctx* ctx, const cs_init_desc* d, double* U, double* ent,
+                         double* bxf, double* byf, double* bzf);
+int cs_state_put(cs_ctx* ctx, const double* U, const double* ent,
+                 const double* bxf, const double* byf, const double* bzf);
+int cs_state_get(cs_ctx* ctx, double* U, double* ent,
+                 double* bxf, double* byf, double* bzf);
+
+/* Whole-stage and whole-step entry points (device resident, on ctx's stream). */
+int cs_stage(cs_ctx* ctx, int32_t irk, double dtcur);
+int cs_step(cs_ctx* ctx, double dtcur, double* dtcurp1);
+int cs_evaluate_timestep(cs_ctx* ctx, double dtcur, double* dtcurp1);
+int cs_synchronize(cs_ctx* ctx);
+
+/* Per-routine entry points with the reference routine names, for
+ * step-by-step parity (each runs on the resident state). */
+int cs_fill_ghosts(cs_ctx* ctx);
+int cs_limit_all_slopes_p12(cs_ctx* ctx);
+int cs_make_facial_fluxes(cs_ctx* ctx);
+int cs_make_edge_efields_p1(cs_ctx* ctx);
+int cs_build_non_stiff_sources(cs_ctx* ctx);
+int cs_update_imex_rk_step_p1(cs_ctx* ctx, double dtmove);
+int cs_cleanup_after_update(cs_ctx* ctx);
+
+/* Intermediate arrays for parity checks (panel boxes, component-major).
+ * which: 0 V (8 comps x 10 modes, comp-major [m*8+c]), 1 entropy modes (4),
+ * 2 flattener (1), 3 dU_dt (8), 4 Efx, 5 Efy, 6 Efz, 7 Bxf_quadpts (5),
+ * 8 Byf_quadpts (5), 9 Bzf_quadpts (5), 10 E_zc mode-1 (3),
+ * 11 face speeds S_L,S_R,S_D,S_U,S_B,S_T (6), 12 entropy fluxes x,y,z (3). */
+int cs_debug_get(cs_ctx* ctx, int32_t which, double* host_out, size_t n_doubles);
+
+/* Timing and launch accounting.  cs_get_stream returns the context's
+ * cudaStream_t (as void*) so a caller can order its own work and events
+ * after the library's.  Between cs_profile_begin and cs_profile_end every
+ * kernel launch is bracketed by CUDA events on that stream; cs_profile_end
+ * synchronizes and returns, per kernel name (32-byte NUL-padded entries in
+ * names), the summed device milliseconds and the launch counts.
+ * cs_launch_count returns the kernels this context has launched. */
+int cs_get_stream(cs_ctx* ctx, void** stream);
+int cs_launch_count(cs_ctx* ctx, int64_t* n);
+int cs_profile_begin(cs_ctx* ctx);
+int cs_profile_end(cs_ctx* ctx, int32_t max_kernels, char* names, double* total_ms,
+                   int64_t* launches, int32_t* n_kernels);
+
+/* Diagnostics: sums over interior zones of 6 panels of volume-weighted
+ * mass, energy and the max |div B| (face-area-weighted, per volume). */
+int cs_diag(cs_ctx* ctx, double* mass, double* energy, double* max_divb);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

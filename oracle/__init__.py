@@ -1,0 +1,138 @@
+"""ORACLE -- test infrastructure only.
+
+ctypes wrapper of ``oracle/liboracle.so``, the CPU restatement of the
+CubeSphere per-stage update (``oracle/oracle.cpp``).  Only the tests,
+``__graft_entry__.smoke`` and the CPU-baseline leg of ``bench.py`` use it,
+and only as the checker / the timed CPU reference; the library never calls
+it.  Parity status: see the header of ``oracle/oracle_core.h``.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "liboracle.so"
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(f"{LIB_PATH} missing: run `python -m cubesphere_b200.build`")
+    lib = ctypes.CDLL(str(LIB_PATH))
+    P, D, dp = ctypes.c_void_p, ctypes.c_double, ctypes.POINTER(ctypes.c_double)
+    ip = ctypes.POINTER(ctypes.c_int32)
+    sig = {
+        "oracle_create": ([P], P),
+        "oracle_destroy": ([P], None),
+        "oracle_set_geometry": ([P, ctypes.c_int, dp], None),
+        "oracle_set_mask_stencil": ([P, ip, ip], None),
+        "oracle_set_state": ([P, dp, dp, dp, dp, dp], None),
+        "oracle_get_state": ([P, dp, dp, dp, dp, dp], None),
+        "oracle_debug_get": ([P, ctypes.c_int, dp], ctypes.c_int),
+        "oracle_update": ([P, D], None),
+        "oracle_evaluate_timestep": ([P, D], D),
+        "oracle_stage": ([P, ctypes.c_int, D], None),
+        "oracle_step": ([P, D], D),
+    }
+    for n in ("oracle_fill_ghosts", "oracle_limit_all_slopes_p12", "oracle_make_facial_fluxes",
+              "oracle_make_edge_efields", "oracle_build_non_stiff_sources", "oracle_cleanup"):
+        sig[n] = ([P], None)
+    for n, (a, r) in sig.items():
+        f = getattr(lib, n)
+        f.argtypes = a
+        f.restype = r
+    _lib = lib
+    return lib
+
+
+def _d(a):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _i(a):
+    assert a.dtype == np.int32 and a.flags.c_contiguous
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+
+
+STATE_KEYS = ("U", "ent", "bxf", "byf", "bzf")
+DEBUG_WHICH = {"V": 0, "ent_modes": 1, "flatten": 2, "dUdt": 3, "Efx": 4, "Efy": 5, "Efz": 6, "Bxq": 7,
+               "Byq": 8, "Bzq": 9, "E1": 10, "speeds": 11, "entflux": 12}
+DEBUG_NCOMP = {"V": 80, "ent_modes": 4, "flatten": 1, "dUdt": 8, "Efx": 1, "Efy": 1, "Efz": 1, "Bxq": 5,
+               "Byq": 5, "Bzq": 5, "E1": 3, "speeds": 6, "entflux": 3}
+
+
+class Oracle:
+    """CPU solve on the geometry, mask and stencil of a library Solve."""
+
+    def __init__(self, solve):
+        self.lib = load()
+        self.s = solve
+        self.h = self.lib.oracle_create(ctypes.byref(solve.params))
+        from cubesphere_b200 import GEOM_FIELDS
+        for f, name in enumerate(GEOM_FIELDS):
+            g = np.ascontiguousarray(solve.geometry(name))
+            self.lib.oracle_set_geometry(self.h, f, _d(g))
+        m = np.ascontiguousarray(solve.mask())
+        st = np.ascontiguousarray(solve.stencil())
+        self.lib.oracle_set_mask_stencil(self.h, _i(m), _i(st))
+
+    def close(self):
+        if self.h:
+            self.lib.oracle_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def put_state(self, st: dict):
+        self.lib.oracle_set_state(self.h, *[_d(np.ascontiguousarray(st[k])) for k in STATE_KEYS])
+
+    def get_state(self) -> dict:
+        st = self.s.empty_state()
+        self.lib.oracle_get_state(self.h, *[_d(st[k]) for k in STATE_KEYS])
+        return st
+
+    def debug(self, name: str) -> np.ndarray:
+        out = self.s.zeros(DEBUG_NCOMP[name])
+        rc = self.lib.oracle_debug_get(self.h, DEBUG_WHICH[name], _d(out))
+        assert rc == 0
+        return out
+
+    def fill_ghosts(self):
+        self.lib.oracle_fill_ghosts(self.h)
+
+    def limit_all_slopes_p12(self):
+        self.lib.oracle_limit_all_slopes_p12(self.h)
+
+    def make_facial_fluxes(self):
+        self.lib.oracle_make_facial_fluxes(self.h)
+
+    def make_edge_efields_p1(self):
+        self.lib.oracle_make_edge_efields(self.h)
+
+    def build_non_stiff_sources(self):
+        self.lib.oracle_build_non_stiff_sources(self.h)
+
+    def update_imex_rk_step_p1(self, dt: float):
+        self.lib.oracle_update(self.h, dt)
+
+    def cleanup_after_update(self):
+        self.lib.oracle_cleanup(self.h)
+
+    def evaluate_timestep(self, dtcur: float) -> float:
+        return self.lib.oracle_evaluate_timestep(self.h, dtcur)
+
+    def stage(self, irk: int, dtcur: float):
+        self.lib.oracle_stage(self.h, irk, dtcur)
+
+    def step(self, dtcur: float) -> float:
+        return self.lib.oracle_step(self.h, dtcur)

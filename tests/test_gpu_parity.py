@@ -1,0 +1,140 @@
+"""GPU parity: the CUDA stage update against the CPU oracle on the same
+geometry and the same seeded state, routine by routine and over whole steps.
+
+Tolerance: 1e-12 relative (max |gpu - oracle| over the compared zones,
+divided by max |oracle| of that field) for the conserved state, the face B
+and the time step; 1e-10 for the intermediate reconstruction arrays, whose
+nonlinear WENO weights amplify the last-bit differences of FMA contraction
+and of the device pow/acos.  Ghost exchange is a copy and must be exact.
+"""
+import numpy as np
+import pytest
+
+import cubesphere_b200 as cs
+from conftest import has_gpu
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not has_gpu(), reason="needs a CUDA device")]
+
+TOL_STATE = 1e-12
+TOL_WORK = 1e-10
+
+
+def rel(a, b):
+    den = np.abs(b).max()
+    return float(np.abs(a - b).max() / (den if den > 0 else 1.0))
+
+
+def make_pair(name):
+    from oracle import Oracle
+    pr = cs.preset(name)
+    s = cs.Solve(**pr["params"])
+    s.mesh_build()
+    s.init_problem(**pr["init"])
+    st = s.get_state()
+    o = Oracle(s)
+    o.put_state(st)
+    return s, o, st
+
+
+def zones(s, a, lo=1, hi=0):
+    """Zones lo..N+hi (angular) and lo..nr+hi (radial) of a panel-box array."""
+    G, N, nr = s.G, s.N, s.nr
+    return a[..., G + lo:G + nr + hi + 1, G + lo:G + N + hi + 1, G + lo:G + N + hi + 1]
+
+
+def faces(s, a, d):
+    """Faces of the interior zones in direction d (0 x, 1 y, 2 z)."""
+    G, N, nr = s.G, s.N, s.nr
+    lo = [1, 1, 1]
+    lo[d] = 0
+    return a[..., G + lo[2]:G + nr + 1, G + lo[1]:G + N + 1, G + lo[0]:G + N + 1]
+
+
+def check_state(s, got, want, tol=TOL_STATE):
+    for q in range(8):
+        e = rel(zones(s, got["U"][q]), zones(s, want["U"][q]))
+        assert e <= tol, ("U", q, e)
+    e = rel(zones(s, got["ent"]), zones(s, want["ent"]))
+    assert e <= tol, ("ent", e)
+    for d, k in enumerate(("bxf", "byf", "bzf")):
+        e = rel(faces(s, got[k], d), faces(s, want[k], d))
+        assert e <= tol, (k, e)
+
+
+@pytest.fixture(scope="module")
+def shell16():
+    return make_pair("shell16")
+
+
+def test_fill_ghosts_is_exact(shell16):
+    s, o, st = shell16
+    s.put_state(st)
+    o.put_state(st)
+    s.fill_ghosts()
+    o.fill_ghosts()
+    g, w = s.get_state(), o.get_state()
+    for k in ("U", "ent", "bxf", "byf", "bzf"):
+        assert np.array_equal(g[k], w[k]), k
+
+
+def test_routines_in_sequence(shell16):
+    s, o, st = shell16
+    s.put_state(st)
+    o.put_state(st)
+    s.fill_ghosts()
+    o.fill_ghosts()
+    s.limit_all_slopes_p12()
+    o.limit_all_slopes_p12()
+    V, Vo = s.debug("V"), o.debug("V")
+    for m in range(10):
+        for c in range(8):
+            e = rel(zones(s, V[m * 8 + c], 0, 1), zones(s, Vo[m * 8 + c], 0, 1))
+            assert e <= TOL_WORK, ("V", m, c, e)
+    for name in ("flatten", "E1", "Bxq", "Byq", "Bzq"):
+        e = rel(zones(s, s.debug(name), 0, 1), zones(s, o.debug(name), 0, 1))
+        assert e <= TOL_WORK, (name, e)
+    s.make_facial_fluxes()
+    o.make_facial_fluxes()
+    e = rel(zones(s, s.debug("dUdt")), zones(s, o.debug("dUdt")))
+    assert e <= TOL_WORK, ("dUdt", e)
+    e = rel(zones(s, s.debug("entflux"), 0, 0), zones(s, o.debug("entflux"), 0, 0))
+    assert e <= TOL_WORK, ("entflux", e)
+    s.make_edge_efields_p1()
+    o.make_edge_efields_p1()
+    for name in ("Efx", "Efy", "Efz"):
+        e = rel(zones(s, s.debug(name), 0, 0), zones(s, o.debug(name), 0, 0))
+        assert e <= TOL_WORK, (name, e)
+    s.build_non_stiff_sources()
+    o.build_non_stiff_sources()
+    e = rel(zones(s, s.debug("dUdt")), zones(s, o.debug("dUdt")))
+    assert e <= TOL_WORK, ("dUdt+src", e)
+    dt = 1e-3
+    s.update_imex_rk_step_p1(dt)
+    o.update_imex_rk_step_p1(dt)
+    check_state(s, s.get_state(), o.get_state())
+    s.cleanup_after_update()
+    o.cleanup_after_update()
+    check_state(s, s.get_state(), o.get_state())
+
+
+@pytest.mark.parametrize("name,nsteps", [("shell16", 2), ("surface32", 2)])
+def test_whole_steps_match_oracle(name, nsteps):
+    s, o, st = make_pair(name)
+    dt_s = s.evaluate_timestep(1e30)
+    dt_o = o.evaluate_timestep(1e30)
+    assert abs(dt_s - dt_o) <= TOL_STATE * dt_o
+    for n in range(nsteps):
+        dt_s = s.step(dt_s)
+        dt_o = o.step(dt_o)
+        assert abs(dt_s - dt_o) <= TOL_STATE * dt_o, (n, dt_s, dt_o)
+        check_state(s, s.get_state(), o.get_state())
+
+
+def test_single_stage_keeps_div_b_at_roundoff(shell16):
+    s, o, st = shell16
+    s.put_state(st)
+    dt = s.evaluate_timestep(1e30)
+    s.stage(1, dt)
+    m, e, divb = s.diag()
+    bmax = np.abs(faces(s, s.get_state()["bxf"], 0)).max()
+    assert divb < 1e-11 * bmax
