@@ -59,7 +59,7 @@ class CsParams(ctypes.Structure):
         ("smallnum", ctypes.c_double), ("cfl_coef", ctypes.c_double), ("flatten_coef", ctypes.c_double),
         ("prs_flatten_coef", ctypes.c_double), ("gm", ctypes.c_double),
         ("bc_lower", ctypes.c_int32), ("bc_upper", ctypes.c_int32), ("rk_scheme", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("flags", ctypes.c_int32),
     ]
 
 
@@ -74,8 +74,9 @@ class CsInitDesc(ctypes.Structure):
 DEFAULT_PARAMS = dict(
     nghost=4, radial_mesh="uniform", rmin=1.0, rmax=2.0, radial_ratio=1.0, gamma=5.0 / 3.0,
     rhofloor=1.0e-12, prsfloor=1.0e-9, smallnum=1.0e-12, cfl_coef=0.2, flatten_coef=0.4,
-    prs_flatten_coef=1.5, gm=0.0, bc_lower=2, bc_upper=2, rk_scheme=CS_RK2,
+    prs_flatten_coef=1.5, gm=0.0, bc_lower=2, bc_upper=2, rk_scheme=CS_RK2, flags=0,
 )
+CS_FLAG_NO_ADP_CACHE = 1
 
 
 def make_params(**kw) -> CsParams:
@@ -83,8 +84,6 @@ def make_params(**kw) -> CsParams:
     d.update(kw)
     p = CsParams()
     for name, _ in CsParams._fields_:
-        if name == "reserved":
-            continue
         v = d[name]
         if name == "radial_mesh" and isinstance(v, str):
             v = RADIAL[v]

@@ -304,6 +304,23 @@ int upload_mesh(Solve& sv) {
   for (int q = 0; q < 3; ++q) { s.Bq[q] = A(NQ); s.fcon[q] = A(2 * NVAR); s.EF[q] = A(1); s.Ef[q] = A(1); s.B0[q] = A(1); }
   for (int q = 0; q < 6; ++q) s.S[q] = A(1);
   s.dUdt = A(NVAR); s.U0 = A(NVAR); s.ent0 = A(1);
+  set_adp_smem_limits();
+  // ADP: the KKT matrix of every zone depends on the geometry only, so its
+  // factors are computed once here and each stage only substitutes.  They
+  // take 10.4 KB per zone; without room for them (or with
+  // CS_FLAG_NO_ADP_CACHE) every stage assembles and factors in place.
+  s.adp_lu = nullptr;
+  s.adp_piv = nullptr;
+  if (!(sv.p.flags & CS_FLAG_NO_ADP_CACHE)) {
+    const long long na = adp_range_count(d);
+    const size_t lu_bytes = (size_t)na * 36 * 36 * sizeof(double), pv_bytes = (size_t)na * 36;
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && lu_bytes + pv_bytes + (size_t)8 * S6 * 60 < fr) {
+      s.adp_lu = (double*)dalloc(sv, lu_bytes, e);
+      s.adp_piv = s.adp_lu ? (int8_t*)dalloc(sv, pv_bytes, e) : nullptr;
+      if (!s.adp_lu || !s.adp_piv) return cuda_fail(sv, e, "cudaMalloc(ADP factors)");
+    }
+  }
   s.giveup = (int32_t*)dalloc(sv, S6 * sizeof(int32_t), e);
   s.dtmin = (unsigned long long*)dalloc(sv, 64, e);
   if (e != cudaSuccess || !s.U || !s.V || !s.E || !s.dtmin) return cuda_fail(sv, e, "cudaMalloc(state)");
@@ -331,6 +348,8 @@ int upload_mesh(Solve& sv) {
   CS_CUDA(sv, cudaMemcpyAsync(f.d_src, hs.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, sv.stream));
   CS_CUDA(sv, cudaMemcpyAsync(f.d_dst, hd.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, sv.stream));
   CS_CUDA(sv, cudaMemcpyAsync(f.d_meta, hm.data(), n, cudaMemcpyHostToDevice, sv.stream));
+  if (s.adp_lu) launch_adp_factor(sv);
+  CS_CUDA(sv, cudaGetLastError());
   CS_CUDA(sv, cudaStreamSynchronize(sv.stream));
   return CS_OK;
 }

@@ -47,6 +47,8 @@ struct DState {
   double *Ef[3];                         // edge EMFs
   double *dUdt;                          // 8
   double *U0, *ent0, *B0[3];             // saved stage-1 state
+  double* adp_lu;                        // ADP KKT factors, [36*36][zones of the ADP range], or null
+  int8_t* adp_piv;                       // their row permutation, [36][zones]
   int32_t* giveup;                       // positivity give-up flags per zone
   unsigned long long* dtmin;             // CFL reduction target (bit pattern of a positive double)
 };
@@ -388,6 +390,9 @@ void launch_flattener(Solve& s);
 void launch_weno(Solve& s);
 void launch_positivity(Solve& s);
 void launch_faceB_adp(Solve& s);
+void launch_adp_factor(Solve& s);
+void set_adp_smem_limits();
+long long adp_range_count(const Dims& d);
 void launch_efield(Solve& s);
 void launch_fluxes(Solve& s);
 void launch_edges(Solve& s);

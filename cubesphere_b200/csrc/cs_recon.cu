@@ -627,6 +627,9 @@ struct AdpSmem {
   int piv[36];
 };
 
+// kFactorOnly: assemble and factor the geometry-only KKT matrix and store
+// the factors and the row permutation for k_adp_solve (once per mesh).
+template <bool kFactorOnly>
 __global__ void __launch_bounds__(32 * ADP_WARPS) k_adp(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
   extern __shared__ unsigned char smem_raw[];
   AdpSmem& S = reinterpret_cast<AdpSmem*>(smem_raw)[threadIdx.x / 32];
@@ -662,8 +665,13 @@ __global__ void __launch_bounds__(32 * ADP_WARPS) k_adp(Dims d, PhysC ph, DGeom 
         S.Q[lane][20 + m] = m == 0 ? nz : nz * bfn[m];
       }
       S.wt[lane] = geo(g, d, BW, q, p, fx, fy, fz);
-      S.bq[lane] = s.Bq[dir][d.at(q, p, fx, fy, fz)];
-      S.vB[lane] = Vat(s, d, 5 + lane / 10, lane % 10, p, i, j, k);
+      if (!kFactorOnly) {
+        S.bq[lane] = s.Bq[dir][d.at(q, p, fx, fy, fz)];
+        S.vB[lane] = Vat(s, d, 5 + lane / 10, lane % 10, p, i, j, k);
+      } else {
+        S.bq[lane] = 0.0;
+        S.vB[lane] = 0.0;
+      }
     }
     __syncwarp();
     // 2. constraint rows C, D and the KKT matrix
@@ -768,6 +776,13 @@ __global__ void __launch_bounds__(32 * ADP_WARPS) k_adp(Dims d, PhysC ph, DGeom 
       }
       __syncwarp();
     }
+    if (kFactorOnly) {
+      const long long n = r.count();
+      for (int e = lane; e < 36 * 36; e += 32) s.adp_lu[(long long)e * n + t] = S.K[e / 36][e % 36];
+      for (int e = lane; e < 36; e += 32) s.adp_piv[(long long)e * n + t] = (int8_t)S.piv[e];
+      __syncwarp();
+      continue;
+    }
     // 4. substitution (one lane, reference order)
     if (lane == 0) {
       double y[36];
@@ -798,6 +813,94 @@ __global__ void __launch_bounds__(32 * ADP_WARPS) k_adp(Dims d, PhysC ph, DGeom 
       U[o5] = U[o5] - aa + bb;
     }
     __syncwarp();
+  }
+}
+
+// STEP 8.d with the stored factors: one thread per zone builds the
+// right-hand side (the same sums in the same order as k_adp) and runs the
+// forward and back substitution against the factors of its zone, which are
+// stored element-major so that a warp reads them coalesced.
+constexpr int ADPS_TPB = 128;
+__global__ void __launch_bounds__(ADPS_TPB) k_adp_solve(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
+  __shared__ double rhs_s[36][ADPS_TPB];
+  const long long n = r.count();
+  const int tid = threadIdx.x;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    int p, i, j, k;
+    r.decode(t, p, i, j, k);
+    if (mask_at(g, d, p, i, j) == 0) continue;
+    const double obl0 = 1.0 / fmax(geo(g, d, CS_G_V_SCALE, 0, p, i, j, k), ph.smallnum);
+    const double vc0 = geo(g, d, CS_G_V_CEN, 0, p, i, j, k), vc1 = geo(g, d, CS_G_V_CEN, 1, p, i, j, k),
+                 vc2 = geo(g, d, CS_G_V_CEN, 2, p, i, j, k);
+    double c0[10];
+    coef10(g, d, p, i, j, k, c0);
+    double rhs[30];
+#pragma unroll
+    for (int a = 0; a < 30; ++a) rhs[a] = 0.0;
+    double D[6];
+#pragma unroll 1
+    for (int f = 0; f < 6; ++f) {
+      const int dir = f / 2;
+      const int fx = (f == 1) ? i - 1 : i, fy = (f == 3) ? j - 1 : j, fz = (f == 5) ? k - 1 : k;
+      const int QP = dir == 0 ? CS_G_XF_QP : (dir == 1 ? CS_G_YF_QP : CS_G_ZF_QP);
+      const int BW = dir == 0 ? CS_G_XB_QW : (dir == 1 ? CS_G_YB_QW : CS_G_ZB_QW);
+      const int NF = dir == 0 ? CS_G_XF_N : (dir == 1 ? CS_G_YF_N : CS_G_ZF_N);
+      const int ns = dir == 2 ? 5 : 1;
+      double dacc = 0.0;
+#pragma unroll
+      for (int q = 0; q < 5; ++q) {
+        const int nq = dir == 2 ? q : 0;
+        const double nx = geo(g, d, NF, nq, p, fx, fy, fz), ny = geo(g, d, NF, ns + nq, p, fx, fy, fz),
+                     nz = geo(g, d, NF, 2 * ns + nq, p, fx, fy, fz);
+        const double x = (geo(g, d, QP, q, p, fx, fy, fz) - vc0) * obl0;
+        const double y = (geo(g, d, QP, 5 + q, p, fx, fy, fz) - vc1) * obl0;
+        const double z = (geo(g, d, QP, 10 + q, p, fx, fy, fz) - vc2) * obl0;
+        const double bfn[10] = {1.0, x, y, z, x * x - c0[4], y * y - c0[5], z * z - c0[6], x * y - c0[7],
+                                y * z - c0[8], x * z - c0[9]};
+        const double bq = s.Bq[dir][d.at(q, p, fx, fy, fz)];
+#pragma unroll
+        for (int m = 0; m < 10; ++m) {
+          rhs[m] = rhs[m] + (m == 0 ? nx : nx * bfn[m]) * bq;
+          rhs[10 + m] = rhs[10 + m] + (m == 0 ? ny : ny * bfn[m]) * bq;
+          rhs[20 + m] = rhs[20 + m] + (m == 0 ? nz : nz * bfn[m]) * bq;
+        }
+        dacc = dacc + geo(g, d, BW, q, p, fx, fy, fz) * bq;
+      }
+      D[f] = dacc;
+    }
+#pragma unroll
+    for (int a = 0; a < 30; ++a) rhs_s[a][tid] = rhs[a] + Vat(s, d, 5 + a / 10, a % 10, p, i, j, k);
+#pragma unroll
+    for (int f = 0; f < 6; ++f) rhs_s[30 + f][tid] = D[f];
+    const double* L = s.adp_lu + t;
+    const int8_t* pv = s.adp_piv + t;
+    double y[36];
+#pragma unroll
+    for (int a = 0; a < 36; ++a) {
+      double acc = rhs_s[pv[(long long)a * n]][tid];
+#pragma unroll
+      for (int b = 0; b < a; ++b) acc -= __ldcs(L + (long long)(a * 36 + b) * n) * y[b];
+      y[a] = acc;
+    }
+#pragma unroll
+    for (int a = 35; a >= 0; --a) {
+      double acc = y[a];
+#pragma unroll
+      for (int b = a + 1; b < 36; ++b) acc -= __ldcs(L + (long long)(a * 36 + b) * n) * y[b];
+      y[a] = acc / __ldcs(L + (long long)(a * 36 + a) * n);
+    }
+#pragma unroll
+    for (int a = 0; a < 30; ++a) Vat(s, d, 5 + a / 10, a % 10, p, i, j, k) = y[a];
+    double* U = s.U;
+    const long long o5 = d.at(4, p, i, j, k);
+    const double u6 = U[d.at(5, p, i, j, k)], u7 = U[d.at(6, p, i, j, k)], u8 = U[d.at(7, p, i, j, k)];
+    const double aa = (u6 * u6 + u7 * u7 + u8 * u8) * ph.ob8pi;
+    const double n6 = y[0], n7 = y[10], n8 = y[20];
+    U[d.at(5, p, i, j, k)] = n6;
+    U[d.at(6, p, i, j, k)] = n7;
+    U[d.at(7, p, i, j, k)] = n8;
+    const double bb = (n6 * n6 + n7 * n7 + n8 * n8) * ph.ob8pi;
+    U[o5] = U[o5] - aa + bb;
   }
 }
 
@@ -1003,18 +1106,37 @@ void launch_faceB_adp(Solve& sv) {
   k_faceB<<<blocks_for(fz.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, fz, 2);
   mark(sv, "k_faceB");
   Range3 a = shrink(d, 1);
-  const size_t smem = sizeof(AdpSmem) * ADP_WARPS;
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(k_adp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr_set = true;
+  if (sv.st.adp_lu) {
+    k_adp_solve<<<blocks_for(a.count(), ADPS_TPB, sv.sm_count), ADPS_TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, a);
+    mark(sv, "k_adp_solve");
+    return;
   }
+  const size_t smem = sizeof(AdpSmem) * ADP_WARPS;
   long long nwarps = a.count();
   long long nblk = (nwarps + ADP_WARPS - 1) / ADP_WARPS;
   long long cap = (long long)sv.sm_count * 16;
   if (nblk > cap) nblk = cap;
-  k_adp<<<(int)nblk, 32 * ADP_WARPS, smem, sv.stream>>>(d, sv.ph, sv.g, sv.st, a);
+  k_adp<false><<<(int)nblk, 32 * ADP_WARPS, smem, sv.stream>>>(d, sv.ph, sv.g, sv.st, a);
   mark(sv, "k_adp");
+}
+
+long long adp_range_count(const Dims& d) { return shrink(d, 1).count(); }
+
+void set_adp_smem_limits() {
+  const int smem = (int)(sizeof(AdpSmem) * ADP_WARPS);
+  cudaFuncSetAttribute(k_adp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaFuncSetAttribute(k_adp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+}
+
+void launch_adp_factor(Solve& sv) {
+  const Dims& d = sv.d;
+  Range3 a = shrink(d, 1);
+  const size_t smem = sizeof(AdpSmem) * ADP_WARPS;
+  long long nblk = (a.count() + ADP_WARPS - 1) / ADP_WARPS;
+  long long cap = (long long)sv.sm_count * 16;
+  if (nblk > cap) nblk = cap;
+  k_adp<true><<<(int)nblk, 32 * ADP_WARPS, smem, sv.stream>>>(d, sv.ph, sv.g, sv.st, a);
+  mark(sv, "k_adp_factor");
 }
 
 void launch_efield(Solve& sv) {

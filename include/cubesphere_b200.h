@@ -83,8 +83,14 @@ typedef struct cs_params {
   double gm;            /* newtonsc * Mstar for the point-mass gravity source */
   int32_t bc_lower, bc_upper; /* radial boundary codes: 2 = outflow */
   int32_t rk_scheme;    /* enum cs_rk_scheme */
-  int32_t reserved;
+  int32_t flags;        /* CS_FLAG_* bits */
 } cs_params;
+
+/* cs_params.flags: do not keep the per-zone factors of the (geometry-only)
+ * ADP constrained least-squares system resident (10.4 KB per zone); factor
+ * it in every stage instead.  The cache is also skipped automatically when
+ * the device lacks the memory.  Results are identical either way. */
+#define CS_FLAG_NO_ADP_CACHE 1
 
 /* Seeded initial-state description (new generator cases of the problem
  * library, built with the reference mechanism of 820init_patch_cube_sphere.f). */

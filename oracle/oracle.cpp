@@ -25,7 +25,7 @@ static const int kNbr[6][4] = {{3, 6, 2, 5}, {1, 4, 3, 6}, {2, 5, 1, 4}, {5, 2, 
 struct Params {
   int32_t ntp, nr, nghost, radial_mesh;
   double rmin, rmax, radial_ratio, gamma, rhofloor, prsfloor, smallnum, cfl_coef, flatten_coef, prs_flatten_coef, gm;
-  int32_t bc_lower, bc_upper, rk_scheme, reserved;
+  int32_t bc_lower, bc_upper, rk_scheme, flags;
 };
 
 struct Ctx {

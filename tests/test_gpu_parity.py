@@ -24,10 +24,10 @@ def rel(a, b):
     return float(np.abs(a - b).max() / (den if den > 0 else 1.0))
 
 
-def make_pair(name):
+def make_pair(name, flags=0):
     from oracle import Oracle
     pr = cs.preset(name)
-    s = cs.Solve(**pr["params"])
+    s = cs.Solve(**pr["params"], flags=flags)
     s.mesh_build()
     s.init_problem(**pr["init"])
     st = s.get_state()
@@ -117,9 +117,11 @@ def test_routines_in_sequence(shell16):
     check_state(s, s.get_state(), o.get_state())
 
 
-@pytest.mark.parametrize("name,nsteps", [("shell16", 2), ("surface32", 2)])
-def test_whole_steps_match_oracle(name, nsteps):
-    s, o, st = make_pair(name)
+@pytest.mark.parametrize("name,nsteps,flags", [("shell16", 2, 0), ("surface32", 2, 0),
+                                               ("shell16", 1, cs.CS_FLAG_NO_ADP_CACHE)])
+def test_whole_steps_match_oracle(name, nsteps, flags):
+    """flags=0 uses the resident ADP factors, CS_FLAG_NO_ADP_CACHE factors per stage."""
+    s, o, st = make_pair(name, flags)
     dt_s = s.evaluate_timestep(1e30)
     dt_o = o.evaluate_timestep(1e30)
     assert abs(dt_s - dt_o) <= TOL_STATE * dt_o
