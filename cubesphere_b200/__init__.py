@@ -77,6 +77,7 @@ DEFAULT_PARAMS = dict(
     prs_flatten_coef=1.5, gm=0.0, bc_lower=2, bc_upper=2, rk_scheme=CS_RK2, flags=0,
 )
 CS_FLAG_NO_ADP_CACHE = 1
+CS_FLAG_NO_OP_CACHE = 2
 
 
 def make_params(**kw) -> CsParams:

@@ -311,6 +311,20 @@ int upload_mesh(Solve& sv) {
   // CS_FLAG_NO_ADP_CACHE) every stage assembles and factors in place.
   s.adp_lu = nullptr;
   s.adp_piv = nullptr;
+  s.op_m9 = nullptr;
+  s.op_m10 = nullptr;
+  // The inverse normal matrices of the STEP 7.b / 9.c least squares are
+  // geometry-only as well (1.4 KB per zone together).
+  if (!(sv.p.flags & CS_FLAG_NO_OP_CACHE)) {
+    const long long nl = lsq_range_count(d);
+    size_t fr = 0, tot = 0;
+    const size_t bytes = (size_t)nl * (81 + 100) * sizeof(double);
+    if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && bytes + (size_t)8 * S6 * 60 < fr) {
+      s.op_m9 = (double*)dalloc(sv, (size_t)nl * 81 * sizeof(double), e);
+      s.op_m10 = s.op_m9 ? (double*)dalloc(sv, (size_t)nl * 100 * sizeof(double), e) : nullptr;
+      if (!s.op_m9 || !s.op_m10) return cuda_fail(sv, e, "cudaMalloc(least-squares operators)");
+    }
+  }
   if (!(sv.p.flags & CS_FLAG_NO_ADP_CACHE)) {
     const long long na = adp_range_count(d);
     const size_t lu_bytes = (size_t)na * 36 * 36 * sizeof(double), pv_bytes = (size_t)na * 36;
@@ -348,6 +362,7 @@ int upload_mesh(Solve& sv) {
   CS_CUDA(sv, cudaMemcpyAsync(f.d_src, hs.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, sv.stream));
   CS_CUDA(sv, cudaMemcpyAsync(f.d_dst, hd.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, sv.stream));
   CS_CUDA(sv, cudaMemcpyAsync(f.d_meta, hm.data(), n, cudaMemcpyHostToDevice, sv.stream));
+  launch_ops_build(sv);
   if (s.adp_lu) launch_adp_factor(sv);
   CS_CUDA(sv, cudaGetLastError());
   CS_CUDA(sv, cudaStreamSynchronize(sv.stream));

@@ -47,6 +47,8 @@ struct DState {
   double *Ef[3];                         // edge EMFs
   double *dUdt;                          // 8
   double *U0, *ent0, *B0[3];             // saved stage-1 state
+  double* op_m9;                         // STEP 7.b inverse normal matrices, [81][zones of shrink(2)], or null
+  double* op_m10;                        // STEP 9.c inverse normal matrices, [100][zones of shrink(2)], or null
   double* adp_lu;                        // ADP KKT factors, [36*36][zones of the ADP range], or null
   int8_t* adp_piv;                       // their row permutation, [36][zones]
   int32_t* giveup;                       // positivity give-up flags per zone
@@ -393,6 +395,8 @@ void launch_faceB_adp(Solve& s);
 void launch_adp_factor(Solve& s);
 void set_adp_smem_limits();
 long long adp_range_count(const Dims& d);
+long long lsq_range_count(const Dims& d);
+void launch_ops_build(Solve& s);
 void launch_efield(Solve& s);
 void launch_fluxes(Solve& s);
 void launch_edges(Solve& s);

@@ -10,6 +10,8 @@
 // The reference scatters each face into both neighbours inside one
 // parallel loop; here each face writes its two one-sided contributions and
 // each zone sums its own six faces in a fixed order.
+#include <algorithm>
+
 #include "cs_solve.h"
 
 namespace cs {
@@ -22,7 +24,14 @@ __device__ __forceinline__ double Vm(const DState& s, const Dims& d, int comp, i
   return s.V[((long long)(mode * NVAR + comp) * NPANEL + p) * d.S + o];
 }
 
-__global__ void __launch_bounds__(TPB) k_flux(Dims d, PhysC ph, DGeom g, DState s, Range3 r, int dir) {
+// One face quadrature point per thread: the five warps of a block take the
+// five points of the same 32 faces, so the zone modes each warp loads are
+// shared through L1 and no thread holds more than one point's state.  The
+// per-point contributions meet in shared memory and are summed in point
+// order (the order of the reference's quadrature loop).
+constexpr int FLUX_FACES = 32;
+__global__ void __launch_bounds__(FLUX_FACES * 5, 3) k_flux(Dims d, PhysC ph, DGeom g, DState s, Range3 r, int dir) {
+  __shared__ double red[5][16][FLUX_FACES];
   const int QP = dir == 0 ? CS_G_XF_QP : (dir == 1 ? CS_G_YF_QP : CS_G_ZF_QP);
   const int QW = dir == 0 ? CS_G_XF_QW : (dir == 1 ? CS_G_YF_QW : CS_G_ZF_QW);
   const int AR = dir == 0 ? CS_G_XF_AREA : (dir == 1 ? CS_G_YF_AREA : CS_G_ZF_AREA);
@@ -30,89 +39,70 @@ __global__ void __launch_bounds__(TPB) k_flux(Dims d, PhysC ph, DGeom g, DState 
   double* SLo = s.S[2 * dir];
   double* SHi = s.S[2 * dir + 1];
   double* EF = s.EF[dir];
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
-    int p, i, j, k;
-    r.decode(t, p, i, j, k);
+  const int lane = threadIdx.x % FLUX_FACES, jq = threadIdx.x / FLUX_FACES;
+  const long long nf = r.count();
+  const long long ntile = (nf + FLUX_FACES - 1) / FLUX_FACES;
+  for (long long tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
+    const long long t = tile * FLUX_FACES + lane;
+    const bool valid = t < nf;
+    int p = 0, i = 0, j = 0, k = 0;
+    if (valid) r.decode(t, p, i, j, k);
     int lx = i, ly = j, lz = k, rx = i, ry = j, rz = k;
-    bool skip = false;
-    if (dir == 0) {
-      const int mL = mask_at(g, d, p, i, j), mR = mask_at(g, d, p, i + 1, j);
-      rx = i + 1;
-      if (mL == 0 && mR == 1) { lx = sten(g, d, p, rx, ry, 1, 0); ly = sten(g, d, p, rx, ry, 1, 1); }
-      else if (mL == 1 && mR == 0) { rx = sten(g, d, p, lx, ly, 0, 0); ry = sten(g, d, p, lx, ly, 0, 1); }
-      else if (mL == 0 && mR == 0) skip = true;
-    } else if (dir == 1) {
-      const int mL = mask_at(g, d, p, i, j), mR = mask_at(g, d, p, i, j + 1);
-      ry = j + 1;
-      if (mL == 0 && mR == 1) { lx = sten(g, d, p, rx, ry, 3, 0); ly = sten(g, d, p, rx, ry, 3, 1); }
-      else if (mL == 1 && mR == 0) { rx = sten(g, d, p, lx, ly, 2, 0); ry = sten(g, d, p, lx, ly, 2, 1); }
-      else if (mL == 0 && mR == 0) skip = true;
-    } else {
-      if (mask_at(g, d, p, i, j) == 0) skip = true;
-      rz = k + 1;
+    bool skip = !valid;
+    if (valid) {
+      if (dir == 0) {
+        const int mL = mask_at(g, d, p, i, j), mR = mask_at(g, d, p, i + 1, j);
+        rx = i + 1;
+        if (mL == 0 && mR == 1) { lx = sten(g, d, p, rx, ry, 1, 0); ly = sten(g, d, p, rx, ry, 1, 1); }
+        else if (mL == 1 && mR == 0) { rx = sten(g, d, p, lx, ly, 0, 0); ry = sten(g, d, p, lx, ly, 0, 1); }
+        else if (mL == 0 && mR == 0) skip = true;
+      } else if (dir == 1) {
+        const int mL = mask_at(g, d, p, i, j), mR = mask_at(g, d, p, i, j + 1);
+        ry = j + 1;
+        if (mL == 0 && mR == 1) { lx = sten(g, d, p, rx, ry, 3, 0); ly = sten(g, d, p, rx, ry, 3, 1); }
+        else if (mL == 1 && mR == 0) { rx = sten(g, d, p, lx, ly, 2, 0); ry = sten(g, d, p, lx, ly, 2, 1); }
+        else if (mL == 0 && mR == 0) skip = true;
+      } else {
+        if (mask_at(g, d, p, i, j) == 0) skip = true;
+        rz = k + 1;
+      }
     }
-    const long long fo = d.idx(i, j, k);
     if (skip) {
 #pragma unroll
-      for (int c = 0; c < 16; ++c) F[((long long)c * NPANEL + p) * d.S + fo] = 0.0;
-      continue;
-    }
-    const long long oL = d.idx(lx, ly, lz), oR = d.idx(rx, ry, rz);
-    const double obl0 = 1.0 / fmax(geo(g, d, CS_G_V_SCALE, 0, p, lx, ly, lz), ph.smallnum);
-    const double obl02 = 1.0 / fmax(geo(g, d, CS_G_V_SCALE, 0, p, rx, ry, rz), ph.smallnum);
-    const double lcx = geo(g, d, CS_G_V_CEN, 0, p, lx, ly, lz), lcy = geo(g, d, CS_G_V_CEN, 1, p, lx, ly, lz),
-                 lcz = geo(g, d, CS_G_V_CEN, 2, p, lx, ly, lz);
-    const double rcx = geo(g, d, CS_G_V_CEN, 0, p, rx, ry, rz), rcy = geo(g, d, CS_G_V_CEN, 1, p, rx, ry, rz),
-                 rcz = geo(g, d, CS_G_V_CEN, 2, p, rx, ry, rz);
-    double cL[10], cR[10];
-#pragma unroll
-    for (int m = 0; m < 10; ++m) {
-      cL[m] = geo(g, d, CS_G_COEF, m, p, lx, ly, lz);
-      cR[m] = geo(g, d, CS_G_COEF, m, p, rx, ry, rz);
-    }
-    const double area = geo(g, d, AR, 0, p, i, j, k);
-    const double volL = geo(g, d, CS_G_V_VOL, 0, p, lx, ly, lz), volR = geo(g, d, CS_G_V_VOL, 0, p, rx, ry, rz);
-    double accL[8], accR[8];
-#pragma unroll
-    for (int c = 0; c < 8; ++c) accL[c] = accR[c] = 0.0;
-    // Frame pieces that do not depend on the quadrature point.
-    double Ax = 0, Ay = 0, Az = 0, Bx = 0, By = 0, Bz = 0, Cx = 0, Cy = 0, Cz = 0, vbx = 0, vby = 0, vbz = 0;
-    if (dir == 0) {
-      Ax = geo(g, d, CS_G_XF_N, 0, p, i, j, k);
-      Ay = geo(g, d, CS_G_XF_N, 1, p, i, j, k);
-      Az = geo(g, d, CS_G_XF_N, 2, p, i, j, k);
-      Cx = geo(g, d, CS_G_XF_CEN, 0, p, i, j, k);
-      Cy = geo(g, d, CS_G_XF_CEN, 1, p, i, j, k);
-      Cz = geo(g, d, CS_G_XF_CEN, 2, p, i, j, k);
-      const double tt = 1.0 / fmax(sqrt(Cx * Cx + Cy * Cy + Cz * Cz), ph.smallnum);
-      Cx = Cx * tt;
-      Cy = Cy * tt;
-      Cz = Cz * tt;
-      Bx = Cy * Az - Cz * Ay;
-      By = Cz * Ax - Cx * Az;
-      Bz = Cx * Ay - Cy * Ax;
-    } else if (dir == 1) {
-      Ax = geo(g, d, CS_G_YF_N, 0, p, i, j, k);
-      Ay = geo(g, d, CS_G_YF_N, 1, p, i, j, k);
-      Az = geo(g, d, CS_G_YF_N, 2, p, i, j, k);
-      Bx = geo(g, d, CS_G_YF_CEN, 0, p, i, j, k);
-      By = geo(g, d, CS_G_YF_CEN, 1, p, i, j, k);
-      Bz = geo(g, d, CS_G_YF_CEN, 2, p, i, j, k);
-      const double tt = 1.0 / fmax(sqrt(Bx * Bx + By * By + Bz * Bz), ph.smallnum);
-      Bx = Bx * tt;
-      By = By * tt;
-      Bz = Bz * tt;
-      Cx = Ay * Bz - Az * By;
-      Cy = Az * Bx - Ax * Bz;
-      Cz = Ax * By - Ay * Bx;
+      for (int c = 0; c < 16; ++c) red[jq][c][lane] = 0.0;
     } else {
-      auto vt = [&](int q, int x, int y) { return geo(g, d, CS_G_VERT, q, p, x, y, k); };
-      vbx = vt(0, i, j) + vt(0, i, j - 1) - vt(0, i - 1, j) - vt(0, i - 1, j - 1);
-      vby = vt(1, i, j) + vt(1, i, j - 1) - vt(1, i - 1, j) - vt(1, i - 1, j - 1);
-      vbz = vt(2, i, j) + vt(2, i, j - 1) - vt(2, i - 1, j) - vt(2, i - 1, j - 1);
-    }
-    for (int jq = 0; jq < 5; ++jq) {
-      if (dir == 2) {
+      const long long oL = d.idx(lx, ly, lz), oR = d.idx(rx, ry, rz);
+      double Ax, Ay, Az, Bx, By, Bz, Cx, Cy, Cz;
+      if (dir == 0) {
+        Ax = geo(g, d, CS_G_XF_N, 0, p, i, j, k);
+        Ay = geo(g, d, CS_G_XF_N, 1, p, i, j, k);
+        Az = geo(g, d, CS_G_XF_N, 2, p, i, j, k);
+        Cx = geo(g, d, CS_G_XF_CEN, 0, p, i, j, k);
+        Cy = geo(g, d, CS_G_XF_CEN, 1, p, i, j, k);
+        Cz = geo(g, d, CS_G_XF_CEN, 2, p, i, j, k);
+        const double tt = 1.0 / fmax(sqrt(Cx * Cx + Cy * Cy + Cz * Cz), ph.smallnum);
+        Cx = Cx * tt;
+        Cy = Cy * tt;
+        Cz = Cz * tt;
+        Bx = Cy * Az - Cz * Ay;
+        By = Cz * Ax - Cx * Az;
+        Bz = Cx * Ay - Cy * Ax;
+      } else if (dir == 1) {
+        Ax = geo(g, d, CS_G_YF_N, 0, p, i, j, k);
+        Ay = geo(g, d, CS_G_YF_N, 1, p, i, j, k);
+        Az = geo(g, d, CS_G_YF_N, 2, p, i, j, k);
+        Bx = geo(g, d, CS_G_YF_CEN, 0, p, i, j, k);
+        By = geo(g, d, CS_G_YF_CEN, 1, p, i, j, k);
+        Bz = geo(g, d, CS_G_YF_CEN, 2, p, i, j, k);
+        const double tt = 1.0 / fmax(sqrt(Bx * Bx + By * By + Bz * Bz), ph.smallnum);
+        Bx = Bx * tt;
+        By = By * tt;
+        Bz = Bz * tt;
+        Cx = Ay * Bz - Az * By;
+        Cy = Az * Bx - Ax * Bz;
+        Cz = Ax * By - Ay * Bx;
+      } else {
+        auto vt = [&](int q, int x, int y) { return geo(g, d, CS_G_VERT, q, p, x, y, k); };
         Ax = geo(g, d, CS_G_ZF_N, jq, p, i, j, k);
         Ay = geo(g, d, CS_G_ZF_N, 5 + jq, p, i, j, k);
         Az = geo(g, d, CS_G_ZF_N, 10 + jq, p, i, j, k);
@@ -120,9 +110,9 @@ __global__ void __launch_bounds__(TPB) k_flux(Dims d, PhysC ph, DGeom g, DState 
         Ax = Ax * tt;
         Ay = Ay * tt;
         Az = Az * tt;
-        Bx = vbx;
-        By = vby;
-        Bz = vbz;
+        Bx = vt(0, i, j) + vt(0, i, j - 1) - vt(0, i - 1, j) - vt(0, i - 1, j - 1);
+        By = vt(1, i, j) + vt(1, i, j - 1) - vt(1, i - 1, j) - vt(1, i - 1, j - 1);
+        Bz = vt(2, i, j) + vt(2, i, j - 1) - vt(2, i - 1, j) - vt(2, i - 1, j - 1);
         tt = Bx * Ax + By * Ay + Bz * Az;
         Bx = Bx - tt * Ax;
         By = By - tt * Ay;
@@ -141,20 +131,36 @@ __global__ void __launch_bounds__(TPB) k_flux(Dims d, PhysC ph, DGeom g, DState 
       }
       const double px = geo(g, d, QP, jq, p, i, j, k), py = geo(g, d, QP, 5 + jq, p, i, j, k),
                    pz = geo(g, d, QP, 10 + jq, p, i, j, k);
-      const double x = (px - lcx) * obl0, y = (py - lcy) * obl0, z = (pz - lcz) * obl0;
-      const double x2 = (px - rcx) * obl02, y2 = (py - rcy) * obl02, z2 = (pz - rcz) * obl02;
-      const double wt = geo(g, d, QW, jq, p, i, j, k);
+      double x, y, z, x2, y2, z2;
+      {
+        const double obl0 = 1.0 / fmax(geo(g, d, CS_G_V_SCALE, 0, p, lx, ly, lz), ph.smallnum);
+        const double obl02 = 1.0 / fmax(geo(g, d, CS_G_V_SCALE, 0, p, rx, ry, rz), ph.smallnum);
+        x = (px - geo(g, d, CS_G_V_CEN, 0, p, lx, ly, lz)) * obl0;
+        y = (py - geo(g, d, CS_G_V_CEN, 1, p, lx, ly, lz)) * obl0;
+        z = (pz - geo(g, d, CS_G_V_CEN, 2, p, lx, ly, lz)) * obl0;
+        x2 = (px - geo(g, d, CS_G_V_CEN, 0, p, rx, ry, rz)) * obl02;
+        y2 = (py - geo(g, d, CS_G_V_CEN, 1, p, rx, ry, rz)) * obl02;
+        z2 = (pz - geo(g, d, CS_G_V_CEN, 2, p, rx, ry, rz)) * obl02;
+      }
       double VL[8], VR[8];
-#pragma unroll
-      for (int c = 0; c < 8; ++c) {
-        double vl[10], vr[10];
+      {
+        double cL[10], cR[10];
 #pragma unroll
         for (int m = 0; m < 10; ++m) {
-          vl[m] = Vm(s, d, c, m, p, oL);
-          vr[m] = Vm(s, d, c, m, p, oR);
+          cL[m] = geo(g, d, CS_G_COEF, m, p, lx, ly, lz);
+          cR[m] = geo(g, d, CS_G_COEF, m, p, rx, ry, rz);
         }
-        VL[c] = d_poly10(vl, cL, x, y, z);
-        VR[c] = d_poly10(vr, cR, x2, y2, z2);
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+          double vl[10], vr[10];
+#pragma unroll
+          for (int m = 0; m < 10; ++m) {
+            vl[m] = Vm(s, d, c, m, p, oL);
+            vr[m] = Vm(s, d, c, m, p, oR);
+          }
+          VL[c] = d_poly10(vl, cL, x, y, z);
+          VR[c] = d_poly10(vr, cR, x2, y2, z2);
+        }
       }
       const double* E = s.ent;
       const double entL = E[((long long)0 * NPANEL + p) * d.S + oL] + E[((long long)1 * NPANEL + p) * d.S + oL] * x +
@@ -178,38 +184,40 @@ __global__ void __launch_bounds__(TPB) k_flux(Dims d, PhysC ph, DGeom g, DState 
       }
       double FlL[8], FlR[8], FL[8], FR[8], SL, SR, entF;
       d_hll(ph, VL, VR, entL, entR, FlL, FlR, FL, FR, SL, SR, entF);
+      const long long fo = d.idx(i, j, k);
       if (jq == 0) {
         SLo[((long long)p) * d.S + fo] = SL;
         SHi[((long long)p) * d.S + fo] = SR;
         EF[((long long)p) * d.S + fo] = entF;
       }
-      // rotate back to global components and accumulate both sides
-      auto back = [&](const double* W, double* O) {
-        O[0] = W[0];
-        O[1] = Ax * W[1] + Bx * W[2] + Cx * W[3];
-        O[2] = Ay * W[1] + By * W[2] + Cy * W[3];
-        O[3] = Az * W[1] + Bz * W[2] + Cz * W[3];
-        O[4] = W[4];
-        O[5] = Ax * W[5] + Bx * W[6] + Cx * W[7];
-        O[6] = Ay * W[5] + By * W[6] + Cy * W[7];
-        O[7] = Az * W[5] + Bz * W[6] + Cz * W[7];
+      const double wt = geo(g, d, QW, jq, p, i, j, k);
+      const double area = geo(g, d, AR, 0, p, i, j, k);
+      const double volL = geo(g, d, CS_G_V_VOL, 0, p, lx, ly, lz), volR = geo(g, d, CS_G_V_VOL, 0, p, rx, ry, rz);
+      // rotate back to global components: fluctuation + flux on each side
+      auto back = [&](const double* W, int c) {
+        if (c == 0 || c == 4) return W[c];
+        const int o = c < 4 ? 1 : 5, a = c - o;
+        const double ea = a == 0 ? Ax : (a == 1 ? Ay : Az), eb = a == 0 ? Bx : (a == 1 ? By : Bz),
+                     ec = a == 0 ? Cx : (a == 1 ? Cy : Cz);
+        return ea * W[o] + eb * W[o + 1] + ec * W[o + 2];
       };
-      double Fm[8], Fp[8], FLL[8], FRR[8];
-      back(FlL, Fm);
-      back(FlR, Fp);
-      back(FL, FLL);
-      back(FR, FRR);
 #pragma unroll
       for (int c = 0; c < 8; ++c) {
-        accL[c] = accL[c] + wt * (Fm[c] + FLL[c]) * area / volL;
-        accR[c] = accR[c] + wt * (Fp[c] - FRR[c]) * area / volR;
+        red[jq][c][lane] = wt * (back(FlL, c) + back(FL, c)) * area / volL;
+        red[jq][8 + c][lane] = wt * (back(FlR, c) - back(FR, c)) * area / volR;
       }
     }
+    __syncthreads();
+    if (valid) {
+      const long long fo = d.idx(i, j, k);
+      for (int c = jq; c < 16; c += 5) {
+        double acc = 0.0;
 #pragma unroll
-    for (int c = 0; c < 8; ++c) {
-      F[((long long)c * NPANEL + p) * d.S + fo] = accL[c];
-      F[((long long)(8 + c) * NPANEL + p) * d.S + fo] = accR[c];
+        for (int q = 0; q < 5; ++q) acc = acc + red[q][c][lane];
+        F[((long long)c * NPANEL + p) * d.S + fo] = acc;
+      }
     }
+    __syncthreads();
   }
 }
 
@@ -270,12 +278,13 @@ void launch_fluxes(Solve& sv) {
   Range3 fx = {-1, N + 1, 0, N + 1, 0, nr + 1};
   Range3 fy = {0, N + 1, -1, N + 1, 0, nr + 1};
   Range3 fz = {0, N + 1, 0, N + 1, -1, nr + 1};
-  k_flux<<<blocks_for(fx.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, fx, 0);
-  mark(sv, "k_flux");
-  k_flux<<<blocks_for(fy.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, fy, 1);
-  mark(sv, "k_flux");
-  k_flux<<<blocks_for(fz.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, fz, 2);
-  mark(sv, "k_flux");
+  const Range3 fr[3] = {fx, fy, fz};
+  for (int dir = 0; dir < 3; ++dir) {
+    const long long nt = (fr[dir].count() + FLUX_FACES - 1) / FLUX_FACES;
+    const int nb = (int)std::min<long long>(nt, (long long)sv.sm_count * 32);
+    k_flux<<<nb, FLUX_FACES * 5, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, fr[dir], dir);
+    mark(sv, "k_flux");
+  }
   Range3 z = {0, N + 1, 0, N + 1, 0, nr + 1};
   k_gather<<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, sv.st, z);
   mark(sv, "k_gather");

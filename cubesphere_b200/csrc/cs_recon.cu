@@ -322,11 +322,63 @@ __device__ __forceinline__ void coef10(const DGeom& g, const Dims& d, int p, int
   for (int t = 0; t < 10; ++t) c[t] = geo(g, d, CS_G_COEF, t, p, i, j, k);
 }
 
+// Row rr of the 18 x 9 least-squares matrix of STEP 7.b (421:3869-4001)
+// for zone (i,j,k): neighbour centroid offsets scaled by l0, quadratic
+// modes corrected by the neighbour's own moments.
+__device__ __forceinline__ void w7b_row(const Dims& d, const PhysC& ph, const DGeom& g, int p, int i, int j, int k,
+                                        const Nbr12& n, int rr, double cx, double cy, double cz, double l0, double obl0,
+                                        const double* c0, double* A, long long& off) {
+  const int w = c_n18[rr][0], dz = c_n18[rr][1];
+  const int zx = w < 0 ? i : n.x[w], zy = w < 0 ? j : n.y[w], zz = k + dz;
+  off = d.idx(zx, zy, zz);
+  const double x = (geo(g, d, CS_G_V_CEN, 0, p, zx, zy, zz) - cx) * obl0;
+  const double y = (geo(g, d, CS_G_V_CEN, 1, p, zx, zy, zz) - cy) * obl0;
+  const double z = (geo(g, d, CS_G_V_CEN, 2, p, zx, zy, zz) - cz) * obl0;
+  const double lj = fmax(geo(g, d, CS_G_V_SCALE, 0, p, zx, zy, zz), ph.smallnum);
+  const double rt = lj / l0, r2 = rt * rt;
+  A[0] = x;
+  A[1] = y;
+  A[2] = z;
+  A[3] = x * x - c0[4] + geo(g, d, CS_G_COEF, 4, p, zx, zy, zz) * r2;
+  A[4] = y * y - c0[5] + geo(g, d, CS_G_COEF, 5, p, zx, zy, zz) * r2;
+  A[5] = z * z - c0[6] + geo(g, d, CS_G_COEF, 6, p, zx, zy, zz) * r2;
+  A[6] = x * y - c0[7] + geo(g, d, CS_G_COEF, 7, p, zx, zy, zz) * r2;
+  A[7] = y * z - c0[8] + geo(g, d, CS_G_COEF, 8, p, zx, zy, zz) * r2;
+  A[8] = x * z - c0[9] + geo(g, d, CS_G_COEF, 9, p, zx, zy, zz) * r2;
+}
+
+// Inverse of the 9 x 9 normal matrix A^T A of STEP 7.b for one zone.
+__device__ __forceinline__ void w7b_minv(const Dims& d, const PhysC& ph, const DGeom& g, int p, int i, int j, int k,
+                                         const Nbr12& n, double cx, double cy, double cz, double l0, double obl0,
+                                         const double* c0, double* Minv) {
+  double M[81];
+#pragma unroll
+  for (int t = 0; t < 81; ++t) M[t] = 0.0;
+  for (int rr = 0; rr < 18; ++rr) {
+    double A[9];
+    long long off;
+    w7b_row(d, ph, g, p, i, j, k, n, rr, cx, cy, cz, l0, obl0, c0, A, off);
+#pragma unroll
+    for (int a = 0; a < 9; ++a)
+#pragma unroll
+      for (int b = a; b < 9; ++b) M[a * 9 + b] = M[a * 9 + b] + A[a] * A[b];
+  }
+#pragma unroll
+  for (int a = 0; a < 9; ++a)
+#pragma unroll
+    for (int b = 0; b < a; ++b) M[a * 9 + b] = M[b * 9 + a];
+  d_matinv<9>(M, Minv);
+}
+
 // STEP 7.b (421:3869-4551): 18-zone quadratic least squares hybridised
-// with the linear WENO slopes (MRWENO weights, flattener damping).
+// with the linear WENO slopes (MRWENO weights, flattener damping).  With
+// kCached the inverse normal matrix (geometry only) comes from the
+// operator cache built at mesh build; the result is the same either way.
+template <bool kCached>
 __global__ void __launch_bounds__(TPB) k_weno7b(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
   const double ob12 = 1.0 / 12.0, ob180 = 1.0 / 180.0, ob144 = 1.0 / 144.0;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
+  const long long nr_ = r.count();
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nr_; t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
     r.decode(t, p, i, j, k);
     if (mask_at(g, d, p, i, j) != 1) continue;
@@ -336,59 +388,43 @@ __global__ void __launch_bounds__(TPB) k_weno7b(Dims d, PhysC ph, DGeom g, DStat
     coef10(g, d, p, i, j, k, c0);
     const double cx = geo(g, d, CS_G_V_CEN, 0, p, i, j, k), cy = geo(g, d, CS_G_V_CEN, 1, p, i, j, k),
                  cz = geo(g, d, CS_G_V_CEN, 2, p, i, j, k);
-    double A[18][9];
-    long long off[18];
+    // kCached: the inverse is read from the cache where it is used (L1
+    // serves the re-reads of the later components).
+    double Minv[kCached ? 1 : 81];
+    if (!kCached) w7b_minv(d, ph, g, p, i, j, k, n, cx, cy, cz, l0, obl0, c0, Minv);
+    const double* mc = s.op_m9 + t;
+    auto MI = [&](int e) { return kCached ? __ldg(mc + (long long)e * nr_) : Minv[kCached ? 0 : e]; };
+    double v0[NVAR];
+#pragma unroll
+    for (int q = 0; q < NVAR; ++q) v0[q] = s.V[((long long)q * NPANEL + p) * d.S + d.idx(i, j, k)];
+    double Y[NVAR][9];
+#pragma unroll
+    for (int q = 0; q < NVAR; ++q)
+#pragma unroll
+      for (int a = 0; a < 9; ++a) Y[q][a] = 0.0;
+#pragma unroll 1
     for (int rr = 0; rr < 18; ++rr) {
-      const int w = c_n18[rr][0], dz = c_n18[rr][1];
-      const int zx = w < 0 ? i : n.x[w], zy = w < 0 ? j : n.y[w], zz = k + dz;
-      off[rr] = d.idx(zx, zy, zz);
-      const double x = (geo(g, d, CS_G_V_CEN, 0, p, zx, zy, zz) - cx) * obl0;
-      const double y = (geo(g, d, CS_G_V_CEN, 1, p, zx, zy, zz) - cy) * obl0;
-      const double z = (geo(g, d, CS_G_V_CEN, 2, p, zx, zy, zz) - cz) * obl0;
-      const double lj = fmax(geo(g, d, CS_G_V_SCALE, 0, p, zx, zy, zz), ph.smallnum);
-      const double rt = lj / l0, r2 = rt * rt;
-      A[rr][0] = x;
-      A[rr][1] = y;
-      A[rr][2] = z;
-      A[rr][3] = x * x - c0[4] + geo(g, d, CS_G_COEF, 4, p, zx, zy, zz) * r2;
-      A[rr][4] = y * y - c0[5] + geo(g, d, CS_G_COEF, 5, p, zx, zy, zz) * r2;
-      A[rr][5] = z * z - c0[6] + geo(g, d, CS_G_COEF, 6, p, zx, zy, zz) * r2;
-      A[rr][6] = x * y - c0[7] + geo(g, d, CS_G_COEF, 7, p, zx, zy, zz) * r2;
-      A[rr][7] = y * z - c0[8] + geo(g, d, CS_G_COEF, 8, p, zx, zy, zz) * r2;
-      A[rr][8] = x * z - c0[9] + geo(g, d, CS_G_COEF, 9, p, zx, zy, zz) * r2;
-    }
-    double M[81], Minv[81];
+      double A[9];
+      long long off;
+      w7b_row(d, ph, g, p, i, j, k, n, rr, cx, cy, cz, l0, obl0, c0, A, off);
 #pragma unroll
-    for (int a = 0; a < 9; ++a)
+      for (int q = 0; q < NVAR; ++q) {
+        const double R = s.V[((long long)q * NPANEL + p) * d.S + off] - v0[q];
 #pragma unroll
-      for (int b = 0; b < 9; ++b) {
-        double sacc = 0.0;
-#pragma unroll
-        for (int rr = 0; rr < 18; ++rr) sacc = sacc + A[rr][a] * A[rr][b];
-        M[a * 9 + b] = sacc;
+        for (int a = 0; a < 9; ++a) Y[q][a] = Y[q][a] + A[a] * R;
       }
-    d_matinv<9>(M, Minv);
+    }
     const double f = s.flatA[d.at(0, p, i, j, k)];
     const double betalo = f + (1.0 - f) * 2.0;
     const double ghi = f * 0.6 + (1.0 - f) * 0.95, glo = 1.0 - ghi, obghi = 1.0 / ghi, grat = glo / ghi;
+#pragma unroll 1
     for (int q = 0; q < NVAR; ++q) {
-      const double* Vq = s.V + ((long long)q * NPANEL + p) * d.S;
-      const double v0 = Vq[d.idx(i, j, k)];
-      double Y[9];
-#pragma unroll
-      for (int a = 0; a < 9; ++a) Y[a] = 0.0;
-#pragma unroll
-      for (int rr = 0; rr < 18; ++rr) {
-        const double R = Vq[off[rr]] - v0;
-#pragma unroll
-        for (int a = 0; a < 9; ++a) Y[a] = Y[a] + A[rr][a] * R;
-      }
       double X[9];
 #pragma unroll
       for (int a = 0; a < 9; ++a) {
         double sacc = 0.0;
 #pragma unroll
-        for (int b = 0; b < 9; ++b) sacc = sacc + Minv[a * 9 + b] * Y[b];
+        for (int b = 0; b < 9; ++b) sacc = sacc + MI(a * 9 + b) * Y[q][b];
         X[a] = sacc;
       }
       const double v2 = Vat(s, d, q, 1, p, i, j, k), v3 = Vat(s, d, q, 2, p, i, j, k), v4 = Vat(s, d, q, 3, p, i, j, k);
@@ -415,6 +451,24 @@ __global__ void __launch_bounds__(TPB) k_weno7b(Dims d, PhysC ph, DGeom g, DStat
 #pragma unroll
       for (int m = 4; m < 10; ++m) Vat(s, d, q, m, p, i, j, k) = (Whi * Phi[m - 1]) * x;
     }
+  }
+}
+
+__global__ void k_ops_m9(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
+  const long long nr_ = r.count();
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nr_; t += (long long)gridDim.x * blockDim.x) {
+    int p, i, j, k;
+    r.decode(t, p, i, j, k);
+    if (mask_at(g, d, p, i, j) != 1) continue;
+    const Nbr12 n = load_nbr(g, d, p, i, j);
+    const double l0 = fmax(geo(g, d, CS_G_V_SCALE, 0, p, i, j, k), ph.smallnum), obl0 = 1.0 / l0;
+    double c0[10];
+    coef10(g, d, p, i, j, k, c0);
+    const double cx = geo(g, d, CS_G_V_CEN, 0, p, i, j, k), cy = geo(g, d, CS_G_V_CEN, 1, p, i, j, k),
+                 cz = geo(g, d, CS_G_V_CEN, 2, p, i, j, k);
+    double Minv[81];
+    w7b_minv(d, ph, g, p, i, j, k, n, cx, cy, cz, l0, obl0, c0, Minv);
+    for (int e = 0; e < 81; ++e) s.op_m9[(long long)e * nr_ + t] = Minv[e];
   }
 }
 
@@ -821,7 +875,7 @@ __global__ void __launch_bounds__(32 * ADP_WARPS) k_adp(Dims d, PhysC ph, DGeom 
 // forward and back substitution against the factors of its zone, which are
 // stored element-major so that a warp reads them coalesced.
 constexpr int ADPS_TPB = 128;
-__global__ void __launch_bounds__(ADPS_TPB) k_adp_solve(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
+__global__ void __launch_bounds__(ADPS_TPB, 4) k_adp_solve(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
   __shared__ double rhs_s[36][ADPS_TPB];
   const long long n = r.count();
   const int tid = threadIdx.x;
@@ -948,11 +1002,70 @@ __global__ void k_efield_b(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
   }
 }
 
+// Row rr (0: the zone itself, 1..18: the STEP 7.b neighbours) of the
+// 19 x 10 interpolation least-squares matrix of STEP 9.c (421:8464-8620).
+__device__ __forceinline__ void e9c_row(const Dims& d, const DGeom& g, int p, int i, int j, int k, const Nbr12& n,
+                                        int rr, double cx, double cy, double cz, double obl0, const double* c0, double* A,
+                                        long long& off) {
+  if (rr == 0) {
+    off = d.idx(i, j, k);
+    A[0] = 1.0;
+    A[1] = 0.0;
+    A[2] = 0.0;
+    A[3] = 0.0;
+#pragma unroll
+    for (int m = 4; m < 10; ++m) A[m] = 0.0 * 0.0 - c0[m];
+    return;
+  }
+  const int w = c_n18[rr - 1][0], dz = c_n18[rr - 1][1];
+  const int zx = w < 0 ? i : n.x[w], zy = w < 0 ? j : n.y[w], zz = k + dz;
+  off = d.idx(zx, zy, zz);
+  const double x = (geo(g, d, CS_G_V_CEN, 0, p, zx, zy, zz) - cx) * obl0;
+  const double y = (geo(g, d, CS_G_V_CEN, 1, p, zx, zy, zz) - cy) * obl0;
+  const double z = (geo(g, d, CS_G_V_CEN, 2, p, zx, zy, zz) - cz) * obl0;
+  A[0] = 1.0;
+  A[1] = x;
+  A[2] = y;
+  A[3] = z;
+  A[4] = x * x - c0[4];
+  A[5] = y * y - c0[5];
+  A[6] = z * z - c0[6];
+  A[7] = x * y - c0[7];
+  A[8] = y * z - c0[8];
+  A[9] = x * z - c0[9];
+}
+
+__device__ __forceinline__ void e9c_minv(const Dims& d, const DGeom& g, int p, int i, int j, int k, const Nbr12& n,
+                                         double cx, double cy, double cz, double obl0, const double* c0, double* Minv) {
+  double M[100];
+#pragma unroll
+  for (int t = 0; t < 100; ++t) M[t] = 0.0;
+  for (int rr = 0; rr < 19; ++rr) {
+    double A[10];
+    long long off;
+    e9c_row(d, g, p, i, j, k, n, rr, cx, cy, cz, obl0, c0, A, off);
+#pragma unroll
+    for (int a = 0; a < 10; ++a)
+#pragma unroll
+      for (int b = a; b < 10; ++b) M[a * 10 + b] = M[a * 10 + b] + A[a] * A[b];
+  }
+#pragma unroll
+  for (int a = 0; a < 10; ++a)
+#pragma unroll
+    for (int b = 0; b < a; ++b) M[a * 10 + b] = M[b * 10 + a];
+  d_matinv<10>(M, Minv);
+}
+
 // STEP 9.c (421:8464-9350): 19-point interpolation least squares
 // hybridised with the slopes; the point value is flattened toward E_pt.
+// Only the point value (mode 1) is stored: the LLF edge solver consumes
+// nothing else.  kCached: the inverse normal matrix comes from the
+// operator cache.
+template <bool kCached>
 __global__ void __launch_bounds__(TPB) k_efield_c(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
   const double ob12 = 1.0 / 12.0, ob180 = 1.0 / 180.0, ob144 = 1.0 / 144.0;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
+  const long long nr_ = r.count();
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nr_; t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
     r.decode(t, p, i, j, k);
     if (mask_at(g, d, p, i, j) != 1) continue;
@@ -962,64 +1075,49 @@ __global__ void __launch_bounds__(TPB) k_efield_c(Dims d, PhysC ph, DGeom g, DSt
     coef10(g, d, p, i, j, k, c0);
     const double cx = geo(g, d, CS_G_V_CEN, 0, p, i, j, k), cy = geo(g, d, CS_G_V_CEN, 1, p, i, j, k),
                  cz = geo(g, d, CS_G_V_CEN, 2, p, i, j, k);
-    double A[19][10];
-    long long off[19];
-    off[0] = d.idx(i, j, k);
-    {
-      const double row0[10] = {1.0, 0.0, 0.0, 0.0, 0.0 * 0.0 - c0[4], 0.0 * 0.0 - c0[5], 0.0 * 0.0 - c0[6],
-                               0.0 * 0.0 - c0[7], 0.0 * 0.0 - c0[8], 0.0 * 0.0 - c0[9]};
-      for (int m = 0; m < 10; ++m) A[0][m] = row0[m];
-    }
-    for (int rr = 0; rr < 18; ++rr) {
-      const int w = c_n18[rr][0], dz = c_n18[rr][1];
-      const int zx = w < 0 ? i : n.x[w], zy = w < 0 ? j : n.y[w], zz = k + dz;
-      off[rr + 1] = d.idx(zx, zy, zz);
-      const double x = (geo(g, d, CS_G_V_CEN, 0, p, zx, zy, zz) - cx) * obl0;
-      const double y = (geo(g, d, CS_G_V_CEN, 1, p, zx, zy, zz) - cy) * obl0;
-      const double z = (geo(g, d, CS_G_V_CEN, 2, p, zx, zy, zz) - cz) * obl0;
-      A[rr + 1][0] = 1.0;
-      A[rr + 1][1] = x;
-      A[rr + 1][2] = y;
-      A[rr + 1][3] = z;
-      A[rr + 1][4] = x * x - c0[4];
-      A[rr + 1][5] = y * y - c0[5];
-      A[rr + 1][6] = z * z - c0[6];
-      A[rr + 1][7] = x * y - c0[7];
-      A[rr + 1][8] = y * z - c0[8];
-      A[rr + 1][9] = x * z - c0[9];
-    }
-    double M[100], Minv[100];
-    for (int a = 0; a < 10; ++a)
-      for (int b = 0; b < 10; ++b) {
-        double acc = 0.0;
-        for (int rr = 0; rr < 19; ++rr) acc = acc + A[rr][a] * A[rr][b];
-        M[a * 10 + b] = acc;
+    double Minv[kCached ? 1 : 100];
+    if (!kCached) e9c_minv(d, g, p, i, j, k, n, cx, cy, cz, obl0, c0, Minv);
+    const double* mc = s.op_m10 + t;
+    auto MI = [&](int e) { return kCached ? __ldg(mc + (long long)e * nr_) : Minv[kCached ? 0 : e]; };
+    double Y[3][10];
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+#pragma unroll
+      for (int a = 0; a < 10; ++a) Y[q][a] = 0.0;
+#pragma unroll 1
+    for (int rr = 0; rr < 19; ++rr) {
+      double A[10];
+      long long off;
+      e9c_row(d, g, p, i, j, k, n, rr, cx, cy, cz, obl0, c0, A, off);
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        const double R = s.Esnap[((long long)q * NPANEL + p) * d.S + off];
+#pragma unroll
+        for (int a = 0; a < 10; ++a) Y[q][a] = Y[q][a] + A[a] * R;
       }
-    d_matinv<10>(M, Minv);
+    }
     const double f = s.flatA[d.at(0, p, i, j, k)];
     const double betalo = f + (1.0 - f) * 2.0;
     const double ghi = f * 0.6 + (1.0 - f) * 0.95, glo = 1.0 - ghi, obghi = 1.0 / ghi, grat = glo / ghi;
+#pragma unroll 1
     for (int q = 0; q < 3; ++q) {
-      const double* Eq = s.Esnap + ((long long)q * NPANEL + p) * d.S;
-      const double Ept = Eq[off[0]];
-      double Y[10];
-      for (int a = 0; a < 10; ++a) Y[a] = 0.0;
-      for (int rr = 0; rr < 19; ++rr) {
-        const double R = Eq[off[rr]];
-        for (int a = 0; a < 10; ++a) Y[a] = Y[a] + A[rr][a] * R;
-      }
       double X[10];
+#pragma unroll
       for (int a = 0; a < 10; ++a) {
         double acc = 0.0;
-        for (int b = 0; b < 10; ++b) acc = acc + Minv[a * 10 + b] * Y[b];
+#pragma unroll
+        for (int b = 0; b < 10; ++b) acc = acc + MI(a * 10 + b) * Y[q][b];
         X[a] = acc;
       }
       double e[4];
-      e[0] = Ept;
+      e[0] = s.Esnap[((long long)q * NPANEL + p) * d.S + d.idx(i, j, k)];
+#pragma unroll
       for (int m = 1; m < 4; ++m) e[m] = s.E[d.at(m * 3 + q, p, i, j, k)];
       const double ISlo = betalo * (e[1] * e[1] + e[2] * e[2] + e[3] * e[3]) * ob12;
       double Phi[10];
+#pragma unroll
       for (int m = 0; m < 4; ++m) Phi[m] = X[m] * obghi - e[m] * grat;
+#pragma unroll
       for (int m = 4; m < 10; ++m) Phi[m] = X[m] * obghi;
       const double IShi = (Phi[1] * Phi[1] + Phi[2] * Phi[2] + Phi[3] * Phi[3]) * ob12 +
                           (Phi[4] * Phi[4]) * (sqr(c0[4] - ob12) + ob180) + (Phi[5] * Phi[5]) * (sqr(c0[5] - ob12) + ob180) +
@@ -1032,10 +1130,26 @@ __global__ void __launch_bounds__(TPB) k_efield_c(Dims d, PhysC ph, DGeom g, DSt
       Whi = Whi * aa;
       const double x = 1.0 - f;
       const double e0 = Whi * Phi[0] + Wlo * e[0];
-      s.E[d.at(q, p, i, j, k)] = Ept * f + e0 * x;
-      for (int m = 1; m < 4; ++m) s.E[d.at(m * 3 + q, p, i, j, k)] = (Whi * Phi[m] + Wlo * e[m]) * x;
-      for (int m = 4; m < 10; ++m) s.E[d.at(m * 3 + q, p, i, j, k)] = (Whi * Phi[m]) * x;
+      s.E[d.at(q, p, i, j, k)] = e[0] * f + e0 * x;
     }
+  }
+}
+
+__global__ void k_ops_m10(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
+  const long long nr_ = r.count();
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nr_; t += (long long)gridDim.x * blockDim.x) {
+    int p, i, j, k;
+    r.decode(t, p, i, j, k);
+    if (mask_at(g, d, p, i, j) != 1) continue;
+    const Nbr12 n = load_nbr(g, d, p, i, j);
+    const double obl0 = 1.0 / fmax(geo(g, d, CS_G_V_SCALE, 0, p, i, j, k), ph.smallnum);
+    double c0[10];
+    coef10(g, d, p, i, j, k, c0);
+    const double cx = geo(g, d, CS_G_V_CEN, 0, p, i, j, k), cy = geo(g, d, CS_G_V_CEN, 1, p, i, j, k),
+                 cz = geo(g, d, CS_G_V_CEN, 2, p, i, j, k);
+    double Minv[100];
+    e9c_minv(d, g, p, i, j, k, n, cx, cy, cz, obl0, c0, Minv);
+    for (int e = 0; e < 100; ++e) s.op_m10[(long long)e * nr_ + t] = Minv[e];
   }
 }
 
@@ -1080,7 +1194,10 @@ void launch_weno(Solve& sv) {
   Range3 a = shrink(d, 1), b = shrink(d, 2);
   k_weno7a<<<blocks_for(a.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, a);
   mark(sv, "k_weno7a");
-  k_weno7b<<<blocks_for(b.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, b);
+  if (sv.st.op_m9)
+    k_weno7b<true><<<blocks_for(b.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, b);
+  else
+    k_weno7b<false><<<blocks_for(b.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, b);
   mark(sv, "k_weno7b");
 }
 
@@ -1121,6 +1238,20 @@ void launch_faceB_adp(Solve& sv) {
 }
 
 long long adp_range_count(const Dims& d) { return shrink(d, 1).count(); }
+long long lsq_range_count(const Dims& d) { return shrink(d, 2).count(); }
+
+void launch_ops_build(Solve& sv) {
+  const Dims& d = sv.d;
+  Range3 b = shrink(d, 2);
+  if (sv.st.op_m9) {
+    k_ops_m9<<<blocks_for(b.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, b);
+    mark(sv, "k_ops_m9");
+  }
+  if (sv.st.op_m10) {
+    k_ops_m10<<<blocks_for(b.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, b);
+    mark(sv, "k_ops_m10");
+  }
+}
 
 void set_adp_smem_limits() {
   const int smem = (int)(sizeof(AdpSmem) * ADP_WARPS);
@@ -1146,7 +1277,10 @@ void launch_efield(Solve& sv) {
   mark(sv, "k_efield_a");
   k_efield_b<<<blocks_for(a.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, a);
   mark(sv, "k_efield_b");
-  k_efield_c<<<blocks_for(b.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, b);
+  if (sv.st.op_m10)
+    k_efield_c<true><<<blocks_for(b.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, b);
+  else
+    k_efield_c<false><<<blocks_for(b.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, b);
   mark(sv, "k_efield_c");
 }
 

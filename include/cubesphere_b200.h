@@ -91,6 +91,9 @@ typedef struct cs_params {
  * it in every stage instead.  The cache is also skipped automatically when
  * the device lacks the memory.  Results are identical either way. */
 #define CS_FLAG_NO_ADP_CACHE 1
+/* cs_params.flags: likewise for the inverse normal matrices of the
+ * least-squares reconstructions of the primitives and of E (1.4 KB per zone). */
+#define CS_FLAG_NO_OP_CACHE 2
 
 /* Seeded initial-state description (new generator cases of the problem
  * library, built with the reference mechanism of 820init_patch_cube_sphere.f). */

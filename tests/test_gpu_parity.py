@@ -118,9 +118,10 @@ def test_routines_in_sequence(shell16):
 
 
 @pytest.mark.parametrize("name,nsteps,flags", [("shell16", 2, 0), ("surface32", 2, 0),
-                                               ("shell16", 1, cs.CS_FLAG_NO_ADP_CACHE)])
+                                               ("shell16", 1, cs.CS_FLAG_NO_ADP_CACHE | cs.CS_FLAG_NO_OP_CACHE)])
 def test_whole_steps_match_oracle(name, nsteps, flags):
-    """flags=0 uses the resident ADP factors, CS_FLAG_NO_ADP_CACHE factors per stage."""
+    """flags=0 uses the resident geometry-only operators (ADP factors, least-squares
+    inverses); the NO_*_CACHE flags rebuild them in every stage."""
     s, o, st = make_pair(name, flags)
     dt_s = s.evaluate_timestep(1e30)
     dt_o = o.evaluate_timestep(1e30)
