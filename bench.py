@@ -42,12 +42,17 @@ ALGO_WORDS_PER_UNIT = {
     # 8 comps x 10 modes in/out of V, flattener, 18-zone centroids (re-reads
     # excluded), coefficients 10
     "k_weno7b": 80 + 1 + 4 + 10 + 72,
-    # face-B quadrature values of 6 faces (30), V B-modes out (30), U(6:8), E
-    # mode 1, geometry of 6 faces (3 normals + 5 weights + 15 points each)
-    "k_adp": 30 + 30 + 4 + 6 * 23 + 14,
-    # 3 faces per zone: 2 x 80 modes of the two zones amortised to 80 per
-    # zone, 3 x (15 + 5 + 3 + 1 + 3) geometry, 16 outputs + 3 speeds
-    "k_flux": 80 + 27 + 2 * 8 + 3 + 1,
+    # resident KKT factors (1296) + pivots (36 bytes), face-B quadrature
+    # values (30), B modes in and out (60), U(5:8) in and out (8), geometry
+    # of the 6 faces (normals 42, points 90, weights 30) and of the zone (14)
+    "k_adp_solve": 1296 + 4.5 + 30 + 60 + 8 + 162 + 14,
+    # 80 modes + 4 entropy modes + 10 moments + scale/centroid in, 30 face
+    # points x 3 coordinates of geometry, 270 face-state values out
+    "k_face_states": 80 + 4 + 14 + 90 + 270,
+    # per face (one launch per direction, units = zones): two face states
+    # (2 x 45), geometry (15 points + 5 weights + normals/centroid 6 + area
+    # + 2 volumes + scale), 16 contributions + 3 speeds/entropy flux out
+    "k_flux": 90 + 30 + 19,
     "k_efield_c": 30 + 8 + 10 + 30,
     "k_positivity": 80 + 4 + 80,
     "k_faceB": 80 + 1 + 20 + 5,
@@ -283,11 +288,13 @@ def run_gpu(args):
     units = 6 * (N + 2 * G - 2) ** 2 * (nr + 2 * G - 2)  # zones of the shrink-1 range (7.a / 8.d / 9.b)
     if dname in ("k_weno7b", "k_efield_c"):
         units = 6 * (N + 2 * G - 4) ** 2 * (nr + 2 * G - 4)
+    if dname in ("k_flux", "k_face_states"):
+        units = 6 * (N + 4) ** 2 * (nr + 4)
     words = ALGO_WORDS_PER_UNIT.get(dname)
     roof = None
     if words is not None:
         per_launch = words * 8.0 * units
-        if dname in ("k_flux", "k_faceB"):
+        if dname == "k_faceB":
             per_launch /= 3.0  # one launch per face direction
         achieved = per_launch / (dms / dcount / 1e3) / 1e9
         roof = {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",

@@ -304,6 +304,8 @@ int upload_mesh(Solve& sv) {
   for (int q = 0; q < 3; ++q) { s.Bq[q] = A(NQ); s.fcon[q] = A(2 * NVAR); s.EF[q] = A(1); s.Ef[q] = A(1); s.B0[q] = A(1); }
   for (int q = 0; q < 6; ++q) s.S[q] = A(1);
   s.dUdt = A(NVAR); s.U0 = A(NVAR); s.ent0 = A(1);
+  s.FS = A(6 * NQ * (NVAR + 1));
+  if (!s.FS) return cuda_fail(sv, e, "cudaMalloc(face states)");
   set_adp_smem_limits();
   // ADP: the KKT matrix of every zone depends on the geometry only, so its
   // factors are computed once here and each stage only substitutes.  They

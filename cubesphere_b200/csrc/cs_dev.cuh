@@ -42,6 +42,7 @@ struct DState {
   double *msonic, *flatA, *flatB;        // flattener work
   double *Bq[3];                         // B at face quadrature points (5 each)
   double *fcon[3];                       // per-face flux contributions: [16][..] (L 8, R 8)
+  double *FS;                            // face states: [(side*5 + point)*9 + var][..], 270 comps
   double *S[6];                          // S_L,S_R (x), S_D,S_U (y), S_B,S_T (z) at j=1
   double *EF[3];                         // entropy fluxes
   double *Ef[3];                         // edge EMFs

@@ -24,6 +24,57 @@ __device__ __forceinline__ double Vm(const DState& s, const Dims& d, int comp, i
   return s.V[((long long)(mode * NVAR + comp) * NPANEL + p) * d.S + o];
 }
 
+// Face states: every active zone evaluates its reconstruction (8
+// primitives and the entropy) at the 5 quadrature points of each of its 6
+// faces, once per stage.  Side f: 0 +x (face i), 1 -x (face i-1), 2 +y,
+// 3 -y, 4 +z, 5 -z.  Layout FS[(f*5 + q)*9 + var][panel][box].
+constexpr int FS_TPB = 64;
+__global__ void __launch_bounds__(FS_TPB) k_face_states(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
+  __shared__ double xs[90][FS_TPB];
+  const int tid = threadIdx.x;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
+    int p, i, j, k;
+    r.decode(t, p, i, j, k);
+    if (mask_at(g, d, p, i, j) != 1) continue;
+    const long long o = d.idx(i, j, k);
+    const double obl0 = 1.0 / fmax(geo(g, d, CS_G_V_SCALE, 0, p, i, j, k), ph.smallnum);
+    const double cx = geo(g, d, CS_G_V_CEN, 0, p, i, j, k), cy = geo(g, d, CS_G_V_CEN, 1, p, i, j, k),
+                 cz = geo(g, d, CS_G_V_CEN, 2, p, i, j, k);
+#pragma unroll 1
+    for (int f = 0; f < 6; ++f) {
+      const int dir = f / 2;
+      const int QP = dir == 0 ? CS_G_XF_QP : (dir == 1 ? CS_G_YF_QP : CS_G_ZF_QP);
+      const int fx = (f == 1) ? i - 1 : i, fy = (f == 3) ? j - 1 : j, fz = (f == 5) ? k - 1 : k;
+#pragma unroll
+      for (int q = 0; q < 5; ++q) {
+        xs[(f * 5 + q) * 3 + 0][tid] = (geo(g, d, QP, q, p, fx, fy, fz) - cx) * obl0;
+        xs[(f * 5 + q) * 3 + 1][tid] = (geo(g, d, QP, 5 + q, p, fx, fy, fz) - cy) * obl0;
+        xs[(f * 5 + q) * 3 + 2][tid] = (geo(g, d, QP, 10 + q, p, fx, fy, fz) - cz) * obl0;
+      }
+    }
+    double c0[10];
+#pragma unroll
+    for (int m = 0; m < 10; ++m) c0[m] = geo(g, d, CS_G_COEF, m, p, i, j, k);
+#pragma unroll 1
+    for (int c = 0; c < 8; ++c) {
+      double v[10];
+#pragma unroll
+      for (int m = 0; m < 10; ++m) v[m] = Vm(s, d, c, m, p, o);
+#pragma unroll 5
+      for (int fq = 0; fq < 30; ++fq)
+        s.FS[((long long)(fq * 9 + c) * NPANEL + p) * d.S + o] =
+            d_poly10(v, c0, xs[fq * 3 + 0][tid], xs[fq * 3 + 1][tid], xs[fq * 3 + 2][tid]);
+    }
+    const double* E = s.ent;
+    const double e0 = E[((long long)0 * NPANEL + p) * d.S + o], e1 = E[((long long)1 * NPANEL + p) * d.S + o],
+                 e2 = E[((long long)2 * NPANEL + p) * d.S + o], e3 = E[((long long)3 * NPANEL + p) * d.S + o];
+#pragma unroll 5
+    for (int fq = 0; fq < 30; ++fq)
+      s.FS[((long long)(fq * 9 + 8) * NPANEL + p) * d.S + o] =
+          e0 + e1 * xs[fq * 3 + 0][tid] + e2 * xs[fq * 3 + 1][tid] + e3 * xs[fq * 3 + 2][tid];
+  }
+}
+
 // One face quadrature point per thread: the five warps of a block take the
 // five points of the same 32 faces, so the zone modes each warp loads are
 // shared through L1 and no thread holds more than one point's state.  The
@@ -131,42 +182,47 @@ __global__ void __launch_bounds__(FLUX_FACES * 5, 3) k_flux(Dims d, PhysC ph, DG
       }
       const double px = geo(g, d, QP, jq, p, i, j, k), py = geo(g, d, QP, 5 + jq, p, i, j, k),
                    pz = geo(g, d, QP, 10 + jq, p, i, j, k);
-      double x, y, z, x2, y2, z2;
-      {
-        const double obl0 = 1.0 / fmax(geo(g, d, CS_G_V_SCALE, 0, p, lx, ly, lz), ph.smallnum);
-        const double obl02 = 1.0 / fmax(geo(g, d, CS_G_V_SCALE, 0, p, rx, ry, rz), ph.smallnum);
-        x = (px - geo(g, d, CS_G_V_CEN, 0, p, lx, ly, lz)) * obl0;
-        y = (py - geo(g, d, CS_G_V_CEN, 1, p, lx, ly, lz)) * obl0;
-        z = (pz - geo(g, d, CS_G_V_CEN, 2, p, lx, ly, lz)) * obl0;
-        x2 = (px - geo(g, d, CS_G_V_CEN, 0, p, rx, ry, rz)) * obl02;
-        y2 = (py - geo(g, d, CS_G_V_CEN, 1, p, rx, ry, rz)) * obl02;
-        z2 = (pz - geo(g, d, CS_G_V_CEN, 2, p, rx, ry, rz)) * obl02;
-      }
-      double VL[8], VR[8];
-      {
-        double cL[10], cR[10];
+      // Face states of the two sides: precomputed unless the side was
+      // remapped through istencil (panel corners), which evaluates the
+      // remapped zone's reconstruction at this face's point here.
+      const bool remapL = lx != i || ly != j;
+      const bool remapR = dir == 0 ? (rx != i + 1 || ry != j) : (dir == 1 ? (rx != i || ry != j + 1) : false);
+      const int fL = 2 * dir, fR = 2 * dir + 1;
+      double VL[8], VR[8], entL, entR;
+      auto eval = [&](int zx, int zy, int zz, double* Vo, double& eo) {
+        const long long oz = d.idx(zx, zy, zz);
+        const double obl = 1.0 / fmax(geo(g, d, CS_G_V_SCALE, 0, p, zx, zy, zz), ph.smallnum);
+        const double x = (px - geo(g, d, CS_G_V_CEN, 0, p, zx, zy, zz)) * obl;
+        const double y = (py - geo(g, d, CS_G_V_CEN, 1, p, zx, zy, zz)) * obl;
+        const double z = (pz - geo(g, d, CS_G_V_CEN, 2, p, zx, zy, zz)) * obl;
+        double cc[10];
 #pragma unroll
-        for (int m = 0; m < 10; ++m) {
-          cL[m] = geo(g, d, CS_G_COEF, m, p, lx, ly, lz);
-          cR[m] = geo(g, d, CS_G_COEF, m, p, rx, ry, rz);
-        }
+        for (int m = 0; m < 10; ++m) cc[m] = geo(g, d, CS_G_COEF, m, p, zx, zy, zz);
 #pragma unroll
         for (int c = 0; c < 8; ++c) {
-          double vl[10], vr[10];
+          double vv[10];
 #pragma unroll
-          for (int m = 0; m < 10; ++m) {
-            vl[m] = Vm(s, d, c, m, p, oL);
-            vr[m] = Vm(s, d, c, m, p, oR);
-          }
-          VL[c] = d_poly10(vl, cL, x, y, z);
-          VR[c] = d_poly10(vr, cR, x2, y2, z2);
+          for (int m = 0; m < 10; ++m) vv[m] = Vm(s, d, c, m, p, oz);
+          Vo[c] = d_poly10(vv, cc, x, y, z);
         }
+        const double* E = s.ent;
+        eo = E[((long long)0 * NPANEL + p) * d.S + oz] + E[((long long)1 * NPANEL + p) * d.S + oz] * x +
+             E[((long long)2 * NPANEL + p) * d.S + oz] * y + E[((long long)3 * NPANEL + p) * d.S + oz] * z;
+      };
+      if (remapL) {
+        eval(lx, ly, lz, VL, entL);
+      } else {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) VL[c] = s.FS[((long long)((fL * 5 + jq) * 9 + c) * NPANEL + p) * d.S + oL];
+        entL = s.FS[((long long)((fL * 5 + jq) * 9 + 8) * NPANEL + p) * d.S + oL];
       }
-      const double* E = s.ent;
-      const double entL = E[((long long)0 * NPANEL + p) * d.S + oL] + E[((long long)1 * NPANEL + p) * d.S + oL] * x +
-                          E[((long long)2 * NPANEL + p) * d.S + oL] * y + E[((long long)3 * NPANEL + p) * d.S + oL] * z;
-      const double entR = E[((long long)0 * NPANEL + p) * d.S + oR] + E[((long long)1 * NPANEL + p) * d.S + oR] * x2 +
-                          E[((long long)2 * NPANEL + p) * d.S + oR] * y2 + E[((long long)3 * NPANEL + p) * d.S + oR] * z2;
+      if (remapR) {
+        eval(rx, ry, rz, VR, entR);
+      } else {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) VR[c] = s.FS[((long long)((fR * 5 + jq) * 9 + c) * NPANEL + p) * d.S + oR];
+        entR = s.FS[((long long)((fR * 5 + jq) * 9 + 8) * NPANEL + p) * d.S + oR];
+      }
 #pragma unroll
       for (int o = 1; o <= 5; o += 4) {
         double a1 = Ax * VL[o] + Ay * VL[o + 1] + Az * VL[o + 2];
@@ -278,6 +334,9 @@ void launch_fluxes(Solve& sv) {
   Range3 fx = {-1, N + 1, 0, N + 1, 0, nr + 1};
   Range3 fy = {0, N + 1, -1, N + 1, 0, nr + 1};
   Range3 fz = {0, N + 1, 0, N + 1, -1, nr + 1};
+  Range3 zs = {-1, N + 2, -1, N + 2, -1, nr + 2};
+  k_face_states<<<blocks_for(zs.count(), FS_TPB, sv.sm_count), FS_TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, zs);
+  mark(sv, "k_face_states");
   const Range3 fr[3] = {fx, fy, fz};
   for (int dir = 0; dir < 3; ++dir) {
     const long long nt = (fr[dir].count() + FLUX_FACES - 1) / FLUX_FACES;
