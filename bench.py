@@ -42,10 +42,12 @@ ALGO_WORDS_PER_UNIT = {
     # 8 comps x 10 modes in/out of V, flattener, 18-zone centroids (re-reads
     # excluded), coefficients 10
     "k_weno7b": 80 + 1 + 4 + 10 + 72,
-    # resident KKT factors (1296) + pivots (36 bytes), face-B quadrature
-    # values (30), B modes in and out (60), U(5:8) in and out (8), geometry
-    # of the 6 faces (normals 42, points 90, weights 30) and of the zone (14)
-    "k_adp_solve": 1296 + 4.5 + 30 + 60 + 8 + 162 + 14,
+    # resident KKT factors (1296) + pivots (36 bytes) + the 36 right-hand
+    # sides in, 30 B modes and U(5:8) out (U read and written: 8)
+    "k_adp_solve": 1296 + 4.5 + 36 + 30 + 8,
+    # face-B quadrature values (30), B modes (30), geometry of the 6 faces
+    # (normals 42, points 90, weights 30) and of the zone (14), 36 out
+    "k_adp_rhs": 30 + 30 + 162 + 14 + 36,
     # 80 modes + 4 entropy modes + 10 moments + scale/centroid in, 30 face
     # points x 3 coordinates of geometry, 270 face-state values out
     "k_face_states": 80 + 4 + 14 + 90 + 270,

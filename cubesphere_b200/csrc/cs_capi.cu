@@ -313,6 +313,7 @@ int upload_mesh(Solve& sv) {
   // CS_FLAG_NO_ADP_CACHE) every stage assembles and factors in place.
   s.adp_lu = nullptr;
   s.adp_piv = nullptr;
+  s.adp_rhs = nullptr;
   s.op_m9 = nullptr;
   s.op_m10 = nullptr;
   // The inverse normal matrices of the STEP 7.b / 9.c least squares are
@@ -328,16 +329,19 @@ int upload_mesh(Solve& sv) {
     }
   }
   if (!(sv.p.flags & CS_FLAG_NO_ADP_CACHE)) {
-    const long long na = adp_range_count(d);
-    const size_t lu_bytes = (size_t)na * 36 * 36 * sizeof(double), pv_bytes = (size_t)na * 36;
+    const long long nf = adp_factor_doubles(d);
+    const size_t lu_bytes = (size_t)nf * sizeof(double), pv_bytes = (size_t)nf / 36;
     size_t fr = 0, tot = 0;
     if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && lu_bytes + pv_bytes + (size_t)8 * S6 * 60 < fr) {
       s.adp_lu = (double*)dalloc(sv, lu_bytes, e);
       s.adp_piv = s.adp_lu ? (int8_t*)dalloc(sv, pv_bytes, e) : nullptr;
-      if (!s.adp_lu || !s.adp_piv) return cuda_fail(sv, e, "cudaMalloc(ADP factors)");
+      s.adp_rhs = s.adp_piv ? (double*)dalloc(sv, (size_t)adp_range_count(d) * 36 * sizeof(double), e) : nullptr;
+      if (!s.adp_lu || !s.adp_piv || !s.adp_rhs) return cuda_fail(sv, e, "cudaMalloc(ADP factors)");
     }
   }
   s.giveup = (int32_t*)dalloc(sv, S6 * sizeof(int32_t), e);
+  s.err_flag = (int*)dalloc(sv, 64, e);
+  if (!s.err_flag) return cuda_fail(sv, e, "cudaMalloc(error flag)");
   s.dtmin = (unsigned long long*)dalloc(sv, 64, e);
   if (e != cudaSuccess || !s.U || !s.V || !s.E || !s.dtmin) return cuda_fail(sv, e, "cudaMalloc(state)");
   for (int q = 0; q < 3; ++q)
@@ -419,8 +423,11 @@ int run_stage(Solve& sv, int irk, double dtcur) {
 
 int read_dt(Solve& sv, double* out) {
   unsigned long long bits = 0;
+  int flag = 0;
   CS_CUDA(sv, cudaMemcpyAsync(&bits, sv.st.dtmin, sizeof(bits), cudaMemcpyDeviceToHost, sv.stream));
+  CS_CUDA(sv, cudaMemcpyAsync(&flag, sv.st.err_flag, sizeof(flag), cudaMemcpyDeviceToHost, sv.stream));
   CS_CUDA(sv, cudaStreamSynchronize(sv.stream));
+  if (flag) return fail(sv, CS_ERR_CUDA, "a bounded device wait gave up (bulk copy did not complete)");
   if (sv.prof.on) prof_harvest(sv);
   std::memcpy(out, &bits, sizeof(bits));
   return CS_OK;

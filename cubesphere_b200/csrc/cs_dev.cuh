@@ -50,8 +50,10 @@ struct DState {
   double *U0, *ent0, *B0[3];             // saved stage-1 state
   double* op_m9;                         // STEP 7.b inverse normal matrices, [81][zones of shrink(2)], or null
   double* op_m10;                        // STEP 9.c inverse normal matrices, [100][zones of shrink(2)], or null
-  double* adp_lu;                        // ADP KKT factors, [36*36][zones of the ADP range], or null
-  int8_t* adp_piv;                       // their row permutation, [36][zones]
+  double* adp_lu;                        // ADP KKT factors: per block of 128 zones, [1296 in use order][128], or null
+  int8_t* adp_piv;                       // their row permutation, per block [36][128]
+  double* adp_rhs;                       // ADP right-hand sides, [36][zones of the ADP range]
+  int* err_flag;                         // device-side error bits (bounded waits that gave up)
   int32_t* giveup;                       // positivity give-up flags per zone
   unsigned long long* dtmin;             // CFL reduction target (bit pattern of a positive double)
 };
@@ -396,6 +398,7 @@ void launch_faceB_adp(Solve& s);
 void launch_adp_factor(Solve& s);
 void set_adp_smem_limits();
 long long adp_range_count(const Dims& d);
+long long adp_factor_doubles(const Dims& d);
 long long lsq_range_count(const Dims& d);
 void launch_ops_build(Solve& s);
 void launch_efield(Solve& s);

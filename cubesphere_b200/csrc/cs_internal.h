@@ -7,7 +7,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/cubesphere_b200.h"
+#include "cubesphere_b200.h"
 
 namespace cs {
 

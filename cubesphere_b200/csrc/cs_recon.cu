@@ -9,6 +9,8 @@
 // each kernel names the reference step it implements.  One thread per zone
 // or face; the ADP solve uses one warp per zone with the 36x36 KKT system
 // in shared memory.
+#include <algorithm>
+
 #include "cs_solve.h"
 
 namespace cs {
@@ -674,6 +676,14 @@ __global__ void __launch_bounds__(TPB) k_faceB(Dims d, PhysC ph, DGeom g, DState
 // the 36x36 KKT system by one warp with Gaussian elimination (scaled
 // partial pivoting) in shared memory.
 constexpr int ADP_WARPS = 4;
+// Resident ADP factors are stored as one stream per block of ADP_ZB zones
+// (zone fastest), in the order the substitution consumes them: the strict
+// lower triangle row by row (630), then for rows 35..0 the entries right of
+// the diagonal followed by the diagonal (666).
+constexpr int ADP_ZB = 128;
+__host__ __device__ constexpr int adp_stream_pos(int a, int b) {
+  return b < a ? a * (a - 1) / 2 + b : 630 + (35 - a) * (36 - a) / 2 + (b == a ? 35 - a : b - a - 1);
+}
 struct AdpSmem {
   double K[36][37];
   double Q[30][31];
@@ -831,9 +841,10 @@ __global__ void __launch_bounds__(32 * ADP_WARPS) k_adp(Dims d, PhysC ph, DGeom 
       __syncwarp();
     }
     if (kFactorOnly) {
-      const long long n = r.count();
-      for (int e = lane; e < 36 * 36; e += 32) s.adp_lu[(long long)e * n + t] = S.K[e / 36][e % 36];
-      for (int e = lane; e < 36; e += 32) s.adp_piv[(long long)e * n + t] = (int8_t)S.piv[e];
+      const long long blk = t / ADP_ZB, z = t % ADP_ZB;
+      for (int e = lane; e < 36 * 36; e += 32)
+        s.adp_lu[(blk * 1296 + adp_stream_pos(e / 36, e % 36)) * ADP_ZB + z] = S.K[e / 36][e % 36];
+      for (int e = lane; e < 36; e += 32) s.adp_piv[(blk * 36 + e) * ADP_ZB + z] = (int8_t)S.piv[e];
       __syncwarp();
       continue;
     }
@@ -870,19 +881,55 @@ __global__ void __launch_bounds__(32 * ADP_WARPS) k_adp(Dims d, PhysC ph, DGeom 
   }
 }
 
-// STEP 8.d with the stored factors: one thread per zone builds the
-// right-hand side (the same sums in the same order as k_adp) and runs the
-// forward and back substitution against the factors of its zone, which are
-// stored element-major so that a warp reads them coalesced.
-constexpr int ADPS_TPB = 128;
-__global__ void __launch_bounds__(ADPS_TPB, 4) k_adp_solve(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
-  __shared__ double rhs_s[36][ADPS_TPB];
+// ---- bulk asynchronous copies (cp.async.bulk) and mbarriers ----
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred P;\n mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n selp.u32 %0, 1, 0, P;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+// Bounded wait on an mbarrier phase: after 2^23 polls (seconds, far beyond
+// any copy) it records an error in *err and returns, so no wait can hang.
+__device__ __noinline__ void mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
+  for (int it = 0; it < (1 << 23); ++it)
+    if (mbar_try_wait(bar, parity)) return;
+  atomicOr(err, 1);
+}
+
+// STEP 8.d right-hand side with the resident factors: one thread per zone
+// forms the 36 entries (the same sums in the same order as k_adp) and
+// stores them element-major, [36][zones of the ADP range].
+constexpr int ADPR_TPB = 128;
+__global__ void __launch_bounds__(ADPR_TPB) k_adp_rhs(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
   const long long n = r.count();
-  const int tid = threadIdx.x;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
     r.decode(t, p, i, j, k);
-    if (mask_at(g, d, p, i, j) == 0) continue;
+    double* out = s.adp_rhs + t;
+    if (mask_at(g, d, p, i, j) != 1) {
+#pragma unroll
+      for (int a = 0; a < 36; ++a) out[(long long)a * n] = 0.0;
+      continue;
+    }
     const double obl0 = 1.0 / fmax(geo(g, d, CS_G_V_SCALE, 0, p, i, j, k), ph.smallnum);
     const double vc0 = geo(g, d, CS_G_V_CEN, 0, p, i, j, k), vc1 = geo(g, d, CS_G_V_CEN, 1, p, i, j, k),
                  vc2 = geo(g, d, CS_G_V_CEN, 2, p, i, j, k);
@@ -891,7 +938,6 @@ __global__ void __launch_bounds__(ADPS_TPB, 4) k_adp_solve(Dims d, PhysC ph, DGe
     double rhs[30];
 #pragma unroll
     for (int a = 0; a < 30; ++a) rhs[a] = 0.0;
-    double D[6];
 #pragma unroll 1
     for (int f = 0; f < 6; ++f) {
       const int dir = f / 2;
@@ -920,42 +966,131 @@ __global__ void __launch_bounds__(ADPS_TPB, 4) k_adp_solve(Dims d, PhysC ph, DGe
         }
         dacc = dacc + geo(g, d, BW, q, p, fx, fy, fz) * bq;
       }
-      D[f] = dacc;
+      out[(long long)(30 + f) * n] = dacc;
     }
 #pragma unroll
-    for (int a = 0; a < 30; ++a) rhs_s[a][tid] = rhs[a] + Vat(s, d, 5 + a / 10, a % 10, p, i, j, k);
-#pragma unroll
-    for (int f = 0; f < 6; ++f) rhs_s[30 + f][tid] = D[f];
-    const double* L = s.adp_lu + t;
-    const int8_t* pv = s.adp_piv + t;
-    double y[36];
-#pragma unroll
-    for (int a = 0; a < 36; ++a) {
-      double acc = rhs_s[pv[(long long)a * n]][tid];
-#pragma unroll
-      for (int b = 0; b < a; ++b) acc -= __ldcs(L + (long long)(a * 36 + b) * n) * y[b];
-      y[a] = acc;
-    }
-#pragma unroll
-    for (int a = 35; a >= 0; --a) {
-      double acc = y[a];
-#pragma unroll
-      for (int b = a + 1; b < 36; ++b) acc -= __ldcs(L + (long long)(a * 36 + b) * n) * y[b];
-      y[a] = acc / __ldcs(L + (long long)(a * 36 + a) * n);
-    }
-#pragma unroll
-    for (int a = 0; a < 30; ++a) Vat(s, d, 5 + a / 10, a % 10, p, i, j, k) = y[a];
-    double* U = s.U;
-    const long long o5 = d.at(4, p, i, j, k);
-    const double u6 = U[d.at(5, p, i, j, k)], u7 = U[d.at(6, p, i, j, k)], u8 = U[d.at(7, p, i, j, k)];
-    const double aa = (u6 * u6 + u7 * u7 + u8 * u8) * ph.ob8pi;
-    const double n6 = y[0], n7 = y[10], n8 = y[20];
-    U[d.at(5, p, i, j, k)] = n6;
-    U[d.at(6, p, i, j, k)] = n7;
-    U[d.at(7, p, i, j, k)] = n8;
-    const double bb = (n6 * n6 + n7 * n7 + n8 * n8) * ph.ob8pi;
-    U[o5] = U[o5] - aa + bb;
+    for (int a = 0; a < 30; ++a) out[(long long)a * n] = rhs[a] + Vat(s, d, 5 + a / 10, a % 10, p, i, j, k);
   }
+}
+
+// STEP 8.d substitution with the resident factors, one thread per zone.
+// The factor stream of the block's 128 zones (1296 x 1 KB, in consumption
+// order) flows through a ring of ADPS_NS shared-memory stages of ADPS_CH
+// elements (16 KB), filled by bulk asynchronous copies that a producer warp
+// issues as soon as the four consumer warps have released a stage
+// (full / empty mbarrier pairs).  The solution vector lives in shared
+// memory so that the loops stay short; the arithmetic (order included) is
+// that of the reference's forward and back substitution.
+constexpr int ADPS_TPB = ADP_ZB;             // consumer threads (one per zone)
+constexpr int ADPS_THREADS = ADPS_TPB + 32;  // + one producer warp
+constexpr int ADPS_CH = 16;
+constexpr int ADPS_NS = 4;
+constexpr int ADPS_NCH = 1296 / ADPS_CH;
+static_assert(1296 % ADPS_CH == 0, "whole chunks");
+struct AdpsSmem {
+  double stage[ADPS_NS][ADPS_CH][ADPS_TPB];
+  double y[36][ADPS_TPB];
+  uint64_t full[ADPS_NS];
+  uint64_t empty[ADPS_NS];
+};
+
+__global__ void __launch_bounds__(ADPS_THREADS, 2) k_adp_solve(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
+  extern __shared__ __align__(128) unsigned char adps_raw[];
+  AdpsSmem& S = *reinterpret_cast<AdpsSmem*>(adps_raw);
+  const int tid = threadIdx.x;
+  const long long n = r.count();
+  const long long nblk = (n + ADP_ZB - 1) / ADP_ZB;
+  if ((long long)blockIdx.x >= nblk) return;
+  const long long my_iters = (nblk - 1 - blockIdx.x) / gridDim.x + 1;
+  const long long total_chunks = my_iters * ADPS_NCH;
+  if (tid == 0) {
+    for (int q = 0; q < ADPS_NS; ++q) {
+      mbar_init(&S.full[q], 1);
+      mbar_init(&S.empty[q], ADPS_TPB / 32);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (tid >= ADPS_TPB) {
+    // producer: chunk gch of this CTA is chunk gch % NCH of zone block
+    // blockIdx.x + (gch / NCH) * gridDim.x
+    if (tid == ADPS_TPB) {
+      for (long long gch = 0; gch < total_chunks; ++gch) {
+        const int slot = (int)(gch % ADPS_NS);
+        if (gch >= ADPS_NS) mbar_wait(&S.empty[slot], (uint32_t)(((gch / ADPS_NS) - 1) & 1), s.err_flag);
+        const long long it = gch / ADPS_NCH, c = gch % ADPS_NCH;
+        const long long blk = blockIdx.x + it * gridDim.x;
+        const double* src = s.adp_lu + (blk * 1296 + c * ADPS_CH) * (long long)ADP_ZB;
+        mbar_expect_tx(&S.full[slot], ADPS_CH * ADP_ZB * sizeof(double));
+        bulk_g2s(&S.stage[slot][0][0], src, ADPS_CH * ADP_ZB * sizeof(double), &S.full[slot]);
+      }
+    }
+    return;
+  }
+  const int lane = tid & 31;
+  long long gch = 0;  // next chunk to consume
+  int within = ADPS_CH;
+  const double* cur = nullptr;
+  // next factor element of this thread's zone
+  auto next = [&]() -> double {
+    if (within == ADPS_CH) {
+      if (gch > 0) {
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&S.empty[(int)((gch - 1) % ADPS_NS)]);
+      }
+      const int slot = (int)(gch % ADPS_NS);
+      mbar_wait(&S.full[slot], (uint32_t)((gch / ADPS_NS) & 1), s.err_flag);
+      cur = &S.stage[slot][0][tid];
+      ++gch;
+      within = 0;
+    }
+    return cur[(within++) * ADPS_TPB];
+  };
+  for (long long it = 0; it < my_iters; ++it) {
+    const long long blk = blockIdx.x + it * gridDim.x;
+    const long long t = blk * ADP_ZB + tid;
+    const bool inr = t < n;
+    const int8_t* pv = s.adp_piv + blk * 36 * ADP_ZB + tid;
+    // permuted right-hand side first (36 independent loads), then the
+    // substitution in place
+#pragma unroll
+    for (int a = 0; a < 36; ++a) S.y[a][tid] = inr ? s.adp_rhs[(long long)pv[a * ADP_ZB] * n + t] : 0.0;
+#pragma unroll 1
+    for (int a = 1; a < 36; ++a) {
+      double acc = S.y[a][tid];
+#pragma unroll 4
+      for (int b = 0; b < a; ++b) acc -= next() * S.y[b][tid];
+      S.y[a][tid] = acc;
+    }
+#pragma unroll 1
+    for (int a = 35; a >= 0; --a) {
+      double acc = S.y[a][tid];
+#pragma unroll 4
+      for (int b = a + 1; b < 36; ++b) acc -= next() * S.y[b][tid];
+      S.y[a][tid] = acc / next();
+    }
+    if (inr) {
+      int p, i, j, k;
+      r.decode(t, p, i, j, k);
+      if (mask_at(g, d, p, i, j) == 1) {
+#pragma unroll
+        for (int a = 0; a < 30; ++a) Vat(s, d, 5 + a / 10, a % 10, p, i, j, k) = S.y[a][tid];
+        double* U = s.U;
+        const long long o5 = d.at(4, p, i, j, k);
+        const double u6 = U[d.at(5, p, i, j, k)], u7 = U[d.at(6, p, i, j, k)], u8 = U[d.at(7, p, i, j, k)];
+        const double aa = (u6 * u6 + u7 * u7 + u8 * u8) * ph.ob8pi;
+        const double n6 = S.y[0][tid], n7 = S.y[10][tid], n8 = S.y[20][tid];
+        U[d.at(5, p, i, j, k)] = n6;
+        U[d.at(6, p, i, j, k)] = n7;
+        U[d.at(7, p, i, j, k)] = n8;
+        const double bb = (n6 * n6 + n7 * n7 + n8 * n8) * ph.ob8pi;
+        U[o5] = U[o5] - aa + bb;
+      }
+    }
+  }
+  // release the last chunk (no producer waits for it; keeps the protocol uniform)
+  __syncwarp();
+  if (lane == 0 && gch > 0) mbar_arrive(&S.empty[(int)((gch - 1) % ADPS_NS)]);
 }
 
 // STEP 9.a (421:6700-6790): zone-centred E = -v x B from the point values.
@@ -1224,7 +1359,11 @@ void launch_faceB_adp(Solve& sv) {
   mark(sv, "k_faceB");
   Range3 a = shrink(d, 1);
   if (sv.st.adp_lu) {
-    k_adp_solve<<<blocks_for(a.count(), ADPS_TPB, sv.sm_count), ADPS_TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, a);
+    k_adp_rhs<<<blocks_for(a.count(), ADPR_TPB, sv.sm_count), ADPR_TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, a);
+    mark(sv, "k_adp_rhs");
+    const long long nblk = (a.count() + ADP_ZB - 1) / ADP_ZB;
+    const int grid = (int)std::min<long long>(nblk, (long long)sv.sm_count * 2);
+    k_adp_solve<<<grid, ADPS_THREADS, sizeof(AdpsSmem), sv.stream>>>(d, sv.ph, sv.g, sv.st, a);
     mark(sv, "k_adp_solve");
     return;
   }
@@ -1253,7 +1392,12 @@ void launch_ops_build(Solve& sv) {
   }
 }
 
+long long adp_factor_doubles(const Dims& d) {
+  return (shrink(d, 1).count() + ADP_ZB - 1) / ADP_ZB * (long long)ADP_ZB * 1296;
+}
+
 void set_adp_smem_limits() {
+  cudaFuncSetAttribute(k_adp_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(AdpsSmem));
   const int smem = (int)(sizeof(AdpSmem) * ADP_WARPS);
   cudaFuncSetAttribute(k_adp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   cudaFuncSetAttribute(k_adp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
