@@ -47,6 +47,7 @@ EXPORTS = [
     "cs_limit_all_slopes_p12", "cs_make_facial_fluxes", "cs_make_edge_efields_p1",
     "cs_build_non_stiff_sources", "cs_update_imex_rk_step_p1", "cs_cleanup_after_update",
     "cs_debug_get", "cs_diag", "cs_get_stream", "cs_launch_count", "cs_profile_begin", "cs_profile_end",
+    "cs_cfl_timestep_noalloc",
 ]
 
 
@@ -142,6 +143,7 @@ def load_library() -> ctypes.CDLL:
         "cs_launch_count": ([P, ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
         "cs_profile_begin": ([P], ctypes.c_int),
         "cs_profile_end": ([P, I, ctypes.c_char_p, dp, ctypes.POINTER(ctypes.c_int64), ip], ctypes.c_int),
+        "cs_cfl_timestep_noalloc": ([P, P, P, P, I, I, I, D, D, D, D, D, P, dp], ctypes.c_int),
     }
     for name in ("cs_fill_ghosts", "cs_limit_all_slopes_p12", "cs_make_facial_fluxes", "cs_make_edge_efields_p1",
                  "cs_build_non_stiff_sources", "cs_cleanup_after_update"):

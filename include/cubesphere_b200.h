@@ -204,6 +204,25 @@ int cs_profile_begin(cs_ctx* ctx);
 int cs_profile_end(cs_ctx* ctx, int32_t max_kernels, char* names, double* total_ms,
                    int64_t* launches, int32_t* n_kernels);
 
+/* CFL time step over caller-owned device arrays, with no device allocation.
+ * No counterpart in the reference: it is the EVALUATE_TIMESTEP reduction
+ * (490evaluate_timestep.f:121-286, the same result as cs_evaluate_timestep)
+ * for callers that cannot let a library allocate device memory, e.g. a host
+ * code whose memory pool owns the whole device or whose step loop must not
+ * call cudaMalloc.  U (8 components), ent, v_scale and mask are panel boxes
+ * of the layout above in device memory; nothing is written to them.  The
+ * reduction scratch is a fixed static device array (6 x 2048 layer partials,
+ * 96 KB), so nr > 2048 is rejected with CS_ERR_ARG; no slot needs clearing
+ * (each is written before it is read).  The first call on a device looks the
+ * scratch up with cudaGetSymbolAddress and must not happen inside a stream
+ * capture.  All calls on a device share the scratch: calls that overlap in
+ * time (other threads or streams) race, so serialize them.  Runs on stream
+ * (cudaStream_t, may be null) and synchronizes it to return *dtcurp1. */
+int cs_cfl_timestep_noalloc(const double* U, const double* ent, const double* v_scale,
+                            const int32_t* mask, int32_t ntp, int32_t nr, int32_t nghost,
+                            double gamma, double rhofloor, double prsfloor, double cfl_coef,
+                            double dtcur, void* stream, double* dtcurp1);
+
 /* Diagnostics: sums over interior zones of 6 panels of volume-weighted
  * mass, energy and the max |div B| (face-area-weighted, per volume). */
 int cs_diag(cs_ctx* ctx, double* mass, double* energy, double* max_divb);
