@@ -79,6 +79,7 @@ DEFAULT_PARAMS = dict(
 )
 CS_FLAG_NO_ADP_CACHE = 1
 CS_FLAG_NO_OP_CACHE = 2
+CS_FLAG_NO_PANEL_SYNC = 4
 
 
 def make_params(**kw) -> CsParams:

@@ -3,6 +3,8 @@
 // transfer, the stage / step sequence and the per-routine entry points.
 #include <algorithm>
 #include <cmath>
+#include <map>
+#include <tuple>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -223,6 +225,119 @@ void prof_harvest(Solve& sv) {
   pf.n = 0;
 }
 
+// Panel-edge ownership maps.  Faces on panel edges and edges on panel
+// boundaries are computed by every panel that holds them (two, or three
+// for the radial edges at cube corners); the copies of all panels but the
+// lowest-numbered one take that owner's value.  Vertex identity follows the
+// ghost-fill index maps: right edge (N, j) ~ right neighbour (j, N), left
+// (0, j) ~ (0, N - j), down (i, 0) ~ (N - i, 0), up (i, N) ~ (N, i).
+struct SyncMaps {
+  std::vector<int32_t> f_dst, f_src;  // face offsets (panel * box + idx)
+  std::vector<int8_t> f_ddir, f_sdir;
+  std::vector<int32_t> e_dst, e_src;  // edge offsets
+  std::vector<int8_t> e_df, e_sf, e_sign;
+};
+
+std::string build_sync_maps(const Solve& sv, SyncMaps& m) {
+  const GeomHost& g = sv.host;
+  const Box& b = g.box;
+  const int N = b.N, nr = b.nr;
+  const long long S = (long long)b.size();
+  const int W = N + 1;
+  std::vector<int> par((size_t)6 * W * W);
+  for (size_t t = 0; t < par.size(); ++t) par[t] = (int)t;
+  auto vid = [&](int p, int i, int j) { return (p * W + j) * W + i; };
+  auto root = [&](int x) {
+    while (par[x] != x) x = par[x] = par[par[x]];
+    return x;
+  };
+  auto unite = [&](int a, int c) {
+    a = root(a);
+    c = root(c);
+    if (a != c) par[std::max(a, c)] = std::min(a, c);
+  };
+  for (int p = 0; p < 6; ++p) {
+    const int rt = kNbr[p][0] - 1, lf = kNbr[p][1] - 1, up = kNbr[p][2] - 1, dn = kNbr[p][3] - 1;
+    for (int t = 0; t <= N; ++t) {
+      unite(vid(p, N, t), vid(rt, t, N));
+      unite(vid(p, 0, t), vid(lf, 0, N - t));
+      unite(vid(p, t, 0), vid(dn, N - t, 0));
+      unite(vid(p, t, N), vid(up, N, t));
+    }
+  }
+  auto vert = [&](int q, int p, int i, int j) { return g.f[CS_G_VERT][((size_t)q * 6 + p) * S + b.idx(i, j, 0)]; };
+  for (int p = 0; p < 6; ++p)
+    for (int j = 0; j <= N; ++j)
+      for (int i = 0; i <= N; ++i) {
+        const int r = root(vid(p, i, j));
+        const int rp = r / (W * W), ri = r % W, rj = (r / W) % W;
+        double dist = 0.0, mag = 0.0;
+        for (int q = 0; q < 3; ++q) {
+          dist = std::max(dist, std::fabs(vert(q, p, i, j) - vert(q, rp, ri, rj)));
+          mag = std::max(mag, std::fabs(vert(q, p, i, j)));
+        }
+        if (dist > 1e-9 * mag) return "panel-edge vertex identities do not match the mesh";
+      }
+  auto off = [&](int p, int i, int j, int k) { return (int32_t)((long long)p * S + (long long)b.idx(i, j, k)); };
+  for (int p = 0; p < 6; ++p) {
+    const int rt = kNbr[p][0] - 1, lf = kNbr[p][1] - 1, up = kNbr[p][2] - 1, dn = kNbr[p][3] - 1;
+    for (int t = 1; t <= N; ++t)
+      for (int k = 1; k <= nr; ++k) {
+        // (dir, panel, i, j) of this copy, then of the partner copy
+        const int c[4][8] = {{0, p, N, t, 1, rt, t, N},
+                             {0, p, 0, t, 0, lf, 0, N + 1 - t},
+                             {1, p, t, 0, 1, dn, N + 1 - t, 0},
+                             {1, p, t, N, 0, up, N, t}};
+        for (const auto& e : c) {
+          if (e[5] >= e[1]) continue;  // this copy is the owner's
+          m.f_ddir.push_back((int8_t)e[0]);
+          m.f_dst.push_back(off(e[1], e[2], e[3], k));
+          m.f_sdir.push_back((int8_t)e[4]);
+          m.f_src.push_back(off(e[5], e[6], e[7], k));
+        }
+      }
+  }
+  struct Copy {
+    int f, p, i, j, k, a, c;
+  };
+  std::map<std::tuple<int, int, int>, std::vector<Copy>> cls;
+  for (int p = 0; p < 6; ++p) {
+    for (int j = 0; j <= N; ++j)
+      for (int i = 0; i <= N; ++i) {
+        if (!(i == 0 || i == N || j == 0 || j == N)) continue;
+        const int r = root(vid(p, i, j));
+        for (int k = 1; k <= nr; ++k) cls[std::make_tuple(r, -1, k)].push_back({2, p, i, j, k, r, r});
+      }
+    for (int k = 0; k <= nr; ++k) {
+      for (int i : {0, N})
+        for (int j = 1; j <= N; ++j) {
+          const int a = root(vid(p, i, j - 1)), c2 = root(vid(p, i, j));
+          cls[std::make_tuple(std::min(a, c2), std::max(a, c2), k)].push_back({1, p, i, j, k, a, c2});
+        }
+      for (int j : {0, N})
+        for (int i = 1; i <= N; ++i) {
+          const int a = root(vid(p, i - 1, j)), c2 = root(vid(p, i, j));
+          cls[std::make_tuple(std::min(a, c2), std::max(a, c2), k)].push_back({0, p, i, j, k, a, c2});
+        }
+    }
+  }
+  for (auto& kv : cls) {
+    auto& v = kv.second;
+    if (v.size() < 2) return "a panel-boundary edge belongs to one panel only";
+    std::sort(v.begin(), v.end(), [](const Copy& x, const Copy& y) { return x.p < y.p; });
+    const Copy& o = v[0];
+    for (size_t q = 1; q < v.size(); ++q) {
+      const Copy& x = v[q];
+      m.e_df.push_back((int8_t)x.f);
+      m.e_dst.push_back(off(x.p, x.i, x.j, x.k));
+      m.e_sf.push_back((int8_t)o.f);
+      m.e_src.push_back(off(o.p, o.i, o.j, o.k));
+      m.e_sign.push_back((int8_t)((x.a == o.a && x.c == o.c) ? 1 : -1));
+    }
+  }
+  return "";
+}
+
 bool check_params(const cs_params& p, std::string& why) {
   if (p.ntp < 2 || p.nr < 1) { why = "ntp must be >= 2 and nr >= 1"; return false; }
   if (p.nghost < 3 || p.nghost > p.ntp - 1) { why = "nghost must be in [3, ntp-1]"; return false; }
@@ -368,6 +483,35 @@ int upload_mesh(Solve& sv) {
   CS_CUDA(sv, cudaMemcpyAsync(f.d_src, hs.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, sv.stream));
   CS_CUDA(sv, cudaMemcpyAsync(f.d_dst, hd.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, sv.stream));
   CS_CUDA(sv, cudaMemcpyAsync(f.d_meta, hm.data(), n, cudaMemcpyHostToDevice, sv.stream));
+  // panel-edge ownership maps
+  if (!(sv.p.flags & CS_FLAG_NO_PANEL_SYNC)) {
+    SyncMaps sm;
+    why = build_sync_maps(sv, sm);
+    if (!why.empty()) return fail(sv, CS_ERR_ARG, why);
+    PanelSync& ps = sv.psync;
+    ps.nf = (long long)sm.f_dst.size();
+    ps.ne = (long long)sm.e_dst.size();
+    auto up32 = [&](const std::vector<int32_t>& v, int32_t*& dptr) -> cudaError_t {
+      dptr = (int32_t*)dalloc(sv, v.size() * sizeof(int32_t) + 16, e);
+      if (!dptr) return e;
+      return cudaMemcpyAsync(dptr, v.data(), v.size() * sizeof(int32_t), cudaMemcpyHostToDevice, sv.stream);
+    };
+    auto up8 = [&](const std::vector<int8_t>& v, int8_t*& dptr) -> cudaError_t {
+      dptr = (int8_t*)dalloc(sv, v.size() + 16, e);
+      if (!dptr) return e;
+      return cudaMemcpyAsync(dptr, v.data(), v.size(), cudaMemcpyHostToDevice, sv.stream);
+    };
+    CS_CUDA(sv, up32(sm.f_dst, ps.f_dst));
+    CS_CUDA(sv, up32(sm.f_src, ps.f_src));
+    CS_CUDA(sv, up8(sm.f_ddir, ps.f_ddir));
+    CS_CUDA(sv, up8(sm.f_sdir, ps.f_sdir));
+    CS_CUDA(sv, up32(sm.e_dst, ps.e_dst));
+    CS_CUDA(sv, up32(sm.e_src, ps.e_src));
+    CS_CUDA(sv, up8(sm.e_df, ps.e_df));
+    CS_CUDA(sv, up8(sm.e_sf, ps.e_sf));
+    CS_CUDA(sv, up8(sm.e_sign, ps.e_sign));
+    CS_CUDA(sv, cudaStreamSynchronize(sv.stream));
+  }
   launch_ops_build(sv);
   if (s.adp_lu) launch_adp_factor(sv);
   CS_CUDA(sv, cudaGetLastError());

@@ -221,6 +221,14 @@ __global__ void k_edges_z(Dims d, DGeom g, DState s, Range3 r) {
   }
 }
 
+// Panel-edge ownership for the EMFs: a non-owner copy of a shared edge
+// takes the owner's value, negated where the two panels run the edge in
+// opposite directions.
+__global__ void k_sync_emf(DState s, PanelSync ps) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < ps.ne; t += (long long)gridDim.x * blockDim.x)
+    s.Ef[ps.e_df[t]][ps.e_dst[t]] = (double)ps.e_sign[t] * s.Ef[ps.e_sf[t]][ps.e_src[t]];
+}
+
 }  // namespace
 
 void launch_edges(Solve& sv) {
@@ -235,6 +243,10 @@ void launch_edges(Solve& sv) {
   mark(sv, "k_edges_y");
   k_edges_z<<<blocks_for(ez.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, sv.st, ez);
   mark(sv, "k_edges_z");
+  if (sv.psync.ne > 0) {
+    k_sync_emf<<<blocks_for(sv.psync.ne, 128, sv.sm_count), 128, 0, sv.stream>>>(sv.st, sv.psync);
+    mark(sv, "k_sync_emf");
+  }
 }
 
 }  // namespace cs

@@ -277,6 +277,26 @@ __global__ void __launch_bounds__(FLUX_FACES * 5, 3) k_flux(Dims d, PhysC ph, DG
   }
 }
 
+// Panel-edge ownership for the face fluxes: a non-owner copy of a shared
+// face takes the owner's two one-sided contributions with the sides
+// exchanged (their normals are opposite) and the negated entropy flux.
+__global__ void k_sync_flux(Dims d, DState s, PanelSync ps) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < ps.nf; t += (long long)gridDim.x * blockDim.x) {
+    const long long dst = ps.f_dst[t], src = ps.f_src[t];
+    const int dd = ps.f_ddir[t], sd = ps.f_sdir[t];
+    const int dp = (int)(dst / d.S), sp = (int)(src / d.S);
+    const long long dof = dst % d.S, sof = src % d.S;
+    double* Fd = s.fcon[dd];
+    const double* Fs = s.fcon[sd];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      Fd[((long long)c * NPANEL + dp) * d.S + dof] = Fs[((long long)(8 + c) * NPANEL + sp) * d.S + sof];
+      Fd[((long long)(8 + c) * NPANEL + dp) * d.S + dof] = Fs[((long long)c * NPANEL + sp) * d.S + sof];
+    }
+    s.EF[dd][dst] = -s.EF[sd][src];
+  }
+}
+
 // dU/dt of each zone from its six faces (x, then y, then z; lower face,
 // upper face) for the zones whose faces were all computed.
 __global__ void k_gather(Dims d, DGeom g, DState s, Range3 r) {
@@ -343,6 +363,10 @@ void launch_fluxes(Solve& sv) {
     const int nb = (int)std::min<long long>(nt, (long long)sv.sm_count * 32);
     k_flux<<<nb, FLUX_FACES * 5, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, fr[dir], dir);
     mark(sv, "k_flux");
+  }
+  if (sv.psync.nf > 0) {
+    k_sync_flux<<<blocks_for(sv.psync.nf, 128, sv.sm_count), 128, 0, sv.stream>>>(d, sv.st, sv.psync);
+    mark(sv, "k_sync_flux");
   }
   Range3 z = {0, N + 1, 0, N + 1, 0, nr + 1};
   k_gather<<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, sv.st, z);

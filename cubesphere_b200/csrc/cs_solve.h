@@ -26,6 +26,15 @@ struct FillMap {
   long long n = 0;
 };
 
+// Panel-edge ownership maps on the device (see build_sync_maps).
+struct PanelSync {
+  int32_t *f_dst = nullptr, *f_src = nullptr;
+  int8_t *f_ddir = nullptr, *f_sdir = nullptr;
+  int32_t *e_dst = nullptr, *e_src = nullptr;
+  int8_t *e_df = nullptr, *e_sf = nullptr, *e_sign = nullptr;
+  long long nf = 0, ne = 0;
+};
+
 // Per-kernel device timing with CUDA events recorded on the solve's
 // stream between consecutive launches (enabled by cs_profile_begin).
 struct Prof {
@@ -47,6 +56,7 @@ struct Solve {
   GeomHost host;             // host geometry (kept for cs_geometry_get)
   std::vector<void*> allocs;  // device allocations owned by the solve
   FillMap fill;
+  PanelSync psync;
   cudaStream_t stream = nullptr;
   int device = 0;
   int sm_count = 148;

@@ -94,6 +94,13 @@ typedef struct cs_params {
 /* cs_params.flags: likewise for the inverse normal matrices of the
  * least-squares reconstructions of the primitives and of E (1.4 KB per zone). */
 #define CS_FLAG_NO_OP_CACHE 2
+/* cs_params.flags: keep each panel's own fluxes and EMFs on the faces and
+ * edges it shares with other panels instead of giving every shared face and
+ * edge the value of its owner (the lowest-numbered panel holding it).  The
+ * default ownership is this library's single-device form of the reference's
+ * defect correction (DRV:3200-3461): conservative, and div B stays at
+ * round-off across panel edges; without it div B grows at the cube corners. */
+#define CS_FLAG_NO_PANEL_SYNC 4
 
 /* Seeded initial-state description (new generator cases of the problem
  * library, built with the reference mechanism of 820init_patch_cube_sphere.f). */

@@ -7,8 +7,15 @@
 // Loop extents written in the reference for NGhost = 4 (e.g. "-2, n+3") are
 // expressed relative to the ghost depth G ("2-G, n+G-1") so that G = 4
 // reproduces them and G = 3 shrinks every stencil range by one layer.
+#include <algorithm>
+#include <cmath>
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <functional>
+#include <map>
+#include <tuple>
 #include <vector>
 
 #include "oracle_core.h"
@@ -39,6 +46,16 @@ struct Ctx {
   std::vector<double> U, ent, Bxf, Byf, Bzf, V, E, msonic, divvel, flat, work, Bqx, Bqy, Bqz, dUdt, SLx, SRx, SDy,
       SUy, SBz, STz, EFx, EFy, EFz, Efx, Efy, Efz, U0, ent0, Bxf0, Byf0, Bzf0;
   double time = 0.0;
+  // per-face, per-point flux contributions to the two zones the face
+  // updates ([dir]: [point*8 + comp][6][S]) and their target zones
+  std::vector<double> cL[3], cR[3];
+  std::vector<long long> tL[3], tR[3];
+  // panel-edge ownership maps (built on first use)
+  struct FaceSync { int dir, pn, i, j, k, odir, opn, oi, oj, ok; };
+  struct EdgeSync { int f, pn, i, j, k, of, opn, oi, oj, ok, sign; };
+  bool maps_built = false;
+  std::vector<FaceSync> fsync;
+  std::vector<EdgeSync> esync;
 
   size_t idx(int i, int j, int k) const { return ((size_t)(k + G) * NJ + (size_t)(j + G)) * NI + (size_t)(i + G); }
   double& a(std::vector<double>& v, int c, int pn, int i, int j, int k) { return v[((size_t)c * 6 + pn) * S + idx(i, j, k)]; }
@@ -968,10 +985,17 @@ void make_facial_fluxes(Ctx& c, int pn) {
   const int N = c.N, G = c.G, nr = c.nr;
   const double sm = c.p.smallnum;
   auto V = [&](int comp, int mode, int i, int j, int k) -> double& { return c.a(c.V, mode * NV + comp, pn, i, j, k); };
-  for (int k = 1 - G; k <= nr + G; ++k)
-    for (int j = 1 - G; j <= N + G; ++j)
-      for (int i = 1 - G; i <= N + G; ++i)
-        for (int q = 0; q < NV; ++q) c.a(c.dUdt, q, pn, i, j, k) = 0.0;
+  for (int dir = 0; dir < 3; ++dir) {
+    for (int t = 0; t < 5 * NV; ++t)
+      for (size_t o = 0; o < c.S; ++o) {
+        c.cL[dir][((size_t)t * 6 + pn) * c.S + o] = 0.0;
+        c.cR[dir][((size_t)t * 6 + pn) * c.S + o] = 0.0;
+      }
+    for (size_t o = 0; o < c.S; ++o) {
+      c.tL[dir][(size_t)pn * c.S + o] = -1;
+      c.tR[dir][(size_t)pn * c.S + o] = -1;
+    }
+  }
   for (int dir = 0; dir < 3; ++dir) {
     const int QP = dir == 0 ? XF_QP : (dir == 1 ? YF_QP : ZF_QP);
     const int QW = dir == 0 ? XF_QW : (dir == 1 ? YF_QW : ZF_QW);
@@ -1087,12 +1111,186 @@ void make_facial_fluxes(Ctx& c, int pn) {
             back(o.FR, FRR);
             double area = c.geo(AR, 0, pn, i, j, k);
             double volL = c.geo(V_VOL, 0, pn, lx, ly, lz), volR = c.geo(V_VOL, 0, pn, rx, ry, rz);
-            for (int q = 0; q < NV; ++q)
-              c.a(c.dUdt, q, pn, lx, ly, lz) = c.a(c.dUdt, q, pn, lx, ly, lz) - wt * (Fm[q] + FLL[q]) * area / volL;
-            for (int q = 0; q < NV; ++q)
-              c.a(c.dUdt, q, pn, rx, ry, rz) = c.a(c.dUdt, q, pn, rx, ry, rz) - wt * (Fp[q] - FRR[q]) * area / volR;
+            const size_t fo = c.idx(i, j, k);
+            for (int q = 0; q < NV; ++q) {
+              c.cL[dir][((size_t)(jq * NV + q) * 6 + pn) * c.S + fo] = wt * (Fm[q] + FLL[q]) * area / volL;
+              c.cR[dir][((size_t)(jq * NV + q) * 6 + pn) * c.S + fo] = wt * (Fp[q] - FRR[q]) * area / volR;
+            }
+            c.tL[dir][(size_t)pn * c.S + fo] = (long long)c.idx(lx, ly, lz);
+            c.tR[dir][(size_t)pn * c.S + fo] = (long long)c.idx(rx, ry, rz);
             if (jq == 0) c.a(EF, 0, pn, i, j, k) = o.entF;
           }
+  }
+}
+
+// Second half of MAKE_FACIAL_FLUXES: every face's per-point contributions
+// are subtracted from the time derivatives of the zones it updates, in the
+// reference's order (direction, quadrature point, face).
+void scatter_facial_fluxes(Ctx& c, int pn) {
+  const int N = c.N, G = c.G, nr = c.nr;
+  for (int k = 1 - G; k <= nr + G; ++k)
+    for (int j = 1 - G; j <= N + G; ++j)
+      for (int i = 1 - G; i <= N + G; ++i)
+        for (int q = 0; q < NV; ++q) c.a(c.dUdt, q, pn, i, j, k) = 0.0;
+  for (int dir = 0; dir < 3; ++dir) {
+    int lo[3] = {0, 0, 0}, hi[3] = {N + 1, N + 1, nr + 1};
+    lo[dir] = -1;
+    for (int jq = 0; jq < 5; ++jq)
+      for (int k = lo[2]; k <= hi[2]; ++k)
+        for (int j = lo[1]; j <= hi[1]; ++j)
+          for (int i = lo[0]; i <= hi[0]; ++i) {
+            const size_t fo = c.idx(i, j, k);
+            const long long l = c.tL[dir][(size_t)pn * c.S + fo], r = c.tR[dir][(size_t)pn * c.S + fo];
+            if (l < 0) continue;
+            for (int q = 0; q < NV; ++q) {
+              double& dl = c.dUdt[((size_t)q * 6 + pn) * c.S + (size_t)l];
+              dl = dl - c.cL[dir][((size_t)(jq * NV + q) * 6 + pn) * c.S + fo];
+            }
+            for (int q = 0; q < NV; ++q) {
+              double& dr = c.dUdt[((size_t)q * 6 + pn) * c.S + (size_t)r];
+              dr = dr - c.cR[dir][((size_t)(jq * NV + q) * 6 + pn) * c.S + fo];
+            }
+          }
+  }
+}
+
+// ------------------------------------------------------------------
+// Panel-edge ownership (the single-device counterpart of the reference's
+// defect correction, DRV:3200-3461 with 485update_defect_imex_rk.f): the
+// face fluxes of the faces on a panel edge and the EMFs of the edges on a
+// panel boundary are computed by both panels (three at a cube corner);
+// every copy takes the value of the copy owned by the lowest-numbered
+// panel, so each face and edge has one value, the update is conservative
+// and CT keeps div B at round-off across panel edges.
+//
+// Vertex identity across panels follows the ghost-fill index maps of
+// FILL_GHOST2D_GLOBAL (203:104-163): right edge (N, j) ~ right neighbour
+// (j, N); left (0, j) ~ (0, N - j); down (i, 0) ~ (N - i, 0); up (i, N) ~ (N, i).
+static void build_sync_maps(Ctx& c) {
+  const int N = c.N, nr = c.nr;
+  const int NV1 = N + 1;
+  std::vector<int> par((size_t)6 * NV1 * NV1);
+  for (size_t t = 0; t < par.size(); ++t) par[t] = (int)t;
+  auto vid = [&](int p, int i, int j) { return (p * NV1 + j) * NV1 + i; };
+  std::function<int(int)> root = [&](int x) {
+    while (par[x] != x) x = par[x] = par[par[x]];
+    return x;
+  };
+  auto unite = [&](int a, int b) {
+    a = root(a);
+    b = root(b);
+    if (a != b) par[std::max(a, b)] = std::min(a, b);
+  };
+  for (int p = 0; p < 6; ++p) {
+    const int rt = kNbr[p][0] - 1, lf = kNbr[p][1] - 1, up = kNbr[p][2] - 1, dn = kNbr[p][3] - 1;
+    for (int t = 0; t <= N; ++t) {
+      unite(vid(p, N, t), vid(rt, t, N));
+      unite(vid(p, 0, t), vid(lf, 0, N - t));
+      unite(vid(p, t, 0), vid(dn, N - t, 0));
+      unite(vid(p, t, N), vid(up, N, t));
+    }
+  }
+  // check the identities against the vertex coordinates
+  for (int p = 0; p < 6; ++p)
+    for (int j = 0; j <= N; ++j)
+      for (int i = 0; i <= N; ++i) {
+        const int r = root(vid(p, i, j));
+        const int rp = r / (NV1 * NV1), ri = r % NV1, rj = (r / NV1) % NV1;
+        for (int q = 0; q < 3; ++q) {
+          const double a = c.geo(G_VERT, q, p, i, j, 0), b = c.geo(G_VERT, q, rp, ri, rj, 0);
+          if (std::fabs(a - b) > 1e-9 * (std::fabs(c.geo(G_VERT, 0, p, i, j, 0)) + std::fabs(c.geo(G_VERT, 1, p, i, j, 0)) +
+                                          std::fabs(c.geo(G_VERT, 2, p, i, j, 0)))) {
+            std::fprintf(stderr, "oracle: panel-edge vertex map mismatch at panel %d (%d,%d)\n", p, i, j);
+            std::abort();
+          }
+        }
+      }
+  // faces on panel edges: (p, dir, i, j) ~ partner, k = 1..nr; the copy of
+  // the higher-numbered panel takes the owner's values
+  c.fsync.clear();
+  for (int p = 0; p < 6; ++p) {
+    const int rt = kNbr[p][0] - 1, lf = kNbr[p][1] - 1, up = kNbr[p][2] - 1, dn = kNbr[p][3] - 1;
+    for (int t = 1; t <= N; ++t)
+      for (int k = 1; k <= nr; ++k) {
+        const Ctx::FaceSync cand[4] = {{0, p, N, t, k, 1, rt, t, N, k},
+                                       {0, p, 0, t, k, 0, lf, 0, N + 1 - t, k},
+                                       {1, p, t, 0, k, 1, dn, N + 1 - t, 0, k},
+                                       {1, p, t, N, k, 0, up, N, t, k}};
+        for (const auto& f : cand)
+          if (f.opn < f.pn) c.fsync.push_back(f);
+      }
+  }
+  // edges on panel boundaries, grouped by their end vertices
+  struct Copy { int f, p, i, j, k, a, b; };  // a -> b: vertex roots in the edge's direction
+  std::map<std::tuple<int, int, int>, std::vector<Copy>> cls;
+  for (int p = 0; p < 6; ++p) {
+    for (int j = 0; j <= N; ++j)
+      for (int i = 0; i <= N; ++i) {
+        const bool bnd = i == 0 || i == N || j == 0 || j == N;
+        if (!bnd) continue;
+        for (int k = 1; k <= nr; ++k) {
+          const int r = root(vid(p, i, j));
+          cls[std::make_tuple(r, -1, k)].push_back({2, p, i, j, k, r, r});
+        }
+      }
+    for (int k = 0; k <= nr; ++k) {
+      for (int i : {0, N})
+        for (int j = 1; j <= N; ++j) {
+          const int a = root(vid(p, i, j - 1)), b = root(vid(p, i, j));
+          cls[std::make_tuple(std::min(a, b), std::max(a, b), k)].push_back({1, p, i, j, k, a, b});
+        }
+      for (int j : {0, N})
+        for (int i = 1; i <= N; ++i) {
+          const int a = root(vid(p, i - 1, j)), b = root(vid(p, i, j));
+          cls[std::make_tuple(std::min(a, b), std::max(a, b), k)].push_back({0, p, i, j, k, a, b});
+        }
+    }
+  }
+  c.esync.clear();
+  for (auto& kv : cls) {
+    auto& v = kv.second;
+    if (v.size() < 2) {
+      std::fprintf(stderr, "oracle: unshared panel-boundary edge\n");
+      std::abort();
+    }
+    std::sort(v.begin(), v.end(), [](const Copy& x, const Copy& y) { return x.p < y.p; });
+    const Copy& o = v[0];
+    for (size_t m = 1; m < v.size(); ++m) {
+      const Copy& x = v[m];
+      const int sign = (x.a == o.a && x.b == o.b) ? 1 : -1;
+      c.esync.push_back({x.f, x.p, x.i, x.j, x.k, o.f, o.p, o.i, o.j, o.k, sign});
+    }
+  }
+  c.maps_built = true;
+}
+
+static bool sync_on(const Ctx& c) { return !(c.p.flags & 4); }
+
+// Non-owner copies of panel-edge faces take the owner's contributions with
+// the two sides exchanged (the normals are opposite) and the negated
+// entropy flux.
+void sync_facial_fluxes(Ctx& c) {
+  if (!sync_on(c)) return;
+  if (!c.maps_built) build_sync_maps(c);
+  for (const auto& f : c.fsync) {
+    const size_t d = c.idx(f.i, f.j, f.k), o = c.idx(f.oi, f.oj, f.ok);
+    for (int t = 0; t < 5 * NV; ++t) {
+      c.cL[f.dir][((size_t)t * 6 + f.pn) * c.S + d] = c.cR[f.odir][((size_t)t * 6 + f.opn) * c.S + o];
+      c.cR[f.dir][((size_t)t * 6 + f.pn) * c.S + d] = c.cL[f.odir][((size_t)t * 6 + f.opn) * c.S + o];
+    }
+    std::vector<double>& EFd = f.dir == 0 ? c.EFx : (f.dir == 1 ? c.EFy : c.EFz);
+    const std::vector<double>& EFo = f.odir == 0 ? c.EFx : (f.odir == 1 ? c.EFy : c.EFz);
+    EFd[(size_t)f.pn * c.S + d] = -EFo[(size_t)f.opn * c.S + o];
+  }
+}
+
+void sync_edge_efields(Ctx& c) {
+  if (!sync_on(c)) return;
+  if (!c.maps_built) build_sync_maps(c);
+  for (const auto& e : c.esync) {
+    std::vector<double>& Ed = e.f == 0 ? c.Efx : (e.f == 1 ? c.Efy : c.Efz);
+    const std::vector<double>& Eo = e.of == 0 ? c.Efx : (e.of == 1 ? c.Efy : c.Efz);
+    Ed[(size_t)e.pn * c.S + c.idx(e.i, e.j, e.k)] = e.sign * Eo[(size_t)e.opn * c.S + c.idx(e.oi, e.oj, e.ok)];
   }
 }
 
@@ -1447,7 +1645,8 @@ double evaluate_timestep(Ctx& c, double dtcur) {
 
 // One RK stage in the driver's order (1000riemann_geomesh_cs_mhd.f:1746-2887):
 // ghost fill, then per panel reconstruction, fluxes, EMFs, sources, the
-// stage combine, the update and the clean-up.
+// stage combine, the update and the clean-up, with the panel-edge
+// ownership applied to the fluxes and EMFs before they are used.
 void stage(Ctx& c, int irk, double dtcur) {
   fill_ghosts(c);
   double dtmove = dtcur;
@@ -1465,7 +1664,16 @@ void stage(Ctx& c, int irk, double dtcur) {
   for (int pn = 0; pn < 6; ++pn) {
     limit_all_slopes_p12(c, pn);
     make_facial_fluxes(c, pn);
+  }
+  sync_facial_fluxes(c);
+#pragma omp parallel for schedule(static, 1)
+  for (int pn = 0; pn < 6; ++pn) {
+    scatter_facial_fluxes(c, pn);
     make_edge_efields(c, pn);
+  }
+  sync_edge_efields(c);
+#pragma omp parallel for schedule(static, 1)
+  for (int pn = 0; pn < 6; ++pn) {
     build_non_stiff_sources(c, pn);
     const size_t S = c.S;
     if (irk == 1) {
@@ -1524,6 +1732,12 @@ void* oracle_create(const void* params) {
   al(c->dUdt, 8); al(c->SLx, 1); al(c->SRx, 1); al(c->SDy, 1); al(c->SUy, 1); al(c->SBz, 1); al(c->STz, 1);
   al(c->EFx, 1); al(c->EFy, 1); al(c->EFz, 1); al(c->Efx, 1); al(c->Efy, 1); al(c->Efz, 1);
   al(c->U0, 8); al(c->ent0, 1); al(c->Bxf0, 1); al(c->Byf0, 1); al(c->Bzf0, 1);
+  for (int d = 0; d < 3; ++d) {
+    al(c->cL[d], 5 * 8);
+    al(c->cR[d], 5 * 8);
+    c->tL[d].assign(S6, -1);
+    c->tR[d].assign(S6, -1);
+  }
   return c;
 }
 
@@ -1595,10 +1809,15 @@ void oracle_limit_all_slopes_p12(void* h) {
   for (int p = 0; p < 6; ++p) limit_all_slopes_p12(*(Ctx*)h, p);
 }
 void oracle_make_facial_fluxes(void* h) {
-  for (int p = 0; p < 6; ++p) make_facial_fluxes(*(Ctx*)h, p);
+  Ctx& c = *(Ctx*)h;
+  for (int p = 0; p < 6; ++p) make_facial_fluxes(c, p);
+  sync_facial_fluxes(c);
+  for (int p = 0; p < 6; ++p) scatter_facial_fluxes(c, p);
 }
 void oracle_make_edge_efields(void* h) {
-  for (int p = 0; p < 6; ++p) make_edge_efields(*(Ctx*)h, p);
+  Ctx& c = *(Ctx*)h;
+  for (int p = 0; p < 6; ++p) make_edge_efields(c, p);
+  sync_edge_efields(c);
 }
 void oracle_build_non_stiff_sources(void* h) {
   for (int p = 0; p < 6; ++p) build_non_stiff_sources(*(Ctx*)h, p);
