@@ -7,7 +7,7 @@
 ``shell128``   6 x 128^2 x 64, r in [1, 2] with geometric radial stretch 1.02,
                4 ghost layers, FP64: hydrostatic 1/r^2 shell with seeded density
                and field perturbations of amplitude 0.05 under point-mass
-               gravity, two-stage RK.
+               gravity, IMEX-RK2 (ARS(2,2,2), gravity implicit).
 ``shell16`` / ``shell32``  the same shell at test sizes.
 """
 from __future__ import annotations
@@ -21,19 +21,19 @@ PRESETS = {
     ),
     "shell128": dict(
         params=dict(ntp=128, nr=64, nghost=4, radial_mesh="stretched", radial_ratio=1.02, rmin=1.0, rmax=2.0,
-                    gamma=5.0 / 3.0, cfl_coef=0.4, rk_scheme=2, gm=1.0),
+                    gamma=5.0 / 3.0, cfl_coef=0.4, rk_scheme=4, gm=1.0),
         init=dict(seed=2025, kind=1, lmax=4, rho_amp=0.05, a_amp=0.05, v_amp=0.0, p0=0.05),
         steps=50,
     ),
     "shell32": dict(
         params=dict(ntp=32, nr=16, nghost=4, radial_mesh="stretched", radial_ratio=1.02, rmin=1.0, rmax=2.0,
-                    gamma=5.0 / 3.0, cfl_coef=0.4, rk_scheme=2, gm=1.0),
+                    gamma=5.0 / 3.0, cfl_coef=0.4, rk_scheme=4, gm=1.0),
         init=dict(seed=2025, kind=1, lmax=4, rho_amp=0.05, a_amp=0.05, v_amp=0.0, p0=0.05),
         steps=10,
     ),
     "shell16": dict(
         params=dict(ntp=16, nr=8, nghost=4, radial_mesh="stretched", radial_ratio=1.02, rmin=1.0, rmax=2.0,
-                    gamma=5.0 / 3.0, cfl_coef=0.4, rk_scheme=2, gm=1.0),
+                    gamma=5.0 / 3.0, cfl_coef=0.4, rk_scheme=4, gm=1.0),
         init=dict(seed=2025, kind=1, lmax=4, rho_amp=0.05, a_amp=0.05, v_amp=0.0, p0=0.05),
         steps=4,
     ),

@@ -344,8 +344,8 @@ bool check_params(const cs_params& p, std::string& why) {
   if (!(p.gamma > 1.0)) { why = "gamma must be > 1"; return false; }
   if (!(p.rmax > p.rmin) || !(p.rmin > 0.0)) { why = "need 0 < rmin < rmax"; return false; }
   if (p.radial_mesh < 0 || p.radial_mesh > 2) { why = "radial_mesh must be 0, 1 or 2"; return false; }
-  if (p.rk_scheme != CS_RK2 && p.rk_scheme != CS_SSPRK3) {
-    why = "rk_scheme must be CS_RK2 or CS_SSPRK3";
+  if (p.rk_scheme != CS_RK2 && p.rk_scheme != CS_SSPRK3 && p.rk_scheme != CS_IMEX_RK2) {
+    why = "rk_scheme must be CS_RK2, CS_SSPRK3 or CS_IMEX_RK2";
     return false;
   }
   if (!(p.smallnum > 0.0) || !(p.rhofloor > 0.0) || !(p.prsfloor > 0.0)) {
@@ -419,6 +419,11 @@ int upload_mesh(Solve& sv) {
   for (int q = 0; q < 3; ++q) { s.Bq[q] = A(NQ); s.fcon[q] = A(2 * NVAR); s.EF[q] = A(1); s.Ef[q] = A(1); s.B0[q] = A(1); }
   for (int q = 0; q < 6; ++q) s.S[q] = A(1);
   s.dUdt = A(NVAR); s.U0 = A(NVAR); s.ent0 = A(1);
+  if (sv.p.rk_scheme == CS_IMEX_RK2) {
+    s.K1 = A(NVAR);
+    for (int q = 0; q < 3; ++q) { s.EF1[q] = A(1); s.Ef1[q] = A(1); }
+    if (!s.K1 || !s.EF1[2] || !s.Ef1[2]) return cuda_fail(sv, e, "cudaMalloc(IMEX stage rates)");
+  }
   s.FS = A(6 * NQ * (NVAR + 1));
   if (!s.FS) return cuda_fail(sv, e, "cudaMalloc(face states)");
   set_adp_smem_limits();
@@ -540,9 +545,45 @@ void limit_all(Solve& sv) {
   launch_efield(sv);
 }
 
+// IMEX-RK2: ARS(2,2,2) (Ascher, Ruuth & Spiteri 1997) with the fluxes, the
+// entropy transport and CT explicit and the point-mass gravity implicit,
+// gamma = 1 - 1/sqrt(2), delta = 1 - 1/(2 gamma):
+//   stage 1: U* = U^n + gamma dt F(U^n);          U2 = U* + gamma dt S(U2)
+//   stage 2: U* = U^n + delta dt F(U^n) + (1-delta) dt F(U2) + (1-gamma) dt S(U2)
+//            U^{n+1} = U* + gamma dt S(U^{n+1})
+// with face B and the entropy advanced by the same explicit weights.
+int run_stage_imex(Solve& sv, int irk, double dtcur) {
+  const double gam = 1.0 - 1.0 / std::sqrt(2.0), del = 1.0 - 1.0 / (2.0 * gam);
+  prof_start(sv);
+  launch_fill_ghosts(sv);
+  limit_all(sv);
+  launch_fluxes(sv);
+  launch_edges(sv);
+  if (irk == 1) {
+    launch_save_stage0(sv);
+    launch_save_stage1_rates(sv);
+    launch_update(sv, gam * dtcur);
+  } else {
+    launch_add_gravity(sv, (1.0 - gam) / (1.0 - del));
+    launch_restore_stage0(sv);
+    DState s1 = sv.st;
+    s1.dUdt = sv.st.K1;
+    for (int q = 0; q < 3; ++q) {
+      s1.EF[q] = sv.st.EF1[q];
+      s1.Ef[q] = sv.st.Ef1[q];
+    }
+    launch_update_with(sv, s1, del * dtcur);
+    launch_update(sv, (1.0 - del) * dtcur);
+  }
+  launch_gravity_implicit(sv, gam * dtcur);
+  launch_cleanup(sv);
+  return launch_check(sv, "stage launch");
+}
+
 int run_stage(Solve& sv, int irk, double dtcur) {
   const int ns = sv.p.rk_scheme == CS_SSPRK3 ? 3 : 2;
   if (irk < 1 || irk > ns) return fail(sv, CS_ERR_ARG, "irk out of range for the RK scheme");
+  if (sv.p.rk_scheme == CS_IMEX_RK2) return run_stage_imex(sv, irk, dtcur);
   double dtmove = dtcur, a0 = 0.0;
   int kind = 0;
   if (sv.p.rk_scheme == CS_SSPRK3) {

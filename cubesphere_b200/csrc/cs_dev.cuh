@@ -48,6 +48,7 @@ struct DState {
   double *Ef[3];                         // edge EMFs
   double *dUdt;                          // 8
   double *U0, *ent0, *B0[3];             // saved stage-1 state
+  double *K1, *EF1[3], *Ef1[3];          // IMEX: first stage's dU/dt, entropy fluxes and EMFs
   double* op_m9;                         // STEP 7.b inverse normal matrices, [81][zones of shrink(2)], or null
   double* op_m10;                        // STEP 9.c inverse normal matrices, [100][zones of shrink(2)], or null
   double* adp_lu;                        // ADP KKT factors: per block of 128 zones, [1296 in use order][128], or null
@@ -408,6 +409,11 @@ void launch_sources(Solve& s);
 void launch_save_stage0(Solve& s);
 void launch_combine(Solve& s, double a0, int kind);
 void launch_update(Solve& s, double dtmove);
+void launch_update_with(Solve& s, const DState& st, double dtmove);
+void launch_gravity_implicit(Solve& s, double a);
+void launch_add_gravity(Solve& s, double c);
+void launch_save_stage1_rates(Solve& s);
+void launch_restore_stage0(Solve& s);
 void launch_cleanup(Solve& s);
 void launch_timestep(Solve& s, double dtcur);
 void launch_fill_ghosts(Solve& s);

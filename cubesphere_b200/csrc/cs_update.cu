@@ -337,19 +337,105 @@ void launch_combine(Solve& sv, double a0, int kind) {
   mark(sv, "k_combine");
 }
 
-void launch_update(Solve& sv, double dtmove) {
+void launch_update_with(Solve& sv, const DState& st, double dtmove) {
   const Dims& d = sv.d;
   Range3 z = zones_all(d);
-  k_update_zones<<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, z, dtmove);
+  k_update_zones<<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, z, dtmove);
   mark(sv, "k_update_zones");
   const int N = d.N, nr = d.nr;
   Range3 fx = {0, N, 1, N, 1, nr}, fy = {1, N, 0, N, 1, nr}, fz = {1, N, 1, N, 0, nr};
-  k_ct<<<blocks_for(fx.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, sv.st, fx, 0, dtmove);
+  k_ct<<<blocks_for(fx.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, st, fx, 0, dtmove);
   mark(sv, "k_ct");
-  k_ct<<<blocks_for(fy.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, sv.st, fy, 1, dtmove);
+  k_ct<<<blocks_for(fy.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, st, fy, 1, dtmove);
   mark(sv, "k_ct");
-  k_ct<<<blocks_for(fz.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, sv.st, fz, 2, dtmove);
+  k_ct<<<blocks_for(fz.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, st, fz, 2, dtmove);
   mark(sv, "k_ct");
+}
+
+void launch_update(Solve& sv, double dtmove) { launch_update_with(sv, sv.st, dtmove); }
+
+// ---- IMEX-RK2: ARS(2,2,2) with the point-mass gravity implicit ----
+// Gravity S(U) = (0, -rho g, -m . g), g = GM x / r^3, on the active zones
+// 0..N+1 (the zones of BUILD_NON_STIFF_SOURCES).  rho is unchanged by it,
+// so the implicit stage U = U* + a S(U) has the closed form
+// m = m* - a rho g, E = E* - a m . g.
+__global__ void k_gravity_implicit(Dims d, PhysC ph, DGeom g, DState s, Range3 r, double a) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
+    int p, i, j, k;
+    r.decode(t, p, i, j, k);
+    if (mask_at(g, d, p, i, j) != 1) continue;
+    const double x = geo(g, d, CS_G_V_CEN, 0, p, i, j, k), y = geo(g, d, CS_G_V_CEN, 1, p, i, j, k),
+                 z = geo(g, d, CS_G_V_CEN, 2, p, i, j, k);
+    const double rad = sqrt(x * x + y * y + z * z);
+    const double gmb = ph.gm * (1.0 / (rad * rad * rad));
+    const double gx = gmb * x, gy = gmb * y, gz = gmb * z;
+    const double rho = s.U[d.at(0, p, i, j, k)];
+    double& m1 = s.U[d.at(1, p, i, j, k)];
+    double& m2 = s.U[d.at(2, p, i, j, k)];
+    double& m3 = s.U[d.at(3, p, i, j, k)];
+    m1 = m1 - a * (gx * rho);
+    m2 = m2 - a * (gy * rho);
+    m3 = m3 - a * (gz * rho);
+    double& e = s.U[d.at(4, p, i, j, k)];
+    e = e - a * (gx * m1 + gy * m2 + gz * m3);
+  }
+}
+
+// dUdt += c S(U) with the gravity of the current state (explicit use of
+// the previous stage's source).
+__global__ void k_add_gravity(Dims d, PhysC ph, DGeom g, DState s, Range3 r, double c) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
+    int p, i, j, k;
+    r.decode(t, p, i, j, k);
+    if (mask_at(g, d, p, i, j) != 1) continue;
+    const double x = geo(g, d, CS_G_V_CEN, 0, p, i, j, k), y = geo(g, d, CS_G_V_CEN, 1, p, i, j, k),
+                 z = geo(g, d, CS_G_V_CEN, 2, p, i, j, k);
+    const double rad = sqrt(x * x + y * y + z * z);
+    const double gmb = ph.gm * (1.0 / (rad * rad * rad));
+    const double gx = gmb * x, gy = gmb * y, gz = gmb * z;
+    const double rho = s.U[d.at(0, p, i, j, k)];
+    const double m1 = s.U[d.at(1, p, i, j, k)], m2 = s.U[d.at(2, p, i, j, k)], m3 = s.U[d.at(3, p, i, j, k)];
+    s.dUdt[d.at(1, p, i, j, k)] += c * (-(gx * rho));
+    s.dUdt[d.at(2, p, i, j, k)] += c * (-(gy * rho));
+    s.dUdt[d.at(3, p, i, j, k)] += c * (-(gz * rho));
+    s.dUdt[d.at(4, p, i, j, k)] += c * (-(gx * m1 + gy * m2 + gz * m3));
+  }
+}
+
+void launch_gravity_implicit(Solve& sv, double a) {
+  if (!(sv.ph.gm > sv.p.smallnum)) return;
+  Range3 z = {0, sv.d.N + 1, 0, sv.d.N + 1, 0, sv.d.nr + 1};
+  k_gravity_implicit<<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(sv.d, sv.ph, sv.g, sv.st, z, a);
+  mark(sv, "k_gravity_implicit");
+}
+
+void launch_add_gravity(Solve& sv, double c) {
+  if (!(sv.ph.gm > sv.p.smallnum)) return;
+  Range3 z = {0, sv.d.N + 1, 0, sv.d.N + 1, 0, sv.d.nr + 1};
+  k_add_gravity<<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(sv.d, sv.ph, sv.g, sv.st, z, c);
+  mark(sv, "k_add_gravity");
+}
+
+// Copies of the first stage's flux divergence, entropy fluxes and EMFs,
+// and the restore of the step's initial state.
+void launch_save_stage1_rates(Solve& sv) {
+  const size_t S6 = (size_t)6 * sv.d.S * sizeof(double);
+  cudaMemcpyAsync(sv.st.K1, sv.st.dUdt, NVAR * S6, cudaMemcpyDeviceToDevice, sv.stream);
+  for (int q = 0; q < 3; ++q) {
+    cudaMemcpyAsync(sv.st.EF1[q], sv.st.EF[q], S6, cudaMemcpyDeviceToDevice, sv.stream);
+    cudaMemcpyAsync(sv.st.Ef1[q], sv.st.Ef[q], S6, cudaMemcpyDeviceToDevice, sv.stream);
+  }
+  mark(sv, "copy_stage1_rates", false);
+}
+
+void launch_restore_stage0(Solve& sv) {
+  const size_t S6 = (size_t)6 * sv.d.S * sizeof(double);
+  cudaMemcpyAsync(sv.st.U, sv.st.U0, NVAR * S6, cudaMemcpyDeviceToDevice, sv.stream);
+  cudaMemcpyAsync(sv.st.ent, sv.st.ent0, S6, cudaMemcpyDeviceToDevice, sv.stream);
+  cudaMemcpyAsync(sv.st.Bxf, sv.st.B0[0], S6, cudaMemcpyDeviceToDevice, sv.stream);
+  cudaMemcpyAsync(sv.st.Byf, sv.st.B0[1], S6, cudaMemcpyDeviceToDevice, sv.stream);
+  cudaMemcpyAsync(sv.st.Bzf, sv.st.B0[2], S6, cudaMemcpyDeviceToDevice, sv.stream);
+  mark(sv, "copy_restore", false);
 }
 
 void launch_cleanup(Solve& sv) {

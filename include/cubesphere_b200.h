@@ -65,7 +65,8 @@ enum cs_radial_mesh { CS_RADIAL_UNIFORM = 0, CS_RADIAL_LOG = 1, CS_RADIAL_STRETC
 /* Time integrators.  CS_RK2 is the reference's two-stage combine
  * (1000riemann_geomesh_cs_mhd.f:2661-2773); CS_SSPRK3 the three-stage
  * Shu-Osher scheme in the same combine form; CS_IMEX_RK2 the two-stage
- * scheme with the radial gravity source taken implicitly. */
+ * ARS(2,2,2) scheme with fluxes, entropy transport and CT explicit and the
+ * point-mass gravity implicit (closed form: gravity leaves rho unchanged). */
 enum cs_rk_scheme { CS_RK2 = 2, CS_SSPRK3 = 3, CS_IMEX_RK2 = 4 };
 
 /* Runtime parameters: the reference's compile-time directives, module

@@ -45,6 +45,8 @@ struct Ctx {
   // state and work arrays, [comp][6][S]
   std::vector<double> U, ent, Bxf, Byf, Bzf, V, E, msonic, divvel, flat, work, Bqx, Bqy, Bqz, dUdt, SLx, SRx, SDy,
       SUy, SBz, STz, EFx, EFy, EFz, Efx, Efy, Efz, U0, ent0, Bxf0, Byf0, Bzf0;
+  // IMEX: the first stage's dU/dt, entropy fluxes and EMFs
+  std::vector<double> K1, EFx1, EFy1, EFz1, Efx1, Efy1, Efz1;
   double time = 0.0;
   // per-face, per-point flux contributions to the two zones the face
   // updates ([dir]: [point*8 + comp][6][S]) and their target zones
@@ -1643,16 +1645,124 @@ double evaluate_timestep(Ctx& c, double dtcur) {
   return dt;
 }
 
+// IMEX-RK2 pieces (ARS(2,2,2), gravity implicit).  Gravity S(U) = (0,
+// -rho g, -m . g) with g = GM x / r^3 on the active zones 0..N+1; the
+// implicit stage U = U* + a S(U) is closed-form because rho is unchanged.
+static void gravity_implicit(Ctx& c, int pn, double a) {
+  if (!(c.p.gm > c.p.smallnum)) return;
+  const int N = c.N, nr = c.nr;
+  for (int k = 0; k <= nr + 1; ++k)
+    for (int j = 0; j <= N + 1; ++j)
+      for (int i = 0; i <= N + 1; ++i) {
+        if (c.m(pn, i, j) != 1) continue;
+        double x = c.geo(V_CEN, 0, pn, i, j, k), y = c.geo(V_CEN, 1, pn, i, j, k), z = c.geo(V_CEN, 2, pn, i, j, k);
+        double rad = std::sqrt(x * x + y * y + z * z);
+        double gmb = c.p.gm * (1.0 / (rad * rad * rad));
+        double gx = gmb * x, gy = gmb * y, gz = gmb * z;
+        double rho = c.a(c.U, 0, pn, i, j, k);
+        double& m1 = c.a(c.U, 1, pn, i, j, k);
+        double& m2 = c.a(c.U, 2, pn, i, j, k);
+        double& m3 = c.a(c.U, 3, pn, i, j, k);
+        m1 = m1 - a * (gx * rho);
+        m2 = m2 - a * (gy * rho);
+        m3 = m3 - a * (gz * rho);
+        double& e = c.a(c.U, 4, pn, i, j, k);
+        e = e - a * (gx * m1 + gy * m2 + gz * m3);
+      }
+}
+
+static void add_gravity(Ctx& c, int pn, double cc) {
+  if (!(c.p.gm > c.p.smallnum)) return;
+  const int N = c.N, nr = c.nr;
+  for (int k = 0; k <= nr + 1; ++k)
+    for (int j = 0; j <= N + 1; ++j)
+      for (int i = 0; i <= N + 1; ++i) {
+        if (c.m(pn, i, j) != 1) continue;
+        double x = c.geo(V_CEN, 0, pn, i, j, k), y = c.geo(V_CEN, 1, pn, i, j, k), z = c.geo(V_CEN, 2, pn, i, j, k);
+        double rad = std::sqrt(x * x + y * y + z * z);
+        double gmb = c.p.gm * (1.0 / (rad * rad * rad));
+        double gx = gmb * x, gy = gmb * y, gz = gmb * z;
+        double rho = c.a(c.U, 0, pn, i, j, k);
+        double m1 = c.a(c.U, 1, pn, i, j, k), m2 = c.a(c.U, 2, pn, i, j, k), m3 = c.a(c.U, 3, pn, i, j, k);
+        c.a(c.dUdt, 1, pn, i, j, k) += cc * (-(gx * rho));
+        c.a(c.dUdt, 2, pn, i, j, k) += cc * (-(gy * rho));
+        c.a(c.dUdt, 3, pn, i, j, k) += cc * (-(gz * rho));
+        c.a(c.dUdt, 4, pn, i, j, k) += cc * (-(gx * m1 + gy * m2 + gz * m3));
+      }
+}
+
+// One ARS(2,2,2) stage: fluxes, entropy transport and CT explicit, gravity
+// implicit; gamma = 1 - 1/sqrt(2), delta = 1 - 1/(2 gamma).
+//   stage 1: U* = U^n + gamma dt F(U^n);  U2 = U* + gamma dt S(U2)
+//   stage 2: U* = U^n + delta dt F(U^n) + (1-delta) dt F(U2) + (1-gamma) dt S(U2)
+//            U^{n+1} = U* + gamma dt S(U^{n+1})
+static void stage_imex(Ctx& c, int irk, double dtcur) {
+  const double gam = 1.0 - 1.0 / std::sqrt(2.0), del = 1.0 - 1.0 / (2.0 * gam);
+  fill_ghosts(c);
+#pragma omp parallel for schedule(static, 1)
+  for (int pn = 0; pn < 6; ++pn) {
+    limit_all_slopes_p12(c, pn);
+    make_facial_fluxes(c, pn);
+  }
+  sync_facial_fluxes(c);
+#pragma omp parallel for schedule(static, 1)
+  for (int pn = 0; pn < 6; ++pn) {
+    scatter_facial_fluxes(c, pn);
+    make_edge_efields(c, pn);
+  }
+  sync_edge_efields(c);
+  if (irk == 1) {
+    c.U0 = c.U;
+    std::memcpy(c.ent0.data(), c.ent.data(), 6 * c.S * sizeof(double));
+    c.Bxf0 = c.Bxf;
+    c.Byf0 = c.Byf;
+    c.Bzf0 = c.Bzf;
+    c.K1 = c.dUdt;
+    c.EFx1 = c.EFx; c.EFy1 = c.EFy; c.EFz1 = c.EFz;
+    c.Efx1 = c.Efx; c.Efy1 = c.Efy; c.Efz1 = c.Efz;
+#pragma omp parallel for schedule(static, 1)
+    for (int pn = 0; pn < 6; ++pn) update(c, pn, gam * dtcur);
+  } else {
+#pragma omp parallel for schedule(static, 1)
+    for (int pn = 0; pn < 6; ++pn) add_gravity(c, pn, (1.0 - gam) / (1.0 - del));
+    c.U = c.U0;
+    std::memcpy(c.ent.data(), c.ent0.data(), 6 * c.S * sizeof(double));
+    c.Bxf = c.Bxf0;
+    c.Byf = c.Byf0;
+    c.Bzf = c.Bzf0;
+    auto swap1 = [&]() {
+      std::swap(c.dUdt, c.K1);
+      std::swap(c.EFx, c.EFx1); std::swap(c.EFy, c.EFy1); std::swap(c.EFz, c.EFz1);
+      std::swap(c.Efx, c.Efx1); std::swap(c.Efy, c.Efy1); std::swap(c.Efz, c.Efz1);
+    };
+    swap1();
+#pragma omp parallel for schedule(static, 1)
+    for (int pn = 0; pn < 6; ++pn) update(c, pn, del * dtcur);
+    swap1();
+#pragma omp parallel for schedule(static, 1)
+    for (int pn = 0; pn < 6; ++pn) update(c, pn, (1.0 - del) * dtcur);
+  }
+#pragma omp parallel for schedule(static, 1)
+  for (int pn = 0; pn < 6; ++pn) {
+    gravity_implicit(c, pn, gam * dtcur);
+    cleanup(c, pn);
+  }
+}
+
 // One RK stage in the driver's order (1000riemann_geomesh_cs_mhd.f:1746-2887):
 // ghost fill, then per panel reconstruction, fluxes, EMFs, sources, the
 // stage combine, the update and the clean-up, with the panel-edge
 // ownership applied to the fluxes and EMFs before they are used.
 void stage(Ctx& c, int irk, double dtcur) {
+  if (c.p.rk_scheme == 4) {
+    stage_imex(c, irk, dtcur);
+    return;
+  }
   fill_ghosts(c);
   double dtmove = dtcur;
   double a0 = 0.0;  // weight of the saved state in the combine
   int scheme = c.p.rk_scheme;
-  if (scheme == 2 || scheme == 4) {
+  if (scheme == 2) {
     if (irk == 2) dtmove = 0.5 * dtcur;
   } else if (scheme == 3) {
     if (irk == 2) { a0 = 0.75; dtmove = 0.25 * dtcur; }
@@ -1732,6 +1842,9 @@ void* oracle_create(const void* params) {
   al(c->dUdt, 8); al(c->SLx, 1); al(c->SRx, 1); al(c->SDy, 1); al(c->SUy, 1); al(c->SBz, 1); al(c->STz, 1);
   al(c->EFx, 1); al(c->EFy, 1); al(c->EFz, 1); al(c->Efx, 1); al(c->Efy, 1); al(c->Efz, 1);
   al(c->U0, 8); al(c->ent0, 1); al(c->Bxf0, 1); al(c->Byf0, 1); al(c->Bzf0, 1);
+  if (c->p.rk_scheme == 4) {
+    al(c->K1, 8); al(c->EFx1, 1); al(c->EFy1, 1); al(c->EFz1, 1); al(c->Efx1, 1); al(c->Efy1, 1); al(c->Efz1, 1);
+  }
   for (int d = 0; d < 3; ++d) {
     al(c->cL[d], 5 * 8);
     al(c->cR[d], 5 * 8);

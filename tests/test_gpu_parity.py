@@ -24,9 +24,10 @@ def rel(a, b):
     return float(np.abs(a - b).max() / (den if den > 0 else 1.0))
 
 
-def make_pair(name, flags=0):
+def make_pair(name, flags=0, **over):
     from oracle import Oracle
     pr = cs.preset(name)
+    pr["params"].update(over)
     s = cs.Solve(**pr["params"], flags=flags)
     s.mesh_build()
     s.init_problem(**pr["init"])
@@ -117,13 +118,15 @@ def test_routines_in_sequence(shell16):
     check_state(s, s.get_state(), o.get_state())
 
 
-@pytest.mark.parametrize("name,nsteps,flags", [("shell16", 2, 0), ("surface32", 2, 0),
-                                               ("shell16", 1, cs.CS_FLAG_NO_ADP_CACHE | cs.CS_FLAG_NO_OP_CACHE),
-                                               ("shell16", 2, cs.CS_FLAG_NO_PANEL_SYNC)])
-def test_whole_steps_match_oracle(name, nsteps, flags):
+@pytest.mark.parametrize("name,nsteps,flags,rk", [
+    ("shell16", 2, 0, cs.CS_IMEX_RK2), ("shell16", 2, 0, cs.CS_RK2), ("surface32", 2, 0, cs.CS_SSPRK3),
+    ("shell16", 1, cs.CS_FLAG_NO_ADP_CACHE | cs.CS_FLAG_NO_OP_CACHE, cs.CS_IMEX_RK2),
+    ("shell16", 2, cs.CS_FLAG_NO_PANEL_SYNC, cs.CS_RK2)])
+def test_whole_steps_match_oracle(name, nsteps, flags, rk):
     """flags=0 uses the resident geometry-only operators (ADP factors, least-squares
-    inverses); the NO_*_CACHE flags rebuild them in every stage."""
-    s, o, st = make_pair(name, flags)
+    inverses) and panel-edge ownership; the flags switch them off.  rk: RK2 (the
+    reference's combine), SSP-RK3, IMEX-RK2 (ARS(2,2,2), gravity implicit)."""
+    s, o, st = make_pair(name, flags, rk_scheme=rk)
     dt_s = s.evaluate_timestep(1e30)
     dt_o = o.evaluate_timestep(1e30)
     assert abs(dt_s - dt_o) <= TOL_STATE * dt_o

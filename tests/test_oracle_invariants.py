@@ -8,8 +8,9 @@ import cubesphere_b200 as cs
 from oracle import Oracle
 
 
-def _setup(flags):
+def _setup(flags, **over):
     pr = cs.preset("shell16")
+    pr["params"].update(over)
     s = cs.Solve(**pr["params"], flags=flags)
     s.mesh_build(device=False)
     st = s.init_problem_host(**pr["init"])
@@ -37,8 +38,9 @@ def test_initial_field_is_divergence_free():
     assert _divb(s, st) < 1e-12
 
 
-def test_panel_edge_ownership_keeps_div_b_at_roundoff():
-    s, o, st = _setup(0)
+@pytest.mark.parametrize("rk", [cs.CS_RK2, cs.CS_IMEX_RK2])
+def test_panel_edge_ownership_keeps_div_b_at_roundoff(rk):
+    s, o, st = _setup(0, rk_scheme=rk)
     dt = o.evaluate_timestep(1e30)
     for _ in range(2):
         dt = o.step(dt)
@@ -48,7 +50,7 @@ def test_panel_edge_ownership_keeps_div_b_at_roundoff():
 def test_per_panel_edges_let_div_b_grow():
     """Without ownership each panel evolves its copy of a shared face with
     its own EMFs; the copies drift apart near the cube corners."""
-    s, o, st = _setup(cs.CS_FLAG_NO_PANEL_SYNC)
+    s, o, st = _setup(cs.CS_FLAG_NO_PANEL_SYNC, rk_scheme=cs.CS_RK2)
     dt = o.evaluate_timestep(1e30)
     dt = o.step(dt)
     assert _divb(s, o.get_state()) > 1e-6
