@@ -9,7 +9,7 @@ replica of the solve: the path does not shard).
 Default workload ``shell128``: 6 panels x 128^2 angular x 64 radial zones,
 radii 1..2 with geometric stretch 1.02, 4 ghost layers, FP64, hydrostatic
 1/r^2 shell with seeded density / field perturbations (amplitude 0.05)
-under point-mass gravity, two-stage RK.  The state (0.8 GB) and the
+under point-mass gravity, IMEX-RK2.  The state (0.8 GB) and the
 per-stage work arrays are far larger than L2, so no L2 flush is needed.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
@@ -61,9 +61,9 @@ ALGO_WORDS_PER_UNIT = {
 }
 
 WORKLOAD_DOC = {
-    "shell128": "FP64 ideal-MHD hydrostatic shell, 6x128^2x64 zones, r 1..2 stretch 1.02, 4 ghosts, RK2, "
+    "shell128": "FP64 ideal-MHD hydrostatic shell, 6x128^2x64 zones, r 1..2 stretch 1.02, 4 ghosts, IMEX-RK2, "
                 "P12 WENO-AO/MRWENO + ADP, HLL fluxes, LLF multi-D EMFs, CT",
-    "shell32": "FP64 ideal-MHD hydrostatic shell, 6x32^2x16 zones, 4 ghosts, RK2",
+    "shell32": "FP64 ideal-MHD hydrostatic shell, 6x32^2x16 zones, 4 ghosts, IMEX-RK2",
     "surface32": "FP64 ideal-MHD surface, 6x32^2x1 zones, 3 ghosts, SSP-RK3",
 }
 
@@ -76,6 +76,7 @@ def parse():
     ap.add_argument("--impl", default="cubesphere_b200", choices=["cubesphere_b200", "reference"])
     ap.add_argument("--workload", default="shell128")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving-form sample")
     ap.add_argument("--profile-json", default="", help="also write the per-kernel device times here")
     return ap.parse_args()
 
@@ -159,6 +160,57 @@ def cpu_baseline_sample(threads: int, steps: int = 1) -> dict:
     return {"value": zones * steps / sec, "unit": "zone-updates/s", "cores": threads, "kind": "port",
             "sample": f"oracle C++ port, shell 6x{s.N}^2x{s.nr} zones (same physics as the workload), "
                       f"{steps} RK2 step(s), {sec:.2f} s"}
+
+
+def serving_sample(seed: int = 7, nreq: int = 16, rate: float = 4.0, max_active: int = 8) -> dict:
+    """Serving form on a bounded sample: Poisson arrivals (seeded rate) of
+    solve requests with panel N from {32, 48}, radial depth from {1, 8, 16}
+    and 10..30 steps, admitted by free device memory into the concurrent
+    server; then the same requests run one at a time (the plain path run
+    sequentially) for the throughput comparison."""
+    import numpy as np
+
+    import cubesphere_b200 as cs
+
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for _ in range(nreq):
+        ntp = int(rng.choice([32, 48]))
+        nr = int(rng.choice([1, 8, 16]))
+        steps = int(rng.integers(10, 31))
+        pr = cs.preset("shell16")
+        params = dict(pr["params"])
+        init = dict(pr["init"])
+        params.update(ntp=ntp, nr=nr, nghost=4 if nr > 1 else 3)
+        init.update(seed=int(rng.integers(1, 1 << 30)))
+        if nr == 1:
+            params.update(gm=0.0, rmin=1.0, rmax=1.05, radial_mesh="uniform", rk_scheme=cs.CS_SSPRK3)
+            init.update(kind=0, v_amp=0.5, p0=1.0, rho_amp=0.1, a_amp=0.1)
+        reqs.append((steps, params, init))
+    gaps = rng.exponential(1.0 / rate, size=nreq)
+
+    def run(max_act, arrivals):
+        srv = cs.Server(max_active=max_act, mem_fraction=0.8)
+        t0 = time.perf_counter()
+        ids = []
+        for q, (steps, params, init) in enumerate(reqs):
+            if arrivals:
+                time.sleep(float(gaps[q]))
+            ids.append(srv.submit(steps, params, init))
+        res = [srv.wait(i) for i in ids]
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+        srv.close()
+        return st, wall, sum(r.zone_updates for r in res), all(r.status == 0 for r in res), res
+
+    st, wall, zu, ok, res = run(max_active, True)
+    st1, wall1, zu1, ok1, _ = run(1, False)
+    return {"requests": nreq, "arrival_rate_per_s": rate, "max_active": max_active, "all_ok": ok and ok1,
+            "p50_latency_s": st["p50_s"], "p99_latency_s": st["p99_s"],
+            "mean_queue_s": float(np.mean([r.queue_s for r in res])),
+            "zone_updates_per_s": zu / wall, "sequential_zone_updates_per_s": zu1 / wall1,
+            "sizes": "N in {32,48}, nr in {1,8,16}, 10-30 steps, FP64 (IMEX-RK2 shells, SSP-RK3 surfaces); "
+                     "wall clock includes host mesh builds"}
 
 
 def run_reference(args):
@@ -307,6 +359,11 @@ def run_gpu(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(min(6, os.cpu_count() or 1), steps=1)
+    s.close()
+    serving = None
+    if not args.no_serving:
+        torch.cuda.synchronize()
+        serving = serving_sample()
 
     if args.profile_json and rank == 0:
         Path(args.profile_json).write_text(_json.dumps(
@@ -326,7 +383,7 @@ def run_gpu(args):
         "roofline": roof, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches,
         "top_kernels": {k: round(v[0] / args.steps, 3) for k, v in
                         sorted(prof.items(), key=lambda kv: -kv[1][0])[:8]},
-        "finite": finite, "dt_last": dt,
+        "finite": finite, "dt_last": dt, "serving": serving,
     }
     if rank == 0:
         print(json.dumps(out), flush=True)

@@ -47,7 +47,8 @@ EXPORTS = [
     "cs_limit_all_slopes_p12", "cs_make_facial_fluxes", "cs_make_edge_efields_p1",
     "cs_build_non_stiff_sources", "cs_update_imex_rk_step_p1", "cs_cleanup_after_update",
     "cs_debug_get", "cs_diag", "cs_get_stream", "cs_launch_count", "cs_profile_begin", "cs_profile_end",
-    "cs_cfl_timestep_noalloc",
+    "cs_cfl_timestep_noalloc", "cs_estimate_device_bytes", "cs_serve_create", "cs_serve_submit",
+    "cs_serve_wait", "cs_serve_state", "cs_serve_stats", "cs_serve_destroy",
 ]
 
 
@@ -103,6 +104,18 @@ def make_init(**kw) -> CsInitDesc:
     return r
 
 
+class CsRequest(ctypes.Structure):
+    _fields_ = [("params", CsParams), ("init", CsInitDesc), ("steps", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
+class CsServeResult(ctypes.Structure):
+    _fields_ = [
+        ("status", ctypes.c_int32), ("reserved", ctypes.c_int32), ("latency_s", ctypes.c_double),
+        ("queue_s", ctypes.c_double), ("mass", ctypes.c_double), ("energy", ctypes.c_double),
+        ("max_divb", ctypes.c_double), ("dt_last", ctypes.c_double), ("zone_updates", ctypes.c_int64),
+    ]
+
+
 _lib = None
 
 
@@ -145,6 +158,13 @@ def load_library() -> ctypes.CDLL:
         "cs_profile_begin": ([P], ctypes.c_int),
         "cs_profile_end": ([P, I, ctypes.c_char_p, dp, ctypes.POINTER(ctypes.c_int64), ip], ctypes.c_int),
         "cs_cfl_timestep_noalloc": ([P, P, P, P, I, I, I, D, D, D, D, D, P, dp], ctypes.c_int),
+        "cs_estimate_device_bytes": ([ctypes.POINTER(CsParams)], ctypes.c_size_t),
+        "cs_serve_create": ([I, D, I, ctypes.POINTER(P)], ctypes.c_int),
+        "cs_serve_submit": ([P, ctypes.POINTER(CsRequest), ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
+        "cs_serve_wait": ([P, ctypes.c_int64, ctypes.POINTER(CsServeResult)], ctypes.c_int),
+        "cs_serve_state": ([P, ctypes.c_int64, dp, dp, dp, dp, dp], ctypes.c_int),
+        "cs_serve_stats": ([P, dp, dp, dp, ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
+        "cs_serve_destroy": ([P], ctypes.c_int),
     }
     for name in ("cs_fill_ghosts", "cs_limit_all_slopes_p12", "cs_make_facial_fluxes", "cs_make_edge_efields_p1",
                  "cs_build_non_stiff_sources", "cs_cleanup_after_update"):
@@ -360,3 +380,64 @@ def geometry_single_zone(isector: int, ntp_global: int, nr_global: int, iscale: 
     if rc:
         raise CsError(f"cs_geometry_single_zone failed ({rc})")
     return out
+
+
+class Server:
+    """Serving loop over the C ABI: requests (solves of any size) are admitted
+    while device memory allows and run concurrently, each in its own context
+    and stream; ``stats`` reports p50 / p99 latency and throughput."""
+
+    def __init__(self, max_active: int = 4, mem_fraction: float = 0.8, keep_state: bool = False):
+        self.lib = load_library()
+        h = ctypes.c_void_p()
+        rc = self.lib.cs_serve_create(max_active, mem_fraction, int(keep_state), ctypes.byref(h))
+        if rc:
+            raise CsError(f"cs_serve_create failed ({rc})")
+        self.h = h
+
+    def submit(self, steps: int, params, init) -> int:
+        r = CsRequest()
+        r.params = params if isinstance(params, CsParams) else make_params(**params)
+        r.init = init if isinstance(init, CsInitDesc) else make_init(**init)
+        r.steps = steps
+        rid = ctypes.c_int64()
+        rc = self.lib.cs_serve_submit(self.h, ctypes.byref(r), ctypes.byref(rid))
+        if rc:
+            raise CsError(f"cs_serve_submit failed ({rc})")
+        return rid.value
+
+    def wait(self, rid: int) -> CsServeResult:
+        out = CsServeResult()
+        self.lib.cs_serve_wait(self.h, rid, ctypes.byref(out))
+        return out
+
+    def state(self, rid: int, params: CsParams) -> dict:
+        ni = params.ntp + 2 * params.nghost + 1
+        nk = params.nr + 2 * params.nghost + 1
+        st = {k: np.zeros(((8 if k == "U" else 1), 6, nk, ni, ni)) for k in STATE_KEYS}
+        rc = self.lib.cs_serve_state(self.h, rid, *[_dptr(st[k]) for k in STATE_KEYS])
+        if rc:
+            raise CsError(f"cs_serve_state failed ({rc})")
+        return st
+
+    def stats(self) -> dict:
+        p50, p99, zu = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        n = ctypes.c_int64()
+        self.lib.cs_serve_stats(self.h, ctypes.byref(p50), ctypes.byref(p99), ctypes.byref(zu), ctypes.byref(n))
+        return {"p50_s": p50.value, "p99_s": p99.value, "zone_updates_per_s": zu.value, "completed": n.value}
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.cs_serve_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def estimate_device_bytes(**params) -> int:
+    p = make_params(**params)
+    return int(load_library().cs_estimate_device_bytes(ctypes.byref(p)))

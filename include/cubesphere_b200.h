@@ -231,6 +231,40 @@ int cs_cfl_timestep_noalloc(const double* U, const double* ent, const double* v_
                             double gamma, double rhofloor, double prsfloor, double cfl_coef,
                             double dtcur, void* stream, double* dtcurp1);
 
+/* Serving (no counterpart in the reference, whose driver runs one solve per
+ * job).  A server admits solve requests as they arrive while device memory
+ * allows (mem_fraction of the free memory at creation, counted with
+ * cs_estimate_device_bytes) and runs at most max_active at once, each in its
+ * own context and stream driven by its own host thread, so requests that
+ * arrive while others run overlap with them on the device.  A request runs
+ * cs_mesh_build, cs_init_problem, steps x cs_step and cs_diag; its result
+ * does not depend on what else runs (every kernel is deterministic).
+ * Latency is measured from submission to completion. */
+typedef struct cs_server cs_server;
+typedef struct cs_request {
+  cs_params params;
+  cs_init_desc init;
+  int32_t steps;
+  int32_t reserved;
+} cs_request;
+typedef struct cs_serve_result {
+  int32_t status;       /* cs_status of the request */
+  int32_t reserved;
+  double latency_s;     /* submission to completion */
+  double queue_s;       /* submission to admission */
+  double mass, energy, max_divb;  /* cs_diag of the final state */
+  double dt_last;       /* the next time step after the last step */
+  int64_t zone_updates; /* interior zones x steps */
+} cs_serve_result;
+size_t cs_estimate_device_bytes(const cs_params* p);
+int cs_serve_create(int32_t max_active, double mem_fraction, int32_t keep_state, cs_server** out);
+int cs_serve_submit(cs_server* sv, const cs_request* req, int64_t* id);
+int cs_serve_wait(cs_server* sv, int64_t id, cs_serve_result* out);   /* blocks; returns the request's status */
+int cs_serve_state(cs_server* sv, int64_t id, double* U, double* ent,
+                   double* bxf, double* byf, double* bzf);           /* final state, when keep_state */
+int cs_serve_stats(cs_server* sv, double* p50_s, double* p99_s, double* zone_updates_per_s, int64_t* completed);
+int cs_serve_destroy(cs_server* sv);                                   /* waits for every request */
+
 /* Diagnostics: sums over interior zones of 6 panels of volume-weighted
  * mass, energy and the max |div B| (face-area-weighted, per volume). */
 int cs_diag(cs_ctx* ctx, double* mass, double* energy, double* max_divb);

@@ -13,7 +13,7 @@ HEADER = Path(__file__).resolve().parent.parent / "include" / "cubesphere_b200.h
 
 def declared():
     text = HEADER.read_text()
-    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(cs_\w+)\s*\(", text, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|size_t|const char\*)\s+(cs_\w+)\s*\(", text, re.M)))
 
 
 def test_header_declares_what_the_binding_lists():
