@@ -27,19 +27,32 @@ namespace {
 struct Harm {
   std::vector<int> a, b, c;
   std::vector<double> w;
+  int deg = 0;
   double scale = 1.0;
+  // powers x^0 .. x^deg by repeated multiplication
+  static void powers(double x, int deg, double* p) {
+    p[0] = 1.0;
+    for (int e = 1; e <= deg; ++e) p[e] = p[e - 1] * x;
+  }
   double value(double u, double v, double t) const {
+    double pu[16], pv[16], pt[16];
+    powers(u, deg, pu);
+    powers(v, deg, pv);
+    powers(t, deg, pt);
     double s = 0.0;
-    for (size_t n = 0; n < w.size(); ++n) s += w[n] * std::pow(u, a[n]) * std::pow(v, b[n]) * std::pow(t, c[n]);
+    for (size_t n = 0; n < w.size(); ++n) s += w[n] * pu[a[n]] * pv[b[n]] * pt[c[n]];
     return s * scale;
   }
   void grad(double u, double v, double t, double g[3]) const {
+    double pu[16], pv[16], pt[16];
+    powers(u, deg, pu);
+    powers(v, deg, pv);
+    powers(t, deg, pt);
     g[0] = g[1] = g[2] = 0.0;
     for (size_t n = 0; n < w.size(); ++n) {
-      double pu = std::pow(u, a[n]), pv = std::pow(v, b[n]), pt = std::pow(t, c[n]);
-      if (a[n] > 0) g[0] += w[n] * a[n] * std::pow(u, a[n] - 1) * pv * pt;
-      if (b[n] > 0) g[1] += w[n] * b[n] * pu * std::pow(v, b[n] - 1) * pt;
-      if (c[n] > 0) g[2] += w[n] * c[n] * pu * pv * std::pow(t, c[n] - 1);
+      if (a[n] > 0) g[0] += w[n] * a[n] * pu[a[n] - 1] * pv[b[n]] * pt[c[n]];
+      if (b[n] > 0) g[1] += w[n] * b[n] * pu[a[n]] * pv[b[n] - 1] * pt[c[n]];
+      if (c[n] > 0) g[2] += w[n] * c[n] * pu[a[n]] * pv[b[n]] * pt[c[n] - 1];
     }
     for (int q = 0; q < 3; ++q) g[q] *= scale;
   }
@@ -59,6 +72,7 @@ struct Normal {
 
 Harm make_harm(Normal& rnd, int lmax) {
   Harm h;
+  h.deg = lmax;
   for (int d = 1; d <= lmax; ++d)
     for (int a = d; a >= 0; --a)
       for (int b = d - a; b >= 0; --b) {
@@ -160,6 +174,7 @@ std::string init_problem_host(const cs_params& p, const cs_init_desc& d, const G
   pr.gm = p.gm;
   pr.ob8pi = 1.0 / (8.0 * (4.0 * std::atan(1.0)));
   int lmax = d.lmax > 0 ? d.lmax : 4;
+  if (lmax > 15) return "init lmax must be <= 15";
   pr.Y = make_harm(rnd, lmax);
   pr.Psi = make_harm(rnd, lmax);
   for (size_t t = 0; t < 8 * NPANEL * S; ++t) U[t] = 0.0;
