@@ -60,6 +60,12 @@ ALGO_WORDS_PER_UNIT = {
     "k_faceB": 80 + 1 + 20 + 5,
 }
 
+# DRAM bytes per unit (read + write) measured by ncu on the shell32 case
+# (profiles/top_kernels_shell32.md: 2.102 GB over 190,608 zones of the ADP
+# range in one launch); the full shell128 launch is too large to capture, so
+# roofline.traffic scales this by the units of a full launch.
+MEASURED_TRAFFIC_PER_UNIT = {"k_adp_solve": 2.102122e9 / 190608}
+
 WORKLOAD_DOC = {
     "shell128": "FP64 ideal-MHD hydrostatic shell, 6x128^2x64 zones, r 1..2 stretch 1.02, 4 ghosts, IMEX-RK2, "
                 "P12 WENO-AO/MRWENO + ADP, HLL fluxes, LLF multi-D EMFs, CT",
@@ -351,8 +357,11 @@ def run_gpu(args):
         if dname == "k_faceB":
             per_launch /= 3.0  # one launch per face direction
         achieved = per_launch / (dms / dcount / 1e3) / 1e9
+        tr = MEASURED_TRAFFIC_PER_UNIT.get(dname)
         roof = {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                "frac": achieved / hbm_peak, "traffic": None, "peak_source": peak_note,
+                "frac": achieved / hbm_peak, "traffic": (tr * units if tr else None),
+                "traffic_source": "ncu dram bytes on shell32, scaled by units" if tr else None,
+                "peak_source": peak_note,
                 "algorithmic_bytes_per_launch": per_launch, "avg_launch_ms": dms / dcount,
                 "share_of_step": dms / sum(v[0] for v in prof.values())}
 
