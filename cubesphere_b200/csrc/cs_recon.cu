@@ -376,6 +376,7 @@ __device__ __forceinline__ void w7b_minv(const Dims& d, const PhysC& ph, const D
 // with the linear WENO slopes (MRWENO weights, flattener damping).  With
 // kCached the inverse normal matrix (geometry only) comes from the
 // operator cache built at mesh build; the result is the same either way.
+constexpr int W7B_QG = NVAR;
 template <bool kCached>
 __global__ void __launch_bounds__(TPB) k_weno7b(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
   const double ob12 = 1.0 / 12.0, ob180 = 1.0 / 180.0, ob144 = 1.0 / 144.0;
@@ -396,62 +397,70 @@ __global__ void __launch_bounds__(TPB) k_weno7b(Dims d, PhysC ph, DGeom g, DStat
     if (!kCached) w7b_minv(d, ph, g, p, i, j, k, n, cx, cy, cz, l0, obl0, c0, Minv);
     const double* mc = s.op_m9 + t;
     auto MI = [&](int e) { return kCached ? __ldg(mc + (long long)e * nr_) : Minv[kCached ? 0 : e]; };
-    double v0[NVAR];
-#pragma unroll
-    for (int q = 0; q < NVAR; ++q) v0[q] = s.V[((long long)q * NPANEL + p) * d.S + d.idx(i, j, k)];
-    double Y[NVAR][9];
-#pragma unroll
-    for (int q = 0; q < NVAR; ++q)
-#pragma unroll
-      for (int a = 0; a < 9; ++a) Y[q][a] = 0.0;
-#pragma unroll 1
-    for (int rr = 0; rr < 18; ++rr) {
-      double A[9];
-      long long off;
-      w7b_row(d, ph, g, p, i, j, k, n, rr, cx, cy, cz, l0, obl0, c0, A, off);
-#pragma unroll
-      for (int q = 0; q < NVAR; ++q) {
-        const double R = s.V[((long long)q * NPANEL + p) * d.S + off] - v0[q];
-#pragma unroll
-        for (int a = 0; a < 9; ++a) Y[q][a] = Y[q][a] + A[a] * R;
-      }
-    }
     const double f = s.flatA[d.at(0, p, i, j, k)];
     const double betalo = f + (1.0 - f) * 2.0;
     const double ghi = f * 0.6 + (1.0 - f) * 0.95, glo = 1.0 - ghi, obghi = 1.0 / ghi, grat = glo / ghi;
+    // The primitives go in groups of W7B_QG, each group rebuilding the
+    // matrix rows; on B200 one group of all eight is faster than smaller
+    // groups (the row rebuild costs more than the extra live sums).  Every
+    // component's sums run over the rows in the same order either way.
 #pragma unroll 1
-    for (int q = 0; q < NVAR; ++q) {
-      double X[9];
+    for (int q0 = 0; q0 < NVAR; q0 += W7B_QG) {
+      double v0[W7B_QG];
 #pragma unroll
-      for (int a = 0; a < 9; ++a) {
-        double sacc = 0.0;
+      for (int qq = 0; qq < W7B_QG; ++qq) v0[qq] = s.V[((long long)(q0 + qq) * NPANEL + p) * d.S + d.idx(i, j, k)];
+      double Y[W7B_QG][9];
 #pragma unroll
-        for (int b = 0; b < 9; ++b) sacc = sacc + MI(a * 9 + b) * Y[q][b];
-        X[a] = sacc;
+      for (int qq = 0; qq < W7B_QG; ++qq)
+#pragma unroll
+        for (int a = 0; a < 9; ++a) Y[qq][a] = 0.0;
+#pragma unroll 1
+      for (int rr = 0; rr < 18; ++rr) {
+        double A[9];
+        long long off;
+        w7b_row(d, ph, g, p, i, j, k, n, rr, cx, cy, cz, l0, obl0, c0, A, off);
+#pragma unroll
+        for (int qq = 0; qq < W7B_QG; ++qq) {
+          const double R = s.V[((long long)(q0 + qq) * NPANEL + p) * d.S + off] - v0[qq];
+#pragma unroll
+          for (int a = 0; a < 9; ++a) Y[qq][a] = Y[qq][a] + A[a] * R;
+        }
       }
-      const double v2 = Vat(s, d, q, 1, p, i, j, k), v3 = Vat(s, d, q, 2, p, i, j, k), v4 = Vat(s, d, q, 3, p, i, j, k);
-      const double ISlo = betalo * (v2 * v2 + v3 * v3 + v4 * v4) * ob12;
-      double Phi[9];
-      Phi[0] = X[0] * obghi - v2 * grat;
-      Phi[1] = X[1] * obghi - v3 * grat;
-      Phi[2] = X[2] * obghi - v4 * grat;
+#pragma unroll 1
+      for (int qq = 0; qq < W7B_QG; ++qq) {
+        const int q = q0 + qq;
+        double X[9];
 #pragma unroll
-      for (int a = 3; a < 9; ++a) Phi[a] = X[a] * obghi;
-      const double IShi = (Phi[0] * Phi[0] + Phi[1] * Phi[1] + Phi[2] * Phi[2]) * ob12 +
-                          (Phi[3] * Phi[3]) * (sqr(c0[4] - ob12) + ob180) + (Phi[4] * Phi[4]) * (sqr(c0[5] - ob12) + ob180) +
-                          (Phi[5] * Phi[5]) * (sqr(c0[6] - ob12) + ob180) + (Phi[6] * Phi[6]) * (c0[7] * c0[7] + ob144) +
-                          (Phi[7] * Phi[7]) * (c0[8] * c0[8] + ob144) + (Phi[8] * Phi[8]) * (c0[9] * c0[9] + ob144);
-      const double tau = fabs(IShi - ISlo);
-      double Wlo = glo * (1.0 + tau / (ISlo + ph.smallnum)), Whi = ghi * (1.0 + tau / (IShi + ph.smallnum));
-      const double aa = 1.0 / (Wlo + Whi);
-      Wlo = Wlo * aa;
-      Whi = Whi * aa;
-      const double x = 1.0 - f;
-      Vat(s, d, q, 1, p, i, j, k) = (Whi * Phi[0] + Wlo * v2) * x;
-      Vat(s, d, q, 2, p, i, j, k) = (Whi * Phi[1] + Wlo * v3) * x;
-      Vat(s, d, q, 3, p, i, j, k) = (Whi * Phi[2] + Wlo * v4) * x;
+        for (int a = 0; a < 9; ++a) {
+          double sacc = 0.0;
 #pragma unroll
-      for (int m = 4; m < 10; ++m) Vat(s, d, q, m, p, i, j, k) = (Whi * Phi[m - 1]) * x;
+          for (int b = 0; b < 9; ++b) sacc = sacc + MI(a * 9 + b) * Y[qq][b];
+          X[a] = sacc;
+        }
+        const double v2 = Vat(s, d, q, 1, p, i, j, k), v3 = Vat(s, d, q, 2, p, i, j, k), v4 = Vat(s, d, q, 3, p, i, j, k);
+        const double ISlo = betalo * (v2 * v2 + v3 * v3 + v4 * v4) * ob12;
+        double Phi[9];
+        Phi[0] = X[0] * obghi - v2 * grat;
+        Phi[1] = X[1] * obghi - v3 * grat;
+        Phi[2] = X[2] * obghi - v4 * grat;
+#pragma unroll
+        for (int a = 3; a < 9; ++a) Phi[a] = X[a] * obghi;
+        const double IShi = (Phi[0] * Phi[0] + Phi[1] * Phi[1] + Phi[2] * Phi[2]) * ob12 +
+                            (Phi[3] * Phi[3]) * (sqr(c0[4] - ob12) + ob180) + (Phi[4] * Phi[4]) * (sqr(c0[5] - ob12) + ob180) +
+                            (Phi[5] * Phi[5]) * (sqr(c0[6] - ob12) + ob180) + (Phi[6] * Phi[6]) * (c0[7] * c0[7] + ob144) +
+                            (Phi[7] * Phi[7]) * (c0[8] * c0[8] + ob144) + (Phi[8] * Phi[8]) * (c0[9] * c0[9] + ob144);
+        const double tau = fabs(IShi - ISlo);
+        double Wlo = glo * (1.0 + tau / (ISlo + ph.smallnum)), Whi = ghi * (1.0 + tau / (IShi + ph.smallnum));
+        const double aa = 1.0 / (Wlo + Whi);
+        Wlo = Wlo * aa;
+        Whi = Whi * aa;
+        const double x = 1.0 - f;
+        Vat(s, d, q, 1, p, i, j, k) = (Whi * Phi[0] + Wlo * v2) * x;
+        Vat(s, d, q, 2, p, i, j, k) = (Whi * Phi[1] + Wlo * v3) * x;
+        Vat(s, d, q, 3, p, i, j, k) = (Whi * Phi[2] + Wlo * v4) * x;
+#pragma unroll
+        for (int m = 4; m < 10; ++m) Vat(s, d, q, m, p, i, j, k) = (Whi * Phi[m - 1]) * x;
+      }
     }
   }
 }
@@ -1197,7 +1206,7 @@ __device__ __forceinline__ void e9c_minv(const Dims& d, const DGeom& g, int p, i
 // nothing else.  kCached: the inverse normal matrix comes from the
 // operator cache.
 template <bool kCached>
-__global__ void __launch_bounds__(TPB) k_efield_c(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
+__global__ void __launch_bounds__(TPB, 4) k_efield_c(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
   const double ob12 = 1.0 / 12.0, ob180 = 1.0 / 180.0, ob144 = 1.0 / 144.0;
   const long long nr_ = r.count();
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nr_; t += (long long)gridDim.x * blockDim.x) {
