@@ -49,6 +49,7 @@ EXPORTS = [
     "cs_debug_get", "cs_diag", "cs_get_stream", "cs_launch_count", "cs_profile_begin", "cs_profile_end",
     "cs_cfl_timestep_noalloc", "cs_estimate_device_bytes", "cs_serve_create", "cs_serve_submit",
     "cs_serve_wait", "cs_serve_state", "cs_serve_stats", "cs_serve_destroy",
+    "cs_snapshot_save", "cs_snapshot_load", "cs_snapshot_write_host", "cs_snapshot_read_host",
 ]
 
 
@@ -165,6 +166,12 @@ def load_library() -> ctypes.CDLL:
         "cs_serve_state": ([P, ctypes.c_int64, dp, dp, dp, dp, dp], ctypes.c_int),
         "cs_serve_stats": ([P, dp, dp, dp, ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
         "cs_serve_destroy": ([P], ctypes.c_int),
+        "cs_snapshot_save": ([P, ctypes.c_char_p, D, D, ctypes.c_int64], ctypes.c_int),
+        "cs_snapshot_load": ([P, ctypes.c_char_p, dp, dp, ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
+        "cs_snapshot_write_host": ([ctypes.c_char_p, ctypes.POINTER(CsParams), dp, dp, dp, dp, dp, D, D,
+                                    ctypes.c_int64], ctypes.c_int),
+        "cs_snapshot_read_host": ([ctypes.c_char_p, ctypes.POINTER(CsParams), dp, dp, dp, dp, dp, dp, dp,
+                                   ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
     }
     for name in ("cs_fill_ghosts", "cs_limit_all_slopes_p12", "cs_make_facial_fluxes", "cs_make_edge_efields_p1",
                  "cs_build_non_stiff_sources", "cs_cleanup_after_update"):
@@ -358,6 +365,16 @@ class Solve:
             out[key] = (float(ms[q]), int(cnt[q]))
         return out
 
+    def snapshot_save(self, path: str, time: float, dtcur: float, step: int) -> None:
+        self._check(self.lib.cs_snapshot_save(self.h, str(path).encode(), time, dtcur, step), "cs_snapshot_save")
+
+    def snapshot_load(self, path: str) -> tuple:
+        """Loads a snapshot into the resident state; returns (time, dtcur, step)."""
+        t, d, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_int64()
+        self._check(self.lib.cs_snapshot_load(self.h, str(path).encode(), ctypes.byref(t), ctypes.byref(d),
+                                              ctypes.byref(n)), "cs_snapshot_load")
+        return t.value, d.value, n.value
+
     def diag(self) -> tuple:
         m, e, d = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         self._check(self.lib.cs_diag(self.h, ctypes.byref(m), ctypes.byref(e), ctypes.byref(d)), "cs_diag")
@@ -441,3 +458,19 @@ class Server:
 def estimate_device_bytes(**params) -> int:
     p = make_params(**params)
     return int(load_library().cs_estimate_device_bytes(ctypes.byref(p)))
+
+
+def snapshot_write_host(path, params: CsParams, st: dict, time: float, dtcur: float, step: int) -> int:
+    """Writes host arrays as a snapshot file (no device); returns the status."""
+    lib = load_library()
+    return lib.cs_snapshot_write_host(str(path).encode(), ctypes.byref(params),
+                                      *[_dptr(np.ascontiguousarray(st[k])) for k in STATE_KEYS], time, dtcur, step)
+
+
+def snapshot_read_host(path, params: CsParams, st: dict):
+    """Reads a snapshot into host arrays; returns (status, time, dtcur, step)."""
+    lib = load_library()
+    t, d, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_int64()
+    rc = lib.cs_snapshot_read_host(str(path).encode(), ctypes.byref(params), *[_dptr(st[k]) for k in STATE_KEYS],
+                                   ctypes.byref(t), ctypes.byref(d), ctypes.byref(n))
+    return rc, t.value, d.value, n.value

@@ -935,6 +935,33 @@ int cs_debug_get(cs_ctx* ctx, int32_t which, double* host_out, size_t n) {
   return CS_OK;
 }
 
+int cs_snapshot_save(cs_ctx* ctx, const char* path, double time, double dtcur, int64_t step) {
+  if (!ctx || !path) return CS_ERR_ARG;
+  Solve& sv = ctx->sv;
+  if (int rc = cs::need(sv, true)) return rc;
+  const size_t S6 = (size_t)6 * sv.d.S;
+  std::vector<double> U(cs::NVAR * S6), ent(S6), bx(S6), by(S6), bz(S6);
+  if (int rc = cs_state_get(ctx, U.data(), ent.data(), bx.data(), by.data(), bz.data())) return rc;
+  const int rc = cs_snapshot_write_host(path, &sv.p, U.data(), ent.data(), bx.data(), by.data(), bz.data(), time,
+                                        dtcur, step);
+  if (rc) return cs::fail(sv, rc, std::string("cannot write snapshot ") + path);
+  return CS_OK;
+}
+
+int cs_snapshot_load(cs_ctx* ctx, const char* path, double* time, double* dtcur, int64_t* step) {
+  if (!ctx || !path || !time || !dtcur || !step) return CS_ERR_ARG;
+  Solve& sv = ctx->sv;
+  if (int rc = cs::need(sv, false)) return rc;
+  const size_t S6 = (size_t)6 * sv.d.S;
+  std::vector<double> U(cs::NVAR * S6), ent(S6), bx(S6), by(S6), bz(S6);
+  const int rc = cs_snapshot_read_host(path, &sv.p, U.data(), ent.data(), bx.data(), by.data(), bz.data(), time,
+                                       dtcur, step);
+  if (rc == CS_ERR_STATE) return cs::fail(sv, rc, "snapshot belongs to another mesh or physics");
+  if (rc == CS_ERR_NUMERIC) return cs::fail(sv, rc, "snapshot payload does not match its hash");
+  if (rc) return cs::fail(sv, rc, std::string("cannot read snapshot ") + path);
+  return cs_state_put(ctx, U.data(), ent.data(), bx.data(), by.data(), bz.data());
+}
+
 int cs_diag(cs_ctx* ctx, double* mass, double* energy, double* max_divb) {
   if (!ctx || !mass || !energy || !max_divb) return CS_ERR_ARG;
   Solve& sv = ctx->sv;

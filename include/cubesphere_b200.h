@@ -231,6 +231,24 @@ int cs_cfl_timestep_noalloc(const double* U, const double* ent, const double* v_
                             double gamma, double rhofloor, double prsfloor, double cfl_coef,
                             double dtcur, void* stream, double* dtcurp1);
 
+/* Snapshots (checkpoint / resume): the reference's riemann.in (time, dtcur;
+ * 1000riemann_geomesh_cs_mhd.f:1798-1804, read under RESTART at :1527-1666)
+ * plus its WRITEDATA / READDATA state files, as one binary file: magic
+ * "CSB2SNP1", a uint32 length, a JSON header (parameters, time, dtcur, step,
+ * array list, FNV-1a 64-bit hash of the payload) and the FP64 arrays U (8),
+ * entropy, Bxf, Byf, Bzf in the panel-box layout.  Loading returns
+ * CS_ERR_STATE when the file belongs to other mesh / physics parameters and
+ * CS_ERR_NUMERIC when the payload does not match its hash; a loaded state
+ * continues bit for bit.  The _host forms work on host arrays, no device. */
+int cs_snapshot_save(cs_ctx* ctx, const char* path, double time, double dtcur, int64_t step);
+int cs_snapshot_load(cs_ctx* ctx, const char* path, double* time, double* dtcur, int64_t* step);
+int cs_snapshot_write_host(const char* path, const cs_params* p, const double* U, const double* ent,
+                           const double* bxf, const double* byf, const double* bzf,
+                           double time, double dtcur, int64_t step);
+int cs_snapshot_read_host(const char* path, const cs_params* p, double* U, double* ent,
+                          double* bxf, double* byf, double* bzf,
+                          double* time, double* dtcur, int64_t* step);
+
 /* Serving (no counterpart in the reference, whose driver runs one solve per
  * job).  A server admits solve requests as they arrive while device memory
  * allows (mem_fraction of the free memory at creation, counted with
