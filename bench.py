@@ -83,6 +83,7 @@ def parse():
     ap.add_argument("--workload", default="shell128")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-form sample")
+    ap.add_argument("--no-precision", action="store_true", help="skip the FP32 precision-form sample")
     ap.add_argument("--profile-json", default="", help="also write the per-kernel device times here")
     return ap.parse_args()
 
@@ -219,6 +220,63 @@ def serving_sample(seed: int = 7, nreq: int = 16, rate: float = 4.0, max_active:
                      "wall clock includes host mesh builds"}
 
 
+def precision_sample(pr, dts, steps, ref_state, zones, world, allmax) -> dict:
+    """The precision form (CS_FLAG_FP32) on the same workload: the same
+    initial state and time steps as the FP64 run, the last `steps` of them
+    timed with CUDA events; relative L1 errors of the final state against
+    the FP64 run's (interior zones; faces for B) and its max |div B|."""
+    import numpy as np
+    import torch
+
+    import cubesphere_b200 as cs
+
+    f = cs.Solve(**pr["params"], flags=cs.CS_FLAG_FP32)
+    f.mesh_build()
+    f.init_problem(**pr["init"])
+    stream = torch.cuda.ExternalStream(f.stream_ptr())
+    f.evaluate_timestep(1e30)
+    w = len(dts) - steps
+    for n in range(w):
+        f.step(dts[n])
+    f.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for n in range(w, len(dts)):
+        f.step(dts[n])
+    e1.record(stream)
+    e1.synchronize()
+    ms = allmax(e0.elapsed_time(e1))
+    got = f.get_state()
+    _, _, divb = f.diag()
+    G, N, nr = f.G, f.N, f.nr
+    I = f.interior
+
+    def l1(a, b):
+        return float(np.abs(a - b).sum() / max(np.abs(b).sum(), 1e-300))
+
+    def fc(a, d):
+        lo = [1, 1, 1]
+        lo[d] = 0
+        return a[..., G + lo[2]:G + nr + 1, G + lo[1]:G + N + 1, G + lo[0]:G + N + 1]
+
+    def linf(a, b):
+        return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+    fields = {"rho": (I(got["U"][0]), I(ref_state["U"][0])), "momentum": (I(got["U"][1:4]), I(ref_state["U"][1:4])),
+              "energy": (I(got["U"][4]), I(ref_state["U"][4])), "entropy": (I(got["ent"]), I(ref_state["ent"])),
+              "face_B": (np.concatenate([fc(got[k], d).ravel() for d, k in enumerate(("bxf", "byf", "bzf"))]),
+                         np.concatenate([fc(ref_state[k], d).ravel() for d, k in enumerate(("bxf", "byf", "bzf"))]))}
+    err = {k: l1(*v) for k, v in fields.items()}
+    err_inf = {k: linf(*v) for k, v in fields.items()}
+    bmax = float(np.abs(fc(got["bxf"], 0)).max())
+    f.close()
+    return {"value": zones * steps * world / (ms / 1e3), "unit": "zone-updates/s", "ms_per_step": ms / steps,
+            "dtype": "f32 state/reconstruction/fluxes, f64 face B/EMFs/geometry/operators",
+            "steps_compared": len(dts), "l1_rel_err_vs_f64": err, "linf_rel_err_vs_f64": err_inf,
+            "max_divb_over_bmax": float(divb) / bmax}
+
+
 def run_reference(args):
     world, rank, local = dist_setup()
     if rank != 0:
@@ -278,7 +336,9 @@ def run_gpu(args):
     zones = 6 * s.N * s.N * s.nr
     stream = torch.cuda.ExternalStream(s.stream_ptr())
     dt = s.evaluate_timestep(1e30)
+    dts = []  # the time step of every step from the initial state
     for _ in range(max(args.warmup, 3)):
+        dts.append(dt)
         dt = s.step(dt)
 
     # ---- device-resident timing
@@ -293,6 +353,7 @@ def run_gpu(args):
     clocks.start()
     e0.record(stream)
     for _ in range(args.steps):
+        dts.append(dt)
         dt = s.step(dt)
     e1.record(stream)
     e1.synchronize()
@@ -309,6 +370,7 @@ def run_gpu(args):
         nc = 8 if k == "U" else 1
         host[k] = torch.empty(s.shape(nc), dtype=torch.float64, pin_memory=True).numpy()
     s.get_state(host)
+    ref_state = {k: v.copy() for k, v in host.items()} if not args.no_precision else None
     h2d = sum(a.nbytes for a in host.values())
     d2h = h2d
     barrier()
@@ -369,6 +431,10 @@ def run_gpu(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(min(6, os.cpu_count() or 1), steps=1)
     s.close()
+    precision = None
+    if ref_state is not None:
+        torch.cuda.synchronize()
+        precision = precision_sample(pr, dts, args.steps, ref_state, zones, world, allmax)
     serving = None
     if not args.no_serving:
         torch.cuda.synchronize()
@@ -392,7 +458,7 @@ def run_gpu(args):
         "roofline": roof, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches,
         "top_kernels": {k: round(v[0] / args.steps, 3) for k, v in
                         sorted(prof.items(), key=lambda kv: -kv[1][0])[:8]},
-        "finite": finite, "dt_last": dt, "serving": serving,
+        "finite": finite, "dt_last": dt, "precision_form": precision, "serving": serving,
     }
     if rank == 0:
         print(json.dumps(out), flush=True)

@@ -383,45 +383,24 @@ int ensure_host_mesh(Solve& sv) {
   return CS_OK;
 }
 
-int upload_mesh(Solve& sv) {
-  const Box& b = sv.host.box;
-  Dims& d = sv.d;
-  d.N = b.N; d.nr = b.nr; d.G = b.G; d.NI = b.NI; d.NJ = b.NJ; d.NK = b.NK;
-  d.S = (long long)b.size();
-  CS_CUDA(sv, cudaGetDevice(&sv.device));
-  CS_CUDA(sv, cudaDeviceGetAttribute(&sv.sm_count, cudaDevAttrMultiProcessorCount, sv.device));
-  CS_CUDA(sv, cudaStreamCreateWithFlags(&sv.stream, cudaStreamNonBlocking));
-  cudaError_t e = cudaSuccess;
+// State and work arrays of the form R (double: the plain form; float: the
+// precision form, whose face B, EMFs and operators stay FP64).
+template <typename R>
+int alloc_state(Solve& sv, DStateT<R>& s) {
+  const Dims& d = sv.d;
   const size_t S6 = (size_t)6 * d.S;
-  for (int f = 0; f < CS_G_NFIELDS; ++f) {
-    const size_t bytes = sv.host.f[f].size() * sizeof(double);
-    double* p = (double*)dalloc(sv, bytes, e);
-    if (!p) return cuda_fail(sv, e, "cudaMalloc(geometry)");
-    CS_CUDA(sv, cudaMemcpyAsync(p, sv.host.f[f].data(), bytes, cudaMemcpyHostToDevice, sv.stream));
-    sv.g.f[f] = p;
-  }
-  int32_t* m = (int32_t*)dalloc(sv, sv.host.mask.size() * sizeof(int32_t), e);
-  if (!m) return cuda_fail(sv, e, "cudaMalloc(mask)");
-  CS_CUDA(sv, cudaMemcpyAsync(m, sv.host.mask.data(), sv.host.mask.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
-                              sv.stream));
-  sv.g.mask = m;
-  int32_t* st = (int32_t*)dalloc(sv, sv.host.stencil.size() * sizeof(int32_t), e);
-  if (!st) return cuda_fail(sv, e, "cudaMalloc(stencil)");
-  CS_CUDA(sv, cudaMemcpyAsync(st, sv.host.stencil.data(), sv.host.stencil.size() * sizeof(int32_t),
-                              cudaMemcpyHostToDevice, sv.stream));
-  sv.g.st = st;
-  // State and work arrays.
-  auto A = [&](int ncomp) -> double* { return (double*)dalloc(sv, (size_t)ncomp * S6 * sizeof(double), e); };
-  DState& s = sv.st;
-  s.U = A(NVAR); s.ent = A(4); s.Bxf = A(1); s.Byf = A(1); s.Bzf = A(1);
+  cudaError_t e = cudaSuccess;
+  auto A = [&](int ncomp) -> R* { return (R*)dalloc(sv, (size_t)ncomp * S6 * sizeof(R), e); };
+  auto D = [&](int ncomp) -> double* { return (double*)dalloc(sv, (size_t)ncomp * S6 * sizeof(double), e); };
+  s.U = A(NVAR); s.ent = A(4); s.Bxf = D(1); s.Byf = D(1); s.Bzf = D(1);
   s.V = A(NVAR * NMODE); s.E = A(3 * NMODE); s.Esnap = A(3);
   s.msonic = A(1); s.flatA = A(1); s.flatB = A(1);
-  for (int q = 0; q < 3; ++q) { s.Bq[q] = A(NQ); s.fcon[q] = A(2 * NVAR); s.EF[q] = A(1); s.Ef[q] = A(1); s.B0[q] = A(1); }
+  for (int q = 0; q < 3; ++q) { s.Bq[q] = D(NQ); s.fcon[q] = A(2 * NVAR); s.EF[q] = A(1); s.Ef[q] = D(1); s.B0[q] = D(1); }
   for (int q = 0; q < 6; ++q) s.S[q] = A(1);
   s.dUdt = A(NVAR); s.U0 = A(NVAR); s.ent0 = A(1);
   if (sv.p.rk_scheme == CS_IMEX_RK2) {
     s.K1 = A(NVAR);
-    for (int q = 0; q < 3; ++q) { s.EF1[q] = A(1); s.Ef1[q] = A(1); }
+    for (int q = 0; q < 3; ++q) { s.EF1[q] = A(1); s.Ef1[q] = D(1); }
     if (!s.K1 || !s.EF1[2] || !s.Ef1[2]) return cuda_fail(sv, e, "cudaMalloc(IMEX stage rates)");
   }
   s.FS = A(6 * NQ * (NVAR + 1));
@@ -466,6 +445,39 @@ int upload_mesh(Solve& sv) {
   if (e != cudaSuccess || !s.U || !s.V || !s.E || !s.dtmin) return cuda_fail(sv, e, "cudaMalloc(state)");
   for (int q = 0; q < 3; ++q)
     if (!s.Bq[q] || !s.fcon[q] || !s.EF[q] || !s.Ef[q] || !s.B0[q]) return fail(sv, CS_ERR_NOMEM, "cudaMalloc(work)");
+  return CS_OK;
+}
+
+int upload_mesh(Solve& sv) {
+  const Box& b = sv.host.box;
+  Dims& d = sv.d;
+  d.N = b.N; d.nr = b.nr; d.G = b.G; d.NI = b.NI; d.NJ = b.NJ; d.NK = b.NK;
+  d.S = (long long)b.size();
+  CS_CUDA(sv, cudaGetDevice(&sv.device));
+  CS_CUDA(sv, cudaDeviceGetAttribute(&sv.sm_count, cudaDevAttrMultiProcessorCount, sv.device));
+  CS_CUDA(sv, cudaStreamCreateWithFlags(&sv.stream, cudaStreamNonBlocking));
+  cudaError_t e = cudaSuccess;
+  const size_t S6 = (size_t)6 * d.S;
+  for (int f = 0; f < CS_G_NFIELDS; ++f) {
+    const size_t bytes = sv.host.f[f].size() * sizeof(double);
+    double* p = (double*)dalloc(sv, bytes, e);
+    if (!p) return cuda_fail(sv, e, "cudaMalloc(geometry)");
+    CS_CUDA(sv, cudaMemcpyAsync(p, sv.host.f[f].data(), bytes, cudaMemcpyHostToDevice, sv.stream));
+    sv.g.f[f] = p;
+  }
+  int32_t* m = (int32_t*)dalloc(sv, sv.host.mask.size() * sizeof(int32_t), e);
+  if (!m) return cuda_fail(sv, e, "cudaMalloc(mask)");
+  CS_CUDA(sv, cudaMemcpyAsync(m, sv.host.mask.data(), sv.host.mask.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                              sv.stream));
+  sv.g.mask = m;
+  int32_t* st = (int32_t*)dalloc(sv, sv.host.stencil.size() * sizeof(int32_t), e);
+  if (!st) return cuda_fail(sv, e, "cudaMalloc(stencil)");
+  CS_CUDA(sv, cudaMemcpyAsync(st, sv.host.stencil.data(), sv.host.stencil.size() * sizeof(int32_t),
+                              cudaMemcpyHostToDevice, sv.stream));
+  sv.g.st = st;
+  // State and work arrays.
+  sv.fp32 = (sv.p.flags & CS_FLAG_FP32) != 0;
+  if (int rc = sv.fp32 ? alloc_state(sv, sv.stF) : alloc_state(sv, sv.st)) return rc;
   // Ghost-exchange map.
   std::vector<MapEntry> map;
   std::string why = build_fill_map(sv, map);
@@ -518,7 +530,7 @@ int upload_mesh(Solve& sv) {
     CS_CUDA(sv, cudaStreamSynchronize(sv.stream));
   }
   launch_ops_build(sv);
-  if (s.adp_lu) launch_adp_factor(sv);
+  if (sv.fp32 ? sv.stF.adp_lu != nullptr : sv.st.adp_lu != nullptr) launch_adp_factor(sv);
   CS_CUDA(sv, cudaGetLastError());
   CS_CUDA(sv, cudaStreamSynchronize(sv.stream));
   return CS_OK;
@@ -545,6 +557,18 @@ void limit_all(Solve& sv) {
   launch_efield(sv);
 }
 
+// The state with the first stage's rates in place of the current ones.
+template <typename R>
+DStateT<R> first_stage_rates(const DStateT<R>& st) {
+  DStateT<R> s1 = st;
+  s1.dUdt = st.K1;
+  for (int q = 0; q < 3; ++q) {
+    s1.EF[q] = st.EF1[q];
+    s1.Ef[q] = st.Ef1[q];
+  }
+  return s1;
+}
+
 // IMEX-RK2: ARS(2,2,2) (Ascher, Ruuth & Spiteri 1997) with the fluxes, the
 // entropy transport and CT explicit and the point-mass gravity implicit,
 // gamma = 1 - 1/sqrt(2), delta = 1 - 1/(2 gamma):
@@ -566,13 +590,10 @@ int run_stage_imex(Solve& sv, int irk, double dtcur) {
   } else {
     launch_add_gravity(sv, (1.0 - gam) / (1.0 - del));
     launch_restore_stage0(sv);
-    DState s1 = sv.st;
-    s1.dUdt = sv.st.K1;
-    for (int q = 0; q < 3; ++q) {
-      s1.EF[q] = sv.st.EF1[q];
-      s1.Ef[q] = sv.st.Ef1[q];
-    }
-    launch_update_with(sv, s1, del * dtcur);
+    if (sv.fp32)
+      launch_update_with(sv, first_stage_rates(sv.stF), del * dtcur);
+    else
+      launch_update_with(sv, first_stage_rates(sv.st), del * dtcur);
     launch_update(sv, (1.0 - del) * dtcur);
   }
   launch_gravity_implicit(sv, gam * dtcur);
@@ -609,13 +630,51 @@ int run_stage(Solve& sv, int irk, double dtcur) {
 int read_dt(Solve& sv, double* out) {
   unsigned long long bits = 0;
   int flag = 0;
-  CS_CUDA(sv, cudaMemcpyAsync(&bits, sv.st.dtmin, sizeof(bits), cudaMemcpyDeviceToHost, sv.stream));
-  CS_CUDA(sv, cudaMemcpyAsync(&flag, sv.st.err_flag, sizeof(flag), cudaMemcpyDeviceToHost, sv.stream));
+  const unsigned long long* dtmin = sv.fp32 ? sv.stF.dtmin : sv.st.dtmin;
+  const int* err_flag = sv.fp32 ? sv.stF.err_flag : sv.st.err_flag;
+  CS_CUDA(sv, cudaMemcpyAsync(&bits, dtmin, sizeof(bits), cudaMemcpyDeviceToHost, sv.stream));
+  CS_CUDA(sv, cudaMemcpyAsync(&flag, err_flag, sizeof(flag), cudaMemcpyDeviceToHost, sv.stream));
   CS_CUDA(sv, cudaStreamSynchronize(sv.stream));
   if (flag) return fail(sv, CS_ERR_CUDA, "a bounded device wait gave up (bulk copy did not complete)");
   if (sv.prof.on) prof_harvest(sv);
   std::memcpy(out, &bits, sizeof(bits));
   return CS_OK;
+}
+
+// Device-to-host copy of one debug array; arrays of the state's type R
+// are widened to double on the host.
+template <typename R>
+cudaError_t debug_copy(Solve& sv, const DStateT<R>& s, int which, size_t nc, double* host_out) {
+  const size_t S6 = (size_t)6 * sv.d.S;
+  std::vector<R> tmp;
+  auto cp = [&](double* dst, const R* src, size_t n) -> cudaError_t {
+    tmp.resize(n);
+    cudaError_t e = cudaMemcpyAsync(tmp.data(), src, n * sizeof(R), cudaMemcpyDeviceToHost, sv.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(sv.stream);
+    for (size_t t = 0; e == cudaSuccess && t < n; ++t) dst[t] = (double)tmp[t];
+    return e;
+  };
+  auto cpd = [&](double* dst, const double* src, size_t n) -> cudaError_t {
+    cudaError_t e = cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyDeviceToHost, sv.stream);
+    return e == cudaSuccess ? cudaStreamSynchronize(sv.stream) : e;
+  };
+  cudaError_t e = cudaSuccess;
+  switch (which) {
+    case 0: e = cp(host_out, s.V, nc * S6); break;
+    case 1: e = cp(host_out, s.ent, nc * S6); break;
+    case 2: e = cp(host_out, s.flatA, S6); break;
+    case 3: e = cp(host_out, s.dUdt, nc * S6); break;
+    case 4: case 5: case 6: e = cpd(host_out, s.Ef[which - 4], S6); break;
+    case 7: case 8: case 9: e = cpd(host_out, s.Bq[which - 7], nc * S6); break;
+    case 10: e = cp(host_out, s.E, 3 * S6); break;
+    case 11:
+      for (int q = 0; q < 6 && e == cudaSuccess; ++q) e = cp(host_out + q * S6, s.S[q], S6);
+      break;
+    case 12:
+      for (int q = 0; q < 3 && e == cudaSuccess; ++q) e = cp(host_out + q * S6, s.EF[q], S6);
+      break;
+  }
+  return e;
 }
 
 size_t field_ncomp_debug(int which) {
@@ -754,12 +813,28 @@ int cs_state_put(cs_ctx* ctx, const double* U, const double* ent, const double* 
   if (!ctx || !U || !ent || !bxf || !byf || !bzf) return CS_ERR_ARG;
   Solve& sv = ctx->sv;
   if (int rc = cs::need(sv, false)) return rc;
-  const size_t S6 = (size_t)6 * sv.d.S * sizeof(double);
-  CS_CUDA(sv, cudaMemcpyAsync(sv.st.U, U, cs::NVAR * S6, cudaMemcpyHostToDevice, sv.stream));
-  CS_CUDA(sv, cudaMemcpyAsync(sv.st.ent, ent, S6, cudaMemcpyHostToDevice, sv.stream));
-  CS_CUDA(sv, cudaMemcpyAsync(sv.st.Bxf, bxf, S6, cudaMemcpyHostToDevice, sv.stream));
-  CS_CUDA(sv, cudaMemcpyAsync(sv.st.Byf, byf, S6, cudaMemcpyHostToDevice, sv.stream));
-  CS_CUDA(sv, cudaMemcpyAsync(sv.st.Bzf, bzf, S6, cudaMemcpyHostToDevice, sv.stream));
+  const size_t S6 = (size_t)6 * sv.d.S;
+  if (sv.fp32) {
+    // The precision form keeps U and the entropy in FP32 on the device.
+    std::vector<float> u(cs::NVAR * S6 + S6);
+    for (size_t t = 0; t < cs::NVAR * S6; ++t) u[t] = (float)U[t];
+    for (size_t t = 0; t < S6; ++t) u[cs::NVAR * S6 + t] = (float)ent[t];
+    CS_CUDA(sv, cudaMemcpyAsync(sv.stF.U, u.data(), cs::NVAR * S6 * sizeof(float), cudaMemcpyHostToDevice, sv.stream));
+    CS_CUDA(sv, cudaMemcpyAsync(sv.stF.ent, u.data() + cs::NVAR * S6, S6 * sizeof(float), cudaMemcpyHostToDevice,
+                                sv.stream));
+    CS_CUDA(sv, cudaMemcpyAsync(sv.stF.Bxf, bxf, S6 * sizeof(double), cudaMemcpyHostToDevice, sv.stream));
+    CS_CUDA(sv, cudaMemcpyAsync(sv.stF.Byf, byf, S6 * sizeof(double), cudaMemcpyHostToDevice, sv.stream));
+    CS_CUDA(sv, cudaMemcpyAsync(sv.stF.Bzf, bzf, S6 * sizeof(double), cudaMemcpyHostToDevice, sv.stream));
+    CS_CUDA(sv, cudaStreamSynchronize(sv.stream));
+    sv.has_state = true;
+    return CS_OK;
+  }
+  const size_t B = S6 * sizeof(double);
+  CS_CUDA(sv, cudaMemcpyAsync(sv.st.U, U, cs::NVAR * B, cudaMemcpyHostToDevice, sv.stream));
+  CS_CUDA(sv, cudaMemcpyAsync(sv.st.ent, ent, B, cudaMemcpyHostToDevice, sv.stream));
+  CS_CUDA(sv, cudaMemcpyAsync(sv.st.Bxf, bxf, B, cudaMemcpyHostToDevice, sv.stream));
+  CS_CUDA(sv, cudaMemcpyAsync(sv.st.Byf, byf, B, cudaMemcpyHostToDevice, sv.stream));
+  CS_CUDA(sv, cudaMemcpyAsync(sv.st.Bzf, bzf, B, cudaMemcpyHostToDevice, sv.stream));
   CS_CUDA(sv, cudaStreamSynchronize(sv.stream));
   sv.has_state = true;
   return CS_OK;
@@ -769,12 +844,26 @@ int cs_state_get(cs_ctx* ctx, double* U, double* ent, double* bxf, double* byf, 
   if (!ctx || !U || !ent || !bxf || !byf || !bzf) return CS_ERR_ARG;
   Solve& sv = ctx->sv;
   if (int rc = cs::need(sv, true)) return rc;
-  const size_t S6 = (size_t)6 * sv.d.S * sizeof(double);
-  CS_CUDA(sv, cudaMemcpyAsync(U, sv.st.U, cs::NVAR * S6, cudaMemcpyDeviceToHost, sv.stream));
-  CS_CUDA(sv, cudaMemcpyAsync(ent, sv.st.ent, S6, cudaMemcpyDeviceToHost, sv.stream));
-  CS_CUDA(sv, cudaMemcpyAsync(bxf, sv.st.Bxf, S6, cudaMemcpyDeviceToHost, sv.stream));
-  CS_CUDA(sv, cudaMemcpyAsync(byf, sv.st.Byf, S6, cudaMemcpyDeviceToHost, sv.stream));
-  CS_CUDA(sv, cudaMemcpyAsync(bzf, sv.st.Bzf, S6, cudaMemcpyDeviceToHost, sv.stream));
+  const size_t S6 = (size_t)6 * sv.d.S;
+  if (sv.fp32) {
+    std::vector<float> u(cs::NVAR * S6 + S6);
+    CS_CUDA(sv, cudaMemcpyAsync(u.data(), sv.stF.U, cs::NVAR * S6 * sizeof(float), cudaMemcpyDeviceToHost, sv.stream));
+    CS_CUDA(sv, cudaMemcpyAsync(u.data() + cs::NVAR * S6, sv.stF.ent, S6 * sizeof(float), cudaMemcpyDeviceToHost,
+                                sv.stream));
+    CS_CUDA(sv, cudaMemcpyAsync(bxf, sv.stF.Bxf, S6 * sizeof(double), cudaMemcpyDeviceToHost, sv.stream));
+    CS_CUDA(sv, cudaMemcpyAsync(byf, sv.stF.Byf, S6 * sizeof(double), cudaMemcpyDeviceToHost, sv.stream));
+    CS_CUDA(sv, cudaMemcpyAsync(bzf, sv.stF.Bzf, S6 * sizeof(double), cudaMemcpyDeviceToHost, sv.stream));
+    CS_CUDA(sv, cudaStreamSynchronize(sv.stream));
+    for (size_t t = 0; t < cs::NVAR * S6; ++t) U[t] = u[t];
+    for (size_t t = 0; t < S6; ++t) ent[t] = u[cs::NVAR * S6 + t];
+    return CS_OK;
+  }
+  const size_t B = S6 * sizeof(double);
+  CS_CUDA(sv, cudaMemcpyAsync(U, sv.st.U, cs::NVAR * B, cudaMemcpyDeviceToHost, sv.stream));
+  CS_CUDA(sv, cudaMemcpyAsync(ent, sv.st.ent, B, cudaMemcpyDeviceToHost, sv.stream));
+  CS_CUDA(sv, cudaMemcpyAsync(bxf, sv.st.Bxf, B, cudaMemcpyDeviceToHost, sv.stream));
+  CS_CUDA(sv, cudaMemcpyAsync(byf, sv.st.Byf, B, cudaMemcpyDeviceToHost, sv.stream));
+  CS_CUDA(sv, cudaMemcpyAsync(bzf, sv.st.Bzf, B, cudaMemcpyDeviceToHost, sv.stream));
   CS_CUDA(sv, cudaStreamSynchronize(sv.stream));
   return CS_OK;
 }
@@ -909,29 +998,9 @@ int cs_debug_get(cs_ctx* ctx, int32_t which, double* host_out, size_t n) {
   const size_t S6 = (size_t)6 * sv.d.S;
   if (nc == 0) return cs::fail(sv, CS_ERR_ARG, "unknown debug array");
   if (n != nc * S6) return cs::fail(sv, CS_ERR_ARG, "debug buffer size mismatch");
-  const cs::DState& s = sv.st;
-  const size_t B = S6 * sizeof(double);
-  auto cp = [&](double* dst, const double* src, size_t bytes) {
-    return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, sv.stream);
-  };
-  cudaError_t e = cudaSuccess;
-  switch (which) {
-    case 0: e = cp(host_out, s.V, nc * B); break;
-    case 1: e = cp(host_out, s.ent, nc * B); break;
-    case 2: e = cp(host_out, s.flatA, B); break;
-    case 3: e = cp(host_out, s.dUdt, nc * B); break;
-    case 4: case 5: case 6: e = cp(host_out, s.Ef[which - 4], B); break;
-    case 7: case 8: case 9: e = cp(host_out, s.Bq[which - 7], nc * B); break;
-    case 10: e = cp(host_out, s.E, 3 * B); break;
-    case 11:
-      for (int q = 0; q < 6 && e == cudaSuccess; ++q) e = cp(host_out + q * S6, s.S[q], B);
-      break;
-    case 12:
-      for (int q = 0; q < 3 && e == cudaSuccess; ++q) e = cp(host_out + q * S6, s.EF[q], B);
-      break;
-  }
+  const cudaError_t e = sv.fp32 ? cs::debug_copy(sv, sv.stF, which, nc, host_out)
+                                 : cs::debug_copy(sv, sv.st, which, nc, host_out);
   if (e != cudaSuccess) return cs::cuda_fail(sv, e, "cs_debug_get copy");
-  CS_CUDA(sv, cudaStreamSynchronize(sv.stream));
   return CS_OK;
 }
 

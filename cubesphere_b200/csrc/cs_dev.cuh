@@ -35,20 +35,28 @@ struct DGeom {
   const int32_t* st;    // [6][12][2][NJ][NI]
 };
 
-// Mutable per-solve arrays.
-struct DState {
-  double *U, *ent, *Bxf, *Byf, *Bzf;     // state (U: 8 comps, ent: 4 modes)
-  double *V, *E, *Esnap;                 // V: 80 (mode*8+comp), E: 30 (mode*3+comp), Esnap: 3
-  double *msonic, *flatA, *flatB;        // flattener work
+// Mutable per-solve arrays.  R is the storage and arithmetic type of the
+// state, the reconstruction, the face states and fluxes and the stage update
+// (double in the plain form, float in the precision form); face B, its
+// quadrature values, the EMFs and the resident operators are FP64 always.
+template <typename R>
+struct DStateT {
+  using real = R;
+  R *U, *ent;                            // state (U: 8 comps, ent: 4 modes)
+  double *Bxf, *Byf, *Bzf;               // face-normal B
+  R *V, *E, *Esnap;                      // V: 80 (mode*8+comp), E: 30 (mode*3+comp), Esnap: 3
+  R *msonic, *flatA, *flatB;             // flattener work
   double *Bq[3];                         // B at face quadrature points (5 each)
-  double *fcon[3];                       // per-face flux contributions: [16][..] (L 8, R 8)
-  double *FS;                            // face states: [(side*5 + point)*9 + var][..], 270 comps
-  double *S[6];                          // S_L,S_R (x), S_D,S_U (y), S_B,S_T (z) at j=1
-  double *EF[3];                         // entropy fluxes
+  R *fcon[3];                            // per-face flux contributions: [16][..] (L 8, R 8)
+  R *FS;                                 // face states: [(side*5 + point)*9 + var][..], 270 comps
+  R *S[6];                               // S_L,S_R (x), S_D,S_U (y), S_B,S_T (z) at j=1
+  R *EF[3];                              // entropy fluxes
   double *Ef[3];                         // edge EMFs
-  double *dUdt;                          // 8
-  double *U0, *ent0, *B0[3];             // saved stage-1 state
-  double *K1, *EF1[3], *Ef1[3];          // IMEX: first stage's dU/dt, entropy fluxes and EMFs
+  R *dUdt;                               // 8
+  R *U0, *ent0;                          // saved stage-1 state
+  double *B0[3];
+  R *K1, *EF1[3];                        // IMEX: first stage's dU/dt and entropy fluxes
+  double *Ef1[3];                        // IMEX: first stage's EMFs
   double* op_m9;                         // STEP 7.b inverse normal matrices, [81][zones of shrink(2)], or null
   double* op_m10;                        // STEP 9.c inverse normal matrices, [100][zones of shrink(2)], or null
   double* adp_lu;                        // ADP KKT factors: per block of 128 zones, [1296 in use order][128], or null
@@ -58,6 +66,7 @@ struct DState {
   int32_t* giveup;                       // positivity give-up flags per zone
   unsigned long long* dtmin;             // CFL reduction target (bit pattern of a positive double)
 };
+using DState = DStateT<double>;
 
 __device__ __forceinline__ int mask_at(const DGeom& g, const Dims& d, int p, int i, int j) {
   return g.mask[(long long)p * d.S + d.idx(i, j, 0)];
@@ -67,6 +76,11 @@ __device__ __forceinline__ int sten(const DGeom& g, const Dims& d, int p, int i,
 }
 __device__ __forceinline__ double geo(const DGeom& g, const Dims& d, int f, int c, int p, int i, int j, int k) {
   return __ldg(g.f[f] + d.at(c, p, i, j, k));
+}
+
+template <typename R>
+__device__ __forceinline__ R geoR(const DGeom& g, const Dims& d, int f, int c, int p, int i, int j, int k) {
+  return (R)__ldg(g.f[f] + d.at(c, p, i, j, k));
 }
 
 // Decode a flat thread index over panels x a 3-D index range.
@@ -87,37 +101,40 @@ struct Range3 {
 };
 
 // ---------------- pointwise physics (ideal MHD, adiabatic) ----------------
-__device__ __forceinline__ double sqr(double x) { return x * x; }
+template <typename R>
+__device__ __forceinline__ R sqr(R x) { return x * x; }
 
 // Conserved -> primitive with density/pressure floors and the entropy
 // fallback; updates ent and re-derives the total energy.  Returns the
 // floor flag.
-__device__ __forceinline__ int d_cons_to_prim(const PhysC& ph, double& ent, double* U, double* V) {
+template <typename R>
+__device__ __forceinline__ int d_cons_to_prim(const PhysC& ph, R& ent, R* U, R* V) {
   int flag = 0;
-  U[0] = fmax(U[0], ph.rhofloor);
+  U[0] = fmax(U[0], R(ph.rhofloor));
   V[0] = U[0];
-  const double a = V[0] / (V[0] * V[0] + ph.rhofloor * ph.rhofloor);
+  const R a = V[0] / (V[0] * V[0] + R(ph.rhofloor) * R(ph.rhofloor));
   V[1] = U[1] * a;
   V[2] = U[2] * a;
   V[3] = U[3] * a;
   V[5] = U[5];
   V[6] = U[6];
   V[7] = U[7];
-  const double v2 = V[1] * V[1] + V[2] * V[2] + V[3] * V[3];
-  const double b2 = V[5] * V[5] + V[6] * V[6] + V[7] * V[7];
-  V[4] = (ph.gamma - 1.0) * (U[4] - 0.5 * V[0] * v2 - ph.ob8pi * b2);
-  if (V[4] <= ph.prsfloor) {
-    V[4] = fmax(ph.prsfloor, ent * pow(V[0], ph.gamma - 1.0));
+  const R v2 = V[1] * V[1] + V[2] * V[2] + V[3] * V[3];
+  const R b2 = V[5] * V[5] + V[6] * V[6] + V[7] * V[7];
+  V[4] = (R(ph.gamma) - R(1.0)) * (U[4] - R(0.5) * V[0] * v2 - R(ph.ob8pi) * b2);
+  if (V[4] <= R(ph.prsfloor)) {
+    V[4] = fmax(R(ph.prsfloor), ent * pow(V[0], R(ph.gamma) - R(1.0)));
     flag = 1;
   }
-  ent = V[4] / pow(V[0], ph.gamma - 1.0);
-  U[4] = V[4] / (ph.gamma - 1.0) + 0.5 * V[0] * v2 + ph.ob8pi * b2;
+  ent = V[4] / pow(V[0], R(ph.gamma) - R(1.0));
+  U[4] = V[4] / (R(ph.gamma) - R(1.0)) + R(0.5) * V[0] * v2 + R(ph.ob8pi) * b2;
   return flag;
 }
 
-__device__ __forceinline__ void d_prim_to_cons(const PhysC& ph, double ent, double* U, double* V) {
-  V[0] = fmax(V[0], ph.rhofloor);
-  if (V[4] <= ph.prsfloor) V[4] = fmax(ph.prsfloor, ent * pow(V[0], ph.gamma - 1.0));
+template <typename R>
+__device__ __forceinline__ void d_prim_to_cons(const PhysC& ph, R ent, R* U, R* V) {
+  V[0] = fmax(V[0], R(ph.rhofloor));
+  if (V[4] <= R(ph.prsfloor)) V[4] = fmax(R(ph.prsfloor), ent * pow(V[0], R(ph.gamma) - R(1.0)));
   U[0] = V[0];
   U[1] = V[0] * V[1];
   U[2] = V[0] * V[2];
@@ -125,33 +142,35 @@ __device__ __forceinline__ void d_prim_to_cons(const PhysC& ph, double ent, doub
   U[5] = V[5];
   U[6] = V[6];
   U[7] = V[7];
-  U[4] = V[4] / (ph.gamma - 1.0) + 0.5 * V[0] * (V[1] * V[1] + V[2] * V[2] + V[3] * V[3]) +
-         ph.ob8pi * (V[5] * V[5] + V[6] * V[6] + V[7] * V[7]);
+  U[4] = V[4] / (R(ph.gamma) - R(1.0)) + R(0.5) * V[0] * (V[1] * V[1] + V[2] * V[2] + V[3] * V[3]) +
+         R(ph.ob8pi) * (V[5] * V[5] + V[6] * V[6] + V[7] * V[7]);
 }
 
 // Fast magnetosonic extremal speeds along the local x axis.
-__device__ __forceinline__ void d_wavespeeds(const PhysC& ph, const double* V, double& smin, double& smax) {
-  const double cs2 = ph.gamma * V[4] / V[0];
-  const double b2r = (V[5] * V[5] + V[6] * V[6] + V[7] * V[7]) / (ph.fourpi * V[0]);
-  const double bb = -(cs2 + b2r);
-  const double cc = cs2 * V[5] * V[5] / (ph.fourpi * V[0]);
-  const double mf = sqrt((-bb + sqrt(bb * bb - 4.0 * cc)) / 2.0);
+template <typename R>
+__device__ __forceinline__ void d_wavespeeds(const PhysC& ph, const R* V, R& smin, R& smax) {
+  const R cs2 = R(ph.gamma) * V[4] / V[0];
+  const R b2r = (V[5] * V[5] + V[6] * V[6] + V[7] * V[7]) / (R(ph.fourpi) * V[0]);
+  const R bb = -(cs2 + b2r);
+  const R cc = cs2 * V[5] * V[5] / (R(ph.fourpi) * V[0]);
+  const R mf = sqrt((-bb + sqrt(bb * bb - R(4.0) * cc)) / R(2.0));
   smin = V[1] - mf;
   smax = V[1] + mf;
 }
 
-__device__ __forceinline__ void d_flux_x(const PhysC& ph, const double* V, double* F) {
-  const double u4 = V[4] / (ph.gamma - 1.0) + 0.5 * V[0] * (V[1] * V[1] + V[2] * V[2] + V[3] * V[3]) +
-                    ph.ob8pi * (V[5] * V[5] + V[6] * V[6] + V[7] * V[7]);
-  const double b2 = V[5] * V[5] + V[6] * V[6] + V[7] * V[7];
-  const double vdb = V[1] * V[5] + V[2] * V[6] + V[3] * V[7];
-  const double pt = V[4] + ph.ob8pi * b2;
+template <typename R>
+__device__ __forceinline__ void d_flux_x(const PhysC& ph, const R* V, R* F) {
+  const R u4 = V[4] / (R(ph.gamma) - R(1.0)) + R(0.5) * V[0] * (V[1] * V[1] + V[2] * V[2] + V[3] * V[3]) +
+                    R(ph.ob8pi) * (V[5] * V[5] + V[6] * V[6] + V[7] * V[7]);
+  const R b2 = V[5] * V[5] + V[6] * V[6] + V[7] * V[7];
+  const R vdb = V[1] * V[5] + V[2] * V[6] + V[3] * V[7];
+  const R pt = V[4] + R(ph.ob8pi) * b2;
   F[0] = V[1] * V[0];
-  F[1] = V[1] * (V[0] * V[1]) + pt - ph.ob4pi * V[5] * V[5];
-  F[2] = V[1] * (V[0] * V[2]) - ph.ob4pi * V[5] * V[6];
-  F[3] = V[1] * (V[0] * V[3]) - ph.ob4pi * V[5] * V[7];
-  F[4] = V[1] * u4 + pt * V[1] - ph.ob4pi * V[5] * vdb;
-  F[5] = 0.0;
+  F[1] = V[1] * (V[0] * V[1]) + pt - R(ph.ob4pi) * V[5] * V[5];
+  F[2] = V[1] * (V[0] * V[2]) - R(ph.ob4pi) * V[5] * V[6];
+  F[3] = V[1] * (V[0] * V[3]) - R(ph.ob4pi) * V[5] * V[7];
+  F[4] = V[1] * u4 + pt * V[1] - R(ph.ob4pi) * V[5] * vdb;
+  F[5] = R(0.0);
   F[6] = V[1] * V[6] - V[5] * V[2];
   F[7] = V[1] * V[7] - V[5] * V[3];
 }
@@ -159,56 +178,57 @@ __device__ __forceinline__ void d_flux_x(const PhysC& ph, const double* V, doubl
 // HLL solve at one quadrature point in the face frame.  Outputs the left
 // and right fluctuations, the two physical fluxes (all in the face frame),
 // the extremal speeds and the entropy flux.
-__device__ __forceinline__ void d_hll(const PhysC& ph, double* VL, double* VR, double entL, double entR, double* FlL,
-                                      double* FlR, double* FL, double* FR, double& SL, double& SR, double& entF) {
-  const double bx = 0.5 * (VL[5] + VR[5]);
+template <typename R>
+__device__ __forceinline__ void d_hll(const PhysC& ph, R* VL, R* VR, R entL, R entR, R* FlL,
+                                      R* FlR, R* FL, R* FR, R& SL, R& SR, R& entF) {
+  const R bx = R(0.5) * (VL[5] + VR[5]);
   VL[5] = bx;
   VR[5] = bx;
-  double UL[8], UR[8];
+  R UL[8], UR[8];
   d_prim_to_cons(ph, entL, UL, VL);
   d_prim_to_cons(ph, entR, UR, VR);
   d_flux_x(ph, VL, FL);
   d_flux_x(ph, VR, FR);
-  double smin, smax;
-  SR = -1.0e30;
-  SL = 1.0e30;
+  R smin, smax;
+  SR = -R(1.0e30);
+  SL = R(1.0e30);
   d_wavespeeds(ph, VL, smin, smax);
   SL = fmin(SL, smin);
   SR = fmax(SR, smax);
   d_wavespeeds(ph, VR, smin, smax);
   SL = fmin(SL, smin);
   SR = fmax(SR, smax);
-  double Vm[8];
+  R Vm[8];
 #pragma unroll
-  for (int c = 0; c < 8; ++c) Vm[c] = 0.5 * (VL[c] + VR[c]);
+  for (int c = 0; c < 8; ++c) Vm[c] = R(0.5) * (VL[c] + VR[c]);
   d_wavespeeds(ph, Vm, smin, smax);
   SL = fmin(SL, smin);
   SR = fmax(SR, smax);
-  const double t3 = 1.0 / (SR - SL), t1 = SR * t3, t2 = SL * t3;
-  double Us[8];
+  const R t3 = R(1.0) / (SR - SL), t1 = SR * t3, t2 = SL * t3;
+  R Us[8];
 #pragma unroll
   for (int c = 0; c < 8; ++c) Us[c] = t1 * UR[c] - t2 * UL[c] - t3 * (FR[c] - FL[c]);
-  const double entU = t1 * entR - t2 * entL - t3 * (entR * VR[1] - entL * VL[1]);
-  const double pent = entU * pow(Us[0], ph.gamma - 1.0);
-  const double peng = (ph.gamma - 1.0) * (Us[4] - 0.5 * (Us[1] * Us[1] + Us[2] * Us[2] + Us[3] * Us[3]) / Us[0] -
-                                          ph.ob8pi * (Us[5] * Us[5] + Us[6] * Us[6] + Us[7] * Us[7]));
-  if (peng <= ph.prsfloor) Us[4] = Us[4] + (pent - peng) / (ph.gamma - 1.0);
-  if (SL >= 0.0) {
+  const R entU = t1 * entR - t2 * entL - t3 * (entR * VR[1] - entL * VL[1]);
+  const R pent = entU * pow(Us[0], R(ph.gamma) - R(1.0));
+  const R peng = (R(ph.gamma) - R(1.0)) * (Us[4] - R(0.5) * (Us[1] * Us[1] + Us[2] * Us[2] + Us[3] * Us[3]) / Us[0] -
+                                          R(ph.ob8pi) * (Us[5] * Us[5] + Us[6] * Us[6] + Us[7] * Us[7]));
+  if (peng <= R(ph.prsfloor)) Us[4] = Us[4] + (pent - peng) / (R(ph.gamma) - R(1.0));
+  if (SL >= R(0.0)) {
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
       FlR[c] = SL * (UL[c] - UL[c]) + SR * (UR[c] - UL[c]);
-      FlL[c] = 0.0;
+      FlL[c] = R(0.0);
     }
     entF = entL * VL[1];
-  } else if (SR <= 0.0) {
+  } else if (SR <= R(0.0)) {
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
       FlL[c] = SL * (UR[c] - UL[c]) + SR * (UR[c] - UR[c]);
-      FlR[c] = 0.0;
+      FlR[c] = R(0.0);
     }
     entF = entR * VR[1];
   } else {
-    const double s1 = 1.0 / (SR - SL), s2 = SR * SL * s1;
+    const R s1 = R(1.0) / (SR - SL), s2 = SR * SL * s1;
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
       FlL[c] = SL * (Us[c] - UL[c]);
@@ -310,35 +330,36 @@ __device__ __forceinline__ double d_rs3(double SR1, double SL1, double SR2, doub
 }
 
 // Taylor polynomial (10 modes) at scaled offset (x,y,z).
-__device__ __forceinline__ double d_poly10(const double* v, const double* c, double x, double y, double z) {
+template <typename R>
+__device__ __forceinline__ R d_poly10(const R* v, const R* c, R x, R y, R z) {
   return v[0] + v[1] * x + v[2] * y + v[3] * z + v[4] * (x * x - c[4]) + v[5] * (y * y - c[5]) +
          v[6] * (z * z - c[6]) + v[7] * (x * y - c[7]) + v[8] * (y * z - c[8]) + v[9] * (x * z - c[9]);
 }
 
 // In-register Gaussian elimination with scaled partial pivoting for the
 // small (9x9, 10x10) normal matrices; returns the inverse, row-major.
-template <int n>
-__device__ __forceinline__ void d_matinv(const double* A, double* Ainv) {
-  double M[n * n];
-  double sc[n];
+template <int n, typename R>
+__device__ __forceinline__ void d_matinv(const R* A, R* Ainv) {
+  R M[n * n];
+  R sc[n];
   int pv[n];
 #pragma unroll
   for (int t = 0; t < n * n; ++t) M[t] = A[t];
 #pragma unroll
   for (int i = 0; i < n; ++i) {
-    double m = 0.0;
+    R m = R(0.0);
 #pragma unroll
     for (int j = 0; j < n; ++j) m = fmax(m, fabs(M[i * n + j]));
-    sc[i] = (m == 0.0) ? 0.0 : 1.0 / m;
+    sc[i] = (m == R(0.0)) ? R(0.0) : R(1.0) / m;
     pv[i] = i;
   }
 #pragma unroll
   for (int k = 0; k < n; ++k) {
     int p = k;
-    double best = -1.0;
+    R best = -R(1.0);
 #pragma unroll
     for (int i = k; i < n; ++i) {
-      const double v = fabs(M[i * n + k]) * sc[i];
+      const R v = fabs(M[i * n + k]) * sc[i];
       if (v > best) {
         best = v;
         p = i;
@@ -347,22 +368,22 @@ __device__ __forceinline__ void d_matinv(const double* A, double* Ainv) {
     if (p != k) {
 #pragma unroll
       for (int j = 0; j < n; ++j) {
-        const double t = M[k * n + j];
+        const R t = M[k * n + j];
         M[k * n + j] = M[p * n + j];
         M[p * n + j] = t;
       }
-      const double t = sc[k];
+      const R t = sc[k];
       sc[k] = sc[p];
       sc[p] = t;
       const int ti = pv[k];
       pv[k] = pv[p];
       pv[p] = ti;
     }
-    if (M[k * n + k] == 0.0) M[k * n + k] = 1.0e-20;
-    const double inv = 1.0 / M[k * n + k];
+    if (M[k * n + k] == R(0.0)) M[k * n + k] = R(1.0e-20);
+    const R inv = R(1.0) / M[k * n + k];
 #pragma unroll
     for (int i = k + 1; i < n; ++i) {
-      const double l = M[i * n + k] * inv;
+      const R l = M[i * n + k] * inv;
       M[i * n + k] = l;
 #pragma unroll
       for (int j = k + 1; j < n; ++j) M[i * n + j] -= l * M[k * n + j];
@@ -370,17 +391,17 @@ __device__ __forceinline__ void d_matinv(const double* A, double* Ainv) {
   }
 #pragma unroll
   for (int c = 0; c < n; ++c) {
-    double y[n];
+    R y[n];
 #pragma unroll
     for (int i = 0; i < n; ++i) {
-      double s = (pv[i] == c) ? 1.0 : 0.0;
+      R s = (pv[i] == c) ? R(1.0) : R(0.0);
 #pragma unroll
       for (int j = 0; j < i; ++j) s -= M[i * n + j] * y[j];
       y[i] = s;
     }
 #pragma unroll
     for (int i = n - 1; i >= 0; --i) {
-      double s = y[i];
+      R s = y[i];
 #pragma unroll
       for (int j = i + 1; j < n; ++j) s -= M[i * n + j] * Ainv[j * n + c];
       Ainv[i * n + c] = s / M[i * n + i];
@@ -409,7 +430,8 @@ void launch_sources(Solve& s);
 void launch_save_stage0(Solve& s);
 void launch_combine(Solve& s, double a0, int kind);
 void launch_update(Solve& s, double dtmove);
-void launch_update_with(Solve& s, const DState& st, double dtmove);
+template <typename R>
+void launch_update_with(Solve& s, const DStateT<R>& st, double dtmove);
 void launch_gravity_implicit(Solve& s, double a);
 void launch_add_gravity(Solve& s, double c);
 void launch_save_stage1_rates(Solve& s);

@@ -15,13 +15,16 @@ namespace {
 
 constexpr int TPB = 128;
 
-__device__ __forceinline__ double E1(const DState& s, const Dims& d, int q, int p, int i, int j, int k) {
+template <typename R>
+__device__ __forceinline__ double E1(const DStateT<R>& s, const Dims& d, int q, int p, int i, int j, int k) {
   return s.E[d.at(q, p, i, j, k)];
 }
-__device__ __forceinline__ double Sg(const double* a, const Dims& d, int p, int i, int j, int k) {
+template <typename T>
+__device__ __forceinline__ double Sg(const T* a, const Dims& d, int p, int i, int j, int k) {
   return a[d.at(0, p, i, j, k)];
 }
-__device__ __forceinline__ double Bqa(const DState& s, const Dims& d, int dir, int q, int p, int i, int j, int k) {
+template <typename R>
+__device__ __forceinline__ double Bqa(const DStateT<R>& s, const Dims& d, int dir, int q, int p, int i, int j, int k) {
   return s.Bq[dir][d.at(q, p, i, j, k)];
 }
 
@@ -70,7 +73,8 @@ __device__ __forceinline__ void llf4(double& SR, double& SL, double& SU, double&
 }
 
 // x-edges (460:393-1493): i in 1..N, j in 0..N, k in 0..nr.
-__global__ void k_edges_x(Dims d, DGeom g, DState s, Range3 r) {
+template <typename R>
+__global__ void k_edges_x(Dims d, DGeom g, DStateT<R> s, Range3 r) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
     r.decode(t, p, i, j, k);
@@ -101,7 +105,8 @@ __global__ void k_edges_x(Dims d, DGeom g, DState s, Range3 r) {
 }
 
 // y-edges (460:1497-2587): i in 0..N, j in 1..N, k in 0..nr.
-__global__ void k_edges_y(Dims d, DGeom g, DState s, Range3 r) {
+template <typename R>
+__global__ void k_edges_y(Dims d, DGeom g, DStateT<R> s, Range3 r) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
     r.decode(t, p, i, j, k);
@@ -134,7 +139,8 @@ __global__ void k_edges_y(Dims d, DGeom g, DState s, Range3 r) {
 // z-edges (460:2591-3721): i, j in 0..N, k in 1..nr, skipped where a
 // neighbour is masked; the four cube corners (460:3725-7037) use the
 // three-state solver.
-__global__ void k_edges_z(Dims d, DGeom g, DState s, Range3 r) {
+template <typename R>
+__global__ void k_edges_z(Dims d, DGeom g, DStateT<R> s, Range3 r) {
   const int N = d.N;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
@@ -224,29 +230,38 @@ __global__ void k_edges_z(Dims d, DGeom g, DState s, Range3 r) {
 // Panel-edge ownership for the EMFs: a non-owner copy of a shared edge
 // takes the owner's value, negated where the two panels run the edge in
 // opposite directions.
-__global__ void k_sync_emf(DState s, PanelSync ps) {
+template <typename R>
+__global__ void k_sync_emf(DStateT<R> s, PanelSync ps) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < ps.ne; t += (long long)gridDim.x * blockDim.x)
     s.Ef[ps.e_df[t]][ps.e_dst[t]] = (double)ps.e_sign[t] * s.Ef[ps.e_sf[t]][ps.e_src[t]];
 }
 
 }  // namespace
 
-void launch_edges(Solve& sv) {
+template <typename R>
+void launch_edges_t(Solve& sv, DStateT<R>& st) {
   const Dims& d = sv.d;
   const int N = d.N, nr = d.nr;
   Range3 ex = {1, N, 0, N, 0, nr};
   Range3 ey = {0, N, 1, N, 0, nr};
   Range3 ez = {0, N, 0, N, 1, nr};
-  k_edges_x<<<blocks_for(ex.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, sv.st, ex);
+  k_edges_x<R><<<blocks_for(ex.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, st, ex);
   mark(sv, "k_edges_x");
-  k_edges_y<<<blocks_for(ey.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, sv.st, ey);
+  k_edges_y<R><<<blocks_for(ey.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, st, ey);
   mark(sv, "k_edges_y");
-  k_edges_z<<<blocks_for(ez.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, sv.st, ez);
+  k_edges_z<R><<<blocks_for(ez.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, st, ez);
   mark(sv, "k_edges_z");
   if (sv.psync.ne > 0) {
-    k_sync_emf<<<blocks_for(sv.psync.ne, 128, sv.sm_count), 128, 0, sv.stream>>>(sv.st, sv.psync);
+    k_sync_emf<R><<<blocks_for(sv.psync.ne, 128, sv.sm_count), 128, 0, sv.stream>>>(st, sv.psync);
     mark(sv, "k_sync_emf");
   }
+}
+
+void launch_edges(Solve& sv) {
+  if (sv.fp32)
+    launch_edges_t(sv, sv.stF);
+  else
+    launch_edges_t(sv, sv.st);
 }
 
 }  // namespace cs

@@ -20,7 +20,8 @@ namespace {
 
 constexpr int TPB = 128;
 
-__device__ __forceinline__ double Vm(const DState& s, const Dims& d, int comp, int mode, int p, long long o) {
+template <typename R>
+__device__ __forceinline__ R Vm(const DStateT<R>& s, const Dims& d, int comp, int mode, int p, long long o) {
   return s.V[((long long)(mode * NVAR + comp) * NPANEL + p) * d.S + o];
 }
 
@@ -29,17 +30,18 @@ __device__ __forceinline__ double Vm(const DState& s, const Dims& d, int comp, i
 // faces, once per stage.  Side f: 0 +x (face i), 1 -x (face i-1), 2 +y,
 // 3 -y, 4 +z, 5 -z.  Layout FS[(f*5 + q)*9 + var][panel][box].
 constexpr int FS_TPB = 64;
-__global__ void __launch_bounds__(FS_TPB) k_face_states(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
-  __shared__ double xs[90][FS_TPB];
+template <typename R>
+__global__ void __launch_bounds__(FS_TPB) k_face_states(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
+  __shared__ R xs[90][FS_TPB];
   const int tid = threadIdx.x;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
     r.decode(t, p, i, j, k);
     if (mask_at(g, d, p, i, j) != 1) continue;
     const long long o = d.idx(i, j, k);
-    const double obl0 = 1.0 / fmax(geo(g, d, CS_G_V_SCALE, 0, p, i, j, k), ph.smallnum);
-    const double cx = geo(g, d, CS_G_V_CEN, 0, p, i, j, k), cy = geo(g, d, CS_G_V_CEN, 1, p, i, j, k),
-                 cz = geo(g, d, CS_G_V_CEN, 2, p, i, j, k);
+    const R obl0 = R(1.0) / fmax(geoR<R>(g, d, CS_G_V_SCALE, 0, p, i, j, k), R(ph.smallnum));
+    const R cx = geoR<R>(g, d, CS_G_V_CEN, 0, p, i, j, k), cy = geoR<R>(g, d, CS_G_V_CEN, 1, p, i, j, k),
+                 cz = geoR<R>(g, d, CS_G_V_CEN, 2, p, i, j, k);
 #pragma unroll 1
     for (int f = 0; f < 6; ++f) {
       const int dir = f / 2;
@@ -47,17 +49,17 @@ __global__ void __launch_bounds__(FS_TPB) k_face_states(Dims d, PhysC ph, DGeom 
       const int fx = (f == 1) ? i - 1 : i, fy = (f == 3) ? j - 1 : j, fz = (f == 5) ? k - 1 : k;
 #pragma unroll
       for (int q = 0; q < 5; ++q) {
-        xs[(f * 5 + q) * 3 + 0][tid] = (geo(g, d, QP, q, p, fx, fy, fz) - cx) * obl0;
-        xs[(f * 5 + q) * 3 + 1][tid] = (geo(g, d, QP, 5 + q, p, fx, fy, fz) - cy) * obl0;
-        xs[(f * 5 + q) * 3 + 2][tid] = (geo(g, d, QP, 10 + q, p, fx, fy, fz) - cz) * obl0;
+        xs[(f * 5 + q) * 3 + 0][tid] = (geoR<R>(g, d, QP, q, p, fx, fy, fz) - cx) * obl0;
+        xs[(f * 5 + q) * 3 + 1][tid] = (geoR<R>(g, d, QP, 5 + q, p, fx, fy, fz) - cy) * obl0;
+        xs[(f * 5 + q) * 3 + 2][tid] = (geoR<R>(g, d, QP, 10 + q, p, fx, fy, fz) - cz) * obl0;
       }
     }
-    double c0[10];
+    R c0[10];
 #pragma unroll
-    for (int m = 0; m < 10; ++m) c0[m] = geo(g, d, CS_G_COEF, m, p, i, j, k);
+    for (int m = 0; m < 10; ++m) c0[m] = geoR<R>(g, d, CS_G_COEF, m, p, i, j, k);
 #pragma unroll 1
     for (int c = 0; c < 8; ++c) {
-      double v[10];
+      R v[10];
 #pragma unroll
       for (int m = 0; m < 10; ++m) v[m] = Vm(s, d, c, m, p, o);
 #pragma unroll 5
@@ -65,8 +67,8 @@ __global__ void __launch_bounds__(FS_TPB) k_face_states(Dims d, PhysC ph, DGeom 
         s.FS[((long long)(fq * 9 + c) * NPANEL + p) * d.S + o] =
             d_poly10(v, c0, xs[fq * 3 + 0][tid], xs[fq * 3 + 1][tid], xs[fq * 3 + 2][tid]);
     }
-    const double* E = s.ent;
-    const double e0 = E[((long long)0 * NPANEL + p) * d.S + o], e1 = E[((long long)1 * NPANEL + p) * d.S + o],
+    const R* E = s.ent;
+    const R e0 = E[((long long)0 * NPANEL + p) * d.S + o], e1 = E[((long long)1 * NPANEL + p) * d.S + o],
                  e2 = E[((long long)2 * NPANEL + p) * d.S + o], e3 = E[((long long)3 * NPANEL + p) * d.S + o];
 #pragma unroll 5
     for (int fq = 0; fq < 30; ++fq)
@@ -81,15 +83,16 @@ __global__ void __launch_bounds__(FS_TPB) k_face_states(Dims d, PhysC ph, DGeom 
 // per-point contributions meet in shared memory and are summed in point
 // order (the order of the reference's quadrature loop).
 constexpr int FLUX_FACES = 32;
-__global__ void __launch_bounds__(FLUX_FACES * 5, 4) k_flux(Dims d, PhysC ph, DGeom g, DState s, Range3 r, int dir) {
-  __shared__ double red[5][16][FLUX_FACES];
+template <typename R>
+__global__ void __launch_bounds__(FLUX_FACES * 5, 4) k_flux(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r, int dir) {
+  __shared__ R red[5][16][FLUX_FACES];
   const int QP = dir == 0 ? CS_G_XF_QP : (dir == 1 ? CS_G_YF_QP : CS_G_ZF_QP);
   const int QW = dir == 0 ? CS_G_XF_QW : (dir == 1 ? CS_G_YF_QW : CS_G_ZF_QW);
   const int AR = dir == 0 ? CS_G_XF_AREA : (dir == 1 ? CS_G_YF_AREA : CS_G_ZF_AREA);
-  double* F = s.fcon[dir];
-  double* SLo = s.S[2 * dir];
-  double* SHi = s.S[2 * dir + 1];
-  double* EF = s.EF[dir];
+  R* F = s.fcon[dir];
+  R* SLo = s.S[2 * dir];
+  R* SHi = s.S[2 * dir + 1];
+  R* EF = s.EF[dir];
   const int lane = threadIdx.x % FLUX_FACES, jq = threadIdx.x / FLUX_FACES;
   const long long nf = r.count();
   const long long ntile = (nf + FLUX_FACES - 1) / FLUX_FACES;
@@ -120,18 +123,18 @@ __global__ void __launch_bounds__(FLUX_FACES * 5, 4) k_flux(Dims d, PhysC ph, DG
     }
     if (skip) {
 #pragma unroll
-      for (int c = 0; c < 16; ++c) red[jq][c][lane] = 0.0;
+      for (int c = 0; c < 16; ++c) red[jq][c][lane] = R(0.0);
     } else {
       const long long oL = d.idx(lx, ly, lz), oR = d.idx(rx, ry, rz);
-      double Ax, Ay, Az, Bx, By, Bz, Cx, Cy, Cz;
+      R Ax, Ay, Az, Bx, By, Bz, Cx, Cy, Cz;
       if (dir == 0) {
-        Ax = geo(g, d, CS_G_XF_N, 0, p, i, j, k);
-        Ay = geo(g, d, CS_G_XF_N, 1, p, i, j, k);
-        Az = geo(g, d, CS_G_XF_N, 2, p, i, j, k);
-        Cx = geo(g, d, CS_G_XF_CEN, 0, p, i, j, k);
-        Cy = geo(g, d, CS_G_XF_CEN, 1, p, i, j, k);
-        Cz = geo(g, d, CS_G_XF_CEN, 2, p, i, j, k);
-        const double tt = 1.0 / fmax(sqrt(Cx * Cx + Cy * Cy + Cz * Cz), ph.smallnum);
+        Ax = geoR<R>(g, d, CS_G_XF_N, 0, p, i, j, k);
+        Ay = geoR<R>(g, d, CS_G_XF_N, 1, p, i, j, k);
+        Az = geoR<R>(g, d, CS_G_XF_N, 2, p, i, j, k);
+        Cx = geoR<R>(g, d, CS_G_XF_CEN, 0, p, i, j, k);
+        Cy = geoR<R>(g, d, CS_G_XF_CEN, 1, p, i, j, k);
+        Cz = geoR<R>(g, d, CS_G_XF_CEN, 2, p, i, j, k);
+        const R tt = R(1.0) / fmax(sqrt(Cx * Cx + Cy * Cy + Cz * Cz), R(ph.smallnum));
         Cx = Cx * tt;
         Cy = Cy * tt;
         Cz = Cz * tt;
@@ -139,13 +142,13 @@ __global__ void __launch_bounds__(FLUX_FACES * 5, 4) k_flux(Dims d, PhysC ph, DG
         By = Cz * Ax - Cx * Az;
         Bz = Cx * Ay - Cy * Ax;
       } else if (dir == 1) {
-        Ax = geo(g, d, CS_G_YF_N, 0, p, i, j, k);
-        Ay = geo(g, d, CS_G_YF_N, 1, p, i, j, k);
-        Az = geo(g, d, CS_G_YF_N, 2, p, i, j, k);
-        Bx = geo(g, d, CS_G_YF_CEN, 0, p, i, j, k);
-        By = geo(g, d, CS_G_YF_CEN, 1, p, i, j, k);
-        Bz = geo(g, d, CS_G_YF_CEN, 2, p, i, j, k);
-        const double tt = 1.0 / fmax(sqrt(Bx * Bx + By * By + Bz * Bz), ph.smallnum);
+        Ax = geoR<R>(g, d, CS_G_YF_N, 0, p, i, j, k);
+        Ay = geoR<R>(g, d, CS_G_YF_N, 1, p, i, j, k);
+        Az = geoR<R>(g, d, CS_G_YF_N, 2, p, i, j, k);
+        Bx = geoR<R>(g, d, CS_G_YF_CEN, 0, p, i, j, k);
+        By = geoR<R>(g, d, CS_G_YF_CEN, 1, p, i, j, k);
+        Bz = geoR<R>(g, d, CS_G_YF_CEN, 2, p, i, j, k);
+        const R tt = R(1.0) / fmax(sqrt(Bx * Bx + By * By + Bz * Bz), R(ph.smallnum));
         Bx = Bx * tt;
         By = By * tt;
         Bz = Bz * tt;
@@ -153,11 +156,11 @@ __global__ void __launch_bounds__(FLUX_FACES * 5, 4) k_flux(Dims d, PhysC ph, DG
         Cy = Az * Bx - Ax * Bz;
         Cz = Ax * By - Ay * Bx;
       } else {
-        auto vt = [&](int q, int x, int y) { return geo(g, d, CS_G_VERT, q, p, x, y, k); };
-        Ax = geo(g, d, CS_G_ZF_N, jq, p, i, j, k);
-        Ay = geo(g, d, CS_G_ZF_N, 5 + jq, p, i, j, k);
-        Az = geo(g, d, CS_G_ZF_N, 10 + jq, p, i, j, k);
-        double tt = 1.0 / fmax(sqrt(Ax * Ax + Ay * Ay + Az * Az), ph.smallnum);
+        auto vt = [&](int q, int x, int y) { return geoR<R>(g, d, CS_G_VERT, q, p, x, y, k); };
+        Ax = geoR<R>(g, d, CS_G_ZF_N, jq, p, i, j, k);
+        Ay = geoR<R>(g, d, CS_G_ZF_N, 5 + jq, p, i, j, k);
+        Az = geoR<R>(g, d, CS_G_ZF_N, 10 + jq, p, i, j, k);
+        R tt = R(1.0) / fmax(sqrt(Ax * Ax + Ay * Ay + Az * Az), R(ph.smallnum));
         Ax = Ax * tt;
         Ay = Ay * tt;
         Az = Az * tt;
@@ -168,44 +171,44 @@ __global__ void __launch_bounds__(FLUX_FACES * 5, 4) k_flux(Dims d, PhysC ph, DG
         Bx = Bx - tt * Ax;
         By = By - tt * Ay;
         Bz = Bz - tt * Az;
-        tt = 1.0 / fmax(sqrt(Bx * Bx + By * By + Bz * Bz), ph.smallnum);
+        tt = R(1.0) / fmax(sqrt(Bx * Bx + By * By + Bz * Bz), R(ph.smallnum));
         Bx = Bx * tt;
         By = By * tt;
         Bz = Bz * tt;
         Cx = Ay * Bz - Az * By;
         Cy = Az * Bx - Ax * Bz;
         Cz = Ax * By - Ay * Bx;
-        tt = 1.0 / fmax(sqrt(Cx * Cx + Cy * Cy + Cz * Cz), ph.smallnum);
+        tt = R(1.0) / fmax(sqrt(Cx * Cx + Cy * Cy + Cz * Cz), R(ph.smallnum));
         Cx = Cx * tt;
         Cy = Cy * tt;
         Cz = Cz * tt;
       }
-      const double px = geo(g, d, QP, jq, p, i, j, k), py = geo(g, d, QP, 5 + jq, p, i, j, k),
-                   pz = geo(g, d, QP, 10 + jq, p, i, j, k);
+      const R px = geoR<R>(g, d, QP, jq, p, i, j, k), py = geoR<R>(g, d, QP, 5 + jq, p, i, j, k),
+                   pz = geoR<R>(g, d, QP, 10 + jq, p, i, j, k);
       // Face states of the two sides: precomputed unless the side was
       // remapped through istencil (panel corners), which evaluates the
       // remapped zone's reconstruction at this face's point here.
       const bool remapL = lx != i || ly != j;
       const bool remapR = dir == 0 ? (rx != i + 1 || ry != j) : (dir == 1 ? (rx != i || ry != j + 1) : false);
       const int fL = 2 * dir, fR = 2 * dir + 1;
-      double VL[8], VR[8], entL, entR;
-      auto eval = [&](int zx, int zy, int zz, double* Vo, double& eo) {
+      R VL[8], VR[8], entL, entR;
+      auto eval = [&](int zx, int zy, int zz, R* Vo, R& eo) {
         const long long oz = d.idx(zx, zy, zz);
-        const double obl = 1.0 / fmax(geo(g, d, CS_G_V_SCALE, 0, p, zx, zy, zz), ph.smallnum);
-        const double x = (px - geo(g, d, CS_G_V_CEN, 0, p, zx, zy, zz)) * obl;
-        const double y = (py - geo(g, d, CS_G_V_CEN, 1, p, zx, zy, zz)) * obl;
-        const double z = (pz - geo(g, d, CS_G_V_CEN, 2, p, zx, zy, zz)) * obl;
-        double cc[10];
+        const R obl = R(1.0) / fmax(geoR<R>(g, d, CS_G_V_SCALE, 0, p, zx, zy, zz), R(ph.smallnum));
+        const R x = (px - geoR<R>(g, d, CS_G_V_CEN, 0, p, zx, zy, zz)) * obl;
+        const R y = (py - geoR<R>(g, d, CS_G_V_CEN, 1, p, zx, zy, zz)) * obl;
+        const R z = (pz - geoR<R>(g, d, CS_G_V_CEN, 2, p, zx, zy, zz)) * obl;
+        R cc[10];
 #pragma unroll
-        for (int m = 0; m < 10; ++m) cc[m] = geo(g, d, CS_G_COEF, m, p, zx, zy, zz);
+        for (int m = 0; m < 10; ++m) cc[m] = geoR<R>(g, d, CS_G_COEF, m, p, zx, zy, zz);
 #pragma unroll
         for (int c = 0; c < 8; ++c) {
-          double vv[10];
+          R vv[10];
 #pragma unroll
           for (int m = 0; m < 10; ++m) vv[m] = Vm(s, d, c, m, p, oz);
           Vo[c] = d_poly10(vv, cc, x, y, z);
         }
-        const double* E = s.ent;
+        const R* E = s.ent;
         eo = E[((long long)0 * NPANEL + p) * d.S + oz] + E[((long long)1 * NPANEL + p) * d.S + oz] * x +
              E[((long long)2 * NPANEL + p) * d.S + oz] * y + E[((long long)3 * NPANEL + p) * d.S + oz] * z;
       };
@@ -225,9 +228,9 @@ __global__ void __launch_bounds__(FLUX_FACES * 5, 4) k_flux(Dims d, PhysC ph, DG
       }
 #pragma unroll
       for (int o = 1; o <= 5; o += 4) {
-        double a1 = Ax * VL[o] + Ay * VL[o + 1] + Az * VL[o + 2];
-        double b1 = Bx * VL[o] + By * VL[o + 1] + Bz * VL[o + 2];
-        double c1 = Cx * VL[o] + Cy * VL[o + 1] + Cz * VL[o + 2];
+        R a1 = Ax * VL[o] + Ay * VL[o + 1] + Az * VL[o + 2];
+        R b1 = Bx * VL[o] + By * VL[o + 1] + Bz * VL[o + 2];
+        R c1 = Cx * VL[o] + Cy * VL[o + 1] + Cz * VL[o + 2];
         VL[o] = a1;
         VL[o + 1] = b1;
         VL[o + 2] = c1;
@@ -238,7 +241,7 @@ __global__ void __launch_bounds__(FLUX_FACES * 5, 4) k_flux(Dims d, PhysC ph, DG
         VR[o + 1] = b1;
         VR[o + 2] = c1;
       }
-      double FlL[8], FlR[8], FL[8], FR[8], SL, SR, entF;
+      R FlL[8], FlR[8], FL[8], FR[8], SL, SR, entF;
       d_hll(ph, VL, VR, entL, entR, FlL, FlR, FL, FR, SL, SR, entF);
       const long long fo = d.idx(i, j, k);
       if (jq == 0) {
@@ -246,14 +249,14 @@ __global__ void __launch_bounds__(FLUX_FACES * 5, 4) k_flux(Dims d, PhysC ph, DG
         SHi[((long long)p) * d.S + fo] = SR;
         EF[((long long)p) * d.S + fo] = entF;
       }
-      const double wt = geo(g, d, QW, jq, p, i, j, k);
-      const double area = geo(g, d, AR, 0, p, i, j, k);
-      const double volL = geo(g, d, CS_G_V_VOL, 0, p, lx, ly, lz), volR = geo(g, d, CS_G_V_VOL, 0, p, rx, ry, rz);
+      const R wt = geoR<R>(g, d, QW, jq, p, i, j, k);
+      const R area = geoR<R>(g, d, AR, 0, p, i, j, k);
+      const R volL = geoR<R>(g, d, CS_G_V_VOL, 0, p, lx, ly, lz), volR = geoR<R>(g, d, CS_G_V_VOL, 0, p, rx, ry, rz);
       // rotate back to global components: fluctuation + flux on each side
-      auto back = [&](const double* W, int c) {
+      auto back = [&](const R* W, int c) {
         if (c == 0 || c == 4) return W[c];
         const int o = c < 4 ? 1 : 5, a = c - o;
-        const double ea = a == 0 ? Ax : (a == 1 ? Ay : Az), eb = a == 0 ? Bx : (a == 1 ? By : Bz),
+        const R ea = a == 0 ? Ax : (a == 1 ? Ay : Az), eb = a == 0 ? Bx : (a == 1 ? By : Bz),
                      ec = a == 0 ? Cx : (a == 1 ? Cy : Cz);
         return ea * W[o] + eb * W[o + 1] + ec * W[o + 2];
       };
@@ -267,7 +270,7 @@ __global__ void __launch_bounds__(FLUX_FACES * 5, 4) k_flux(Dims d, PhysC ph, DG
     if (valid) {
       const long long fo = d.idx(i, j, k);
       for (int c = jq; c < 16; c += 5) {
-        double acc = 0.0;
+        R acc = R(0.0);
 #pragma unroll
         for (int q = 0; q < 5; ++q) acc = acc + red[q][c][lane];
         F[((long long)c * NPANEL + p) * d.S + fo] = acc;
@@ -280,14 +283,15 @@ __global__ void __launch_bounds__(FLUX_FACES * 5, 4) k_flux(Dims d, PhysC ph, DG
 // Panel-edge ownership for the face fluxes: a non-owner copy of a shared
 // face takes the owner's two one-sided contributions with the sides
 // exchanged (their normals are opposite) and the negated entropy flux.
-__global__ void k_sync_flux(Dims d, DState s, PanelSync ps) {
+template <typename R>
+__global__ void k_sync_flux(Dims d, DStateT<R> s, PanelSync ps) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < ps.nf; t += (long long)gridDim.x * blockDim.x) {
     const long long dst = ps.f_dst[t], src = ps.f_src[t];
     const int dd = ps.f_ddir[t], sd = ps.f_sdir[t];
     const int dp = (int)(dst / d.S), sp = (int)(src / d.S);
     const long long dof = dst % d.S, sof = src % d.S;
-    double* Fd = s.fcon[dd];
-    const double* Fs = s.fcon[sd];
+    R* Fd = s.fcon[dd];
+    const R* Fs = s.fcon[sd];
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
       Fd[((long long)c * NPANEL + dp) * d.S + dof] = Fs[((long long)(8 + c) * NPANEL + sp) * d.S + sof];
@@ -299,20 +303,21 @@ __global__ void k_sync_flux(Dims d, DState s, PanelSync ps) {
 
 // dU/dt of each zone from its six faces (x, then y, then z; lower face,
 // upper face) for the zones whose faces were all computed.
-__global__ void k_gather(Dims d, DGeom g, DState s, Range3 r) {
+template <typename R>
+__global__ void k_gather(Dims d, DGeom g, DStateT<R> s, Range3 r) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
     r.decode(t, p, i, j, k);
-    double acc[8];
+    R acc[8];
 #pragma unroll
-    for (int c = 0; c < 8; ++c) acc[c] = 0.0;
+    for (int c = 0; c < 8; ++c) acc[c] = R(0.0);
     if (mask_at(g, d, p, i, j) == 1) {
       const long long ox[2] = {d.idx(i - 1, j, k), d.idx(i, j, k)};
       const long long oy[2] = {d.idx(i, j - 1, k), d.idx(i, j, k)};
       const long long oz[2] = {d.idx(i, j, k - 1), d.idx(i, j, k)};
       const long long* os[3] = {ox, oy, oz};
       for (int dir = 0; dir < 3; ++dir) {
-        const double* F = s.fcon[dir];
+        const R* F = s.fcon[dir];
 #pragma unroll
         for (int c = 0; c < 8; ++c) {
           acc[c] = acc[c] - F[((long long)(8 + c) * NPANEL + p) * d.S + os[dir][0]];
@@ -326,19 +331,20 @@ __global__ void k_gather(Dims d, DGeom g, DState s, Range3 r) {
 }
 
 // Point-mass gravity on zones 0..N+1 (470:147-244).
-__global__ void k_sources(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
+template <typename R>
+__global__ void k_sources(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
     r.decode(t, p, i, j, k);
     if (mask_at(g, d, p, i, j) != 1) continue;
-    const double x = geo(g, d, CS_G_V_CEN, 0, p, i, j, k), y = geo(g, d, CS_G_V_CEN, 1, p, i, j, k),
-                 z = geo(g, d, CS_G_V_CEN, 2, p, i, j, k);
-    const double rho = s.V[d.at(0, p, i, j, k)], vx = s.V[d.at(1, p, i, j, k)], vy = s.V[d.at(2, p, i, j, k)],
+    const R x = geoR<R>(g, d, CS_G_V_CEN, 0, p, i, j, k), y = geoR<R>(g, d, CS_G_V_CEN, 1, p, i, j, k),
+                 z = geoR<R>(g, d, CS_G_V_CEN, 2, p, i, j, k);
+    const R rho = s.V[d.at(0, p, i, j, k)], vx = s.V[d.at(1, p, i, j, k)], vy = s.V[d.at(2, p, i, j, k)],
                  vz = s.V[d.at(3, p, i, j, k)];
-    const double rad = sqrt(x * x + y * y + z * z);
-    const double gmb = ph.gm * (1.0 / (rad * rad * rad));
-    const double S2 = -(gmb * x * rho), S3 = -(gmb * y * rho), S4 = -(gmb * z * rho);
-    const double S5 = vx * S2 + vy * S3 + vz * S4;
+    const R rad = sqrt(x * x + y * y + z * z);
+    const R gmb = R(ph.gm) * (R(1.0) / (rad * rad * rad));
+    const R S2 = -(gmb * x * rho), S3 = -(gmb * y * rho), S4 = -(gmb * z * rho);
+    const R S5 = vx * S2 + vy * S3 + vz * S4;
     s.dUdt[d.at(1, p, i, j, k)] += S2;
     s.dUdt[d.at(2, p, i, j, k)] += S3;
     s.dUdt[d.at(3, p, i, j, k)] += S4;
@@ -348,37 +354,53 @@ __global__ void k_sources(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
 
 }  // namespace
 
-void launch_fluxes(Solve& sv) {
+template <typename R>
+void launch_fluxes_t(Solve& sv, DStateT<R>& st) {
   const Dims& d = sv.d;
   const int N = d.N, nr = d.nr;
   Range3 fx = {-1, N + 1, 0, N + 1, 0, nr + 1};
   Range3 fy = {0, N + 1, -1, N + 1, 0, nr + 1};
   Range3 fz = {0, N + 1, 0, N + 1, -1, nr + 1};
   Range3 zs = {-1, N + 2, -1, N + 2, -1, nr + 2};
-  k_face_states<<<blocks_for(zs.count(), FS_TPB, sv.sm_count), FS_TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, zs);
+  k_face_states<R><<<blocks_for(zs.count(), FS_TPB, sv.sm_count), FS_TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, zs);
   mark(sv, "k_face_states");
   const Range3 fr[3] = {fx, fy, fz};
   for (int dir = 0; dir < 3; ++dir) {
     const long long nt = (fr[dir].count() + FLUX_FACES - 1) / FLUX_FACES;
     const int nb = (int)std::min<long long>(nt, (long long)sv.sm_count * 32);
-    k_flux<<<nb, FLUX_FACES * 5, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, fr[dir], dir);
+    k_flux<R><<<nb, FLUX_FACES * 5, 0, sv.stream>>>(d, sv.ph, sv.g, st, fr[dir], dir);
     mark(sv, "k_flux");
   }
   if (sv.psync.nf > 0) {
-    k_sync_flux<<<blocks_for(sv.psync.nf, 128, sv.sm_count), 128, 0, sv.stream>>>(d, sv.st, sv.psync);
+    k_sync_flux<R><<<blocks_for(sv.psync.nf, 128, sv.sm_count), 128, 0, sv.stream>>>(d, st, sv.psync);
     mark(sv, "k_sync_flux");
   }
   Range3 z = {0, N + 1, 0, N + 1, 0, nr + 1};
-  k_gather<<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, sv.st, z);
+  k_gather<R><<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, st, z);
   mark(sv, "k_gather");
 }
 
-void launch_sources(Solve& sv) {
+void launch_fluxes(Solve& sv) {
+  if (sv.fp32)
+    launch_fluxes_t(sv, sv.stF);
+  else
+    launch_fluxes_t(sv, sv.st);
+}
+
+template <typename R>
+void launch_sources_t(Solve& sv, DStateT<R>& st) {
   if (!(sv.ph.gm > sv.p.smallnum)) return;
   const Dims& d = sv.d;
   Range3 z = {0, d.N + 1, 0, d.N + 1, 0, d.nr + 1};
-  k_sources<<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, z);
+  k_sources<R><<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, z);
   mark(sv, "k_sources");
+}
+
+void launch_sources(Solve& sv) {
+  if (sv.fp32)
+    launch_sources_t(sv, sv.stF);
+  else
+    launch_sources_t(sv, sv.st);
 }
 
 }  // namespace cs

@@ -19,26 +19,28 @@ namespace {
 
 constexpr int TPB = 128;
 
-__device__ __forceinline__ double& Vat(const DState& s, const Dims& d, int comp, int mode, int p, int i, int j, int k) {
+template <typename R>
+__device__ __forceinline__ R& Vat(const DStateT<R>& s, const Dims& d, int comp, int mode, int p, int i, int j, int k) {
   return s.V[d.at(mode * NVAR + comp, p, i, j, k)];
 }
 
 // STEP 2 (zone part, 421:597-635) and STEP 5 (421:1497-1628).
-__global__ void k_prim(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
+template <typename R>
+__global__ void k_prim(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
     r.decode(t, p, i, j, k);
     const int m = mask_at(g, d, p, i, j);
-    double U[8], V[8];
+    R U[8], V[8];
 #pragma unroll
     for (int c = 0; c < 8; ++c) U[c] = s.U[d.at(c, p, i, j, k)];
     if (m == 0) {
 #pragma unroll
-      for (int c = 0; c < 8; ++c) U[c] = 0.0;
-      U[0] = ph.rhofloor;
-      U[4] = ph.prsfloor / (ph.gamma - 1.0);
+      for (int c = 0; c < 8; ++c) U[c] = R(0.0);
+      U[0] = R(ph.rhofloor);
+      U[4] = R(ph.prsfloor) / (R(ph.gamma) - R(1.0));
     }
-    double en = s.ent[d.at(0, p, i, j, k)];
+    R en = s.ent[d.at(0, p, i, j, k)];
     d_cons_to_prim(ph, en, U, V);
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
@@ -46,21 +48,22 @@ __global__ void k_prim(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
       s.V[d.at(c, p, i, j, k)] = V[c];
     }
     s.ent[d.at(0, p, i, j, k)] = en;
-    s.ent[d.at(1, p, i, j, k)] = 0.0;
-    s.ent[d.at(2, p, i, j, k)] = 0.0;
-    s.ent[d.at(3, p, i, j, k)] = 0.0;
+    s.ent[d.at(1, p, i, j, k)] = R(0.0);
+    s.ent[d.at(2, p, i, j, k)] = R(0.0);
+    s.ent[d.at(3, p, i, j, k)] = R(0.0);
     // Modes 2..10 stay zero wherever the P12 steps do not write them.
     const int lo = 3 - d.G, hx = d.N + d.G - 2, hz = d.nr + d.G - 2;
     const bool full = m == 1 && i >= lo && i <= hx && j >= lo && j <= hx && k >= lo && k <= hz;
     if (!full)
-      for (int q = NVAR; q < NVAR * NMODE; ++q) s.V[d.at(q, p, i, j, k)] = 0.0;
-    const double a12 = (V[5] * V[5] + V[6] * V[6] + V[7] * V[7]) * ph.ob4pi;
-    s.msonic[d.at(0, p, i, j, k)] = sqrt((ph.gamma * V[4] + a12) / V[0]);
+      for (int q = NVAR; q < NVAR * NMODE; ++q) s.V[d.at(q, p, i, j, k)] = R(0.0);
+    const R a12 = (V[5] * V[5] + V[6] * V[6] + V[7] * V[7]) * R(ph.ob4pi);
+    s.msonic[d.at(0, p, i, j, k)] = sqrt((R(ph.gamma) * V[4] + a12) / V[0]);
   }
 }
 
 // Masked-face zeroing (421:658-759; 485:383-484).
-__global__ void k_zero_masked_faces(Dims d, DGeom g, DState s, Range3 r) {
+template <typename R>
+__global__ void k_zero_masked_faces(Dims d, DGeom g, DStateT<R> s, Range3 r) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
     r.decode(t, p, i, j, k);
@@ -75,7 +78,8 @@ __global__ void k_zero_masked_faces(Dims d, DGeom g, DState s, Range3 r) {
 
 // Tri-corner face-B synchronisation (421:779-962; 485:504-687).  One
 // thread per (panel, corner, ghost column, k).
-__global__ void k_tricorner(Dims d, DGeom g, DState s) {
+template <typename R>
+__global__ void k_tricorner(Dims d, DGeom g, DStateT<R> s) {
   const long long n = 6LL * 4 * d.G * (d.NK - 1);
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
     long long u = t;
@@ -123,56 +127,57 @@ __global__ void k_tricorner(Dims d, DGeom g, DState s) {
 }
 
 // STEP 6.a (421:1837-2131): velocity divergence and the divergence flattener.
-__global__ void k_flat_a(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
+template <typename R>
+__global__ void k_flat_a(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
     r.decode(t, p, i, j, k);
     const int lo = 2 - d.G, hx = d.N + d.G - 1, hz = d.nr + d.G - 1;
-    double fl = 0.0;
+    R fl = R(0.0);
     if (i >= lo && i <= hx && j >= lo && j <= hx && k >= lo && k <= hz) {
       const int xr = sten(g, d, p, i, j, 0, 0), yr = sten(g, d, p, i, j, 0, 1);
       const int xl = sten(g, d, p, i, j, 1, 0), yl = sten(g, d, p, i, j, 1, 1);
       const int xu = sten(g, d, p, i, j, 2, 0), yu = sten(g, d, p, i, j, 2, 1);
       const int xd = sten(g, d, p, i, j, 3, 0), yd = sten(g, d, p, i, j, 3, 1);
-      const double obl0 = 1.0 / fmax(geo(g, d, CS_G_V_SCALE, 0, p, i, j, k), ph.smallnum);
-      const double* ms = s.msonic;
-      double w = ms[d.at(0, p, i, j, k)];
+      const R obl0 = R(1.0) / fmax(geoR<R>(g, d, CS_G_V_SCALE, 0, p, i, j, k), R(ph.smallnum));
+      const R* ms = s.msonic;
+      R w = ms[d.at(0, p, i, j, k)];
       w = fmin(w, ms[d.at(0, p, xr, yr, k)]);
       w = fmin(w, ms[d.at(0, p, xl, yl, k)]);
       w = fmin(w, ms[d.at(0, p, xu, yu, k)]);
       w = fmin(w, ms[d.at(0, p, xd, yd, k)]);
       w = fmin(w, ms[d.at(0, p, i, j, k + 1)]);
       w = fmin(w, ms[d.at(0, p, i, j, k - 1)]);
-      double dv = 0.0;
-      auto term = [&](int ax, int ay, int az, int bx, int by, int bz, double nx, double ny, double nz) {
-        const double x = (geo(g, d, CS_G_V_CEN, 0, p, bx, by, bz) - geo(g, d, CS_G_V_CEN, 0, p, ax, ay, az)) * obl0;
-        const double y = (geo(g, d, CS_G_V_CEN, 1, p, bx, by, bz) - geo(g, d, CS_G_V_CEN, 1, p, ax, ay, az)) * obl0;
-        const double z = (geo(g, d, CS_G_V_CEN, 2, p, bx, by, bz) - geo(g, d, CS_G_V_CEN, 2, p, ax, ay, az)) * obl0;
-        const double a11 = 0.5 / fmax(sqrt(x * x + y * y + z * z), ph.smallnum);
+      R dv = R(0.0);
+      auto term = [&](int ax, int ay, int az, int bx, int by, int bz, R nx, R ny, R nz) {
+        const R x = (geoR<R>(g, d, CS_G_V_CEN, 0, p, bx, by, bz) - geoR<R>(g, d, CS_G_V_CEN, 0, p, ax, ay, az)) * obl0;
+        const R y = (geoR<R>(g, d, CS_G_V_CEN, 1, p, bx, by, bz) - geoR<R>(g, d, CS_G_V_CEN, 1, p, ax, ay, az)) * obl0;
+        const R z = (geoR<R>(g, d, CS_G_V_CEN, 2, p, bx, by, bz) - geoR<R>(g, d, CS_G_V_CEN, 2, p, ax, ay, az)) * obl0;
+        const R a11 = R(0.5) / fmax(sqrt(x * x + y * y + z * z), R(ph.smallnum));
         dv = dv + nx * a11 * (Vat(s, d, 1, 0, p, bx, by, bz) - Vat(s, d, 1, 0, p, ax, ay, az)) +
              ny * a11 * (Vat(s, d, 2, 0, p, bx, by, bz) - Vat(s, d, 2, 0, p, ax, ay, az)) +
              nz * a11 * (Vat(s, d, 3, 0, p, bx, by, bz) - Vat(s, d, 3, 0, p, ax, ay, az));
       };
-      term(i, j, k, xr, yr, k, geo(g, d, CS_G_XF_N, 0, p, i, j, k), geo(g, d, CS_G_XF_N, 1, p, i, j, k),
-           geo(g, d, CS_G_XF_N, 2, p, i, j, k));
-      term(xl, yl, k, i, j, k, geo(g, d, CS_G_XF_N, 0, p, i - 1, j, k), geo(g, d, CS_G_XF_N, 1, p, i - 1, j, k),
-           geo(g, d, CS_G_XF_N, 2, p, i - 1, j, k));
-      term(i, j, k, xu, yu, k, geo(g, d, CS_G_YF_N, 0, p, i, j, k), geo(g, d, CS_G_YF_N, 1, p, i, j, k),
-           geo(g, d, CS_G_YF_N, 2, p, i, j, k));
-      term(xd, yd, k, i, j, k, geo(g, d, CS_G_YF_N, 0, p, i, j - 1, k), geo(g, d, CS_G_YF_N, 1, p, i, j - 1, k),
-           geo(g, d, CS_G_YF_N, 2, p, i, j - 1, k));
-      double nx = geo(g, d, CS_G_ZF_CEN, 0, p, i, j, k), ny = geo(g, d, CS_G_ZF_CEN, 1, p, i, j, k),
-             nz = geo(g, d, CS_G_ZF_CEN, 2, p, i, j, k);
-      const double a12 = 1.0 / fmax(sqrt(nx * nx + ny * ny + nz * nz), ph.smallnum);
+      term(i, j, k, xr, yr, k, geoR<R>(g, d, CS_G_XF_N, 0, p, i, j, k), geoR<R>(g, d, CS_G_XF_N, 1, p, i, j, k),
+           geoR<R>(g, d, CS_G_XF_N, 2, p, i, j, k));
+      term(xl, yl, k, i, j, k, geoR<R>(g, d, CS_G_XF_N, 0, p, i - 1, j, k), geoR<R>(g, d, CS_G_XF_N, 1, p, i - 1, j, k),
+           geoR<R>(g, d, CS_G_XF_N, 2, p, i - 1, j, k));
+      term(i, j, k, xu, yu, k, geoR<R>(g, d, CS_G_YF_N, 0, p, i, j, k), geoR<R>(g, d, CS_G_YF_N, 1, p, i, j, k),
+           geoR<R>(g, d, CS_G_YF_N, 2, p, i, j, k));
+      term(xd, yd, k, i, j, k, geoR<R>(g, d, CS_G_YF_N, 0, p, i, j - 1, k), geoR<R>(g, d, CS_G_YF_N, 1, p, i, j - 1, k),
+           geoR<R>(g, d, CS_G_YF_N, 2, p, i, j - 1, k));
+      R nx = geoR<R>(g, d, CS_G_ZF_CEN, 0, p, i, j, k), ny = geoR<R>(g, d, CS_G_ZF_CEN, 1, p, i, j, k),
+             nz = geoR<R>(g, d, CS_G_ZF_CEN, 2, p, i, j, k);
+      const R a12 = R(1.0) / fmax(sqrt(nx * nx + ny * ny + nz * nz), R(ph.smallnum));
       nx = nx * a12;
       ny = ny * a12;
       nz = nz * a12;
       term(i, j, k, i, j, k + 1, nx, ny, nz);
       term(i, j, k - 1, i, j, k, nx, ny, nz);
-      double a13 = fabs(dv) / (ph.flatten_coef * w);
-      a13 = a13 - 1.0;
-      fl = (a13 <= 0.0) ? 0.0 : fmin(1.0, a13);
-      if (mask_at(g, d, p, i, j) != 1) fl = 0.0;
+      R a13 = fabs(dv) / (R(ph.flatten_coef) * w);
+      a13 = a13 - R(1.0);
+      fl = (a13 <= R(0.0)) ? R(0.0) : fmin(R(1.0), a13);
+      if (mask_at(g, d, p, i, j) != 1) fl = R(0.0);
     }
     s.flatA[d.at(0, p, i, j, k)] = fl;
   }
@@ -180,12 +185,13 @@ __global__ void k_flat_a(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
 
 // STEP 6.b (pressure-ratio raise, pass 0) and 6.c (upwinding, pass 1),
 // 421:2150-2458: dst(self) = max over the six neighbours of src.
-__global__ void k_flat_bc(Dims d, PhysC ph, DGeom g, DState s, Range3 r, const double* src, double* dst, int pass) {
+template <typename R>
+__global__ void k_flat_bc(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r, const R* src, R* dst, int pass) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
     r.decode(t, p, i, j, k);
     const int lo = 2 - d.G, hx = d.N + d.G - 1, hz = d.nr + d.G - 1;
-    double fl = src[d.at(0, p, i, j, k)];
+    R fl = src[d.at(0, p, i, j, k)];
     if (i >= lo && i <= hx && j >= lo && j <= hx && k >= lo && k <= hz) {
       int xs[6], ys[6];
 #pragma unroll
@@ -196,10 +202,10 @@ __global__ void k_flat_bc(Dims d, PhysC ph, DGeom g, DState s, Range3 r, const d
       xs[4] = xs[5] = i;
       ys[4] = ys[5] = j;
       const int zs[6] = {k, k, k, k, k + 1, k - 1};
-      const double p0 = Vat(s, d, 4, 0, p, i, j, k);
+      const R p0 = Vat(s, d, 4, 0, p, i, j, k);
 #pragma unroll
       for (int w = 0; w < 6; ++w) {
-        const bool take = pass == 1 || (Vat(s, d, 4, 0, p, xs[w], ys[w], zs[w]) > ph.prs_flatten_coef * p0);
+        const bool take = pass == 1 || (Vat(s, d, 4, 0, p, xs[w], ys[w], zs[w]) > R(ph.prs_flatten_coef) * p0);
         if (take) fl = fmax(fl, src[d.at(0, p, xs[w], ys[w], zs[w])]);
       }
     }
@@ -226,25 +232,26 @@ __device__ __forceinline__ Nbr12 load_nbr(const DGeom& g, const Dims& d, int p, 
   return n;
 }
 
+template <typename R>
 __device__ void stencil_inv(const Dims& d, const PhysC& ph, const DGeom& g, int p, int i, int j, int k, const Nbr12& n,
-                            double Ai[8][9]) {
-  const double obl0 = 1.0 / fmax(geo(g, d, CS_G_V_SCALE, 0, p, i, j, k), ph.smallnum);
-  const double cx = geo(g, d, CS_G_V_CEN, 0, p, i, j, k), cy = geo(g, d, CS_G_V_CEN, 1, p, i, j, k),
-               cz = geo(g, d, CS_G_V_CEN, 2, p, i, j, k);
+                            R Ai[8][9]) {
+  const R obl0 = R(1.0) / fmax(geoR<R>(g, d, CS_G_V_SCALE, 0, p, i, j, k), R(ph.smallnum));
+  const R cx = geoR<R>(g, d, CS_G_V_CEN, 0, p, i, j, k), cy = geoR<R>(g, d, CS_G_V_CEN, 1, p, i, j, k),
+               cz = geoR<R>(g, d, CS_G_V_CEN, 2, p, i, j, k);
 #pragma unroll
   for (int st = 0; st < 8; ++st) {
     const int w1 = c_st8[st][0], w2 = c_st8[st][1], dz = c_st8[st][2];
-    const double a11 = (geo(g, d, CS_G_V_CEN, 0, p, n.x[w1], n.y[w1], k) - cx) * obl0;
-    const double a12 = (geo(g, d, CS_G_V_CEN, 1, p, n.x[w1], n.y[w1], k) - cy) * obl0;
-    const double a13 = (geo(g, d, CS_G_V_CEN, 2, p, n.x[w1], n.y[w1], k) - cz) * obl0;
-    const double a21 = (geo(g, d, CS_G_V_CEN, 0, p, n.x[w2], n.y[w2], k) - cx) * obl0;
-    const double a22 = (geo(g, d, CS_G_V_CEN, 1, p, n.x[w2], n.y[w2], k) - cy) * obl0;
-    const double a23 = (geo(g, d, CS_G_V_CEN, 2, p, n.x[w2], n.y[w2], k) - cz) * obl0;
-    const double a31 = (geo(g, d, CS_G_V_CEN, 0, p, i, j, k + dz) - cx) * obl0;
-    const double a32 = (geo(g, d, CS_G_V_CEN, 1, p, i, j, k + dz) - cy) * obl0;
-    const double a33 = (geo(g, d, CS_G_V_CEN, 2, p, i, j, k + dz) - cz) * obl0;
-    double ob = (-a13 * a22 * a31 + a12 * a23 * a31 + a13 * a21 * a32 - a11 * a23 * a32 - a12 * a21 * a33 + a11 * a22 * a33);
-    ob = copysign(1.0, ob) / fmax(1.0e-32, fabs(ob));
+    const R a11 = (geoR<R>(g, d, CS_G_V_CEN, 0, p, n.x[w1], n.y[w1], k) - cx) * obl0;
+    const R a12 = (geoR<R>(g, d, CS_G_V_CEN, 1, p, n.x[w1], n.y[w1], k) - cy) * obl0;
+    const R a13 = (geoR<R>(g, d, CS_G_V_CEN, 2, p, n.x[w1], n.y[w1], k) - cz) * obl0;
+    const R a21 = (geoR<R>(g, d, CS_G_V_CEN, 0, p, n.x[w2], n.y[w2], k) - cx) * obl0;
+    const R a22 = (geoR<R>(g, d, CS_G_V_CEN, 1, p, n.x[w2], n.y[w2], k) - cy) * obl0;
+    const R a23 = (geoR<R>(g, d, CS_G_V_CEN, 2, p, n.x[w2], n.y[w2], k) - cz) * obl0;
+    const R a31 = (geoR<R>(g, d, CS_G_V_CEN, 0, p, i, j, k + dz) - cx) * obl0;
+    const R a32 = (geoR<R>(g, d, CS_G_V_CEN, 1, p, i, j, k + dz) - cy) * obl0;
+    const R a33 = (geoR<R>(g, d, CS_G_V_CEN, 2, p, i, j, k + dz) - cz) * obl0;
+    R ob = (-a13 * a22 * a31 + a12 * a23 * a31 + a13 * a21 * a32 - a11 * a23 * a32 - a12 * a21 * a33 + a11 * a22 * a33);
+    ob = copysign(R(1.0), ob) / fmax(R(1.0e-32), fabs(ob));
     Ai[st][0] = (-a23 * a32 + a22 * a33) * ob;
     Ai[st][1] = (a13 * a32 - a12 * a33) * ob;
     Ai[st][2] = (-a13 * a22 + a12 * a23) * ob;
@@ -258,26 +265,30 @@ __device__ void stencil_inv(const Dims& d, const PhysC& ph, const DGeom& g, int 
 }
 
 // WENO of the eight linear stencils plus their mean (weight 100).
-__device__ void weno8(const Dims& d, const PhysC& ph, int p, int i, int j, int k, const Nbr12& n, const double Ai[8][9],
-                      const double* f, long long cstride_off, double gr[3]) {
-  const double f0 = f[cstride_off + d.idx(i, j, k)];
-  double X[3][9];
+template <typename R>
+__device__ void weno8(const Dims& d, const PhysC& ph, int p, int i, int j, int k, const Nbr12& n, const R Ai[8][9],
+                      const R* f, long long cstride_off, R gr[3]) {
+  const R f0 = f[cstride_off + d.idx(i, j, k)];
+  R X[3][9];
 #pragma unroll
   for (int st = 0; st < 8; ++st) {
     const int w1 = c_st8[st][0], w2 = c_st8[st][1], dz = c_st8[st][2];
-    const double R0 = f[cstride_off + d.idx(n.x[w1], n.y[w1], k)] - f0;
-    const double R1 = f[cstride_off + d.idx(n.x[w2], n.y[w2], k)] - f0;
-    const double R2 = f[cstride_off + d.idx(i, j, k + dz)] - f0;
+    const R R0 = f[cstride_off + d.idx(n.x[w1], n.y[w1], k)] - f0;
+    const R R1 = f[cstride_off + d.idx(n.x[w2], n.y[w2], k)] - f0;
+    const R R2 = f[cstride_off + d.idx(i, j, k + dz)] - f0;
 #pragma unroll
     for (int rr = 0; rr < 3; ++rr) X[rr][st] = Ai[st][rr * 3 + 0] * R0 + Ai[st][rr * 3 + 1] * R1 + Ai[st][rr * 3 + 2] * R2;
   }
 #pragma unroll
   for (int rr = 0; rr < 3; ++rr)
-    X[rr][8] = 0.125 * (X[rr][0] + X[rr][1] + X[rr][2] + X[rr][3] + X[rr][4] + X[rr][5] + X[rr][6] + X[rr][7]);
+    X[rr][8] = R(0.125) * (X[rr][0] + X[rr][1] + X[rr][2] + X[rr][3] + X[rr][4] + X[rr][5] + X[rr][6] + X[rr][7]);
+  // The nonlinear weights (IS + eps)^-4 span far more than the FP32 range,
+  // so they are formed in FP64 in every form.
   double W[9];
 #pragma unroll
   for (int st = 0; st < 9; ++st) {
-    const double IS = X[0][st] * X[0][st] + X[1][st] * X[1][st] + X[2][st] * X[2][st];
+    const double x0 = X[0][st], x1 = X[1][st], x2 = X[2][st];
+    const double IS = x0 * x0 + x1 * x1 + x2 * x2;
     const double t = IS + ph.smallnum;
     const double t2 = t * t;
     W[st] = (st < 8 ? 1.0 : 100.0) / (t2 * t2);
@@ -287,77 +298,81 @@ __device__ void weno8(const Dims& d, const PhysC& ph, int p, int i, int j, int k
   for (int st = 0; st < 9; ++st) W[st] = W[st] * a11;
 #pragma unroll
   for (int rr = 0; rr < 3; ++rr) {
-    double t = W[0] * X[rr][0];
+    double t = W[0] * (double)X[rr][0];
 #pragma unroll
-    for (int st = 1; st < 9; ++st) t = t + W[st] * X[rr][st];
-    gr[rr] = t;
+    for (int st = 1; st < 9; ++st) t = t + W[st] * (double)X[rr][st];
+    gr[rr] = (R)t;
   }
 }
 
 // STEP 7.a (421:2515-3804): linear WENO slopes of the 8 primitives and the entropy.
-__global__ void k_weno7a(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
+template <typename R>
+__global__ void k_weno7a(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
     r.decode(t, p, i, j, k);
     if (mask_at(g, d, p, i, j) != 1) continue;
     const Nbr12 n = load_nbr(g, d, p, i, j);
-    double Ai[8][9];
+    R Ai[8][9];
     stencil_inv(d, ph, g, p, i, j, k, n, Ai);
     for (int q = 0; q < NVAR; ++q) {
-      double gr[3];
+      R gr[3];
       weno8(d, ph, p, i, j, k, n, Ai, s.V, ((long long)(0 * NVAR + q) * NPANEL + p) * d.S, gr);
       Vat(s, d, q, 1, p, i, j, k) = gr[0];
       Vat(s, d, q, 2, p, i, j, k) = gr[1];
       Vat(s, d, q, 3, p, i, j, k) = gr[2];
     }
-    double gr[3];
+    R gr[3];
     weno8(d, ph, p, i, j, k, n, Ai, s.ent, (long long)p * d.S, gr);
-    const double om = 1.0 - s.flatA[d.at(0, p, i, j, k)];
+    const R om = R(1.0) - s.flatA[d.at(0, p, i, j, k)];
     s.ent[d.at(1, p, i, j, k)] = gr[0] * om;
     s.ent[d.at(2, p, i, j, k)] = gr[1] * om;
     s.ent[d.at(3, p, i, j, k)] = gr[2] * om;
   }
 }
 
-__device__ __forceinline__ void coef10(const DGeom& g, const Dims& d, int p, int i, int j, int k, double* c) {
+template <typename R>
+__device__ __forceinline__ void coef10(const DGeom& g, const Dims& d, int p, int i, int j, int k, R* c) {
 #pragma unroll
-  for (int t = 0; t < 10; ++t) c[t] = geo(g, d, CS_G_COEF, t, p, i, j, k);
+  for (int t = 0; t < 10; ++t) c[t] = geoR<R>(g, d, CS_G_COEF, t, p, i, j, k);
 }
 
 // Row rr of the 18 x 9 least-squares matrix of STEP 7.b (421:3869-4001)
 // for zone (i,j,k): neighbour centroid offsets scaled by l0, quadratic
 // modes corrected by the neighbour's own moments.
+template <typename R>
 __device__ __forceinline__ void w7b_row(const Dims& d, const PhysC& ph, const DGeom& g, int p, int i, int j, int k,
-                                        const Nbr12& n, int rr, double cx, double cy, double cz, double l0, double obl0,
-                                        const double* c0, double* A, long long& off) {
+                                        const Nbr12& n, int rr, R cx, R cy, R cz, R l0, R obl0,
+                                        const R* c0, R* A, long long& off) {
   const int w = c_n18[rr][0], dz = c_n18[rr][1];
   const int zx = w < 0 ? i : n.x[w], zy = w < 0 ? j : n.y[w], zz = k + dz;
   off = d.idx(zx, zy, zz);
-  const double x = (geo(g, d, CS_G_V_CEN, 0, p, zx, zy, zz) - cx) * obl0;
-  const double y = (geo(g, d, CS_G_V_CEN, 1, p, zx, zy, zz) - cy) * obl0;
-  const double z = (geo(g, d, CS_G_V_CEN, 2, p, zx, zy, zz) - cz) * obl0;
-  const double lj = fmax(geo(g, d, CS_G_V_SCALE, 0, p, zx, zy, zz), ph.smallnum);
-  const double rt = lj / l0, r2 = rt * rt;
+  const R x = (geoR<R>(g, d, CS_G_V_CEN, 0, p, zx, zy, zz) - cx) * obl0;
+  const R y = (geoR<R>(g, d, CS_G_V_CEN, 1, p, zx, zy, zz) - cy) * obl0;
+  const R z = (geoR<R>(g, d, CS_G_V_CEN, 2, p, zx, zy, zz) - cz) * obl0;
+  const R lj = fmax(geoR<R>(g, d, CS_G_V_SCALE, 0, p, zx, zy, zz), R(ph.smallnum));
+  const R rt = lj / l0, r2 = rt * rt;
   A[0] = x;
   A[1] = y;
   A[2] = z;
-  A[3] = x * x - c0[4] + geo(g, d, CS_G_COEF, 4, p, zx, zy, zz) * r2;
-  A[4] = y * y - c0[5] + geo(g, d, CS_G_COEF, 5, p, zx, zy, zz) * r2;
-  A[5] = z * z - c0[6] + geo(g, d, CS_G_COEF, 6, p, zx, zy, zz) * r2;
-  A[6] = x * y - c0[7] + geo(g, d, CS_G_COEF, 7, p, zx, zy, zz) * r2;
-  A[7] = y * z - c0[8] + geo(g, d, CS_G_COEF, 8, p, zx, zy, zz) * r2;
-  A[8] = x * z - c0[9] + geo(g, d, CS_G_COEF, 9, p, zx, zy, zz) * r2;
+  A[3] = x * x - c0[4] + geoR<R>(g, d, CS_G_COEF, 4, p, zx, zy, zz) * r2;
+  A[4] = y * y - c0[5] + geoR<R>(g, d, CS_G_COEF, 5, p, zx, zy, zz) * r2;
+  A[5] = z * z - c0[6] + geoR<R>(g, d, CS_G_COEF, 6, p, zx, zy, zz) * r2;
+  A[6] = x * y - c0[7] + geoR<R>(g, d, CS_G_COEF, 7, p, zx, zy, zz) * r2;
+  A[7] = y * z - c0[8] + geoR<R>(g, d, CS_G_COEF, 8, p, zx, zy, zz) * r2;
+  A[8] = x * z - c0[9] + geoR<R>(g, d, CS_G_COEF, 9, p, zx, zy, zz) * r2;
 }
 
 // Inverse of the 9 x 9 normal matrix A^T A of STEP 7.b for one zone.
+template <typename R>
 __device__ __forceinline__ void w7b_minv(const Dims& d, const PhysC& ph, const DGeom& g, int p, int i, int j, int k,
-                                         const Nbr12& n, double cx, double cy, double cz, double l0, double obl0,
-                                         const double* c0, double* Minv) {
-  double M[81];
+                                         const Nbr12& n, R cx, R cy, R cz, R l0, R obl0,
+                                         const R* c0, R* Minv) {
+  R M[81];
 #pragma unroll
-  for (int t = 0; t < 81; ++t) M[t] = 0.0;
+  for (int t = 0; t < 81; ++t) M[t] = R(0.0);
   for (int rr = 0; rr < 18; ++rr) {
-    double A[9];
+    R A[9];
     long long off;
     w7b_row(d, ph, g, p, i, j, k, n, rr, cx, cy, cz, l0, obl0, c0, A, off);
 #pragma unroll
@@ -377,84 +392,84 @@ __device__ __forceinline__ void w7b_minv(const Dims& d, const PhysC& ph, const D
 // kCached the inverse normal matrix (geometry only) comes from the
 // operator cache built at mesh build; the result is the same either way.
 constexpr int W7B_QG = NVAR;
-template <bool kCached>
-__global__ void __launch_bounds__(TPB) k_weno7b(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
-  const double ob12 = 1.0 / 12.0, ob180 = 1.0 / 180.0, ob144 = 1.0 / 144.0;
+template <bool kCached, typename R>
+__global__ void __launch_bounds__(TPB) k_weno7b(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
+  const R ob12 = R(1.0) / R(12.0), ob180 = R(1.0) / R(180.0), ob144 = R(1.0) / R(144.0);
   const long long nr_ = r.count();
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nr_; t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
     r.decode(t, p, i, j, k);
     if (mask_at(g, d, p, i, j) != 1) continue;
     const Nbr12 n = load_nbr(g, d, p, i, j);
-    const double l0 = fmax(geo(g, d, CS_G_V_SCALE, 0, p, i, j, k), ph.smallnum), obl0 = 1.0 / l0;
-    double c0[10];
+    const R l0 = fmax(geoR<R>(g, d, CS_G_V_SCALE, 0, p, i, j, k), R(ph.smallnum)), obl0 = R(1.0) / l0;
+    R c0[10];
     coef10(g, d, p, i, j, k, c0);
-    const double cx = geo(g, d, CS_G_V_CEN, 0, p, i, j, k), cy = geo(g, d, CS_G_V_CEN, 1, p, i, j, k),
-                 cz = geo(g, d, CS_G_V_CEN, 2, p, i, j, k);
+    const R cx = geoR<R>(g, d, CS_G_V_CEN, 0, p, i, j, k), cy = geoR<R>(g, d, CS_G_V_CEN, 1, p, i, j, k),
+                 cz = geoR<R>(g, d, CS_G_V_CEN, 2, p, i, j, k);
     // kCached: the inverse is read from the cache where it is used (L1
     // serves the re-reads of the later components).
-    double Minv[kCached ? 1 : 81];
+    R Minv[kCached ? 1 : 81];
     if (!kCached) w7b_minv(d, ph, g, p, i, j, k, n, cx, cy, cz, l0, obl0, c0, Minv);
     const double* mc = s.op_m9 + t;
-    auto MI = [&](int e) { return kCached ? __ldg(mc + (long long)e * nr_) : Minv[kCached ? 0 : e]; };
-    const double f = s.flatA[d.at(0, p, i, j, k)];
-    const double betalo = f + (1.0 - f) * 2.0;
-    const double ghi = f * 0.6 + (1.0 - f) * 0.95, glo = 1.0 - ghi, obghi = 1.0 / ghi, grat = glo / ghi;
+    auto MI = [&](int e) { return kCached ? (R)__ldg(mc + (long long)e * nr_) : Minv[kCached ? 0 : e]; };
+    const R f = s.flatA[d.at(0, p, i, j, k)];
+    const R betalo = f + (R(1.0) - f) * R(2.0);
+    const R ghi = f * R(0.6) + (R(1.0) - f) * R(0.95), glo = R(1.0) - ghi, obghi = R(1.0) / ghi, grat = glo / ghi;
     // The primitives go in groups of W7B_QG, each group rebuilding the
     // matrix rows; on B200 one group of all eight is faster than smaller
     // groups (the row rebuild costs more than the extra live sums).  Every
     // component's sums run over the rows in the same order either way.
 #pragma unroll 1
     for (int q0 = 0; q0 < NVAR; q0 += W7B_QG) {
-      double v0[W7B_QG];
+      R v0[W7B_QG];
 #pragma unroll
       for (int qq = 0; qq < W7B_QG; ++qq) v0[qq] = s.V[((long long)(q0 + qq) * NPANEL + p) * d.S + d.idx(i, j, k)];
-      double Y[W7B_QG][9];
+      R Y[W7B_QG][9];
 #pragma unroll
       for (int qq = 0; qq < W7B_QG; ++qq)
 #pragma unroll
-        for (int a = 0; a < 9; ++a) Y[qq][a] = 0.0;
+        for (int a = 0; a < 9; ++a) Y[qq][a] = R(0.0);
 #pragma unroll 1
       for (int rr = 0; rr < 18; ++rr) {
-        double A[9];
+        R A[9];
         long long off;
         w7b_row(d, ph, g, p, i, j, k, n, rr, cx, cy, cz, l0, obl0, c0, A, off);
 #pragma unroll
         for (int qq = 0; qq < W7B_QG; ++qq) {
-          const double R = s.V[((long long)(q0 + qq) * NPANEL + p) * d.S + off] - v0[qq];
+          const R Rv = s.V[((long long)(q0 + qq) * NPANEL + p) * d.S + off] - v0[qq];
 #pragma unroll
-          for (int a = 0; a < 9; ++a) Y[qq][a] = Y[qq][a] + A[a] * R;
+          for (int a = 0; a < 9; ++a) Y[qq][a] = Y[qq][a] + A[a] * Rv;
         }
       }
 #pragma unroll 1
       for (int qq = 0; qq < W7B_QG; ++qq) {
         const int q = q0 + qq;
-        double X[9];
+        R X[9];
 #pragma unroll
         for (int a = 0; a < 9; ++a) {
-          double sacc = 0.0;
+          R sacc = R(0.0);
 #pragma unroll
           for (int b = 0; b < 9; ++b) sacc = sacc + MI(a * 9 + b) * Y[qq][b];
           X[a] = sacc;
         }
-        const double v2 = Vat(s, d, q, 1, p, i, j, k), v3 = Vat(s, d, q, 2, p, i, j, k), v4 = Vat(s, d, q, 3, p, i, j, k);
-        const double ISlo = betalo * (v2 * v2 + v3 * v3 + v4 * v4) * ob12;
-        double Phi[9];
+        const R v2 = Vat(s, d, q, 1, p, i, j, k), v3 = Vat(s, d, q, 2, p, i, j, k), v4 = Vat(s, d, q, 3, p, i, j, k);
+        const R ISlo = betalo * (v2 * v2 + v3 * v3 + v4 * v4) * ob12;
+        R Phi[9];
         Phi[0] = X[0] * obghi - v2 * grat;
         Phi[1] = X[1] * obghi - v3 * grat;
         Phi[2] = X[2] * obghi - v4 * grat;
 #pragma unroll
         for (int a = 3; a < 9; ++a) Phi[a] = X[a] * obghi;
-        const double IShi = (Phi[0] * Phi[0] + Phi[1] * Phi[1] + Phi[2] * Phi[2]) * ob12 +
+        const R IShi = (Phi[0] * Phi[0] + Phi[1] * Phi[1] + Phi[2] * Phi[2]) * ob12 +
                             (Phi[3] * Phi[3]) * (sqr(c0[4] - ob12) + ob180) + (Phi[4] * Phi[4]) * (sqr(c0[5] - ob12) + ob180) +
                             (Phi[5] * Phi[5]) * (sqr(c0[6] - ob12) + ob180) + (Phi[6] * Phi[6]) * (c0[7] * c0[7] + ob144) +
                             (Phi[7] * Phi[7]) * (c0[8] * c0[8] + ob144) + (Phi[8] * Phi[8]) * (c0[9] * c0[9] + ob144);
-        const double tau = fabs(IShi - ISlo);
-        double Wlo = glo * (1.0 + tau / (ISlo + ph.smallnum)), Whi = ghi * (1.0 + tau / (IShi + ph.smallnum));
-        const double aa = 1.0 / (Wlo + Whi);
+        const R tau = fabs(IShi - ISlo);
+        R Wlo = glo * (R(1.0) + tau / (ISlo + R(ph.smallnum))), Whi = ghi * (R(1.0) + tau / (IShi + R(ph.smallnum)));
+        const R aa = R(1.0) / (Wlo + Whi);
         Wlo = Wlo * aa;
         Whi = Whi * aa;
-        const double x = 1.0 - f;
+        const R x = R(1.0) - f;
         Vat(s, d, q, 1, p, i, j, k) = (Whi * Phi[0] + Wlo * v2) * x;
         Vat(s, d, q, 2, p, i, j, k) = (Whi * Phi[1] + Wlo * v3) * x;
         Vat(s, d, q, 3, p, i, j, k) = (Whi * Phi[2] + Wlo * v4) * x;
@@ -465,7 +480,8 @@ __global__ void __launch_bounds__(TPB) k_weno7b(Dims d, PhysC ph, DGeom g, DStat
   }
 }
 
-__global__ void k_ops_m9(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
+template <typename R>
+__global__ void k_ops_m9(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
   const long long nr_ = r.count();
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nr_; t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
@@ -485,7 +501,8 @@ __global__ void k_ops_m9(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
 
 // STEP 7.c (440:204-829): shrink the higher modes until the 27 nodal
 // values of density, pressure and entropy lie in the expanded local range.
-__global__ void __launch_bounds__(TPB) k_positivity(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
+template <typename R>
+__global__ void __launch_bounds__(TPB) k_positivity(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
     r.decode(t, p, i, j, k);
@@ -602,7 +619,8 @@ __global__ void __launch_bounds__(TPB) k_positivity(Dims d, PhysC ph, DGeom g, D
 
 // A zone that exhausted the shrink passes also zeroes its entropy value
 // (440:569-575); applied after every zone has read its neighbours.
-__global__ void k_apply_giveup(Dims d, DState s, Range3 r) {
+template <typename R>
+__global__ void k_apply_giveup(Dims d, DStateT<R> s, Range3 r) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
     r.decode(t, p, i, j, k);
@@ -612,7 +630,8 @@ __global__ void k_apply_giveup(Dims d, DState s, Range3 r) {
 
 // STEP 8.a-c (421:4686-5567): B at the five quadrature points of each face,
 // averaged from both sides and shifted to the facial mean.
-__global__ void __launch_bounds__(TPB) k_faceB(Dims d, PhysC ph, DGeom g, DState s, Range3 r, int dir) {
+template <typename R>
+__global__ void __launch_bounds__(TPB) k_faceB(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r, int dir) {
   const int QP = dir == 0 ? CS_G_XF_QP : (dir == 1 ? CS_G_YF_QP : CS_G_ZF_QP);
   const int BW = dir == 0 ? CS_G_XB_QW : (dir == 1 ? CS_G_YB_QW : CS_G_ZB_QW);
   const int NF = dir == 0 ? CS_G_XF_N : (dir == 1 ? CS_G_YF_N : CS_G_ZF_N);
@@ -702,8 +721,8 @@ struct AdpSmem {
 
 // kFactorOnly: assemble and factor the geometry-only KKT matrix and store
 // the factors and the row permutation for k_adp_solve (once per mesh).
-template <bool kFactorOnly>
-__global__ void __launch_bounds__(32 * ADP_WARPS) k_adp(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
+template <bool kFactorOnly, typename R>
+__global__ void __launch_bounds__(32 * ADP_WARPS) k_adp(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
   extern __shared__ unsigned char smem_raw[];
   AdpSmem& S = reinterpret_cast<AdpSmem*>(smem_raw)[threadIdx.x / 32];
   const int lane = threadIdx.x & 31;
@@ -875,7 +894,7 @@ __global__ void __launch_bounds__(32 * ADP_WARPS) k_adp(Dims d, PhysC ph, DGeom 
     // 5. write back the modes, zone B and the energy adjustment
     if (lane < 30) Vat(s, d, 5 + lane / 10, lane % 10, p, i, j, k) = S.sol[lane];
     if (lane == 0) {
-      double* U = s.U;
+      R* U = s.U;
       const long long o5 = d.at(4, p, i, j, k);
       const double u6 = U[d.at(5, p, i, j, k)], u7 = U[d.at(6, p, i, j, k)], u8 = U[d.at(7, p, i, j, k)];
       const double aa = (u6 * u6 + u7 * u7 + u8 * u8) * ph.ob8pi;
@@ -928,7 +947,8 @@ __device__ __noinline__ void mbar_wait(uint64_t* bar, uint32_t parity, int* err)
 // forms the 36 entries (the same sums in the same order as k_adp) and
 // stores them element-major, [36][zones of the ADP range].
 constexpr int ADPR_TPB = 128;
-__global__ void __launch_bounds__(ADPR_TPB) k_adp_rhs(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
+template <typename R>
+__global__ void __launch_bounds__(ADPR_TPB) k_adp_rhs(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
   const long long n = r.count();
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
@@ -1003,7 +1023,8 @@ struct AdpsSmem {
   uint64_t empty[ADPS_NS];
 };
 
-__global__ void __launch_bounds__(ADPS_THREADS, 2) k_adp_solve(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
+template <typename R>
+__global__ void __launch_bounds__(ADPS_THREADS, 2) k_adp_solve(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
   extern __shared__ __align__(128) unsigned char adps_raw[];
   AdpsSmem& S = *reinterpret_cast<AdpsSmem*>(adps_raw);
   const int tid = threadIdx.x;
@@ -1084,7 +1105,7 @@ __global__ void __launch_bounds__(ADPS_THREADS, 2) k_adp_solve(Dims d, PhysC ph,
       if (mask_at(g, d, p, i, j) == 1) {
 #pragma unroll
         for (int a = 0; a < 30; ++a) Vat(s, d, 5 + a / 10, a % 10, p, i, j, k) = S.y[a][tid];
-        double* U = s.U;
+        R* U = s.U;
         const long long o5 = d.at(4, p, i, j, k);
         const double u6 = U[d.at(5, p, i, j, k)], u7 = U[d.at(6, p, i, j, k)], u8 = U[d.at(7, p, i, j, k)];
         const double aa = (u6 * u6 + u7 * u7 + u8 * u8) * ph.ob8pi;
@@ -1103,21 +1124,22 @@ __global__ void __launch_bounds__(ADPS_THREADS, 2) k_adp_solve(Dims d, PhysC ph,
 }
 
 // STEP 9.a (421:6700-6790): zone-centred E = -v x B from the point values.
-__global__ void k_efield_a(Dims d, DGeom g, DState s, Range3 r) {
+template <typename R>
+__global__ void k_efield_a(Dims d, DGeom g, DStateT<R> s, Range3 r) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
     r.decode(t, p, i, j, k);
-    double co[10];
+    R co[10];
     coef10(g, d, p, i, j, k, co);
-    double pv[8];
+    R pv[8];
     for (int q = 1; q < 8; ++q) {
       if (q == 4) continue;
-      double acc = Vat(s, d, q, 0, p, i, j, k);
+      R acc = Vat(s, d, q, 0, p, i, j, k);
       for (int m = 4; m < 10; ++m) acc = acc - Vat(s, d, q, m, p, i, j, k) * co[m];
       pv[q] = acc;
     }
-    const double vx = pv[1], vy = pv[2], vz = pv[3], Bx = pv[5], By = pv[6], Bz = pv[7];
-    const double ex = -(vy * Bz - vz * By), ey = -(vz * Bx - vx * Bz), ez = -(vx * By - vy * Bx);
+    const R vx = pv[1], vy = pv[2], vz = pv[3], Bx = pv[5], By = pv[6], Bz = pv[7];
+    const R ex = -(vy * Bz - vz * By), ey = -(vz * Bx - vx * Bz), ez = -(vx * By - vy * Bx);
     s.E[d.at(0, p, i, j, k)] = ex;
     s.E[d.at(1, p, i, j, k)] = ey;
     s.E[d.at(2, p, i, j, k)] = ez;
@@ -1128,16 +1150,17 @@ __global__ void k_efield_a(Dims d, DGeom g, DState s, Range3 r) {
 }
 
 // STEP 9.b (421:6840-8400): linear WENO slopes of the E point values.
-__global__ void k_efield_b(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
+template <typename R>
+__global__ void k_efield_b(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
     r.decode(t, p, i, j, k);
     if (mask_at(g, d, p, i, j) != 1) continue;
     const Nbr12 n = load_nbr(g, d, p, i, j);
-    double Ai[8][9];
+    R Ai[8][9];
     stencil_inv(d, ph, g, p, i, j, k, n, Ai);
     for (int q = 0; q < 3; ++q) {
-      double gr[3];
+      R gr[3];
       weno8(d, ph, p, i, j, k, n, Ai, s.Esnap, ((long long)q * NPANEL + p) * d.S, gr);
       s.E[d.at(3 + q, p, i, j, k)] = gr[0];
       s.E[d.at(6 + q, p, i, j, k)] = gr[1];
@@ -1148,26 +1171,27 @@ __global__ void k_efield_b(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
 
 // Row rr (0: the zone itself, 1..18: the STEP 7.b neighbours) of the
 // 19 x 10 interpolation least-squares matrix of STEP 9.c (421:8464-8620).
+template <typename R>
 __device__ __forceinline__ void e9c_row(const Dims& d, const DGeom& g, int p, int i, int j, int k, const Nbr12& n,
-                                        int rr, double cx, double cy, double cz, double obl0, const double* c0, double* A,
+                                        int rr, R cx, R cy, R cz, R obl0, const R* c0, R* A,
                                         long long& off) {
   if (rr == 0) {
     off = d.idx(i, j, k);
-    A[0] = 1.0;
-    A[1] = 0.0;
-    A[2] = 0.0;
-    A[3] = 0.0;
+    A[0] = R(1.0);
+    A[1] = R(0.0);
+    A[2] = R(0.0);
+    A[3] = R(0.0);
 #pragma unroll
-    for (int m = 4; m < 10; ++m) A[m] = 0.0 * 0.0 - c0[m];
+    for (int m = 4; m < 10; ++m) A[m] = R(0.0) * R(0.0) - c0[m];
     return;
   }
   const int w = c_n18[rr - 1][0], dz = c_n18[rr - 1][1];
   const int zx = w < 0 ? i : n.x[w], zy = w < 0 ? j : n.y[w], zz = k + dz;
   off = d.idx(zx, zy, zz);
-  const double x = (geo(g, d, CS_G_V_CEN, 0, p, zx, zy, zz) - cx) * obl0;
-  const double y = (geo(g, d, CS_G_V_CEN, 1, p, zx, zy, zz) - cy) * obl0;
-  const double z = (geo(g, d, CS_G_V_CEN, 2, p, zx, zy, zz) - cz) * obl0;
-  A[0] = 1.0;
+  const R x = (geoR<R>(g, d, CS_G_V_CEN, 0, p, zx, zy, zz) - cx) * obl0;
+  const R y = (geoR<R>(g, d, CS_G_V_CEN, 1, p, zx, zy, zz) - cy) * obl0;
+  const R z = (geoR<R>(g, d, CS_G_V_CEN, 2, p, zx, zy, zz) - cz) * obl0;
+  A[0] = R(1.0);
   A[1] = x;
   A[2] = y;
   A[3] = z;
@@ -1179,13 +1203,14 @@ __device__ __forceinline__ void e9c_row(const Dims& d, const DGeom& g, int p, in
   A[9] = x * z - c0[9];
 }
 
+template <typename R>
 __device__ __forceinline__ void e9c_minv(const Dims& d, const DGeom& g, int p, int i, int j, int k, const Nbr12& n,
-                                         double cx, double cy, double cz, double obl0, const double* c0, double* Minv) {
-  double M[100];
+                                         R cx, R cy, R cz, R obl0, const R* c0, R* Minv) {
+  R M[100];
 #pragma unroll
-  for (int t = 0; t < 100; ++t) M[t] = 0.0;
+  for (int t = 0; t < 100; ++t) M[t] = R(0.0);
   for (int rr = 0; rr < 19; ++rr) {
-    double A[10];
+    R A[10];
     long long off;
     e9c_row(d, g, p, i, j, k, n, rr, cx, cy, cz, obl0, c0, A, off);
 #pragma unroll
@@ -1205,81 +1230,82 @@ __device__ __forceinline__ void e9c_minv(const Dims& d, const DGeom& g, int p, i
 // Only the point value (mode 1) is stored: the LLF edge solver consumes
 // nothing else.  kCached: the inverse normal matrix comes from the
 // operator cache.
-template <bool kCached>
-__global__ void __launch_bounds__(TPB, 4) k_efield_c(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
-  const double ob12 = 1.0 / 12.0, ob180 = 1.0 / 180.0, ob144 = 1.0 / 144.0;
+template <bool kCached, typename R>
+__global__ void __launch_bounds__(TPB, 4) k_efield_c(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
+  const R ob12 = R(1.0) / R(12.0), ob180 = R(1.0) / R(180.0), ob144 = R(1.0) / R(144.0);
   const long long nr_ = r.count();
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nr_; t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
     r.decode(t, p, i, j, k);
     if (mask_at(g, d, p, i, j) != 1) continue;
     const Nbr12 n = load_nbr(g, d, p, i, j);
-    const double obl0 = 1.0 / fmax(geo(g, d, CS_G_V_SCALE, 0, p, i, j, k), ph.smallnum);
-    double c0[10];
+    const R obl0 = R(1.0) / fmax(geoR<R>(g, d, CS_G_V_SCALE, 0, p, i, j, k), R(ph.smallnum));
+    R c0[10];
     coef10(g, d, p, i, j, k, c0);
-    const double cx = geo(g, d, CS_G_V_CEN, 0, p, i, j, k), cy = geo(g, d, CS_G_V_CEN, 1, p, i, j, k),
-                 cz = geo(g, d, CS_G_V_CEN, 2, p, i, j, k);
-    double Minv[kCached ? 1 : 100];
+    const R cx = geoR<R>(g, d, CS_G_V_CEN, 0, p, i, j, k), cy = geoR<R>(g, d, CS_G_V_CEN, 1, p, i, j, k),
+                 cz = geoR<R>(g, d, CS_G_V_CEN, 2, p, i, j, k);
+    R Minv[kCached ? 1 : 100];
     if (!kCached) e9c_minv(d, g, p, i, j, k, n, cx, cy, cz, obl0, c0, Minv);
     const double* mc = s.op_m10 + t;
-    auto MI = [&](int e) { return kCached ? __ldg(mc + (long long)e * nr_) : Minv[kCached ? 0 : e]; };
-    double Y[3][10];
+    auto MI = [&](int e) { return kCached ? (R)__ldg(mc + (long long)e * nr_) : Minv[kCached ? 0 : e]; };
+    R Y[3][10];
 #pragma unroll
     for (int q = 0; q < 3; ++q)
 #pragma unroll
-      for (int a = 0; a < 10; ++a) Y[q][a] = 0.0;
+      for (int a = 0; a < 10; ++a) Y[q][a] = R(0.0);
 #pragma unroll 1
     for (int rr = 0; rr < 19; ++rr) {
-      double A[10];
+      R A[10];
       long long off;
       e9c_row(d, g, p, i, j, k, n, rr, cx, cy, cz, obl0, c0, A, off);
 #pragma unroll
       for (int q = 0; q < 3; ++q) {
-        const double R = s.Esnap[((long long)q * NPANEL + p) * d.S + off];
+        const R Rv = s.Esnap[((long long)q * NPANEL + p) * d.S + off];
 #pragma unroll
-        for (int a = 0; a < 10; ++a) Y[q][a] = Y[q][a] + A[a] * R;
+        for (int a = 0; a < 10; ++a) Y[q][a] = Y[q][a] + A[a] * Rv;
       }
     }
-    const double f = s.flatA[d.at(0, p, i, j, k)];
-    const double betalo = f + (1.0 - f) * 2.0;
-    const double ghi = f * 0.6 + (1.0 - f) * 0.95, glo = 1.0 - ghi, obghi = 1.0 / ghi, grat = glo / ghi;
+    const R f = s.flatA[d.at(0, p, i, j, k)];
+    const R betalo = f + (R(1.0) - f) * R(2.0);
+    const R ghi = f * R(0.6) + (R(1.0) - f) * R(0.95), glo = R(1.0) - ghi, obghi = R(1.0) / ghi, grat = glo / ghi;
 #pragma unroll 1
     for (int q = 0; q < 3; ++q) {
-      double X[10];
+      R X[10];
 #pragma unroll
       for (int a = 0; a < 10; ++a) {
-        double acc = 0.0;
+        R acc = R(0.0);
 #pragma unroll
         for (int b = 0; b < 10; ++b) acc = acc + MI(a * 10 + b) * Y[q][b];
         X[a] = acc;
       }
-      double e[4];
+      R e[4];
       e[0] = s.Esnap[((long long)q * NPANEL + p) * d.S + d.idx(i, j, k)];
 #pragma unroll
       for (int m = 1; m < 4; ++m) e[m] = s.E[d.at(m * 3 + q, p, i, j, k)];
-      const double ISlo = betalo * (e[1] * e[1] + e[2] * e[2] + e[3] * e[3]) * ob12;
-      double Phi[10];
+      const R ISlo = betalo * (e[1] * e[1] + e[2] * e[2] + e[3] * e[3]) * ob12;
+      R Phi[10];
 #pragma unroll
       for (int m = 0; m < 4; ++m) Phi[m] = X[m] * obghi - e[m] * grat;
 #pragma unroll
       for (int m = 4; m < 10; ++m) Phi[m] = X[m] * obghi;
-      const double IShi = (Phi[1] * Phi[1] + Phi[2] * Phi[2] + Phi[3] * Phi[3]) * ob12 +
+      const R IShi = (Phi[1] * Phi[1] + Phi[2] * Phi[2] + Phi[3] * Phi[3]) * ob12 +
                           (Phi[4] * Phi[4]) * (sqr(c0[4] - ob12) + ob180) + (Phi[5] * Phi[5]) * (sqr(c0[5] - ob12) + ob180) +
                           (Phi[6] * Phi[6]) * (sqr(c0[6] - ob12) + ob180) + (Phi[7] * Phi[7]) * (c0[7] * c0[7] + ob144) +
                           (Phi[8] * Phi[8]) * (c0[8] * c0[8] + ob144) + (Phi[9] * Phi[9]) * (c0[9] * c0[9] + ob144);
-      const double tau = fabs(IShi - ISlo);
-      double Wlo = glo * (1.0 + tau / (ISlo + ph.smallnum)), Whi = ghi * (1.0 + tau / (IShi + ph.smallnum));
-      const double aa = 1.0 / (Wlo + Whi);
+      const R tau = fabs(IShi - ISlo);
+      R Wlo = glo * (R(1.0) + tau / (ISlo + R(ph.smallnum))), Whi = ghi * (R(1.0) + tau / (IShi + R(ph.smallnum)));
+      const R aa = R(1.0) / (Wlo + Whi);
       Wlo = Wlo * aa;
       Whi = Whi * aa;
-      const double x = 1.0 - f;
-      const double e0 = Whi * Phi[0] + Wlo * e[0];
+      const R x = R(1.0) - f;
+      const R e0 = Whi * Phi[0] + Wlo * e[0];
       s.E[d.at(q, p, i, j, k)] = e[0] * f + e0 * x;
     }
   }
 }
 
-__global__ void k_ops_m10(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
+template <typename R>
+__global__ void k_ops_m10(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
   const long long nr_ = r.count();
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nr_; t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
@@ -1304,75 +1330,116 @@ inline Range3 shrink(const Dims& d, int s) {
 
 }  // namespace
 
-void launch_prim_and_masks(Solve& sv) {
+template <typename R>
+void launch_prim_and_masks_t(Solve& sv, DStateT<R>& st) {
   const Dims& d = sv.d;
   Range3 z = zones_all(d);
-  k_prim<<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, z);
+  k_prim<R><<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, z);
   mark(sv, "k_prim");
   launch_face_masks(sv);
 }
 
-void launch_face_masks(Solve& sv) {
+void launch_prim_and_masks(Solve& sv) {
+  if (sv.fp32)
+    launch_prim_and_masks_t(sv, sv.stF);
+  else
+    launch_prim_and_masks_t(sv, sv.st);
+}
+
+template <typename R>
+void launch_face_masks_t(Solve& sv, DStateT<R>& st) {
   const Dims& d = sv.d;
   Range3 f = {-d.G, d.N + d.G, -d.G, d.N + d.G, -d.G, d.nr + d.G};
-  k_zero_masked_faces<<<blocks_for(f.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, sv.st, f);
+  k_zero_masked_faces<R><<<blocks_for(f.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, st, f);
   mark(sv, "k_zero_masked_faces");
-  k_tricorner<<<blocks_for(6LL * 4 * d.G * (d.NK - 1), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, sv.st);
+  k_tricorner<R><<<blocks_for(6LL * 4 * d.G * (d.NK - 1), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, st);
   mark(sv, "k_tricorner");
 }
 
-void launch_flattener(Solve& sv) {
+void launch_face_masks(Solve& sv) {
+  if (sv.fp32)
+    launch_face_masks_t(sv, sv.stF);
+  else
+    launch_face_masks_t(sv, sv.st);
+}
+
+template <typename R>
+void launch_flattener_t(Solve& sv, DStateT<R>& st) {
   const Dims& d = sv.d;
   Range3 z = zones_all(d);
   const int nb = blocks_for(z.count(), TPB, sv.sm_count);
-  k_flat_a<<<nb, TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, z);
+  k_flat_a<R><<<nb, TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, z);
   mark(sv, "k_flat_a");
-  k_flat_bc<<<nb, TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, z, sv.st.flatA, sv.st.flatB, 0);
+  k_flat_bc<R><<<nb, TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, z, st.flatA, st.flatB, 0);
   mark(sv, "k_flat_bc");
-  k_flat_bc<<<nb, TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, z, sv.st.flatB, sv.st.flatA, 1);
+  k_flat_bc<R><<<nb, TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, z, st.flatB, st.flatA, 1);
   mark(sv, "k_flat_bc");
 }
 
-void launch_weno(Solve& sv) {
+void launch_flattener(Solve& sv) {
+  if (sv.fp32)
+    launch_flattener_t(sv, sv.stF);
+  else
+    launch_flattener_t(sv, sv.st);
+}
+
+template <typename R>
+void launch_weno_t(Solve& sv, DStateT<R>& st) {
   const Dims& d = sv.d;
   Range3 a = shrink(d, 1), b = shrink(d, 2);
-  k_weno7a<<<blocks_for(a.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, a);
+  k_weno7a<R><<<blocks_for(a.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, a);
   mark(sv, "k_weno7a");
-  if (sv.st.op_m9)
-    k_weno7b<true><<<blocks_for(b.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, b);
+  if (st.op_m9)
+    k_weno7b<true, R><<<blocks_for(b.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
   else
-    k_weno7b<false><<<blocks_for(b.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, b);
+    k_weno7b<false, R><<<blocks_for(b.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
   mark(sv, "k_weno7b");
 }
 
-void launch_positivity(Solve& sv) {
+void launch_weno(Solve& sv) {
+  if (sv.fp32)
+    launch_weno_t(sv, sv.stF);
+  else
+    launch_weno_t(sv, sv.st);
+}
+
+template <typename R>
+void launch_positivity_t(Solve& sv, DStateT<R>& st) {
   const Dims& d = sv.d;
   Range3 z = zones_all(d);
-  k_positivity<<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, z);
+  k_positivity<R><<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, z);
   mark(sv, "k_positivity");
-  k_apply_giveup<<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.st, z);
+  k_apply_giveup<R><<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, st, z);
   mark(sv, "k_apply_giveup");
 }
 
-void launch_faceB_adp(Solve& sv) {
+void launch_positivity(Solve& sv) {
+  if (sv.fp32)
+    launch_positivity_t(sv, sv.stF);
+  else
+    launch_positivity_t(sv, sv.st);
+}
+
+template <typename R>
+void launch_faceB_adp_t(Solve& sv, DStateT<R>& st) {
   const Dims& d = sv.d;
   const int G = d.G, N = d.N, nr = d.nr;
   Range3 fx = {1 - G, N + G - 1, 2 - G, N + G - 1, 2 - G, nr + G - 1};
   Range3 fy = {2 - G, N + G - 1, 1 - G, N + G - 1, 2 - G, nr + G - 1};
   Range3 fz = {2 - G, N + G - 1, 2 - G, N + G - 1, 1 - G, nr + G - 1};
-  k_faceB<<<blocks_for(fx.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, fx, 0);
+  k_faceB<R><<<blocks_for(fx.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, fx, 0);
   mark(sv, "k_faceB");
-  k_faceB<<<blocks_for(fy.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, fy, 1);
+  k_faceB<R><<<blocks_for(fy.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, fy, 1);
   mark(sv, "k_faceB");
-  k_faceB<<<blocks_for(fz.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, fz, 2);
+  k_faceB<R><<<blocks_for(fz.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, fz, 2);
   mark(sv, "k_faceB");
   Range3 a = shrink(d, 1);
-  if (sv.st.adp_lu) {
-    k_adp_rhs<<<blocks_for(a.count(), ADPR_TPB, sv.sm_count), ADPR_TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, a);
+  if (st.adp_lu) {
+    k_adp_rhs<R><<<blocks_for(a.count(), ADPR_TPB, sv.sm_count), ADPR_TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, a);
     mark(sv, "k_adp_rhs");
     const long long nblk = (a.count() + ADP_ZB - 1) / ADP_ZB;
     const int grid = (int)std::min<long long>(nblk, (long long)sv.sm_count * 2);
-    k_adp_solve<<<grid, ADPS_THREADS, sizeof(AdpsSmem), sv.stream>>>(d, sv.ph, sv.g, sv.st, a);
+    k_adp_solve<R><<<grid, ADPS_THREADS, sizeof(AdpsSmem), sv.stream>>>(d, sv.ph, sv.g, st, a);
     mark(sv, "k_adp_solve");
     return;
   }
@@ -1381,24 +1448,39 @@ void launch_faceB_adp(Solve& sv) {
   long long nblk = (nwarps + ADP_WARPS - 1) / ADP_WARPS;
   long long cap = (long long)sv.sm_count * 16;
   if (nblk > cap) nblk = cap;
-  k_adp<false><<<(int)nblk, 32 * ADP_WARPS, smem, sv.stream>>>(d, sv.ph, sv.g, sv.st, a);
+  k_adp<false, R><<<(int)nblk, 32 * ADP_WARPS, smem, sv.stream>>>(d, sv.ph, sv.g, st, a);
   mark(sv, "k_adp");
+}
+
+void launch_faceB_adp(Solve& sv) {
+  if (sv.fp32)
+    launch_faceB_adp_t(sv, sv.stF);
+  else
+    launch_faceB_adp_t(sv, sv.st);
 }
 
 long long adp_range_count(const Dims& d) { return shrink(d, 1).count(); }
 long long lsq_range_count(const Dims& d) { return shrink(d, 2).count(); }
 
-void launch_ops_build(Solve& sv) {
+template <typename R>
+void launch_ops_build_t(Solve& sv, DStateT<R>& st) {
   const Dims& d = sv.d;
   Range3 b = shrink(d, 2);
-  if (sv.st.op_m9) {
-    k_ops_m9<<<blocks_for(b.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, b);
+  if (st.op_m9) {
+    k_ops_m9<R><<<blocks_for(b.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
     mark(sv, "k_ops_m9");
   }
-  if (sv.st.op_m10) {
-    k_ops_m10<<<blocks_for(b.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, b);
+  if (st.op_m10) {
+    k_ops_m10<R><<<blocks_for(b.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
     mark(sv, "k_ops_m10");
   }
+}
+
+void launch_ops_build(Solve& sv) {
+  if (sv.fp32)
+    launch_ops_build_t(sv, sv.stF);
+  else
+    launch_ops_build_t(sv, sv.st);
 }
 
 long long adp_factor_doubles(const Dims& d) {
@@ -1406,35 +1488,54 @@ long long adp_factor_doubles(const Dims& d) {
 }
 
 void set_adp_smem_limits() {
-  cudaFuncSetAttribute(k_adp_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(AdpsSmem));
   const int smem = (int)(sizeof(AdpSmem) * ADP_WARPS);
-  cudaFuncSetAttribute(k_adp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  cudaFuncSetAttribute(k_adp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaFuncSetAttribute(k_adp_solve<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(AdpsSmem));
+  cudaFuncSetAttribute(k_adp_solve<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(AdpsSmem));
+  cudaFuncSetAttribute(k_adp<false, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaFuncSetAttribute(k_adp<true, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaFuncSetAttribute(k_adp<false, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaFuncSetAttribute(k_adp<true, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
 }
 
-void launch_adp_factor(Solve& sv) {
+template <typename R>
+void launch_adp_factor_t(Solve& sv, DStateT<R>& st) {
   const Dims& d = sv.d;
   Range3 a = shrink(d, 1);
   const size_t smem = sizeof(AdpSmem) * ADP_WARPS;
   long long nblk = (a.count() + ADP_WARPS - 1) / ADP_WARPS;
   long long cap = (long long)sv.sm_count * 16;
   if (nblk > cap) nblk = cap;
-  k_adp<true><<<(int)nblk, 32 * ADP_WARPS, smem, sv.stream>>>(d, sv.ph, sv.g, sv.st, a);
+  k_adp<true, R><<<(int)nblk, 32 * ADP_WARPS, smem, sv.stream>>>(d, sv.ph, sv.g, st, a);
   mark(sv, "k_adp_factor");
 }
 
-void launch_efield(Solve& sv) {
+void launch_adp_factor(Solve& sv) {
+  if (sv.fp32)
+    launch_adp_factor_t(sv, sv.stF);
+  else
+    launch_adp_factor_t(sv, sv.st);
+}
+
+template <typename R>
+void launch_efield_t(Solve& sv, DStateT<R>& st) {
   const Dims& d = sv.d;
   Range3 z = zones_all(d), a = shrink(d, 1), b = shrink(d, 2);
-  k_efield_a<<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, sv.st, z);
+  k_efield_a<R><<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, st, z);
   mark(sv, "k_efield_a");
-  k_efield_b<<<blocks_for(a.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, a);
+  k_efield_b<R><<<blocks_for(a.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, a);
   mark(sv, "k_efield_b");
-  if (sv.st.op_m10)
-    k_efield_c<true><<<blocks_for(b.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, b);
+  if (st.op_m10)
+    k_efield_c<true, R><<<blocks_for(b.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
   else
-    k_efield_c<false><<<blocks_for(b.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, sv.st, b);
+    k_efield_c<false, R><<<blocks_for(b.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
   mark(sv, "k_efield_c");
+}
+
+void launch_efield(Solve& sv) {
+  if (sv.fp32)
+    launch_efield_t(sv, sv.stF);
+  else
+    launch_efield_t(sv, sv.st);
 }
 
 }  // namespace cs

@@ -25,13 +25,19 @@ namespace cs {
 size_t estimate_device_bytes(const cs_params& p) {
   const Box b(p.ntp, p.nr, p.nghost);
   const size_t S6 = (size_t)6 * b.size();
-  // words per point: geometry 126, state 15, V 80 + E 30 + E snapshot 3,
-  // flattener 3, face-B quadrature 15, face contributions 48, entropy
-  // fluxes 3, EMFs 3, saved faces 3, speeds 6, dU/dt 8, U0 8, ent0 1,
-  // face states 270
-  size_t words = 126 + 15 + 113 + 3 + 15 + 48 + 3 + 3 + 3 + 6 + 8 + 8 + 1 + 270;
-  if (p.rk_scheme == CS_IMEX_RK2) words += 14;
-  size_t bytes = words * S6 * sizeof(double) + S6 * 2 * sizeof(int32_t);
+  // words per point of the state's type: U 8 + entropy 4, V 80 + E 30 +
+  // E snapshot 3, flattener 3, face contributions 48, entropy fluxes 3,
+  // speeds 6, dU/dt 8, U0 8, ent0 1, face states 270 (IMEX: + 11);
+  // FP64 in both forms: geometry 126, face B 3, face-B quadrature 15,
+  // EMFs 3, saved faces 3 (IMEX: + 3)
+  size_t rwords = 12 + 113 + 3 + 48 + 3 + 6 + 8 + 8 + 1 + 270;
+  size_t dwords = 126 + 3 + 15 + 3 + 3;
+  if (p.rk_scheme == CS_IMEX_RK2) {
+    rwords += 11;
+    dwords += 3;
+  }
+  const size_t rsize = (p.flags & CS_FLAG_FP32) ? sizeof(float) : sizeof(double);
+  size_t bytes = (rwords * rsize + dwords * sizeof(double)) * S6 + S6 * 2 * sizeof(int32_t);
   // ghost map: per panel 4 strips of G layers, 12 field words per point,
   // 17 bytes per entry (offsets, meta, staging value)
   bytes += (size_t)6 * 4 * (p.nghost + 1) * (p.ntp + 2 * p.nghost + 1) * (p.nr + 2 * p.nghost + 1) * 12 * 17;

@@ -52,7 +52,9 @@ struct Solve {
   Dims d{};
   PhysC ph{};
   DGeom g{};
-  DState st{};
+  DState st{};                // state of the plain (FP64) form
+  DStateT<float> stF{};       // state of the precision (FP32 bulk) form
+  bool fp32 = false;          // which of the two this solve uses
   GeomHost host;             // host geometry (kept for cs_geometry_get)
   std::vector<void*> allocs;  // device allocations owned by the solve
   FillMap fill;

@@ -16,41 +16,55 @@ namespace {
 
 constexpr int TPB = 128;
 
-__device__ __forceinline__ double* fill_base(const DState& s, int f) {
+// Fields the ghost exchange moves: 0 U, 1 entropy (the state's type R),
+// 2..4 face B (always FP64).  Values travel as doubles.
+template <typename R>
+__device__ __forceinline__ double fill_load(const DStateT<R>& s, int f, int32_t at) {
   switch (f) {
-    case 0: return s.U;
-    case 1: return s.ent;
-    case 2: return s.Bxf;
-    case 3: return s.Byf;
-    default: return s.Bzf;
+    case 0: return (double)s.U[at];
+    case 1: return (double)s.ent[at];
+    case 2: return s.Bxf[at];
+    case 3: return s.Byf[at];
+    default: return s.Bzf[at];
+  }
+}
+template <typename R>
+__device__ __forceinline__ void fill_store(const DStateT<R>& s, int f, int32_t at, double v) {
+  switch (f) {
+    case 0: s.U[at] = (R)v; break;
+    case 1: s.ent[at] = (R)v; break;
+    case 2: s.Bxf[at] = v; break;
+    case 3: s.Byf[at] = v; break;
+    default: s.Bzf[at] = v;
   }
 }
 
 // Phase 1 of the exchange: every destination value is computed from the
 // pre-exchange arrays (the reference reads all sources from buffers packed
 // before any ghost is written).
-__global__ void k_fill_gather(DState s, const int32_t* __restrict__ src, const int32_t* __restrict__ dst,
+template <typename R>
+__global__ void k_fill_gather(DStateT<R> s, const int32_t* __restrict__ src, const int32_t* __restrict__ dst,
                               const uint8_t* __restrict__ meta, double* __restrict__ tmp, long long n) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
     const int m = meta[t];
-    double v = fill_base(s, (m >> 5) & 7)[src[t]];
+    double v = fill_load(s, (m >> 5) & 7, src[t]);
     if (m & 8) v = -v;
-    if (m & 16) v = (fill_base(s, m & 7)[dst[t]] + v) * 0.5;
+    if (m & 16) v = (fill_load(s, m & 7, dst[t]) + v) * 0.5;
     tmp[t] = v;
   }
 }
 
-__global__ void k_fill_scatter(DState s, const int32_t* __restrict__ dst, const uint8_t* __restrict__ meta,
+template <typename R>
+__global__ void k_fill_scatter(DStateT<R> s, const int32_t* __restrict__ dst, const uint8_t* __restrict__ meta,
                                const double* __restrict__ tmp, long long n) {
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-    double* b = fill_base(s, meta[t] & 7);
-    b[dst[t]] = tmp[t];
-  }
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+    fill_store(s, meta[t] & 7, dst[t], tmp[t]);
 }
 
 // Radial outflow padding below k = 1 and above k = nr (826:190-420).  Two
 // columns that share an x- or y-face copy the same value into it.
-__global__ void k_pad_radial(Dims d, DGeom g, DState s, int bc_lower, int bc_upper) {
+template <typename R>
+__global__ void k_pad_radial(Dims d, DGeom g, DStateT<R> s, int bc_lower, int bc_upper) {
   const int n1 = d.N + 2 * d.G;
   const long long n = 6LL * n1 * n1;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
@@ -91,13 +105,18 @@ __global__ void k_pad_radial(Dims d, DGeom g, DState s, int bc_lower, int bc_upp
 }
 
 // RK stage combine on the whole box: kind 0 is the two-stage average
-// (x + x0) / 2, kind 1 the Shu-Osher form a0 x0 + (1 - a0) x.
+// (x + x0) / 2, kind 1 the Shu-Osher form a0 x0 + (1 - a0) x.  Segments
+// 0..1 (U, entropy) hold the state's type R, 2..4 (face B) FP64.
+template <typename R>
 struct CombineSeg {
-  double* x[5];
-  const double* x0[5];
+  R* x[2];
+  const R* x0[2];
+  double* b[3];
+  const double* b0[3];
   long long n[5];
 };
-__global__ void k_combine(CombineSeg sg, long long total, double a0, int kind) {
+template <typename R>
+__global__ void k_combine(CombineSeg<R> sg, long long total, double a0, int kind) {
   const double a1 = 1.0 - a0;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
     long long u = t;
@@ -106,29 +125,35 @@ __global__ void k_combine(CombineSeg sg, long long total, double a0, int kind) {
       u -= sg.n[q];
       ++q;
     }
-    const double x = sg.x[q][u], x0 = sg.x0[q][u];
-    sg.x[q][u] = kind == 1 ? a0 * x0 + a1 * x : (x + x0) * 0.5;
+    if (q < 2) {
+      const double x = sg.x[q][u], x0 = sg.x0[q][u];
+      sg.x[q][u] = (R)(kind == 1 ? a0 * x0 + a1 * x : (x + x0) * 0.5);
+    } else {
+      const double x = sg.b[q - 2][u], x0 = sg.b0[q - 2][u];
+      sg.b[q - 2][u] = kind == 1 ? a0 * x0 + a1 * x : (x + x0) * 0.5;
+    }
   }
 }
 
 // Zone update (484:212-372): U += dt dU/dt on every zone, then on the
 // interior the entropy update and the conserved->primitive repair.
-__global__ void k_update_zones(Dims d, PhysC ph, DGeom g, DState s, Range3 r, double dt) {
+template <typename R>
+__global__ void k_update_zones(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r, R dt) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
     r.decode(t, p, i, j, k);
-    double U[8];
+    R U[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) U[q] = s.U[d.at(q, p, i, j, k)] + dt * s.dUdt[d.at(q, p, i, j, k)];
     if (i >= 1 && i <= d.N && j >= 1 && j <= d.N && k >= 1 && k <= d.nr) {
-      const double div = geo(g, d, CS_G_XF_AREA, 0, p, i, j, k) * s.EF[0][d.at(0, p, i, j, k)] -
-                         geo(g, d, CS_G_XF_AREA, 0, p, i - 1, j, k) * s.EF[0][d.at(0, p, i - 1, j, k)] +
-                         geo(g, d, CS_G_YF_AREA, 0, p, i, j, k) * s.EF[1][d.at(0, p, i, j, k)] -
-                         geo(g, d, CS_G_YF_AREA, 0, p, i, j - 1, k) * s.EF[1][d.at(0, p, i, j - 1, k)] +
-                         geo(g, d, CS_G_ZF_AREA, 0, p, i, j, k) * s.EF[2][d.at(0, p, i, j, k)] -
-                         geo(g, d, CS_G_ZF_AREA, 0, p, i, j, k - 1) * s.EF[2][d.at(0, p, i, j, k - 1)];
-      double en = s.ent[d.at(0, p, i, j, k)] - dt * div / geo(g, d, CS_G_V_VOL, 0, p, i, j, k);
-      double V[8];
+      const R div = geoR<R>(g, d, CS_G_XF_AREA, 0, p, i, j, k) * s.EF[0][d.at(0, p, i, j, k)] -
+                         geoR<R>(g, d, CS_G_XF_AREA, 0, p, i - 1, j, k) * s.EF[0][d.at(0, p, i - 1, j, k)] +
+                         geoR<R>(g, d, CS_G_YF_AREA, 0, p, i, j, k) * s.EF[1][d.at(0, p, i, j, k)] -
+                         geoR<R>(g, d, CS_G_YF_AREA, 0, p, i, j - 1, k) * s.EF[1][d.at(0, p, i, j - 1, k)] +
+                         geoR<R>(g, d, CS_G_ZF_AREA, 0, p, i, j, k) * s.EF[2][d.at(0, p, i, j, k)] -
+                         geoR<R>(g, d, CS_G_ZF_AREA, 0, p, i, j, k - 1) * s.EF[2][d.at(0, p, i, j, k - 1)];
+      R en = s.ent[d.at(0, p, i, j, k)] - dt * div / geoR<R>(g, d, CS_G_V_VOL, 0, p, i, j, k);
+      R V[8];
       d_cons_to_prim(ph, en, U, V);
       s.ent[d.at(0, p, i, j, k)] = en;
     }
@@ -153,7 +178,8 @@ __device__ __forceinline__ double vang(const DGeom& g, const Dims& d, int p, int
 
 // Constrained-transport face update (484:376-906): Stokes circulation of
 // the edge EMFs with spherical arc lengths for the angular edges.
-__global__ void k_ct(Dims d, DGeom g, DState s, Range3 r, int dir, double dt) {
+template <typename R>
+__global__ void k_ct(Dims d, DGeom g, DStateT<R> s, Range3 r, int dir, double dt) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
     r.decode(t, p, i, j, k);
@@ -193,7 +219,8 @@ __global__ void k_ct(Dims d, DGeom g, DState s, Range3 r, int dir, double dt) {
 // Clean-up zone pass (485:688-1273): least-squares zone-centred B from the
 // six face values on active zones with the matching total-energy fix, then
 // the conserved->primitive repair on every zone.
-__global__ void k_cleanup_zones(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
+template <typename R>
+__global__ void k_cleanup_zones(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
     r.decode(t, p, i, j, k);
@@ -266,7 +293,8 @@ __global__ void k_set_u64(unsigned long long* p, unsigned long long v) { *p = v;
 // CFL limit over the active interior zones; the minimum positive double is
 // found with an integer atomicMin on its bit pattern (positive IEEE doubles
 // order like their bit patterns).
-__global__ void k_timestep(Dims d, PhysC ph, DGeom g, DState s, Range3 r) {
+template <typename R>
+__global__ void k_timestep(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
   double dtl = 1.0e300;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
@@ -299,102 +327,133 @@ inline Range3 zones_all(const Dims& d) { return {1 - d.G, d.N + d.G, 1 - d.G, d.
 
 }  // namespace
 
-void launch_fill_ghosts(Solve& sv) {
+template <typename R>
+void launch_fill_ghosts_t(Solve& sv, const DStateT<R>& st) {
   const FillMap& f = sv.fill;
   if (f.n > 0) {
     const int nb = blocks_for(f.n, 256, sv.sm_count);
-    k_fill_gather<<<nb, 256, 0, sv.stream>>>(sv.st, f.d_src, f.d_dst, f.d_meta, f.d_tmp, f.n);
+    k_fill_gather<R><<<nb, 256, 0, sv.stream>>>(st, f.d_src, f.d_dst, f.d_meta, f.d_tmp, f.n);
     mark(sv, "k_fill_gather");
-    k_fill_scatter<<<nb, 256, 0, sv.stream>>>(sv.st, f.d_dst, f.d_meta, f.d_tmp, f.n);
+    k_fill_scatter<R><<<nb, 256, 0, sv.stream>>>(st, f.d_dst, f.d_meta, f.d_tmp, f.n);
     mark(sv, "k_fill_scatter");
   }
   const int n1 = sv.d.N + 2 * sv.d.G;
-  k_pad_radial<<<blocks_for(6LL * n1 * n1, TPB, sv.sm_count), TPB, 0, sv.stream>>>(sv.d, sv.g, sv.st, sv.p.bc_lower,
-                                                                                   sv.p.bc_upper);
+  k_pad_radial<R><<<blocks_for(6LL * n1 * n1, TPB, sv.sm_count), TPB, 0, sv.stream>>>(sv.d, sv.g, st, sv.p.bc_lower,
+                                                                                      sv.p.bc_upper);
   mark(sv, "k_pad_radial");
 }
+void launch_fill_ghosts(Solve& sv) {
+  if (sv.fp32)
+    launch_fill_ghosts_t(sv, sv.stF);
+  else
+    launch_fill_ghosts_t(sv, sv.st);
+}
 
-void launch_save_stage0(Solve& sv) {
-  const size_t S6 = (size_t)6 * sv.d.S * sizeof(double);
-  cudaMemcpyAsync(sv.st.U0, sv.st.U, NVAR * S6, cudaMemcpyDeviceToDevice, sv.stream);
-  cudaMemcpyAsync(sv.st.ent0, sv.st.ent, S6, cudaMemcpyDeviceToDevice, sv.stream);
-  cudaMemcpyAsync(sv.st.B0[0], sv.st.Bxf, S6, cudaMemcpyDeviceToDevice, sv.stream);
-  cudaMemcpyAsync(sv.st.B0[1], sv.st.Byf, S6, cudaMemcpyDeviceToDevice, sv.stream);
-  cudaMemcpyAsync(sv.st.B0[2], sv.st.Bzf, S6, cudaMemcpyDeviceToDevice, sv.stream);
+template <typename R>
+void launch_save_stage0_t(Solve& sv, const DStateT<R>& st) {
+  const size_t S6 = (size_t)6 * sv.d.S;
+  cudaMemcpyAsync(st.U0, st.U, NVAR * S6 * sizeof(R), cudaMemcpyDeviceToDevice, sv.stream);
+  cudaMemcpyAsync(st.ent0, st.ent, S6 * sizeof(R), cudaMemcpyDeviceToDevice, sv.stream);
+  cudaMemcpyAsync(st.B0[0], st.Bxf, S6 * sizeof(double), cudaMemcpyDeviceToDevice, sv.stream);
+  cudaMemcpyAsync(st.B0[1], st.Byf, S6 * sizeof(double), cudaMemcpyDeviceToDevice, sv.stream);
+  cudaMemcpyAsync(st.B0[2], st.Bzf, S6 * sizeof(double), cudaMemcpyDeviceToDevice, sv.stream);
   mark(sv, "copy_stage0", false);
 }
-
-void launch_combine(Solve& sv, double a0, int kind) {
-  const long long S6 = 6LL * sv.d.S;
-  CombineSeg sg;
-  sg.x[0] = sv.st.U;   sg.x0[0] = sv.st.U0;    sg.n[0] = NVAR * S6;
-  sg.x[1] = sv.st.ent; sg.x0[1] = sv.st.ent0;  sg.n[1] = S6;
-  sg.x[2] = sv.st.Bxf; sg.x0[2] = sv.st.B0[0]; sg.n[2] = S6;
-  sg.x[3] = sv.st.Byf; sg.x0[3] = sv.st.B0[1]; sg.n[3] = S6;
-  sg.x[4] = sv.st.Bzf; sg.x0[4] = sv.st.B0[2]; sg.n[4] = S6;
-  const long long total = (NVAR + 4) * S6;
-  k_combine<<<blocks_for(total, 256, sv.sm_count), 256, 0, sv.stream>>>(sg, total, a0, kind);
-  mark(sv, "k_combine");
+void launch_save_stage0(Solve& sv) {
+  if (sv.fp32)
+    launch_save_stage0_t(sv, sv.stF);
+  else
+    launch_save_stage0_t(sv, sv.st);
 }
 
-void launch_update_with(Solve& sv, const DState& st, double dtmove) {
+template <typename R>
+void launch_combine_t(Solve& sv, const DStateT<R>& st, double a0, int kind) {
+  const long long S6 = 6LL * sv.d.S;
+  CombineSeg<R> sg;
+  sg.x[0] = st.U;     sg.x0[0] = st.U0;    sg.n[0] = NVAR * S6;
+  sg.x[1] = st.ent;   sg.x0[1] = st.ent0;  sg.n[1] = S6;
+  sg.b[0] = st.Bxf;   sg.b0[0] = st.B0[0]; sg.n[2] = S6;
+  sg.b[1] = st.Byf;   sg.b0[1] = st.B0[1]; sg.n[3] = S6;
+  sg.b[2] = st.Bzf;   sg.b0[2] = st.B0[2]; sg.n[4] = S6;
+  const long long total = (NVAR + 4) * S6;
+  k_combine<R><<<blocks_for(total, 256, sv.sm_count), 256, 0, sv.stream>>>(sg, total, a0, kind);
+  mark(sv, "k_combine");
+}
+void launch_combine(Solve& sv, double a0, int kind) {
+  if (sv.fp32)
+    launch_combine_t(sv, sv.stF, a0, kind);
+  else
+    launch_combine_t(sv, sv.st, a0, kind);
+}
+
+template <typename R>
+void launch_update_with(Solve& sv, const DStateT<R>& st, double dtmove) {
   const Dims& d = sv.d;
   Range3 z = zones_all(d);
-  k_update_zones<<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, z, dtmove);
+  k_update_zones<R><<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, z, dtmove);
   mark(sv, "k_update_zones");
   const int N = d.N, nr = d.nr;
   Range3 fx = {0, N, 1, N, 1, nr}, fy = {1, N, 0, N, 1, nr}, fz = {1, N, 1, N, 0, nr};
-  k_ct<<<blocks_for(fx.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, st, fx, 0, dtmove);
+  k_ct<R><<<blocks_for(fx.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, st, fx, 0, dtmove);
   mark(sv, "k_ct");
-  k_ct<<<blocks_for(fy.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, st, fy, 1, dtmove);
+  k_ct<R><<<blocks_for(fy.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, st, fy, 1, dtmove);
   mark(sv, "k_ct");
-  k_ct<<<blocks_for(fz.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, st, fz, 2, dtmove);
+  k_ct<R><<<blocks_for(fz.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, st, fz, 2, dtmove);
   mark(sv, "k_ct");
 }
+template void launch_update_with<double>(Solve&, const DStateT<double>&, double);
+template void launch_update_with<float>(Solve&, const DStateT<float>&, double);
 
-void launch_update(Solve& sv, double dtmove) { launch_update_with(sv, sv.st, dtmove); }
+void launch_update(Solve& sv, double dtmove) {
+  if (sv.fp32)
+    launch_update_with(sv, sv.stF, dtmove);
+  else
+    launch_update_with(sv, sv.st, dtmove);
+}
 
 // ---- IMEX-RK2: ARS(2,2,2) with the point-mass gravity implicit ----
 // Gravity S(U) = (0, -rho g, -m . g), g = GM x / r^3, on the active zones
 // 0..N+1 (the zones of BUILD_NON_STIFF_SOURCES).  rho is unchanged by it,
 // so the implicit stage U = U* + a S(U) has the closed form
 // m = m* - a rho g, E = E* - a m . g.
-__global__ void k_gravity_implicit(Dims d, PhysC ph, DGeom g, DState s, Range3 r, double a) {
+template <typename R>
+__global__ void k_gravity_implicit(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r, R a) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
     r.decode(t, p, i, j, k);
     if (mask_at(g, d, p, i, j) != 1) continue;
-    const double x = geo(g, d, CS_G_V_CEN, 0, p, i, j, k), y = geo(g, d, CS_G_V_CEN, 1, p, i, j, k),
-                 z = geo(g, d, CS_G_V_CEN, 2, p, i, j, k);
-    const double rad = sqrt(x * x + y * y + z * z);
-    const double gmb = ph.gm * (1.0 / (rad * rad * rad));
-    const double gx = gmb * x, gy = gmb * y, gz = gmb * z;
-    const double rho = s.U[d.at(0, p, i, j, k)];
-    double& m1 = s.U[d.at(1, p, i, j, k)];
-    double& m2 = s.U[d.at(2, p, i, j, k)];
-    double& m3 = s.U[d.at(3, p, i, j, k)];
+    const R x = geoR<R>(g, d, CS_G_V_CEN, 0, p, i, j, k), y = geoR<R>(g, d, CS_G_V_CEN, 1, p, i, j, k),
+                 z = geoR<R>(g, d, CS_G_V_CEN, 2, p, i, j, k);
+    const R rad = sqrt(x * x + y * y + z * z);
+    const R gmb = R(ph.gm) * (R(1.0) / (rad * rad * rad));
+    const R gx = gmb * x, gy = gmb * y, gz = gmb * z;
+    const R rho = s.U[d.at(0, p, i, j, k)];
+    R& m1 = s.U[d.at(1, p, i, j, k)];
+    R& m2 = s.U[d.at(2, p, i, j, k)];
+    R& m3 = s.U[d.at(3, p, i, j, k)];
     m1 = m1 - a * (gx * rho);
     m2 = m2 - a * (gy * rho);
     m3 = m3 - a * (gz * rho);
-    double& e = s.U[d.at(4, p, i, j, k)];
+    R& e = s.U[d.at(4, p, i, j, k)];
     e = e - a * (gx * m1 + gy * m2 + gz * m3);
   }
 }
 
 // dUdt += c S(U) with the gravity of the current state (explicit use of
 // the previous stage's source).
-__global__ void k_add_gravity(Dims d, PhysC ph, DGeom g, DState s, Range3 r, double c) {
+template <typename R>
+__global__ void k_add_gravity(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r, R c) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
     r.decode(t, p, i, j, k);
     if (mask_at(g, d, p, i, j) != 1) continue;
-    const double x = geo(g, d, CS_G_V_CEN, 0, p, i, j, k), y = geo(g, d, CS_G_V_CEN, 1, p, i, j, k),
-                 z = geo(g, d, CS_G_V_CEN, 2, p, i, j, k);
-    const double rad = sqrt(x * x + y * y + z * z);
-    const double gmb = ph.gm * (1.0 / (rad * rad * rad));
-    const double gx = gmb * x, gy = gmb * y, gz = gmb * z;
-    const double rho = s.U[d.at(0, p, i, j, k)];
-    const double m1 = s.U[d.at(1, p, i, j, k)], m2 = s.U[d.at(2, p, i, j, k)], m3 = s.U[d.at(3, p, i, j, k)];
+    const R x = geoR<R>(g, d, CS_G_V_CEN, 0, p, i, j, k), y = geoR<R>(g, d, CS_G_V_CEN, 1, p, i, j, k),
+                 z = geoR<R>(g, d, CS_G_V_CEN, 2, p, i, j, k);
+    const R rad = sqrt(x * x + y * y + z * z);
+    const R gmb = R(ph.gm) * (R(1.0) / (rad * rad * rad));
+    const R gx = gmb * x, gy = gmb * y, gz = gmb * z;
+    const R rho = s.U[d.at(0, p, i, j, k)];
+    const R m1 = s.U[d.at(1, p, i, j, k)], m2 = s.U[d.at(2, p, i, j, k)], m3 = s.U[d.at(3, p, i, j, k)];
     s.dUdt[d.at(1, p, i, j, k)] += c * (-(gx * rho));
     s.dUdt[d.at(2, p, i, j, k)] += c * (-(gy * rho));
     s.dUdt[d.at(3, p, i, j, k)] += c * (-(gz * rho));
@@ -402,59 +461,101 @@ __global__ void k_add_gravity(Dims d, PhysC ph, DGeom g, DState s, Range3 r, dou
   }
 }
 
-void launch_gravity_implicit(Solve& sv, double a) {
-  if (!(sv.ph.gm > sv.p.smallnum)) return;
+template <typename R>
+void launch_gravity_implicit_t(Solve& sv, const DStateT<R>& st, double a) {
   Range3 z = {0, sv.d.N + 1, 0, sv.d.N + 1, 0, sv.d.nr + 1};
-  k_gravity_implicit<<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(sv.d, sv.ph, sv.g, sv.st, z, a);
+  k_gravity_implicit<R><<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(sv.d, sv.ph, sv.g, st, z, a);
   mark(sv, "k_gravity_implicit");
 }
+void launch_gravity_implicit(Solve& sv, double a) {
+  if (!(sv.ph.gm > sv.p.smallnum)) return;
+  if (sv.fp32)
+    launch_gravity_implicit_t(sv, sv.stF, a);
+  else
+    launch_gravity_implicit_t(sv, sv.st, a);
+}
 
+template <typename R>
+void launch_add_gravity_t(Solve& sv, const DStateT<R>& st, double c) {
+  Range3 z = {0, sv.d.N + 1, 0, sv.d.N + 1, 0, sv.d.nr + 1};
+  k_add_gravity<R><<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(sv.d, sv.ph, sv.g, st, z, c);
+  mark(sv, "k_add_gravity");
+}
 void launch_add_gravity(Solve& sv, double c) {
   if (!(sv.ph.gm > sv.p.smallnum)) return;
-  Range3 z = {0, sv.d.N + 1, 0, sv.d.N + 1, 0, sv.d.nr + 1};
-  k_add_gravity<<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(sv.d, sv.ph, sv.g, sv.st, z, c);
-  mark(sv, "k_add_gravity");
+  if (sv.fp32)
+    launch_add_gravity_t(sv, sv.stF, c);
+  else
+    launch_add_gravity_t(sv, sv.st, c);
 }
 
 // Copies of the first stage's flux divergence, entropy fluxes and EMFs,
 // and the restore of the step's initial state.
-void launch_save_stage1_rates(Solve& sv) {
-  const size_t S6 = (size_t)6 * sv.d.S * sizeof(double);
-  cudaMemcpyAsync(sv.st.K1, sv.st.dUdt, NVAR * S6, cudaMemcpyDeviceToDevice, sv.stream);
+template <typename R>
+void launch_save_stage1_rates_t(Solve& sv, const DStateT<R>& st) {
+  const size_t S6 = (size_t)6 * sv.d.S;
+  cudaMemcpyAsync(st.K1, st.dUdt, NVAR * S6 * sizeof(R), cudaMemcpyDeviceToDevice, sv.stream);
   for (int q = 0; q < 3; ++q) {
-    cudaMemcpyAsync(sv.st.EF1[q], sv.st.EF[q], S6, cudaMemcpyDeviceToDevice, sv.stream);
-    cudaMemcpyAsync(sv.st.Ef1[q], sv.st.Ef[q], S6, cudaMemcpyDeviceToDevice, sv.stream);
+    cudaMemcpyAsync(st.EF1[q], st.EF[q], S6 * sizeof(R), cudaMemcpyDeviceToDevice, sv.stream);
+    cudaMemcpyAsync(st.Ef1[q], st.Ef[q], S6 * sizeof(double), cudaMemcpyDeviceToDevice, sv.stream);
   }
   mark(sv, "copy_stage1_rates", false);
 }
+void launch_save_stage1_rates(Solve& sv) {
+  if (sv.fp32)
+    launch_save_stage1_rates_t(sv, sv.stF);
+  else
+    launch_save_stage1_rates_t(sv, sv.st);
+}
 
-void launch_restore_stage0(Solve& sv) {
-  const size_t S6 = (size_t)6 * sv.d.S * sizeof(double);
-  cudaMemcpyAsync(sv.st.U, sv.st.U0, NVAR * S6, cudaMemcpyDeviceToDevice, sv.stream);
-  cudaMemcpyAsync(sv.st.ent, sv.st.ent0, S6, cudaMemcpyDeviceToDevice, sv.stream);
-  cudaMemcpyAsync(sv.st.Bxf, sv.st.B0[0], S6, cudaMemcpyDeviceToDevice, sv.stream);
-  cudaMemcpyAsync(sv.st.Byf, sv.st.B0[1], S6, cudaMemcpyDeviceToDevice, sv.stream);
-  cudaMemcpyAsync(sv.st.Bzf, sv.st.B0[2], S6, cudaMemcpyDeviceToDevice, sv.stream);
+template <typename R>
+void launch_restore_stage0_t(Solve& sv, const DStateT<R>& st) {
+  const size_t S6 = (size_t)6 * sv.d.S;
+  cudaMemcpyAsync(st.U, st.U0, NVAR * S6 * sizeof(R), cudaMemcpyDeviceToDevice, sv.stream);
+  cudaMemcpyAsync(st.ent, st.ent0, S6 * sizeof(R), cudaMemcpyDeviceToDevice, sv.stream);
+  cudaMemcpyAsync(st.Bxf, st.B0[0], S6 * sizeof(double), cudaMemcpyDeviceToDevice, sv.stream);
+  cudaMemcpyAsync(st.Byf, st.B0[1], S6 * sizeof(double), cudaMemcpyDeviceToDevice, sv.stream);
+  cudaMemcpyAsync(st.Bzf, st.B0[2], S6 * sizeof(double), cudaMemcpyDeviceToDevice, sv.stream);
   mark(sv, "copy_restore", false);
 }
-
-void launch_cleanup(Solve& sv) {
-  launch_face_masks(sv);
-  Range3 z = zones_all(sv.d);
-  k_cleanup_zones<<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(sv.d, sv.ph, sv.g, sv.st, z);
-  mark(sv, "k_cleanup_zones");
+void launch_restore_stage0(Solve& sv) {
+  if (sv.fp32)
+    launch_restore_stage0_t(sv, sv.stF);
+  else
+    launch_restore_stage0_t(sv, sv.st);
 }
 
-void launch_timestep(Solve& sv, double dtcur) {
+template <typename R>
+void launch_cleanup_t(Solve& sv, const DStateT<R>& st) {
+  Range3 z = zones_all(sv.d);
+  k_cleanup_zones<R><<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(sv.d, sv.ph, sv.g, st, z);
+  mark(sv, "k_cleanup_zones");
+}
+void launch_cleanup(Solve& sv) {
+  launch_face_masks(sv);
+  if (sv.fp32)
+    launch_cleanup_t(sv, sv.stF);
+  else
+    launch_cleanup_t(sv, sv.st);
+}
+
+template <typename R>
+void launch_timestep_t(Solve& sv, const DStateT<R>& st, double dtcur) {
   const double start = 1.1 * dtcur;
   unsigned long long bits;
   static_assert(sizeof(bits) == sizeof(start), "double is 64-bit");
   std::memcpy(&bits, &start, sizeof(bits));
-  k_set_u64<<<1, 1, 0, sv.stream>>>(sv.st.dtmin, bits);
+  k_set_u64<<<1, 1, 0, sv.stream>>>(st.dtmin, bits);
   mark(sv, "k_set_u64");
   Range3 r = {1, sv.d.N, 1, sv.d.N, 1, sv.d.nr};
-  k_timestep<<<blocks_for(r.count(), 256, sv.sm_count), 256, 0, sv.stream>>>(sv.d, sv.ph, sv.g, sv.st, r);
+  k_timestep<R><<<blocks_for(r.count(), 256, sv.sm_count), 256, 0, sv.stream>>>(sv.d, sv.ph, sv.g, st, r);
   mark(sv, "k_timestep");
+}
+void launch_timestep(Solve& sv, double dtcur) {
+  if (sv.fp32)
+    launch_timestep_t(sv, sv.stF, dtcur);
+  else
+    launch_timestep_t(sv, sv.st, dtcur);
 }
 
 }  // namespace cs

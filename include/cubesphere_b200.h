@@ -102,6 +102,15 @@ typedef struct cs_params {
  * defect correction (DRV:3200-3461): conservative, and div B stays at
  * round-off across panel edges; without it div B grows at the cube corners. */
 #define CS_FLAG_NO_PANEL_SYNC 4
+/* cs_params.flags: the precision form.  The bulk of the stage (conserved
+ * state, entropy, primitives and their modes, the flattener, face states and
+ * fluxes, dU/dt, the stage copies) is stored and computed in FP32; face B,
+ * its quadrature values, the edge EMFs, the geometry and the resident
+ * operators stay FP64, so the CT update keeps div B at FP64 round-off.
+ * The WENO nonlinear weights are formed in FP64.  The reference has no
+ * such form (it computes everything in REAL*8); the state read and written
+ * through cs_state_get / cs_state_put stays FP64 at the boundary. */
+#define CS_FLAG_FP32 8
 
 /* Seeded initial-state description (new generator cases of the problem
  * library, built with the reference mechanism of 820init_patch_cube_sphere.f). */
