@@ -169,12 +169,15 @@ def cpu_baseline_sample(threads: int, steps: int = 1) -> dict:
                       f"{steps} RK2 step(s), {sec:.2f} s"}
 
 
-def serving_sample(seed: int = 7, nreq: int = 16, rate: float = 4.0, max_active: int = 8) -> dict:
+def serving_sample(seed: int = 7, nreq: int = 24, rate: float = 8.0, max_active: int = 8) -> dict:
     """Serving form on a bounded sample: Poisson arrivals (seeded rate) of
-    solve requests with panel N from {32, 48}, radial depth from {1, 8, 16}
-    and 10..30 steps, admitted by free device memory into the concurrent
-    server; then the same requests run one at a time (the plain path run
-    sequentially) for the throughput comparison."""
+    solve requests with panel N from {32, 48, 64}, radial depth from
+    {1, 16, 32} and 20..60 steps, admitted by free device memory into the
+    concurrent server (meshes cached between requests), in the plain FP64
+    form and in the precision form; then the FP64 requests run one at a time
+    (the plain path run sequentially, all submitted at once) for the
+    throughput comparison.  Throughput = zone updates / (last completion -
+    first submission); a fresh server per run, so mesh builds are inside."""
     import numpy as np
 
     import cubesphere_b200 as cs
@@ -182,9 +185,9 @@ def serving_sample(seed: int = 7, nreq: int = 16, rate: float = 4.0, max_active:
     rng = np.random.default_rng(seed)
     reqs = []
     for _ in range(nreq):
-        ntp = int(rng.choice([32, 48]))
-        nr = int(rng.choice([1, 8, 16]))
-        steps = int(rng.integers(10, 31))
+        ntp = int(rng.choice([32, 48, 64]))
+        nr = int(rng.choice([1, 16, 32]))
+        steps = int(rng.integers(20, 61))
         pr = cs.preset("shell16")
         params = dict(pr["params"])
         init = dict(pr["init"])
@@ -196,28 +199,31 @@ def serving_sample(seed: int = 7, nreq: int = 16, rate: float = 4.0, max_active:
         reqs.append((steps, params, init))
     gaps = rng.exponential(1.0 / rate, size=nreq)
 
-    def run(max_act, arrivals):
+    def run(max_act, arrivals, flags=0):
         srv = cs.Server(max_active=max_act, mem_fraction=0.8)
-        t0 = time.perf_counter()
         ids = []
         for q, (steps, params, init) in enumerate(reqs):
-            if arrivals:
+            if arrivals and q:
                 time.sleep(float(gaps[q]))
-            ids.append(srv.submit(steps, params, init))
+            ids.append(srv.submit(steps, dict(params, flags=flags), init))
         res = [srv.wait(i) for i in ids]
-        wall = time.perf_counter() - t0
         st = srv.stats()
         srv.close()
-        return st, wall, sum(r.zone_updates for r in res), all(r.status == 0 for r in res), res
+        return {"p50_latency_s": st["p50_s"], "p99_latency_s": st["p99_s"],
+                "mean_queue_s": float(np.mean([r.queue_s for r in res])),
+                "zone_updates_per_s": st["zone_updates_per_s"],
+                "meshes_reused": int(sum(r.mesh_reused for r in res)),
+                "all_ok": all(r.status == 0 for r in res)}
 
-    st, wall, zu, ok, res = run(max_active, True)
-    st1, wall1, zu1, ok1, _ = run(1, False)
-    return {"requests": nreq, "arrival_rate_per_s": rate, "max_active": max_active, "all_ok": ok and ok1,
-            "p50_latency_s": st["p50_s"], "p99_latency_s": st["p99_s"],
-            "mean_queue_s": float(np.mean([r.queue_s for r in res])),
-            "zone_updates_per_s": zu / wall, "sequential_zone_updates_per_s": zu1 / wall1,
-            "sizes": "N in {32,48}, nr in {1,8,16}, 10-30 steps, FP64 (IMEX-RK2 shells, SSP-RK3 surfaces); "
-                     "wall clock includes host mesh builds"}
+    f64 = run(max_active, True)
+    f32 = run(max_active, True, cs.CS_FLAG_FP32)
+    seq = run(1, False)
+    return {"requests": nreq, "arrival_rate_per_s": rate, "max_active": max_active,
+            "zone_updates": int(sum(6 * p["ntp"] ** 2 * p["nr"] * n for n, p, _ in reqs)),
+            "f64": f64, "f32_precision_form": f32, "f64_sequential": seq,
+            "f32_vs_f64_sequential": f32["zone_updates_per_s"] / max(seq["zone_updates_per_s"], 1e-30),
+            "sizes": "N in {32,48,64}, nr in {1,16,32}, 20-60 steps (IMEX-RK2 shells, SSP-RK3 surfaces); "
+                     "latency = submission to completion, mesh builds included"}
 
 
 def precision_sample(pr, dts, steps, ref_state, zones, world, allmax) -> dict:

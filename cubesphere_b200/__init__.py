@@ -41,9 +41,9 @@ CS_RK2, CS_SSPRK3, CS_IMEX_RK2 = 2, 3, 4
 
 EXPORTS = [
     "cs_geom_ncomp", "cs_create", "cs_destroy", "cs_last_error", "cs_box_dims", "cs_params_check",
-    "cs_mesh_build", "cs_mesh_build_host", "cs_geometry_get", "cs_mask_get", "cs_stencil_get",
+    "cs_mesh_build", "cs_mesh_share", "cs_mesh_build_host", "cs_geometry_get", "cs_mask_get", "cs_stencil_get",
     "cs_geometry_single_zone", "cs_init_problem", "cs_init_problem_host", "cs_state_put", "cs_state_get",
-    "cs_stage", "cs_step", "cs_evaluate_timestep", "cs_synchronize", "cs_fill_ghosts",
+    "cs_stage", "cs_step", "cs_steps", "cs_evaluate_timestep", "cs_synchronize", "cs_fill_ghosts",
     "cs_limit_all_slopes_p12", "cs_make_facial_fluxes", "cs_make_edge_efields_p1",
     "cs_build_non_stiff_sources", "cs_update_imex_rk_step_p1", "cs_cleanup_after_update",
     "cs_debug_get", "cs_diag", "cs_get_stream", "cs_launch_count", "cs_profile_begin", "cs_profile_end",
@@ -112,7 +112,7 @@ class CsRequest(ctypes.Structure):
 
 class CsServeResult(ctypes.Structure):
     _fields_ = [
-        ("status", ctypes.c_int32), ("reserved", ctypes.c_int32), ("latency_s", ctypes.c_double),
+        ("status", ctypes.c_int32), ("mesh_reused", ctypes.c_int32), ("latency_s", ctypes.c_double),
         ("queue_s", ctypes.c_double), ("mass", ctypes.c_double), ("energy", ctypes.c_double),
         ("max_divb", ctypes.c_double), ("dt_last", ctypes.c_double), ("zone_updates", ctypes.c_int64),
     ]
@@ -139,6 +139,7 @@ def load_library() -> ctypes.CDLL:
         "cs_params_check": ([ctypes.POINTER(CsParams)], ctypes.c_char_p),
         "cs_box_dims": ([P, ip, ip, ip], ctypes.c_int),
         "cs_mesh_build": ([P], ctypes.c_int),
+        "cs_mesh_share": ([P, P], ctypes.c_int),
         "cs_mesh_build_host": ([P], ctypes.c_int),
         "cs_geometry_get": ([P, ctypes.c_int, dp, S], ctypes.c_int),
         "cs_mask_get": ([P, ip, S], ctypes.c_int),
@@ -150,6 +151,7 @@ def load_library() -> ctypes.CDLL:
         "cs_state_get": ([P, dp, dp, dp, dp, dp], ctypes.c_int),
         "cs_stage": ([P, I, D], ctypes.c_int),
         "cs_step": ([P, D, dp], ctypes.c_int),
+        "cs_steps": ([P, ctypes.c_int32, ctypes.c_double, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
         "cs_evaluate_timestep": ([P, D, dp], ctypes.c_int),
         "cs_synchronize": ([P], ctypes.c_int),
         "cs_update_imex_rk_step_p1": ([P, D], ctypes.c_int),
@@ -250,6 +252,10 @@ class Solve:
         rc = self.lib.cs_mesh_build(self.h) if device else self.lib.cs_mesh_build_host(self.h)
         self._check(rc, "cs_mesh_build")
 
+    def mesh_share(self, other: "Solve") -> None:
+        """Use the resident mesh of `other` (same mesh parameters) instead of building one."""
+        self._check(self.lib.cs_mesh_share(self.h, other.h), "cs_mesh_share")
+
     def geometry(self, field: str | int) -> np.ndarray:
         f = GEOM[field] if isinstance(field, str) else field
         out = self.zeros(GEOM_NCOMP[f])
@@ -298,6 +304,12 @@ class Solve:
     def step(self, dtcur: float) -> float:
         out = ctypes.c_double()
         self._check(self.lib.cs_step(self.h, dtcur, ctypes.byref(out)), "cs_step")
+        return out.value
+
+    def steps(self, nsteps: int, dtcur: float) -> float:
+        """nsteps steps (graph replay, device-resident time step); returns the next time step."""
+        out = ctypes.c_double()
+        self._check(self.lib.cs_steps(self.h, nsteps, dtcur, ctypes.byref(out)), "cs_steps")
         return out.value
 
     def evaluate_timestep(self, dtcur: float) -> float:

@@ -13,10 +13,6 @@
 
 #include "cs_solve.h"
 
-struct cs_ctx {
-  cs::Solve sv;
-};
-
 namespace cs {
 namespace {
 
@@ -53,8 +49,11 @@ void free_all(Solve& sv) {
   sv.prof.name.clear();
   for (void* p : sv.allocs) cudaFree(p);
   sv.allocs.clear();
+  if (sv.graph_exec) cudaGraphExecDestroy(sv.graph_exec);
+  sv.graph_exec = nullptr;
   if (sv.stream) cudaStreamDestroy(sv.stream);
   sv.stream = nullptr;
+  sv.mesh = std::make_shared<MeshRes>();  // drops this solve's share of the mesh
 }
 
 // Host construction of the ghost-exchange map.  The strips are visited in
@@ -67,7 +66,7 @@ struct MapEntry {
 };
 
 std::string build_fill_map(const Solve& sv, std::vector<MapEntry>& out) {
-  const GeomHost& g = sv.host;
+  const GeomHost& g = sv.mesh->host;
   const Box& b = g.box;
   const int N = b.N, G = b.G, nr = b.nr;
   const long long S = (long long)b.size();
@@ -239,7 +238,7 @@ struct SyncMaps {
 };
 
 std::string build_sync_maps(const Solve& sv, SyncMaps& m) {
-  const GeomHost& g = sv.host;
+  const GeomHost& g = sv.mesh->host;
   const Box& b = g.box;
   const int N = b.N, nr = b.nr;
   const long long S = (long long)b.size();
@@ -377,8 +376,8 @@ PhysC make_phys(const cs_params& p) {
 }
 
 int ensure_host_mesh(Solve& sv) {
-  if (!sv.host.f[0].empty()) return CS_OK;
-  std::string e = build_geometry(sv.p, sv.host);
+  if (!sv.mesh->host.f[0].empty()) return CS_OK;
+  std::string e = build_geometry(sv.p, sv.mesh->host);
   if (!e.empty()) return fail(sv, CS_ERR_ARG, e);
   return CS_OK;
 }
@@ -405,79 +404,61 @@ int alloc_state(Solve& sv, DStateT<R>& s) {
   }
   s.FS = A(6 * NQ * (NVAR + 1));
   if (!s.FS) return cuda_fail(sv, e, "cudaMalloc(face states)");
-  set_adp_smem_limits();
-  // ADP: the KKT matrix of every zone depends on the geometry only, so its
-  // factors are computed once here and each stage only substitutes.  They
-  // take 10.4 KB per zone; without room for them (or with
-  // CS_FLAG_NO_ADP_CACHE) every stage assembles and factors in place.
-  s.adp_lu = nullptr;
-  s.adp_piv = nullptr;
+  // resident geometry-only operators of the mesh (null until built)
+  const MeshRes& m = *sv.mesh;
+  s.op_m9 = m.op_m9;
+  s.op_m10 = m.op_m10;
+  s.adp_lu = m.adp_lu;
+  s.adp_piv = m.adp_piv;
   s.adp_rhs = nullptr;
-  s.op_m9 = nullptr;
-  s.op_m10 = nullptr;
-  // The inverse normal matrices of the STEP 7.b / 9.c least squares are
-  // geometry-only as well (1.4 KB per zone together).
-  if (!(sv.p.flags & CS_FLAG_NO_OP_CACHE)) {
-    const long long nl = lsq_range_count(d);
-    size_t fr = 0, tot = 0;
-    const size_t bytes = (size_t)nl * (81 + 100) * sizeof(double);
-    if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && bytes + (size_t)8 * S6 * 60 < fr) {
-      s.op_m9 = (double*)dalloc(sv, (size_t)nl * 81 * sizeof(double), e);
-      s.op_m10 = s.op_m9 ? (double*)dalloc(sv, (size_t)nl * 100 * sizeof(double), e) : nullptr;
-      if (!s.op_m9 || !s.op_m10) return cuda_fail(sv, e, "cudaMalloc(least-squares operators)");
-    }
-  }
-  if (!(sv.p.flags & CS_FLAG_NO_ADP_CACHE)) {
-    const long long nf = adp_factor_doubles(d);
-    const size_t lu_bytes = (size_t)nf * sizeof(double), pv_bytes = (size_t)nf / 36;
-    size_t fr = 0, tot = 0;
-    if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && lu_bytes + pv_bytes + (size_t)8 * S6 * 60 < fr) {
-      s.adp_lu = (double*)dalloc(sv, lu_bytes, e);
-      s.adp_piv = s.adp_lu ? (int8_t*)dalloc(sv, pv_bytes, e) : nullptr;
-      s.adp_rhs = s.adp_piv ? (double*)dalloc(sv, (size_t)adp_range_count(d) * 36 * sizeof(double), e) : nullptr;
-      if (!s.adp_lu || !s.adp_piv || !s.adp_rhs) return cuda_fail(sv, e, "cudaMalloc(ADP factors)");
-    }
+  if (m.adp_lu) {
+    s.adp_rhs = (double*)dalloc(sv, (size_t)adp_range_count(d) * 36 * sizeof(double), e);
+    if (!s.adp_rhs) return cuda_fail(sv, e, "cudaMalloc(ADP right-hand sides)");
   }
   s.giveup = (int32_t*)dalloc(sv, S6 * sizeof(int32_t), e);
   s.err_flag = (int*)dalloc(sv, 64, e);
   if (!s.err_flag) return cuda_fail(sv, e, "cudaMalloc(error flag)");
   s.dtmin = (unsigned long long*)dalloc(sv, 64, e);
+  s.dt = (double*)dalloc(sv, 64, e);
+  if (!s.dt) return cuda_fail(sv, e, "cudaMalloc(time step)");
   if (e != cudaSuccess || !s.U || !s.V || !s.E || !s.dtmin) return cuda_fail(sv, e, "cudaMalloc(state)");
   for (int q = 0; q < 3; ++q)
     if (!s.Bq[q] || !s.fcon[q] || !s.EF[q] || !s.Ef[q] || !s.B0[q]) return fail(sv, CS_ERR_NOMEM, "cudaMalloc(work)");
   return CS_OK;
 }
 
-int upload_mesh(Solve& sv) {
-  const Box& b = sv.host.box;
-  Dims& d = sv.d;
-  d.N = b.N; d.nr = b.nr; d.G = b.G; d.NI = b.NI; d.NJ = b.NJ; d.NK = b.NK;
-  d.S = (long long)b.size();
-  CS_CUDA(sv, cudaGetDevice(&sv.device));
-  CS_CUDA(sv, cudaDeviceGetAttribute(&sv.sm_count, cudaDevAttrMultiProcessorCount, sv.device));
-  CS_CUDA(sv, cudaStreamCreateWithFlags(&sv.stream, cudaStreamNonBlocking));
+// Device allocation owned by a mesh (freed with its last user).
+void* mdalloc(Solve& sv, MeshRes& m, size_t bytes, cudaError_t& e) {
+  void* p = nullptr;
+  e = cudaMalloc(&p, bytes);
+  if (e != cudaSuccess) return nullptr;
+  m.allocs.push_back(p);
+  m.bytes += bytes;
+  e = cudaMemsetAsync(p, 0, bytes, sv.stream);
+  return p;
+}
+
+// Geometry, mask, stencil, ghost-exchange map and panel-ownership maps of
+// a mesh that is not on the device yet.
+int mesh_upload(Solve& sv, MeshRes& m) {
   cudaError_t e = cudaSuccess;
-  const size_t S6 = (size_t)6 * d.S;
   for (int f = 0; f < CS_G_NFIELDS; ++f) {
-    const size_t bytes = sv.host.f[f].size() * sizeof(double);
-    double* p = (double*)dalloc(sv, bytes, e);
+    const size_t bytes = m.host.f[f].size() * sizeof(double);
+    double* p = (double*)mdalloc(sv, m, bytes, e);
     if (!p) return cuda_fail(sv, e, "cudaMalloc(geometry)");
-    CS_CUDA(sv, cudaMemcpyAsync(p, sv.host.f[f].data(), bytes, cudaMemcpyHostToDevice, sv.stream));
-    sv.g.f[f] = p;
+    CS_CUDA(sv, cudaMemcpyAsync(p, m.host.f[f].data(), bytes, cudaMemcpyHostToDevice, sv.stream));
+    m.g.f[f] = p;
   }
-  int32_t* m = (int32_t*)dalloc(sv, sv.host.mask.size() * sizeof(int32_t), e);
-  if (!m) return cuda_fail(sv, e, "cudaMalloc(mask)");
-  CS_CUDA(sv, cudaMemcpyAsync(m, sv.host.mask.data(), sv.host.mask.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+  int32_t* mk = (int32_t*)mdalloc(sv, m, m.host.mask.size() * sizeof(int32_t), e);
+  if (!mk) return cuda_fail(sv, e, "cudaMalloc(mask)");
+  CS_CUDA(sv, cudaMemcpyAsync(mk, m.host.mask.data(), m.host.mask.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
                               sv.stream));
-  sv.g.mask = m;
-  int32_t* st = (int32_t*)dalloc(sv, sv.host.stencil.size() * sizeof(int32_t), e);
+  m.g.mask = mk;
+  int32_t* st = (int32_t*)mdalloc(sv, m, m.host.stencil.size() * sizeof(int32_t), e);
   if (!st) return cuda_fail(sv, e, "cudaMalloc(stencil)");
-  CS_CUDA(sv, cudaMemcpyAsync(st, sv.host.stencil.data(), sv.host.stencil.size() * sizeof(int32_t),
+  CS_CUDA(sv, cudaMemcpyAsync(st, m.host.stencil.data(), m.host.stencil.size() * sizeof(int32_t),
                               cudaMemcpyHostToDevice, sv.stream));
-  sv.g.st = st;
-  // State and work arrays.
-  sv.fp32 = (sv.p.flags & CS_FLAG_FP32) != 0;
-  if (int rc = sv.fp32 ? alloc_state(sv, sv.stF) : alloc_state(sv, sv.st)) return rc;
+  m.g.st = st;
   // Ghost-exchange map.
   std::vector<MapEntry> map;
   std::string why = build_fill_map(sv, map);
@@ -490,13 +471,12 @@ int upload_mesh(Solve& sv) {
   std::vector<int32_t> hs(n), hd(n);
   std::vector<uint8_t> hm(n);
   for (size_t t = 0; t < n; ++t) { hs[t] = map[t].src; hd[t] = map[t].dst; hm[t] = map[t].meta; }
-  FillMap& f = sv.fill;
+  FillMap& f = m.fill;
   f.n = (long long)n;
-  f.d_src = (int32_t*)dalloc(sv, n * sizeof(int32_t) + 16, e);
-  f.d_dst = (int32_t*)dalloc(sv, n * sizeof(int32_t) + 16, e);
-  f.d_meta = (uint8_t*)dalloc(sv, n + 16, e);
-  f.d_tmp = (double*)dalloc(sv, n * sizeof(double) + 16, e);
-  if (!f.d_src || !f.d_dst || !f.d_meta || !f.d_tmp) return cuda_fail(sv, e, "cudaMalloc(ghost map)");
+  f.d_src = (int32_t*)mdalloc(sv, m, n * sizeof(int32_t) + 16, e);
+  f.d_dst = (int32_t*)mdalloc(sv, m, n * sizeof(int32_t) + 16, e);
+  f.d_meta = (uint8_t*)mdalloc(sv, m, n + 16, e);
+  if (!f.d_src || !f.d_dst || !f.d_meta) return cuda_fail(sv, e, "cudaMalloc(ghost map)");
   CS_CUDA(sv, cudaMemcpyAsync(f.d_src, hs.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, sv.stream));
   CS_CUDA(sv, cudaMemcpyAsync(f.d_dst, hd.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, sv.stream));
   CS_CUDA(sv, cudaMemcpyAsync(f.d_meta, hm.data(), n, cudaMemcpyHostToDevice, sv.stream));
@@ -505,16 +485,16 @@ int upload_mesh(Solve& sv) {
     SyncMaps sm;
     why = build_sync_maps(sv, sm);
     if (!why.empty()) return fail(sv, CS_ERR_ARG, why);
-    PanelSync& ps = sv.psync;
+    PanelSync& ps = m.psync;
     ps.nf = (long long)sm.f_dst.size();
     ps.ne = (long long)sm.e_dst.size();
     auto up32 = [&](const std::vector<int32_t>& v, int32_t*& dptr) -> cudaError_t {
-      dptr = (int32_t*)dalloc(sv, v.size() * sizeof(int32_t) + 16, e);
+      dptr = (int32_t*)mdalloc(sv, m, v.size() * sizeof(int32_t) + 16, e);
       if (!dptr) return e;
       return cudaMemcpyAsync(dptr, v.data(), v.size() * sizeof(int32_t), cudaMemcpyHostToDevice, sv.stream);
     };
     auto up8 = [&](const std::vector<int8_t>& v, int8_t*& dptr) -> cudaError_t {
-      dptr = (int8_t*)dalloc(sv, v.size() + 16, e);
+      dptr = (int8_t*)mdalloc(sv, m, v.size() + 16, e);
       if (!dptr) return e;
       return cudaMemcpyAsync(dptr, v.data(), v.size(), cudaMemcpyHostToDevice, sv.stream);
     };
@@ -529,12 +509,98 @@ int upload_mesh(Solve& sv) {
     CS_CUDA(sv, up8(sm.e_sign, ps.e_sign));
     CS_CUDA(sv, cudaStreamSynchronize(sv.stream));
   }
-  launch_ops_build(sv);
-  if (sv.fp32 ? sv.stF.adp_lu != nullptr : sv.st.adp_lu != nullptr) launch_adp_factor(sv);
-  CS_CUDA(sv, cudaGetLastError());
-  CS_CUDA(sv, cudaStreamSynchronize(sv.stream));
   return CS_OK;
 }
+
+// Resident geometry-only operators of a new mesh, where the device has room
+// for them after the first solve's state, computed by that solve's stream.
+template <typename R>
+int mesh_operators(Solve& sv, MeshRes& m, DStateT<R>& s) {
+  const Dims& d = sv.d;
+  const size_t S6 = (size_t)6 * d.S;
+  cudaError_t e = cudaSuccess;
+  // ADP: the KKT matrix of every zone depends on the geometry only, so its
+  // factors are computed once here and each stage only substitutes.  They
+  // take 10.4 KB per zone; without room for them (or with
+  // CS_FLAG_NO_ADP_CACHE) every stage assembles and factors in place.
+  // The inverse normal matrices of the STEP 7.b / 9.c least squares are
+  // geometry-only as well (1.4 KB per zone together).
+  if (!(sv.p.flags & CS_FLAG_NO_OP_CACHE)) {
+    const long long nl = lsq_range_count(d);
+    size_t fr = 0, tot = 0;
+    const size_t bytes = (size_t)nl * (81 + 100) * sizeof(double);
+    if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && bytes + (size_t)8 * S6 * 60 < fr) {
+      m.op_m9 = (double*)mdalloc(sv, m, (size_t)nl * 81 * sizeof(double), e);
+      m.op_m10 = m.op_m9 ? (double*)mdalloc(sv, m, (size_t)nl * 100 * sizeof(double), e) : nullptr;
+      if (!m.op_m9 || !m.op_m10) return cuda_fail(sv, e, "cudaMalloc(least-squares operators)");
+    }
+  }
+  if (!(sv.p.flags & CS_FLAG_NO_ADP_CACHE)) {
+    const long long nf = adp_factor_doubles(d);
+    const size_t lu_bytes = (size_t)nf * sizeof(double), pv_bytes = (size_t)nf / 36;
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && lu_bytes + pv_bytes + (size_t)8 * S6 * 60 < fr) {
+      m.adp_lu = (double*)mdalloc(sv, m, lu_bytes, e);
+      m.adp_piv = m.adp_lu ? (int8_t*)mdalloc(sv, m, pv_bytes, e) : nullptr;
+      s.adp_rhs = m.adp_piv ? (double*)dalloc(sv, (size_t)adp_range_count(d) * 36 * sizeof(double), e) : nullptr;
+      if (!m.adp_lu || !m.adp_piv || !s.adp_rhs) return cuda_fail(sv, e, "cudaMalloc(ADP factors)");
+    }
+  }
+  s.op_m9 = m.op_m9;
+  s.op_m10 = m.op_m10;
+  s.adp_lu = m.adp_lu;
+  s.adp_piv = m.adp_piv;
+  launch_ops_build(sv);
+  if (m.adp_lu) launch_adp_factor(sv);
+  CS_CUDA(sv, cudaGetLastError());
+  return CS_OK;
+}
+
+}  // namespace
+
+std::string mesh_key(const cs_params& p) {
+  char b[320];
+  std::snprintf(b, sizeof b, "%d/%d/%d/%d/%.17g/%.17g/%.17g/%.17g/%d", p.ntp, p.nr, p.nghost, p.radial_mesh, p.rmin,
+                p.rmax, p.radial_ratio, p.smallnum,
+                p.flags & (CS_FLAG_NO_ADP_CACHE | CS_FLAG_NO_OP_CACHE | CS_FLAG_NO_PANEL_SYNC | CS_FLAG_FP32));
+  return b;
+}
+
+int mesh_attach(Solve& sv, const std::shared_ptr<MeshRes>& mp) {
+  sv.mesh = mp;
+  MeshRes& m = *mp;
+  if (m.host.f[0].empty()) {
+    std::string why = build_geometry(sv.p, m.host);
+    if (!why.empty()) return fail(sv, CS_ERR_ARG, why);
+  }
+  const Box& b = m.host.box;
+  Dims& d = sv.d;
+  d.N = b.N; d.nr = b.nr; d.G = b.G; d.NI = b.NI; d.NJ = b.NJ; d.NK = b.NK;
+  d.S = (long long)b.size();
+  CS_CUDA(sv, cudaGetDevice(&sv.device));
+  CS_CUDA(sv, cudaDeviceGetAttribute(&sv.sm_count, cudaDevAttrMultiProcessorCount, sv.device));
+  CS_CUDA(sv, cudaStreamCreateWithFlags(&sv.stream, cudaStreamNonBlocking));
+  set_adp_smem_limits();
+  const bool fresh = !m.on_device;
+  if (fresh)
+    if (int rc = mesh_upload(sv, m)) return rc;
+  sv.g = m.g;
+  sv.psync = m.psync;
+  sv.fill = m.fill;
+  cudaError_t e = cudaSuccess;
+  sv.fill.d_tmp = (double*)dalloc(sv, (size_t)sv.fill.n * sizeof(double) + 16, e);
+  if (!sv.fill.d_tmp) return cuda_fail(sv, e, "cudaMalloc(ghost staging)");
+  // State and work arrays.
+  sv.fp32 = (sv.p.flags & CS_FLAG_FP32) != 0;
+  if (int rc = sv.fp32 ? alloc_state(sv, sv.stF) : alloc_state(sv, sv.st)) return rc;
+  if (fresh)
+    if (int rc = sv.fp32 ? mesh_operators(sv, m, sv.stF) : mesh_operators(sv, m, sv.st)) return rc;
+  CS_CUDA(sv, cudaStreamSynchronize(sv.stream));
+  m.on_device = true;
+  return CS_OK;
+}
+
+namespace {
 
 int launch_check(Solve& sv, const char* what) {
   cudaError_t e = cudaGetLastError();
@@ -576,7 +642,7 @@ DStateT<R> first_stage_rates(const DStateT<R>& st) {
 //   stage 2: U* = U^n + delta dt F(U^n) + (1-delta) dt F(U2) + (1-gamma) dt S(U2)
 //            U^{n+1} = U* + gamma dt S(U^{n+1})
 // with face B and the entropy advanced by the same explicit weights.
-int run_stage_imex(Solve& sv, int irk, double dtcur) {
+int run_stage_imex(Solve& sv, int irk) {
   const double gam = 1.0 - 1.0 / std::sqrt(2.0), del = 1.0 - 1.0 / (2.0 * gam);
   prof_start(sv);
   launch_fill_ghosts(sv);
@@ -586,33 +652,34 @@ int run_stage_imex(Solve& sv, int irk, double dtcur) {
   if (irk == 1) {
     launch_save_stage0(sv);
     launch_save_stage1_rates(sv);
-    launch_update(sv, gam * dtcur);
+    launch_update(sv, gam);
   } else {
     launch_add_gravity(sv, (1.0 - gam) / (1.0 - del));
     launch_restore_stage0(sv);
     if (sv.fp32)
-      launch_update_with(sv, first_stage_rates(sv.stF), del * dtcur);
+      launch_update_with(sv, first_stage_rates(sv.stF), del);
     else
-      launch_update_with(sv, first_stage_rates(sv.st), del * dtcur);
-    launch_update(sv, (1.0 - del) * dtcur);
+      launch_update_with(sv, first_stage_rates(sv.st), del);
+    launch_update(sv, 1.0 - del);
   }
-  launch_gravity_implicit(sv, gam * dtcur);
+  launch_gravity_implicit(sv, gam);
   launch_cleanup(sv);
   return launch_check(sv, "stage launch");
 }
 
-int run_stage(Solve& sv, int irk, double dtcur) {
+// One RK stage of the scheme at the device-resident time step.
+int run_stage(Solve& sv, int irk) {
   const int ns = sv.p.rk_scheme == CS_SSPRK3 ? 3 : 2;
   if (irk < 1 || irk > ns) return fail(sv, CS_ERR_ARG, "irk out of range for the RK scheme");
-  if (sv.p.rk_scheme == CS_IMEX_RK2) return run_stage_imex(sv, irk, dtcur);
-  double dtmove = dtcur, a0 = 0.0;
+  if (sv.p.rk_scheme == CS_IMEX_RK2) return run_stage_imex(sv, irk);
+  double dtmove = 1.0, a0 = 0.0;  // dtmove: fraction of the step
   int kind = 0;
   if (sv.p.rk_scheme == CS_SSPRK3) {
     kind = 1;
-    if (irk == 2) { a0 = 0.75; dtmove = 0.25 * dtcur; }
-    if (irk == 3) { a0 = 1.0 / 3.0; dtmove = (2.0 / 3.0) * dtcur; }
+    if (irk == 2) { a0 = 0.75; dtmove = 0.25; }
+    if (irk == 3) { a0 = 1.0 / 3.0; dtmove = 2.0 / 3.0; }
   } else if (irk == 2) {
-    dtmove = 0.5 * dtcur;
+    dtmove = 0.5;
   }
   prof_start(sv);
   launch_fill_ghosts(sv);
@@ -625,6 +692,43 @@ int run_stage(Solve& sv, int irk, double dtcur) {
   launch_update(sv, dtmove);
   launch_cleanup(sv);
   return launch_check(sv, "stage launch");
+}
+
+// One whole step at the device-resident time step: the stages, then the
+// CFL reduction that leaves the next step on the device.
+int run_step(Solve& sv) {
+  const int ns = sv.p.rk_scheme == CS_SSPRK3 ? 3 : 2;
+  for (int irk = 1; irk <= ns; ++irk)
+    if (int rc = run_stage(sv, irk)) return rc;
+  prof_start(sv);
+  launch_timestep(sv);
+  return launch_check(sv, "timestep launch");
+}
+
+// The launches of run_step captured once into a CUDA graph on the solve's
+// stream (its buffers never move), so that a run of steps is one graph
+// launch per step and one host synchronisation at the end.
+int step_graph(Solve& sv) {
+  if (sv.graph_exec) return CS_OK;
+  const long long l0 = sv.launches;
+  cudaGraph_t g = nullptr;
+  CS_CUDA(sv, cudaStreamBeginCapture(sv.stream, cudaStreamCaptureModeThreadLocal));
+  const int rc = run_step(sv);
+  const cudaError_t e = cudaStreamEndCapture(sv.stream, &g);
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return cuda_fail(sv, e, "cudaStreamEndCapture(step)");
+  const cudaError_t ei = cudaGraphInstantiate(&sv.graph_exec, g, 0);
+  cudaGraphDestroy(g);
+  if (ei != cudaSuccess) {
+    sv.graph_exec = nullptr;
+    return cuda_fail(sv, ei, "cudaGraphInstantiate(step)");
+  }
+  sv.graph_kernels = sv.launches - l0;
+  sv.launches = l0;
+  return CS_OK;
 }
 
 int read_dt(Solve& sv, double* out) {
@@ -746,7 +850,26 @@ int cs_mesh_build(cs_ctx* ctx) {
   if (sv.has_mesh) return cs::fail(sv, CS_ERR_STATE, "mesh already built on this context");
   int rc = cs::ensure_host_mesh(sv);
   if (rc) return rc;
-  rc = cs::upload_mesh(sv);
+  rc = cs::mesh_attach(sv, sv.mesh);
+  if (rc) {
+    cs::free_all(sv);
+    return rc;
+  }
+  sv.has_mesh = true;
+  return CS_OK;
+}
+
+int cs_mesh_share(cs_ctx* ctx, const cs_ctx* from) {
+  if (!ctx || !from) return CS_ERR_ARG;
+  Solve& sv = ctx->sv;
+  if (sv.has_mesh) return cs::fail(sv, CS_ERR_STATE, "mesh already built on this context");
+  if (!from->sv.has_mesh) return cs::fail(sv, CS_ERR_STATE, "the source context has no device mesh");
+  if (cs::mesh_key(sv.p) != cs::mesh_key(from->sv.p))
+    return cs::fail(sv, CS_ERR_ARG, "the two contexts' mesh parameters differ");
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev != from->sv.device)
+    return cs::fail(sv, CS_ERR_ARG, "the source context lives on another device");
+  const int rc = cs::mesh_attach(sv, from->sv.mesh);
   if (rc) {
     cs::free_all(sv);
     return rc;
@@ -758,8 +881,8 @@ int cs_mesh_build(cs_ctx* ctx) {
 int cs_geometry_get(cs_ctx* ctx, int field, double* host_out, size_t n) {
   if (!ctx || !host_out || field < 0 || field >= CS_G_NFIELDS) return CS_ERR_ARG;
   Solve& sv = ctx->sv;
-  if (sv.host.f[0].empty()) return cs::fail(sv, CS_ERR_STATE, "no mesh: call cs_mesh_build or cs_mesh_build_host");
-  const std::vector<double>& v = sv.host.f[field];
+  if (sv.mesh->host.f[0].empty()) return cs::fail(sv, CS_ERR_STATE, "no mesh: call cs_mesh_build or cs_mesh_build_host");
+  const std::vector<double>& v = sv.mesh->host.f[field];
   if (n != v.size()) return cs::fail(sv, CS_ERR_ARG, "geometry buffer size mismatch");
   std::memcpy(host_out, v.data(), n * sizeof(double));
   return CS_OK;
@@ -768,18 +891,18 @@ int cs_geometry_get(cs_ctx* ctx, int field, double* host_out, size_t n) {
 int cs_mask_get(cs_ctx* ctx, int32_t* host_out, size_t n) {
   if (!ctx || !host_out) return CS_ERR_ARG;
   Solve& sv = ctx->sv;
-  if (sv.host.mask.empty()) return cs::fail(sv, CS_ERR_STATE, "no mesh");
-  if (n != sv.host.mask.size()) return cs::fail(sv, CS_ERR_ARG, "mask buffer size mismatch");
-  std::memcpy(host_out, sv.host.mask.data(), n * sizeof(int32_t));
+  if (sv.mesh->host.mask.empty()) return cs::fail(sv, CS_ERR_STATE, "no mesh");
+  if (n != sv.mesh->host.mask.size()) return cs::fail(sv, CS_ERR_ARG, "mask buffer size mismatch");
+  std::memcpy(host_out, sv.mesh->host.mask.data(), n * sizeof(int32_t));
   return CS_OK;
 }
 
 int cs_stencil_get(cs_ctx* ctx, int32_t* host_out, size_t n) {
   if (!ctx || !host_out) return CS_ERR_ARG;
   Solve& sv = ctx->sv;
-  if (sv.host.stencil.empty()) return cs::fail(sv, CS_ERR_STATE, "no mesh");
-  if (n != sv.host.stencil.size()) return cs::fail(sv, CS_ERR_ARG, "stencil buffer size mismatch");
-  std::memcpy(host_out, sv.host.stencil.data(), n * sizeof(int32_t));
+  if (sv.mesh->host.stencil.empty()) return cs::fail(sv, CS_ERR_STATE, "no mesh");
+  if (n != sv.mesh->host.stencil.size()) return cs::fail(sv, CS_ERR_ARG, "stencil buffer size mismatch");
+  std::memcpy(host_out, sv.mesh->host.stencil.data(), n * sizeof(int32_t));
   return CS_OK;
 }
 
@@ -803,7 +926,7 @@ int cs_init_problem_host(cs_ctx* ctx, const cs_init_desc* d, double* U, double* 
   Solve& sv = ctx->sv;
   int rc = cs::ensure_host_mesh(sv);
   if (rc) return rc;
-  std::string e = cs::init_problem_host(sv.p, *d, sv.host, U, ent, bxf, byf, bzf);
+  std::string e = cs::init_problem_host(sv.p, *d, sv.mesh->host, U, ent, bxf, byf, bzf);
   if (!e.empty()) return cs::fail(sv, CS_ERR_ARG, e);
   return CS_OK;
 }
@@ -874,7 +997,7 @@ int cs_init_problem(cs_ctx* ctx, const cs_init_desc* d) {
   if (int rc = cs::need(sv, false)) return rc;
   const size_t S6 = (size_t)6 * sv.d.S;
   std::vector<double> U(cs::NVAR * S6), ent(S6), bx(S6), by(S6), bz(S6);
-  std::string e = cs::init_problem_host(sv.p, *d, sv.host, U.data(), ent.data(), bx.data(), by.data(), bz.data());
+  std::string e = cs::init_problem_host(sv.p, *d, sv.mesh->host, U.data(), ent.data(), bx.data(), by.data(), bz.data());
   if (!e.empty()) return cs::fail(sv, CS_ERR_ARG, e);
   return cs_state_put(ctx, U.data(), ent.data(), bx.data(), by.data(), bz.data());
 }
@@ -884,7 +1007,8 @@ int cs_stage(cs_ctx* ctx, int32_t irk, double dtcur) {
   Solve& sv = ctx->sv;
   if (int rc = cs::need(sv, true)) return rc;
   if (!(dtcur > 0.0)) return cs::fail(sv, CS_ERR_ARG, "dtcur must be > 0");
-  return cs::run_stage(sv, irk, dtcur);
+  cs::launch_set_dt(sv, dtcur);
+  return cs::run_stage(sv, irk);
 }
 
 int cs_evaluate_timestep(cs_ctx* ctx, double dtcur, double* dtcurp1) {
@@ -893,7 +1017,8 @@ int cs_evaluate_timestep(cs_ctx* ctx, double dtcur, double* dtcurp1) {
   if (int rc = cs::need(sv, true)) return rc;
   if (!(dtcur > 0.0)) return cs::fail(sv, CS_ERR_ARG, "dtcur must be > 0");
   cs::prof_start(sv);
-  cs::launch_timestep(sv, dtcur);
+  cs::launch_set_dt(sv, dtcur);
+  cs::launch_timestep(sv);
   if (int rc = cs::launch_check(sv, "timestep launch")) return rc;
   return cs::read_dt(sv, dtcurp1);
 }
@@ -903,12 +1028,30 @@ int cs_step(cs_ctx* ctx, double dtcur, double* dtcurp1) {
   Solve& sv = ctx->sv;
   if (int rc = cs::need(sv, true)) return rc;
   if (!(dtcur > 0.0)) return cs::fail(sv, CS_ERR_ARG, "dtcur must be > 0");
-  const int ns = sv.p.rk_scheme == CS_SSPRK3 ? 3 : 2;
-  for (int irk = 1; irk <= ns; ++irk)
-    if (int rc = cs::run_stage(sv, irk, dtcur)) return rc;
-  cs::prof_start(sv);
-  cs::launch_timestep(sv, dtcur);
-  if (int rc = cs::launch_check(sv, "timestep launch")) return rc;
+  cs::launch_set_dt(sv, dtcur);
+  if (int rc = cs::run_step(sv)) return rc;
+  return cs::read_dt(sv, dtcurp1);
+}
+
+int cs_steps(cs_ctx* ctx, int32_t nsteps, double dtcur, double* dtcurp1) {
+  if (!ctx || !dtcurp1 || nsteps < 0) return CS_ERR_ARG;
+  Solve& sv = ctx->sv;
+  if (int rc = cs::need(sv, true)) return rc;
+  if (!(dtcur > 0.0)) return cs::fail(sv, CS_ERR_ARG, "dtcur must be > 0");
+  if (nsteps == 0) {
+    *dtcurp1 = dtcur;
+    return CS_OK;
+  }
+  cs::launch_set_dt(sv, dtcur);
+  if (sv.prof.on) {
+    // profiled: the same launches one by one, so each can be timed
+    for (int n = 0; n < nsteps; ++n)
+      if (int rc = cs::run_step(sv)) return rc;
+  } else {
+    if (int rc = cs::step_graph(sv)) return rc;
+    for (int n = 0; n < nsteps; ++n) CS_CUDA(sv, cudaGraphLaunch(sv.graph_exec, sv.stream));
+    sv.launches += sv.graph_kernels * nsteps;
+  }
   return cs::read_dt(sv, dtcurp1);
 }
 
@@ -986,7 +1129,8 @@ int cs_update_imex_rk_step_p1(cs_ctx* ctx, double dtmove) {
   if (!ctx) return CS_ERR_ARG;
   Solve& sv = ctx->sv;
   if (int rc = cs::need(sv, true)) return rc;
-  cs::launch_update(sv, dtmove);
+  cs::launch_set_dt(sv, dtmove);
+  cs::launch_update(sv, 1.0);
   return cs::launch_check(sv, "cs_update_imex_rk_step_p1");
 }
 
@@ -1038,8 +1182,8 @@ int cs_diag(cs_ctx* ctx, double* mass, double* energy, double* max_divb) {
   const size_t S6 = (size_t)6 * sv.d.S;
   std::vector<double> U(cs::NVAR * S6), ent(S6), bx(S6), by(S6), bz(S6);
   if (int rc = cs_state_get(ctx, U.data(), ent.data(), bx.data(), by.data(), bz.data())) return rc;
-  const cs::Box& b = sv.host.box;
-  const auto& G = sv.host.f;
+  const cs::Box& b = sv.mesh->host.box;
+  const auto& G = sv.mesh->host.f;
   double m = 0.0, en = 0.0, dv = 0.0;
   for (int p = 0; p < 6; ++p)
     for (int k = 1; k <= b.nr; ++k)

@@ -65,6 +65,7 @@ struct DStateT {
   int* err_flag;                         // device-side error bits (bounded waits that gave up)
   int32_t* giveup;                       // positivity give-up flags per zone
   unsigned long long* dtmin;             // CFL reduction target (bit pattern of a positive double)
+  double* dt;                            // the solve's current time step (device scalar)
 };
 using DState = DStateT<double>;
 
@@ -429,15 +430,19 @@ void launch_edges(Solve& s);
 void launch_sources(Solve& s);
 void launch_save_stage0(Solve& s);
 void launch_combine(Solve& s, double a0, int kind);
-void launch_update(Solve& s, double dtmove);
+// Update, CT and implicit gravity advance by scale times the device-resident
+// time step (DStateT::dt), which launch_set_dt sets and launch_timestep
+// replaces with the next step.
+void launch_update(Solve& s, double scale);
 template <typename R>
-void launch_update_with(Solve& s, const DStateT<R>& st, double dtmove);
-void launch_gravity_implicit(Solve& s, double a);
+void launch_update_with(Solve& s, const DStateT<R>& st, double scale);
+void launch_gravity_implicit(Solve& s, double scale);
 void launch_add_gravity(Solve& s, double c);
 void launch_save_stage1_rates(Solve& s);
 void launch_restore_stage0(Solve& s);
 void launch_cleanup(Solve& s);
-void launch_timestep(Solve& s, double dtcur);
+void launch_timestep(Solve& s);
+void launch_set_dt(Solve& s, double dt);
 void launch_fill_ghosts(Solve& s);
 
 }  // namespace cs

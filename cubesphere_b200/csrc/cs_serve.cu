@@ -19,35 +19,48 @@
 
 namespace cs {
 
-// Device bytes cs_mesh_build allocates for these parameters (state, work
-// arrays, ghost and panel maps, and the resident operators unless the flags
-// turn them off), with a margin for allocation granularity.
-size_t estimate_device_bytes(const cs_params& p) {
+// Device bytes of one solve's own state and work arrays, and of the mesh
+// resources it shares with other solves on the same mesh (geometry, maps,
+// resident operators), with margins for allocation granularity.
+size_t state_device_bytes(const cs_params& p) {
   const Box b(p.ntp, p.nr, p.nghost);
   const size_t S6 = (size_t)6 * b.size();
   // words per point of the state's type: U 8 + entropy 4, V 80 + E 30 +
   // E snapshot 3, flattener 3, face contributions 48, entropy fluxes 3,
   // speeds 6, dU/dt 8, U0 8, ent0 1, face states 270 (IMEX: + 11);
-  // FP64 in both forms: geometry 126, face B 3, face-B quadrature 15,
-  // EMFs 3, saved faces 3 (IMEX: + 3)
+  // FP64 in both forms: face B 3, face-B quadrature 15, EMFs 3, saved
+  // faces 3 (IMEX: + 3)
   size_t rwords = 12 + 113 + 3 + 48 + 3 + 6 + 8 + 8 + 1 + 270;
-  size_t dwords = 126 + 3 + 15 + 3 + 3;
+  size_t dwords = 3 + 15 + 3 + 3;
   if (p.rk_scheme == CS_IMEX_RK2) {
     rwords += 11;
     dwords += 3;
   }
   const size_t rsize = (p.flags & CS_FLAG_FP32) ? sizeof(float) : sizeof(double);
-  size_t bytes = (rwords * rsize + dwords * sizeof(double)) * S6 + S6 * 2 * sizeof(int32_t);
+  size_t bytes = (rwords * rsize + dwords * sizeof(double)) * S6 + S6 * sizeof(int32_t);
+  // ghost staging values (one per map entry, see mesh_device_bytes)
+  bytes += (size_t)6 * 4 * (p.nghost + 1) * (p.ntp + 2 * p.nghost + 1) * (p.nr + 2 * p.nghost + 1) * 12 * 8;
+  const size_t na = (size_t)6 * (p.ntp + 2 * p.nghost - 2) * (p.ntp + 2 * p.nghost - 2) * (p.nr + 2 * p.nghost - 2);
+  if (!(p.flags & CS_FLAG_NO_ADP_CACHE)) bytes += na * 36 * sizeof(double);  // ADP right-hand sides
+  return bytes + ((size_t)64 << 20);
+}
+
+size_t mesh_device_bytes(const cs_params& p) {
+  const Box b(p.ntp, p.nr, p.nghost);
+  const size_t S6 = (size_t)6 * b.size();
+  // geometry 126 words, mask and stencil
+  size_t bytes = 126 * S6 * sizeof(double) + S6 * sizeof(int32_t) + (size_t)6 * 48 * b.NI * b.NJ;
   // ghost map: per panel 4 strips of G layers, 12 field words per point,
-  // 17 bytes per entry (offsets, meta, staging value)
-  bytes += (size_t)6 * 4 * (p.nghost + 1) * (p.ntp + 2 * p.nghost + 1) * (p.nr + 2 * p.nghost + 1) * 12 * 17;
-  bytes += (size_t)128 << 20;
+  // 9 bytes per entry (offsets, meta); panel-ownership maps are smaller
+  bytes += (size_t)6 * 4 * (p.nghost + 1) * (p.ntp + 2 * p.nghost + 1) * (p.nr + 2 * p.nghost + 1) * 12 * 9 * 2;
   const size_t nl = (size_t)6 * (p.ntp + 2 * p.nghost - 4) * (p.ntp + 2 * p.nghost - 4) * (p.nr + 2 * p.nghost - 4);
   const size_t na = (size_t)6 * (p.ntp + 2 * p.nghost - 2) * (p.ntp + 2 * p.nghost - 2) * (p.nr + 2 * p.nghost - 2);
   if (!(p.flags & CS_FLAG_NO_OP_CACHE)) bytes += nl * 181 * sizeof(double);
-  if (!(p.flags & CS_FLAG_NO_ADP_CACHE)) bytes += (na + 128) * (1296 * 8 + 36 + 36 * 8);
-  return bytes;
+  if (!(p.flags & CS_FLAG_NO_ADP_CACHE)) bytes += (na + 128) * (1296 * 8 + 36);
+  return bytes + ((size_t)64 << 20);
 }
+
+size_t estimate_device_bytes(const cs_params& p) { return state_device_bytes(p) + mesh_device_bytes(p); }
 
 namespace {
 
@@ -60,9 +73,19 @@ struct Request {
   int status = -1;  // -1 pending or running, else the final cs_status
   std::string err;
   double mass = 0, energy = 0, divb = 0, dt_last = 0;
-  size_t bytes = 0;
+  size_t bytes = 0;      // own state, reserved while it runs
+  std::string mesh;      // mesh key
+  bool mesh_builder = false;
+  bool mesh_reused = false;
   long long zone_updates = 0;
   std::vector<double> U, ent, bx, by, bz;  // final state (when kept)
+};
+
+// A resident mesh of the server's cache: built by the first request that
+// needs it, then shared by every later request on the same mesh.
+struct MeshEntry {
+  std::shared_ptr<MeshRes> mesh;  // null while it is being built
+  size_t bytes = 0;               // estimated device bytes, reserved while cached
 };
 
 }  // namespace
@@ -80,7 +103,9 @@ struct cs_server {
   int active = 0;
   int keep_state = 0;
   int device = 0;
-  size_t budget = 0, reserved = 0;
+  size_t budget = 0, reserved = 0;  // reserved: running states + cached meshes
+  std::map<std::string, cs::MeshEntry> meshes;
+  long long mesh_builds = 0;
   int64_t next_id = 1;
   bool started = false;
   cs::Clock::time_point t0, t_last_done;
@@ -101,13 +126,45 @@ void run_request(cs_server* sv, int64_t id) {
   }
   cs_ctx* ctx = nullptr;
   int rc = cs_create(&r->req.params, &ctx);
-  if (!rc) rc = cs_mesh_build(ctx);
+  if (!rc && r->mesh_builder) {
+    rc = cs_mesh_build(ctx);
+    {
+      std::lock_guard<std::mutex> lk(sv->mu);
+      auto it = sv->meshes.find(r->mesh);
+      if (rc) {
+        sv->reserved -= it->second.bytes;
+        sv->meshes.erase(it);
+      } else {
+        it->second.mesh = ctx->sv.mesh;
+        sv->mesh_builds += 1;
+      }
+    }
+    sv->cv.notify_all();
+  } else if (!rc) {
+    std::shared_ptr<MeshRes> m;
+    {
+      std::unique_lock<std::mutex> lk(sv->mu);
+      sv->cv.wait(lk, [&] {
+        auto it = sv->meshes.find(r->mesh);
+        return it == sv->meshes.end() || it->second.mesh != nullptr;
+      });
+      auto it = sv->meshes.find(r->mesh);
+      if (it != sv->meshes.end()) m = it->second.mesh;
+    }
+    if (!m) {
+      rc = cs_mesh_build(ctx);  // its builder failed: build a private mesh
+    } else {
+      rc = mesh_attach(ctx->sv, m);
+      if (!rc) ctx->sv.has_mesh = true;  // on failure cs_destroy below frees what it left
+      r->mesh_reused = !rc;
+    }
+  }
   if (!rc) rc = cs_init_problem(ctx, &r->req.init);
   double dt = 1e30, dtn = 0.0;
   if (!rc) rc = cs_evaluate_timestep(ctx, dt, &dtn);
   dt = dtn;
-  for (int s = 0; !rc && s < r->req.steps; ++s) {
-    rc = cs_step(ctx, dt, &dtn);
+  if (!rc && r->req.steps > 0) {
+    rc = cs_steps(ctx, r->req.steps, dt, &dtn);  // graph replay, one host sync
     dt = dtn;
   }
   double m = 0, e = 0, dv = 0;
@@ -152,9 +209,31 @@ void run_request(cs_server* sv, int64_t id) {
   sv->cv.notify_all();
 }
 
+// Device bytes a request needs beyond what is reserved already: its own
+// state, plus its mesh unless that is cached (or being built).
+size_t admission_bytes(cs_server* sv, const Request& r) {
+  return r.bytes + (sv->meshes.count(r.mesh) ? 0 : mesh_device_bytes(r.req.params));
+}
+
+// Frees cached meshes that no running solve uses, oldest key first, until
+// `need` more bytes fit in the budget; returns whether they do.
+bool make_room(cs_server* sv, size_t need) {
+  for (auto it = sv->meshes.begin(); sv->reserved + need > sv->budget && it != sv->meshes.end();) {
+    if (it->second.mesh && it->second.mesh.use_count() == 1) {
+      sv->reserved -= it->second.bytes;
+      it = sv->meshes.erase(it);
+    } else {
+      ++it;
+    }
+  }
+  return sv->reserved + need <= sv->budget;
+}
+
 // Admission: the oldest pending request starts when a slot is free and its
-// estimated device memory fits in what the running requests leave of the
-// budget.  A request larger than the whole budget fails at once.
+// estimated device memory (its state, plus its mesh unless the mesh is
+// cached) fits in what the running requests and the cached meshes leave of
+// the budget; idle cached meshes are freed to make room.  A request larger
+// than the whole budget fails at once.
 void scheduler(cs_server* sv) {
   cudaSetDevice(sv->device);
   std::unique_lock<std::mutex> lk(sv->mu);
@@ -163,18 +242,26 @@ void scheduler(cs_server* sv) {
       if (sv->stop) return true;
       if (sv->pending.empty() || sv->active >= sv->max_active) return false;
       const Request& r = sv->reqs[sv->pending.front()];
-      return r.bytes > sv->budget || sv->reserved + r.bytes <= sv->budget;
+      const size_t need = admission_bytes(sv, r);
+      return r.bytes + mesh_device_bytes(r.req.params) > sv->budget || make_room(sv, need);
     });
     if (sv->stop) break;
     const int64_t id = sv->pending.front();
     sv->pending.pop_front();
     Request& r = sv->reqs[id];
-    if (r.bytes > sv->budget) {
+    if (r.bytes + mesh_device_bytes(r.req.params) > sv->budget) {
       r.status = CS_ERR_NOMEM;
       r.err = "request needs more device memory than the server's budget";
       r.t_start = r.t_done = Clock::now();
       sv->cv.notify_all();
       continue;
+    }
+    if (!sv->meshes.count(r.mesh)) {
+      MeshEntry me;
+      me.bytes = mesh_device_bytes(r.req.params);
+      sv->reserved += me.bytes;
+      sv->meshes[r.mesh] = me;
+      r.mesh_builder = true;
     }
     sv->reserved += r.bytes;
     sv->active += 1;
@@ -212,7 +299,8 @@ int cs_serve_submit(cs_server* sv, const cs_request* req, int64_t* id) {
   cs::Request r;
   r.req = *req;
   r.t_submit = cs::Clock::now();
-  r.bytes = cs::estimate_device_bytes(req->params);
+  r.bytes = cs::state_device_bytes(req->params);
+  r.mesh = cs::mesh_key(req->params);
   {
     std::lock_guard<std::mutex> lk(sv->mu);
     r.id = sv->next_id++;
@@ -236,7 +324,7 @@ int cs_serve_wait(cs_server* sv, int64_t id, cs_serve_result* out) {
   sv->cv.wait(lk, [&] { return it->second.status >= 0; });
   const cs::Request& r = it->second;
   out->status = r.status;
-  out->reserved = 0;
+  out->mesh_reused = r.mesh_reused ? 1 : 0;
   out->latency_s = std::chrono::duration<double>(r.t_done - r.t_submit).count();
   out->queue_s = std::chrono::duration<double>(r.t_start - r.t_submit).count();
   out->mass = r.mass;

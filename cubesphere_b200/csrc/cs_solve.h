@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <cstring>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -47,6 +48,31 @@ struct Prof {
   std::vector<long long> count;
 };
 
+// What depends on the mesh parameters only: the host geometry, its device
+// copy, the ghost-exchange and panel-ownership maps and the resident
+// geometry-only operators.  Built once and shared read-only by every solve
+// on the same mesh (cs_mesh_share, the serving mesh cache); freed with its
+// last user.
+struct MeshRes {
+  GeomHost host;
+  DGeom g{};
+  FillMap fill{};       // d_tmp stays null here: the staging buffer is per solve
+  PanelSync psync{};
+  double* op_m9 = nullptr;
+  double* op_m10 = nullptr;
+  double* adp_lu = nullptr;
+  int8_t* adp_piv = nullptr;
+  std::vector<void*> allocs;
+  size_t bytes = 0;     // device bytes held
+  bool on_device = false;
+  MeshRes() = default;
+  MeshRes(const MeshRes&) = delete;
+  MeshRes& operator=(const MeshRes&) = delete;
+  ~MeshRes() {
+    for (void* q : allocs) cudaFree(q);
+  }
+};
+
 struct Solve {
   cs_params p{};
   Dims d{};
@@ -55,7 +81,7 @@ struct Solve {
   DState st{};                // state of the plain (FP64) form
   DStateT<float> stF{};       // state of the precision (FP32 bulk) form
   bool fp32 = false;          // which of the two this solve uses
-  GeomHost host;             // host geometry (kept for cs_geometry_get)
+  std::shared_ptr<MeshRes> mesh = std::make_shared<MeshRes>();
   std::vector<void*> allocs;  // device allocations owned by the solve
   FillMap fill;
   PanelSync psync;
@@ -64,9 +90,19 @@ struct Solve {
   int sm_count = 148;
   bool has_mesh = false, has_state = false;
   long long launches = 0;  // kernels launched by this solve
+  cudaGraphExec_t graph_exec = nullptr;  // one step, captured by cs_steps
+  long long graph_kernels = 0;           // kernels in that graph
   Prof prof;
   std::string err;
 };
+
+// Attaches a solve (parameters set, no mesh yet) to a resident mesh and
+// allocates its own state; builds the mesh first when it is not on the
+// device yet.  Defined with the C ABI.
+int mesh_attach(Solve& sv, const std::shared_ptr<MeshRes>& m);
+// Identity of the mesh a parameter set needs (solves with equal keys can
+// share one MeshRes).
+std::string mesh_key(const cs_params& p);
 
 // Called after every launch (kernel == false for copies): counts kernel
 // launches and, when profiling, records an event on the stream.
@@ -83,3 +119,8 @@ inline int blocks_for(long long n, int threads, int sm_count) {
 }
 
 }  // namespace cs
+
+// The opaque context of the C ABI: one resident solve.
+struct cs_ctx {
+  cs::Solve sv;
+};

@@ -136,9 +136,11 @@ __global__ void k_combine(CombineSeg<R> sg, long long total, double a0, int kind
 }
 
 // Zone update (484:212-372): U += dt dU/dt on every zone, then on the
-// interior the entropy update and the conserved->primitive repair.
+// interior the entropy update and the conserved->primitive repair.  The
+// time step is scale times the device-resident step of the solve.
 template <typename R>
-__global__ void k_update_zones(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r, R dt) {
+__global__ void k_update_zones(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r, double scale) {
+  const R dt = (R)(scale * *s.dt);
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
     r.decode(t, p, i, j, k);
@@ -179,7 +181,8 @@ __device__ __forceinline__ double vang(const DGeom& g, const Dims& d, int p, int
 // Constrained-transport face update (484:376-906): Stokes circulation of
 // the edge EMFs with spherical arc lengths for the angular edges.
 template <typename R>
-__global__ void k_ct(Dims d, DGeom g, DStateT<R> s, Range3 r, int dir, double dt) {
+__global__ void k_ct(Dims d, DGeom g, DStateT<R> s, Range3 r, int dir, double scale) {
+  const double dt = scale * *s.dt;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
     r.decode(t, p, i, j, k);
@@ -288,7 +291,14 @@ __global__ void k_cleanup_zones(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 
   }
 }
 
-__global__ void k_set_u64(unsigned long long* p, unsigned long long v) { *p = v; }
+__global__ void k_set_f64(double* p, double v) { *p = v; }
+
+// The CFL reduction starts from 1.1 times the current step (490:121-286);
+// its result becomes the solve's next step.
+__global__ void k_dt_start(const double* dt, unsigned long long* dtmin) {
+  *dtmin = (unsigned long long)__double_as_longlong(1.1 * *dt);
+}
+__global__ void k_dt_commit(const unsigned long long* dtmin, double* dt) { *dt = __longlong_as_double((long long)*dtmin); }
 
 // CFL limit over the active interior zones; the minimum positive double is
 // found with an integer atomicMin on its bit pattern (positive IEEE doubles
@@ -387,28 +397,28 @@ void launch_combine(Solve& sv, double a0, int kind) {
 }
 
 template <typename R>
-void launch_update_with(Solve& sv, const DStateT<R>& st, double dtmove) {
+void launch_update_with(Solve& sv, const DStateT<R>& st, double scale) {
   const Dims& d = sv.d;
   Range3 z = zones_all(d);
-  k_update_zones<R><<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, z, dtmove);
+  k_update_zones<R><<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, z, scale);
   mark(sv, "k_update_zones");
   const int N = d.N, nr = d.nr;
   Range3 fx = {0, N, 1, N, 1, nr}, fy = {1, N, 0, N, 1, nr}, fz = {1, N, 1, N, 0, nr};
-  k_ct<R><<<blocks_for(fx.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, st, fx, 0, dtmove);
+  k_ct<R><<<blocks_for(fx.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, st, fx, 0, scale);
   mark(sv, "k_ct");
-  k_ct<R><<<blocks_for(fy.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, st, fy, 1, dtmove);
+  k_ct<R><<<blocks_for(fy.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, st, fy, 1, scale);
   mark(sv, "k_ct");
-  k_ct<R><<<blocks_for(fz.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, st, fz, 2, dtmove);
+  k_ct<R><<<blocks_for(fz.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, st, fz, 2, scale);
   mark(sv, "k_ct");
 }
 template void launch_update_with<double>(Solve&, const DStateT<double>&, double);
 template void launch_update_with<float>(Solve&, const DStateT<float>&, double);
 
-void launch_update(Solve& sv, double dtmove) {
+void launch_update(Solve& sv, double scale) {
   if (sv.fp32)
-    launch_update_with(sv, sv.stF, dtmove);
+    launch_update_with(sv, sv.stF, scale);
   else
-    launch_update_with(sv, sv.st, dtmove);
+    launch_update_with(sv, sv.st, scale);
 }
 
 // ---- IMEX-RK2: ARS(2,2,2) with the point-mass gravity implicit ----
@@ -417,7 +427,8 @@ void launch_update(Solve& sv, double dtmove) {
 // so the implicit stage U = U* + a S(U) has the closed form
 // m = m* - a rho g, E = E* - a m . g.
 template <typename R>
-__global__ void k_gravity_implicit(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r, R a) {
+__global__ void k_gravity_implicit(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r, double scale) {
+  const R a = (R)(scale * *s.dt);
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
     r.decode(t, p, i, j, k);
@@ -462,17 +473,18 @@ __global__ void k_add_gravity(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r,
 }
 
 template <typename R>
-void launch_gravity_implicit_t(Solve& sv, const DStateT<R>& st, double a) {
+void launch_gravity_implicit_t(Solve& sv, const DStateT<R>& st, double scale) {
   Range3 z = {0, sv.d.N + 1, 0, sv.d.N + 1, 0, sv.d.nr + 1};
-  k_gravity_implicit<R><<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(sv.d, sv.ph, sv.g, st, z, a);
+  k_gravity_implicit<R><<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(sv.d, sv.ph, sv.g, st, z,
+                                                                                        scale);
   mark(sv, "k_gravity_implicit");
 }
-void launch_gravity_implicit(Solve& sv, double a) {
+void launch_gravity_implicit(Solve& sv, double scale) {
   if (!(sv.ph.gm > sv.p.smallnum)) return;
   if (sv.fp32)
-    launch_gravity_implicit_t(sv, sv.stF, a);
+    launch_gravity_implicit_t(sv, sv.stF, scale);
   else
-    launch_gravity_implicit_t(sv, sv.st, a);
+    launch_gravity_implicit_t(sv, sv.st, scale);
 }
 
 template <typename R>
@@ -540,22 +552,25 @@ void launch_cleanup(Solve& sv) {
 }
 
 template <typename R>
-void launch_timestep_t(Solve& sv, const DStateT<R>& st, double dtcur) {
-  const double start = 1.1 * dtcur;
-  unsigned long long bits;
-  static_assert(sizeof(bits) == sizeof(start), "double is 64-bit");
-  std::memcpy(&bits, &start, sizeof(bits));
-  k_set_u64<<<1, 1, 0, sv.stream>>>(st.dtmin, bits);
-  mark(sv, "k_set_u64");
+void launch_timestep_t(Solve& sv, const DStateT<R>& st) {
+  k_dt_start<<<1, 1, 0, sv.stream>>>(st.dt, st.dtmin);
+  mark(sv, "k_dt_start");
   Range3 r = {1, sv.d.N, 1, sv.d.N, 1, sv.d.nr};
   k_timestep<R><<<blocks_for(r.count(), 256, sv.sm_count), 256, 0, sv.stream>>>(sv.d, sv.ph, sv.g, st, r);
   mark(sv, "k_timestep");
+  k_dt_commit<<<1, 1, 0, sv.stream>>>(st.dtmin, st.dt);
+  mark(sv, "k_dt_commit");
 }
-void launch_timestep(Solve& sv, double dtcur) {
+void launch_timestep(Solve& sv) {
   if (sv.fp32)
-    launch_timestep_t(sv, sv.stF, dtcur);
+    launch_timestep_t(sv, sv.stF);
   else
-    launch_timestep_t(sv, sv.st, dtcur);
+    launch_timestep_t(sv, sv.st);
+}
+
+void launch_set_dt(Solve& sv, double dt) {
+  k_set_f64<<<1, 1, 0, sv.stream>>>(sv.fp32 ? sv.stF.dt : sv.st.dt, dt);
+  mark(sv, "k_set_dt");
 }
 
 }  // namespace cs

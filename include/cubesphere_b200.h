@@ -159,6 +159,17 @@ const char* cs_params_check(const cs_params* p);
 
 /* Mesh: builds the 6-panel geometry on the host and keeps it resident on the device. */
 int cs_mesh_build(cs_ctx* ctx);
+/* Mesh shared with another context: ctx (created, no mesh yet) uses the
+ * resident mesh of `from` (geometry, ghost-exchange and panel-ownership
+ * maps, resident operators) instead of building its own, and allocates only
+ * its state.  The parameters that define the mesh (ntp, nr, nghost,
+ * radial_mesh, rmin, rmax, radial_ratio, smallnum and the NO_ADP_CACHE,
+ * NO_OP_CACHE, NO_PANEL_SYNC and FP32 flags) must be equal, and both
+ * contexts on the current device.  The mesh is freed with the last context
+ * that uses it.  The reference builds the mesh once per patch and run
+ * (MAKE_MESH_GNOMONIC_CS_SECTOR, 201) and has no counterpart for sharing
+ * it between solves. */
+int cs_mesh_share(cs_ctx* ctx, const cs_ctx* from);
 /* Host-only mesh build (no device is touched); the geometry, mask and
  * stencil getters below then work without a GPU. */
 int cs_mesh_build_host(cs_ctx* ctx);
@@ -188,6 +199,14 @@ int cs_state_get(cs_ctx* ctx, double* U, double* ent,
 /* Whole-stage and whole-step entry points (device resident, on ctx's stream). */
 int cs_stage(cs_ctx* ctx, int32_t irk, double dtcur);
 int cs_step(cs_ctx* ctx, double dtcur, double* dtcurp1);
+/* nsteps steps, each at the time step the previous one chose (the driver's
+ * time loop, 1000riemann_geomesh_cs_mhd.f:1738-2908, with dtcur taken from
+ * EVALUATE_TIMESTEP after every step); the same results as nsteps calls of
+ * cs_step feeding each dtcurp1 into the next.  The time step stays on the
+ * device between steps, the step is captured once into a CUDA graph and
+ * replayed, and the host synchronises once, at the end, to return the next
+ * time step.  (Without the graph while cs_profile_begin is active.) */
+int cs_steps(cs_ctx* ctx, int32_t nsteps, double dtcur, double* dtcurp1);
 int cs_evaluate_timestep(cs_ctx* ctx, double dtcur, double* dtcurp1);
 int cs_synchronize(cs_ctx* ctx);
 
@@ -260,13 +279,17 @@ int cs_snapshot_read_host(const char* path, const cs_params* p, double* U, doubl
 
 /* Serving (no counterpart in the reference, whose driver runs one solve per
  * job).  A server admits solve requests as they arrive while device memory
- * allows (mem_fraction of the free memory at creation, counted with
- * cs_estimate_device_bytes) and runs at most max_active at once, each in its
- * own context and stream driven by its own host thread, so requests that
- * arrive while others run overlap with them on the device.  A request runs
- * cs_mesh_build, cs_init_problem, steps x cs_step and cs_diag; its result
- * does not depend on what else runs (every kernel is deterministic).
- * Latency is measured from submission to completion. */
+ * allows (mem_fraction of the free memory at creation) and runs at most
+ * max_active at once, each in its own context and stream driven by its own
+ * host thread, so requests that arrive while others run overlap with them
+ * on the device.  Meshes stay resident between requests: the first request
+ * on a mesh builds it (cs_mesh_build), later requests with the same mesh
+ * parameters attach to it (as cs_mesh_share) and allocate only their state;
+ * a cached mesh that no running request uses is freed when an admission
+ * needs its memory.  A request then runs cs_init_problem, cs_steps and
+ * cs_diag; its result does not depend on what else runs (every kernel
+ * is deterministic).  Latency is measured from submission to completion.
+ * cs_estimate_device_bytes counts a solve's state and its mesh. */
 typedef struct cs_server cs_server;
 typedef struct cs_request {
   cs_params params;
@@ -276,7 +299,7 @@ typedef struct cs_request {
 } cs_request;
 typedef struct cs_serve_result {
   int32_t status;       /* cs_status of the request */
-  int32_t reserved;
+  int32_t mesh_reused;  /* 1 when the request ran on a cached resident mesh */
   double latency_s;     /* submission to completion */
   double queue_s;       /* submission to admission */
   double mass, energy, max_divb;  /* cs_diag of the final state */

@@ -148,3 +148,28 @@ def test_steps_keep_div_b_at_roundoff_across_panel_edges(shell16):
     m, e, divb = s.diag()
     bmax = np.abs(faces(s, s.get_state()["bxf"], 0)).max()
     assert divb < 1e-12 * bmax, divb / bmax
+
+
+@pytest.mark.parametrize("name,rk,flags", [("shell16", cs.CS_IMEX_RK2, 0), ("surface32", cs.CS_SSPRK3, 0),
+                                           ("shell16", cs.CS_RK2, 0), ("shell16", cs.CS_IMEX_RK2, cs.CS_FLAG_FP32)])
+def test_steps_graph_matches_step_loop(name, rk, flags):
+    """cs_steps (one captured step replayed, time step kept on the device)
+    gives bit for bit the state and time step of the cs_step loop."""
+    pr = cs.preset(name)
+    pr["params"]["rk_scheme"] = rk
+    out = []
+    for graph in (False, True):
+        s = cs.Solve(**pr["params"], flags=flags)
+        s.mesh_build()
+        s.init_problem(**pr["init"])
+        dt = s.evaluate_timestep(1e30)
+        if graph:
+            dt = s.steps(3, dt)
+        else:
+            for _ in range(3):
+                dt = s.step(dt)
+        out.append((dt, s.get_state()))
+    (d0, s0), (d1, s1) = out
+    assert d0 == d1
+    for k in s0:
+        assert np.array_equal(s0[k], s1[k]), k

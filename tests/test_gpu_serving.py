@@ -56,3 +56,58 @@ def test_request_larger_than_the_budget_is_refused():
     rid = srv.submit(1, *_req(16, 8, 1))
     assert srv.wait(rid).status == 4  # CS_ERR_NOMEM
     srv.close()
+
+
+def test_requests_on_one_mesh_share_it_and_match_a_private_build():
+    """The first request on a mesh builds it; later requests with the same
+    mesh parameters (different seeds) run on the cached resident mesh and
+    give the same state as a solve that builds its own mesh."""
+    pa, ia = _req(16, 8, 21)
+    srv = cs.Server(max_active=2, keep_state=True)
+    first = srv.submit(2, pa, ia)
+    assert srv.wait(first).status == 0
+    ids = [srv.submit(2, pa, dict(ia, seed=22 + q)) for q in range(3)]
+    res = [srv.wait(i) for i in ids]
+    assert srv.wait(first).mesh_reused == 0
+    assert all(r.status == 0 and r.mesh_reused == 1 for r in res)
+    served = srv.state(ids[-1], cs.make_params(**pa))
+    srv.close()
+    s = cs.Solve(**pa)
+    s.mesh_build()
+    s.init_problem(**dict(ia, seed=24))
+    dt = s.evaluate_timestep(1e30)
+    for _ in range(2):
+        dt = s.step(dt)
+    own = s.get_state()
+    for k in own:
+        assert np.array_equal(own[k], served[k]), k
+
+
+def test_mesh_share_gives_the_same_steps():
+    pa, ia = _req(16, 4, 31)
+    a = cs.Solve(**pa)
+    a.mesh_build()
+    b = cs.Solve(**pa)
+    b.mesh_share(a)
+    for s in (a, b):
+        s.init_problem(**ia)
+    da, db = a.evaluate_timestep(1e30), b.evaluate_timestep(1e30)
+    for _ in range(2):
+        da, db = a.step(da), b.step(db)
+    assert da == db
+    sa, sb = a.get_state(), b.get_state()
+    for k in sa:
+        assert np.array_equal(sa[k], sb[k]), k
+    a.close()  # the mesh lives on with b
+    db = b.step(db)
+    assert np.isfinite(b.get_state()["U"]).all()
+
+
+def test_mesh_share_refuses_another_mesh():
+    pa, _ = _req(16, 4, 1)
+    pb, _ = _req(16, 8, 1)
+    a = cs.Solve(**pa)
+    a.mesh_build()
+    b = cs.Solve(**pb)
+    with pytest.raises(cs.CsError):
+        b.mesh_share(a)
