@@ -84,6 +84,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-form sample")
     ap.add_argument("--no-precision", action="store_true", help="skip the FP32 precision-form sample")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-form sample")
     ap.add_argument("--profile-json", default="", help="also write the per-kernel device times here")
     return ap.parse_args()
 
@@ -224,6 +225,67 @@ def serving_sample(seed: int = 7, nreq: int = 24, rate: float = 8.0, max_active:
             "f32_vs_f64_sequential": f32["zone_updates_per_s"] / max(seq["zone_updates_per_s"], 1e-30),
             "sizes": "N in {32,48,64}, nr in {1,16,32}, 20-60 steps (IMEX-RK2 shells, SSP-RK3 surfaces); "
                      "latency = submission to completion, mesh builds included"}
+
+
+def batch_sample(seed: int = 11, nsol: int = 16, steps: int = 4) -> dict:
+    """Batched form on a bounded sample: nsol independent solves with panel N
+    from {32, 48, 64} and radial depth from {1, 16, 32} (seeded), in the
+    precision form, advanced together (one graph launch per step, launch
+    shapes autotuned per size class) and, for comparison, one after another
+    (cs_steps per member), each over `steps` steps, timed by the host clock
+    around calls that return after the device work has finished; solves on
+    equal meshes share one resident mesh."""
+    import numpy as np
+    import torch
+
+    import cubesphere_b200 as cs
+
+    rng = np.random.default_rng(seed)
+    sols, meshes = [], {}
+    for q in range(nsol):
+        ntp = int(rng.choice([32, 48, 64]))
+        nr = int(rng.choice([1, 16, 32]))
+        pr = cs.preset("shell16")
+        params, init = dict(pr["params"]), dict(pr["init"])
+        params.update(ntp=ntp, nr=nr, nghost=4 if nr > 1 else 3, flags=cs.CS_FLAG_FP32)
+        init.update(seed=int(rng.integers(1, 1 << 30)))
+        if nr == 1:
+            params.update(gm=0.0, rmin=1.0, rmax=1.05, radial_mesh="uniform", rk_scheme=cs.CS_SSPRK3)
+            init.update(kind=0, v_amp=0.5, p0=1.0, rho_amp=0.1, a_amp=0.1)
+        s = cs.Solve(**params)
+        if (ntp, nr) in meshes:
+            s.mesh_share(meshes[(ntp, nr)])
+        else:
+            s.mesh_build()
+            meshes[(ntp, nr)] = s
+        s.init_problem(**init)
+        sols.append(s)
+    zones = sum(6 * s.N * s.N * s.nr for s in sols)
+    dts = [s.evaluate_timestep(1e30) for s in sols]
+    b = cs.Batch(sols)
+    t_tune = time.perf_counter()
+    b.autotune(1)
+    t_tune = time.perf_counter() - t_tune
+    fr = sorted({b.grid_fraction(q) for q in range(nsol)})
+    dts = b.steps(1, dts)  # warm-up: builds the batch graph
+    torch.cuda.synchronize()
+    # every call below returns after reading the members' next time steps,
+    # i.e. after their device work has finished
+    t0 = time.perf_counter()
+    dts = b.steps(steps, dts)
+    bat_s = time.perf_counter() - t0
+    b.close()
+    t0 = time.perf_counter()
+    dts = [s.steps(steps, d) for s, d in zip(sols, dts)]  # one member after another
+    seq_s = time.perf_counter() - t0
+    ok = all(np.isfinite(d) and d > 0 for d in dts)
+    for s in sols:
+        s.close()
+    return {"solves": nsol, "zones": zones, "steps": steps, "dtype": "f32 bulk (precision form)",
+            "batched_zone_updates_per_s": zones * steps / bat_s,
+            "sequential_zone_updates_per_s": zones * steps / seq_s,
+            "autotune_s": t_tune, "grid_fractions_chosen": fr, "distinct_meshes": len(meshes), "finite": ok,
+            "sizes": "N in {32,48,64}, nr in {1,16,32}; host wall clock around the device-synchronised runs"}
 
 
 def precision_sample(pr, dts, steps, ref_state, zones, world, allmax) -> dict:
@@ -441,6 +503,10 @@ def run_gpu(args):
     if ref_state is not None:
         torch.cuda.synchronize()
         precision = precision_sample(pr, dts, args.steps, ref_state, zones, world, allmax)
+    batch = None
+    if not args.no_batch:
+        torch.cuda.synchronize()
+        batch = batch_sample()
     serving = None
     if not args.no_serving:
         torch.cuda.synchronize()
@@ -464,7 +530,7 @@ def run_gpu(args):
         "roofline": roof, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches,
         "top_kernels": {k: round(v[0] / args.steps, 3) for k, v in
                         sorted(prof.items(), key=lambda kv: -kv[1][0])[:8]},
-        "finite": finite, "dt_last": dt, "precision_form": precision, "serving": serving,
+        "finite": finite, "dt_last": dt, "precision_form": precision, "batch": batch, "serving": serving,
     }
     if rank == 0:
         print(json.dumps(out), flush=True)

@@ -49,6 +49,8 @@ EXPORTS = [
     "cs_debug_get", "cs_diag", "cs_get_stream", "cs_launch_count", "cs_profile_begin", "cs_profile_end",
     "cs_cfl_timestep_noalloc", "cs_estimate_device_bytes", "cs_serve_create", "cs_serve_submit",
     "cs_serve_wait", "cs_serve_state", "cs_serve_stats", "cs_serve_destroy",
+    "cs_batch_create", "cs_batch_steps", "cs_batch_autotune", "cs_batch_grid_fraction", "cs_batch_last_error",
+    "cs_batch_destroy",
     "cs_snapshot_save", "cs_snapshot_load", "cs_snapshot_write_host", "cs_snapshot_read_host",
 ]
 
@@ -169,6 +171,14 @@ def load_library() -> ctypes.CDLL:
         "cs_serve_state": ([P, ctypes.c_int64, dp, dp, dp, dp, dp], ctypes.c_int),
         "cs_serve_stats": ([P, dp, dp, dp, ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
         "cs_serve_destroy": ([P], ctypes.c_int),
+        "cs_batch_create": ([ctypes.POINTER(ctypes.c_void_p), ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)],
+                            ctypes.c_int),
+        "cs_batch_steps": ([P, ctypes.c_int32, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)],
+                           ctypes.c_int),
+        "cs_batch_autotune": ([P, ctypes.c_int32, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
+        "cs_batch_grid_fraction": ([P, ctypes.c_int32, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
+        "cs_batch_last_error": ([P], ctypes.c_char_p),
+        "cs_batch_destroy": ([P], ctypes.c_int),
         "cs_snapshot_save": ([P, ctypes.c_char_p, D, D, ctypes.c_int64], ctypes.c_int),
         "cs_snapshot_load": ([P, ctypes.c_char_p, dp, dp, ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
         "cs_snapshot_write_host": ([ctypes.c_char_p, ctypes.POINTER(CsParams), dp, dp, dp, dp, dp, D, D,
@@ -410,6 +420,53 @@ def geometry_single_zone(isector: int, ntp_global: int, nr_global: int, iscale: 
     if rc:
         raise CsError(f"cs_geometry_single_zone failed ({rc})")
     return out
+
+
+class Batch:
+    """Batched form: independent solves advanced together, one CUDA graph
+    launch per step for all members (each member's step a child graph)."""
+
+    def __init__(self, members: list):
+        self.lib = load_library()
+        self.members = list(members)
+        arr = (ctypes.c_void_p * len(self.members))(*[m.h.value for m in self.members])
+        h = ctypes.c_void_p()
+        rc = self.lib.cs_batch_create(arr, len(self.members), ctypes.byref(h))
+        if rc:
+            raise CsError(f"cs_batch_create failed ({rc})")
+        self.h = h
+
+    def _check(self, rc: int, what: str) -> None:
+        if rc:
+            raise CsError(f"{what} failed ({rc}): {self.lib.cs_batch_last_error(self.h).decode()}")
+
+    def steps(self, nsteps: int, dts) -> list:
+        n = len(self.members)
+        din = (ctypes.c_double * n)(*dts)
+        dout = (ctypes.c_double * n)()
+        self._check(self.lib.cs_batch_steps(self.h, nsteps, din, dout), "cs_batch_steps")
+        return list(dout)
+
+    def autotune(self, trial_steps: int = 2) -> float:
+        ms = ctypes.c_double()
+        self._check(self.lib.cs_batch_autotune(self.h, trial_steps, ctypes.byref(ms)), "cs_batch_autotune")
+        return ms.value
+
+    def grid_fraction(self, member: int) -> float:
+        f = ctypes.c_double()
+        self._check(self.lib.cs_batch_grid_fraction(self.h, member, ctypes.byref(f)), "cs_batch_grid_fraction")
+        return f.value
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.cs_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Server:

@@ -14,10 +14,6 @@
 #include "cs_solve.h"
 
 namespace cs {
-namespace {
-
-const int kNbr[6][4] = {{3, 6, 2, 5}, {1, 4, 3, 6}, {2, 5, 1, 4}, {5, 2, 6, 3}, {6, 3, 4, 1}, {4, 1, 5, 2}};
-
 int fail(Solve& sv, int code, const std::string& msg) {
   sv.err = msg;
   return code;
@@ -26,6 +22,10 @@ int fail(Solve& sv, int code, const std::string& msg) {
 int cuda_fail(Solve& sv, cudaError_t e, const char* what) {
   return fail(sv, CS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
+
+namespace {
+
+const int kNbr[6][4] = {{3, 6, 2, 5}, {1, 4, 3, 6}, {2, 5, 1, 4}, {5, 2, 6, 3}, {6, 3, 4, 1}, {4, 1, 5, 2}};
 
 #define CS_CUDA(sv, call)                                   \
   do {                                                      \
@@ -49,8 +49,7 @@ void free_all(Solve& sv) {
   sv.prof.name.clear();
   for (void* p : sv.allocs) cudaFree(p);
   sv.allocs.clear();
-  if (sv.graph_exec) cudaGraphExecDestroy(sv.graph_exec);
-  sv.graph_exec = nullptr;
+  drop_graph(sv);
   if (sv.stream) cudaStreamDestroy(sv.stream);
   sv.stream = nullptr;
   sv.mesh = std::make_shared<MeshRes>();  // drops this solve's share of the mesh
@@ -694,6 +693,8 @@ int run_stage(Solve& sv, int irk) {
   return launch_check(sv, "stage launch");
 }
 
+}  // namespace
+
 // One whole step at the device-resident time step: the stages, then the
 // CFL reduction that leaves the next step on the device.
 int run_step(Solve& sv) {
@@ -715,20 +716,28 @@ int step_graph(Solve& sv) {
   CS_CUDA(sv, cudaStreamBeginCapture(sv.stream, cudaStreamCaptureModeThreadLocal));
   const int rc = run_step(sv);
   const cudaError_t e = cudaStreamEndCapture(sv.stream, &g);
+  sv.graph_kernels = sv.launches - l0;
+  sv.launches = l0;
   if (rc) {
     if (g) cudaGraphDestroy(g);
     return rc;
   }
   if (e != cudaSuccess) return cuda_fail(sv, e, "cudaStreamEndCapture(step)");
   const cudaError_t ei = cudaGraphInstantiate(&sv.graph_exec, g, 0);
-  cudaGraphDestroy(g);
   if (ei != cudaSuccess) {
+    cudaGraphDestroy(g);
     sv.graph_exec = nullptr;
     return cuda_fail(sv, ei, "cudaGraphInstantiate(step)");
   }
-  sv.graph_kernels = sv.launches - l0;
-  sv.launches = l0;
+  sv.graph = g;
   return CS_OK;
+}
+
+void drop_graph(Solve& sv) {
+  if (sv.graph_exec) cudaGraphExecDestroy(sv.graph_exec);
+  if (sv.graph) cudaGraphDestroy(sv.graph);
+  sv.graph_exec = nullptr;
+  sv.graph = nullptr;
 }
 
 int read_dt(Solve& sv, double* out) {
@@ -744,6 +753,8 @@ int read_dt(Solve& sv, double* out) {
   std::memcpy(out, &bits, sizeof(bits));
   return CS_OK;
 }
+
+namespace {
 
 // Device-to-host copy of one debug array; arrays of the state's type R
 // are widened to double on the host.

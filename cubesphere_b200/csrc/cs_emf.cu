@@ -245,14 +245,14 @@ void launch_edges_t(Solve& sv, DStateT<R>& st) {
   Range3 ex = {1, N, 0, N, 0, nr};
   Range3 ey = {0, N, 1, N, 0, nr};
   Range3 ez = {0, N, 0, N, 1, nr};
-  k_edges_x<R><<<blocks_for(ex.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, st, ex);
+  k_edges_x<R><<<blocks_for(ex.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.g, st, ex);
   mark(sv, "k_edges_x");
-  k_edges_y<R><<<blocks_for(ey.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, st, ey);
+  k_edges_y<R><<<blocks_for(ey.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.g, st, ey);
   mark(sv, "k_edges_y");
-  k_edges_z<R><<<blocks_for(ez.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, st, ez);
+  k_edges_z<R><<<blocks_for(ez.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.g, st, ez);
   mark(sv, "k_edges_z");
   if (sv.psync.ne > 0) {
-    k_sync_emf<R><<<blocks_for(sv.psync.ne, 128, sv.sm_count), 128, 0, sv.stream>>>(st, sv.psync);
+    k_sync_emf<R><<<blocks_for(sv.psync.ne, 128, grid_sms(sv)), 128, 0, sv.stream>>>(st, sv.psync);
     mark(sv, "k_sync_emf");
   }
 }

@@ -362,21 +362,21 @@ void launch_fluxes_t(Solve& sv, DStateT<R>& st) {
   Range3 fy = {0, N + 1, -1, N + 1, 0, nr + 1};
   Range3 fz = {0, N + 1, 0, N + 1, -1, nr + 1};
   Range3 zs = {-1, N + 2, -1, N + 2, -1, nr + 2};
-  k_face_states<R><<<blocks_for(zs.count(), FS_TPB, sv.sm_count), FS_TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, zs);
+  k_face_states<R><<<blocks_for(zs.count(), FS_TPB, grid_sms(sv)), FS_TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, zs);
   mark(sv, "k_face_states");
   const Range3 fr[3] = {fx, fy, fz};
   for (int dir = 0; dir < 3; ++dir) {
     const long long nt = (fr[dir].count() + FLUX_FACES - 1) / FLUX_FACES;
-    const int nb = (int)std::min<long long>(nt, (long long)sv.sm_count * 32);
+    const int nb = (int)std::min<long long>(nt, (long long)grid_sms(sv) * 32);
     k_flux<R><<<nb, FLUX_FACES * 5, 0, sv.stream>>>(d, sv.ph, sv.g, st, fr[dir], dir);
     mark(sv, "k_flux");
   }
   if (sv.psync.nf > 0) {
-    k_sync_flux<R><<<blocks_for(sv.psync.nf, 128, sv.sm_count), 128, 0, sv.stream>>>(d, st, sv.psync);
+    k_sync_flux<R><<<blocks_for(sv.psync.nf, 128, grid_sms(sv)), 128, 0, sv.stream>>>(d, st, sv.psync);
     mark(sv, "k_sync_flux");
   }
   Range3 z = {0, N + 1, 0, N + 1, 0, nr + 1};
-  k_gather<R><<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, st, z);
+  k_gather<R><<<blocks_for(z.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.g, st, z);
   mark(sv, "k_gather");
 }
 
@@ -392,7 +392,7 @@ void launch_sources_t(Solve& sv, DStateT<R>& st) {
   if (!(sv.ph.gm > sv.p.smallnum)) return;
   const Dims& d = sv.d;
   Range3 z = {0, d.N + 1, 0, d.N + 1, 0, d.nr + 1};
-  k_sources<R><<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, z);
+  k_sources<R><<<blocks_for(z.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, z);
   mark(sv, "k_sources");
 }
 

@@ -1334,7 +1334,7 @@ template <typename R>
 void launch_prim_and_masks_t(Solve& sv, DStateT<R>& st) {
   const Dims& d = sv.d;
   Range3 z = zones_all(d);
-  k_prim<R><<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, z);
+  k_prim<R><<<blocks_for(z.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, z);
   mark(sv, "k_prim");
   launch_face_masks(sv);
 }
@@ -1350,9 +1350,9 @@ template <typename R>
 void launch_face_masks_t(Solve& sv, DStateT<R>& st) {
   const Dims& d = sv.d;
   Range3 f = {-d.G, d.N + d.G, -d.G, d.N + d.G, -d.G, d.nr + d.G};
-  k_zero_masked_faces<R><<<blocks_for(f.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, st, f);
+  k_zero_masked_faces<R><<<blocks_for(f.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.g, st, f);
   mark(sv, "k_zero_masked_faces");
-  k_tricorner<R><<<blocks_for(6LL * 4 * d.G * (d.NK - 1), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, st);
+  k_tricorner<R><<<blocks_for(6LL * 4 * d.G * (d.NK - 1), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.g, st);
   mark(sv, "k_tricorner");
 }
 
@@ -1367,7 +1367,7 @@ template <typename R>
 void launch_flattener_t(Solve& sv, DStateT<R>& st) {
   const Dims& d = sv.d;
   Range3 z = zones_all(d);
-  const int nb = blocks_for(z.count(), TPB, sv.sm_count);
+  const int nb = blocks_for(z.count(), TPB, grid_sms(sv));
   k_flat_a<R><<<nb, TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, z);
   mark(sv, "k_flat_a");
   k_flat_bc<R><<<nb, TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, z, st.flatA, st.flatB, 0);
@@ -1387,12 +1387,12 @@ template <typename R>
 void launch_weno_t(Solve& sv, DStateT<R>& st) {
   const Dims& d = sv.d;
   Range3 a = shrink(d, 1), b = shrink(d, 2);
-  k_weno7a<R><<<blocks_for(a.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, a);
+  k_weno7a<R><<<blocks_for(a.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, a);
   mark(sv, "k_weno7a");
   if (st.op_m9)
-    k_weno7b<true, R><<<blocks_for(b.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
+    k_weno7b<true, R><<<blocks_for(b.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
   else
-    k_weno7b<false, R><<<blocks_for(b.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
+    k_weno7b<false, R><<<blocks_for(b.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
   mark(sv, "k_weno7b");
 }
 
@@ -1407,9 +1407,9 @@ template <typename R>
 void launch_positivity_t(Solve& sv, DStateT<R>& st) {
   const Dims& d = sv.d;
   Range3 z = zones_all(d);
-  k_positivity<R><<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, z);
+  k_positivity<R><<<blocks_for(z.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, z);
   mark(sv, "k_positivity");
-  k_apply_giveup<R><<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, st, z);
+  k_apply_giveup<R><<<blocks_for(z.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, st, z);
   mark(sv, "k_apply_giveup");
 }
 
@@ -1427,18 +1427,18 @@ void launch_faceB_adp_t(Solve& sv, DStateT<R>& st) {
   Range3 fx = {1 - G, N + G - 1, 2 - G, N + G - 1, 2 - G, nr + G - 1};
   Range3 fy = {2 - G, N + G - 1, 1 - G, N + G - 1, 2 - G, nr + G - 1};
   Range3 fz = {2 - G, N + G - 1, 2 - G, N + G - 1, 1 - G, nr + G - 1};
-  k_faceB<R><<<blocks_for(fx.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, fx, 0);
+  k_faceB<R><<<blocks_for(fx.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, fx, 0);
   mark(sv, "k_faceB");
-  k_faceB<R><<<blocks_for(fy.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, fy, 1);
+  k_faceB<R><<<blocks_for(fy.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, fy, 1);
   mark(sv, "k_faceB");
-  k_faceB<R><<<blocks_for(fz.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, fz, 2);
+  k_faceB<R><<<blocks_for(fz.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, fz, 2);
   mark(sv, "k_faceB");
   Range3 a = shrink(d, 1);
   if (st.adp_lu) {
-    k_adp_rhs<R><<<blocks_for(a.count(), ADPR_TPB, sv.sm_count), ADPR_TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, a);
+    k_adp_rhs<R><<<blocks_for(a.count(), ADPR_TPB, grid_sms(sv)), ADPR_TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, a);
     mark(sv, "k_adp_rhs");
     const long long nblk = (a.count() + ADP_ZB - 1) / ADP_ZB;
-    const int grid = (int)std::min<long long>(nblk, (long long)sv.sm_count * 2);
+    const int grid = (int)std::min<long long>(nblk, (long long)grid_sms(sv) * 2);
     k_adp_solve<R><<<grid, ADPS_THREADS, sizeof(AdpsSmem), sv.stream>>>(d, sv.ph, sv.g, st, a);
     mark(sv, "k_adp_solve");
     return;
@@ -1446,7 +1446,7 @@ void launch_faceB_adp_t(Solve& sv, DStateT<R>& st) {
   const size_t smem = sizeof(AdpSmem) * ADP_WARPS;
   long long nwarps = a.count();
   long long nblk = (nwarps + ADP_WARPS - 1) / ADP_WARPS;
-  long long cap = (long long)sv.sm_count * 16;
+  long long cap = (long long)grid_sms(sv) * 16;
   if (nblk > cap) nblk = cap;
   k_adp<false, R><<<(int)nblk, 32 * ADP_WARPS, smem, sv.stream>>>(d, sv.ph, sv.g, st, a);
   mark(sv, "k_adp");
@@ -1467,11 +1467,11 @@ void launch_ops_build_t(Solve& sv, DStateT<R>& st) {
   const Dims& d = sv.d;
   Range3 b = shrink(d, 2);
   if (st.op_m9) {
-    k_ops_m9<R><<<blocks_for(b.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
+    k_ops_m9<R><<<blocks_for(b.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
     mark(sv, "k_ops_m9");
   }
   if (st.op_m10) {
-    k_ops_m10<R><<<blocks_for(b.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
+    k_ops_m10<R><<<blocks_for(b.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
     mark(sv, "k_ops_m10");
   }
 }
@@ -1503,7 +1503,7 @@ void launch_adp_factor_t(Solve& sv, DStateT<R>& st) {
   Range3 a = shrink(d, 1);
   const size_t smem = sizeof(AdpSmem) * ADP_WARPS;
   long long nblk = (a.count() + ADP_WARPS - 1) / ADP_WARPS;
-  long long cap = (long long)sv.sm_count * 16;
+  long long cap = (long long)grid_sms(sv) * 16;
   if (nblk > cap) nblk = cap;
   k_adp<true, R><<<(int)nblk, 32 * ADP_WARPS, smem, sv.stream>>>(d, sv.ph, sv.g, st, a);
   mark(sv, "k_adp_factor");
@@ -1520,14 +1520,14 @@ template <typename R>
 void launch_efield_t(Solve& sv, DStateT<R>& st) {
   const Dims& d = sv.d;
   Range3 z = zones_all(d), a = shrink(d, 1), b = shrink(d, 2);
-  k_efield_a<R><<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, st, z);
+  k_efield_a<R><<<blocks_for(z.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.g, st, z);
   mark(sv, "k_efield_a");
-  k_efield_b<R><<<blocks_for(a.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, a);
+  k_efield_b<R><<<blocks_for(a.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, a);
   mark(sv, "k_efield_b");
   if (st.op_m10)
-    k_efield_c<true, R><<<blocks_for(b.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
+    k_efield_c<true, R><<<blocks_for(b.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
   else
-    k_efield_c<false, R><<<blocks_for(b.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
+    k_efield_c<false, R><<<blocks_for(b.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
   mark(sv, "k_efield_c");
 }
 

@@ -90,8 +90,10 @@ struct Solve {
   int sm_count = 148;
   bool has_mesh = false, has_state = false;
   long long launches = 0;  // kernels launched by this solve
-  cudaGraphExec_t graph_exec = nullptr;  // one step, captured by cs_steps
+  cudaGraph_t graph = nullptr;           // one step, captured by cs_steps / cs_batch_steps
+  cudaGraphExec_t graph_exec = nullptr;  // its executable form
   long long graph_kernels = 0;           // kernels in that graph
+  double grid_frac = 1.0;                // share of the SMs a launch's grid is sized for (autotuned in batches)
   Prof prof;
   std::string err;
 };
@@ -100,6 +102,16 @@ struct Solve {
 // allocates its own state; builds the mesh first when it is not on the
 // device yet.  Defined with the C ABI.
 int mesh_attach(Solve& sv, const std::shared_ptr<MeshRes>& m);
+// One whole step at the device-resident time step (stages and CFL
+// reduction), and its capture into sv.graph / sv.graph_exec (kept until
+// drop_graph or the solve's end).  Defined with the C ABI.
+int run_step(Solve& sv);
+int step_graph(Solve& sv);
+void drop_graph(Solve& sv);
+// Device-to-host read of the next time step and of the error flags.
+int read_dt(Solve& sv, double* out);
+int fail(Solve& sv, int code, const std::string& msg);
+int cuda_fail(Solve& sv, cudaError_t e, const char* what);
 // Identity of the mesh a parameter set needs (solves with equal keys can
 // share one MeshRes).
 std::string mesh_key(const cs_params& p);
@@ -109,6 +121,13 @@ std::string mesh_key(const cs_params& p);
 void mark(Solve& sv, const char* name, bool kernel = true);
 // Records the start event of a profiled sequence (no-op when off).
 void prof_start(Solve& sv);
+
+// SMs a launch of this solve sizes its grid for (every kernel loops over
+// its range with a grid stride, so the grid size never changes results).
+inline int grid_sms(const Solve& sv) {
+  const int n = (int)(sv.sm_count * sv.grid_frac + 0.5);
+  return n < 1 ? 1 : n;
+}
 
 inline int blocks_for(long long n, int threads, int sm_count) {
   long long b = (n + threads - 1) / threads;

@@ -341,14 +341,14 @@ template <typename R>
 void launch_fill_ghosts_t(Solve& sv, const DStateT<R>& st) {
   const FillMap& f = sv.fill;
   if (f.n > 0) {
-    const int nb = blocks_for(f.n, 256, sv.sm_count);
+    const int nb = blocks_for(f.n, 256, grid_sms(sv));
     k_fill_gather<R><<<nb, 256, 0, sv.stream>>>(st, f.d_src, f.d_dst, f.d_meta, f.d_tmp, f.n);
     mark(sv, "k_fill_gather");
     k_fill_scatter<R><<<nb, 256, 0, sv.stream>>>(st, f.d_dst, f.d_meta, f.d_tmp, f.n);
     mark(sv, "k_fill_scatter");
   }
   const int n1 = sv.d.N + 2 * sv.d.G;
-  k_pad_radial<R><<<blocks_for(6LL * n1 * n1, TPB, sv.sm_count), TPB, 0, sv.stream>>>(sv.d, sv.g, st, sv.p.bc_lower,
+  k_pad_radial<R><<<blocks_for(6LL * n1 * n1, TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(sv.d, sv.g, st, sv.p.bc_lower,
                                                                                       sv.p.bc_upper);
   mark(sv, "k_pad_radial");
 }
@@ -386,7 +386,7 @@ void launch_combine_t(Solve& sv, const DStateT<R>& st, double a0, int kind) {
   sg.b[1] = st.Byf;   sg.b0[1] = st.B0[1]; sg.n[3] = S6;
   sg.b[2] = st.Bzf;   sg.b0[2] = st.B0[2]; sg.n[4] = S6;
   const long long total = (NVAR + 4) * S6;
-  k_combine<R><<<blocks_for(total, 256, sv.sm_count), 256, 0, sv.stream>>>(sg, total, a0, kind);
+  k_combine<R><<<blocks_for(total, 256, grid_sms(sv)), 256, 0, sv.stream>>>(sg, total, a0, kind);
   mark(sv, "k_combine");
 }
 void launch_combine(Solve& sv, double a0, int kind) {
@@ -400,15 +400,15 @@ template <typename R>
 void launch_update_with(Solve& sv, const DStateT<R>& st, double scale) {
   const Dims& d = sv.d;
   Range3 z = zones_all(d);
-  k_update_zones<R><<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, z, scale);
+  k_update_zones<R><<<blocks_for(z.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, z, scale);
   mark(sv, "k_update_zones");
   const int N = d.N, nr = d.nr;
   Range3 fx = {0, N, 1, N, 1, nr}, fy = {1, N, 0, N, 1, nr}, fz = {1, N, 1, N, 0, nr};
-  k_ct<R><<<blocks_for(fx.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, st, fx, 0, scale);
+  k_ct<R><<<blocks_for(fx.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.g, st, fx, 0, scale);
   mark(sv, "k_ct");
-  k_ct<R><<<blocks_for(fy.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, st, fy, 1, scale);
+  k_ct<R><<<blocks_for(fy.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.g, st, fy, 1, scale);
   mark(sv, "k_ct");
-  k_ct<R><<<blocks_for(fz.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(d, sv.g, st, fz, 2, scale);
+  k_ct<R><<<blocks_for(fz.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.g, st, fz, 2, scale);
   mark(sv, "k_ct");
 }
 template void launch_update_with<double>(Solve&, const DStateT<double>&, double);
@@ -475,7 +475,7 @@ __global__ void k_add_gravity(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r,
 template <typename R>
 void launch_gravity_implicit_t(Solve& sv, const DStateT<R>& st, double scale) {
   Range3 z = {0, sv.d.N + 1, 0, sv.d.N + 1, 0, sv.d.nr + 1};
-  k_gravity_implicit<R><<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(sv.d, sv.ph, sv.g, st, z,
+  k_gravity_implicit<R><<<blocks_for(z.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(sv.d, sv.ph, sv.g, st, z,
                                                                                         scale);
   mark(sv, "k_gravity_implicit");
 }
@@ -490,7 +490,7 @@ void launch_gravity_implicit(Solve& sv, double scale) {
 template <typename R>
 void launch_add_gravity_t(Solve& sv, const DStateT<R>& st, double c) {
   Range3 z = {0, sv.d.N + 1, 0, sv.d.N + 1, 0, sv.d.nr + 1};
-  k_add_gravity<R><<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(sv.d, sv.ph, sv.g, st, z, c);
+  k_add_gravity<R><<<blocks_for(z.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(sv.d, sv.ph, sv.g, st, z, c);
   mark(sv, "k_add_gravity");
 }
 void launch_add_gravity(Solve& sv, double c) {
@@ -540,7 +540,7 @@ void launch_restore_stage0(Solve& sv) {
 template <typename R>
 void launch_cleanup_t(Solve& sv, const DStateT<R>& st) {
   Range3 z = zones_all(sv.d);
-  k_cleanup_zones<R><<<blocks_for(z.count(), TPB, sv.sm_count), TPB, 0, sv.stream>>>(sv.d, sv.ph, sv.g, st, z);
+  k_cleanup_zones<R><<<blocks_for(z.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(sv.d, sv.ph, sv.g, st, z);
   mark(sv, "k_cleanup_zones");
 }
 void launch_cleanup(Solve& sv) {
@@ -556,7 +556,7 @@ void launch_timestep_t(Solve& sv, const DStateT<R>& st) {
   k_dt_start<<<1, 1, 0, sv.stream>>>(st.dt, st.dtmin);
   mark(sv, "k_dt_start");
   Range3 r = {1, sv.d.N, 1, sv.d.N, 1, sv.d.nr};
-  k_timestep<R><<<blocks_for(r.count(), 256, sv.sm_count), 256, 0, sv.stream>>>(sv.d, sv.ph, sv.g, st, r);
+  k_timestep<R><<<blocks_for(r.count(), 256, grid_sms(sv)), 256, 0, sv.stream>>>(sv.d, sv.ph, sv.g, st, r);
   mark(sv, "k_timestep");
   k_dt_commit<<<1, 1, 0, sv.stream>>>(st.dtmin, st.dt);
   mark(sv, "k_dt_commit");

@@ -315,6 +315,29 @@ int cs_serve_state(cs_server* sv, int64_t id, double* U, double* ent,
 int cs_serve_stats(cs_server* sv, double* p50_s, double* p99_s, double* zone_updates_per_s, int64_t* completed);
 int cs_serve_destroy(cs_server* sv);                                   /* waits for every request */
 
+/* Batched form (no counterpart in the reference): independent solves of
+ * different sizes (each its own context, mesh, state and time step, all on
+ * the current device) advanced together.  Each member's step is captured
+ * once into a CUDA graph (the capture cs_steps uses) and the batch embeds
+ * every member's step as an independent child of one graph, so that one
+ * graph launch advances every member by one step and the device runs the
+ * members side by side.  cs_batch_steps takes and returns one time step per
+ * member (dtcur[n], dtcurp1[n]) and gives every member the same results as
+ * cs_steps on it alone.  cs_batch_autotune chooses, per size class (members
+ * with equal mesh parameters), the share of the SMs each launch's grid is
+ * sized for (1, 1/2, 1/4 or 1/8; every kernel strides over its range, so
+ * results do not change) by timing trial_steps batch steps per candidate,
+ * and restores the members' states afterwards; it returns the best batch
+ * step time in ms.  Members must not be stepped elsewhere while in a batch;
+ * destroying the batch leaves them to the caller. */
+typedef struct cs_batch cs_batch;
+int cs_batch_create(cs_ctx* const* members, int32_t n, cs_batch** out);
+int cs_batch_steps(cs_batch* b, int32_t nsteps, const double* dtcur, double* dtcurp1);
+int cs_batch_autotune(cs_batch* b, int32_t trial_steps, double* best_ms_per_step);
+int cs_batch_grid_fraction(const cs_batch* b, int32_t member, double* frac);
+const char* cs_batch_last_error(const cs_batch* b);
+int cs_batch_destroy(cs_batch* b);
+
 /* Diagnostics: sums over interior zones of 6 panels of volume-weighted
  * mass, energy and the max |div B| (face-area-weighted, per volume). */
 int cs_diag(cs_ctx* ctx, double* mass, double* energy, double* max_divb);
