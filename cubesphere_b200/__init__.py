@@ -85,6 +85,7 @@ CS_FLAG_NO_ADP_CACHE = 1
 CS_FLAG_NO_OP_CACHE = 2
 CS_FLAG_NO_PANEL_SYNC = 4
 CS_FLAG_FP32 = 8
+CS_FLAG_ADP_PER_PANEL = 16
 
 
 def make_params(**kw) -> CsParams:

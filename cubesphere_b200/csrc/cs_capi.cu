@@ -409,6 +409,7 @@ int alloc_state(Solve& sv, DStateT<R>& s) {
   s.op_m10 = m.op_m10;
   s.adp_lu = m.adp_lu;
   s.adp_piv = m.adp_piv;
+  s.adp_pmap = m.adp_pmap;
   s.adp_rhs = nullptr;
   if (m.adp_lu) {
     s.adp_rhs = (double*)dalloc(sv, (size_t)adp_range_count(d) * 36 * sizeof(double), e);
@@ -511,6 +512,77 @@ int mesh_upload(Solve& sv, MeshRes& m) {
   return CS_OK;
 }
 
+// The rotation of the cube that carries panel 1 onto panel p, as a signed
+// permutation x'_a = s_a x_perm(a) with determinant +1, if the vertices of
+// the whole box agree with it to 1e-12 of the largest coordinate (the
+// reference's sector construction gives this symmetry); and the map it
+// induces on the 30 B-mode unknowns of the ADP system, unknown (c, m) =
+// 10 c + m with the basis 1, x, y, z, x^2, y^2, z^2, xy, yz, xz (minus their
+// moments): panel p's row entry (c, m) is sgn * panel 1's entry src.
+// pmap[p][0][v] = u with src(u) = v, pmap[p][1][v] = sgn(u); identity on
+// the 6 multipliers.
+bool adp_panel_maps(const GeomHost& h, int8_t* pmap) {
+  const size_t S = h.box.size();
+  const std::vector<double>& V = h.f[CS_G_VERT];
+  double vmax = 0.0;
+  for (double x : V) vmax = std::max(vmax, std::fabs(x));
+  const double tol = 1e-12 * vmax;
+  const int perms[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+  const int psign[6] = {1, -1, -1, 1, 1, -1};
+  for (int p = 0; p < 6; ++p) {
+    int found = -1, sg[3] = {1, 1, 1};
+    for (int pi = 0; pi < 6 && found < 0; ++pi)
+      for (int sm = 0; sm < 8 && found < 0; ++sm) {
+        const int s3[3] = {(sm & 1) ? -1 : 1, (sm & 2) ? -1 : 1, (sm & 4) ? -1 : 1};
+        if (psign[pi] * s3[0] * s3[1] * s3[2] != 1) continue;
+        bool ok = true;
+        for (int a = 0; a < 3 && ok; ++a) {
+          const double* src = V.data() + ((size_t)perms[pi][a] * 6 + 0) * S;
+          const double* dst = V.data() + ((size_t)a * 6 + p) * S;
+          for (size_t o = 0; o < S; ++o)
+            if (std::fabs(s3[a] * src[o] - dst[o]) > tol) {
+              ok = false;
+              break;
+            }
+        }
+        if (ok) {
+          found = pi;
+          for (int a = 0; a < 3; ++a) sg[a] = s3[a];
+        }
+      }
+    if (found < 0) return false;
+    const int* pm = perms[found];
+    auto pair_mode = [](int a, int b) {
+      const int lo = std::min(a, b), hi = std::max(a, b);
+      return lo == 0 ? (hi == 1 ? 7 : 9) : 8;  // xy 7, yz 8, xz 9
+    };
+    int8_t* um = pmap + p * 72;
+    int8_t* sgm = um + 36;
+    for (int c = 0; c < 3; ++c)
+      for (int mm = 0; mm < 10; ++mm) {
+        int mu = 0, sig = 1;
+        if (mm >= 1 && mm <= 3) {
+          mu = 1 + pm[mm - 1];
+          sig = sg[mm - 1];
+        } else if (mm >= 4 && mm <= 6) {
+          mu = 4 + pm[mm - 4];
+        } else if (mm >= 7) {
+          const int a = mm == 8 ? 1 : 0, b = mm == 7 ? 1 : 2;
+          mu = pair_mode(pm[a], pm[b]);
+          sig = sg[a] * sg[b];
+        }
+        const int u = c * 10 + mm, v = pm[c] * 10 + mu;
+        um[v] = (int8_t)u;
+        sgm[v] = (int8_t)(sg[c] * sig);
+      }
+    for (int v = 30; v < 36; ++v) {
+      um[v] = (int8_t)v;
+      sgm[v] = 1;
+    }
+  }
+  return true;
+}
+
 // Resident geometry-only operators of a new mesh, where the device has room
 // for them after the first solve's state, computed by that solve's stream.
 template <typename R>
@@ -535,7 +607,9 @@ int mesh_operators(Solve& sv, MeshRes& m, DStateT<R>& s) {
     }
   }
   if (!(sv.p.flags & CS_FLAG_NO_ADP_CACHE)) {
-    const long long nf = adp_factor_doubles(d);
+    int8_t pmap[6 * 72];
+    const bool shared = !(sv.p.flags & CS_FLAG_ADP_PER_PANEL) && adp_panel_maps(m.host, pmap);
+    const long long nf = adp_factor_doubles(d, shared);
     const size_t lu_bytes = (size_t)nf * sizeof(double), pv_bytes = (size_t)nf / 36;
     size_t fr = 0, tot = 0;
     if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && lu_bytes + pv_bytes + (size_t)8 * S6 * 60 < fr) {
@@ -543,8 +617,15 @@ int mesh_operators(Solve& sv, MeshRes& m, DStateT<R>& s) {
       m.adp_piv = m.adp_lu ? (int8_t*)mdalloc(sv, m, pv_bytes, e) : nullptr;
       s.adp_rhs = m.adp_piv ? (double*)dalloc(sv, (size_t)adp_range_count(d) * 36 * sizeof(double), e) : nullptr;
       if (!m.adp_lu || !m.adp_piv || !s.adp_rhs) return cuda_fail(sv, e, "cudaMalloc(ADP factors)");
+      if (shared) {
+        m.adp_pmap = (int8_t*)mdalloc(sv, m, sizeof pmap, e);
+        if (!m.adp_pmap) return cuda_fail(sv, e, "cudaMalloc(ADP panel maps)");
+        CS_CUDA(sv, cudaMemcpyAsync(m.adp_pmap, pmap, sizeof pmap, cudaMemcpyHostToDevice, sv.stream));
+        CS_CUDA(sv, cudaStreamSynchronize(sv.stream));  // pmap is a stack array
+      }
     }
   }
+  s.adp_pmap = m.adp_pmap;
   s.op_m9 = m.op_m9;
   s.op_m10 = m.op_m10;
   s.adp_lu = m.adp_lu;
@@ -561,7 +642,8 @@ std::string mesh_key(const cs_params& p) {
   char b[320];
   std::snprintf(b, sizeof b, "%d/%d/%d/%d/%.17g/%.17g/%.17g/%.17g/%d", p.ntp, p.nr, p.nghost, p.radial_mesh, p.rmin,
                 p.rmax, p.radial_ratio, p.smallnum,
-                p.flags & (CS_FLAG_NO_ADP_CACHE | CS_FLAG_NO_OP_CACHE | CS_FLAG_NO_PANEL_SYNC | CS_FLAG_FP32));
+                p.flags & (CS_FLAG_NO_ADP_CACHE | CS_FLAG_NO_OP_CACHE | CS_FLAG_NO_PANEL_SYNC | CS_FLAG_FP32 |
+                           CS_FLAG_ADP_PER_PANEL));
   return b;
 }
 

@@ -62,6 +62,7 @@ struct DStateT {
   double* adp_lu;                        // ADP KKT factors: per block of 128 zones, [1296 in use order][128], or null
   int8_t* adp_piv;                       // their row permutation, per block [36][128]
   double* adp_rhs;                       // ADP right-hand sides, [36][zones of the ADP range]
+  const int8_t* adp_pmap;                // factors shared by the panels: per panel [unknown map 36][sign 36], or null
   int* err_flag;                         // device-side error bits (bounded waits that gave up)
   int32_t* giveup;                       // positivity give-up flags per zone
   unsigned long long* dtmin;             // CFL reduction target (bit pattern of a positive double)
@@ -421,7 +422,7 @@ void launch_faceB_adp(Solve& s);
 void launch_adp_factor(Solve& s);
 void set_adp_smem_limits();
 long long adp_range_count(const Dims& d);
-long long adp_factor_doubles(const Dims& d);
+long long adp_factor_doubles(const Dims& d, bool shared);
 long long lsq_range_count(const Dims& d);
 void launch_ops_build(Solve& s);
 void launch_efield(Solve& s);

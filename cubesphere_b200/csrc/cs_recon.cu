@@ -11,6 +11,8 @@
 // in shared memory.
 #include <algorithm>
 
+#include <utility>
+
 #include "cs_solve.h"
 
 namespace cs {
@@ -712,6 +714,17 @@ constexpr int ADP_ZB = 128;
 __host__ __device__ constexpr int adp_stream_pos(int a, int b) {
   return b < a ? a * (a - 1) / 2 + b : 630 + (35 - a) * (36 - a) / 2 + (b == a ? 35 - a : b - a - 1);
 }
+// Factor stream of the panel-shared cache: blocks of ADP6_ZB zones; the
+// strict lower triangle column by column (630: column b, rows b+1..35),
+// then for rows 35..0 the entries right of the diagonal followed by the
+// diagonal (666).  Column order lets the forward pass update 35 - b rows
+// independently per column; each row still receives its terms in
+// ascending column order, so the arithmetic is that of the row order.
+constexpr int ADP6_ZB = 32;
+__host__ __device__ constexpr int adp6_stream_pos(int a, int b) {
+  return b < a ? b * 35 - b * (b - 1) / 2 + (a - b - 1)
+               : 630 + (35 - a) * (36 - a) / 2 + (b == a ? 35 - a : b - a - 1);
+}
 struct AdpSmem {
   double K[36][37];
   double Q[30][31];
@@ -721,13 +734,16 @@ struct AdpSmem {
 
 // kFactorOnly: assemble and factor the geometry-only KKT matrix and store
 // the factors and the row permutation for k_adp_solve (once per mesh).
+// tmax: zones of the range handled (all of it, or panel 1's share when the
+// factors are shared by the six panels); zb: zones per factor block.
 template <bool kFactorOnly, typename R>
-__global__ void __launch_bounds__(32 * ADP_WARPS) k_adp(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
+__global__ void __launch_bounds__(32 * ADP_WARPS) k_adp(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r,
+                                                        long long tmax, int zb) {
   extern __shared__ unsigned char smem_raw[];
   AdpSmem& S = reinterpret_cast<AdpSmem*>(smem_raw)[threadIdx.x / 32];
   const int lane = threadIdx.x & 31;
   const long long nw = (long long)gridDim.x * ADP_WARPS;
-  for (long long t = blockIdx.x * (long long)ADP_WARPS + threadIdx.x / 32; t < r.count(); t += nw) {
+  for (long long t = blockIdx.x * (long long)ADP_WARPS + threadIdx.x / 32; t < tmax; t += nw) {
     int p, i, j, k;
     r.decode(t, p, i, j, k);
     if (mask_at(g, d, p, i, j) == 0) continue;
@@ -869,10 +885,12 @@ __global__ void __launch_bounds__(32 * ADP_WARPS) k_adp(Dims d, PhysC ph, DGeom 
       __syncwarp();
     }
     if (kFactorOnly) {
-      const long long blk = t / ADP_ZB, z = t % ADP_ZB;
-      for (int e = lane; e < 36 * 36; e += 32)
-        s.adp_lu[(blk * 1296 + adp_stream_pos(e / 36, e % 36)) * ADP_ZB + z] = S.K[e / 36][e % 36];
-      for (int e = lane; e < 36; e += 32) s.adp_piv[(blk * 36 + e) * ADP_ZB + z] = (int8_t)S.piv[e];
+      const long long blk = t / zb, z = t % zb;
+      for (int e = lane; e < 36 * 36; e += 32) {
+        const int pos = zb == ADP6_ZB ? adp6_stream_pos(e / 36, e % 36) : adp_stream_pos(e / 36, e % 36);
+        s.adp_lu[(blk * 1296 + pos) * zb + z] = S.K[e / 36][e % 36];
+      }
+      for (int e = lane; e < 36; e += 32) s.adp_piv[(blk * 36 + e) * zb + z] = (int8_t)S.piv[e];
       __syncwarp();
       continue;
     }
@@ -1330,6 +1348,173 @@ inline Range3 shrink(const Dims& d, int s) {
 
 }  // namespace
 
+// STEP 8.d substitution with factors shared by the six panels.  The six
+// panels of the cubed sphere are rotations of panel 1 by signed
+// permutations R_p (vertex(p, i,j,k) = R_p vertex(1, i,j,k), checked when
+// the mesh is uploaded), so the KKT matrix of zone (i,j,k) of panel p is
+// T_p K_1 T_p^T, T_p being the signed permutation of the 30 B-mode
+// unknowns that R_p induces (identity on the 6 multipliers).  Panel 1's
+// factor stream then serves all six panels: r' = T_p^T r, y' = K_1^-1 r',
+// y = T_p y'.  A CTA takes ADP6_ZB zone positions and all six panels (one
+// consumer warp per panel, one zone per lane, y in registers); a producer
+// warp streams the positions' factors (4 KB stages, in consumption order)
+// through the ring, so each factor byte read from HBM serves six solves.
+// adp_pmap[p][0][v] is the panel-p unknown u fed by panel-1 unknown v,
+// adp_pmap[p][1][v] its sign.
+constexpr int ADP6_CONS = 6 * 32;
+constexpr int ADP6_THREADS = ADP6_CONS + 32;
+constexpr int ADP6_CH = 16;
+constexpr int ADP6_NS = 12;
+constexpr int ADP6_NCH = 1296 / ADP6_CH;
+struct Adp6Smem {
+  double stage[ADP6_NS][ADP6_CH][ADP6_ZB];
+  uint64_t full[ADP6_NS];
+  uint64_t empty[ADP6_NS];
+};
+
+// Element e of the panel-shared factor stream (adp6_stream_pos order):
+// row a, column b; b == a is a diagonal entry of the backward pass.
+struct AdpElem {
+  int a, b;
+};
+__host__ __device__ constexpr AdpElem adp_elem(int e) {
+  if (e < 630) {
+    int b = 0;
+    while (e >= 35 - b) {
+      e -= 35 - b;
+      ++b;
+    }
+    return AdpElem{b + 1 + e, b};
+  }
+  int r = e - 630, a = 35;
+  while (r >= 36 - a) {
+    r -= 36 - a;
+    --a;
+  }
+  return r < 35 - a ? AdpElem{a, a + 1 + r} : AdpElem{a, a};
+}
+static_assert(adp_elem(0).a == 1 && adp_elem(0).b == 0 && adp_elem(34).a == 35 && adp_elem(34).b == 0 &&
+                  adp_elem(35).a == 2 && adp_elem(35).b == 1 && adp_elem(629).a == 35 && adp_elem(629).b == 34,
+              "forward");
+static_assert(adp6_stream_pos(35, 0) == 34 && adp6_stream_pos(2, 1) == 35 && adp6_stream_pos(35, 34) == 629 &&
+                  adp6_stream_pos(35, 35) == 630 && adp6_stream_pos(0, 0) == 1295,
+              "stream positions");
+static_assert(adp_elem(630).a == 35 && adp_elem(630).b == 35 && adp_elem(631).a == 34 && adp_elem(631).b == 35 &&
+                  adp_elem(632).b == 34 && adp_elem(1295).a == 0 && adp_elem(1295).b == 0,
+              "backward");
+
+// One stream element applied to y in registers (every index a compile-time
+// constant): forward and backward eliminations y[a] -= f y[b], the
+// diagonal y[a] /= f -- the substitution order of the reference.
+template <int E>
+__device__ __forceinline__ void adp6_apply(double (&y)[36], double f) {
+  constexpr AdpElem x = adp_elem(E);
+  if constexpr (x.a == x.b)
+    y[x.a] = y[x.a] / f;
+  else
+    y[x.a] -= f * y[x.b];
+}
+template <int C, int... W>
+__device__ __forceinline__ void adp6_chunk(double (&y)[36], const double* cur, std::integer_sequence<int, W...>) {
+  (adp6_apply<C * ADP6_CH + W>(y, cur[W * ADP6_ZB]), ...);
+}
+// The whole stream of one zone block, chunk by chunk through the ring:
+// release the previous stage, wait for this one, apply its 16 elements.
+template <int... C>
+__device__ __forceinline__ void adp6_substitute(double (&y)[36], Adp6Smem& S, int lane, long long& gch, int* err,
+                                                std::integer_sequence<int, C...>) {
+  auto acquire = [&]() -> const double* {
+    if (gch > 0) {
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&S.empty[(int)((gch - 1) % ADP6_NS)]);
+    }
+    const int slot = (int)(gch % ADP6_NS);
+    mbar_wait(&S.full[slot], (uint32_t)((gch / ADP6_NS) & 1), err);
+    ++gch;
+    return &S.stage[slot][0][lane];
+  };
+  (adp6_chunk<C>(y, acquire(), std::make_integer_sequence<int, ADP6_CH>{}), ...);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(ADP6_THREADS, 2) k_adp_solve6(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
+  extern __shared__ __align__(128) unsigned char adp6_raw[];
+  Adp6Smem& S = *reinterpret_cast<Adp6Smem*>(adp6_raw);
+  const int tid = threadIdx.x;
+  const long long n = r.count(), n1 = n / 6;
+  const long long nblk = (n1 + ADP6_ZB - 1) / ADP6_ZB;
+  if ((long long)blockIdx.x >= nblk) return;
+  const long long my_iters = (nblk - 1 - blockIdx.x) / gridDim.x + 1;
+  const long long total_chunks = my_iters * ADP6_NCH;
+  if (tid == 0) {
+    for (int q = 0; q < ADP6_NS; ++q) {
+      mbar_init(&S.full[q], 1);
+      mbar_init(&S.empty[q], ADP6_CONS / 32);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (tid >= ADP6_CONS) {
+    if (tid == ADP6_CONS) {
+      for (long long gch = 0; gch < total_chunks; ++gch) {
+        const int slot = (int)(gch % ADP6_NS);
+        if (gch >= ADP6_NS) mbar_wait(&S.empty[slot], (uint32_t)(((gch / ADP6_NS) - 1) & 1), s.err_flag);
+        const long long it = gch / ADP6_NCH, c = gch % ADP6_NCH;
+        const long long blk = blockIdx.x + it * gridDim.x;
+        const double* src = s.adp_lu + (blk * 1296 + c * ADP6_CH) * (long long)ADP6_ZB;
+        mbar_expect_tx(&S.full[slot], ADP6_CH * ADP6_ZB * sizeof(double));
+        bulk_g2s(&S.stage[slot][0][0], src, ADP6_CH * ADP6_ZB * sizeof(double), &S.full[slot]);
+      }
+    }
+    return;
+  }
+  const int lane = tid & 31, p = tid >> 5;
+  const int8_t* umap = s.adp_pmap + p * 72;
+  const int8_t* smap = umap + 36;
+  long long gch = 0;
+  for (long long it = 0; it < my_iters; ++it) {
+    const long long blk = blockIdx.x + it * gridDim.x;
+    const long long t1 = blk * ADP6_ZB + lane, t = p * n1 + t1;
+    const bool inr = t1 < n1;
+    const int8_t* pv = s.adp_piv + blk * 36 * ADP6_ZB + lane;
+    double y[36];
+#pragma unroll
+    for (int a = 0; a < 36; ++a) {
+      const int v = inr ? pv[a * ADP6_ZB] : 0;
+      const int u = __ldg(umap + v);
+      y[a] = inr ? (double)__ldg(smap + v) * s.adp_rhs[(long long)u * n + t] : 0.0;
+    }
+    adp6_substitute(y, S, lane, gch, s.err_flag, std::make_integer_sequence<int, ADP6_NCH>{});
+    if (inr) {
+      int pp, i, j, k;
+      r.decode(t, pp, i, j, k);
+      if (mask_at(g, d, p, i, j) == 1) {
+        double nb[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int v = 0; v < 30; ++v) {
+          const int u = __ldg(umap + v);
+          const double val = (double)__ldg(smap + v) * y[v];
+          Vat(s, d, 5 + u / 10, u % 10, p, i, j, k) = (R)val;
+          if (v % 10 == 0) {
+            if (u == 0) nb[0] = val;
+            if (u == 10) nb[1] = val;
+            if (u == 20) nb[2] = val;
+          }
+        }
+        R* U = s.U;
+        const long long o5 = d.at(4, p, i, j, k);
+        const double u6 = U[d.at(5, p, i, j, k)], u7 = U[d.at(6, p, i, j, k)], u8 = U[d.at(7, p, i, j, k)];
+        const double aa = (u6 * u6 + u7 * u7 + u8 * u8) * ph.ob8pi;
+        U[d.at(5, p, i, j, k)] = nb[0];
+        U[d.at(6, p, i, j, k)] = nb[1];
+        U[d.at(7, p, i, j, k)] = nb[2];
+        const double bb = (nb[0] * nb[0] + nb[1] * nb[1] + nb[2] * nb[2]) * ph.ob8pi;
+        U[o5] = U[o5] - aa + bb;
+      }
+    }
+  }
+}
+
 template <typename R>
 void launch_prim_and_masks_t(Solve& sv, DStateT<R>& st) {
   const Dims& d = sv.d;
@@ -1434,6 +1619,15 @@ void launch_faceB_adp_t(Solve& sv, DStateT<R>& st) {
   k_faceB<R><<<blocks_for(fz.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, fz, 2);
   mark(sv, "k_faceB");
   Range3 a = shrink(d, 1);
+  if (st.adp_lu && st.adp_pmap) {
+    k_adp_rhs<R><<<blocks_for(a.count(), ADPR_TPB, grid_sms(sv)), ADPR_TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, a);
+    mark(sv, "k_adp_rhs");
+    const long long nblk = (a.count() / 6 + ADP6_ZB - 1) / ADP6_ZB;
+    const int grid = (int)std::min<long long>(nblk, (long long)grid_sms(sv) * 2);
+    k_adp_solve6<R><<<grid, ADP6_THREADS, sizeof(Adp6Smem), sv.stream>>>(d, sv.ph, sv.g, st, a);
+    mark(sv, "k_adp_solve6");
+    return;
+  }
   if (st.adp_lu) {
     k_adp_rhs<R><<<blocks_for(a.count(), ADPR_TPB, grid_sms(sv)), ADPR_TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, a);
     mark(sv, "k_adp_rhs");
@@ -1448,7 +1642,7 @@ void launch_faceB_adp_t(Solve& sv, DStateT<R>& st) {
   long long nblk = (nwarps + ADP_WARPS - 1) / ADP_WARPS;
   long long cap = (long long)grid_sms(sv) * 16;
   if (nblk > cap) nblk = cap;
-  k_adp<false, R><<<(int)nblk, 32 * ADP_WARPS, smem, sv.stream>>>(d, sv.ph, sv.g, st, a);
+  k_adp<false, R><<<(int)nblk, 32 * ADP_WARPS, smem, sv.stream>>>(d, sv.ph, sv.g, st, a, a.count(), ADP_ZB);
   mark(sv, "k_adp");
 }
 
@@ -1483,7 +1677,8 @@ void launch_ops_build(Solve& sv) {
     launch_ops_build_t(sv, sv.st);
 }
 
-long long adp_factor_doubles(const Dims& d) {
+long long adp_factor_doubles(const Dims& d, bool shared) {
+  if (shared) return (shrink(d, 1).count() / 6 + ADP6_ZB - 1) / ADP6_ZB * (long long)ADP6_ZB * 1296;
   return (shrink(d, 1).count() + ADP_ZB - 1) / ADP_ZB * (long long)ADP_ZB * 1296;
 }
 
@@ -1491,6 +1686,8 @@ void set_adp_smem_limits() {
   const int smem = (int)(sizeof(AdpSmem) * ADP_WARPS);
   cudaFuncSetAttribute(k_adp_solve<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(AdpsSmem));
   cudaFuncSetAttribute(k_adp_solve<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(AdpsSmem));
+  cudaFuncSetAttribute(k_adp_solve6<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Adp6Smem));
+  cudaFuncSetAttribute(k_adp_solve6<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Adp6Smem));
   cudaFuncSetAttribute(k_adp<false, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   cudaFuncSetAttribute(k_adp<true, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   cudaFuncSetAttribute(k_adp<false, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -1502,10 +1699,13 @@ void launch_adp_factor_t(Solve& sv, DStateT<R>& st) {
   const Dims& d = sv.d;
   Range3 a = shrink(d, 1);
   const size_t smem = sizeof(AdpSmem) * ADP_WARPS;
-  long long nblk = (a.count() + ADP_WARPS - 1) / ADP_WARPS;
+  // shared factors: panel 1's zones only, in blocks of ADP6_ZB
+  const long long tmax = st.adp_pmap ? a.count() / 6 : a.count();
+  long long nblk = (tmax + ADP_WARPS - 1) / ADP_WARPS;
   long long cap = (long long)grid_sms(sv) * 16;
   if (nblk > cap) nblk = cap;
-  k_adp<true, R><<<(int)nblk, 32 * ADP_WARPS, smem, sv.stream>>>(d, sv.ph, sv.g, st, a);
+  k_adp<true, R><<<(int)nblk, 32 * ADP_WARPS, smem, sv.stream>>>(d, sv.ph, sv.g, st, a, tmax,
+                                                                 st.adp_pmap ? ADP6_ZB : ADP_ZB);
   mark(sv, "k_adp_factor");
 }
 

@@ -62,6 +62,7 @@ struct MeshRes {
   double* op_m10 = nullptr;
   double* adp_lu = nullptr;
   int8_t* adp_piv = nullptr;
+  int8_t* adp_pmap = nullptr;  // ADP factors shared by the panels: per panel [unknown map][sign]
   std::vector<void*> allocs;
   size_t bytes = 0;     // device bytes held
   bool on_device = false;

@@ -111,6 +111,17 @@ typedef struct cs_params {
  * such form (it computes everything in REAL*8); the state read and written
  * through cs_state_get / cs_state_put stays FP64 at the boundary. */
 #define CS_FLAG_FP32 8
+/* cs_params.flags: keep one set of ADP factors per panel.  By default the
+ * resident ADP factors are panel 1's only and serve all six panels: the
+ * panels are rotations of panel 1 by signed permutations (checked on the
+ * vertices when the mesh is uploaded), under which the KKT matrix of a zone
+ * transforms by the induced signed permutation of the unknowns, so one
+ * factor read from HBM serves six solves and the cache takes 1/6 of the
+ * memory (1.7 KB per zone).  The reference factors every zone's system
+ * (420/421 STEP 8.d); its solutions agree with the per-panel factors to
+ * round-off.  This flag restores per-panel factors; meshes without the
+ * symmetry use them anyway. */
+#define CS_FLAG_ADP_PER_PANEL 16
 
 /* Seeded initial-state description (new generator cases of the problem
  * library, built with the reference mechanism of 820init_patch_cube_sphere.f). */

@@ -173,3 +173,32 @@ def test_steps_graph_matches_step_loop(name, rk, flags):
     assert d0 == d1
     for k in s0:
         assert np.array_equal(s0[k], s1[k]), k
+
+
+@pytest.mark.parametrize("name,rk", [("shell16", cs.CS_IMEX_RK2), ("surface32", cs.CS_SSPRK3)])
+def test_shared_panel_adp_matches_per_panel_factors(name, rk):
+    """The default ADP factors (panel 1's, serving all six panels through
+    the panel rotations) give the B modes of the per-panel factors to
+    round-off, and the same steps within the parity tolerance."""
+    pr = cs.preset(name)
+    pr["params"]["rk_scheme"] = rk
+    out = []
+    for flags in (0, cs.CS_FLAG_ADP_PER_PANEL):
+        s = cs.Solve(**pr["params"], flags=flags)
+        s.mesh_build()
+        s.init_problem(**pr["init"])
+        s.fill_ghosts()
+        s.limit_all_slopes_p12()
+        V = s.debug("V")
+        s.init_problem(**pr["init"])
+        dt = s.evaluate_timestep(1e30)
+        for _ in range(2):
+            dt = s.step(dt)
+        out.append((s, V, dt, s.get_state()))
+    (s, V0, d0, st0), (_, V1, d1, st1) = out
+    for m in range(10):
+        for c in (5, 6, 7):
+            e = rel(zones(s, V0[m * 8 + c], 0, 1), zones(s, V1[m * 8 + c], 0, 1))
+            assert e <= 1e-11, ("B mode", m, c, e)
+    assert abs(d0 - d1) <= TOL_STATE * d1
+    check_state(s, st0, st1)
