@@ -45,6 +45,8 @@ ALGO_WORDS_PER_UNIT = {
     # resident KKT factors (1296) + pivots (36 bytes) + the 36 right-hand
     # sides in, 30 B modes and U(5:8) out (U read and written: 8)
     "k_adp_solve": 1296 + 4.5 + 36 + 30 + 8,
+    # the same with the factors shared by the six panels (1/6 per zone)
+    "k_adp_solve6": (1296 + 4.5) / 6 + 36 + 30 + 8,
     # face-B quadrature values (30), B modes (30), geometry of the 6 faces
     # (normals 42, points 90, weights 30) and of the zone (14), 36 out
     "k_adp_rhs": 30 + 30 + 162 + 14 + 36,
@@ -61,10 +63,30 @@ ALGO_WORDS_PER_UNIT = {
 }
 
 # DRAM bytes per unit (read + write) measured by ncu on the shell32 case
-# (profiles/top_kernels_shell32.md: 2.102 GB over 190,608 zones of the ADP
-# range in one launch); the full shell128 launch is too large to capture, so
-# roofline.traffic scales this by the units of a full launch.
-MEASURED_TRAFFIC_PER_UNIT = {"k_adp_solve": 2.102122e9 / 190608}
+# (profiles/top_kernels_shell32.md; units: 190,608 zones of the ADP range,
+# 155,520 of the face-state / flux / least-squares ranges); the full
+# shell128 launches are too large to capture, so roofline.traffic scales
+# these by the units of a full launch.
+MEASURED_TRAFFIC_PER_UNIT = {
+    "k_adp_solve6": (397.223e6 + 36.802e6) / 190608,
+    "k_flux": (150.981e6 + 18.666e6 + 155.124e6 + 20.591e6 + 168.570e6 + 19.579e6) / 3 / 155520,
+    "k_weno7b": (180.634e6 + 121.688e6) / 155520,
+    "k_face_states": (254.736e6 + 308.688e6) / 155520,
+    "k_efield_c": (377.176e6 + 120.228e6) / 155520,
+}
+# FP64 operations per unit (2 x DFMA + DADD + DMUL thread instructions),
+# from the same ncu captures.  The path is FP64-bound, so the roofline also
+# reports these against the B200's nominal FP64 rate: 148 SMs x 64 FP64
+# FMA/clock x 2 x 1.965 GHz = 37.2 TFLOP/s (no measured FP64 peak exists for
+# this pool).
+FP64_FLOP_PER_UNIT = {
+    "k_adp_solve6": 6.012e8 / 190608,
+    "k_flux": (7.649e8 + 7.649e8 + 8.373e8) / 3 / 155520,
+    "k_weno7b": 9.076e8 / 155520,
+    "k_face_states": 1.163e9 / 155520,
+    "k_efield_c": 3.706e8 / 155520,
+}
+FP64_NOMINAL_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12
 
 WORKLOAD_DOC = {
     "shell128": "FP64 ideal-MHD hydrostatic shell, 6x128^2x64 zones, r 1..2 stretch 1.02, 4 ghosts, IMEX-RK2, "
@@ -494,6 +516,12 @@ def run_gpu(args):
                 "peak_source": peak_note,
                 "algorithmic_bytes_per_launch": per_launch, "avg_launch_ms": dms / dcount,
                 "share_of_step": dms / sum(v[0] for v in prof.values())}
+        fl = FP64_FLOP_PER_UNIT.get(dname)
+        if fl:
+            tf = fl * units / (dms / dcount / 1e3) / 1e12
+            roof["fp64"] = {"achieved_tflops": tf, "peak_tflops": FP64_NOMINAL_TFLOPS, "frac": tf / FP64_NOMINAL_TFLOPS,
+                            "peak_source": "nominal (148 SMs x 64 FMA/clk x 2 x 1.965 GHz)",
+                            "flop_per_unit_source": "ncu DFMA/DADD/DMUL counts on shell32"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
