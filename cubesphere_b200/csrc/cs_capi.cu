@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <map>
+#include <mutex>
 #include <tuple>
 #include <cstdio>
 #include <cstring>
@@ -33,26 +34,83 @@ const int kNbr[6][4] = {{3, 6, 2, 5}, {1, 4, 3, 6}, {2, 5, 1, 4}, {5, 2, 6, 3}, 
     if (e_ != cudaSuccess) return cs::cuda_fail(sv, e_, #call); \
   } while (0)
 
+// Stream-ordered pool for the per-solve arrays: allocation and release are
+// ordered on the solve's stream and never synchronise the device, so solves
+// that start and end while others run (the serving loop, batches) do not
+// stall one another.  Freed memory stays in the pool for the next solve and
+// goes back to the device when the last solve on it ends.
+struct SolvePool {
+  std::mutex mu;
+  cudaMemPool_t pool = nullptr;
+  int live = 0;
+};
+SolvePool& solve_pool(int dev) {
+  static SolvePool pools[64];
+  return pools[dev & 63];
+}
+
+cudaError_t pool_acquire(Solve& sv) {
+  SolvePool& sp = solve_pool(sv.device);
+  std::lock_guard<std::mutex> lk(sp.mu);
+  if (!sp.pool) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = sv.device;
+    cudaError_t e = cudaMemPoolCreate(&sp.pool, &props);
+    if (e != cudaSuccess) {
+      sp.pool = nullptr;
+      return e;
+    }
+    uint64_t keep = ~0ULL;
+    cudaMemPoolSetAttribute(sp.pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  sp.live += 1;
+  sv.pool = sp.pool;
+  return cudaSuccess;
+}
+
+void pool_release(Solve& sv) {
+  if (!sv.pool) return;
+  SolvePool& sp = solve_pool(sv.device);
+  std::lock_guard<std::mutex> lk(sp.mu);
+  sp.live -= 1;
+  if (sp.live == 0) cudaMemPoolTrimTo(sp.pool, 0);
+  sv.pool = nullptr;
+}
+
 void* dalloc(Solve& sv, size_t bytes, cudaError_t& e) {
   void* p = nullptr;
-  e = cudaMalloc(&p, bytes);
+  e = cudaMallocFromPoolAsync(&p, bytes, sv.pool, sv.stream);
   if (e != cudaSuccess) return nullptr;
   sv.allocs.push_back(p);
   e = cudaMemsetAsync(p, 0, bytes, sv.stream);
   return p;
 }
 
+}  // namespace
+
+void* solve_alloc(Solve& sv, size_t bytes, cudaError_t& e) { return dalloc(sv, bytes, e); }
+
+namespace {
+
 void free_all(Solve& sv) {
   if (sv.stream) cudaStreamSynchronize(sv.stream);
   for (cudaEvent_t e : sv.prof.ev) cudaEventDestroy(e);
   sv.prof.ev.clear();
   sv.prof.name.clear();
-  for (void* p : sv.allocs) cudaFree(p);
-  sv.allocs.clear();
   drop_graph(sv);
-  if (sv.stream) cudaStreamDestroy(sv.stream);
+  for (void* p : sv.allocs) cudaFreeAsync(p, sv.stream);
+  sv.allocs.clear();
+  if (sv.stream) {
+    cudaStreamSynchronize(sv.stream);
+    cudaStreamDestroy(sv.stream);
+  }
   sv.stream = nullptr;
+  pool_release(sv);
   sv.mesh = std::make_shared<MeshRes>();  // drops this solve's share of the mesh
+  sv.init_buf = nullptr;
+  sv.init_buf_bytes = 0;
 }
 
 // Host construction of the ghost-exchange map.  The strips are visited in
@@ -661,6 +719,7 @@ int mesh_attach(Solve& sv, const std::shared_ptr<MeshRes>& mp) {
   CS_CUDA(sv, cudaGetDevice(&sv.device));
   CS_CUDA(sv, cudaDeviceGetAttribute(&sv.sm_count, cudaDevAttrMultiProcessorCount, sv.device));
   CS_CUDA(sv, cudaStreamCreateWithFlags(&sv.stream, cudaStreamNonBlocking));
+  CS_CUDA(sv, pool_acquire(sv));
   set_adp_smem_limits();
   const bool fresh = !m.on_device;
   if (fresh)
@@ -1088,11 +1147,9 @@ int cs_init_problem(cs_ctx* ctx, const cs_init_desc* d) {
   if (!ctx || !d) return CS_ERR_ARG;
   Solve& sv = ctx->sv;
   if (int rc = cs::need(sv, false)) return rc;
-  const size_t S6 = (size_t)6 * sv.d.S;
-  std::vector<double> U(cs::NVAR * S6), ent(S6), bx(S6), by(S6), bz(S6);
-  std::string e = cs::init_problem_host(sv.p, *d, sv.mesh->host, U.data(), ent.data(), bx.data(), by.data(), bz.data());
-  if (!e.empty()) return cs::fail(sv, CS_ERR_ARG, e);
-  return cs_state_put(ctx, U.data(), ent.data(), bx.data(), by.data(), bz.data());
+  if (int rc = cs::init_problem_device(sv, *d)) return rc;
+  sv.has_state = true;
+  return CS_OK;
 }
 
 int cs_stage(cs_ctx* ctx, int32_t irk, double dtcur) {

@@ -57,6 +57,22 @@ void zone_volume_rule(const GeomHost& g, int pn, int i, int j, int k, double sma
 std::string init_problem_host(const cs_params& p, const cs_init_desc& d, const GeomHost& g, double* U, double* ent,
                               double* bx, double* by, double* bz);
 
+// The two seeded harmonic sums of an initial-state description (Y for the
+// density, Psi for the vector potential), as init_problem_host draws them:
+// terms w_n u^a_n v^b_n t^c_n of degree 1..deg, times scale.
+struct InitHarmonics {
+  int deg = 0;
+  std::vector<int> a, b, c;
+  std::vector<double> w;
+  double scale = 1.0;
+};
+std::string init_harmonics(const cs_init_desc& d, InitHarmonics& Y, InitHarmonics& Psi);
+
+// The 27-point isoparametric volume rule of the 20-node zone element:
+// shape functions N[27][20], derivatives dx, dy, dz [27][20], weights w[27],
+// packed in that order (2187 doubles).
+void vol_rule_pack(double* out);
+
 // Golden-vector helper: geometry of a single coarse zone extracted with a
 // refinement stride (the reference's iscale) from a sector mesh of
 // ntp_global zones, with no ghost layers.  Used by the quadrature-point test

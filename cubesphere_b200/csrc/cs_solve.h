@@ -87,6 +87,9 @@ struct Solve {
   FillMap fill;
   PanelSync psync;
   cudaStream_t stream = nullptr;
+  cudaMemPool_t pool = nullptr;  // stream-ordered pool of the solve's own arrays
+  unsigned char* init_buf = nullptr;  // seeded harmonic terms of cs_init_problem
+  size_t init_buf_bytes = 0;
   int device = 0;
   int sm_count = 148;
   bool has_mesh = false, has_state = false;
@@ -113,6 +116,10 @@ void drop_graph(Solve& sv);
 int read_dt(Solve& sv, double* out);
 int fail(Solve& sv, int code, const std::string& msg);
 int cuda_fail(Solve& sv, cudaError_t e, const char* what);
+// Device allocation owned by the solve (stream-ordered, zero-filled).
+void* solve_alloc(Solve& sv, size_t bytes, cudaError_t& e);
+// The seeded initial state built on the device (cs_init_problem).
+int init_problem_device(Solve& sv, const cs_init_desc& desc);
 // Identity of the mesh a parameter set needs (solves with equal keys can
 // share one MeshRes).
 std::string mesh_key(const cs_params& p);

@@ -158,6 +158,25 @@ struct Problem {
 
 }  // namespace
 
+std::string init_harmonics(const cs_init_desc& d, InitHarmonics& Y, InitHarmonics& Psi) {
+  const int lmax = d.lmax > 0 ? d.lmax : 4;
+  if (lmax > 15) return "init lmax must be <= 15";
+  Normal rnd(d.seed);
+  const Harm hy = make_harm(rnd, lmax);
+  const Harm hp = make_harm(rnd, lmax);
+  for (int q = 0; q < 2; ++q) {
+    const Harm& h = q ? hp : hy;
+    InitHarmonics& o = q ? Psi : Y;
+    o.deg = h.deg;
+    o.a = h.a;
+    o.b = h.b;
+    o.c = h.c;
+    o.w = h.w;
+    o.scale = h.scale;
+  }
+  return "";
+}
+
 std::string init_problem_host(const cs_params& p, const cs_init_desc& d, const GeomHost& g, double* U, double* ent,
                               double* bx, double* by, double* bz) {
   const Box& b = g.box;

@@ -259,6 +259,22 @@ struct VolRule {
   }
 };
 
+}  // namespace
+
+void vol_rule_pack(double* out) {
+  static const VolRule VR;
+  for (int q = 0; q < 27; ++q)
+    for (int n = 0; n < 20; ++n) {
+      out[q * 20 + n] = VR.N[q][n];
+      out[540 + q * 20 + n] = VR.dx[q][n];
+      out[1080 + q * 20 + n] = VR.dy[q][n];
+      out[1620 + q * 20 + n] = VR.dz[q][n];
+    }
+  for (int q = 0; q < 27; ++q) out[2160 + q] = VR.w[q];
+}
+
+namespace {
+
 inline V3 onto_radius(V3 mid, double r, double smallnum) {
   double t = std::fmax(smallnum, vnorm(mid));
   return vscale(mid, r / t);

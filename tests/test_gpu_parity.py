@@ -202,3 +202,29 @@ def test_shared_panel_adp_matches_per_panel_factors(name, rk):
             assert e <= 1e-11, ("B mode", m, c, e)
     assert abs(d0 - d1) <= TOL_STATE * d1
     check_state(s, st0, st1)
+
+
+@pytest.mark.parametrize("name,flags", [("shell16", 0), ("surface32", 0), ("shell16", cs.CS_FLAG_FP32)])
+def test_device_initial_state_matches_host(name, flags):
+    """cs_init_problem builds the seeded state on the device; it agrees with
+    the host construction (cs_init_problem_host) to 1e-13 of each field's
+    largest value (face B: of the largest face component, since the radial
+    one of the shell is round-off around zero; FP32 form: to FP32
+    rounding), is zero where the host leaves the state zero, and its face B
+    is divergence-free to round-off."""
+    pr = cs.preset(name)
+    s = cs.Solve(**pr["params"], flags=flags)
+    s.mesh_build()
+    host = s.init_problem_host(**pr["init"])
+    s.init_problem(**pr["init"])
+    dev = s.get_state()
+    tol = 1e-13 if not flags else 1e-7
+    bden = max(np.abs(host[k]).max() for k in ("bxf", "byf", "bzf"))
+    for k in host:
+        den = bden if k in ("bxf", "byf", "bzf") else np.abs(host[k]).max()
+        assert np.abs(dev[k] - host[k]).max() <= tol * den, (k, np.abs(dev[k] - host[k]).max() / den)
+    for k in ("U", "ent"):
+        assert np.array_equal(dev[k] == 0, host[k] == 0), k
+    m, e, divb = s.diag()
+    bmax = np.abs(faces(s, dev["bxf"], 0)).max()
+    assert divb < 1e-12 * bmax
