@@ -111,6 +111,7 @@ void free_all(Solve& sv) {
   sv.mesh = std::make_shared<MeshRes>();  // drops this solve's share of the mesh
   sv.init_buf = nullptr;
   sv.init_buf_bytes = 0;
+  sv.diag_buf = nullptr;
 }
 
 // Host construction of the ghost-exchange map.  The strips are visited in
@@ -1329,32 +1330,19 @@ int cs_diag(cs_ctx* ctx, double* mass, double* energy, double* max_divb) {
   if (!ctx || !mass || !energy || !max_divb) return CS_ERR_ARG;
   Solve& sv = ctx->sv;
   if (int rc = cs::need(sv, true)) return rc;
-  const size_t S6 = (size_t)6 * sv.d.S;
-  std::vector<double> U(cs::NVAR * S6), ent(S6), bx(S6), by(S6), bz(S6);
-  if (int rc = cs_state_get(ctx, U.data(), ent.data(), bx.data(), by.data(), bz.data())) return rc;
-  const cs::Box& b = sv.mesh->host.box;
-  const auto& G = sv.mesh->host.f;
-  double m = 0.0, en = 0.0, dv = 0.0;
-  for (int p = 0; p < 6; ++p)
-    for (int k = 1; k <= b.nr; ++k)
-      for (int j = 1; j <= b.N; ++j)
-        for (int i = 1; i <= b.N; ++i) {
-          const size_t o = (size_t)p * b.size() + b.idx(i, j, k);
-          const double vol = G[CS_G_V_VOL][o];
-          m += U[o] * vol;
-          en += U[4 * S6 + o] * vol;
-          auto at = [&](int a, int c, int e2) { return (size_t)p * b.size() + b.idx(a, c, e2); };
-          const double flux = G[CS_G_XF_AREA][at(i, j, k)] * bx[at(i, j, k)] -
-                              G[CS_G_XF_AREA][at(i - 1, j, k)] * bx[at(i - 1, j, k)] +
-                              G[CS_G_YF_AREA][at(i, j, k)] * by[at(i, j, k)] -
-                              G[CS_G_YF_AREA][at(i, j - 1, k)] * by[at(i, j - 1, k)] +
-                              G[CS_G_ZF_AREA][at(i, j, k)] * bz[at(i, j, k)] -
-                              G[CS_G_ZF_AREA][at(i, j, k - 1)] * bz[at(i, j, k - 1)];
-          dv = std::fmax(dv, std::fabs(flux) / vol);
-        }
-  *mass = m;
-  *energy = en;
-  *max_divb = dv;
+  if (!sv.diag_buf) {
+    cudaError_t e = cudaSuccess;
+    sv.diag_buf = (double*)cs::solve_alloc(sv, cs::diag_scratch_doubles() * sizeof(double), e);
+    if (!sv.diag_buf) return cs::cuda_fail(sv, e, "cudaMalloc(diagnostics)");
+  }
+  double* part = sv.diag_buf + 4;
+  cs::launch_diag(sv, part, sv.diag_buf);
+  double out[3];
+  CS_CUDA(sv, cudaMemcpyAsync(out, sv.diag_buf, sizeof out, cudaMemcpyDeviceToHost, sv.stream));
+  CS_CUDA(sv, cudaStreamSynchronize(sv.stream));
+  *mass = out[0];
+  *energy = out[1];
+  *max_divb = out[2];
   return CS_OK;
 }
 

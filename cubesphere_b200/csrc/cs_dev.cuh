@@ -444,6 +444,10 @@ void launch_restore_stage0(Solve& s);
 void launch_cleanup(Solve& s);
 void launch_timestep(Solve& s);
 void launch_set_dt(Solve& s, double dt);
+// Mass, energy and max |div B| of the interior into out[0..2] (part: the
+// diag_scratch_doubles() partial sums).
+void launch_diag(Solve& s, double* part, double* out);
+size_t diag_scratch_doubles();
 void launch_fill_ghosts(Solve& s);
 
 }  // namespace cs

@@ -90,6 +90,7 @@ struct Solve {
   cudaMemPool_t pool = nullptr;  // stream-ordered pool of the solve's own arrays
   unsigned char* init_buf = nullptr;  // seeded harmonic terms of cs_init_problem
   size_t init_buf_bytes = 0;
+  double* diag_buf = nullptr;         // cs_diag: result and partial sums
   int device = 0;
   int sm_count = 148;
   bool has_mesh = false, has_state = false;

@@ -568,6 +568,85 @@ void launch_timestep(Solve& sv) {
     launch_timestep_t(sv, sv.st);
 }
 
+// Conservation diagnostics over the interior zones (FP64): volume-weighted
+// sums of rho and of the total energy, and the largest |div B| (face-area
+// weighted circulation of the face B over the zone volume).  A fixed grid
+// of DIAG_BLOCKS blocks writes partial sums that one block then adds in a
+// fixed order, so the result does not depend on launch shapes or timing.
+constexpr int DIAG_BLOCKS = 512, DIAG_TPB = 256;
+template <typename R>
+__global__ void __launch_bounds__(DIAG_TPB) k_diag_partial(Dims d, DGeom g, DStateT<R> s, Range3 r, double* part) {
+  double m = 0.0, e = 0.0, dv = 0.0;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
+    int p, i, j, k;
+    r.decode(t, p, i, j, k);
+    const double vol = geo(g, d, CS_G_V_VOL, 0, p, i, j, k);
+    m += (double)s.U[d.at(0, p, i, j, k)] * vol;
+    e += (double)s.U[d.at(4, p, i, j, k)] * vol;
+    const double flux = geo(g, d, CS_G_XF_AREA, 0, p, i, j, k) * s.Bxf[d.at(0, p, i, j, k)] -
+                        geo(g, d, CS_G_XF_AREA, 0, p, i - 1, j, k) * s.Bxf[d.at(0, p, i - 1, j, k)] +
+                        geo(g, d, CS_G_YF_AREA, 0, p, i, j, k) * s.Byf[d.at(0, p, i, j, k)] -
+                        geo(g, d, CS_G_YF_AREA, 0, p, i, j - 1, k) * s.Byf[d.at(0, p, i, j - 1, k)] +
+                        geo(g, d, CS_G_ZF_AREA, 0, p, i, j, k) * s.Bzf[d.at(0, p, i, j, k)] -
+                        geo(g, d, CS_G_ZF_AREA, 0, p, i, j, k - 1) * s.Bzf[d.at(0, p, i, j, k - 1)];
+    dv = fmax(dv, fabs(flux) / vol);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    m += __shfl_down_sync(0xffffffffu, m, o);
+    e += __shfl_down_sync(0xffffffffu, e, o);
+    dv = fmax(dv, __shfl_down_sync(0xffffffffu, dv, o));
+  }
+  __shared__ double red[3][DIAG_TPB / 32];
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    red[0][w] = m;
+    red[1][w] = e;
+    red[2][w] = dv;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, b = 0.0, c = 0.0;
+    for (int q = 0; q < DIAG_TPB / 32; ++q) {
+      a += red[0][q];
+      b += red[1][q];
+      c = fmax(c, red[2][q]);
+    }
+    part[3 * blockIdx.x] = a;
+    part[3 * blockIdx.x + 1] = b;
+    part[3 * blockIdx.x + 2] = c;
+  }
+}
+__global__ void k_diag_final(const double* part, int n, double* out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    double a = 0.0, b = 0.0, c = 0.0;
+    for (int q = 0; q < n; ++q) {
+      a += part[3 * q];
+      b += part[3 * q + 1];
+      c = fmax(c, part[3 * q + 2]);
+    }
+    out[0] = a;
+    out[1] = b;
+    out[2] = c;
+  }
+}
+
+template <typename R>
+void launch_diag_t(Solve& sv, const DStateT<R>& st, double* part, double* out) {
+  const Range3 r = {1, sv.d.N, 1, sv.d.N, 1, sv.d.nr};
+  k_diag_partial<R><<<DIAG_BLOCKS, DIAG_TPB, 0, sv.stream>>>(sv.d, sv.g, st, r, part);
+  mark(sv, "k_diag_partial");
+  k_diag_final<<<1, 32, 0, sv.stream>>>(part, DIAG_BLOCKS, out);
+  mark(sv, "k_diag_final");
+}
+void launch_diag(Solve& sv, double* part, double* out) {
+  if (sv.fp32)
+    launch_diag_t(sv, sv.stF, part, out);
+  else
+    launch_diag_t(sv, sv.st, part, out);
+}
+size_t diag_scratch_doubles() { return 3 * DIAG_BLOCKS + 4; }
+
 void launch_set_dt(Solve& sv, double dt) {
   k_set_f64<<<1, 1, 0, sv.stream>>>(sv.fp32 ? sv.stF.dt : sv.st.dt, dt);
   mark(sv, "k_set_dt");

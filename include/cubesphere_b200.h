@@ -350,7 +350,9 @@ const char* cs_batch_last_error(const cs_batch* b);
 int cs_batch_destroy(cs_batch* b);
 
 /* Diagnostics: sums over interior zones of 6 panels of volume-weighted
- * mass, energy and the max |div B| (face-area-weighted, per volume). */
+ * mass, energy and the max |div B| (face-area-weighted, per volume),
+ * reduced on the device in FP64 in a fixed order (the same numbers for the
+ * same state whatever the launch shapes). */
 int cs_diag(cs_ctx* ctx, double* mass, double* energy, double* max_divb);
 
 #ifdef __cplusplus

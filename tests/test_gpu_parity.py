@@ -228,3 +228,27 @@ def test_device_initial_state_matches_host(name, flags):
     m, e, divb = s.diag()
     bmax = np.abs(faces(s, dev["bxf"], 0)).max()
     assert divb < 1e-12 * bmax
+
+
+def test_diag_matches_host_sums(shell16):
+    """cs_diag (device reduction) against the same sums in numpy."""
+    s, o, st = shell16
+    s.put_state(st)
+    dt = s.evaluate_timestep(1e30)
+    s.step(dt)
+    got = s.get_state()
+    vol = s.geometry("V_VOL")[0]
+    m, e, divb = s.diag()
+    I = s.interior
+    assert abs(m - (I(got["U"][0]) * I(vol)).sum()) <= 1e-13 * abs(m)
+    assert abs(e - (I(got["U"][4]) * I(vol)).sum()) <= 1e-13 * abs(e)
+    G, N, nr = s.G, s.N, s.nr
+    ax, ay, az = s.geometry("XF_AREA")[0], s.geometry("YF_AREA")[0], s.geometry("ZF_AREA")[0]
+    bx, by, bz = got["bxf"][0], got["byf"][0], got["bzf"][0]
+    sl = lambda a, di, dj, dk: a[:, G + 1 + dk:G + nr + 1 + dk, G + 1 + dj:G + N + 1 + dj, G + 1 + di:G + N + 1 + di]
+    flux = (sl(ax * bx, 0, 0, 0) - sl(ax * bx, -1, 0, 0) + sl(ay * by, 0, 0, 0) - sl(ay * by, 0, -1, 0) +
+            sl(az * bz, 0, 0, 0) - sl(az * bz, 0, 0, -1))
+    ref = (np.abs(flux) / I(vol)).max()
+    bmax = np.abs(faces(s, got["bxf"], 0)).max()
+    # both are round-off sized (their last bits differ with FMA contraction)
+    assert divb < 1e-12 * bmax and ref < 1e-12 * bmax
