@@ -168,6 +168,36 @@ def dist_setup():
     return world, rank, local
 
 
+class Ranks:
+    """Process-group plumbing of a multi-GPU run: every rank times its own
+    replica; barrier() lines the ranks up around the timed region and
+    allmax() takes the slowest rank's device time (NCCL on the GPUs; the
+    same calls work on a gloo group, which the CPU tests use)."""
+
+    def __init__(self, dist=None, device=None):
+        self.dist = dist
+        self.device = device
+
+    def barrier(self) -> None:
+        if self.dist is not None:
+            self.dist.barrier()
+
+    def allmax(self, x: float) -> float:
+        if self.dist is None:
+            return x
+        import torch
+
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+
+def replica_throughput(zones: int, steps: int, world: int, ms_max: float) -> float:
+    """Whole-job zone-updates/s: every rank advances its own replica of
+    `zones` zones by `steps` steps; the job takes the slowest rank's time."""
+    return zones * steps * world / (ms_max / 1e3)
+
+
 def cpu_baseline_sample(threads: int, steps: int = 1) -> dict:
     """The oracle (CPU port) on a bounded sample of the workload: the same
     shell physics on 6 x 16^2 x 8 zones, ``steps`` RK2 steps."""
@@ -408,16 +438,8 @@ def run_gpu(args):
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    def allmax(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    ranks = Ranks(dist, "cuda")
+    barrier, allmax = ranks.barrier, ranks.allmax
 
     pr = cs.preset(args.workload)
     s = cs.Solve(**pr["params"])
@@ -452,7 +474,7 @@ def run_gpu(args):
     launches = s.launch_count() - l0
     ms = allmax(e0.elapsed_time(e1))
     barrier()
-    value = zones * args.steps * world / (ms / 1e3)
+    value = replica_throughput(zones, args.steps, world, ms)
 
     # ---- end to end through the C ABI with pinned host buffers
     host = {}
@@ -477,7 +499,7 @@ def run_gpu(args):
     f1.record(stream)
     f1.synchronize()
     ms_e2e = allmax(f0.elapsed_time(f1))
-    e2e = zones * k_e2e * world / (ms_e2e / 1e3)
+    e2e = replica_throughput(zones, k_e2e, world, ms_e2e)
     finite = bool(np.isfinite(host["U"]).all())
 
     # ---- roofline of the dominant kernel (by device time in the timed region)
