@@ -50,7 +50,7 @@ EXPORTS = [
     "cs_cfl_timestep_noalloc", "cs_estimate_device_bytes", "cs_serve_create", "cs_serve_submit",
     "cs_serve_wait", "cs_serve_state", "cs_serve_stats", "cs_serve_destroy",
     "cs_batch_create", "cs_batch_steps", "cs_batch_autotune", "cs_batch_grid_fraction", "cs_batch_last_error",
-    "cs_batch_destroy",
+    "cs_batch_destroy", "cs_twod_rs_ez",
     "cs_snapshot_save", "cs_snapshot_load", "cs_snapshot_write_host", "cs_snapshot_read_host",
 ]
 
@@ -180,6 +180,7 @@ def load_library() -> ctypes.CDLL:
         "cs_batch_grid_fraction": ([P, ctypes.c_int32, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
         "cs_batch_last_error": ([P], ctypes.c_char_p),
         "cs_batch_destroy": ([P], ctypes.c_int),
+        "cs_twod_rs_ez": ([ctypes.c_int32, ctypes.c_int32, dp, dp], ctypes.c_int),
         "cs_snapshot_save": ([P, ctypes.c_char_p, D, D, ctypes.c_int64], ctypes.c_int),
         "cs_snapshot_load": ([P, ctypes.c_char_p, dp, dp, ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
         "cs_snapshot_write_host": ([ctypes.c_char_p, ctypes.POINTER(CsParams), dp, dp, dp, dp, dp, D, D,
@@ -524,6 +525,17 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def twod_rs_ez(kind: int, cases: np.ndarray) -> np.ndarray:
+    """ESSz of the device multidimensional Riemann solver for each row of
+    `cases` (kind 4: 11 inputs, kind 3: 10 inputs; see cs_twod_rs_ez)."""
+    a = np.ascontiguousarray(cases, dtype=np.float64)
+    out = np.zeros(a.shape[0])
+    rc = load_library().cs_twod_rs_ez(kind, a.shape[0], _dptr(a), _dptr(out))
+    if rc:
+        raise CsError(f"cs_twod_rs_ez failed ({rc})")
+    return out
 
 
 def estimate_device_bytes(**params) -> int:

@@ -265,3 +265,40 @@ void launch_edges(Solve& sv) {
 }
 
 }  // namespace cs
+
+// Known-answer access to the two multidimensional Riemann solvers: one
+// thread per case evaluates the device function the edge kernels call.
+namespace {
+__global__ void k_twod_rs_ez(int n, int kind, const double* in, double* out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  if (kind == 4) {
+    const double* a = in + (long long)t * 11;
+    out[t] = cs::d_rs4(a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7], a[8], a[9], a[10]);
+  } else {
+    const double* a = in + (long long)t * 10;
+    out[t] = cs::d_rs3(a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7], a[8], a[9]);
+  }
+}
+}  // namespace
+
+extern "C" int cs_twod_rs_ez(int32_t kind, int32_t n, const double* in, double* out) {
+  if ((kind != 3 && kind != 4) || n < 0 || (n > 0 && (!in || !out))) return CS_ERR_ARG;
+  if (n == 0) return CS_OK;
+  const size_t nin = (size_t)n * (kind == 4 ? 11 : 10);
+  double *din = nullptr, *dout = nullptr;
+  if (cudaMalloc(&din, nin * sizeof(double)) != cudaSuccess) return CS_ERR_CUDA;
+  if (cudaMalloc(&dout, (size_t)n * sizeof(double)) != cudaSuccess) {
+    cudaFree(din);
+    return CS_ERR_CUDA;
+  }
+  cudaError_t e = cudaMemcpy(din, in, nin * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    k_twod_rs_ez<<<(n + 127) / 128, 128>>>(n, kind, din, dout);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(out, dout, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost);
+  cudaFree(din);
+  cudaFree(dout);
+  return e == cudaSuccess ? CS_OK : CS_ERR_CUDA;
+}

@@ -349,6 +349,15 @@ int cs_batch_grid_fraction(const cs_batch* b, int32_t member, double* frac);
 const char* cs_batch_last_error(const cs_batch* b);
 int cs_batch_destroy(cs_batch* b);
 
+/* Known-answer access to the multidimensional HLL Riemann solvers of the
+ * edge EMFs (Two_D_RS_Ez_4State_HLL, 620riemann_2d/630_2d_rs_ez_two_d_rs_ez_4state_hll.f:10;
+ * Two_D_RS_Ez_3State_HLL, 631_2d_rs_ez_two_d_rs_ez_3state_hll.f:9), with the
+ * single Ez the edge kernels pass for all states: for kind 4, n cases of
+ * (S_R, S_L, S_U, S_D, cos_t, sin_t, Ez, Bneta_U, Bneta_D, By_R, By_L); for
+ * kind 3, n cases of (S_R1, S_L1, S_R2, S_L2, S_R3, S_L3, Ez, Bneta_1,
+ * Bneta_2, Bneta_3).  out[n] = ESSz, evaluated on the current device. */
+int cs_twod_rs_ez(int32_t kind, int32_t n, const double* in, double* out);
+
 /* Diagnostics: sums over interior zones of 6 panels of volume-weighted
  * mass, energy and the max |div B| (face-area-weighted, per volume),
  * reduced on the device in FP64 in a fixed order (the same numbers for the

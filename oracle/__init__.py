@@ -38,6 +38,8 @@ def load() -> ctypes.CDLL:
         "oracle_evaluate_timestep": ([P, D], D),
         "oracle_stage": ([P, ctypes.c_int, D], None),
         "oracle_step": ([P, D], D),
+        "oracle_twod_rs_ez_4state": ([dp], D),
+        "oracle_twod_rs_ez_3state": ([dp], D),
     }
     for n in ("oracle_fill_ghosts", "oracle_limit_all_slopes_p12", "oracle_make_facial_fluxes",
               "oracle_make_edge_efields", "oracle_build_non_stiff_sources", "oracle_cleanup"):
@@ -136,3 +138,16 @@ class Oracle:
 
     def step(self, dtcur: float) -> float:
         return self.lib.oracle_step(self.h, dtcur)
+
+
+def twod_rs_ez_4state(S_R, S_L, S_U, S_D, cos_t, sin_t, Ez_RU, Ez_LU, Ez_LD, Ez_RD, Bneta_U, Bneta_D, By_R, By_L):
+    """Two_D_RS_Ez_4State_HLL (630_2d_rs_ez_two_d_rs_ez_4state_hll.f:10): ESSz."""
+    a = np.array([S_R, S_L, S_U, S_D, cos_t, sin_t, Ez_RU, Ez_LU, Ez_LD, Ez_RD, Bneta_U, Bneta_D, By_R, By_L],
+                 dtype=np.float64)
+    return load().oracle_twod_rs_ez_4state(_d(a))
+
+
+def twod_rs_ez_3state(S_R1, S_L1, S_R2, S_L2, S_R3, S_L3, Ez_1, Ez_2, Ez_3, Bneta_1, Bneta_2, Bneta_3):
+    """Two_D_RS_Ez_3State_HLL (631_2d_rs_ez_two_d_rs_ez_3state_hll.f:9): ESSz."""
+    a = np.array([S_R1, S_L1, S_R2, S_L2, S_R3, S_L3, Ez_1, Ez_2, Ez_3, Bneta_1, Bneta_2, Bneta_3], dtype=np.float64)
+    return load().oracle_twod_rs_ez_3state(_d(a))

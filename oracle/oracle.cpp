@@ -1952,4 +1952,13 @@ double oracle_step(void* h, double dtcur) {
   return evaluate_timestep(*c, dtcur);
 }
 
+// The two multidimensional Riemann solvers with four / three separate Ez
+// (the reference's argument lists), for known-answer tests.
+double oracle_twod_rs_ez_4state(const double* a) {
+  return twod_rs_ez_4state(a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7], a[8], a[9], a[10], a[11], a[12], a[13]);
+}
+double oracle_twod_rs_ez_3state(const double* a) {
+  return twod_rs_ez_3state(a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7], a[8], a[9], a[10], a[11]);
+}
+
 }  // extern "C"

@@ -252,3 +252,17 @@ def test_diag_matches_host_sums(shell16):
     bmax = np.abs(faces(s, got["bxf"], 0)).max()
     # both are round-off sized (their last bits differ with FMA contraction)
     assert divb < 1e-12 * bmax and ref < 1e-12 * bmax
+
+
+def test_device_ghost_fill_reproduces_a_manufactured_linear_field():
+    """The known answer of the reference's ghost-fill test (the manufactured
+    linear field, 801:105-225) through the device fill."""
+    from test_oracle_invariants import _empty_ghosts, _ghost_check, manufactured_linear_state
+
+    pr = cs.preset("shell16")
+    s = cs.Solve(**pr["params"], flags=cs.CS_FLAG_NO_PANEL_SYNC)
+    s.mesh_build()
+    exact = manufactured_linear_state(s)
+    s.put_state(_empty_ghosts(s, exact))
+    s.fill_ghosts()
+    _ghost_check(s, s.get_state(), exact)

@@ -69,3 +69,88 @@ def test_ghost_fill_copies_neighbour_interior_values():
             for i in range(N + 1, N + G + 1):
                 src = U[rt, k, G + (2 * N + 1 - i), G + j]
                 assert U[0, k, G + j, G + i] == src
+
+
+def manufactured_linear_state(s):
+    """The reference's manufactured field (iproblem 0, 801: exact linear U
+    and B = (x, -2y, z)) on the solve's geometry: every conserved component
+    a_q + b_q . centroid on the active zones, face B the quadrature average
+    of B . n over each face; zero elsewhere."""
+    G = s.G
+    cen = s.geometry("V_CEN")
+    active = s.mask() == 1  # [panel, k, j, i]
+    coef = np.array([[1.0, 0.3, -0.2, 0.1], [0.2, 0.5, 0.1, -0.3], [-0.1, 0.2, 0.4, 0.1], [0.3, -0.1, 0.2, 0.6],
+                     [5.0, 0.1, 0.2, 0.3], [0.1, 1.0, 0.0, 0.0], [0.0, 0.0, -2.0, 0.0], [0.0, 0.0, 0.0, 1.0]])
+    st = s.empty_state()
+    for q in range(8):
+        val = coef[q, 0] + coef[q, 1] * cen[0] + coef[q, 2] * cen[1] + coef[q, 3] * cen[2]
+        st["U"][q] = np.where(active, val, 0.0)
+    st["ent"][0] = np.where(active, 1.0 + 0.1 * cen[0], 0.0)
+    for d, (k, QP, QW, NF) in enumerate((("bxf", "XF_QP", "XF_QW", "XF_N"), ("byf", "YF_QP", "YF_QW", "YF_N"),
+                                         ("bzf", "ZF_QP", "ZF_QW", "ZF_N"))):
+        qp, qw, nf = s.geometry(QP), s.geometry(QW), s.geometry(NF)
+        acc = 0.0
+        for q in range(5):
+            x, y, z = qp[q], qp[5 + q], qp[10 + q]
+            n = (nf[q], nf[5 + q], nf[10 + q]) if d == 2 else (nf[0], nf[1], nf[2])
+            acc = acc + qw[q] * (x * n[0] - 2.0 * y * n[1] + z * n[2])
+        st[k][0] = acc
+    return st
+
+
+# interior index ranges of each field in (i, j): zones 1..N, x-faces 0..N in i, y-faces 0..N in j
+_LO = {"U": (1, 1), "ent": (1, 1), "bxf": (0, 1), "byf": (1, 0), "bzf": (1, 1)}
+
+
+def _outside(s, key):
+    """[j, i] mask of the box points outside the field's interior range."""
+    G, N = s.G, s.N
+    box = np.arange(-G, N + G + 1)
+    li, lj = _LO[key]
+    return (box[None, :] < li) | (box[None, :] > N) | (box[:, None] < lj) | (box[:, None] > N)
+
+
+def _ghost_check(s, filled, exact):
+    """Ghost zones and faces (angular strips, radial interior) whose
+    neighbouring zones are all active hold the manufactured values."""
+    G, N, nr = s.G, s.N, s.nr
+    ks = slice(G + 1, G + nr + 1)
+    act = s.mask()[:, ks] == 1  # [panel, k, j, i]
+    sel = _outside(s, "U")[None, None] & act
+    U, Ue = filled["U"][:, :, ks], exact["U"][:, :, ks]
+    assert np.count_nonzero(sel) > 0
+    assert np.abs(np.where(sel[None], U - Ue, 0.0)).max() <= 1e-12 * np.abs(Ue).max()
+    for d, k in enumerate(("bxf", "byf")):
+        both = act & np.roll(act, -1, axis=3 - d)  # active zones on both sides of the face
+        edge = np.zeros_like(both)  # the last face of the box has no zone beyond it
+        if d == 0:
+            edge[..., -1] = True
+        else:
+            edge[..., -1, :] = True
+        fsel = _outside(s, k)[None, None] & both & ~edge
+        B, Be = filled[k][0][:, ks], exact[k][0][:, ks]
+        assert np.count_nonzero(fsel) > 0
+        assert np.abs(np.where(fsel, B - Be, 0.0)).max() <= 1e-12 * np.abs(Be).max(), k
+
+
+def _empty_ghosts(s, st):
+    """A copy of st with every box point outside each field's interior zeroed."""
+    out = {}
+    for k, v in st.items():
+        out[k] = np.where(_outside(s, k), 0.0, v)
+    return out
+
+
+def test_ghost_fill_reproduces_a_manufactured_linear_field():
+    """Known answer of the reference's ghost-fill test (309, with the
+    manufactured field of 801:105-225): after the fill, the ghost zones and
+    faces hold the linear field evaluated on their own geometry."""
+    pr = cs.preset("shell16")
+    s = cs.Solve(**pr["params"], flags=cs.CS_FLAG_NO_PANEL_SYNC)
+    s.mesh_build(device=False)
+    exact = manufactured_linear_state(s)
+    start = _empty_ghosts(s, exact)  # only the fill can put the ghost values there
+    o = Oracle(s)
+    o.put_state(start)
+    o.fill_ghosts()
+    _ghost_check(s, o.get_state(), exact)
