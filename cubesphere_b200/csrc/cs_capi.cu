@@ -464,8 +464,8 @@ int alloc_state(Solve& sv, DStateT<R>& s) {
   if (!s.FS) return cuda_fail(sv, e, "cudaMalloc(face states)");
   // resident geometry-only operators of the mesh (null until built)
   const MeshRes& m = *sv.mesh;
-  s.op_m9 = m.op_m9;
-  s.op_m10 = m.op_m10;
+  s.op_m9 = (R*)m.op_m9;
+  s.op_m10 = (R*)m.op_m10;
   s.adp_lu = m.adp_lu;
   s.adp_piv = m.adp_piv;
   s.adp_pmap = m.adp_pmap;
@@ -658,10 +658,10 @@ int mesh_operators(Solve& sv, MeshRes& m, DStateT<R>& s) {
   if (!(sv.p.flags & CS_FLAG_NO_OP_CACHE)) {
     const long long nl = lsq_range_count(d);
     size_t fr = 0, tot = 0;
-    const size_t bytes = (size_t)nl * (81 + 100) * sizeof(double);
+    const size_t bytes = (size_t)nl * (81 + 100) * sizeof(R);
     if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && bytes + (size_t)8 * S6 * 60 < fr) {
-      m.op_m9 = (double*)mdalloc(sv, m, (size_t)nl * 81 * sizeof(double), e);
-      m.op_m10 = m.op_m9 ? (double*)mdalloc(sv, m, (size_t)nl * 100 * sizeof(double), e) : nullptr;
+      m.op_m9 = mdalloc(sv, m, (size_t)nl * 81 * sizeof(R), e);
+      m.op_m10 = m.op_m9 ? mdalloc(sv, m, (size_t)nl * 100 * sizeof(R), e) : nullptr;
       if (!m.op_m9 || !m.op_m10) return cuda_fail(sv, e, "cudaMalloc(least-squares operators)");
     }
   }
@@ -685,8 +685,8 @@ int mesh_operators(Solve& sv, MeshRes& m, DStateT<R>& s) {
     }
   }
   s.adp_pmap = m.adp_pmap;
-  s.op_m9 = m.op_m9;
-  s.op_m10 = m.op_m10;
+  s.op_m9 = (R*)m.op_m9;
+  s.op_m10 = (R*)m.op_m10;
   s.adp_lu = m.adp_lu;
   s.adp_piv = m.adp_piv;
   launch_ops_build(sv);

@@ -412,7 +412,7 @@ __global__ void __launch_bounds__(TPB) k_weno7b(Dims d, PhysC ph, DGeom g, DStat
     // serves the re-reads of the later components).
     R Minv[kCached ? 1 : 81];
     if (!kCached) w7b_minv(d, ph, g, p, i, j, k, n, cx, cy, cz, l0, obl0, c0, Minv);
-    const double* mc = s.op_m9 + t;
+    const R* mc = s.op_m9 + t;
     auto MI = [&](int e) { return kCached ? (R)__ldg(mc + (long long)e * nr_) : Minv[kCached ? 0 : e]; };
     const R f = s.flatA[d.at(0, p, i, j, k)];
     const R betalo = f + (R(1.0) - f) * R(2.0);
@@ -497,7 +497,7 @@ __global__ void k_ops_m9(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
                  cz = geo(g, d, CS_G_V_CEN, 2, p, i, j, k);
     double Minv[81];
     w7b_minv(d, ph, g, p, i, j, k, n, cx, cy, cz, l0, obl0, c0, Minv);
-    for (int e = 0; e < 81; ++e) s.op_m9[(long long)e * nr_ + t] = Minv[e];
+    for (int e = 0; e < 81; ++e) s.op_m9[(long long)e * nr_ + t] = (R)Minv[e];
   }
 }
 
@@ -1264,7 +1264,7 @@ __global__ void __launch_bounds__(TPB, 4) k_efield_c(Dims d, PhysC ph, DGeom g, 
                  cz = geoR<R>(g, d, CS_G_V_CEN, 2, p, i, j, k);
     R Minv[kCached ? 1 : 100];
     if (!kCached) e9c_minv(d, g, p, i, j, k, n, cx, cy, cz, obl0, c0, Minv);
-    const double* mc = s.op_m10 + t;
+    const R* mc = s.op_m10 + t;
     auto MI = [&](int e) { return kCached ? (R)__ldg(mc + (long long)e * nr_) : Minv[kCached ? 0 : e]; };
     R Y[3][10];
 #pragma unroll
@@ -1337,7 +1337,7 @@ __global__ void k_ops_m10(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
                  cz = geo(g, d, CS_G_V_CEN, 2, p, i, j, k);
     double Minv[100];
     e9c_minv(d, g, p, i, j, k, n, cx, cy, cz, obl0, c0, Minv);
-    for (int e = 0; e < 100; ++e) s.op_m10[(long long)e * nr_ + t] = Minv[e];
+    for (int e = 0; e < 100; ++e) s.op_m10[(long long)e * nr_ + t] = (R)Minv[e];
   }
 }
 

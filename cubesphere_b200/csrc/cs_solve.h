@@ -58,8 +58,8 @@ struct MeshRes {
   DGeom g{};
   FillMap fill{};       // d_tmp stays null here: the staging buffer is per solve
   PanelSync psync{};
-  double* op_m9 = nullptr;
-  double* op_m10 = nullptr;
+  void* op_m9 = nullptr;   // least-squares inverses in the state's type (FP32 in the precision form)
+  void* op_m10 = nullptr;
   double* adp_lu = nullptr;
   int8_t* adp_piv = nullptr;
   int8_t* adp_pmap = nullptr;  // ADP factors shared by the panels: per panel [unknown map][sign]

@@ -104,9 +104,10 @@ typedef struct cs_params {
 #define CS_FLAG_NO_PANEL_SYNC 4
 /* cs_params.flags: the precision form.  The bulk of the stage (conserved
  * state, entropy, primitives and their modes, the flattener, face states and
- * fluxes, dU/dt, the stage copies) is stored and computed in FP32; face B,
- * its quadrature values, the edge EMFs, the geometry and the resident
- * operators stay FP64, so the CT update keeps div B at FP64 round-off.
+ * fluxes, dU/dt, the stage copies, the resident least-squares inverses) is
+ * stored and computed in FP32; face B, its quadrature values, the ADP
+ * system and its factors, the edge EMFs and the geometry stay FP64, so the
+ * CT update keeps div B at FP64 round-off.
  * The WENO nonlinear weights are formed in FP64.  The reference has no
  * such form (it computes everything in REAL*8); the state read and written
  * through cs_state_get / cs_state_put stays FP64 at the boundary. */

@@ -1,7 +1,7 @@
 """The precision form (CS_FLAG_FP32) against the plain FP64 form.
 
 The precision form stores and computes the bulk of the stage in FP32 and
-keeps face B, the EMFs, the geometry and the resident operators in FP64.
+keeps face B, the ADP system, the EMFs and the geometry in FP64.
 It is not a parity form: its results differ from the FP64 ones by the FP32
 rounding of the state, carried through the nonlinear reconstruction.  The
 bounds below are stated per field as relative L1 errors,
