@@ -107,6 +107,8 @@ def parse():
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-form sample")
     ap.add_argument("--no-precision", action="store_true", help="skip the FP32 precision-form sample")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-form sample")
+    ap.add_argument("--flags", type=int, default=0,
+                    help="cs_params.flags of the timed solve (8: the precision form); the default is the plain FP64 form")
     ap.add_argument("--profile-json", default="", help="also write the per-kernel device times here")
     return ap.parse_args()
 
@@ -392,7 +394,7 @@ def precision_sample(pr, dts, steps, ref_state, zones, world, allmax) -> dict:
     bmax = float(np.abs(fc(got["bxf"], 0)).max())
     f.close()
     return {"value": zones * steps * world / (ms / 1e3), "unit": "zone-updates/s", "ms_per_step": ms / steps,
-            "dtype": "f32 state/reconstruction/fluxes, f64 face B/EMFs/geometry/operators",
+            "dtype": "f32 state/reconstruction/fluxes/least-squares inverses, f64 face B/ADP/EMFs/geometry",
             "steps_compared": len(dts), "l1_rel_err_vs_f64": err, "linf_rel_err_vs_f64": err_inf,
             "max_divb_over_bmax": float(divb) / bmax}
 
@@ -442,7 +444,7 @@ def run_gpu(args):
     barrier, allmax = ranks.barrier, ranks.allmax
 
     pr = cs.preset(args.workload)
-    s = cs.Solve(**pr["params"])
+    s = cs.Solve(**pr["params"], flags=args.flags)
     s.mesh_build()
     s.init_problem(**pr["init"])
     zones = 6 * s.N * s.N * s.nr
@@ -482,7 +484,7 @@ def run_gpu(args):
         nc = 8 if k == "U" else 1
         host[k] = torch.empty(s.shape(nc), dtype=torch.float64, pin_memory=True).numpy()
     s.get_state(host)
-    ref_state = {k: v.copy() for k, v in host.items()} if not args.no_precision else None
+    ref_state = {k: v.copy() for k, v in host.items()} if not (args.no_precision or args.flags) else None
     h2d = sum(a.nbytes for a in host.values())
     d2h = h2d
     barrier()
@@ -570,9 +572,10 @@ def run_gpu(args):
     out = {
         "metric": "zone-updates/s", "value": value, "unit": "zone-updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 bulk / f64 B" if args.flags & cs.CS_FLAG_FP32 else "f64",
         "data": "synthetic (seeded harmonic density / vector-potential perturbations)",
-        "config": {"workload": args.workload, "desc": WORKLOAD_DOC.get(args.workload, ""),
+        "config": {"workload": args.workload, "desc": WORKLOAD_DOC.get(args.workload, ""), "flags": args.flags,
                    "zones": zones, "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (state and work arrays >> 126 MB), no flush"},
         "e2e": {"value": e2e, "unit": "zone-updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
