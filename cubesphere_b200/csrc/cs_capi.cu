@@ -24,6 +24,16 @@ int cuda_fail(Solve& sv, cudaError_t e, const char* what) {
   return fail(sv, CS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+// FP64 <-> FP32 copies of the precision form's state at the FP64 boundary.
+__global__ void k_narrow(const double* __restrict__ in, float* __restrict__ out, long long n) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+    out[t] = (float)in[t];
+}
+__global__ void k_widen(const float* __restrict__ in, double* __restrict__ out, long long n) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+    out[t] = (double)in[t];
+}
+
 namespace {
 
 const int kNbr[6][4] = {{3, 6, 2, 5}, {1, 4, 3, 6}, {2, 5, 1, 4}, {5, 2, 6, 3}, {6, 3, 4, 1}, {4, 1, 5, 2}};
@@ -1091,13 +1101,19 @@ int cs_state_put(cs_ctx* ctx, const double* U, const double* ent, const double* 
   if (int rc = cs::need(sv, false)) return rc;
   const size_t S6 = (size_t)6 * sv.d.S;
   if (sv.fp32) {
-    // The precision form keeps U and the entropy in FP32 on the device.
-    std::vector<float> u(cs::NVAR * S6 + S6);
-    for (size_t t = 0; t < cs::NVAR * S6; ++t) u[t] = (float)U[t];
-    for (size_t t = 0; t < S6; ++t) u[cs::NVAR * S6 + t] = (float)ent[t];
-    CS_CUDA(sv, cudaMemcpyAsync(sv.stF.U, u.data(), cs::NVAR * S6 * sizeof(float), cudaMemcpyHostToDevice, sv.stream));
-    CS_CUDA(sv, cudaMemcpyAsync(sv.stF.ent, u.data() + cs::NVAR * S6, S6 * sizeof(float), cudaMemcpyHostToDevice,
-                                sv.stream));
+    // The precision form keeps U and the entropy in FP32 on the device: the
+    // FP64 host values go through a stream-ordered staging buffer and are
+    // rounded on the device.
+    const size_t nu = cs::NVAR * S6;
+    double* stage = nullptr;
+    CS_CUDA(sv, cudaMallocFromPoolAsync((void**)&stage, (nu + S6) * sizeof(double), sv.pool, sv.stream));
+    CS_CUDA(sv, cudaMemcpyAsync(stage, U, nu * sizeof(double), cudaMemcpyHostToDevice, sv.stream));
+    CS_CUDA(sv, cudaMemcpyAsync(stage + nu, ent, S6 * sizeof(double), cudaMemcpyHostToDevice, sv.stream));
+    cs::k_narrow<<<cs::blocks_for((long long)nu, 256, sv.sm_count), 256, 0, sv.stream>>>(stage, sv.stF.U, (long long)nu);
+    cs::k_narrow<<<cs::blocks_for((long long)S6, 256, sv.sm_count), 256, 0, sv.stream>>>(stage + nu, sv.stF.ent,
+                                                                                       (long long)S6);
+    CS_CUDA(sv, cudaGetLastError());
+    CS_CUDA(sv, cudaFreeAsync(stage, sv.stream));
     CS_CUDA(sv, cudaMemcpyAsync(sv.stF.Bxf, bxf, S6 * sizeof(double), cudaMemcpyHostToDevice, sv.stream));
     CS_CUDA(sv, cudaMemcpyAsync(sv.stF.Byf, byf, S6 * sizeof(double), cudaMemcpyHostToDevice, sv.stream));
     CS_CUDA(sv, cudaMemcpyAsync(sv.stF.Bzf, bzf, S6 * sizeof(double), cudaMemcpyHostToDevice, sv.stream));
@@ -1122,16 +1138,21 @@ int cs_state_get(cs_ctx* ctx, double* U, double* ent, double* bxf, double* byf, 
   if (int rc = cs::need(sv, true)) return rc;
   const size_t S6 = (size_t)6 * sv.d.S;
   if (sv.fp32) {
-    std::vector<float> u(cs::NVAR * S6 + S6);
-    CS_CUDA(sv, cudaMemcpyAsync(u.data(), sv.stF.U, cs::NVAR * S6 * sizeof(float), cudaMemcpyDeviceToHost, sv.stream));
-    CS_CUDA(sv, cudaMemcpyAsync(u.data() + cs::NVAR * S6, sv.stF.ent, S6 * sizeof(float), cudaMemcpyDeviceToHost,
-                                sv.stream));
+    // widened to FP64 on the device, through a stream-ordered staging buffer
+    const size_t nu = cs::NVAR * S6;
+    double* stage = nullptr;
+    CS_CUDA(sv, cudaMallocFromPoolAsync((void**)&stage, (nu + S6) * sizeof(double), sv.pool, sv.stream));
+    cs::k_widen<<<cs::blocks_for((long long)nu, 256, sv.sm_count), 256, 0, sv.stream>>>(sv.stF.U, stage, (long long)nu);
+    cs::k_widen<<<cs::blocks_for((long long)S6, 256, sv.sm_count), 256, 0, sv.stream>>>(sv.stF.ent, stage + nu,
+                                                                                      (long long)S6);
+    CS_CUDA(sv, cudaGetLastError());
+    CS_CUDA(sv, cudaMemcpyAsync(U, stage, nu * sizeof(double), cudaMemcpyDeviceToHost, sv.stream));
+    CS_CUDA(sv, cudaMemcpyAsync(ent, stage + nu, S6 * sizeof(double), cudaMemcpyDeviceToHost, sv.stream));
+    CS_CUDA(sv, cudaFreeAsync(stage, sv.stream));
     CS_CUDA(sv, cudaMemcpyAsync(bxf, sv.stF.Bxf, S6 * sizeof(double), cudaMemcpyDeviceToHost, sv.stream));
     CS_CUDA(sv, cudaMemcpyAsync(byf, sv.stF.Byf, S6 * sizeof(double), cudaMemcpyDeviceToHost, sv.stream));
     CS_CUDA(sv, cudaMemcpyAsync(bzf, sv.stF.Bzf, S6 * sizeof(double), cudaMemcpyDeviceToHost, sv.stream));
     CS_CUDA(sv, cudaStreamSynchronize(sv.stream));
-    for (size_t t = 0; t < cs::NVAR * S6; ++t) U[t] = u[t];
-    for (size_t t = 0; t < S6; ++t) ent[t] = u[cs::NVAR * S6 + t];
     return CS_OK;
   }
   const size_t B = S6 * sizeof(double);
