@@ -668,9 +668,9 @@ int mesh_operators(Solve& sv, MeshRes& m, DStateT<R>& s) {
   if (!(sv.p.flags & CS_FLAG_NO_OP_CACHE)) {
     const long long nl = lsq_range_count(d);
     size_t fr = 0, tot = 0;
-    const size_t bytes = (size_t)nl * (81 + 100) * sizeof(R);
+    const size_t bytes = (size_t)nl * (162 + 100) * sizeof(R);
     if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && bytes + (size_t)8 * S6 * 60 < fr) {
-      m.op_m9 = mdalloc(sv, m, (size_t)nl * 81 * sizeof(R), e);
+      m.op_m9 = mdalloc(sv, m, (size_t)nl * 162 * sizeof(R), e);
       m.op_m10 = m.op_m9 ? mdalloc(sv, m, (size_t)nl * 100 * sizeof(R), e) : nullptr;
       if (!m.op_m9 || !m.op_m10) return cuda_fail(sv, e, "cudaMalloc(least-squares operators)");
     }

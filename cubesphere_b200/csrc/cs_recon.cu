@@ -408,12 +408,15 @@ __global__ void __launch_bounds__(TPB) k_weno7b(Dims d, PhysC ph, DGeom g, DStat
     coef10(g, d, p, i, j, k, c0);
     const R cx = geoR<R>(g, d, CS_G_V_CEN, 0, p, i, j, k), cy = geoR<R>(g, d, CS_G_V_CEN, 1, p, i, j, k),
                  cz = geoR<R>(g, d, CS_G_V_CEN, 2, p, i, j, k);
-    // kCached: the inverse is read from the cache where it is used (L1
-    // serves the re-reads of the later components).
+    // kCached: the least-squares solution operator comes from the cache as
+    // W_rr = Minv A_rr^T, one 9-vector per stencil row (geometry only), so
+    // the slopes are X = sum_rr W_rr (V_rr - V_0) with no row rebuild and
+    // no neighbour geometry; without the cache the rows are rebuilt and the
+    // inverse applied to their sums.
     R Minv[kCached ? 1 : 81];
     if (!kCached) w7b_minv(d, ph, g, p, i, j, k, n, cx, cy, cz, l0, obl0, c0, Minv);
-    const R* mc = s.op_m9 + t;
-    auto MI = [&](int e) { return kCached ? (R)__ldg(mc + (long long)e * nr_) : Minv[kCached ? 0 : e]; };
+    const R* wc = s.op_m9 + t;
+    auto MI = [&](int e) { return Minv[kCached ? 0 : e]; };
     const R f = s.flatA[d.at(0, p, i, j, k)];
     const R betalo = f + (R(1.0) - f) * R(2.0);
     const R ghi = f * R(0.6) + (R(1.0) - f) * R(0.95), glo = R(1.0) - ghi, obghi = R(1.0) / ghi, grat = glo / ghi;
@@ -435,7 +438,14 @@ __global__ void __launch_bounds__(TPB) k_weno7b(Dims d, PhysC ph, DGeom g, DStat
       for (int rr = 0; rr < 18; ++rr) {
         R A[9];
         long long off;
-        w7b_row(d, ph, g, p, i, j, k, n, rr, cx, cy, cz, l0, obl0, c0, A, off);
+        if (kCached) {
+          const int w = c_n18[rr][0];
+          off = d.idx(w < 0 ? i : n.x[w], w < 0 ? j : n.y[w], k + c_n18[rr][1]);
+#pragma unroll
+          for (int a = 0; a < 9; ++a) A[a] = __ldg(wc + (long long)(rr * 9 + a) * nr_);
+        } else {
+          w7b_row(d, ph, g, p, i, j, k, n, rr, cx, cy, cz, l0, obl0, c0, A, off);
+        }
 #pragma unroll
         for (int qq = 0; qq < W7B_QG; ++qq) {
           const R Rv = s.V[((long long)(q0 + qq) * NPANEL + p) * d.S + off] - v0[qq];
@@ -449,10 +459,14 @@ __global__ void __launch_bounds__(TPB) k_weno7b(Dims d, PhysC ph, DGeom g, DStat
         R X[9];
 #pragma unroll
         for (int a = 0; a < 9; ++a) {
-          R sacc = R(0.0);
+          if (kCached) {
+            X[a] = Y[qq][a];
+          } else {
+            R sacc = R(0.0);
 #pragma unroll
-          for (int b = 0; b < 9; ++b) sacc = sacc + MI(a * 9 + b) * Y[qq][b];
-          X[a] = sacc;
+            for (int b = 0; b < 9; ++b) sacc = sacc + MI(a * 9 + b) * Y[qq][b];
+            X[a] = sacc;
+          }
         }
         const R v2 = Vat(s, d, q, 1, p, i, j, k), v3 = Vat(s, d, q, 2, p, i, j, k), v4 = Vat(s, d, q, 3, p, i, j, k);
         const R ISlo = betalo * (v2 * v2 + v3 * v3 + v4 * v4) * ob12;
@@ -497,7 +511,17 @@ __global__ void k_ops_m9(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
                  cz = geo(g, d, CS_G_V_CEN, 2, p, i, j, k);
     double Minv[81];
     w7b_minv(d, ph, g, p, i, j, k, n, cx, cy, cz, l0, obl0, c0, Minv);
-    for (int e = 0; e < 81; ++e) s.op_m9[(long long)e * nr_ + t] = (R)Minv[e];
+    // W_rr = Minv A_rr^T for the 18 stencil rows, [rr * 9 + a][zones]
+    for (int rr = 0; rr < 18; ++rr) {
+      double A[9];
+      long long off;
+      w7b_row(d, ph, g, p, i, j, k, n, rr, cx, cy, cz, l0, obl0, c0, A, off);
+      for (int a = 0; a < 9; ++a) {
+        double w = 0.0;
+        for (int b = 0; b < 9; ++b) w = w + Minv[a * 9 + b] * A[b];
+        s.op_m9[(long long)(rr * 9 + a) * nr_ + t] = (R)w;
+      }
+    }
   }
 }
 
