@@ -663,15 +663,16 @@ int mesh_operators(Solve& sv, MeshRes& m, DStateT<R>& s) {
   // factors are computed once here and each stage only substitutes.  They
   // take 10.4 KB per zone; without room for them (or with
   // CS_FLAG_NO_ADP_CACHE) every stage assembles and factors in place.
-  // The inverse normal matrices of the STEP 7.b / 9.c least squares are
-  // geometry-only as well (1.4 KB per zone together).
+  // The least-squares solution operators of STEPS 7.b / 9.c are
+  // geometry-only as well: the row weights Minv A_row^T (2.8 KB per zone
+  // in FP64).
   if (!(sv.p.flags & CS_FLAG_NO_OP_CACHE)) {
     const long long nl = lsq_range_count(d);
     size_t fr = 0, tot = 0;
-    const size_t bytes = (size_t)nl * (162 + 100) * sizeof(R);
+    const size_t bytes = (size_t)nl * (162 + 190) * sizeof(R);
     if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && bytes + (size_t)8 * S6 * 60 < fr) {
       m.op_m9 = mdalloc(sv, m, (size_t)nl * 162 * sizeof(R), e);
-      m.op_m10 = m.op_m9 ? mdalloc(sv, m, (size_t)nl * 100 * sizeof(R), e) : nullptr;
+      m.op_m10 = m.op_m9 ? mdalloc(sv, m, (size_t)nl * 190 * sizeof(R), e) : nullptr;
       if (!m.op_m9 || !m.op_m10) return cuda_fail(sv, e, "cudaMalloc(least-squares operators)");
     }
   }

@@ -57,8 +57,8 @@ struct DStateT {
   double *B0[3];
   R *K1, *EF1[3];                        // IMEX: first stage's dU/dt and entropy fluxes
   double *Ef1[3];                        // IMEX: first stage's EMFs
-  R* op_m9;                              // STEP 7.b inverse normal matrices, [81][zones of shrink(2)], or null
-  R* op_m10;                             // STEP 9.c inverse normal matrices, [100][zones of shrink(2)], or null
+  R* op_m9;                              // STEP 7.b row weights Minv A_rr^T, [18 x 9][zones of shrink(2)], or null
+  R* op_m10;                             // STEP 9.c row weights Minv A_rr^T, [19 x 10][zones of shrink(2)], or null
   double* adp_lu;                        // ADP KKT factors: per block of 128 zones, [1296 in use order][128], or null
   int8_t* adp_piv;                       // their row permutation, per block [36][128]
   double* adp_rhs;                       // ADP right-hand sides, [36][zones of the ADP range]

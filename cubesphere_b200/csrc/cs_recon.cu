@@ -1286,10 +1286,12 @@ __global__ void __launch_bounds__(TPB, 4) k_efield_c(Dims d, PhysC ph, DGeom g, 
     coef10(g, d, p, i, j, k, c0);
     const R cx = geoR<R>(g, d, CS_G_V_CEN, 0, p, i, j, k), cy = geoR<R>(g, d, CS_G_V_CEN, 1, p, i, j, k),
                  cz = geoR<R>(g, d, CS_G_V_CEN, 2, p, i, j, k);
+    // kCached: the solution operator comes from the cache as the row weights
+    // W_rr = Minv A_rr^T (geometry only), so X = sum_rr W_rr E_rr directly.
     R Minv[kCached ? 1 : 100];
     if (!kCached) e9c_minv(d, g, p, i, j, k, n, cx, cy, cz, obl0, c0, Minv);
-    const R* mc = s.op_m10 + t;
-    auto MI = [&](int e) { return kCached ? (R)__ldg(mc + (long long)e * nr_) : Minv[kCached ? 0 : e]; };
+    const R* wc = s.op_m10 + t;
+    auto MI = [&](int e) { return Minv[kCached ? 0 : e]; };
     R Y[3][10];
 #pragma unroll
     for (int q = 0; q < 3; ++q)
@@ -1299,7 +1301,18 @@ __global__ void __launch_bounds__(TPB, 4) k_efield_c(Dims d, PhysC ph, DGeom g, 
     for (int rr = 0; rr < 19; ++rr) {
       R A[10];
       long long off;
-      e9c_row(d, g, p, i, j, k, n, rr, cx, cy, cz, obl0, c0, A, off);
+      if (kCached) {
+        if (rr == 0) {
+          off = d.idx(i, j, k);
+        } else {
+          const int w = c_n18[rr - 1][0];
+          off = d.idx(w < 0 ? i : n.x[w], w < 0 ? j : n.y[w], k + c_n18[rr - 1][1]);
+        }
+#pragma unroll
+        for (int a = 0; a < 10; ++a) A[a] = __ldg(wc + (long long)(rr * 10 + a) * nr_);
+      } else {
+        e9c_row(d, g, p, i, j, k, n, rr, cx, cy, cz, obl0, c0, A, off);
+      }
 #pragma unroll
       for (int q = 0; q < 3; ++q) {
         const R Rv = s.Esnap[((long long)q * NPANEL + p) * d.S + off];
@@ -1315,10 +1328,14 @@ __global__ void __launch_bounds__(TPB, 4) k_efield_c(Dims d, PhysC ph, DGeom g, 
       R X[10];
 #pragma unroll
       for (int a = 0; a < 10; ++a) {
-        R acc = R(0.0);
+        if (kCached) {
+          X[a] = Y[q][a];
+        } else {
+          R acc = R(0.0);
 #pragma unroll
-        for (int b = 0; b < 10; ++b) acc = acc + MI(a * 10 + b) * Y[q][b];
-        X[a] = acc;
+          for (int b = 0; b < 10; ++b) acc = acc + MI(a * 10 + b) * Y[q][b];
+          X[a] = acc;
+        }
       }
       R e[4];
       e[0] = s.Esnap[((long long)q * NPANEL + p) * d.S + d.idx(i, j, k)];
@@ -1361,7 +1378,17 @@ __global__ void k_ops_m10(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
                  cz = geo(g, d, CS_G_V_CEN, 2, p, i, j, k);
     double Minv[100];
     e9c_minv(d, g, p, i, j, k, n, cx, cy, cz, obl0, c0, Minv);
-    for (int e = 0; e < 100; ++e) s.op_m10[(long long)e * nr_ + t] = (R)Minv[e];
+    // W_rr = Minv A_rr^T for the 19 rows (the zone and its 18 neighbours)
+    for (int rr = 0; rr < 19; ++rr) {
+      double A[10];
+      long long off;
+      e9c_row(d, g, p, i, j, k, n, rr, cx, cy, cz, obl0, c0, A, off);
+      for (int a = 0; a < 10; ++a) {
+        double w = 0.0;
+        for (int b = 0; b < 10; ++b) w = w + Minv[a * 10 + b] * A[b];
+        s.op_m10[(long long)(rr * 10 + a) * nr_ + t] = (R)w;
+      }
+    }
   }
 }
 

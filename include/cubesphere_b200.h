@@ -92,8 +92,12 @@ typedef struct cs_params {
  * it in every stage instead.  The cache is also skipped automatically when
  * the device lacks the memory.  Results are identical either way. */
 #define CS_FLAG_NO_ADP_CACHE 1
-/* cs_params.flags: likewise for the inverse normal matrices of the
- * least-squares reconstructions of the primitives and of E (1.4 KB per zone). */
+/* cs_params.flags: likewise for the least-squares solution operators of
+ * the reconstructions of the primitives and of E (STEPS 7.b / 9.c): per
+ * zone, each stencil row's weights W = Minv A_row^T (2.8 KB per zone in
+ * FP64, 1.4 KB in the precision form); without them every stage rebuilds
+ * the rows and the normal matrices and inverts them (same results to
+ * round-off). */
 #define CS_FLAG_NO_OP_CACHE 2
 /* cs_params.flags: keep each panel's own fluxes and EMFs on the faces and
  * edges it shares with other panels instead of giving every shared face and
