@@ -39,9 +39,9 @@ ALGO_WORDS_PER_UNIT = {
     # 8 prims x 4 one-sided stencils' neighbours are re-reads; compulsory: 9
     # comps of V/ent mode 1 + 3 centroid + scale + 9 x 3 gradient modes out
     "k_weno7a": 9 + 4 + 27,
-    # 8 comps x 10 modes in/out of V, flattener, 18-zone centroids (re-reads
-    # excluded), coefficients 10
-    "k_weno7b": 80 + 1 + 4 + 10 + 72,
+    # V modes 0-3 of 8 comps in (32), modes 1-9 out (72), flattener, 10
+    # moments, the resident row weights (18 x 9); neighbours' V are re-reads
+    "k_weno7b": 32 + 72 + 1 + 10 + 162,
     # resident KKT factors (1296) + pivots (36 bytes) + the 36 right-hand
     # sides in, 30 B modes and U(5:8) out (U read and written: 8)
     "k_adp_solve": 1296 + 4.5 + 36 + 30 + 8,
@@ -57,7 +57,9 @@ ALGO_WORDS_PER_UNIT = {
     # (2 x 45), geometry (15 points + 5 weights + normals/centroid 6 + area
     # + 2 volumes + scale), 16 contributions + 3 speeds/entropy flux out
     "k_flux": 90 + 30 + 19,
-    "k_efield_c": 30 + 8 + 10 + 30,
+    # E snapshot (3) and modes 1-3 (9) in, E mode 0 out (3), flattener,
+    # moments, the resident row weights (19 x 10)
+    "k_efield_c": 3 + 9 + 3 + 1 + 10 + 190,
     "k_positivity": 80 + 4 + 80,
     "k_faceB": 80 + 1 + 20 + 5,
 }
@@ -70,9 +72,9 @@ ALGO_WORDS_PER_UNIT = {
 MEASURED_TRAFFIC_PER_UNIT = {
     "k_adp_solve6": (397.223e6 + 36.802e6) / 190608,
     "k_flux": (150.981e6 + 18.666e6 + 155.124e6 + 20.591e6 + 168.570e6 + 19.579e6) / 3 / 155520,
-    "k_weno7b": (180.634e6 + 121.688e6) / 155520,
+    "k_weno7b": (269.9e6 + 124.4e6) / 155520,
     "k_face_states": (254.736e6 + 308.688e6) / 155520,
-    "k_efield_c": (377.176e6 + 120.228e6) / 155520,
+    "k_efield_c": (268.4e6 + 53.59e6) / 155520,
 }
 # FP64 operations per unit (2 x DFMA + DADD + DMUL thread instructions),
 # from the same ncu captures.  The path is FP64-bound, so the roofline also
@@ -82,9 +84,9 @@ MEASURED_TRAFFIC_PER_UNIT = {
 FP64_FLOP_PER_UNIT = {
     "k_adp_solve6": 6.012e8 / 190608,
     "k_flux": (7.649e8 + 7.649e8 + 8.373e8) / 3 / 155520,
-    "k_weno7b": 9.076e8 / 155520,
+    "k_weno7b": 5.79e8 / 155520,
     "k_face_states": 1.163e9 / 155520,
-    "k_efield_c": 3.706e8 / 155520,
+    "k_efield_c": 2.32e8 / 155520,
 }
 FP64_NOMINAL_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12
 
