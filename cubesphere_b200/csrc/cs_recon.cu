@@ -453,7 +453,7 @@ __global__ void __launch_bounds__(TPB) k_weno7b(Dims d, PhysC ph, DGeom g, DStat
           for (int a = 0; a < 9; ++a) Y[qq][a] = Y[qq][a] + A[a] * Rv;
         }
       }
-#pragma unroll 1
+#pragma unroll
       for (int qq = 0; qq < W7B_QG; ++qq) {
         const int q = q0 + qq;
         R X[9];
