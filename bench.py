@@ -50,6 +50,8 @@ ALGO_WORDS_PER_UNIT = {
     # face-B quadrature values (30), B modes (30), geometry of the 6 faces
     # (normals 42, points 90, weights 30) and of the zone (14), 36 out
     "k_adp_rhs": 30 + 30 + 162 + 14 + 36,
+    # the same with panel 1's geometry serving the six panels (1/6 per zone)
+    "k_adp_rhs6": 30 + 30 + (162 + 14) / 6 + 36,
     # 80 modes + 4 entropy modes + 10 moments + scale/centroid in, 30 face
     # points x 3 coordinates of geometry, 270 face-state values out
     "k_face_states": 80 + 4 + 14 + 90 + 270,

@@ -1044,6 +1044,74 @@ __global__ void __launch_bounds__(ADPR_TPB) k_adp_rhs(Dims d, PhysC ph, DGeom g,
   }
 }
 
+// The same right-hand sides for the six panels from panel 1's geometry:
+// one thread per zone position forms r1 = sum_q row_1(q) bq_p(q) with
+// panel 1's quadrature rows and panel p's face values, then rhs_p =
+// T_p r1 + vB_p (the rows of panel p are T_p times panel 1's, see
+// k_adp_solve6), so the geometry is read once for six panels.
+template <typename R>
+__global__ void __launch_bounds__(ADPR_TPB) k_adp_rhs6(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
+  const long long n = r.count(), n1 = n / 6;
+  for (long long t1 = blockIdx.x * (long long)blockDim.x + threadIdx.x; t1 < n1;
+       t1 += (long long)gridDim.x * blockDim.x) {
+    int p0, i, j, k;
+    r.decode(t1, p0, i, j, k);
+    const double obl0 = 1.0 / fmax(geo(g, d, CS_G_V_SCALE, 0, 0, i, j, k), ph.smallnum);
+    const double vc0 = geo(g, d, CS_G_V_CEN, 0, 0, i, j, k), vc1 = geo(g, d, CS_G_V_CEN, 1, 0, i, j, k),
+                 vc2 = geo(g, d, CS_G_V_CEN, 2, 0, i, j, k);
+    double c0[10];
+    coef10(g, d, 0, i, j, k, c0);
+#pragma unroll 1
+    for (int p = 0; p < 6; ++p) {
+      double* out = s.adp_rhs + p * n1 + t1;
+      if (mask_at(g, d, p, i, j) != 1) {
+#pragma unroll
+        for (int a = 0; a < 36; ++a) out[(long long)a * n] = 0.0;
+        continue;
+      }
+      double rhs[30];
+#pragma unroll
+      for (int a = 0; a < 30; ++a) rhs[a] = 0.0;
+#pragma unroll 1
+      for (int f = 0; f < 6; ++f) {
+        const int dir = f / 2;
+        const int fx = (f == 1) ? i - 1 : i, fy = (f == 3) ? j - 1 : j, fz = (f == 5) ? k - 1 : k;
+        const int QP = dir == 0 ? CS_G_XF_QP : (dir == 1 ? CS_G_YF_QP : CS_G_ZF_QP);
+        const int BW = dir == 0 ? CS_G_XB_QW : (dir == 1 ? CS_G_YB_QW : CS_G_ZB_QW);
+        const int NF = dir == 0 ? CS_G_XF_N : (dir == 1 ? CS_G_YF_N : CS_G_ZF_N);
+        const int ns = dir == 2 ? 5 : 1;
+        double dacc = 0.0;
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+          const int nq = dir == 2 ? q : 0;
+          const double nx = geo(g, d, NF, nq, 0, fx, fy, fz), ny = geo(g, d, NF, ns + nq, 0, fx, fy, fz),
+                       nz = geo(g, d, NF, 2 * ns + nq, 0, fx, fy, fz);
+          const double x = (geo(g, d, QP, q, 0, fx, fy, fz) - vc0) * obl0;
+          const double y = (geo(g, d, QP, 5 + q, 0, fx, fy, fz) - vc1) * obl0;
+          const double z = (geo(g, d, QP, 10 + q, 0, fx, fy, fz) - vc2) * obl0;
+          const double bfn[10] = {1.0, x, y, z, x * x - c0[4], y * y - c0[5], z * z - c0[6], x * y - c0[7],
+                                  y * z - c0[8], x * z - c0[9]};
+          const double bq = s.Bq[dir][d.at(q, p, fx, fy, fz)];
+#pragma unroll
+          for (int m = 0; m < 10; ++m) {
+            rhs[m] = rhs[m] + (m == 0 ? nx : nx * bfn[m]) * bq;
+            rhs[10 + m] = rhs[10 + m] + (m == 0 ? ny : ny * bfn[m]) * bq;
+            rhs[20 + m] = rhs[20 + m] + (m == 0 ? nz : nz * bfn[m]) * bq;
+          }
+          dacc = dacc + geo(g, d, BW, q, 0, fx, fy, fz) * bq;
+        }
+        out[(long long)(30 + f) * n] = dacc;
+      }
+      const int8_t* umap = s.adp_pmap + p * 72;
+#pragma unroll
+      for (int v = 0; v < 30; ++v) {
+        const int u = __ldg(umap + v);
+        out[(long long)u * n] = (double)__ldg(umap + 36 + v) * rhs[v] + Vat(s, d, 5 + u / 10, u % 10, p, i, j, k);
+      }
+    }
+  }
+}
+
 // STEP 8.d substitution with the resident factors, one thread per zone.
 // The factor stream of the block's 128 zones (1296 x 1 KB, in consumption
 // order) flows through a ring of ADPS_NS shared-memory stages of ADPS_CH
@@ -1671,8 +1739,9 @@ void launch_faceB_adp_t(Solve& sv, DStateT<R>& st) {
   mark(sv, "k_faceB");
   Range3 a = shrink(d, 1);
   if (st.adp_lu && st.adp_pmap) {
-    k_adp_rhs<R><<<blocks_for(a.count(), ADPR_TPB, grid_sms(sv)), ADPR_TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, a);
-    mark(sv, "k_adp_rhs");
+    k_adp_rhs6<R><<<blocks_for(a.count() / 6, ADPR_TPB, grid_sms(sv)), ADPR_TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st,
+                                                                                                  a);
+    mark(sv, "k_adp_rhs6");
     const long long nblk = (a.count() / 6 + ADP6_ZB - 1) / ADP6_ZB;
     const int grid = (int)std::min<long long>(nblk, (long long)grid_sms(sv) * 2);
     k_adp_solve6<R><<<grid, ADP6_THREADS, sizeof(Adp6Smem), sv.stream>>>(d, sv.ph, sv.g, st, a);
