@@ -262,10 +262,13 @@ __global__ void __launch_bounds__(FLUX_FACES * 5, sizeof(R) == 4 ? 5 : 4) k_flux
                      ec = a == 0 ? Cx : (a == 1 ? Cy : Cz);
         return ea * W[o] + eb * W[o + 1] + ec * W[o + 2];
       };
+      // area / volume once per side (the reference divides every term; the
+      // products differ from it in the last bit only)
+      const R aL = area / volL, aR = area / volR;
 #pragma unroll
       for (int c = 0; c < 8; ++c) {
-        red[jq][c][lane] = wt * (back(FlL, c) + back(FL, c)) * area / volL;
-        red[jq][8 + c][lane] = wt * (back(FlR, c) - back(FR, c)) * area / volR;
+        red[jq][c][lane] = wt * (back(FlL, c) + back(FL, c)) * aL;
+        red[jq][8 + c][lane] = wt * (back(FlR, c) - back(FR, c)) * aR;
       }
     }
     __syncthreads();
