@@ -1,10 +1,12 @@
 #!/usr/bin/env python
 """Throughput of the CubeSphere per-stage volume update on B200.
 
-One step = one full RK time step (all stages, the CFL reduction and its
-read-back) of a resident solve.  The metric is zone-updates/s: interior
-zones x steps / device seconds, summed over ranks (each rank runs its own
-replica of the solve: the path does not shard).
+One step = one full RK time step (all stages and the CFL reduction) of a
+resident solve; the timed steps are replayed from the captured step graph
+(cs_steps: time step kept on the device, one host synchronisation at the
+end).  The metric is zone-updates/s: interior zones x steps / device
+seconds, summed over ranks (each rank runs its own replica of the solve:
+one solve is not split across GPUs here).
 
 Default workload ``shell128``: 6 panels x 128^2 angular x 64 radial zones,
 radii 1..2 with geometric stretch 1.02, 4 ghost layers, FP64, hydrostatic
@@ -91,6 +93,9 @@ FP64_FLOP_PER_UNIT = {
     "k_efield_c": 2.32e8 / 155520,
 }
 FP64_NOMINAL_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12
+
+# Steps after which the precision form's state is compared with the FP64 one.
+PRECISION_STEPS = 10
 
 WORKLOAD_DOC = {
     "shell128": "FP64 ideal-MHD hydrostatic shell, 6x128^2x64 zones, r 1..2 stretch 1.02, 4 ghosts, IMEX-RK2, "
@@ -347,10 +352,11 @@ def batch_sample(seed: int = 11, nsol: int = 16, steps: int = 4) -> dict:
 
 
 def precision_sample(pr, dts, steps, ref_state, zones, world, allmax) -> dict:
-    """The precision form (CS_FLAG_FP32) on the same workload: the same
-    initial state and time steps as the FP64 run, the last `steps` of them
-    timed with CUDA events; relative L1 errors of the final state against
-    the FP64 run's (interior zones; faces for B) and its max |div B|."""
+    """The precision form (CS_FLAG_FP32) on the same workload: from the same
+    initial state with the same time steps as the FP64 run (`dts`), the
+    relative L1 / Linf errors of its state against the FP64 state after
+    those steps (interior zones; faces for B) and its max |div B|; then
+    `steps` further steps timed with CUDA events as in the FP64 timing."""
     import numpy as np
     import torch
 
@@ -361,20 +367,19 @@ def precision_sample(pr, dts, steps, ref_state, zones, world, allmax) -> dict:
     f.init_problem(**pr["init"])
     stream = torch.cuda.ExternalStream(f.stream_ptr())
     f.evaluate_timestep(1e30)
-    w = len(dts) - steps
-    for n in range(w):
-        f.step(dts[n])
+    dt = dts[0]
+    for d in dts:
+        dt = f.step(d)
+    got = f.get_state()
+    _, _, divb = f.diag()
     f.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for n in range(w, len(dts)):
-        f.step(dts[n])
+    f.steps(steps, dt)
     e1.record(stream)
     e1.synchronize()
     ms = allmax(e0.elapsed_time(e1))
-    got = f.get_state()
-    _, _, divb = f.diag()
     G, N, nr = f.G, f.N, f.nr
     I = f.interior
 
@@ -458,8 +463,19 @@ def run_gpu(args):
     for _ in range(max(args.warmup, 3)):
         dts.append(dt)
         dt = s.step(dt)
+    # the precision form is compared with this state after PRECISION_STEPS
+    # steps of known time step (untimed)
+    ref_state = None
+    if not (args.no_precision or args.flags):
+        while len(dts) < PRECISION_STEPS:
+            dts.append(dt)
+            dt = s.step(dt)
+        ref_state = s.get_state()
+    s.steps(1, dt)  # captures the step graph before the timed region
 
-    # ---- device-resident timing
+    # ---- device-resident timing: args.steps steps replayed from the
+    # captured step graph (device-resident time step, one host
+    # synchronisation at the end)
     clocks = Clocks(local)
     barrier()
     torch.cuda.synchronize()
@@ -467,20 +483,23 @@ def run_gpu(args):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     l0 = s.launch_count()
-    s.profile_begin()
     clocks.start()
     e0.record(stream)
-    for _ in range(args.steps):
-        dts.append(dt)
-        dt = s.step(dt)
+    dt = s.steps(args.steps, dt)
     e1.record(stream)
     e1.synchronize()
     clk = clocks.stop()
-    prof = s.profile_end()
     launches = s.launch_count() - l0
     ms = allmax(e0.elapsed_time(e1))
     barrier()
     value = replica_throughput(zones, args.steps, world, ms)
+
+    # ---- per-kernel device times: one more step with events between the
+    # launches (untimed; feeds top_kernels and the roofline)
+    s.profile_begin()
+    dt = s.step(dt)
+    prof = s.profile_end()
+    prof_steps = 1
 
     # ---- end to end through the C ABI with pinned host buffers
     host = {}
@@ -488,7 +507,6 @@ def run_gpu(args):
         nc = 8 if k == "U" else 1
         host[k] = torch.empty(s.shape(nc), dtype=torch.float64, pin_memory=True).numpy()
     s.get_state(host)
-    ref_state = {k: v.copy() for k, v in host.items()} if not (args.no_precision or args.flags) else None
     h2d = sum(a.nbytes for a in host.values())
     d2h = h2d
     barrier()
@@ -558,7 +576,7 @@ def run_gpu(args):
     precision = None
     if ref_state is not None:
         torch.cuda.synchronize()
-        precision = precision_sample(pr, dts, args.steps, ref_state, zones, world, allmax)
+        precision = precision_sample(pr, dts[:PRECISION_STEPS], args.steps, ref_state, zones, world, allmax)
     batch = None
     if not args.no_batch:
         torch.cuda.synchronize()
@@ -585,7 +603,7 @@ def run_gpu(args):
         "e2e": {"value": e2e, "unit": "zone-updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "steps": k_e2e},
         "roofline": roof, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches,
-        "top_kernels": {k: round(v[0] / args.steps, 3) for k, v in
+        "top_kernels": {k: round(v[0] / prof_steps, 3) for k, v in
                         sorted(prof.items(), key=lambda kv: -kv[1][0])[:8]},
         "finite": finite, "dt_last": dt, "precision_form": precision, "batch": batch, "serving": serving,
     }
