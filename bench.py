@@ -357,7 +357,6 @@ def precision_sample(pr, dts, steps, ref_state, zones, world, allmax) -> dict:
     relative L1 / Linf errors of its state against the FP64 state after
     those steps (interior zones; faces for B) and its max |div B|; then
     `steps` further steps timed with CUDA events as in the FP64 timing."""
-    import numpy as np
     import torch
 
     import cubesphere_b200 as cs
@@ -380,32 +379,71 @@ def precision_sample(pr, dts, steps, ref_state, zones, world, allmax) -> dict:
     e1.record(stream)
     e1.synchronize()
     ms = allmax(e0.elapsed_time(e1))
-    G, N, nr = f.G, f.N, f.nr
-    I = f.interior
+    err, err_inf, divb_rel = state_errors(f, got, ref_state, divb)
+    f.close()
+    return {"value": zones * steps * world / (ms / 1e3), "unit": "zone-updates/s", "ms_per_step": ms / steps,
+            "dtype": "f32 state/reconstruction/fluxes/least-squares inverses, f64 face B/ADP/EMFs/geometry",
+            "steps_compared": len(dts), "l1_rel_err_vs_f64": err, "linf_rel_err_vs_f64": err_inf,
+            "max_divb_over_bmax": divb_rel, "long_run": precision_long_sample()}
+
+
+def state_errors(s, got, ref, divb):
+    """Relative L1 and Linf errors of `got` against `ref` per field (interior
+    zones; the three face-B components as one field) and max |div B| over
+    max |B|."""
+    import numpy as np
+
+    G, N, nr = s.G, s.N, s.nr
+    I = s.interior
 
     def l1(a, b):
         return float(np.abs(a - b).sum() / max(np.abs(b).sum(), 1e-300))
+
+    def linf(a, b):
+        return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
 
     def fc(a, d):
         lo = [1, 1, 1]
         lo[d] = 0
         return a[..., G + lo[2]:G + nr + 1, G + lo[1]:G + N + 1, G + lo[0]:G + N + 1]
 
-    def linf(a, b):
-        return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
-
-    fields = {"rho": (I(got["U"][0]), I(ref_state["U"][0])), "momentum": (I(got["U"][1:4]), I(ref_state["U"][1:4])),
-              "energy": (I(got["U"][4]), I(ref_state["U"][4])), "entropy": (I(got["ent"]), I(ref_state["ent"])),
+    fields = {"rho": (I(got["U"][0]), I(ref["U"][0])), "momentum": (I(got["U"][1:4]), I(ref["U"][1:4])),
+              "energy": (I(got["U"][4]), I(ref["U"][4])), "entropy": (I(got["ent"]), I(ref["ent"])),
               "face_B": (np.concatenate([fc(got[k], d).ravel() for d, k in enumerate(("bxf", "byf", "bzf"))]),
-                         np.concatenate([fc(ref_state[k], d).ravel() for d, k in enumerate(("bxf", "byf", "bzf"))]))}
-    err = {k: l1(*v) for k, v in fields.items()}
-    err_inf = {k: linf(*v) for k, v in fields.items()}
+                         np.concatenate([fc(ref[k], d).ravel() for d, k in enumerate(("bxf", "byf", "bzf"))]))}
     bmax = float(np.abs(fc(got["bxf"], 0)).max())
+    return ({k: l1(*v) for k, v in fields.items()}, {k: linf(*v) for k, v in fields.items()}, float(divb) / bmax)
+
+
+def precision_long_sample(name: str = "shell32", nsteps: int = 200) -> dict:
+    """The precision form over a long run on a small shell: both forms from
+    the same initial state with the FP64 run's time steps, errors after
+    `nsteps` steps."""
+    import cubesphere_b200 as cs
+
+    pr = cs.preset(name)
+    s = cs.Solve(**pr["params"])
+    s.mesh_build()
+    s.init_problem(**pr["init"])
+    dt = s.evaluate_timestep(1e30)
+    dts = []
+    for _ in range(nsteps):
+        dts.append(dt)
+        dt = s.step(dt)
+    ref = s.get_state()
+    s.close()
+    f = cs.Solve(**pr["params"], flags=cs.CS_FLAG_FP32)
+    f.mesh_build()
+    f.init_problem(**pr["init"])
+    f.evaluate_timestep(1e30)
+    for d in dts:
+        f.step(d)
+    got = f.get_state()
+    _, _, divb = f.diag()
+    err, err_inf, divb_rel = state_errors(f, got, ref, divb)
     f.close()
-    return {"value": zones * steps * world / (ms / 1e3), "unit": "zone-updates/s", "ms_per_step": ms / steps,
-            "dtype": "f32 state/reconstruction/fluxes/least-squares inverses, f64 face B/ADP/EMFs/geometry",
-            "steps_compared": len(dts), "l1_rel_err_vs_f64": err, "linf_rel_err_vs_f64": err_inf,
-            "max_divb_over_bmax": float(divb) / bmax}
+    return {"workload": name, "steps_compared": nsteps, "l1_rel_err_vs_f64": err, "linf_rel_err_vs_f64": err_inf,
+            "max_divb_over_bmax": divb_rel}
 
 
 def run_reference(args):

@@ -130,3 +130,17 @@ def test_fp32_routines_track_fp64():
     for c in range(8):
         assert l1(s.interior(V32[c]), s.interior(V64[c])) <= 1e-4, ("V", c)
     assert l1(s.interior(D32[0]), s.interior(D64[0])) <= 1e-4
+
+
+def test_fp32_form_long_run_stays_within_1e_5():
+    """Over 200 steps (shell16, IMEX-RK2) the precision form's relative L1
+    error stays below 1e-5 in every field, with div B at round-off."""
+    s64, dts = run("shell16", 0, 200)
+    s32, _ = run("shell16", cs.CS_FLAG_FP32, 200, dts=dts)
+    want, got = s64.get_state(), s32.get_state()
+    err = field_errors(s64, got, want)
+    for k in ("rho", "mom", "E", "ent", "B"):
+        assert err[k] <= 1e-5, (k, err[k], err)
+    _, _, divb = s32.diag()
+    bmax = np.abs(faces(s32, got["bxf"], 0)).max()
+    assert divb < 1e-11 * bmax, divb / bmax
