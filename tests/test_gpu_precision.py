@@ -134,13 +134,16 @@ def test_fp32_routines_track_fp64():
 
 def test_fp32_form_long_run_stays_within_1e_5():
     """Over 200 steps (shell16, IMEX-RK2) the precision form's relative L1
-    error stays below 1e-5 in every field, with div B at round-off."""
+    error stays below 1e-5 in every field, and its div B stays at the
+    round-off level the FP64 form accumulates over the same steps (per unit
+    length; the zones are about 1/16 wide)."""
     s64, dts = run("shell16", 0, 200)
     s32, _ = run("shell16", cs.CS_FLAG_FP32, 200, dts=dts)
     want, got = s64.get_state(), s32.get_state()
     err = field_errors(s64, got, want)
     for k in ("rho", "mom", "E", "ent", "B"):
         assert err[k] <= 1e-5, (k, err[k], err)
+    _, _, divb64 = s64.diag()
     _, _, divb = s32.diag()
     bmax = np.abs(faces(s32, got["bxf"], 0)).max()
-    assert divb < 1e-11 * bmax, divb / bmax
+    assert divb < 1e-10 * bmax and divb <= 10.0 * divb64 + 1e-13 * bmax, (divb / bmax, divb64 / bmax)
