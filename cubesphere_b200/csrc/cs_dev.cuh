@@ -211,10 +211,13 @@ __device__ __forceinline__ void d_hll(const PhysC& ph, R* VL, R* VR, R entL, R e
 #pragma unroll
   for (int c = 0; c < 8; ++c) Us[c] = t1 * UR[c] - t2 * UL[c] - t3 * (FR[c] - FL[c]);
   const R entU = t1 * entR - t2 * entL - t3 * (entR * VR[1] - entL * VL[1]);
-  const R pent = entU * pow(Us[0], R(ph.gamma) - R(1.0));
   const R peng = (R(ph.gamma) - R(1.0)) * (Us[4] - R(0.5) * (Us[1] * Us[1] + Us[2] * Us[2] + Us[3] * Us[3]) / Us[0] -
                                           R(ph.ob8pi) * (Us[5] * Us[5] + Us[6] * Us[6] + Us[7] * Us[7]));
-  if (peng <= R(ph.prsfloor)) Us[4] = Us[4] + (pent - peng) / (R(ph.gamma) - R(1.0));
+  // The entropy pressure (a pow) is formed only where the floor needs it.
+  if (peng <= R(ph.prsfloor)) {
+    const R pent = entU * pow(Us[0], R(ph.gamma) - R(1.0));
+    Us[4] = Us[4] + (pent - peng) / (R(ph.gamma) - R(1.0));
+  }
   if (SL >= R(0.0)) {
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
