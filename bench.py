@@ -75,7 +75,7 @@ ALGO_WORDS_PER_UNIT = {
 # these by the units of a full launch.
 MEASURED_TRAFFIC_PER_UNIT = {
     "k_adp_solve6": (397.223e6 + 36.802e6) / 190608,
-    "k_flux": (150.981e6 + 18.666e6 + 155.124e6 + 20.591e6 + 168.570e6 + 19.579e6) / 3 / 155520,
+    "k_flux": (150.846e6 + 18.736e6 + 155.063e6 + 19.871e6 + 168.527e6 + 18.285e6) / 3 / 155520,
     "k_weno7b": (269.9e6 + 124.4e6) / 155520,
     "k_face_states": (254.736e6 + 308.688e6) / 155520,
     "k_efield_c": (268.4e6 + 53.59e6) / 155520,
@@ -87,7 +87,7 @@ MEASURED_TRAFFIC_PER_UNIT = {
 # this pool).
 FP64_FLOP_PER_UNIT = {
     "k_adp_solve6": 6.012e8 / 190608,
-    "k_flux": (7.649e8 + 7.649e8 + 8.373e8) / 3 / 155520,
+    "k_flux": (5.448e8 + 5.448e8 + 6.120e8) / 3 / 155520,
     "k_weno7b": 5.79e8 / 155520,
     "k_face_states": 1.163e9 / 155520,
     "k_efield_c": 2.32e8 / 155520,
