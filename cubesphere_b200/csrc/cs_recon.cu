@@ -308,8 +308,11 @@ __device__ void weno8(const Dims& d, const PhysC& ph, int p, int i, int j, int k
 }
 
 // STEP 7.a (421:2515-3804): linear WENO slopes of the 8 primitives and the entropy.
+// Occupancy: 3 blocks per SM suit the FP64 instantiation, 4 the FP32 one
+// (measured on the 6 x 128^2 x 64 shell; the spills cost less than the
+// extra resident warps gain).
 template <typename R>
-__global__ void k_weno7a(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
+__global__ void __launch_bounds__(TPB, sizeof(R) == 4 ? 4 : 3) k_weno7a(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
     r.decode(t, p, i, j, k);
@@ -1049,8 +1052,9 @@ __global__ void __launch_bounds__(ADPR_TPB) k_adp_rhs(Dims d, PhysC ph, DGeom g,
 // panel 1's quadrature rows and panel p's face values, then rhs_p =
 // T_p r1 + vB_p (the rows of panel p are T_p times panel 1's, see
 // k_adp_solve6), so the geometry is read once for six panels.
+// Four blocks per SM (128 registers) beat three at 168 (measured).
 template <typename R>
-__global__ void __launch_bounds__(ADPR_TPB) k_adp_rhs6(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
+__global__ void __launch_bounds__(ADPR_TPB, 4) k_adp_rhs6(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
   const long long n = r.count(), n1 = n / 6;
   for (long long t1 = blockIdx.x * (long long)blockDim.x + threadIdx.x; t1 < n1;
        t1 += (long long)gridDim.x * blockDim.x) {
@@ -1260,8 +1264,10 @@ __global__ void k_efield_a(Dims d, DGeom g, DStateT<R> s, Range3 r) {
 }
 
 // STEP 9.b (421:6840-8400): linear WENO slopes of the E point values.
+// Three blocks per SM (measured: faster than two at 255 registers, and than
+// four).
 template <typename R>
-__global__ void k_efield_b(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
+__global__ void __launch_bounds__(TPB, 3) k_efield_b(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
     r.decode(t, p, i, j, k);
