@@ -83,10 +83,10 @@ __global__ void __launch_bounds__(FS_TPB) k_face_states(Dims d, PhysC ph, DGeom 
 // per-point contributions meet in shared memory and are summed in point
 // order (the order of the reference's quadrature loop).
 constexpr int FLUX_FACES = 32;
-// Registers / occupancy: 4 blocks per SM suit the FP64 instantiation, 6 the
+// Registers / occupancy: 4 blocks per SM suit the FP64 instantiation, 7 the
 // FP32 one (measured on the 6 x 128^2 x 64 shell).
 template <typename R>
-__global__ void __launch_bounds__(FLUX_FACES * 5, sizeof(R) == 4 ? 6 : 4) k_flux(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r, int dir) {
+__global__ void __launch_bounds__(FLUX_FACES * 5, sizeof(R) == 4 ? 7 : 4) k_flux(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r, int dir) {
   __shared__ R red[5][16][FLUX_FACES];
   const int QP = dir == 0 ? CS_G_XF_QP : (dir == 1 ? CS_G_YF_QP : CS_G_ZF_QP);
   const int QW = dir == 0 ? CS_G_XF_QW : (dir == 1 ? CS_G_YF_QW : CS_G_ZF_QW);
