@@ -1345,9 +1345,9 @@ __device__ __forceinline__ void e9c_minv(const Dims& d, const DGeom& g, int p, i
 // hybridised with the slopes; the point value is flattened toward E_pt.
 // Only the point value (mode 1) is stored: the LLF edge solver consumes
 // nothing else.  kCached: the inverse normal matrix comes from the
-// operator cache.
+// operator cache.  Blocks per SM: 4 for FP64, 6 for FP32 (measured).
 template <bool kCached, typename R>
-__global__ void __launch_bounds__(TPB, 4) k_efield_c(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
+__global__ void __launch_bounds__(TPB, sizeof(R) == 4 ? 6 : 4) k_efield_c(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
   const R ob12 = R(1.0) / R(12.0), ob180 = R(1.0) / R(180.0), ob144 = R(1.0) / R(144.0);
   const long long nr_ = r.count();
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nr_; t += (long long)gridDim.x * blockDim.x) {
