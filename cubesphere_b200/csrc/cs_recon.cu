@@ -528,10 +528,56 @@ __global__ void k_ops_m9(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
   }
 }
 
+// Node a of the 27 positivity nodes of zone (i,j,k), as its offset from the
+// centroid vc scaled by obl0: 0-7 the vertices (bit 0: +x side, bit 1: +y,
+// bit 2: +z), 8-13 the face centroids (+x, -x, +y, -y, +z, -z), 14-25 the
+// edge midpoints, 26 the centroid.  Read from the geometry where it is
+// used, so no thread keeps the 81 coordinates.
+__device__ __forceinline__ void pos_vertex(const DGeom& g, const Dims& d, int p, int i, int j, int k, int v,
+                                           double* c) {
+  const int vi = i - 1 + (v & 1), vj = j - 1 + ((v >> 1) & 1), vk = k - 1 + (v >> 2);
+#pragma unroll
+  for (int q = 0; q < 3; ++q) c[q] = geo(g, d, CS_G_VERT, q, p, vi, vj, vk);
+}
+
+__device__ __forceinline__ void pos_node(const DGeom& g, const Dims& d, int p, int i, int j, int k, int a,
+                                         const double* vc, double obl0, double& x, double& y, double& z) {
+  double c[3];
+  if (a < 8) {
+    pos_vertex(g, d, p, i, j, k, a, c);
+  } else if (a < 14) {
+    const int f = a - 8, dir = f >> 1, lo = f & 1;
+    const int F = dir == 0 ? CS_G_XF_CEN : (dir == 1 ? CS_G_YF_CEN : CS_G_ZF_CEN);
+    const int fi = i - (dir == 0 ? lo : 0), fj = j - (dir == 1 ? lo : 0), fk = k - (dir == 2 ? lo : 0);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) c[q] = geo(g, d, F, q, p, fi, fj, fk);
+  } else if (a < 26) {
+    // vertex pairs along x (0-3), y (4-7), z (8-11)
+    const int e = a - 14, ax = e >> 2, w = e & 3;
+    int v0;
+    if (ax == 0) v0 = 2 * w;
+    else if (ax == 1) v0 = (w & 1) | ((w >> 1) << 2);
+    else v0 = w;
+    const int v1 = v0 | (1 << ax);
+    double c0[3], c1[3];
+    pos_vertex(g, d, p, i, j, k, v0, c0);
+    pos_vertex(g, d, p, i, j, k, v1, c1);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) c[q] = (c0[q] + c1[q]) * 0.5;
+  } else {
+#pragma unroll
+    for (int q = 0; q < 3; ++q) c[q] = vc[q];
+  }
+  x = (c[0] - vc[0]) * obl0;
+  y = (c[1] - vc[1]) * obl0;
+  z = (c[2] - vc[2]) * obl0;
+}
+
 // STEP 7.c (440:204-829): shrink the higher modes until the 27 nodal
 // values of density, pressure and entropy lie in the expanded local range.
+// Four blocks per SM (measured).
 template <typename R>
-__global__ void __launch_bounds__(TPB) k_positivity(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
+__global__ void __launch_bounds__(TPB, 4) k_positivity(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
     r.decode(t, p, i, j, k);
@@ -577,31 +623,6 @@ __global__ void __launch_bounds__(TPB) k_positivity(Dims d, PhysC ph, DGeom g, D
     }
 #pragma unroll
     for (int m = 0; m < 4; ++m) ep[m] = s.ent[d.at(m, p, i, j, k)];
-    // the 27 nodes: 8 vertices, 6 face centroids, 12 edge midpoints, centroid
-    double xyz[27][3];
-    {
-      double v8[8][3];
-      const int vi[8] = {i - 1, i, i - 1, i, i - 1, i, i - 1, i}, vj[8] = {j - 1, j - 1, j, j, j - 1, j - 1, j, j},
-                vk[8] = {k - 1, k - 1, k - 1, k - 1, k, k, k, k};
-      for (int a = 0; a < 8; ++a)
-        for (int q = 0; q < 3; ++q) v8[a][q] = geo(g, d, CS_G_VERT, q, p, vi[a], vj[a], vk[a]);
-      for (int a = 0; a < 8; ++a)
-        for (int q = 0; q < 3; ++q) xyz[a][q] = v8[a][q];
-      for (int q = 0; q < 3; ++q) {
-        xyz[8][q] = geo(g, d, CS_G_XF_CEN, q, p, i, j, k);
-        xyz[9][q] = geo(g, d, CS_G_XF_CEN, q, p, i - 1, j, k);
-        xyz[10][q] = geo(g, d, CS_G_YF_CEN, q, p, i, j, k);
-        xyz[11][q] = geo(g, d, CS_G_YF_CEN, q, p, i, j - 1, k);
-        xyz[12][q] = geo(g, d, CS_G_ZF_CEN, q, p, i, j, k);
-        xyz[13][q] = geo(g, d, CS_G_ZF_CEN, q, p, i, j, k - 1);
-      }
-      const int pr[12][2] = {{0, 1}, {2, 3}, {4, 5}, {6, 7}, {0, 2}, {1, 3}, {4, 6}, {5, 7}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
-      for (int e = 0; e < 12; ++e)
-        for (int q = 0; q < 3; ++q) xyz[14 + e][q] = (v8[pr[e][0]][q] + v8[pr[e][1]][q]) * 0.5;
-      for (int q = 0; q < 3; ++q) xyz[26][q] = vc[q];
-      for (int a = 0; a < 27; ++a)
-        for (int q = 0; q < 3; ++q) xyz[a][q] = (xyz[a][q] - vc[q]) * obl0;
-    }
     const int niter = 15;
     const double ratio = pow(0.10, 1.0 / (double)niter);
     double scale = 1.0;  // cumulative shrink of the higher modes
@@ -613,7 +634,8 @@ __global__ void __launch_bounds__(TPB) k_positivity(Dims d, PhysC ph, DGeom g, D
       }
       bool pass = true;
       for (int a = 0; a < 27 && pass; ++a) {
-        const double x = xyz[a][0], y = xyz[a][1], z = xyz[a][2];
+        double x, y, z;
+        pos_node(g, d, p, i, j, k, a, vc, obl0, x, y, z);
         const double v1 = d_poly10(vr, c0, x, y, z), v5 = d_poly10(vp, c0, x, y, z);
         const double en = ep[0] + ep[1] * x + ep[2] * y + ep[3] * z;
         if (v1 < mn0 || v1 > mx0 || v5 < mn4 || v5 > mx4 || en < emin || en > emax) pass = false;
