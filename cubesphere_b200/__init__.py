@@ -41,7 +41,7 @@ CS_RK2, CS_SSPRK3, CS_IMEX_RK2 = 2, 3, 4
 
 EXPORTS = [
     "cs_geom_ncomp", "cs_create", "cs_destroy", "cs_last_error", "cs_box_dims", "cs_params_check",
-    "cs_mesh_build", "cs_mesh_share", "cs_mesh_build_host", "cs_geometry_get", "cs_mask_get", "cs_stencil_get",
+    "cs_mesh_build", "cs_mesh_share", "cs_mesh_device_bytes", "cs_mesh_build_host", "cs_geometry_get", "cs_mask_get", "cs_stencil_get",
     "cs_geometry_single_zone", "cs_init_problem", "cs_init_problem_host", "cs_state_put", "cs_state_get",
     "cs_stage", "cs_step", "cs_steps", "cs_evaluate_timestep", "cs_synchronize", "cs_fill_ghosts",
     "cs_limit_all_slopes_p12", "cs_make_facial_fluxes", "cs_make_edge_efields_p1",
@@ -86,6 +86,7 @@ CS_FLAG_NO_OP_CACHE = 2
 CS_FLAG_NO_PANEL_SYNC = 4
 CS_FLAG_FP32 = 8
 CS_FLAG_ADP_PER_PANEL = 16
+CS_FLAG_LSQ_PER_PANEL = 32
 
 
 def make_params(**kw) -> CsParams:
@@ -143,6 +144,7 @@ def load_library() -> ctypes.CDLL:
         "cs_box_dims": ([P, ip, ip, ip], ctypes.c_int),
         "cs_mesh_build": ([P], ctypes.c_int),
         "cs_mesh_share": ([P, P], ctypes.c_int),
+        "cs_mesh_device_bytes": ([P, ctypes.POINTER(ctypes.c_uint64)], ctypes.c_int),
         "cs_mesh_build_host": ([P], ctypes.c_int),
         "cs_geometry_get": ([P, ctypes.c_int, dp, S], ctypes.c_int),
         "cs_mask_get": ([P, ip, S], ctypes.c_int),
@@ -267,6 +269,12 @@ class Solve:
     def mesh_share(self, other: "Solve") -> None:
         """Use the resident mesh of `other` (same mesh parameters) instead of building one."""
         self._check(self.lib.cs_mesh_share(self.h, other.h), "cs_mesh_share")
+
+    def mesh_device_bytes(self) -> int:
+        """Device bytes held by this solve's mesh (shared with attached solves)."""
+        out = ctypes.c_uint64()
+        self._check(self.lib.cs_mesh_device_bytes(self.h, ctypes.byref(out)), "cs_mesh_device_bytes")
+        return out.value
 
     def geometry(self, field: str | int) -> np.ndarray:
         f = GEOM[field] if isinstance(field, str) else field

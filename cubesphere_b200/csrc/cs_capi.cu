@@ -476,6 +476,8 @@ int alloc_state(Solve& sv, DStateT<R>& s) {
   const MeshRes& m = *sv.mesh;
   s.op_m9 = (R*)m.op_m9;
   s.op_m10 = (R*)m.op_m10;
+  s.lsq_map9 = m.m9_shared ? (const LsqPanelMap*)m.lsq_map : nullptr;
+  s.lsq_map10 = m.m10_shared ? (const LsqPanelMap*)m.lsq_map : nullptr;
   s.adp_lu = m.adp_lu;
   s.adp_piv = m.adp_piv;
   s.adp_pmap = m.adp_pmap;
@@ -590,7 +592,10 @@ int mesh_upload(Solve& sv, MeshRes& m) {
 // moments): panel p's row entry (c, m) is sgn * panel 1's entry src.
 // pmap[p][0][v] = u with src(u) = v, pmap[p][1][v] = sgn(u); identity on
 // the 6 multipliers.
-bool adp_panel_maps(const GeomHost& h, int8_t* pmap) {
+// The rotation taking panel 1 to panel p, where the vertices show one: a
+// signed permutation with coordinate a of panel p = sg[a] x coordinate
+// pm[a] of panel 1 at every vertex (to 1e-12 of the largest coordinate).
+bool panel_rotations(const GeomHost& h, int pm[6][3], int sg[6][3]) {
   const size_t S = h.box.size();
   const std::vector<double>& V = h.f[CS_G_VERT];
   double vmax = 0.0;
@@ -599,7 +604,7 @@ bool adp_panel_maps(const GeomHost& h, int8_t* pmap) {
   const int perms[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
   const int psign[6] = {1, -1, -1, 1, 1, -1};
   for (int p = 0; p < 6; ++p) {
-    int found = -1, sg[3] = {1, 1, 1};
+    int found = -1;
     for (int pi = 0; pi < 6 && found < 0; ++pi)
       for (int sm = 0; sm < 8 && found < 0; ++sm) {
         const int s3[3] = {(sm & 1) ? -1 : 1, (sm & 2) ? -1 : 1, (sm & 4) ? -1 : 1};
@@ -616,37 +621,84 @@ bool adp_panel_maps(const GeomHost& h, int8_t* pmap) {
         }
         if (ok) {
           found = pi;
-          for (int a = 0; a < 3; ++a) sg[a] = s3[a];
+          for (int a = 0; a < 3; ++a) {
+            pm[p][a] = perms[pi][a];
+            sg[p][a] = s3[a];
+          }
         }
       }
     if (found < 0) return false;
-    const int* pm = perms[found];
-    auto pair_mode = [](int a, int b) {
-      const int lo = std::min(a, b), hi = std::max(a, b);
-      return lo == 0 ? (hi == 1 ? 7 : 9) : 8;  // xy 7, yz 8, xz 9
-    };
+  }
+  return true;
+}
+
+// Mode mm of a 10-mode polynomial (0 the constant, 1-3 x y z, 4-6 xx yy zz,
+// 7-9 xy yz xz) on panel p equals sig x mode mu on panel 1 under the
+// rotation (pm, sg).
+void rotated_mode(const int* pm, const int* sg, int mm, int& mu, int& sig) {
+  auto pair_mode = [](int a, int b) {
+    const int lo = std::min(a, b), hi = std::max(a, b);
+    return lo == 0 ? (hi == 1 ? 7 : 9) : 8;  // xy 7, yz 8, xz 9
+  };
+  mu = 0;
+  sig = 1;
+  if (mm >= 1 && mm <= 3) {
+    mu = 1 + pm[mm - 1];
+    sig = sg[mm - 1];
+  } else if (mm >= 4 && mm <= 6) {
+    mu = 4 + pm[mm - 4];
+  } else if (mm >= 7) {
+    const int a = mm == 8 ? 1 : 0, b = mm == 7 ? 1 : 2;
+    mu = pair_mode(pm[a], pm[b]);
+    sig = sg[a] * sg[b];
+  }
+}
+
+// Per panel: the map of the 36 ADP unknowns (30 B modes, 6 multipliers) to
+// panel 1's, with signs.  False where the panels are not rotations of
+// panel 1.
+bool adp_panel_maps(const GeomHost& h, int8_t* pmap) {
+  int pm[6][3], sg[6][3];
+  if (!panel_rotations(h, pm, sg)) return false;
+  for (int p = 0; p < 6; ++p) {
     int8_t* um = pmap + p * 72;
     int8_t* sgm = um + 36;
     for (int c = 0; c < 3; ++c)
       for (int mm = 0; mm < 10; ++mm) {
-        int mu = 0, sig = 1;
-        if (mm >= 1 && mm <= 3) {
-          mu = 1 + pm[mm - 1];
-          sig = sg[mm - 1];
-        } else if (mm >= 4 && mm <= 6) {
-          mu = 4 + pm[mm - 4];
-        } else if (mm >= 7) {
-          const int a = mm == 8 ? 1 : 0, b = mm == 7 ? 1 : 2;
-          mu = pair_mode(pm[a], pm[b]);
-          sig = sg[a] * sg[b];
-        }
-        const int u = c * 10 + mm, v = pm[c] * 10 + mu;
+        int mu, sig;
+        rotated_mode(pm[p], sg[p], mm, mu, sig);
+        const int u = c * 10 + mm, v = pm[p][c] * 10 + mu;
         um[v] = (int8_t)u;
-        sgm[v] = (int8_t)(sg[c] * sig);
+        sgm[v] = (int8_t)(sg[p][c] * sig);
       }
     for (int v = 30; v < 36; ++v) {
       um[v] = (int8_t)v;
       sgm[v] = 1;
+    }
+  }
+  return true;
+}
+
+// Per panel: which of panel 1's least-squares modes (and sign) each mode
+// reads.  Besides the rotation, the rows need the same neighbours in the
+// same order: every panel's stencil table and mask must equal panel 1's.
+bool lsq_panel_maps(const GeomHost& h, LsqPanelMap* q) {
+  int pm[6][3], sg[6][3];
+  if (!panel_rotations(h, pm, sg)) return false;
+  const size_t ns = h.stencil.size() / 6, nm = h.mask.size() / 6;
+  for (int p = 1; p < 6; ++p) {
+    if (!std::equal(h.stencil.begin() + p * ns, h.stencil.begin() + (p + 1) * ns, h.stencil.begin())) return false;
+    if (!std::equal(h.mask.begin() + p * nm, h.mask.begin() + (p + 1) * nm, h.mask.begin())) return false;
+  }
+  for (int p = 0; p < 6; ++p) {
+    q[p].src = 0;
+    q[p].neg = 0;
+    q[p].pad = 0;
+    for (int mm = 0; mm < 10; ++mm) {
+      int mu, sig;
+      rotated_mode(pm[p], sg[p], mm, mu, sig);
+      q[p].src |= (unsigned long long)mu << (4 * mm);
+      if (sig < 0) q[p].neg |= 1u << mm;
     }
   }
   return true;
@@ -667,13 +719,27 @@ int mesh_operators(Solve& sv, MeshRes& m, DStateT<R>& s) {
   // geometry-only as well: the row weights Minv A_row^T (2.8 KB per zone
   // in FP64).
   if (!(sv.p.flags & CS_FLAG_NO_OP_CACHE)) {
+    // Panel-shared row weights where the mesh allows: STEP 9.c's always,
+    // STEP 7.b's in the precision form only (the FP64 k_weno7b, at its
+    // register limit, measured slower with them).
+    LsqPanelMap qmap[6];
+    const bool shared = !(sv.p.flags & CS_FLAG_LSQ_PER_PANEL) && lsq_panel_maps(m.host, qmap);
+    m.m10_shared = shared;
+    m.m9_shared = shared && sizeof(R) == 4;
     const long long nl = lsq_range_count(d);
+    const long long n9 = m.m9_shared ? nl / 6 : nl, n10 = m.m10_shared ? nl / 6 : nl;
     size_t fr = 0, tot = 0;
-    const size_t bytes = (size_t)nl * (162 + 190) * sizeof(R);
+    const size_t bytes = (size_t)(n9 * 162 + n10 * 190) * sizeof(R);
     if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && bytes + (size_t)8 * S6 * 60 < fr) {
-      m.op_m9 = mdalloc(sv, m, (size_t)nl * 162 * sizeof(R), e);
-      m.op_m10 = m.op_m9 ? mdalloc(sv, m, (size_t)nl * 190 * sizeof(R), e) : nullptr;
+      m.op_m9 = mdalloc(sv, m, (size_t)n9 * 162 * sizeof(R), e);
+      m.op_m10 = m.op_m9 ? mdalloc(sv, m, (size_t)n10 * 190 * sizeof(R), e) : nullptr;
       if (!m.op_m9 || !m.op_m10) return cuda_fail(sv, e, "cudaMalloc(least-squares operators)");
+      if (shared) {
+        m.lsq_map = mdalloc(sv, m, sizeof qmap, e);
+        if (!m.lsq_map) return cuda_fail(sv, e, "cudaMalloc(least-squares panel maps)");
+        CS_CUDA(sv, cudaMemcpyAsync(m.lsq_map, qmap, sizeof qmap, cudaMemcpyHostToDevice, sv.stream));
+        CS_CUDA(sv, cudaStreamSynchronize(sv.stream));  // qmap is a stack array
+      }
     }
   }
   if (!(sv.p.flags & CS_FLAG_NO_ADP_CACHE)) {
@@ -698,6 +764,8 @@ int mesh_operators(Solve& sv, MeshRes& m, DStateT<R>& s) {
   s.adp_pmap = m.adp_pmap;
   s.op_m9 = (R*)m.op_m9;
   s.op_m10 = (R*)m.op_m10;
+  s.lsq_map9 = m.m9_shared ? (const LsqPanelMap*)m.lsq_map : nullptr;
+  s.lsq_map10 = m.m10_shared ? (const LsqPanelMap*)m.lsq_map : nullptr;
   s.adp_lu = m.adp_lu;
   s.adp_piv = m.adp_piv;
   launch_ops_build(sv);
@@ -713,7 +781,7 @@ std::string mesh_key(const cs_params& p) {
   std::snprintf(b, sizeof b, "%d/%d/%d/%d/%.17g/%.17g/%.17g/%.17g/%d", p.ntp, p.nr, p.nghost, p.radial_mesh, p.rmin,
                 p.rmax, p.radial_ratio, p.smallnum,
                 p.flags & (CS_FLAG_NO_ADP_CACHE | CS_FLAG_NO_OP_CACHE | CS_FLAG_NO_PANEL_SYNC | CS_FLAG_FP32 |
-                           CS_FLAG_ADP_PER_PANEL));
+                           CS_FLAG_ADP_PER_PANEL | CS_FLAG_LSQ_PER_PANEL));
   return b;
 }
 
@@ -1241,6 +1309,14 @@ int cs_get_stream(cs_ctx* ctx, void** stream) {
   if (!ctx || !stream) return CS_ERR_ARG;
   if (int rc = cs::need(ctx->sv, false)) return rc;
   *stream = (void*)ctx->sv.stream;
+  return CS_OK;
+}
+
+int cs_mesh_device_bytes(cs_ctx* ctx, uint64_t* bytes) {
+  if (!ctx || !bytes) return CS_ERR_ARG;
+  Solve& sv = ctx->sv;
+  if (int rc = cs::need(sv, false)) return rc;
+  *bytes = (uint64_t)sv.mesh->bytes;
   return CS_OK;
 }
 

@@ -35,10 +35,20 @@ struct DGeom {
   const int32_t* st;    // [6][12][2][NJ][NI]
 };
 
+// How panel p reads panel 1's least-squares row weights: mode m (0 the
+// constant, 1-3 x y z, 4-6 xx yy zz, 7-9 xy yz xz) takes panel 1's mode
+// (src >> 4m) & 15, negated where bit m of neg is set.
+struct LsqPanelMap {
+  unsigned long long src;
+  unsigned int neg;
+  unsigned int pad;
+};
+constexpr unsigned long long LSQ_IDENTITY_SRC = 0x9876543210ULL;
+
 // Mutable per-solve arrays.  R is the storage and arithmetic type of the
 // state, the reconstruction, the face states and fluxes and the stage update
 // (double in the plain form, float in the precision form); face B, its
-// quadrature values, the EMFs and the resident operators are FP64 always.
+// quadrature values, the EMFs and the ADP factors are FP64 always.
 template <typename R>
 struct DStateT {
   using real = R;
@@ -59,6 +69,8 @@ struct DStateT {
   double *Ef1[3];                        // IMEX: first stage's EMFs
   R* op_m9;                              // STEP 7.b row weights Minv A_rr^T, [18 x 9][zones of shrink(2)], or null
   R* op_m10;                             // STEP 9.c row weights Minv A_rr^T, [19 x 10][zones of shrink(2)], or null
+  const LsqPanelMap* lsq_map9;           // op_m9 shared by the panels (panel 1's zones only), or null
+  const LsqPanelMap* lsq_map10;          // op_m10 likewise
   double* adp_lu;                        // ADP KKT factors: per block of 128 zones, [1296 in use order][128], or null
   int8_t* adp_piv;                       // their row permutation, per block [36][128]
   double* adp_rhs;                       // ADP right-hand sides, [36][zones of the ADP range]

@@ -392,16 +392,66 @@ __device__ __forceinline__ void w7b_minv(const Dims& d, const PhysC& ph, const D
   d_matinv<9>(M, Minv);
 }
 
+// Zones of a least-squares range in the order a stage visits them.  With
+// the row weights shared by the panels (kShared), iteration it covers tile
+// it / 6 of panel it % 6, so the six blocks that read one tile's weights run
+// side by side and five of them find the weights in L2; otherwise the plain
+// grid-stride order.  t indexes the range, tw the stored weights (panel 1's
+// zone when shared); nw is their stride.
+template <bool kShared>
+struct LsqOrder {
+  long long nr, npp, nw, nit;
+  __device__ explicit LsqOrder(const Range3& r) {
+    nr = r.count();
+    npp = nr / 6;
+    nw = kShared ? npp : nr;
+    nit = kShared ? 6 * ((npp + blockDim.x - 1) / blockDim.x) : nr;
+  }
+  __device__ long long begin() const {
+    return kShared ? (long long)blockIdx.x : blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  }
+  __device__ long long stride() const { return kShared ? (long long)gridDim.x : (long long)gridDim.x * blockDim.x; }
+  __device__ bool zone(long long it, long long& t, long long& tw) const {
+    if (!kShared) {
+      t = tw = it;
+      return true;
+    }
+    tw = (it / 6) * blockDim.x + threadIdx.x;
+    t = (it % 6) * npp + tw;
+    return tw < npp;
+  }
+};
+
+// Mode mm of panel p's least-squares solution from the sums Y over panel
+// 1's row weights: sign x Y at panel 1's mode (src >> 4mm) & 15, which lies
+// in mm's group (the constant, x y z, xx yy zz, xy yz xz), so the choice is
+// a select among three registers.  Y holds modes M0.. (M0 = 0 with the
+// constant, 1 without).
+template <int M0, typename R>
+__device__ __forceinline__ R lsq_rotated(const R* Y, int mm, unsigned long long src, unsigned int neg) {
+  const int mu = (int)((src >> (4 * mm)) & 15);
+  R v;
+  if (mm == 0) {
+    v = Y[0 - M0];
+  } else {
+    const int g0 = 1 + 3 * ((mm - 1) / 3);
+    v = mu == g0 ? Y[g0 - M0] : (mu == g0 + 1 ? Y[g0 + 1 - M0] : Y[g0 + 2 - M0]);
+  }
+  return ((neg >> mm) & 1u) ? -v : v;
+}
+
 // STEP 7.b (421:3869-4551): 18-zone quadratic least squares hybridised
 // with the linear WENO slopes (MRWENO weights, flattener damping).  With
 // kCached the inverse normal matrix (geometry only) comes from the
 // operator cache built at mesh build; the result is the same either way.
 constexpr int W7B_QG = NVAR;
-template <bool kCached, typename R>
+template <bool kCached, bool kShared, typename R>
 __global__ void __launch_bounds__(TPB) k_weno7b(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
   const R ob12 = R(1.0) / R(12.0), ob180 = R(1.0) / R(180.0), ob144 = R(1.0) / R(144.0);
-  const long long nr_ = r.count();
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nr_; t += (long long)gridDim.x * blockDim.x) {
+  const LsqOrder<kShared> ord(r);
+  for (long long it = ord.begin(); it < ord.nit; it += ord.stride()) {
+    long long t, tw;
+    if (!ord.zone(it, t, tw)) continue;
     int p, i, j, k;
     r.decode(t, p, i, j, k);
     if (mask_at(g, d, p, i, j) != 1) continue;
@@ -418,7 +468,8 @@ __global__ void __launch_bounds__(TPB) k_weno7b(Dims d, PhysC ph, DGeom g, DStat
     // inverse applied to their sums.
     R Minv[kCached ? 1 : 81];
     if (!kCached) w7b_minv(d, ph, g, p, i, j, k, n, cx, cy, cz, l0, obl0, c0, Minv);
-    const R* wc = s.op_m9 + t;
+    // kShared: panel 1's row weights; the sums are rotated at the end
+    const R* wc = s.op_m9 + tw;
     auto MI = [&](int e) { return Minv[kCached ? 0 : e]; };
     const R f = s.flatA[d.at(0, p, i, j, k)];
     const R betalo = f + (R(1.0) - f) * R(2.0);
@@ -445,7 +496,7 @@ __global__ void __launch_bounds__(TPB) k_weno7b(Dims d, PhysC ph, DGeom g, DStat
           const int w = c_n18[rr][0];
           off = d.idx(w < 0 ? i : n.x[w], w < 0 ? j : n.y[w], k + c_n18[rr][1]);
 #pragma unroll
-          for (int a = 0; a < 9; ++a) A[a] = __ldg(wc + (long long)(rr * 9 + a) * nr_);
+          for (int a = 0; a < 9; ++a) A[a] = __ldg(wc + (long long)(rr * 9 + a) * ord.nw);
         } else {
           w7b_row(d, ph, g, p, i, j, k, n, rr, cx, cy, cz, l0, obl0, c0, A, off);
         }
@@ -456,6 +507,8 @@ __global__ void __launch_bounds__(TPB) k_weno7b(Dims d, PhysC ph, DGeom g, DStat
           for (int a = 0; a < 9; ++a) Y[qq][a] = Y[qq][a] + A[a] * Rv;
         }
       }
+      const unsigned long long qsrc = kShared ? s.lsq_map9[p].src : LSQ_IDENTITY_SRC;
+      const unsigned int qneg = kShared ? s.lsq_map9[p].neg : 0u;
 #pragma unroll
       for (int qq = 0; qq < W7B_QG; ++qq) {
         const int q = q0 + qq;
@@ -463,7 +516,7 @@ __global__ void __launch_bounds__(TPB) k_weno7b(Dims d, PhysC ph, DGeom g, DStat
 #pragma unroll
         for (int a = 0; a < 9; ++a) {
           if (kCached) {
-            X[a] = Y[qq][a];
+            X[a] = kShared ? lsq_rotated<1>(Y[qq], a + 1, qsrc, qneg) : Y[qq][a];
           } else {
             R sacc = R(0.0);
 #pragma unroll
@@ -501,7 +554,8 @@ __global__ void __launch_bounds__(TPB) k_weno7b(Dims d, PhysC ph, DGeom g, DStat
 
 template <typename R>
 __global__ void k_ops_m9(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
-  const long long nr_ = r.count();
+  // shared by the panels: panel 1's zones only (the first sixth of the range)
+  const long long nr_ = s.lsq_map9 ? r.count() / 6 : r.count();
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nr_; t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
     r.decode(t, p, i, j, k);
@@ -1368,11 +1422,13 @@ __device__ __forceinline__ void e9c_minv(const Dims& d, const DGeom& g, int p, i
 // Only the point value (mode 1) is stored: the LLF edge solver consumes
 // nothing else.  kCached: the inverse normal matrix comes from the
 // operator cache.  Blocks per SM: 4 for FP64, 6 for FP32 (measured).
-template <bool kCached, typename R>
+template <bool kCached, bool kShared, typename R>
 __global__ void __launch_bounds__(TPB, sizeof(R) == 4 ? 6 : 4) k_efield_c(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
   const R ob12 = R(1.0) / R(12.0), ob180 = R(1.0) / R(180.0), ob144 = R(1.0) / R(144.0);
-  const long long nr_ = r.count();
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nr_; t += (long long)gridDim.x * blockDim.x) {
+  const LsqOrder<kShared> ord(r);
+  for (long long it = ord.begin(); it < ord.nit; it += ord.stride()) {
+    long long t, tw;
+    if (!ord.zone(it, t, tw)) continue;
     int p, i, j, k;
     r.decode(t, p, i, j, k);
     if (mask_at(g, d, p, i, j) != 1) continue;
@@ -1386,7 +1442,7 @@ __global__ void __launch_bounds__(TPB, sizeof(R) == 4 ? 6 : 4) k_efield_c(Dims d
     // W_rr = Minv A_rr^T (geometry only), so X = sum_rr W_rr E_rr directly.
     R Minv[kCached ? 1 : 100];
     if (!kCached) e9c_minv(d, g, p, i, j, k, n, cx, cy, cz, obl0, c0, Minv);
-    const R* wc = s.op_m10 + t;
+    const R* wc = s.op_m10 + tw;
     auto MI = [&](int e) { return Minv[kCached ? 0 : e]; };
     R Y[3][10];
 #pragma unroll
@@ -1405,7 +1461,7 @@ __global__ void __launch_bounds__(TPB, sizeof(R) == 4 ? 6 : 4) k_efield_c(Dims d
           off = d.idx(w < 0 ? i : n.x[w], w < 0 ? j : n.y[w], k + c_n18[rr - 1][1]);
         }
 #pragma unroll
-        for (int a = 0; a < 10; ++a) A[a] = __ldg(wc + (long long)(rr * 10 + a) * nr_);
+        for (int a = 0; a < 10; ++a) A[a] = __ldg(wc + (long long)(rr * 10 + a) * ord.nw);
       } else {
         e9c_row(d, g, p, i, j, k, n, rr, cx, cy, cz, obl0, c0, A, off);
       }
@@ -1419,13 +1475,15 @@ __global__ void __launch_bounds__(TPB, sizeof(R) == 4 ? 6 : 4) k_efield_c(Dims d
     const R f = s.flatA[d.at(0, p, i, j, k)];
     const R betalo = f + (R(1.0) - f) * R(2.0);
     const R ghi = f * R(0.6) + (R(1.0) - f) * R(0.95), glo = R(1.0) - ghi, obghi = R(1.0) / ghi, grat = glo / ghi;
+    const unsigned long long qsrc = kShared ? s.lsq_map10[p].src : LSQ_IDENTITY_SRC;
+    const unsigned int qneg = kShared ? s.lsq_map10[p].neg : 0u;
 #pragma unroll 1
     for (int q = 0; q < 3; ++q) {
       R X[10];
 #pragma unroll
       for (int a = 0; a < 10; ++a) {
         if (kCached) {
-          X[a] = Y[q][a];
+          X[a] = kShared ? lsq_rotated<0>(Y[q], a, qsrc, qneg) : Y[q][a];
         } else {
           R acc = R(0.0);
 #pragma unroll
@@ -1461,7 +1519,7 @@ __global__ void __launch_bounds__(TPB, sizeof(R) == 4 ? 6 : 4) k_efield_c(Dims d
 
 template <typename R>
 __global__ void k_ops_m10(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
-  const long long nr_ = r.count();
+  const long long nr_ = s.lsq_map10 ? r.count() / 6 : r.count();
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nr_; t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
     r.decode(t, p, i, j, k);
@@ -1722,9 +1780,12 @@ void launch_weno_t(Solve& sv, DStateT<R>& st) {
   k_weno7a<R><<<blocks_for(a.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, a);
   mark(sv, "k_weno7a");
   if (st.op_m9)
-    k_weno7b<true, R><<<blocks_for(b.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
+    if (st.lsq_map9)
+      k_weno7b<true, true, R><<<blocks_for(b.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
+    else
+      k_weno7b<true, false, R><<<blocks_for(b.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
   else
-    k_weno7b<false, R><<<blocks_for(b.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
+    k_weno7b<false, false, R><<<blocks_for(b.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
   mark(sv, "k_weno7b");
 }
 
@@ -1873,9 +1934,12 @@ void launch_efield_t(Solve& sv, DStateT<R>& st) {
   k_efield_b<R><<<blocks_for(a.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, a);
   mark(sv, "k_efield_b");
   if (st.op_m10)
-    k_efield_c<true, R><<<blocks_for(b.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
+    if (st.lsq_map10)
+      k_efield_c<true, true, R><<<blocks_for(b.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
+    else
+      k_efield_c<true, false, R><<<blocks_for(b.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
   else
-    k_efield_c<false, R><<<blocks_for(b.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
+    k_efield_c<false, false, R><<<blocks_for(b.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
   mark(sv, "k_efield_c");
 }
 

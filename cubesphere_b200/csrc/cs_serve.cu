@@ -55,7 +55,13 @@ size_t mesh_device_bytes(const cs_params& p) {
   bytes += (size_t)6 * 4 * (p.nghost + 1) * (p.ntp + 2 * p.nghost + 1) * (p.nr + 2 * p.nghost + 1) * 12 * 9 * 2;
   const size_t nl = (size_t)6 * (p.ntp + 2 * p.nghost - 4) * (p.ntp + 2 * p.nghost - 4) * (p.nr + 2 * p.nghost - 4);
   const size_t na = (size_t)6 * (p.ntp + 2 * p.nghost - 2) * (p.ntp + 2 * p.nghost - 2) * (p.nr + 2 * p.nghost - 2);
-  if (!(p.flags & CS_FLAG_NO_OP_CACHE)) bytes += nl * 352 * ((p.flags & CS_FLAG_FP32) ? sizeof(float) : sizeof(double));
+  if (!(p.flags & CS_FLAG_NO_OP_CACHE)) {
+    // row weights shared by the six panels unless per-panel ones are asked
+    // for: STEP 9.c's always, STEP 7.b's in the precision form
+    const bool f32 = (p.flags & CS_FLAG_FP32) != 0, per = (p.flags & CS_FLAG_LSQ_PER_PANEL) != 0;
+    const size_t n9 = (per || !f32) ? nl : nl / 6, n10 = per ? nl : nl / 6;
+    bytes += (n9 * 162 + n10 * 190) * (f32 ? sizeof(float) : sizeof(double));
+  }
   if (!(p.flags & CS_FLAG_NO_ADP_CACHE)) {
     // factors shared by the six panels unless per-panel ones are asked for
     const size_t nz = (p.flags & CS_FLAG_ADP_PER_PANEL) ? na : na / 6;

@@ -60,6 +60,8 @@ struct MeshRes {
   PanelSync psync{};
   void* op_m9 = nullptr;   // least-squares inverses in the state's type (FP32 in the precision form)
   void* op_m10 = nullptr;
+  void* lsq_map = nullptr;  // LsqPanelMap[6] when row weights are panel 1's only
+  bool m9_shared = false, m10_shared = false;  // which of op_m9 / op_m10 are panel 1's only
   double* adp_lu = nullptr;
   int8_t* adp_piv = nullptr;
   int8_t* adp_pmap = nullptr;  // ADP factors shared by the panels: per panel [unknown map][sign]

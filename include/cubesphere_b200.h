@@ -127,6 +127,20 @@ typedef struct cs_params {
  * round-off.  This flag restores per-panel factors; meshes without the
  * symmetry use them anyway. */
 #define CS_FLAG_ADP_PER_PANEL 16
+/* cs_params.flags: keep one set of least-squares row weights per panel.  By
+ * default the resident row weights W_r = Minv A_r^T of STEP 9.c (and of
+ * STEP 7.b in the precision form) are panel 1's only: where every panel is
+ * a signed-permutation rotation of panel 1 with the same stencil table and
+ * mask, a zone's rows transform by the induced signed permutation Q of the
+ * modes, so W_r(panel p) = Q^T W_r(panel 1); the stage sums over panel 1's
+ * weights and rotates the sums (a select and a sign per mode), and the six
+ * blocks that read one tile's weights run side by side so five of them hit
+ * L2.  The row weights then take 1.55 KB per zone in FP64 (STEP 7.b's stay
+ * per panel there: its kernel, at its register limit, measured slower
+ * shared) and 0.23 KB in the precision form, against 2.8 and 1.4 KB.  The
+ * results agree with per-panel weights to round-off.  This flag restores
+ * per-panel weights; meshes without the symmetry use them anyway. */
+#define CS_FLAG_LSQ_PER_PANEL 32
 
 /* Seeded initial-state description (new generator cases of the problem
  * library, built with the reference mechanism of 820init_patch_cube_sphere.f). */
@@ -180,12 +194,20 @@ int cs_mesh_build(cs_ctx* ctx);
  * maps, resident operators) instead of building its own, and allocates only
  * its state.  The parameters that define the mesh (ntp, nr, nghost,
  * radial_mesh, rmin, rmax, radial_ratio, smallnum and the NO_ADP_CACHE,
- * NO_OP_CACHE, NO_PANEL_SYNC and FP32 flags) must be equal, and both
+ * NO_OP_CACHE, NO_PANEL_SYNC, FP32, ADP_PER_PANEL and LSQ_PER_PANEL flags)
+ * must be equal, and both
  * contexts on the current device.  The mesh is freed with the last context
  * that uses it.  The reference builds the mesh once per patch and run
  * (MAKE_MESH_GNOMONIC_CS_SECTOR, 201) and has no counterpart for sharing
  * it between solves. */
 int cs_mesh_share(cs_ctx* ctx, const cs_ctx* from);
+/* Device bytes held by the context's mesh: geometry, mask, stencil,
+ * ghost-exchange and panel-ownership maps and the resident operators (ADP
+ * factors, least-squares row weights).  Contexts attached to one mesh
+ * report the same figure; cs_estimate_device_bytes plans it before a
+ * build.  No reference counterpart (the reference does not account device
+ * memory). */
+int cs_mesh_device_bytes(cs_ctx* ctx, uint64_t* bytes);
 /* Host-only mesh build (no device is touched); the geometry, mask and
  * stencil getters below then work without a GPU. */
 int cs_mesh_build_host(cs_ctx* ctx);

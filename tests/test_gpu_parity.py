@@ -204,6 +204,46 @@ def test_shared_panel_adp_matches_per_panel_factors(name, rk):
     check_state(s, st0, st1)
 
 
+@pytest.mark.parametrize("name,rk,form", [("shell16", cs.CS_IMEX_RK2, 0), ("surface32", cs.CS_SSPRK3, 0),
+                                          ("shell16", cs.CS_IMEX_RK2, cs.CS_FLAG_FP32)])
+def test_shared_panel_row_weights_match_per_panel(name, rk, form):
+    """The default least-squares row weights (panel 1's, summed and then
+    rotated to each panel's modes) hold a sixth of the per-panel weights on
+    the device (STEP 9.c's; STEP 7.b's too in the precision form), give the
+    slopes of STEP 7.b and the E point values of STEP 9.c of the per-panel
+    weights to round-off, and the same steps within the parity tolerance
+    (FP64) or to FP32 rounding (precision form)."""
+    pr = cs.preset(name)
+    pr["params"]["rk_scheme"] = rk
+    out = []
+    for flags in (form, form | cs.CS_FLAG_LSQ_PER_PANEL):
+        s = cs.Solve(**pr["params"], flags=flags)
+        s.mesh_build()
+        s.init_problem(**pr["init"])
+        s.fill_ghosts()
+        s.limit_all_slopes_p12()
+        V, E1 = s.debug("V"), s.debug("E1")
+        s.init_problem(**pr["init"])
+        dt = s.evaluate_timestep(1e30)
+        for _ in range(2):
+            dt = s.step(dt)
+        out.append((s, s.mesh_device_bytes(), V, E1, dt, s.get_state()))
+    (s, b0, V0, E0, d0, st0), (_, b1, V1, E1, d1, st1) = out
+    nl = 6 * (s.N + 2 * s.G - 4) ** 2 * (s.nr + 2 * s.G - 4)
+    words, size = (352, 4) if form else (190, 8)  # shared: both operators in FP32, STEP 9.c's in FP64
+    assert b1 - b0 == (nl - nl // 6) * words * size - 6 * 16  # the weights, less the six panel maps
+    tw, ts = (1e-5, 1e-5) if form else (1e-11, TOL_STATE)
+    for m in range(10):
+        for c in range(8):
+            e = rel(zones(s, V0[m * 8 + c], 0, 1), zones(s, V1[m * 8 + c], 0, 1))
+            assert e <= tw, ("V mode", m, c, e)
+    for q in range(3):
+        e = rel(zones(s, E0[q], 0, 1), zones(s, E1[q], 0, 1))
+        assert e <= tw, ("E point value", q, e)
+    assert abs(d0 - d1) <= ts * d1
+    check_state(s, st0, st1, tol=ts)
+
+
 @pytest.mark.parametrize("name,flags", [("shell16", 0), ("surface32", 0), ("shell16", cs.CS_FLAG_FP32)])
 def test_device_initial_state_matches_host(name, flags):
     """cs_init_problem builds the seeded state on the device; it agrees with
