@@ -62,8 +62,9 @@ ALGO_WORDS_PER_UNIT = {
     # + 2 volumes + scale), 16 contributions + 3 speeds/entropy flux out
     "k_flux": 90 + 30 + 19,
     # E snapshot (3) and modes 1-3 (9) in, E mode 0 out (3), flattener,
-    # moments, the resident row weights (19 x 10)
-    "k_efield_c": 3 + 9 + 3 + 1 + 10 + 190,
+    # moments, the resident row weights (19 x 10, panel 1's serving the six
+    # panels: 1/6 per zone)
+    "k_efield_c": 3 + 9 + 3 + 1 + 10 + 190 / 6,
     "k_positivity": 80 + 4 + 80,
     "k_faceB": 80 + 1 + 20 + 5,
 }

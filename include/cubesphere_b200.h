@@ -94,8 +94,9 @@ typedef struct cs_params {
 #define CS_FLAG_NO_ADP_CACHE 1
 /* cs_params.flags: likewise for the least-squares solution operators of
  * the reconstructions of the primitives and of E (STEPS 7.b / 9.c): per
- * zone, each stencil row's weights W = Minv A_row^T (2.8 KB per zone in
- * FP64, 1.4 KB in the precision form); without them every stage rebuilds
+ * zone, each stencil row's weights W = Minv A_row^T (1.55 KB per zone in
+ * FP64 and 0.23 KB in the precision form, shared by the panels by default:
+ * see CS_FLAG_LSQ_PER_PANEL); without them every stage rebuilds
  * the rows and the normal matrices and inverts them (same results to
  * round-off). */
 #define CS_FLAG_NO_OP_CACHE 2
