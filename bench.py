@@ -79,7 +79,7 @@ MEASURED_TRAFFIC_PER_UNIT = {
     "k_flux": (150.846e6 + 18.736e6 + 155.063e6 + 19.871e6 + 168.527e6 + 18.285e6) / 3 / 155520,
     "k_weno7b": (269.9e6 + 124.4e6) / 155520,
     "k_face_states": (254.736e6 + 308.688e6) / 155520,
-    "k_efield_c": (268.4e6 + 53.59e6) / 155520,
+    "k_efield_c": (68.69e6 + 7.622e6) / 155520,
 }
 # FP64 operations per unit (2 x DFMA + DADD + DMUL thread instructions),
 # from the same ncu captures.  The path is FP64-bound, so the roofline also
@@ -91,7 +91,7 @@ FP64_FLOP_PER_UNIT = {
     "k_flux": (5.448e8 + 5.448e8 + 6.120e8) / 3 / 155520,
     "k_weno7b": 5.79e8 / 155520,
     "k_face_states": 1.163e9 / 155520,
-    "k_efield_c": 2.32e8 / 155520,
+    "k_efield_c": 2.367e8 / 155520,
 }
 FP64_NOMINAL_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12
 
