@@ -62,7 +62,7 @@ __global__ void __launch_bounds__(FS_TPB) k_face_states(Dims d, PhysC ph, DGeom 
       R v[10];
 #pragma unroll
       for (int m = 0; m < 10; ++m) v[m] = Vm(s, d, c, m, p, o);
-#pragma unroll 5
+#pragma unroll
       for (int fq = 0; fq < 30; ++fq)
         s.FS[((long long)(fq * 9 + c) * NPANEL + p) * d.S + o] =
             d_poly10(v, c0, xs[fq * 3 + 0][tid], xs[fq * 3 + 1][tid], xs[fq * 3 + 2][tid]);
