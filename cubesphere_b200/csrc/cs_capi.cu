@@ -713,11 +713,11 @@ int mesh_operators(Solve& sv, MeshRes& m, DStateT<R>& s) {
   cudaError_t e = cudaSuccess;
   // ADP: the KKT matrix of every zone depends on the geometry only, so its
   // factors are computed once here and each stage only substitutes.  They
-  // take 10.4 KB per zone; without room for them (or with
-  // CS_FLAG_NO_ADP_CACHE) every stage assembles and factors in place.
-  // The least-squares solution operators of STEPS 7.b / 9.c are
-  // geometry-only as well: the row weights Minv A_row^T (2.8 KB per zone
-  // in FP64).
+  // take 10.4 KB per zone per panel (1.7 KB shared by the panels); without
+  // room for them (or with CS_FLAG_NO_ADP_CACHE) every stage assembles and
+  // factors in place.  The least-squares solution operators of STEPS
+  // 7.b / 9.c are geometry-only as well: the row weights Minv A_row^T
+  // (2.8 KB per zone in FP64 per panel, 1.55 KB with STEP 9.c's shared).
   if (!(sv.p.flags & CS_FLAG_NO_OP_CACHE)) {
     // Panel-shared row weights where the mesh allows: STEP 9.c's always,
     // STEP 7.b's in the precision form only (the FP64 k_weno7b, at its

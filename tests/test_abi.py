@@ -52,3 +52,18 @@ def test_geometry_getter_checks_buffer_size():
     buf = np.zeros(5)
     rc = s.lib.cs_geometry_get(s.h, 0, buf.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), buf.size)
     assert rc == 1
+
+
+def test_device_estimate_counts_panel_shared_row_weights():
+    """The planning estimate counts the least-squares row weights the mesh
+    build keeps: panel 1's serving the six panels by default (STEP 9.c's in
+    FP64, both sets in the precision form), one set per panel with
+    CS_FLAG_LSQ_PER_PANEL."""
+    kw = dict(ntp=32, nr=16, nghost=4)
+    nl = 6 * (32 + 2 * 4 - 4) ** 2 * (16 + 2 * 4 - 4)
+    f64 = cs.estimate_device_bytes(**kw)
+    f64_pp = cs.estimate_device_bytes(**kw, flags=cs.CS_FLAG_LSQ_PER_PANEL)
+    assert f64_pp - f64 == (nl - nl // 6) * 190 * 8
+    f32 = cs.estimate_device_bytes(**kw, flags=cs.CS_FLAG_FP32)
+    f32_pp = cs.estimate_device_bytes(**kw, flags=cs.CS_FLAG_FP32 | cs.CS_FLAG_LSQ_PER_PANEL)
+    assert f32_pp - f32 == (nl - nl // 6) * 352 * 4
