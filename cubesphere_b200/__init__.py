@@ -33,7 +33,7 @@ DEBUG = {
     "V": (0, 80), "ent_modes": (1, 4), "flatten": (2, 1), "dUdt": (3, 8),
     "Efx": (4, 1), "Efy": (5, 1), "Efz": (6, 1),
     "Bxq": (7, 5), "Byq": (8, 5), "Bzq": (9, 5), "E1": (10, 3),
-    "speeds": (11, 6), "entflux": (12, 3),
+    "speeds": (11, 6), "entflux": (12, 3), "positivity": (13, 1),
 }
 
 RADIAL = {"uniform": 0, "log": 1, "stretched": 2}
@@ -50,7 +50,7 @@ EXPORTS = [
     "cs_cfl_timestep_noalloc", "cs_estimate_device_bytes", "cs_serve_create", "cs_serve_submit",
     "cs_serve_wait", "cs_serve_state", "cs_serve_stats", "cs_serve_destroy",
     "cs_batch_create", "cs_batch_steps", "cs_batch_autotune", "cs_batch_grid_fraction", "cs_batch_last_error",
-    "cs_batch_destroy", "cs_twod_rs_ez",
+    "cs_batch_destroy", "cs_twod_rs_ez", "cs_pointwise",
     "cs_snapshot_save", "cs_snapshot_load", "cs_snapshot_write_host", "cs_snapshot_read_host",
 ]
 
@@ -183,6 +183,7 @@ def load_library() -> ctypes.CDLL:
         "cs_batch_last_error": ([P], ctypes.c_char_p),
         "cs_batch_destroy": ([P], ctypes.c_int),
         "cs_twod_rs_ez": ([ctypes.c_int32, ctypes.c_int32, dp, dp], ctypes.c_int),
+        "cs_pointwise": ([ctypes.POINTER(CsParams), ctypes.c_int32, ctypes.c_int32, dp, dp], ctypes.c_int),
         "cs_snapshot_save": ([P, ctypes.c_char_p, D, D, ctypes.c_int64], ctypes.c_int),
         "cs_snapshot_load": ([P, ctypes.c_char_p, dp, dp, ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
         "cs_snapshot_write_host": ([ctypes.c_char_p, ctypes.POINTER(CsParams), dp, dp, dp, dp, dp, D, D,
@@ -543,6 +544,23 @@ def twod_rs_ez(kind: int, cases: np.ndarray) -> np.ndarray:
     rc = load_library().cs_twod_rs_ez(kind, a.shape[0], _dptr(a), _dptr(out))
     if rc:
         raise CsError(f"cs_twod_rs_ez failed ({rc})")
+    return out
+
+
+def pointwise(kind: int, cases: np.ndarray, **params) -> np.ndarray:
+    """The device pointwise physics on each row of `cases` (see cs_pointwise):
+    kind 0 PRIM_TO_CONS (8 prims + entropy -> 8 conserved), 1 CONS_TO_PRIM
+    (8 conserved + entropy -> 8 prims, entropy, floor flag, 8 conserved),
+    2 the HLL solve (V_L, V_R, ent_L, ent_R -> Fluct_L, Fluct_R, F_L, F_R,
+    S_L, S_R, entropy flux); params as for Solve (flags=CS_FLAG_FP32 for
+    the precision form)."""
+    nin, nout = {0: (9, 8), 1: (9, 18), 2: (18, 35)}[kind]
+    a = np.ascontiguousarray(cases, dtype=np.float64).reshape(-1, nin)
+    out = np.zeros((a.shape[0], nout))
+    p = make_params(**params)
+    rc = load_library().cs_pointwise(ctypes.byref(p), kind, a.shape[0], _dptr(a), _dptr(out))
+    if rc:
+        raise CsError(f"cs_pointwise failed ({rc})")
     return out
 
 

@@ -71,12 +71,15 @@ def build_library(verbose: bool = False) -> Path:
 
 
 def build_oracle() -> Path:
-    srcs = [ORACLE_DIR / "oracle.cpp"]
-    deps = srcs + [ORACLE_DIR / "oracle_core.h"]
+    """The oracle library: oracle.cpp plus the host mesh builder and seeded
+    initial state compiled from their sources (mesh.cpp, init.cpp), so that
+    a CPU solve loads nothing else."""
+    srcs = [ORACLE_DIR / "oracle.cpp", CSRC / "mesh.cpp", CSRC / "init.cpp"]
+    deps = srcs + [ORACLE_DIR / "oracle_core.h", CSRC / "cs_internal.h", ROOT / "include" / "cubesphere_b200.h"]
     if _stale(ORACLE_LIB, deps):
         # No FMA contraction: the oracle evaluates every expression as written.
         _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-ffp-contract=off", "-fopenmp",
-              "-o", str(ORACLE_LIB)] + [str(s) for s in srcs])
+              "-I", str(ROOT / "include"), "-I", str(CSRC), "-o", str(ORACLE_LIB)] + [str(s) for s in srcs])
     return ORACLE_LIB
 
 

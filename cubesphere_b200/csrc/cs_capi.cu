@@ -1009,13 +1009,64 @@ cudaError_t debug_copy(Solve& sv, const DStateT<R>& s, int which, size_t nc, dou
     case 12:
       for (int q = 0; q < 3 && e == cudaSuccess; ++q) e = cp(host_out + q * S6, s.EF[q], S6);
       break;
+    case 13: {
+      std::vector<int32_t> flags(S6);
+      e = cudaMemcpyAsync(flags.data(), s.giveup, S6 * sizeof(int32_t), cudaMemcpyDeviceToHost, sv.stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(sv.stream);
+      for (size_t t = 0; e == cudaSuccess && t < S6; ++t) host_out[t] = (double)flags[t];
+      break;
+    }
   }
   return e;
 }
 
 size_t field_ncomp_debug(int which) {
-  static const int nc[13] = {NVAR * NMODE, 4, 1, NVAR, 1, 1, 1, NQ, NQ, NQ, 3, 6, 3};
-  return (which < 0 || which > 12) ? 0 : (size_t)nc[which];
+  static const int nc[14] = {NVAR * NMODE, 4, 1, NVAR, 1, 1, 1, NQ, NQ, NQ, 3, 6, 3, 1};
+  return (which < 0 || which > 13) ? 0 : (size_t)nc[which];
+}
+
+// Known-answer access to the pointwise physics the stage kernels call: one
+// thread per case, in the state type R of the form (see cs_pointwise).
+template <typename R>
+__global__ void k_pointwise(PhysC ph, int kind, int n, const double* in, double* out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  if (kind == 0) {
+    const double* a = in + (long long)t * 9;
+    R V[8], U[8];
+    for (int c = 0; c < 8; ++c) V[c] = (R)a[c];
+    d_prim_to_cons(ph, (R)a[8], U, V);
+    for (int c = 0; c < 8; ++c) out[(long long)t * 8 + c] = (double)U[c];
+  } else if (kind == 1) {
+    const double* a = in + (long long)t * 9;
+    R V[8], U[8];
+    for (int c = 0; c < 8; ++c) U[c] = (R)a[c];
+    R ent = (R)a[8];
+    const int flag = d_cons_to_prim(ph, ent, U, V);
+    double* o = out + (long long)t * 18;
+    for (int c = 0; c < 8; ++c) o[c] = (double)V[c];
+    o[8] = (double)ent;
+    o[9] = (double)flag;
+    for (int c = 0; c < 8; ++c) o[10 + c] = (double)U[c];
+  } else {
+    const double* a = in + (long long)t * 18;
+    R VL[8], VR[8], FlL[8], FlR[8], FL[8], FR[8], SL, SR, entF;
+    for (int c = 0; c < 8; ++c) {
+      VL[c] = (R)a[c];
+      VR[c] = (R)a[8 + c];
+    }
+    d_hll(ph, VL, VR, (R)a[16], (R)a[17], FlL, FlR, FL, FR, SL, SR, entF);
+    double* o = out + (long long)t * 35;
+    for (int c = 0; c < 8; ++c) {
+      o[c] = (double)FlL[c];
+      o[8 + c] = (double)FlR[c];
+      o[16 + c] = (double)FL[c];
+      o[24 + c] = (double)FR[c];
+    }
+    o[32] = (double)SL;
+    o[33] = (double)SR;
+    o[34] = (double)entF;
+  }
 }
 
 }  // namespace
@@ -1395,6 +1446,34 @@ int cs_debug_get(cs_ctx* ctx, int32_t which, double* host_out, size_t n) {
                                  : cs::debug_copy(sv, sv.st, which, nc, host_out);
   if (e != cudaSuccess) return cs::cuda_fail(sv, e, "cs_debug_get copy");
   return CS_OK;
+}
+
+int cs_pointwise(const cs_params* p, int32_t kind, int32_t n, const double* in, double* out) {
+  if (!p || kind < 0 || kind > 2 || n < 0 || (n > 0 && (!in || !out))) return CS_ERR_ARG;
+  std::string why;
+  if (!cs::check_params(*p, why)) return CS_ERR_ARG;
+  if (n == 0) return CS_OK;
+  static const int nin[3] = {9, 9, 18}, nout[3] = {8, 18, 35};
+  const size_t bi = (size_t)n * nin[kind] * sizeof(double), bo = (size_t)n * nout[kind] * sizeof(double);
+  double *din = nullptr, *dout = nullptr;
+  if (cudaMalloc(&din, bi) != cudaSuccess) return CS_ERR_CUDA;
+  if (cudaMalloc(&dout, bo) != cudaSuccess) {
+    cudaFree(din);
+    return CS_ERR_CUDA;
+  }
+  const cs::PhysC ph = cs::make_phys(*p);
+  cudaError_t e = cudaMemcpy(din, in, bi, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    if (p->flags & CS_FLAG_FP32)
+      cs::k_pointwise<float><<<(n + 127) / 128, 128>>>(ph, kind, n, din, dout);
+    else
+      cs::k_pointwise<double><<<(n + 127) / 128, 128>>>(ph, kind, n, din, dout);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(out, dout, bo, cudaMemcpyDeviceToHost);
+  cudaFree(din);
+  cudaFree(dout);
+  return e == cudaSuccess ? CS_OK : CS_ERR_CUDA;
 }
 
 int cs_snapshot_save(cs_ctx* ctx, const char* path, double time, double dtcur, int64_t step) {

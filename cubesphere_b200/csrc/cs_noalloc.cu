@@ -5,8 +5,6 @@
 // and cs_evaluate_timestep: min(1.1 dtcur, min over the active interior
 // zones of cfl * v_scale / (|v| + c_fast)), with the conserved->primitive
 // repair applied in registers only (the arrays are not written).
-#include <mutex>
-
 #include "cs_solve.h"
 
 namespace cs {
@@ -65,9 +63,6 @@ __global__ void k_cfl_final(const double* part, int nparts, double start, double
   }
 }
 
-std::mutex g_sym_mu;
-double* g_sym_addr[64] = {nullptr};
-
 }  // namespace
 }  // namespace cs
 
@@ -78,18 +73,12 @@ extern "C" int cs_cfl_timestep_noalloc(const double* U, const double* ent, const
   if (!U || !ent || !v_scale || !mask || !dtcurp1) return CS_ERR_ARG;
   if (ntp < 1 || nr < 1 || nghost < 1 || !(dtcur > 0.0) || !(gamma > 1.0)) return CS_ERR_ARG;
   if (nr > cs::kMaxLayers) return CS_ERR_ARG;  // scratch holds 6 * 2048 layer partials
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return CS_ERR_CUDA;
+  // The scratch's device address in the current device's context, looked
+  // up on every call: an address kept from an earlier call would be stale
+  // after cudaDeviceReset or under another context.  The first lookup on a
+  // device may load the module.
   double* scratch = nullptr;
-  {
-    std::lock_guard<std::mutex> lk(cs::g_sym_mu);
-    if (!cs::g_sym_addr[dev]) {
-      // once per device; may load the module, so it must not run inside a
-      // stream capture
-      if (cudaGetSymbolAddress((void**)&cs::g_sym_addr[dev], cs::g_cfl_scratch) != cudaSuccess) return CS_ERR_CUDA;
-    }
-    scratch = cs::g_sym_addr[dev];
-  }
+  if (cudaGetSymbolAddress((void**)&scratch, cs::g_cfl_scratch) != cudaSuccess || !scratch) return CS_ERR_CUDA;
   cs::Dims d;
   d.N = ntp;
   d.nr = nr;

@@ -718,7 +718,8 @@ __global__ void __launch_bounds__(TPB, 4) k_positivity(Dims d, PhysC ph, DGeom g
         }
       for (int m = 1; m < 4; ++m) s.ent[d.at(m, p, i, j, k)] = gave_up ? 0.0 : ep[m];
     }
-    s.giveup[d.at(0, p, i, j, k)] = gave_up;
+    // bit 0: gave up; bits 1-4: shrink passes applied
+    s.giveup[d.at(0, p, i, j, k)] = gave_up | (nshrink << 1);
   }
 }
 
@@ -729,7 +730,7 @@ __global__ void k_apply_giveup(Dims d, DStateT<R> s, Range3 r) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
     r.decode(t, p, i, j, k);
-    if (s.giveup[d.at(0, p, i, j, k)]) s.ent[d.at(0, p, i, j, k)] = 0.0;
+    if (s.giveup[d.at(0, p, i, j, k)] & 1) s.ent[d.at(0, p, i, j, k)] = 0.0;
   }
 }
 

@@ -146,6 +146,11 @@ void run_request(cs_server* sv, int64_t id) {
         sv->meshes.erase(it);
       } else {
         it->second.mesh = ctx->sv.mesh;
+        // account the mesh at what it holds (per-panel operators where the
+        // panel-sharing check failed take more than the estimate)
+        const size_t held = ctx->sv.mesh->bytes;
+        sv->reserved = sv->reserved - it->second.bytes + held;
+        it->second.bytes = held;
         sv->mesh_builds += 1;
       }
     }

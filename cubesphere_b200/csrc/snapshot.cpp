@@ -80,6 +80,11 @@ int cs_snapshot_write_host(const char* path, const cs_params* p, const double* U
         ",\"nghost\":" + std::to_string(p->nghost) + ",\"radial_mesh\":" + std::to_string(p->radial_mesh);
   js += ",\"rmin\":" + fmt_double(p->rmin) + ",\"rmax\":" + fmt_double(p->rmax) +
         ",\"radial_ratio\":" + fmt_double(p->radial_ratio) + ",\"gamma\":" + fmt_double(p->gamma);
+  js += ",\"rhofloor\":" + fmt_double(p->rhofloor) + ",\"prsfloor\":" + fmt_double(p->prsfloor) +
+        ",\"smallnum\":" + fmt_double(p->smallnum) + ",\"cfl_coef\":" + fmt_double(p->cfl_coef) +
+        ",\"flatten_coef\":" + fmt_double(p->flatten_coef) +
+        ",\"prs_flatten_coef\":" + fmt_double(p->prs_flatten_coef) + ",\"gm\":" + fmt_double(p->gm) +
+        ",\"bc_lower\":" + std::to_string(p->bc_lower) + ",\"bc_upper\":" + std::to_string(p->bc_upper);
   js += ",\"rk_scheme\":" + std::to_string(p->rk_scheme) + ",\"time\":" + fmt_double(time) +
         ",\"dtcur\":" + fmt_double(dtcur) + ",\"step\":" + std::to_string((long long)step);
   js += ",\"arrays\":[{\"name\":\"U\",\"components\":8,\"doubles\":" + std::to_string(cnt[0]) +
@@ -122,7 +127,12 @@ int cs_snapshot_read_host(const char* path, const cs_params* p, double* U, doubl
     double want;
   } checks[] = {{"ntp", (double)p->ntp},       {"nr", (double)p->nr},         {"nghost", (double)p->nghost},
                 {"radial_mesh", (double)p->radial_mesh}, {"rmin", p->rmin}, {"rmax", p->rmax},
-                {"radial_ratio", p->radial_ratio},       {"gamma", p->gamma}};
+                {"radial_ratio", p->radial_ratio},       {"gamma", p->gamma},
+                {"rhofloor", p->rhofloor},               {"prsfloor", p->prsfloor},
+                {"smallnum", p->smallnum},               {"cfl_coef", p->cfl_coef},
+                {"flatten_coef", p->flatten_coef},       {"prs_flatten_coef", p->prs_flatten_coef},
+                {"gm", p->gm},                           {"bc_lower", (double)p->bc_lower},
+                {"bc_upper", (double)p->bc_upper},       {"rk_scheme", (double)p->rk_scheme}};
   for (const auto& c : checks)
     if (!find_num(js, c.key, v) || v != c.want) {
       std::fclose(f);

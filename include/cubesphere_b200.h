@@ -263,7 +263,9 @@ int cs_cleanup_after_update(cs_ctx* ctx);
  * which: 0 V (8 comps x 10 modes, comp-major [m*8+c]), 1 entropy modes (4),
  * 2 flattener (1), 3 dU_dt (8), 4 Efx, 5 Efy, 6 Efz, 7 Bxf_quadpts (5),
  * 8 Byf_quadpts (5), 9 Bzf_quadpts (5), 10 E_zc mode-1 (3),
- * 11 face speeds S_L,S_R,S_D,S_U,S_B,S_T (6), 12 entropy fluxes x,y,z (3). */
+ * 11 face speeds S_L,S_R,S_D,S_U,S_B,S_T (6), 12 entropy fluxes x,y,z (3),
+ * 13 positivity record of STEP 7.c per zone (1): 2 x the shrink passes
+ * applied (0-15) plus 1 where the zone gave up (440:553-830). */
 int cs_debug_get(cs_ctx* ctx, int32_t which, double* host_out, size_t n_doubles);
 
 /* Timing and launch accounting.  cs_get_stream returns the context's
@@ -288,11 +290,15 @@ int cs_profile_end(cs_ctx* ctx, int32_t max_kernels, char* names, double* total_
  * of the layout above in device memory; nothing is written to them.  The
  * reduction scratch is a fixed static device array (6 x 2048 layer partials,
  * 96 KB), so nr > 2048 is rejected with CS_ERR_ARG; no slot needs clearing
- * (each is written before it is read).  The first call on a device looks the
- * scratch up with cudaGetSymbolAddress and must not happen inside a stream
- * capture.  All calls on a device share the scratch: calls that overlap in
- * time (other threads or streams) race, so serialize them.  Runs on stream
- * (cudaStream_t, may be null) and synchronizes it to return *dtcurp1. */
+ * (each is written before it is read).  Every call looks the scratch up
+ * with cudaGetSymbolAddress in the current device's context (the first
+ * call on a device may load the module), so no address outlives a
+ * cudaDeviceReset.  All calls on a device share the scratch: calls that
+ * overlap in time (other threads or streams) race, so serialize them.
+ * Runs on stream (cudaStream_t, may be null) and synchronizes it to return
+ * *dtcurp1 through a copy to host memory, so no call may be made on a
+ * stream that is being captured.  FP64 state only: U and ent hold doubles,
+ * as in the plain form (not the CS_FLAG_FP32 form's device arrays). */
 int cs_cfl_timestep_noalloc(const double* U, const double* ent, const double* v_scale,
                             const int32_t* mask, int32_t ntp, int32_t nr, int32_t nghost,
                             double gamma, double rhofloor, double prsfloor, double cfl_coef,
@@ -385,6 +391,19 @@ int cs_batch_destroy(cs_batch* b);
  * kind 3, n cases of (S_R1, S_L1, S_R2, S_L2, S_R3, S_L3, Ez, Bneta_1,
  * Bneta_2, Bneta_3).  out[n] = ESSz, evaluated on the current device. */
 int cs_twod_rs_ez(int32_t kind, int32_t n, const double* in, double* out);
+
+/* Known-answer access to the pointwise physics of the stage kernels,
+ * evaluated on the current device in the state type of the form that
+ * p->flags selects (FP64, or FP32 with CS_FLAG_FP32), with the physics
+ * constants of p: for kind 0, PRIM_TO_CONS (661pde_3d_prim_to_cons.f:14):
+ * n cases of (V[8], ent) -> U[8]; for kind 1, CONS_TO_PRIM
+ * (662pde_3d_cons_to_prim.f:14): n cases of (U[8], ent) -> (V[8], ent,
+ * floor flag, U[8] after the floors); for kind 2, the HLL solve of
+ * OneD_RS_MHD_Ptwise (610_1d_rs_oned_rs_mhd_ptwise.f:100-237) in the face
+ * frame: n cases of (V_L[8], V_R[8], ent_L, ent_R) -> (Fluct_L[8],
+ * Fluct_R[8], F_L[8], F_R[8], S_L, S_R, entropy flux).  The reference's
+ * _T/_660riemann_3d/660pde_3d_test_program.f:58-142 runs kind 0 then 1. */
+int cs_pointwise(const cs_params* p, int32_t kind, int32_t n, const double* in, double* out);
 
 /* Diagnostics: sums over interior zones of 6 panels of volume-weighted
  * mass, energy and the max |div B| (face-area-weighted, per volume),

@@ -40,6 +40,11 @@ def load() -> ctypes.CDLL:
         "oracle_step": ([P, D], D),
         "oracle_twod_rs_ez_4state": ([dp], D),
         "oracle_twod_rs_ez_3state": ([dp], D),
+        "oracle_build_mesh": ([P, ctypes.c_char_p, ctypes.c_int], ctypes.c_int),
+        "oracle_init_problem": ([P, P, ctypes.c_char_p, ctypes.c_int], ctypes.c_int),
+        "oracle_get_geometry": ([P, ctypes.c_int, dp], None),
+        "oracle_get_mask_stencil": ([P, ip, ip], None),
+        "oracle_pointwise": ([P, ctypes.c_int, ctypes.c_int, dp, dp], ctypes.c_int),
     }
     for n in ("oracle_fill_ghosts", "oracle_limit_all_slopes_p12", "oracle_make_facial_fluxes",
               "oracle_make_edge_efields", "oracle_build_non_stiff_sources", "oracle_cleanup"):
@@ -64,18 +69,55 @@ def _i(a):
 
 STATE_KEYS = ("U", "ent", "bxf", "byf", "bzf")
 DEBUG_WHICH = {"V": 0, "ent_modes": 1, "flatten": 2, "dUdt": 3, "Efx": 4, "Efy": 5, "Efz": 6, "Bxq": 7,
-               "Byq": 8, "Bzq": 9, "E1": 10, "speeds": 11, "entflux": 12}
+               "Byq": 8, "Bzq": 9, "E1": 10, "speeds": 11, "entflux": 12, "positivity": 13}
 DEBUG_NCOMP = {"V": 80, "ent_modes": 4, "flatten": 1, "dUdt": 8, "Efx": 1, "Efy": 1, "Efz": 1, "Bxq": 5,
-               "Byq": 5, "Bzq": 5, "E1": 3, "speeds": 6, "entflux": 3}
+               "Byq": 5, "Bzq": 5, "E1": 3, "speeds": 6, "entflux": 3, "positivity": 1}
+
+
+class _Shape:
+    """Panel-box shapes of a parameter set (the library's layout)."""
+
+    def __init__(self, params):
+        self.params = params
+        self.N, self.nr, self.G = params.ntp, params.nr, params.nghost
+        self.NI = self.NJ = self.N + 2 * self.G + 1
+        self.NK = self.nr + 2 * self.G + 1
+
+    def shape(self, ncomp: int) -> tuple:
+        return (ncomp, 6, self.NK, self.NJ, self.NI)
+
+    def zeros(self, ncomp: int) -> np.ndarray:
+        return np.zeros(self.shape(ncomp), dtype=np.float64)
+
+    def empty_state(self) -> dict:
+        return {"U": self.zeros(8), "ent": self.zeros(1), "bxf": self.zeros(1), "byf": self.zeros(1),
+                "bzf": self.zeros(1)}
+
+    def interior(self, a: np.ndarray) -> np.ndarray:
+        G, N, nr = self.G, self.N, self.nr
+        return a[..., G + 1:G + nr + 1, G + 1:G + N + 1, G + 1:G + N + 1]
 
 
 class Oracle:
-    """CPU solve on the geometry, mask and stencil of a library Solve."""
+    """CPU solve.  Given a library Solve, it runs on that solve's geometry,
+    mask and stencil; given ``params`` (a ``cubesphere_b200.CsParams``)
+    instead, it builds its own mesh with the host mesh builder compiled into
+    ``liboracle.so`` and needs no other library (``init_problem`` then
+    writes the seeded initial state)."""
 
-    def __init__(self, solve):
+    def __init__(self, solve=None, params=None, mesh: bool = True):
         self.lib = load()
-        self.s = solve
-        self.h = self.lib.oracle_create(ctypes.byref(solve.params))
+        if solve is None and params is None:
+            raise ValueError("Oracle needs a Solve or a parameter set")
+        self.s = solve if solve is not None else _Shape(params)
+        self.h = self.lib.oracle_create(ctypes.byref(self.s.params))
+        if solve is None:
+            if not mesh:  # pointwise physics only
+                return
+            why = ctypes.create_string_buffer(256)
+            if self.lib.oracle_build_mesh(self.h, why, 256):
+                raise RuntimeError("oracle mesh build failed: " + why.value.decode())
+            return
         from cubesphere_b200 import GEOM_FIELDS
         for f, name in enumerate(GEOM_FIELDS):
             g = np.ascontiguousarray(solve.geometry(name))
@@ -83,6 +125,34 @@ class Oracle:
         m = np.ascontiguousarray(solve.mask())
         st = np.ascontiguousarray(solve.stencil())
         self.lib.oracle_set_mask_stencil(self.h, _i(m), _i(st))
+
+    def pointwise(self, kind: int, cases: np.ndarray) -> np.ndarray:
+        """The pointwise physics on rows of ``cases`` (the layouts of the
+        library's ``cs_pointwise``): kind 0 PRIM_TO_CONS, 1 CONS_TO_PRIM,
+        2 the HLL solve."""
+        nin, nout = {0: (9, 8), 1: (9, 18), 2: (18, 35)}[kind]
+        a = np.ascontiguousarray(cases, dtype=np.float64).reshape(-1, nin)
+        out = np.zeros((a.shape[0], nout))
+        assert self.lib.oracle_pointwise(self.h, kind, a.shape[0], _d(a), _d(out)) == 0
+        return out
+
+    def init_problem(self, desc) -> None:
+        """The seeded initial state of a ``cubesphere_b200.CsInitDesc``."""
+        why = ctypes.create_string_buffer(256)
+        if self.lib.oracle_init_problem(self.h, ctypes.byref(desc), why, 256):
+            raise RuntimeError("oracle initial state failed: " + why.value.decode())
+
+    def geometry(self, f: int) -> np.ndarray:
+        from cubesphere_b200 import GEOM_NCOMP
+        out = self.s.zeros(GEOM_NCOMP[f])
+        self.lib.oracle_get_geometry(self.h, f, _d(out))
+        return out
+
+    def mask_stencil(self):
+        m = np.zeros((6, self.s.NK, self.s.NJ, self.s.NI), dtype=np.int32)
+        st = np.zeros((6, 12, 2, self.s.NJ, self.s.NI), dtype=np.int32)
+        self.lib.oracle_get_mask_stencil(self.h, _i(m), _i(st))
+        return m, st
 
     def close(self):
         if self.h:

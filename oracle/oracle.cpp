@@ -19,6 +19,11 @@
 #include <vector>
 
 #include "oracle_core.h"
+// The host mesh builder and seeded initial state (a restatement of the
+// reference's mesh chain, 201-253, and of 820init_patch_cube_sphere.f, pinned
+// by the golden _T/_200mesh/test_quadpoints.out) are compiled into this
+// library from their own sources, so a CPU solve needs no other library.
+#include "cs_internal.h"
 
 namespace oracle {
 
@@ -45,6 +50,8 @@ struct Ctx {
   // state and work arrays, [comp][6][S]
   std::vector<double> U, ent, Bxf, Byf, Bzf, V, E, msonic, divvel, flat, work, Bqx, Bqy, Bqz, dUdt, SLx, SRx, SDy,
       SUy, SBz, STz, EFx, EFy, EFz, Efx, Efy, Efz, U0, ent0, Bxf0, Byf0, Bzf0;
+  // STEP 7.c record per zone: 2 x shrink passes + 1 where the zone gave up
+  std::vector<double> pos;
   // IMEX: the first stage's dU/dt, entropy fluxes and EMFs
   std::vector<double> K1, EFx1, EFy1, EFz1, Efx1, Efy1, Efz1;
   double time = 0.0;
@@ -68,6 +75,12 @@ struct Ctx {
     return st[(((size_t)pn * 12 + w) * 2 + c) * ((size_t)NI * NJ) + (size_t)(j + G) * NI + (i + G)];
   }
 };
+
+// Zone loops run on all host threads.  Every loop marked OMP_ZONES writes
+// only the zone, face or edge of its own iteration and reads values that
+// no iteration of the same loop writes, so its results do not depend on
+// the thread count or schedule (bit-identical to a serial run).
+#define OMP_ZONES _Pragma("omp parallel for collapse(2) schedule(static)")
 
 static inline double sq(double x) { return x * x; }
 static inline double pow4(double x) {
@@ -108,12 +121,14 @@ void fill_ghosts(Ctx& c) {
     const int rt = kNbr[pn][0] - 1, lf = kNbr[pn][1] - 1, up = kNbr[pn][2] - 1, dn = kNbr[pn][3] - 1;
     auto inner = [&](int j, int k) { return j >= 1 && j <= N && k >= 1 && k <= nr; };
     // ---- x direction: right strip
+    OMP_ZONES
     for (int k = 1 - G; k <= nr + G; ++k)
       for (int j = 1 - G; j <= N + G; ++j)
         for (int i = N + 1; i <= N + G; ++i) {
           for (int q = 0; q < NV; ++q) c.a(c.U, q, pn, i, j, k) = src(U, q, rt, j, 2 * N + 1 - i, k);
           c.a(c.ent, 0, pn, i, j, k) = src(ent, 0, rt, j, 2 * N + 1 - i, k);
         }
+    OMP_ZONES
     for (int k = 1 - G; k <= nr + G; ++k)
       for (int j = 1 - G; j <= N + G; ++j)
         for (int i = N; i <= N + G; ++i) {
@@ -122,19 +137,23 @@ void fill_ghosts(Ctx& c) {
           double& d = c.a(c.Bxf, 0, pn, i, j, k);
           d = (i == N && inner(j, k)) ? (d + v) * 0.5 : v;
         }
+    OMP_ZONES
     for (int k = 1 - G; k <= nr + G; ++k)
       for (int j = -G; j <= N + G; ++j)
         for (int i = N + 1; i <= N + G; ++i) c.a(c.Byf, 0, pn, i, j, k) = src(Bx, 0, rt, j, 2 * N + 1 - i, k);
+    OMP_ZONES
     for (int k = -G; k <= nr + G; ++k)
       for (int j = 1 - G; j <= N + G; ++j)
         for (int i = N + 1; i <= N + G; ++i) c.a(c.Bzf, 0, pn, i, j, k) = src(Bz, 0, rt, j, 2 * N + 1 - i, k);
     // ---- x direction: left strip
+    OMP_ZONES
     for (int k = 1 - G; k <= nr + G; ++k)
       for (int j = 1 - G; j <= N + G; ++j)
         for (int i = 1 - G; i <= 0; ++i) {
           for (int q = 0; q < NV; ++q) c.a(c.U, q, pn, i, j, k) = src(U, q, lf, 1 - i, N + 1 - j, k);
           c.a(c.ent, 0, pn, i, j, k) = src(ent, 0, lf, 1 - i, N + 1 - j, k);
         }
+    OMP_ZONES
     for (int k = 1 - G; k <= nr + G; ++k)
       for (int j = 1 - G; j <= N + G; ++j)
         for (int i = -G; i <= 0; ++i) {
@@ -143,9 +162,11 @@ void fill_ghosts(Ctx& c) {
           double& d = c.a(c.Bxf, 0, pn, i, j, k);
           d = (i == 0 && inner(j, k)) ? (d + v) * 0.5 : v;
         }
+    OMP_ZONES
     for (int k = 1 - G; k <= nr + G; ++k)
       for (int j = -G; j <= N + G; ++j)
         for (int i = 1 - G; i <= 0; ++i) c.a(c.Byf, 0, pn, i, j, k) = -src(By, 0, lf, 1 - i, N - j, k);
+    OMP_ZONES
     for (int k = -G; k <= nr + G; ++k)
       for (int j = 1 - G; j <= N + G; ++j)
         for (int i = 1 - G; i <= 0; ++i) c.a(c.Bzf, 0, pn, i, j, k) = src(Bz, 0, lf, 1 - i, N + 1 - j, k);
@@ -154,12 +175,14 @@ void fill_ghosts(Ctx& c) {
     const int up = kNbr[pn][2] - 1, dn = kNbr[pn][3] - 1;
     auto inner = [&](int i, int k) { return i >= 1 && i <= N && k >= 1 && k <= nr; };
     // ---- y direction: down strip
+    OMP_ZONES
     for (int k = 1 - G; k <= nr + G; ++k)
       for (int j = 1 - G; j <= 0; ++j)
         for (int i = 1 - G; i <= N + G; ++i) {
           for (int q = 0; q < NV; ++q) c.a(c.U, q, pn, i, j, k) = src(U, q, dn, N + 1 - i, 1 - j, k);
           c.a(c.ent, 0, pn, i, j, k) = src(ent, 0, dn, N + 1 - i, 1 - j, k);
         }
+    OMP_ZONES
     for (int k = 1 - G; k <= nr + G; ++k)
       for (int j = -G; j <= 0; ++j)
         for (int i = 1 - G; i <= N + G; ++i) {
@@ -168,19 +191,23 @@ void fill_ghosts(Ctx& c) {
           double& d = c.a(c.Byf, 0, pn, i, j, k);
           d = (j == 0 && inner(i, k)) ? (d + v) * 0.5 : v;
         }
+    OMP_ZONES
     for (int k = 1 - G; k <= nr + G; ++k)
       for (int j = 1 - G; j <= 0; ++j)
         for (int i = -G; i <= N + G; ++i) c.a(c.Bxf, 0, pn, i, j, k) = -src(Bx, 0, dn, N - i, 1 - j, k);
+    OMP_ZONES
     for (int k = -G; k <= nr + G; ++k)
       for (int j = 1 - G; j <= 0; ++j)
         for (int i = 1 - G; i <= N + G; ++i) c.a(c.Bzf, 0, pn, i, j, k) = src(Bz, 0, dn, N + 1 - i, 1 - j, k);
     // ---- y direction: up strip
+    OMP_ZONES
     for (int k = 1 - G; k <= nr + G; ++k)
       for (int j = N + 1; j <= N + G; ++j)
         for (int i = 1 - G; i <= N + G; ++i) {
           for (int q = 0; q < NV; ++q) c.a(c.U, q, pn, i, j, k) = src(U, q, up, 2 * N + 1 - j, i, k);
           c.a(c.ent, 0, pn, i, j, k) = src(ent, 0, up, 2 * N + 1 - j, i, k);
         }
+    OMP_ZONES
     for (int k = 1 - G; k <= nr + G; ++k)
       for (int j = N; j <= N + G; ++j)
         for (int i = 1 - G; i <= N + G; ++i) {
@@ -189,9 +216,11 @@ void fill_ghosts(Ctx& c) {
           double& d = c.a(c.Byf, 0, pn, i, j, k);
           d = (j == N && inner(i, k)) ? (d + v) * 0.5 : v;
         }
+    OMP_ZONES
     for (int k = 1 - G; k <= nr + G; ++k)
       for (int j = N + 1; j <= N + G; ++j)
         for (int i = -G; i <= N + G; ++i) c.a(c.Bxf, 0, pn, i, j, k) = src(By, 0, up, 2 * N + 1 - j, i, k);
+    OMP_ZONES
     for (int k = -G; k <= nr + G; ++k)
       for (int j = N + 1; j <= N + G; ++j)
         for (int i = 1 - G; i <= N + G; ++i) c.a(c.Bzf, 0, pn, i, j, k) = src(Bz, 0, up, 2 * N + 1 - j, i, k);
@@ -276,16 +305,19 @@ static void tricorner_sync(Ctx& c, int pn) {
 
 static void zero_masked_faces(Ctx& c, int pn) {
   const int N = c.N, G = c.G, nr = c.nr;
+  OMP_ZONES
   for (int k = 1 - G; k <= nr + G; ++k)
     for (int j = 1 - G; j <= N + G; ++j)
       for (int i = -G; i <= N + G; ++i)
         if (c.m(pn, std::max(i, 1 - G), j) == 0 && c.m(pn, std::min(i + 1, N + G), j) == 0)
           c.a(c.Bxf, 0, pn, i, j, k) = 0.0;
+  OMP_ZONES
   for (int k = 1 - G; k <= nr + G; ++k)
     for (int j = -G; j <= N + G; ++j)
       for (int i = 1 - G; i <= N + G; ++i)
         if (c.m(pn, i, std::max(j, 1 - G)) == 0 && c.m(pn, i, std::min(j + 1, N + G)) == 0)
           c.a(c.Byf, 0, pn, i, j, k) = 0.0;
+  OMP_ZONES
   for (int k = -G; k <= nr + G; ++k)
     for (int j = 1 - G; j <= N + G; ++j)
       for (int i = 1 - G; i <= N + G; ++i)
@@ -427,6 +459,7 @@ void limit_all_slopes_p12(Ctx& c, int pn) {
   auto V = [&](int comp, int mode, int i, int j, int k) -> double& { return c.a(c.V, mode * NV + comp, pn, i, j, k); };
   auto E = [&](int comp, int mode, int i, int j, int k) -> double& { return c.a(c.E, mode * 3 + comp, pn, i, j, k); };
   // STEP 2 (:597-759)
+  OMP_ZONES
   for (int k = 1 - G; k <= nr + G; ++k)
     for (int j = 1 - G; j <= N + G; ++j)
       for (int i = 1 - G; i <= N + G; ++i) {
@@ -444,6 +477,7 @@ void limit_all_slopes_p12(Ctx& c, int pn) {
   // STEP 3 (:779-962)
   tricorner_sync(c, pn);
   // STEP 5 (:1497-1628)
+  OMP_ZONES
   for (int k = 1 - G; k <= nr + G; ++k)
     for (int j = 1 - G; j <= N + G; ++j)
       for (int i = 1 - G; i <= N + G; ++i) {
@@ -462,9 +496,11 @@ void limit_all_slopes_p12(Ctx& c, int pn) {
         c.a(c.msonic, 0, pn, i, j, k) = std::sqrt(ms / V(0, 0, i, j, k));
       }
   // STEP 6 flattener (:1797-2458)
+  OMP_ZONES
   for (int k = 1 - G; k <= nr + G; ++k)
     for (int j = 1 - G; j <= N + G; ++j)
       for (int i = 1 - G; i <= N + G; ++i) c.a(c.flat, 0, pn, i, j, k) = 0.0;
+  OMP_ZONES
   for (int k = 2 - G; k <= nr + G - 1; ++k)
     for (int j = 2 - G; j <= N + G - 1; ++j)
       for (int i = 2 - G; i <= N + G - 1; ++i) {
@@ -508,9 +544,11 @@ void limit_all_slopes_p12(Ctx& c, int pn) {
       }
   for (int pass = 0; pass < 2; ++pass) {
     // pass 0: STEP 6.b (pressure-ratio raise), pass 1: STEP 6.c (upwinding)
+    OMP_ZONES
     for (int k = 1 - G; k <= nr + G; ++k)
       for (int j = 1 - G; j <= N + G; ++j)
         for (int i = 1 - G; i <= N + G; ++i) c.a(c.work, 0, pn, i, j, k) = c.a(c.flat, 0, pn, i, j, k);
+    OMP_ZONES
     for (int k = 2 - G; k <= nr + G - 1; ++k)
       for (int j = 2 - G; j <= N + G - 1; ++j)
         for (int i = 2 - G; i <= N + G - 1; ++i) {
@@ -525,6 +563,7 @@ void limit_all_slopes_p12(Ctx& c, int pn) {
         }
   }
   // STEP 7.a (:2515-3804)
+  OMP_ZONES
   for (int k = 2 - G; k <= nr + G - 1; ++k)
     for (int j = 2 - G; j <= N + G - 1; ++j)
       for (int i = 2 - G; i <= N + G - 1; ++i) {
@@ -545,6 +584,7 @@ void limit_all_slopes_p12(Ctx& c, int pn) {
         for (int r = 0; r < 3; ++r) c.a(c.ent, 1 + r, pn, i, j, k) = gr[r] * om;
       }
   // STEP 7.b (:3869-4551)
+  OMP_ZONES
   for (int k = 3 - G; k <= nr + G - 2; ++k)
     for (int j = 3 - G; j <= N + G - 2; ++j)
       for (int i = 3 - G; i <= N + G - 2; ++i) {
@@ -623,8 +663,10 @@ void limit_all_slopes_p12(Ctx& c, int pn) {
   // zeroes its own entropy, 440:569-575), so the result is order-free.
   {
     const std::vector<double> ent_snap(c.ent.begin() + (size_t)pn * c.S, c.ent.begin() + (size_t)(pn + 1) * c.S);
+    std::fill(c.pos.begin() + (size_t)pn * c.S, c.pos.begin() + (size_t)(pn + 1) * c.S, 0.0);
     const int niter = 15;
     const double ratio = std::pow(0.10, 1.0 / (double)niter), ef = 0.2;
+    OMP_ZONES
     for (int k = 2 - G; k <= nr + G - 1; ++k)
       for (int j = 2 - G; j <= N + G - 1; ++j)
         for (int i = 2 - G; i <= N + G - 1; ++i) {
@@ -697,11 +739,13 @@ void limit_all_slopes_p12(Ctx& c, int pn) {
           double xyz[27][3];
           for (int nd = 0; nd < 27; ++nd)
             for (int q = 0; q < 3; ++q) xyz[nd][q] = (vert[nd][q] - vc[q]) * obl0;
+          int shrinks = 0, gave_up = 0;
           for (int iter = 1; iter <= niter + 1; ++iter) {
             if (iter == niter + 1) {
               for (int q = 0; q < NV; ++q)
                 for (int t = 1; t < 10; ++t) Vp[q][t] = 0.0;
               for (int t = 0; t < 4; ++t) ep[t] = 0.0;
+              gave_up = 1;
               break;
             }
             bool pass = true;
@@ -717,7 +761,9 @@ void limit_all_slopes_p12(Ctx& c, int pn) {
             for (int q = 0; q < NV; ++q)
               for (int t = 1; t < 10; ++t) Vp[q][t] = ratio * Vp[q][t];
             for (int t = 1; t < 4; ++t) ep[t] = ratio * ep[t];
+            ++shrinks;
           }
+          c.a(c.pos, 0, pn, i, j, k) = gave_up + 2 * shrinks;
           for (int q = 0; q < NV; ++q)
             for (int t = 0; t < 10; ++t) V(q, t, i, j, k) = Vp[q][t];
           for (int t = 0; t < 4; ++t) c.a(c.ent, t, pn, i, j, k) = ep[t];
@@ -732,6 +778,7 @@ void limit_all_slopes_p12(Ctx& c, int pn) {
     const int BW = dir == 0 ? XB_QW : (dir == 1 ? YB_QW : ZB_QW);
     int lo[3] = {2 - G, 2 - G, 2 - G}, hi[3] = {N + G - 1, N + G - 1, nr + G - 1};
     lo[dir] = 1 - G;
+    OMP_ZONES
     for (int k = lo[2]; k <= hi[2]; ++k)
       for (int j = lo[1]; j <= hi[1]; ++j)
         for (int i = lo[0]; i <= hi[0]; ++i) {
@@ -786,6 +833,7 @@ void limit_all_slopes_p12(Ctx& c, int pn) {
             c.a(Bq, q, pn, i, j, k) = 0.5 * (nx * (bx + bx2) + ny * (by + by2) + nz * (bz + bz2));
           }
         }
+    OMP_ZONES
     for (int k = lo[2]; k <= hi[2]; ++k)
       for (int j = lo[1]; j <= hi[1]; ++j)
         for (int i = lo[0]; i <= hi[0]; ++i) {
@@ -795,6 +843,7 @@ void limit_all_slopes_p12(Ctx& c, int pn) {
         }
   }
   // STEP 8.d ADP constrained least squares (:5617-6677)
+  OMP_ZONES
   for (int k = 2 - G; k <= nr + G - 1; ++k)
     for (int j = 2 - G; j <= N + G - 1; ++j)
       for (int i = 2 - G; i <= N + G - 1; ++i) {
@@ -869,6 +918,7 @@ void limit_all_slopes_p12(Ctx& c, int pn) {
         c.a(c.U, 4, pn, i, j, k) = c.a(c.U, 4, pn, i, j, k) - aa + bb;
       }
   // STEP 9.a zone-centred E = -v x B at the centroid (:6700-6790)
+  OMP_ZONES
   for (int k = 1 - G; k <= nr + G; ++k)
     for (int j = 1 - G; j <= N + G; ++j)
       for (int i = 1 - G; i <= N + G; ++i) {
@@ -886,6 +936,7 @@ void limit_all_slopes_p12(Ctx& c, int pn) {
         E(2, 0, i, j, k) = -(vx * By - vy * Bx);
       }
   // STEP 9.b WENO gradients of E (:6840-8400)
+  OMP_ZONES
   for (int k = 2 - G; k <= nr + G - 1; ++k)
     for (int j = 2 - G; j <= N + G - 1; ++j)
       for (int i = 2 - G; i <= N + G - 1; ++i) {
@@ -908,6 +959,7 @@ void limit_all_slopes_p12(Ctx& c, int pn) {
   for (int q = 0; q < 3; ++q)
     std::memcpy(&esnap[(size_t)q * c.S], &c.E[((size_t)q * 6 + pn) * c.S], c.S * sizeof(double));
   auto E1s = [&](int q, int x, int y, int z) { return esnap[(size_t)q * c.S + c.idx(x, y, z)]; };
+  OMP_ZONES
   for (int k = 3 - G; k <= nr + G - 2; ++k)
     for (int j = 3 - G; j <= N + G - 2; ++j)
       for (int i = 3 - G; i <= N + G - 2; ++i) {
@@ -988,12 +1040,14 @@ void make_facial_fluxes(Ctx& c, int pn) {
   const double sm = c.p.smallnum;
   auto V = [&](int comp, int mode, int i, int j, int k) -> double& { return c.a(c.V, mode * NV + comp, pn, i, j, k); };
   for (int dir = 0; dir < 3; ++dir) {
+#pragma omp parallel for collapse(2) schedule(static)
     for (int t = 0; t < 5 * NV; ++t)
-      for (size_t o = 0; o < c.S; ++o) {
+      for (long long o = 0; o < (long long)c.S; ++o) {
         c.cL[dir][((size_t)t * 6 + pn) * c.S + o] = 0.0;
         c.cR[dir][((size_t)t * 6 + pn) * c.S + o] = 0.0;
       }
-    for (size_t o = 0; o < c.S; ++o) {
+#pragma omp parallel for schedule(static)
+    for (long long o = 0; o < (long long)c.S; ++o) {
       c.tL[dir][(size_t)pn * c.S + o] = -1;
       c.tR[dir][(size_t)pn * c.S + o] = -1;
     }
@@ -1007,7 +1061,8 @@ void make_facial_fluxes(Ctx& c, int pn) {
     std::vector<double>& EF = dir == 0 ? c.EFx : (dir == 1 ? c.EFy : c.EFz);
     int lo[3] = {0, 0, 0}, hi[3] = {N + 1, N + 1, nr + 1};
     lo[dir] = -1;
-    for (int jq = 0; jq < 5; ++jq)
+    for (int jq = 0; jq < 5; ++jq) {
+      OMP_ZONES
       for (int k = lo[2]; k <= hi[2]; ++k)
         for (int j = lo[1]; j <= hi[1]; ++j)
           for (int i = lo[0]; i <= hi[0]; ++i) {
@@ -1122,38 +1177,64 @@ void make_facial_fluxes(Ctx& c, int pn) {
             c.tR[dir][(size_t)pn * c.S + fo] = (long long)c.idx(rx, ry, rz);
             if (jq == 0) c.a(EF, 0, pn, i, j, k) = o.entF;
           }
+    }
   }
 }
 
 // Second half of MAKE_FACIAL_FLUXES: every face's per-point contributions
 // are subtracted from the time derivatives of the zones it updates, in the
-// reference's order (direction, quadrature point, face).
+// reference's order (direction, quadrature point, face).  The x and y faces
+// of plane k update zones of plane k only, so whole planes go to one thread
+// each and every zone still receives its terms in that order; a z face k
+// updates zones k (its lower side) and k + 1 (its upper side), so each zone
+// collects the upper-side term of face k - 1 and then the lower-side term of
+// face k, point by point, as the face loop would apply them.
 void scatter_facial_fluxes(Ctx& c, int pn) {
   const int N = c.N, G = c.G, nr = c.nr;
+  OMP_ZONES
   for (int k = 1 - G; k <= nr + G; ++k)
     for (int j = 1 - G; j <= N + G; ++j)
       for (int i = 1 - G; i <= N + G; ++i)
         for (int q = 0; q < NV; ++q) c.a(c.dUdt, q, pn, i, j, k) = 0.0;
-  for (int dir = 0; dir < 3; ++dir) {
+  auto sub = [&](int dir, int jq, size_t fo, long long z, const std::vector<double>& cc) {
+    for (int q = 0; q < NV; ++q) {
+      double& d = c.dUdt[((size_t)q * 6 + pn) * c.S + (size_t)z];
+      d = d - cc[((size_t)(jq * NV + q) * 6 + pn) * c.S + fo];
+    }
+  };
+  for (int dir = 0; dir < 2; ++dir) {
     int lo[3] = {0, 0, 0}, hi[3] = {N + 1, N + 1, nr + 1};
     lo[dir] = -1;
-    for (int jq = 0; jq < 5; ++jq)
-      for (int k = lo[2]; k <= hi[2]; ++k)
+#pragma omp parallel for schedule(static)
+    for (int k = lo[2]; k <= hi[2]; ++k)
+      for (int jq = 0; jq < 5; ++jq)
         for (int j = lo[1]; j <= hi[1]; ++j)
           for (int i = lo[0]; i <= hi[0]; ++i) {
             const size_t fo = c.idx(i, j, k);
             const long long l = c.tL[dir][(size_t)pn * c.S + fo], r = c.tR[dir][(size_t)pn * c.S + fo];
             if (l < 0) continue;
-            for (int q = 0; q < NV; ++q) {
-              double& dl = c.dUdt[((size_t)q * 6 + pn) * c.S + (size_t)l];
-              dl = dl - c.cL[dir][((size_t)(jq * NV + q) * 6 + pn) * c.S + fo];
-            }
-            for (int q = 0; q < NV; ++q) {
-              double& dr = c.dUdt[((size_t)q * 6 + pn) * c.S + (size_t)r];
-              dr = dr - c.cR[dir][((size_t)(jq * NV + q) * 6 + pn) * c.S + fo];
-            }
+            sub(dir, jq, fo, l, c.cL[dir]);
+            sub(dir, jq, fo, r, c.cR[dir]);
           }
   }
+  // z faces k in [-1, nr + 1] over (i, j) in [0, N + 1]^2: lower side zone
+  // (i, j, k), upper side (i, j, k + 1)
+  OMP_ZONES
+  for (int kz = -1; kz <= nr + 2; ++kz)
+    for (int j = 0; j <= N + 1; ++j)
+      for (int i = 0; i <= N + 1; ++i) {
+        const long long z = (long long)c.idx(i, j, kz);
+        const bool below = kz - 1 >= -1, above = kz <= nr + 1;
+        const size_t fb = below ? c.idx(i, j, kz - 1) : 0, fa = above ? c.idx(i, j, kz) : 0;
+        const bool ub = below && c.tL[2][(size_t)pn * c.S + fb] >= 0;
+        const bool ua = above && c.tL[2][(size_t)pn * c.S + fa] >= 0;
+        if (ub && c.tR[2][(size_t)pn * c.S + fb] != z) std::abort();
+        if (ua && c.tL[2][(size_t)pn * c.S + fa] != z) std::abort();
+        for (int jq = 0; jq < 5; ++jq) {
+          if (ub) sub(2, jq, fb, z, c.cR[2]);
+          if (ua) sub(2, jq, fa, z, c.cL[2]);
+        }
+      }
 }
 
 // ------------------------------------------------------------------
@@ -1305,6 +1386,7 @@ void make_edge_efields(Ctx& c, int pn) {
   auto vt = [&](int q, int x, int y, int z) { return c.geo(G_VERT, q, pn, x, y, z); };
   auto Bq = [&](std::vector<double>& B, int q, int x, int y, int z) { return c.a(B, q, pn, x, y, z); };
   auto S = [&](std::vector<double>& s, int x, int y, int z) { return c.a(s, 0, pn, x, y, z); };
+  OMP_ZONES
   for (int k = 1 - G; k <= nr + G; ++k)
     for (int j = 1 - G; j <= N + G; ++j)
       for (int i = 1 - G; i <= N + G; ++i) {
@@ -1347,6 +1429,7 @@ void make_edge_efields(Ctx& c, int pn) {
   for (int jq = 0; jq < 3; ++jq) {
     double wt = (jq == 0) ? 4.0 / 6.0 : 1.0 / 6.0;
     // x-edges (:393-1493): zones LD (i,j,k), RD (i,j+1,k), RU (i,j+1,k+1), LU (i,j,k+1)
+    OMP_ZONES
     for (int k = 0; k <= nr; ++k)
       for (int j = 0; j <= N; ++j)
         for (int i = 1; i <= N; ++i) {
@@ -1370,6 +1453,7 @@ void make_edge_efields(Ctx& c, int pn) {
           c.a(c.Efx, 0, pn, i, j, k) = c.a(c.Efx, 0, pn, i, j, k) + wt * ess;
         }
     // y-edges (:1497-2587): LD (i,j,k), RD (i,j,k+1), LU (i+1,j,k), RU (i+1,j,k+1)
+    OMP_ZONES
     for (int k = 0; k <= nr; ++k)
       for (int i = 0; i <= N; ++i)
         for (int j = 1; j <= N; ++j) {
@@ -1393,6 +1477,7 @@ void make_edge_efields(Ctx& c, int pn) {
           c.a(c.Efy, 0, pn, i, j, k) = c.a(c.Efy, 0, pn, i, j, k) + wt * ess;
         }
     // z-edges (:2591-3721): LD (i,j,k), RD (i+1,j,k), RU (i+1,j+1,k), LU (i,j+1,k)
+    OMP_ZONES
     for (int i = 0; i <= N; ++i)
       for (int j = 0; j <= N; ++j)
         for (int k = 1; k <= nr; ++k) {
@@ -1473,6 +1558,7 @@ void build_non_stiff_sources(Ctx& c, int pn) {
   if (!(c.p.gm > c.p.smallnum)) return;
   const int N = c.N, nr = c.nr;
   auto V = [&](int comp, int i, int j, int k) -> double& { return c.a(c.V, comp, pn, i, j, k); };
+  OMP_ZONES
   for (int k = 0; k <= nr + 1; ++k)
     for (int j = 0; j <= N + 1; ++j)
       for (int i = 0; i <= N + 1; ++i) {
@@ -1494,11 +1580,13 @@ void build_non_stiff_sources(Ctx& c, int pn) {
 // UPDATE_IMEX_RK_STEP_P1 for ideal MHD (400riemann_integrate/484update_imex_rk_step_p1.f:212-906).
 void update(Ctx& c, int pn, double dt) {
   const int N = c.N, G = c.G, nr = c.nr;
+  OMP_ZONES
   for (int k = 1 - G; k <= nr + G; ++k)
     for (int j = 1 - G; j <= N + G; ++j)
       for (int i = 1 - G; i <= N + G; ++i)
         for (int q = 0; q < NV; ++q)
           c.a(c.U, q, pn, i, j, k) = c.a(c.U, q, pn, i, j, k) + dt * c.a(c.dUdt, q, pn, i, j, k);
+  OMP_ZONES
   for (int k = 1; k <= nr; ++k)
     for (int j = 1; j <= N; ++j)
       for (int i = 1; i <= N; ++i) {
@@ -1521,6 +1609,7 @@ void update(Ctx& c, int pn, double dt) {
                (vt(2, ax, ay, z) * inv) * (vt(2, bx, by, z) * inv);
     return std::acos(d);
   };
+  OMP_ZONES
   for (int k = 1; k <= nr; ++k)
     for (int j = 1; j <= N; ++j)
       for (int i = 0; i <= N; ++i) {
@@ -1531,6 +1620,7 @@ void update(Ctx& c, int pn, double dt) {
                    lin * c.a(c.Efy, 0, pn, i, j, k - 1);
         c.a(c.Bxf, 0, pn, i, j, k) = c.a(c.Bxf, 0, pn, i, j, k) - dt * s / c.geo(XF_AREA, 0, pn, i, j, k);
       }
+  OMP_ZONES
   for (int k = 1; k <= nr; ++k)
     for (int j = 0; j <= N; ++j)
       for (int i = 1; i <= N; ++i) {
@@ -1541,6 +1631,7 @@ void update(Ctx& c, int pn, double dt) {
                    lin * c.a(c.Efx, 0, pn, i, j, k - 1);
         c.a(c.Byf, 0, pn, i, j, k) = c.a(c.Byf, 0, pn, i, j, k) - dt * s / c.geo(YF_AREA, 0, pn, i, j, k);
       }
+  OMP_ZONES
   for (int k = 0; k <= nr; ++k)
     for (int j = 1; j <= N; ++j)
       for (int i = 1; i <= N; ++i) {
@@ -1561,6 +1652,7 @@ void cleanup(Ctx& c, int pn) {
   const double sm = c.p.smallnum;
   zero_masked_faces(c, pn);
   tricorner_sync(c, pn);
+  OMP_ZONES
   for (int k = 1 - G; k <= nr + G; ++k)
     for (int j = 1 - G; j <= N + G; ++j)
       for (int i = 1 - G; i <= N + G; ++i) {
@@ -1604,6 +1696,7 @@ void cleanup(Ctx& c, int pn) {
         c.a(c.U, 4, pn, i, j, k) = c.a(c.U, 4, pn, i, j, k) - (Bx * Bx + By * By + Bz * Bz) * c.ph.ob8pi +
                                    (nb[0] * nb[0] + nb[1] * nb[1] + nb[2] * nb[2]) * c.ph.ob8pi;
       }
+  OMP_ZONES
   for (int k = 1 - G; k <= nr + G; ++k)
     for (int j = 1 - G; j <= N + G; ++j)
       for (int i = 1 - G; i <= N + G; ++i) {
@@ -1623,6 +1716,7 @@ void cleanup(Ctx& c, int pn) {
 double evaluate_timestep(Ctx& c, double dtcur) {
   double dt = 1.1 * dtcur;
   const int N = c.N, nr = c.nr;
+#pragma omp parallel for collapse(3) schedule(static) reduction(min : dt)
   for (int pn = 0; pn < 6; ++pn)
     for (int k = 1; k <= nr; ++k)
       for (int j = 1; j <= N; ++j)
@@ -1651,6 +1745,7 @@ double evaluate_timestep(Ctx& c, double dtcur) {
 static void gravity_implicit(Ctx& c, int pn, double a) {
   if (!(c.p.gm > c.p.smallnum)) return;
   const int N = c.N, nr = c.nr;
+  OMP_ZONES
   for (int k = 0; k <= nr + 1; ++k)
     for (int j = 0; j <= N + 1; ++j)
       for (int i = 0; i <= N + 1; ++i) {
@@ -1674,6 +1769,7 @@ static void gravity_implicit(Ctx& c, int pn, double a) {
 static void add_gravity(Ctx& c, int pn, double cc) {
   if (!(c.p.gm > c.p.smallnum)) return;
   const int N = c.N, nr = c.nr;
+  OMP_ZONES
   for (int k = 0; k <= nr + 1; ++k)
     for (int j = 0; j <= N + 1; ++j)
       for (int i = 0; i <= N + 1; ++i) {
@@ -1699,13 +1795,11 @@ static void add_gravity(Ctx& c, int pn, double cc) {
 static void stage_imex(Ctx& c, int irk, double dtcur) {
   const double gam = 1.0 - 1.0 / std::sqrt(2.0), del = 1.0 - 1.0 / (2.0 * gam);
   fill_ghosts(c);
-#pragma omp parallel for schedule(static, 1)
   for (int pn = 0; pn < 6; ++pn) {
     limit_all_slopes_p12(c, pn);
     make_facial_fluxes(c, pn);
   }
   sync_facial_fluxes(c);
-#pragma omp parallel for schedule(static, 1)
   for (int pn = 0; pn < 6; ++pn) {
     scatter_facial_fluxes(c, pn);
     make_edge_efields(c, pn);
@@ -1720,10 +1814,8 @@ static void stage_imex(Ctx& c, int irk, double dtcur) {
     c.K1 = c.dUdt;
     c.EFx1 = c.EFx; c.EFy1 = c.EFy; c.EFz1 = c.EFz;
     c.Efx1 = c.Efx; c.Efy1 = c.Efy; c.Efz1 = c.Efz;
-#pragma omp parallel for schedule(static, 1)
     for (int pn = 0; pn < 6; ++pn) update(c, pn, gam * dtcur);
   } else {
-#pragma omp parallel for schedule(static, 1)
     for (int pn = 0; pn < 6; ++pn) add_gravity(c, pn, (1.0 - gam) / (1.0 - del));
     c.U = c.U0;
     std::memcpy(c.ent.data(), c.ent0.data(), 6 * c.S * sizeof(double));
@@ -1736,13 +1828,10 @@ static void stage_imex(Ctx& c, int irk, double dtcur) {
       std::swap(c.Efx, c.Efx1); std::swap(c.Efy, c.Efy1); std::swap(c.Efz, c.Efz1);
     };
     swap1();
-#pragma omp parallel for schedule(static, 1)
     for (int pn = 0; pn < 6; ++pn) update(c, pn, del * dtcur);
     swap1();
-#pragma omp parallel for schedule(static, 1)
     for (int pn = 0; pn < 6; ++pn) update(c, pn, (1.0 - del) * dtcur);
   }
-#pragma omp parallel for schedule(static, 1)
   for (int pn = 0; pn < 6; ++pn) {
     gravity_implicit(c, pn, gam * dtcur);
     cleanup(c, pn);
@@ -1769,20 +1858,18 @@ void stage(Ctx& c, int irk, double dtcur) {
     if (irk == 3) { a0 = 1.0 / 3.0; dtmove = (2.0 / 3.0) * dtcur; }
   }
   // Panels are independent within a stage (each reads only its own,
-  // ghost-filled arrays), so they run on separate host threads.
-#pragma omp parallel for schedule(static, 1)
+  // ghost-filled arrays); the zone loops inside every routine run on all
+  // host threads.
   for (int pn = 0; pn < 6; ++pn) {
     limit_all_slopes_p12(c, pn);
     make_facial_fluxes(c, pn);
   }
   sync_facial_fluxes(c);
-#pragma omp parallel for schedule(static, 1)
   for (int pn = 0; pn < 6; ++pn) {
     scatter_facial_fluxes(c, pn);
     make_edge_efields(c, pn);
   }
   sync_edge_efields(c);
-#pragma omp parallel for schedule(static, 1)
   for (int pn = 0; pn < 6; ++pn) {
     build_non_stiff_sources(c, pn);
     const size_t S = c.S;
@@ -1841,7 +1928,7 @@ void* oracle_create(const void* params) {
   al(c->msonic, 1); al(c->divvel, 1); al(c->flat, 1); al(c->work, 1); al(c->Bqx, 5); al(c->Bqy, 5); al(c->Bqz, 5);
   al(c->dUdt, 8); al(c->SLx, 1); al(c->SRx, 1); al(c->SDy, 1); al(c->SUy, 1); al(c->SBz, 1); al(c->STz, 1);
   al(c->EFx, 1); al(c->EFy, 1); al(c->EFz, 1); al(c->Efx, 1); al(c->Efy, 1); al(c->Efz, 1);
-  al(c->U0, 8); al(c->ent0, 1); al(c->Bxf0, 1); al(c->Byf0, 1); al(c->Bzf0, 1);
+  al(c->U0, 8); al(c->ent0, 1); al(c->Bxf0, 1); al(c->Byf0, 1); al(c->Bzf0, 1); al(c->pos, 1);
   if (c->p.rk_scheme == 4) {
     al(c->K1, 8); al(c->EFx1, 1); al(c->EFy1, 1); al(c->EFz1, 1); al(c->Efx1, 1); al(c->Efy1, 1); al(c->Efz1, 1);
   }
@@ -1855,6 +1942,64 @@ void* oracle_create(const void* params) {
 }
 
 void oracle_destroy(void* h) { delete (Ctx*)h; }
+
+// The solve's own mesh: geometry, mask and stencil from the host mesh
+// builder for the parameters given at creation.  Returns 0, or 1 with the
+// reason in why (a buffer of nwhy bytes).
+int oracle_build_mesh(void* h, char* why, int nwhy) {
+  Ctx* c = (Ctx*)h;
+  static_assert(sizeof(Params) == sizeof(cs_params), "oracle Params mirrors cs_params");
+  cs_params cp;
+  std::memcpy(&cp, &c->p, sizeof(cp));
+  cs::GeomHost gh;
+  const std::string e = cs::build_geometry(cp, gh);
+  if (!e.empty()) {
+    if (why && nwhy > 0) std::snprintf(why, (size_t)nwhy, "%s", e.c_str());
+    return 1;
+  }
+  for (int f = 0; f < NGF; ++f) c->g[f] = std::move(gh.f[f]);
+  c->mask = std::move(gh.mask);
+  c->st = std::move(gh.stencil);
+  c->maps_built = false;
+  return 0;
+}
+
+// The seeded initial state (cs_init_desc) written into the solve's state on
+// its own mesh (oracle_build_mesh first).  Returns 0, or 1 with the reason.
+int oracle_init_problem(void* h, const void* desc, char* why, int nwhy) {
+  Ctx* c = (Ctx*)h;
+  cs_params cp;
+  std::memcpy(&cp, &c->p, sizeof(cp));
+  cs_init_desc d;
+  std::memcpy(&d, desc, sizeof(d));
+  cs::GeomHost gh;  // borrows the solve's geometry for the call
+  gh.box = cs::Box(c->N, c->nr, c->G);
+  for (int f = 0; f < NGF; ++f) gh.f[f] = std::move(c->g[f]);
+  gh.mask = std::move(c->mask);
+  gh.stencil = std::move(c->st);
+  const std::string e = cs::init_problem_host(cp, d, gh, c->U.data(), c->ent.data(), c->Bxf.data(), c->Byf.data(),
+                                              c->Bzf.data());
+  for (int f = 0; f < NGF; ++f) c->g[f] = std::move(gh.f[f]);
+  c->mask = std::move(gh.mask);
+  c->st = std::move(gh.stencil);
+  if (!e.empty()) {
+    if (why && nwhy > 0) std::snprintf(why, (size_t)nwhy, "%s", e.c_str());
+    return 1;
+  }
+  for (size_t t = 6 * c->S; t < c->ent.size(); ++t) c->ent[t] = 0.0;
+  return 0;
+}
+
+// Geometry field f, mask and stencil of the solve (for comparisons).
+void oracle_get_geometry(void* h, int f, double* out) {
+  Ctx* c = (Ctx*)h;
+  std::memcpy(out, c->g[f].data(), c->g[f].size() * sizeof(double));
+}
+void oracle_get_mask_stencil(void* h, int32_t* mask, int32_t* st) {
+  Ctx* c = (Ctx*)h;
+  std::memcpy(mask, c->mask.data(), c->mask.size() * sizeof(int32_t));
+  std::memcpy(st, c->st.data(), c->st.size() * sizeof(int32_t));
+}
 
 // Geometry field f (cs_geom_field order), [comp][6][box] doubles.
 void oracle_set_geometry(void* h, int f, const double* data) {
@@ -1913,6 +2058,7 @@ int oracle_debug_get(void* h, int which, double* out) {
       for (int q = 0; q < 3; ++q) std::memcpy(out + q * S6, s[q]->data(), S6 * sizeof(double));
       break;
     }
+    case 13: cp(c->pos); break;
     default: return 1;
   }
   return 0;
@@ -1950,6 +2096,55 @@ double oracle_step(void* h, double dtcur) {
   for (int irk = 1; irk <= ns; ++irk) stage(*c, irk, dtcur);
   c->time += dtcur;
   return evaluate_timestep(*c, dtcur);
+}
+
+// The pointwise physics on n cases, with the solve's constants; the same
+// cases and layouts as the library's cs_pointwise: kind 0 PRIM_TO_CONS,
+// kind 1 CONS_TO_PRIM, kind 2 the HLL solve of OneD_RS_MHD_Ptwise.
+int oracle_pointwise(void* h, int kind, int n, const double* in, double* out) {
+  const Ctx* c = (const Ctx*)h;
+  for (int t = 0; t < n; ++t) {
+    if (kind == 0) {
+      const double* a = in + (size_t)t * 9;
+      double V[NV], U[NV];
+      for (int q = 0; q < NV; ++q) V[q] = a[q];
+      prim_to_cons(c->ph, a[8], U, V);
+      for (int q = 0; q < NV; ++q) out[(size_t)t * 8 + q] = U[q];
+    } else if (kind == 1) {
+      const double* a = in + (size_t)t * 9;
+      double V[NV], U[NV];
+      for (int q = 0; q < NV; ++q) U[q] = a[q];
+      double ent = a[8];
+      const int flag = cons_to_prim(c->ph, ent, U, V);
+      double* o = out + (size_t)t * 18;
+      for (int q = 0; q < NV; ++q) o[q] = V[q];
+      o[8] = ent;
+      o[9] = flag;
+      for (int q = 0; q < NV; ++q) o[10 + q] = U[q];
+    } else if (kind == 2) {
+      const double* a = in + (size_t)t * 18;
+      double VL[NV], VR[NV];
+      for (int q = 0; q < NV; ++q) {
+        VL[q] = a[q];
+        VR[q] = a[8 + q];
+      }
+      RSOut r;
+      oned_rs_hll(c->ph, VL, VR, a[16], a[17], r);
+      double* o = out + (size_t)t * 35;
+      for (int q = 0; q < NV; ++q) {
+        o[q] = r.FlL[q];
+        o[8 + q] = r.FlR[q];
+        o[16 + q] = r.FL[q];
+        o[24 + q] = r.FR[q];
+      }
+      o[32] = r.SL;
+      o[33] = r.SR;
+      o[34] = r.entF;
+    } else {
+      return 1;
+    }
+  }
+  return 0;
 }
 
 // The two multidimensional Riemann solvers with four / three separate Ez

@@ -38,7 +38,10 @@ def parse(text: str) -> dict:
 
 
 def main() -> int:
-    ref = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        print(__doc__.strip().splitlines()[-1], file=sys.stderr)
+        return 2
+    ref = Path(sys.argv[1])
     src = ref / "_T" / "_200mesh" / "test_quadpoints.out"
     data = parse(src.read_text())
     data["setting"] = {"isector": 1, "ntp_global": 2, "nr_global": 2, "iscale": 2, "rmin": 10.0, "rmax": 11.0,

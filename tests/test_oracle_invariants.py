@@ -154,3 +154,93 @@ def test_ghost_fill_reproduces_a_manufactured_linear_field():
     o.put_state(start)
     o.fill_ghosts()
     _ghost_check(s, o.get_state(), exact)
+
+
+def _linear_errors(s, V):
+    """Max relative error of modes 2-4 against l0 x gradient and max |mode 5-10|
+    of every primitive, away from the radial padding."""
+    from seeded_states import away_from_radial_padding as inner, linear_gradients
+
+    l0 = s.geometry("V_SCALE")[0]
+    out = {}
+    for c, gr in linear_gradients().items():
+        slope = max(np.abs(inner(s, V[m * 8 + c] - gr[m] * l0)).max() for m in range(1, 4))
+        scale = max(abs(gr[m]) for m in range(1, 4)) * np.abs(inner(s, l0)).max()
+        higher = max(np.abs(inner(s, V[m * 8 + c])).max() for m in range(4, 10))
+        out[c] = (slope / scale, higher / scale)
+    return out
+
+
+def test_linear_field_is_reproduced_by_steps_7ab_and_the_adp_solve():
+    """Known answer: a linear primitive field with the divergence-free
+    B = b (x, -2y, z) of 801:105-225 is reproduced exactly by the WENO-AO
+    stencils (7.a), the MRWENO least squares (7.b) and the ADP constrained
+    least squares (8.d, B modes): slopes = l0 x gradient, higher modes 0,
+    to round-off, in every zone clear of the radial padding (the ghost fill
+    across panel edges included)."""
+    from seeded_states import linear_state
+
+    pr = cs.preset("shell16")
+    pr["params"]["flatten_coef"] = 1e30
+    s = cs.Solve(**pr["params"])
+    s.mesh_build(device=False)
+    o = Oracle(s)
+    o.put_state(linear_state(s))
+    o.fill_ghosts()
+    o.limit_all_slopes_p12()
+    assert np.abs(s.interior(o.debug("positivity"))).max() == 0
+    for c, (slope, higher) in _linear_errors(s, o.debug("V")).items():
+        assert slope < 1e-12 and higher < 1e-12, (c, slope, higher)
+
+
+def test_uniform_static_gas_stays_uniform_to_the_mesh_closure():
+    """A uniform gas at rest (no field, no gravity) changes in one step only
+    through the discrete closure of each zone's faces (sum of area x
+    quadrature-weighted normals, 2.5e-8 of the face area on shell16: the
+    reference's quadrature-based areas and normals close to truncation
+    error, not round-off): the pressure force on the open surface gives
+    momentum of at most dt p max|closure| / V = 3.6e-8 here.  Radial layers
+    the upper boundary's volume-scaled outflow copy does not reach stay
+    uniform to 1e-7; the field stays zero exactly."""
+    from seeded_states import uniform_state
+
+    pr = cs.preset("shell16")
+    pr["params"]["gm"] = 0.0
+    s = cs.Solve(**pr["params"])
+    s.mesh_build(device=False)
+    st = uniform_state(s)
+    o = Oracle(s)
+    o.put_state(st)
+    dt = o.evaluate_timestep(1e30)
+    o.step(dt)
+    w = o.get_state()
+    G, N, nr = s.G, s.N, s.nr
+    lower = lambda a: a[..., G + 1:G + nr - 2, G + 1:G + N + 1, G + 1:G + N + 1]  # layers 1 .. nr-3
+    for q in range(8):
+        assert np.abs(lower(w["U"][q] - st["U"][q])).max() <= 1e-7, q
+    for k in ("bxf", "byf", "bzf"):
+        assert np.array_equal(w[k], st[k]), k
+
+
+def test_positivity_shrinks_and_gives_up_on_the_blob_state():
+    """Branch coverage of STEP 7.c (440:553-830): on the blob state some
+    zones shrink their higher modes and some give up; the unperturbed state
+    triggers neither."""
+    from seeded_states import positivity_state
+
+    pr = cs.preset("shell16")
+    s = cs.Solve(**pr["params"])
+    s.mesh_build(device=False)
+    st = s.init_problem_host(**pr["init"])
+    counts = []
+    for state in (st, positivity_state(s, st)):
+        o = Oracle(s)
+        o.put_state(state)
+        o.fill_ghosts()
+        o.limit_all_slopes_p12()
+        rec = s.interior(o.debug("positivity"))
+        counts.append((int(((rec >= 2) & (rec % 2 == 0)).sum()), int((rec % 2 == 1).sum())))
+        o.close()
+    assert counts[0] == (0, 0)
+    shrunk, gave_up = counts[1]
+    assert shrunk >= 10 and gave_up >= 1, counts

@@ -40,6 +40,20 @@ def test_corrupted_payload_and_other_parameters_are_refused(tmp_path):
     assert cs.snapshot_read_host(path, other, s.empty_state())[0] == 3  # CS_ERR_STATE: other physics
 
 
+@pytest.mark.parametrize("change", [dict(rk_scheme=cs.CS_RK2), dict(rhofloor=1e-10), dict(prsfloor=1e-8),
+                                    dict(cfl_coef=0.3), dict(gm=2.0), dict(smallnum=1e-14),
+                                    dict(flatten_coef=0.5), dict(prs_flatten_coef=2.0), dict(bc_upper=0)])
+def test_scheme_and_physics_of_a_snapshot_are_checked(tmp_path, change):
+    """A snapshot resumes only under the integrator, floors, CFL number,
+    gravity, limiter constants and boundary codes it was written with."""
+    s, st = _host_state()
+    path = tmp_path / "d.snap"
+    assert cs.snapshot_write_host(path, s.params, st, 0.0, 1e-3, 0) == 0
+    assert cs.snapshot_read_host(path, s.params, s.empty_state())[0] == 0
+    other = cs.make_params(**dict(cs.preset("shell16")["params"], **change))
+    assert cs.snapshot_read_host(path, other, s.empty_state())[0] == 3
+
+
 @pytest.mark.gpu
 @pytest.mark.skipif(not has_gpu(), reason="needs a CUDA device")
 def test_resume_continues_bit_for_bit(tmp_path):
