@@ -16,8 +16,10 @@ per-stage work arrays are far larger than L2, so no L2 flush is needed.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
-``--impl reference`` times the CPU oracle port of the same path (all host
-threads) on a bounded sample of the workload instead.
+``--impl reference`` times the CPU oracle port of the same path on the same
+workload instead: the oracle builds its own mesh and seeded state (it loads
+no other library) and runs one or more whole steps of the full mesh on all
+host cores, the timed steps bounded to about a minute and a half.
 """
 from __future__ import annotations
 
@@ -70,10 +72,9 @@ ALGO_WORDS_PER_UNIT = {
 }
 
 # DRAM bytes per unit (read + write) measured by ncu on the shell32 case
-# (profiles/top_kernels_shell32.md; units: 190,608 zones of the ADP range,
-# 155,520 of the face-state / flux / least-squares ranges); the full
-# shell128 launches are too large to capture, so roofline.traffic scales
-# these by the units of a full launch.
+# (units: 190,608 zones of the ADP range, 155,520 of the face-state / flux /
+# least-squares ranges); the full shell128 launches are too large to
+# capture, so roofline.traffic scales these by the units of a full launch.
 MEASURED_TRAFFIC_PER_UNIT = {
     "k_adp_solve6": (397.223e6 + 36.802e6) / 190608,
     "k_flux": (150.846e6 + 18.736e6 + 155.063e6 + 19.871e6 + 168.527e6 + 18.285e6) / 3 / 155520,
@@ -83,9 +84,9 @@ MEASURED_TRAFFIC_PER_UNIT = {
 }
 # FP64 operations per unit (2 x DFMA + DADD + DMUL thread instructions),
 # from the same ncu captures.  The path is FP64-bound, so the roofline also
-# reports these against the B200's nominal FP64 rate: 148 SMs x 64 FP64
-# FMA/clock x 2 x 1.965 GHz = 37.2 TFLOP/s (no measured FP64 peak exists for
-# this pool).
+# reports these against the FP64 FMA rate measured on the device in the
+# same run (cs_fp64_fma_rate); the nominal rate, 148 SMs x 64 FP64 FMA per
+# clock x 2 x 1.965 GHz = 37.2 TFLOP/s, is kept for context.
 FP64_FLOP_PER_UNIT = {
     "k_adp_solve6": 6.012e8 / 190608,
     "k_flux": (5.448e8 + 5.448e8 + 6.120e8) / 3 / 155520,
@@ -94,6 +95,18 @@ FP64_FLOP_PER_UNIT = {
     "k_efield_c": 2.367e8 / 155520,
 }
 FP64_NOMINAL_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12
+
+# Compulsory state traffic per zone-update (every stage reads and writes
+# the state once, later stages also read the stage-start state; geometry
+# and operators re-read are overhead): 12 FP64 words of state per zone in
+# the plain form, 9 FP32 + 3 FP64 words (60 B) in the precision form.
+#   two stages (RK2, IMEX-RK2): (24 + 36) words = 480 B; FP32 form 300 B
+#   SSP-RK3: (24 + 36 + 36) words = 768 B; FP32 form 480 B
+def path_bytes_per_zone_update(rk_scheme: int, fp32: bool) -> float:
+    state = 60.0 if fp32 else 96.0
+    stages = 3 if rk_scheme == 3 else 2
+    return state * 2 + state * 3 * (stages - 1)
+
 
 # Steps after which the precision form's state is compared with the FP64 one.
 PRECISION_STEPS = 10
@@ -120,6 +133,10 @@ def parse():
     ap.add_argument("--flags", type=int, default=0,
                     help="cs_params.flags of the timed solve (8: the precision form); the default is the plain FP64 form")
     ap.add_argument("--profile-json", default="", help="also write the per-kernel device times here")
+    ap.add_argument("--precision-workload", default="",
+                    help="also run the precision form against FP64 over --precision-steps steps of this workload "
+                         "(shell256: the 6x256^2x128 statement) and report errors and both forms' times")
+    ap.add_argument("--precision-steps", type=int, default=200)
     return ap.parse_args()
 
 
@@ -210,28 +227,48 @@ def replica_throughput(zones: int, steps: int, world: int, ms_max: float) -> flo
     return zones * steps * world / (ms_max / 1e3)
 
 
-def cpu_baseline_sample(threads: int, steps: int = 1) -> dict:
-    """The oracle (CPU port) on a bounded sample of the workload: the same
-    shell physics on 6 x 16^2 x 8 zones, ``steps`` RK2 steps."""
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_baseline_sample(name: str, steps: int = 1, warmup: int = 0, budget_s: float = 90.0) -> dict:
+    """The oracle (C++ port of the reference CPU path, zone-parallel OpenMP
+    on every host core) on the full workload `name`: its own mesh and
+    seeded initial state (untimed), `warmup` untimed steps, then whole
+    steps timed until `steps` are done or `budget_s` seconds have passed
+    (at least one)."""
+    threads = host_cores()
+    os.environ["OMP_NUM_THREADS"] = str(threads)
     import cubesphere_b200 as cs
     from oracle import Oracle
 
-    os.environ["OMP_NUM_THREADS"] = str(threads)
-    pr = cs.preset("shell16")
-    s = cs.Solve(**pr["params"])
-    s.mesh_build(device=False)
-    st = s.init_problem_host(**pr["init"])
-    o = Oracle(s)
-    o.put_state(st)
-    dt = o.evaluate_timestep(1e30)
+    pr = cs.preset(name)
     t0 = time.perf_counter()
-    for _ in range(steps):
+    o = Oracle(params=cs.make_params(**pr["params"]))
+    o.init_problem(cs.make_init(**pr["init"]))
+    setup = time.perf_counter() - t0
+    dt = o.evaluate_timestep(1e30)
+    for _ in range(warmup):
         dt = o.step(dt)
-    sec = time.perf_counter() - t0
-    zones = 6 * s.N * s.N * s.nr
-    return {"value": zones * steps / sec, "unit": "zone-updates/s", "cores": threads, "kind": "port",
-            "sample": f"oracle C++ port, shell 6x{s.N}^2x{s.nr} zones (same physics as the workload), "
-                      f"{steps} RK2 step(s), {sec:.2f} s"}
+    done, sec = 0, 0.0
+    while done < max(1, steps):
+        t1 = time.perf_counter()
+        dt = o.step(dt)
+        sec += time.perf_counter() - t1
+        done += 1
+        if sec >= budget_s:
+            break
+    o.close()
+    p = pr["params"]
+    zones = 6 * p["ntp"] ** 2 * p["nr"]
+    return {"value": zones * done / sec, "unit": "zone-updates/s", "cores": threads, "kind": "port",
+            "sample": f"oracle C++ port (zone-parallel OpenMP, {threads} threads) on the full {name} workload, "
+                      f"6x{p['ntp']}^2x{p['nr']} zones: {done} whole step(s) timed ({sec:.1f} s) after {warmup} "
+                      f"untimed; mesh + seeded state {setup:.1f} s untimed",
+            "steps_timed": done, "seconds": sec}
 
 
 def serving_sample(seed: int = 7, nreq: int = 24, rate: float = 8.0, max_active: int = 8) -> dict:
@@ -416,55 +453,93 @@ def state_errors(s, got, ref, divb):
     return ({k: l1(*v) for k, v in fields.items()}, {k: linf(*v) for k, v in fields.items()}, float(divb) / bmax)
 
 
-def precision_long_sample(name: str = "shell32", nsteps: int = 200) -> dict:
-    """The precision form over a long run on a small shell: both forms from
-    the same initial state with the FP64 run's time steps, errors after
-    `nsteps` steps."""
+def precision_long_sample(name: str = "shell32", nsteps: int = 200, timed: bool = False) -> dict:
+    """The precision form over a long run: the FP64 form first (its time
+    step of every step recorded, its final state kept on the host, its
+    device freed), then the precision form from the same initial state with
+    the same time steps; relative L1 / Linf errors and max |div B| after
+    `nsteps` steps.  The FP64 run drops the resident operators
+    (CS_FLAG_NO_ADP_CACHE | CS_FLAG_NO_OP_CACHE: the same results to
+    round-off) when the device cannot hold them, as on the 6 x 256^2 x 128
+    shell.  With `timed`, each run's device time per step (CUDA events
+    around the step loop, one host read of the time step per step)."""
+    import torch
+
     import cubesphere_b200 as cs
 
     pr = cs.preset(name)
-    s = cs.Solve(**pr["params"])
-    s.mesh_build()
-    s.init_problem(**pr["init"])
-    dt = s.evaluate_timestep(1e30)
-    dts = []
-    for _ in range(nsteps):
-        dts.append(dt)
-        dt = s.step(dt)
-    ref = s.get_state()
-    s.close()
-    f = cs.Solve(**pr["params"], flags=cs.CS_FLAG_FP32)
-    f.mesh_build()
-    f.init_problem(**pr["init"])
-    f.evaluate_timestep(1e30)
-    for d in dts:
-        f.step(d)
-    got = f.get_state()
-    _, _, divb = f.diag()
-    err, err_inf, divb_rel = state_errors(f, got, ref, divb)
-    f.close()
-    return {"workload": name, "steps_compared": nsteps, "l1_rel_err_vs_f64": err, "linf_rel_err_vs_f64": err_inf,
-            "max_divb_over_bmax": divb_rel}
+    free = torch.cuda.mem_get_info()[0]
+    f64_flags = 0
+    if cs.estimate_device_bytes(**pr["params"]) > 0.9 * free:
+        f64_flags = cs.CS_FLAG_NO_ADP_CACHE | cs.CS_FLAG_NO_OP_CACHE
+
+    def run(flags, dts_in):
+        s = cs.Solve(**pr["params"], flags=flags)
+        s.mesh_build()
+        s.init_problem(**pr["init"])
+        dt = s.evaluate_timestep(1e30)
+        dts = []
+        stream = torch.cuda.ExternalStream(s.stream_ptr())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.synchronize()
+        e0.record(stream)
+        for n in range(nsteps):
+            d = dts_in[n] if dts_in is not None else dt
+            dts.append(d)
+            dt = s.step(d)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / nsteps
+        got = s.get_state()
+        _, _, divb = s.diag()
+        s.close()
+        return got, dts, divb, ms
+
+    ref, dts, _, ms64 = run(f64_flags, None)
+    torch.cuda.synchronize()
+    got, _, divb, ms32 = run(cs.CS_FLAG_FP32, dts)
+    shape = cs.Solve(**pr["params"])
+    err, err_inf, divb_rel = state_errors(shape, got, ref, divb)
+    shape.close()
+    p = pr["params"]
+    out = {"workload": name, "zones": 6 * p["ntp"] ** 2 * p["nr"], "steps_compared": nsteps,
+           "l1_rel_err_vs_f64": err, "linf_rel_err_vs_f64": err_inf, "max_divb_over_bmax": divb_rel,
+           "f64_flags": f64_flags}
+    if timed:
+        zones = out["zones"]
+        out.update({"f64_ms_per_step": ms64, "f32_ms_per_step": ms32,
+                    "f64_zone_updates_per_s": zones / (ms64 / 1e3), "f32_zone_updates_per_s": zones / (ms32 / 1e3),
+                    "timing": "CUDA events around each run's step loop (one host read of the time step per step)"})
+    return out
+
+
+def workload_config(args, zones: int, world: int) -> dict:
+    import cubesphere_b200 as cs
+
+    return {"workload": args.workload, "desc": WORKLOAD_DOC.get(args.workload, ""), "flags": args.flags,
+            "zones": zones, "parallelism": f"replicas x{world}",
+            "precision": "f32 bulk / f64 B" if args.flags & cs.CS_FLAG_FP32 else "f64",
+            "l2": "inputs larger than L2 (state and work arrays >> 126 MB), no flush"}
 
 
 def run_reference(args):
     world, rank, local = dist_setup()
     if rank != 0:
         return 0
-    threads = min(6, os.cpu_count() or 1)  # the oracle parallelises over the 6 panels
-    vals = []
-    for i in range(args.warmup + args.steps):
-        r = cpu_baseline_sample(threads, steps=1)
-        if i >= args.warmup:
-            vals.append(r["value"])
-    v = statistics.mean(vals)
+    import cubesphere_b200 as cs
+
+    p = cs.preset(args.workload)["params"]
+    zones = 6 * p["ntp"] ** 2 * p["nr"]
+    r = cpu_baseline_sample(args.workload, steps=args.steps, warmup=min(args.warmup, 1))
+    v = r["value"]
     out = {
         "metric": "zone-updates/s", "value": v, "unit": "zone-updates/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded harmonic perturbations)",
-        "config": {"workload": args.workload, "sample": "6x16^2x8 shell per step"},
+        "steps": r["steps_timed"], "warmup": min(args.warmup, 1), "ms_per_step": r["seconds"] * 1e3 / r["steps_timed"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded harmonic density / vector-potential perturbations)",
+        "config": workload_config(args, zones, world),
         "impl": "reference",
-        "cpu_baseline": {"value": v, "unit": "zone-updates/s", "cores": threads, "kind": "port",
+        "cpu_baseline": {"value": v, "unit": "zone-updates/s", "cores": r["cores"], "kind": "port",
                          "sample": r["sample"]},
         "e2e": {"value": v, "unit": "zone-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -579,6 +654,14 @@ def run_gpu(args):
             hbm_peak = float(peaks[key])
     if hbm_peak is None:
         hbm_peak, peak_note = 6650.0, "fallback"
+    # Algorithmic bytes of the path (compulsory state traffic per
+    # zone-update); the dominant kernel is charged one stage's share of them
+    # for the zones one launch covers, and its own read/write set and its
+    # measured DRAM traffic are reported beside that.
+    fp32 = bool(args.flags & cs.CS_FLAG_FP32)
+    rk = int(pr["params"]["rk_scheme"])
+    path_b = path_bytes_per_zone_update(rk, fp32)
+    stage_b = path_b / (3 if rk == 3 else 2)
     dom = max(prof.items(), key=lambda kv: kv[1][0])
     dname, (dms, dcount) = dom
     G, N, nr = s.G, s.N, s.nr
@@ -587,35 +670,54 @@ def run_gpu(args):
         units = 6 * (N + 2 * G - 4) ** 2 * (nr + 2 * G - 4)
     if dname in ("k_flux", "k_face_states"):
         units = 6 * (N + 4) ** 2 * (nr + 4)
+    launch_s = dms / dcount / 1e3
+    per_launch = stage_b * units
+    achieved = per_launch / launch_s / 1e9
+    tr = MEASURED_TRAFFIC_PER_UNIT.get(dname)
+    traffic = tr * units if tr else None
     words = ALGO_WORDS_PER_UNIT.get(dname)
-    roof = None
-    if words is not None:
-        per_launch = words * 8.0 * units
-        if dname == "k_faceB":
-            per_launch /= 3.0  # one launch per face direction
-        achieved = per_launch / (dms / dcount / 1e3) / 1e9
-        tr = MEASURED_TRAFFIC_PER_UNIT.get(dname)
-        roof = {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                "frac": achieved / hbm_peak, "traffic": (tr * units if tr else None),
-                "traffic_source": "ncu dram bytes on shell32, scaled by units" if tr else None,
-                "peak_source": peak_note,
-                "algorithmic_bytes_per_launch": per_launch, "avg_launch_ms": dms / dcount,
-                "share_of_step": dms / sum(v[0] for v in prof.values())}
-        fl = FP64_FLOP_PER_UNIT.get(dname)
-        if fl:
-            tf = fl * units / (dms / dcount / 1e3) / 1e12
-            roof["fp64"] = {"achieved_tflops": tf, "peak_tflops": FP64_NOMINAL_TFLOPS, "frac": tf / FP64_NOMINAL_TFLOPS,
-                            "peak_source": "nominal (148 SMs x 64 FMA/clk x 2 x 1.965 GHz)",
-                            "flop_per_unit_source": "ncu DFMA/DADD/DMUL counts on shell32"}
+    per_value = value / world  # one GPU's zone-updates/s
+    roof = {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+            "frac": achieved / hbm_peak, "traffic": traffic, "peak_source": peak_note + " (MEASURED_PEAKS.json hbm_gbs)",
+            "algorithmic_bytes_per_unit": stage_b,
+            "unit_def": f"zone-stage: {path_b:.0f} B per zone-update / {3 if rk == 3 else 2} stages; "
+                        f"{units} zones per launch",
+            "algorithmic_bytes_per_launch": per_launch, "avg_launch_ms": dms / dcount,
+            "share_of_step": dms / sum(v[0] for v in prof.values()),
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum on shell32, scaled by units"
+            if tr else None,
+            "dram_frac": (traffic / launch_s / 1e9 / hbm_peak) if traffic else None,
+            "traffic_ratio": (traffic / per_launch) if traffic else None,
+            "kernel_read_write_bytes_per_launch": (words * 8.0 * units) if words else None,
+            "path": {"bytes_per_zone_update": path_b, "achieved_gbs": path_b * per_value / 1e9,
+                     "frac": path_b * per_value / 1e9 / hbm_peak}}
+    fp64_peak = None
+    try:
+        fp64_peak = cs.fp64_fma_rate(16384)
+    except cs.CsError:
+        pass
+    fl = FP64_FLOP_PER_UNIT.get(dname)
+    if fl and not fp32:
+        tf = fl * units / launch_s / 1e12
+        den = fp64_peak or FP64_NOMINAL_TFLOPS
+        roof["fp64"] = {"achieved_tflops": tf, "peak_tflops": den, "frac": tf / den,
+                        "peak_source": "measured DFMA chains on this device (cs_fp64_fma_rate)" if fp64_peak
+                        else "nominal (148 SMs x 64 FMA/clk x 2 x 1.965 GHz)",
+                        "nominal_tflops": FP64_NOMINAL_TFLOPS,
+                        "flop_per_unit_source": "ncu DFMA/DADD/DMUL counts on shell32"}
 
+    s.close()
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_sample(min(6, os.cpu_count() or 1), steps=1)
-    s.close()
+        cpu = cpu_baseline_sample(args.workload, steps=1, warmup=0, budget_s=60.0)
     precision = None
     if ref_state is not None:
         torch.cuda.synchronize()
         precision = precision_sample(pr, dts[:PRECISION_STEPS], args.steps, ref_state, zones, world, allmax)
+    precision_stated = None
+    if args.precision_workload:
+        torch.cuda.synchronize()
+        precision_stated = precision_long_sample(args.precision_workload, args.precision_steps, timed=True)
     batch = None
     if not args.no_batch:
         torch.cuda.synchronize()
@@ -636,15 +738,14 @@ def run_gpu(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 bulk / f64 B" if args.flags & cs.CS_FLAG_FP32 else "f64",
         "data": "synthetic (seeded harmonic density / vector-potential perturbations)",
-        "config": {"workload": args.workload, "desc": WORKLOAD_DOC.get(args.workload, ""), "flags": args.flags,
-                   "zones": zones, "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (state and work arrays >> 126 MB), no flush"},
+        "config": workload_config(args, zones, world),
         "e2e": {"value": e2e, "unit": "zone-updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "steps": k_e2e},
         "roofline": roof, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches,
         "top_kernels": {k: round(v[0] / prof_steps, 3) for k, v in
                         sorted(prof.items(), key=lambda kv: -kv[1][0])[:8]},
-        "finite": finite, "dt_last": dt, "precision_form": precision, "batch": batch, "serving": serving,
+        "finite": finite, "dt_last": dt, "precision_form": precision, "precision_stated": precision_stated,
+        "batch": batch, "serving": serving,
     }
     if rank == 0:
         print(json.dumps(out), flush=True)

@@ -50,7 +50,8 @@ EXPORTS = [
     "cs_cfl_timestep_noalloc", "cs_estimate_device_bytes", "cs_serve_create", "cs_serve_submit",
     "cs_serve_wait", "cs_serve_state", "cs_serve_stats", "cs_serve_destroy",
     "cs_batch_create", "cs_batch_steps", "cs_batch_autotune", "cs_batch_grid_fraction", "cs_batch_last_error",
-    "cs_batch_destroy", "cs_twod_rs_ez", "cs_pointwise",
+    "cs_batch_destroy", "cs_twod_rs_ez", "cs_pointwise", "cs_fp64_fma_rate", "cs_limit_minmax",
+    "cs_state_put_amr", "cs_state_get_amr",
     "cs_snapshot_save", "cs_snapshot_load", "cs_snapshot_write_host", "cs_snapshot_read_host",
 ]
 
@@ -87,6 +88,7 @@ CS_FLAG_NO_PANEL_SYNC = 4
 CS_FLAG_FP32 = 8
 CS_FLAG_ADP_PER_PANEL = 16
 CS_FLAG_LSQ_PER_PANEL = 32
+CS_FLAG_STEP10 = 64
 
 
 def make_params(**kw) -> CsParams:
@@ -184,6 +186,10 @@ def load_library() -> ctypes.CDLL:
         "cs_batch_destroy": ([P], ctypes.c_int),
         "cs_twod_rs_ez": ([ctypes.c_int32, ctypes.c_int32, dp, dp], ctypes.c_int),
         "cs_pointwise": ([ctypes.POINTER(CsParams), ctypes.c_int32, ctypes.c_int32, dp, dp], ctypes.c_int),
+        "cs_fp64_fma_rate": ([ctypes.c_int32, dp], ctypes.c_int),
+        "cs_limit_minmax": ([P, dp, dp], ctypes.c_int),
+        "cs_state_put_amr": ([P, ctypes.c_int32, dp, dp, dp, dp, dp], ctypes.c_int),
+        "cs_state_get_amr": ([P, ctypes.c_int32, dp, dp, dp, dp, dp], ctypes.c_int),
         "cs_snapshot_save": ([P, ctypes.c_char_p, D, D, ctypes.c_int64], ctypes.c_int),
         "cs_snapshot_load": ([P, ctypes.c_char_p, dp, dp, ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
         "cs_snapshot_write_host": ([ctypes.c_char_p, ctypes.POINTER(CsParams), dp, dp, dp, dp, dp, D, D,
@@ -409,6 +415,13 @@ class Solve:
                                               ctypes.byref(n)), "cs_snapshot_load")
         return t.value, d.value, n.value
 
+    def limit_minmax(self) -> tuple:
+        """STEP 10 of the last LIMIT_ALL_SLOPES_P12 (needs CS_FLAG_STEP10):
+        (v_min[9], v_max[9]) -- 8 primitives and the normalised divergence."""
+        vmin, vmax = np.zeros(9), np.zeros(9)
+        self._check(self.lib.cs_limit_minmax(self.h, _dptr(vmin), _dptr(vmax)), "cs_limit_minmax")
+        return vmin, vmax
+
     def diag(self) -> tuple:
         m, e, d = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         self._check(self.lib.cs_diag(self.h, ctypes.byref(m), ctypes.byref(e), ctypes.byref(d)), "cs_diag")
@@ -562,6 +575,15 @@ def pointwise(kind: int, cases: np.ndarray, **params) -> np.ndarray:
     if rc:
         raise CsError(f"cs_pointwise failed ({rc})")
     return out
+
+
+def fp64_fma_rate(iters: int = 4096) -> float:
+    """Measured FP64 FMA rate of the current device, TFLOP/s."""
+    out = ctypes.c_double()
+    rc = load_library().cs_fp64_fma_rate(iters, ctypes.byref(out))
+    if rc:
+        raise CsError(f"cs_fp64_fma_rate failed ({rc})")
+    return out.value
 
 
 def estimate_device_bytes(**params) -> int:

@@ -8,6 +8,8 @@
                4 ghost layers, FP64: hydrostatic 1/r^2 shell with seeded density
                and field perturbations of amplitude 0.05 under point-mass
                gravity, IMEX-RK2 (ARS(2,2,2), gravity implicit).
+``shell256``   the same shell at 6 x 256^2 x 128 zones: the workload of the
+               precision form's 200-step error statement.
 ``shell16`` / ``shell32``  the same shell at test sizes.
 """
 from __future__ import annotations
@@ -24,6 +26,12 @@ PRESETS = {
                     gamma=5.0 / 3.0, cfl_coef=0.4, rk_scheme=4, gm=1.0),
         init=dict(seed=2025, kind=1, lmax=4, rho_amp=0.05, a_amp=0.05, v_amp=0.0, p0=0.05),
         steps=50,
+    ),
+    "shell256": dict(
+        params=dict(ntp=256, nr=128, nghost=4, radial_mesh="stretched", radial_ratio=1.02, rmin=1.0, rmax=2.0,
+                    gamma=5.0 / 3.0, cfl_coef=0.4, rk_scheme=4, gm=1.0),
+        init=dict(seed=2025, kind=1, lmax=4, rho_amp=0.05, a_amp=0.05, v_amp=0.0, p0=0.05),
+        steps=200,
     ),
     "shell32": dict(
         params=dict(ntp=32, nr=16, nghost=4, radial_mesh="stretched", radial_ratio=1.02, rmin=1.0, rmax=2.0,

@@ -470,8 +470,6 @@ int alloc_state(Solve& sv, DStateT<R>& s) {
     for (int q = 0; q < 3; ++q) { s.EF1[q] = A(1); s.Ef1[q] = D(1); }
     if (!s.K1 || !s.EF1[2] || !s.Ef1[2]) return cuda_fail(sv, e, "cudaMalloc(IMEX stage rates)");
   }
-  s.FS = A(6 * NQ * (NVAR + 1));
-  if (!s.FS) return cuda_fail(sv, e, "cudaMalloc(face states)");
   // resident geometry-only operators of the mesh (null until built)
   const MeshRes& m = *sv.mesh;
   s.op_m9 = (R*)m.op_m9;
@@ -483,10 +481,18 @@ int alloc_state(Solve& sv, DStateT<R>& s) {
   s.adp_pmap = m.adp_pmap;
   s.adp_rhs = nullptr;
   if (m.adp_lu) {
-    s.adp_rhs = (double*)dalloc(sv, (size_t)adp_range_count(d) * 36 * sizeof(double), e);
+    const size_t rsz = m.adp_pmap ? sizeof(R) : sizeof(double);  // panel-shared factors: the state's type
+    s.adp_rhs = dalloc(sv, (size_t)adp_range_count(d) * 36 * rsz, e);
     if (!s.adp_rhs) return cuda_fail(sv, e, "cudaMalloc(ADP right-hand sides)");
   }
   s.giveup = (int32_t*)dalloc(sv, S6 * sizeof(int32_t), e);
+  if (sv.p.flags & CS_FLAG_STEP10) {
+    // STEP 10 keys: 9 min keys all ones (no stage yet), 9 max keys zero
+    sv.step10_keys = (unsigned long long*)dalloc(sv, 18 * sizeof(unsigned long long), e);
+    if (!sv.step10_keys) return cuda_fail(sv, e, "cudaMalloc(STEP 10 keys)");
+    e = cudaMemsetAsync(sv.step10_keys, 0xff, 9 * sizeof(unsigned long long), sv.stream);
+    if (e != cudaSuccess) return cuda_fail(sv, e, "cudaMemsetAsync(STEP 10 keys)");
+  }
   s.err_flag = (int*)dalloc(sv, 64, e);
   if (!s.err_flag) return cuda_fail(sv, e, "cudaMalloc(error flag)");
   s.dtmin = (unsigned long long*)dalloc(sv, 64, e);
@@ -745,13 +751,18 @@ int mesh_operators(Solve& sv, MeshRes& m, DStateT<R>& s) {
   if (!(sv.p.flags & CS_FLAG_NO_ADP_CACHE)) {
     int8_t pmap[6 * 72];
     const bool shared = !(sv.p.flags & CS_FLAG_ADP_PER_PANEL) && adp_panel_maps(m.host, pmap);
+    // panel-shared factors and right-hand sides in the state's type (the
+    // precision form substitutes in FP32), per-panel ones in FP64
+    const size_t esz = shared ? sizeof(R) : sizeof(double);
     const long long nf = adp_factor_doubles(d, shared);
-    const size_t lu_bytes = (size_t)nf * sizeof(double), pv_bytes = (size_t)nf / 36;
+    const size_t lu_bytes = (size_t)nf * esz, pv_bytes = (size_t)nf / 36;
     size_t fr = 0, tot = 0;
-    if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && lu_bytes + pv_bytes + (size_t)8 * S6 * 60 < fr) {
-      m.adp_lu = (double*)mdalloc(sv, m, lu_bytes, e);
+    // room left after them: the FP32 form's state staging (9 FP64 words
+    // per point, cs_state_put / cs_state_get) and 1 GB
+    if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && lu_bytes + pv_bytes + (size_t)8 * S6 * 10 + ((size_t)1 << 30) < fr) {
+      m.adp_lu = mdalloc(sv, m, lu_bytes, e);
       m.adp_piv = m.adp_lu ? (int8_t*)mdalloc(sv, m, pv_bytes, e) : nullptr;
-      s.adp_rhs = m.adp_piv ? (double*)dalloc(sv, (size_t)adp_range_count(d) * 36 * sizeof(double), e) : nullptr;
+      s.adp_rhs = m.adp_piv ? dalloc(sv, (size_t)adp_range_count(d) * 36 * esz, e) : nullptr;
       if (!m.adp_lu || !m.adp_piv || !s.adp_rhs) return cuda_fail(sv, e, "cudaMalloc(ADP factors)");
       if (shared) {
         m.adp_pmap = (int8_t*)mdalloc(sv, m, sizeof pmap, e);
@@ -840,6 +851,7 @@ void limit_all(Solve& sv) {
   launch_weno(sv);
   launch_positivity(sv);
   launch_faceB_adp(sv);
+  launch_step10(sv);
   launch_efield(sv);
 }
 
@@ -1445,6 +1457,98 @@ int cs_debug_get(cs_ctx* ctx, int32_t which, double* host_out, size_t n) {
   const cudaError_t e = sv.fp32 ? cs::debug_copy(sv, sv.stF, which, nc, host_out)
                                  : cs::debug_copy(sv, sv.st, which, nc, host_out);
   if (e != cudaSuccess) return cs::cuda_fail(sv, e, "cs_debug_get copy");
+  return CS_OK;
+}
+
+namespace {
+// The driver's module zone arrays, U_amr(1-G:N+G, 1-G:N+G, 1-G:nr+G, ncomp,
+// patch) and entropygr_amr(1-G:N+G, 1-G:N+G, 1-G:nr+G, patch), Fortran
+// column-major: offset of zone (i, j, k), component c, patch p.
+struct AmrZones {
+  long long ni, nj, nk;
+  int G, ncomp;
+  AmrZones(const cs::Dims& d, int nc) : ni(d.N + 2 * d.G), nj(d.N + 2 * d.G), nk(d.nr + 2 * d.G), G(d.G), ncomp(nc) {}
+  long long off(int c, int p, int i, int j, int k) const {
+    return (((long long)p * ncomp + c) * nk + (k + G - 1)) * nj * ni + (long long)(j + G - 1) * ni + (i + G - 1);
+  }
+  long long off1(int p, int i, int j, int k) const {  // one component per patch
+    return ((long long)p * nk + (k + G - 1)) * nj * ni + (long long)(j + G - 1) * ni + (i + G - 1);
+  }
+};
+
+// Panel-box (U, ent) <-> module-array (U_amr, entropygr_amr) copies of the
+// zones 1-G .. N+G; the panel box's extra lower layer (index -G) is zero.
+void amr_to_box(const cs::Dims& d, int ncomp, const double* U_amr, const double* ent_amr, double* U, double* ent) {
+  const AmrZones a(d, ncomp);
+  const long long S = d.S;
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int p = 0; p < 6; ++p)
+    for (int k = -d.G; k <= d.nr + d.G; ++k)
+      for (int j = -d.G; j <= d.N + d.G; ++j)
+        for (int i = -d.G; i <= d.N + d.G; ++i) {
+          const long long o = d.idx(i, j, k);
+          const bool in = i > -d.G && j > -d.G && k > -d.G;
+          for (int c = 0; c < cs::NVAR; ++c) U[((long long)c * 6 + p) * S + o] = in ? U_amr[a.off(c, p, i, j, k)] : 0.0;
+          ent[(long long)p * S + o] = in ? ent_amr[a.off1(p, i, j, k)] : 0.0;
+        }
+}
+void box_to_amr(const cs::Dims& d, int ncomp, const double* U, const double* ent, double* U_amr, double* ent_amr) {
+  const AmrZones a(d, ncomp);
+  const long long S = d.S;
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int p = 0; p < 6; ++p)
+    for (int k = 1 - d.G; k <= d.nr + d.G; ++k)
+      for (int j = 1 - d.G; j <= d.N + d.G; ++j)
+        for (int i = 1 - d.G; i <= d.N + d.G; ++i) {
+          const long long o = d.idx(i, j, k);
+          for (int c = 0; c < cs::NVAR; ++c) U_amr[a.off(c, p, i, j, k)] = U[((long long)c * 6 + p) * S + o];
+          ent_amr[a.off1(p, i, j, k)] = ent[(long long)p * S + o];
+        }
+}
+}  // namespace
+
+int cs_state_put_amr(cs_ctx* ctx, int32_t n_cc_components, const double* U_amr, const double* entropygr_amr,
+                     const double* Bxf_amr, const double* Byf_amr, const double* Bzf_amr) {
+  if (!ctx || !U_amr || !entropygr_amr || !Bxf_amr || !Byf_amr || !Bzf_amr) return CS_ERR_ARG;
+  Solve& sv = ctx->sv;
+  if (n_cc_components < cs::NVAR) return cs::fail(sv, CS_ERR_ARG, "n_cc_components must be >= 8 (ideal MHD)");
+  if (int rc = cs::need(sv, false)) return rc;
+  const size_t S6 = (size_t)6 * sv.d.S;
+  std::vector<double> U(cs::NVAR * S6), ent(S6);
+  amr_to_box(sv.d, n_cc_components, U_amr, entropygr_amr, U.data(), ent.data());
+  // the face arrays' box (0-G:N+G)^2 x (0-G:nr+G) per patch is the panel box
+  return cs_state_put(ctx, U.data(), ent.data(), Bxf_amr, Byf_amr, Bzf_amr);
+}
+
+int cs_state_get_amr(cs_ctx* ctx, int32_t n_cc_components, double* U_amr, double* entropygr_amr, double* Bxf_amr,
+                     double* Byf_amr, double* Bzf_amr) {
+  if (!ctx || !U_amr || !entropygr_amr || !Bxf_amr || !Byf_amr || !Bzf_amr) return CS_ERR_ARG;
+  Solve& sv = ctx->sv;
+  if (n_cc_components < cs::NVAR) return cs::fail(sv, CS_ERR_ARG, "n_cc_components must be >= 8 (ideal MHD)");
+  if (int rc = cs::need(sv, true)) return rc;
+  const size_t S6 = (size_t)6 * sv.d.S;
+  std::vector<double> U(cs::NVAR * S6), ent(S6);
+  if (int rc = cs_state_get(ctx, U.data(), ent.data(), Bxf_amr, Byf_amr, Bzf_amr)) return rc;
+  box_to_amr(sv.d, n_cc_components, U.data(), ent.data(), U_amr, entropygr_amr);
+  return CS_OK;
+}
+
+int cs_limit_minmax(cs_ctx* ctx, double* v_min, double* v_max) {
+  if (!ctx || !v_min || !v_max) return CS_ERR_ARG;
+  Solve& sv = ctx->sv;
+  if (int rc = cs::need(sv, true)) return rc;
+  if (!sv.step10_keys) return cs::fail(sv, CS_ERR_STATE, "STEP 10 is evaluated only with CS_FLAG_STEP10");
+  unsigned long long keys[18];
+  CS_CUDA(sv, cudaMemcpyAsync(keys, sv.step10_keys, sizeof keys, cudaMemcpyDeviceToHost, sv.stream));
+  CS_CUDA(sv, cudaStreamSynchronize(sv.stream));
+  if (keys[0] == ~0ULL) return cs::fail(sv, CS_ERR_STATE, "no LIMIT_ALL_SLOPES_P12 has run yet");
+  for (int q = 0; q < 18; ++q) {
+    const unsigned long long k = keys[q];
+    const unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffULL) : ~k;
+    double v;
+    std::memcpy(&v, &b, sizeof v);
+    (q < 9 ? v_min[q] : v_max[q - 9]) = v;
+  }
   return CS_OK;
 }
 

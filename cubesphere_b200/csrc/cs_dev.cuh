@@ -58,7 +58,6 @@ struct DStateT {
   R *msonic, *flatA, *flatB;             // flattener work
   double *Bq[3];                         // B at face quadrature points (5 each)
   R *fcon[3];                            // per-face flux contributions: [16][..] (L 8, R 8)
-  R *FS;                                 // face states: [(side*5 + point)*9 + var][..], 270 comps
   R *S[6];                               // S_L,S_R (x), S_D,S_U (y), S_B,S_T (z) at j=1
   R *EF[3];                              // entropy fluxes
   double *Ef[3];                         // edge EMFs
@@ -71,9 +70,10 @@ struct DStateT {
   R* op_m10;                             // STEP 9.c row weights Minv A_rr^T, [19 x 10][zones of shrink(2)], or null
   const LsqPanelMap* lsq_map9;           // op_m9 shared by the panels (panel 1's zones only), or null
   const LsqPanelMap* lsq_map10;          // op_m10 likewise
-  double* adp_lu;                        // ADP KKT factors: per block of 128 zones, [1296 in use order][128], or null
-  int8_t* adp_piv;                       // their row permutation, per block [36][128]
-  double* adp_rhs;                       // ADP right-hand sides, [36][zones of the ADP range]
+  void* adp_lu;                          // ADP KKT factors, per block of zones [1296 in use order][block], or null:
+                                         // FP64 per panel; panel 1's (adp_pmap set) in the state's type R
+  int8_t* adp_piv;                       // their row permutation, per block [36][block]
+  void* adp_rhs;                         // ADP right-hand sides, [36][zones of the ADP range], typed as adp_lu
   const int8_t* adp_pmap;                // factors shared by the panels: per panel [unknown map 36][sign 36], or null
   int* err_flag;                         // device-side error bits (bounded waits that gave up)
   int32_t* giveup;                       // positivity give-up flags per zone
@@ -441,6 +441,8 @@ long long adp_factor_doubles(const Dims& d, bool shared);
 long long lsq_range_count(const Dims& d);
 void launch_ops_build(Solve& s);
 void launch_efield(Solve& s);
+// STEP 10 min / max into Solve::step10_keys (no-op without CS_FLAG_STEP10).
+void launch_step10(Solve& s);
 void launch_fluxes(Solve& s);
 void launch_edges(Solve& s);
 void launch_sources(Solve& s);

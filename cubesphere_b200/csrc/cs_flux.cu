@@ -25,80 +25,54 @@ __device__ __forceinline__ R Vm(const DStateT<R>& s, const Dims& d, int comp, in
   return s.V[((long long)(mode * NVAR + comp) * NPANEL + p) * d.S + o];
 }
 
-// Face states: every active zone evaluates its reconstruction (8
-// primitives and the entropy) at the 5 quadrature points of each of its 6
-// faces, once per stage.  Side f: 0 +x (face i), 1 -x (face i-1), 2 +y,
-// 3 -y, 4 +z, 5 -z.  Layout FS[(f*5 + q)*9 + var][panel][box].
-constexpr int FS_TPB = 64;
-template <typename R>
-__global__ void __launch_bounds__(FS_TPB) k_face_states(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
-  __shared__ R xs[90][FS_TPB];
-  const int tid = threadIdx.x;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
-    int p, i, j, k;
-    r.decode(t, p, i, j, k);
-    if (mask_at(g, d, p, i, j) != 1) continue;
-    const long long o = d.idx(i, j, k);
-    const R obl0 = R(1.0) / fmax(geoR<R>(g, d, CS_G_V_SCALE, 0, p, i, j, k), R(ph.smallnum));
-    const R cx = geoR<R>(g, d, CS_G_V_CEN, 0, p, i, j, k), cy = geoR<R>(g, d, CS_G_V_CEN, 1, p, i, j, k),
-                 cz = geoR<R>(g, d, CS_G_V_CEN, 2, p, i, j, k);
-#pragma unroll 1
-    for (int f = 0; f < 6; ++f) {
-      const int dir = f / 2;
-      const int QP = dir == 0 ? CS_G_XF_QP : (dir == 1 ? CS_G_YF_QP : CS_G_ZF_QP);
-      const int fx = (f == 1) ? i - 1 : i, fy = (f == 3) ? j - 1 : j, fz = (f == 5) ? k - 1 : k;
-#pragma unroll
-      for (int q = 0; q < 5; ++q) {
-        xs[(f * 5 + q) * 3 + 0][tid] = (geoR<R>(g, d, QP, q, p, fx, fy, fz) - cx) * obl0;
-        xs[(f * 5 + q) * 3 + 1][tid] = (geoR<R>(g, d, QP, 5 + q, p, fx, fy, fz) - cy) * obl0;
-        xs[(f * 5 + q) * 3 + 2][tid] = (geoR<R>(g, d, QP, 10 + q, p, fx, fy, fz) - cz) * obl0;
-      }
-    }
-    R c0[10];
-#pragma unroll
-    for (int m = 0; m < 10; ++m) c0[m] = geoR<R>(g, d, CS_G_COEF, m, p, i, j, k);
-#pragma unroll 1
-    for (int c = 0; c < 8; ++c) {
-      R v[10];
-#pragma unroll
-      for (int m = 0; m < 10; ++m) v[m] = Vm(s, d, c, m, p, o);
-#pragma unroll
-      for (int fq = 0; fq < 30; ++fq)
-        s.FS[((long long)(fq * 9 + c) * NPANEL + p) * d.S + o] =
-            d_poly10(v, c0, xs[fq * 3 + 0][tid], xs[fq * 3 + 1][tid], xs[fq * 3 + 2][tid]);
-    }
-    const R* E = s.ent;
-    const R e0 = E[((long long)0 * NPANEL + p) * d.S + o], e1 = E[((long long)1 * NPANEL + p) * d.S + o],
-                 e2 = E[((long long)2 * NPANEL + p) * d.S + o], e3 = E[((long long)3 * NPANEL + p) * d.S + o];
-#pragma unroll 5
-    for (int fq = 0; fq < 30; ++fq)
-      s.FS[((long long)(fq * 9 + 8) * NPANEL + p) * d.S + o] =
-          e0 + e1 * xs[fq * 3 + 0][tid] + e2 * xs[fq * 3 + 1][tid] + e3 * xs[fq * 3 + 2][tid];
-  }
-}
-
-// One face quadrature point per thread: the five warps of a block take the
-// five points of the same 32 faces, so the zone modes each warp loads are
-// shared through L1 and no thread holds more than one point's state.  The
-// per-point contributions meet in shared memory and are summed in point
-// order (the order of the reference's quadrature loop).
+// A block takes 32 faces, in two phases.  Face states (450:545-2931): the
+// first two warps put each side's five quadrature points, in the side
+// zone's scaled coordinates, and its basis moments in shared memory; then
+// the five warps evaluate the 18 (side, primitive or entropy) polynomials
+// of each face at the five points, each reading that variable's modes once,
+// into shared memory, so no face state goes through HBM.  Fluxes: one face
+// quadrature point per thread (warp = point) rotates
+// the two states to the face frame, solves the HLL problem and rotates the
+// contributions back; they meet in shared memory and are summed in point
+// order (the order of the reference's quadrature loop).  One launch covers
+// the three face directions: tile T is tile T / 3 of direction T % 3, so the
+// x, y and z faces of about the same zone rows run side by side and L2
+// serves a zone's modes to all three.
 constexpr int FLUX_FACES = 32;
 // Registers / occupancy: 4 blocks per SM suit the FP64 instantiation, 7 the
 // FP32 one (measured on the 6 x 128^2 x 64 shell).
 template <typename R>
-__global__ void __launch_bounds__(FLUX_FACES * 5, sizeof(R) == 4 ? 7 : 4) k_flux(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r, int dir) {
-  __shared__ R red[5][16][FLUX_FACES];
-  const int QP = dir == 0 ? CS_G_XF_QP : (dir == 1 ? CS_G_YF_QP : CS_G_ZF_QP);
-  const int QW = dir == 0 ? CS_G_XF_QW : (dir == 1 ? CS_G_YF_QW : CS_G_ZF_QW);
-  const int AR = dir == 0 ? CS_G_XF_AREA : (dir == 1 ? CS_G_YF_AREA : CS_G_ZF_AREA);
-  R* F = s.fcon[dir];
-  R* SLo = s.S[2 * dir];
-  R* SHi = s.S[2 * dir + 1];
-  R* EF = s.EF[dir];
+__global__ void __launch_bounds__(FLUX_FACES * 5, sizeof(R) == 4 ? 7 : 4) k_flux(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r0, Range3 r1, Range3 r2) {
+  // the point coordinates and moments are dead once the face states are
+  // formed, so they share their space with the flux contributions
+  union Scratch {
+    R red[5][16][FLUX_FACES];
+    struct {
+      R pc[2][5][3][FLUX_FACES];  // [side][point][x y z][face]
+      R cf[2][6][FLUX_FACES];     // [side][moments 4-9][face]
+    } g;
+  };
+  __shared__ Scratch sc;
+  R(&red)[5][16][FLUX_FACES] = sc.red;
+  __shared__ R fs[2][9][5][FLUX_FACES];  // [side][primitive 0-7, entropy][point][face]
+  __shared__ long long zo[2][FLUX_FACES];  // box offset of each side's zone
   const int lane = threadIdx.x % FLUX_FACES, jq = threadIdx.x / FLUX_FACES;
-  const long long nf = r.count();
-  const long long ntile = (nf + FLUX_FACES - 1) / FLUX_FACES;
-  for (long long tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
+  const long long nt0 = (r0.count() + FLUX_FACES - 1) / FLUX_FACES, nt1 = (r1.count() + FLUX_FACES - 1) / FLUX_FACES,
+                  nt2 = (r2.count() + FLUX_FACES - 1) / FLUX_FACES;
+  const long long ntile = 3 * max(nt0, max(nt1, nt2));
+  for (long long T = blockIdx.x; T < ntile; T += gridDim.x) {
+    const int dir = (int)(T % 3);
+    const long long tile = T / 3;
+    const Range3 r = dir == 0 ? r0 : (dir == 1 ? r1 : r2);
+    if (tile >= (dir == 0 ? nt0 : (dir == 1 ? nt1 : nt2))) continue;  // uniform over the block
+    const long long nf = r.count();
+    const int QP = dir == 0 ? CS_G_XF_QP : (dir == 1 ? CS_G_YF_QP : CS_G_ZF_QP);
+    const int QW = dir == 0 ? CS_G_XF_QW : (dir == 1 ? CS_G_YF_QW : CS_G_ZF_QW);
+    const int AR = dir == 0 ? CS_G_XF_AREA : (dir == 1 ? CS_G_YF_AREA : CS_G_ZF_AREA);
+    R* F = s.fcon[dir];
+    R* SLo = s.S[2 * dir];
+    R* SHi = s.S[2 * dir + 1];
+    R* EF = s.EF[dir];
     const long long t = tile * FLUX_FACES + lane;
     const bool valid = t < nf;
     int p = 0, i = 0, j = 0, k = 0;
@@ -123,11 +97,61 @@ __global__ void __launch_bounds__(FLUX_FACES * 5, sizeof(R) == 4 ? 7 : 4) k_flux
         rz = k + 1;
       }
     }
+    // phase 1a: each side's points and moments (a side remapped through
+    // istencil at a panel corner is the remapped zone)
+    if (jq < 2 && !skip) {
+      const int side = jq;
+      const int zx = side ? rx : lx, zy = side ? ry : ly, zz = side ? rz : lz;
+      zo[side][lane] = d.idx(zx, zy, zz);
+      const R obl = R(1.0) / fmax(geoR<R>(g, d, CS_G_V_SCALE, 0, p, zx, zy, zz), R(ph.smallnum));
+      const R cx = geoR<R>(g, d, CS_G_V_CEN, 0, p, zx, zy, zz), cy = geoR<R>(g, d, CS_G_V_CEN, 1, p, zx, zy, zz),
+              cz = geoR<R>(g, d, CS_G_V_CEN, 2, p, zx, zy, zz);
+#pragma unroll
+      for (int q = 0; q < 5; ++q) {
+        sc.g.pc[side][q][0][lane] = (geoR<R>(g, d, QP, q, p, i, j, k) - cx) * obl;
+        sc.g.pc[side][q][1][lane] = (geoR<R>(g, d, QP, 5 + q, p, i, j, k) - cy) * obl;
+        sc.g.pc[side][q][2][lane] = (geoR<R>(g, d, QP, 10 + q, p, i, j, k) - cz) * obl;
+      }
+#pragma unroll
+      for (int m = 4; m < 10; ++m) sc.g.cf[side][m - 4][lane] = geoR<R>(g, d, CS_G_COEF, m, p, zx, zy, zz);
+    }
+    __syncthreads();
+    // phase 1b: task v = 0..17 (side v / 9, variable v % 9) of this face;
+    // warp jq takes tasks jq, jq + 5, jq + 10, jq + 15
+    if (!skip) {
+#pragma unroll 1
+      for (int v = jq; v < 18; v += 5) {
+        const int side = v / 9, var = v % 9;
+        const long long oz = zo[side][lane];
+        R cc[10];
+        cc[0] = cc[1] = cc[2] = cc[3] = R(0.0);
+#pragma unroll
+        for (int m = 4; m < 10; ++m) cc[m] = sc.g.cf[side][m - 4][lane];
+        if (var < 8) {
+          R w[10];
+#pragma unroll
+          for (int m = 0; m < 10; ++m) w[m] = Vm(s, d, var, m, p, oz);
+#pragma unroll
+          for (int q = 0; q < 5; ++q)
+            fs[side][var][q][lane] =
+                d_poly10(w, cc, sc.g.pc[side][q][0][lane], sc.g.pc[side][q][1][lane], sc.g.pc[side][q][2][lane]);
+        } else {
+          const R* E = s.ent;
+          const R e0 = E[((long long)0 * NPANEL + p) * d.S + oz], e1 = E[((long long)1 * NPANEL + p) * d.S + oz],
+                  e2 = E[((long long)2 * NPANEL + p) * d.S + oz], e3 = E[((long long)3 * NPANEL + p) * d.S + oz];
+#pragma unroll
+          for (int q = 0; q < 5; ++q)
+            fs[side][8][q][lane] = e0 + e1 * sc.g.pc[side][q][0][lane] + e2 * sc.g.pc[side][q][1][lane] +
+                                   e3 * sc.g.pc[side][q][2][lane];
+        }
+      }
+    }
+    __syncthreads();
+    // phase 2: the flux at point jq of face lane
     if (skip) {
 #pragma unroll
       for (int c = 0; c < 16; ++c) red[jq][c][lane] = R(0.0);
     } else {
-      const long long oL = d.idx(lx, ly, lz), oR = d.idx(rx, ry, rz);
       R Ax, Ay, Az, Bx, By, Bz, Cx, Cy, Cz;
       if (dir == 0) {
         Ax = geoR<R>(g, d, CS_G_XF_N, 0, p, i, j, k);
@@ -185,49 +209,13 @@ __global__ void __launch_bounds__(FLUX_FACES * 5, sizeof(R) == 4 ? 7 : 4) k_flux
         Cy = Cy * tt;
         Cz = Cz * tt;
       }
-      const R px = geoR<R>(g, d, QP, jq, p, i, j, k), py = geoR<R>(g, d, QP, 5 + jq, p, i, j, k),
-                   pz = geoR<R>(g, d, QP, 10 + jq, p, i, j, k);
-      // Face states of the two sides: precomputed unless the side was
-      // remapped through istencil (panel corners), which evaluates the
-      // remapped zone's reconstruction at this face's point here.
-      const bool remapL = lx != i || ly != j;
-      const bool remapR = dir == 0 ? (rx != i + 1 || ry != j) : (dir == 1 ? (rx != i || ry != j + 1) : false);
-      const int fL = 2 * dir, fR = 2 * dir + 1;
-      R VL[8], VR[8], entL, entR;
-      auto eval = [&](int zx, int zy, int zz, R* Vo, R& eo) {
-        const long long oz = d.idx(zx, zy, zz);
-        const R obl = R(1.0) / fmax(geoR<R>(g, d, CS_G_V_SCALE, 0, p, zx, zy, zz), R(ph.smallnum));
-        const R x = (px - geoR<R>(g, d, CS_G_V_CEN, 0, p, zx, zy, zz)) * obl;
-        const R y = (py - geoR<R>(g, d, CS_G_V_CEN, 1, p, zx, zy, zz)) * obl;
-        const R z = (pz - geoR<R>(g, d, CS_G_V_CEN, 2, p, zx, zy, zz)) * obl;
-        R cc[10];
+      R VL[8], VR[8];
 #pragma unroll
-        for (int m = 0; m < 10; ++m) cc[m] = geoR<R>(g, d, CS_G_COEF, m, p, zx, zy, zz);
-#pragma unroll
-        for (int c = 0; c < 8; ++c) {
-          R vv[10];
-#pragma unroll
-          for (int m = 0; m < 10; ++m) vv[m] = Vm(s, d, c, m, p, oz);
-          Vo[c] = d_poly10(vv, cc, x, y, z);
-        }
-        const R* E = s.ent;
-        eo = E[((long long)0 * NPANEL + p) * d.S + oz] + E[((long long)1 * NPANEL + p) * d.S + oz] * x +
-             E[((long long)2 * NPANEL + p) * d.S + oz] * y + E[((long long)3 * NPANEL + p) * d.S + oz] * z;
-      };
-      if (remapL) {
-        eval(lx, ly, lz, VL, entL);
-      } else {
-#pragma unroll
-        for (int c = 0; c < 8; ++c) VL[c] = s.FS[((long long)((fL * 5 + jq) * 9 + c) * NPANEL + p) * d.S + oL];
-        entL = s.FS[((long long)((fL * 5 + jq) * 9 + 8) * NPANEL + p) * d.S + oL];
+      for (int c = 0; c < 8; ++c) {
+        VL[c] = fs[0][c][jq][lane];
+        VR[c] = fs[1][c][jq][lane];
       }
-      if (remapR) {
-        eval(rx, ry, rz, VR, entR);
-      } else {
-#pragma unroll
-        for (int c = 0; c < 8; ++c) VR[c] = s.FS[((long long)((fR * 5 + jq) * 9 + c) * NPANEL + p) * d.S + oR];
-        entR = s.FS[((long long)((fR * 5 + jq) * 9 + 8) * NPANEL + p) * d.S + oR];
-      }
+      const R entL = fs[0][8][jq][lane], entR = fs[1][8][jq][lane];
 #pragma unroll
       for (int o = 1; o <= 5; o += 4) {
         R a1 = Ax * VL[o] + Ay * VL[o + 1] + Az * VL[o + 2];
@@ -366,14 +354,10 @@ void launch_fluxes_t(Solve& sv, DStateT<R>& st) {
   Range3 fx = {-1, N + 1, 0, N + 1, 0, nr + 1};
   Range3 fy = {0, N + 1, -1, N + 1, 0, nr + 1};
   Range3 fz = {0, N + 1, 0, N + 1, -1, nr + 1};
-  Range3 zs = {-1, N + 2, -1, N + 2, -1, nr + 2};
-  k_face_states<R><<<blocks_for(zs.count(), FS_TPB, grid_sms(sv)), FS_TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, zs);
-  mark(sv, "k_face_states");
-  const Range3 fr[3] = {fx, fy, fz};
-  for (int dir = 0; dir < 3; ++dir) {
-    const long long nt = (fr[dir].count() + FLUX_FACES - 1) / FLUX_FACES;
+  {
+    const long long nt = 3 * ((std::max(fx.count(), std::max(fy.count(), fz.count())) + FLUX_FACES - 1) / FLUX_FACES);
     const int nb = (int)std::min<long long>(nt, (long long)grid_sms(sv) * 32);
-    k_flux<R><<<nb, FLUX_FACES * 5, 0, sv.stream>>>(d, sv.ph, sv.g, st, fr[dir], dir);
+    k_flux<R><<<nb, FLUX_FACES * 5, 0, sv.stream>>>(d, sv.ph, sv.g, st, fx, fy, fz);
     mark(sv, "k_flux");
   }
   if (sv.psync.nf > 0) {

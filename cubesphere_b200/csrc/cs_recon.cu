@@ -764,11 +764,13 @@ __global__ void __launch_bounds__(TPB) k_faceB(Dims d, PhysC ph, DGeom g, DState
       if (mask_at(g, d, p, i, j) == 0) skip = true;
       rz = k + 1;
     }
-    double bq[5] = {0, 0, 0, 0, 0};
+    // the two sides' values in the state's type; the shift to the facial
+    // mean in FP64, so the values average to the FP64 face B exactly
+    R bq[5] = {R(0), R(0), R(0), R(0), R(0)};
     if (!skip) {
-      const double obl0 = 1.0 / fmax(geo(g, d, CS_G_V_SCALE, 0, p, lx, ly, lz), ph.smallnum);
-      const double obl02 = 1.0 / fmax(geo(g, d, CS_G_V_SCALE, 0, p, rx, ry, rz), ph.smallnum);
-      double cL[10], cR[10], vL[3][10], vR[3][10];
+      const R obl0 = R(1.0) / fmax(geoR<R>(g, d, CS_G_V_SCALE, 0, p, lx, ly, lz), R(ph.smallnum));
+      const R obl02 = R(1.0) / fmax(geoR<R>(g, d, CS_G_V_SCALE, 0, p, rx, ry, rz), R(ph.smallnum));
+      R cL[10], cR[10], vL[3][10], vR[3][10];
       coef10(g, d, p, lx, ly, lz, cL);
       coef10(g, d, p, rx, ry, rz, cR);
 #pragma unroll
@@ -778,30 +780,30 @@ __global__ void __launch_bounds__(TPB) k_faceB(Dims d, PhysC ph, DGeom g, DState
           vL[b][m] = Vat(s, d, 5 + b, m, p, lx, ly, lz);
           vR[b][m] = Vat(s, d, 5 + b, m, p, rx, ry, rz);
         }
-      const double lcx = geo(g, d, CS_G_V_CEN, 0, p, lx, ly, lz), lcy = geo(g, d, CS_G_V_CEN, 1, p, lx, ly, lz),
-                   lcz = geo(g, d, CS_G_V_CEN, 2, p, lx, ly, lz);
-      const double rcx = geo(g, d, CS_G_V_CEN, 0, p, rx, ry, rz), rcy = geo(g, d, CS_G_V_CEN, 1, p, rx, ry, rz),
-                   rcz = geo(g, d, CS_G_V_CEN, 2, p, rx, ry, rz);
+      const R lcx = geoR<R>(g, d, CS_G_V_CEN, 0, p, lx, ly, lz), lcy = geoR<R>(g, d, CS_G_V_CEN, 1, p, lx, ly, lz),
+              lcz = geoR<R>(g, d, CS_G_V_CEN, 2, p, lx, ly, lz);
+      const R rcx = geoR<R>(g, d, CS_G_V_CEN, 0, p, rx, ry, rz), rcy = geoR<R>(g, d, CS_G_V_CEN, 1, p, rx, ry, rz),
+              rcz = geoR<R>(g, d, CS_G_V_CEN, 2, p, rx, ry, rz);
 #pragma unroll
       for (int q = 0; q < 5; ++q) {
         const int nq = dir == 2 ? q : 0, ns = dir == 2 ? 5 : 1;
-        const double nx = geo(g, d, NF, 0 * ns + nq, p, i, j, k), ny = geo(g, d, NF, 1 * ns + nq, p, i, j, k),
-                     nz = geo(g, d, NF, 2 * ns + nq, p, i, j, k);
-        const double px = geo(g, d, QP, q, p, i, j, k), py = geo(g, d, QP, 5 + q, p, i, j, k),
-                     pz = geo(g, d, QP, 10 + q, p, i, j, k);
-        const double x = (px - lcx) * obl0, y = (py - lcy) * obl0, z = (pz - lcz) * obl0;
-        const double x2 = (px - rcx) * obl02, y2 = (py - rcy) * obl02, z2 = (pz - rcz) * obl02;
-        const double bx = d_poly10(vL[0], cL, x, y, z), by = d_poly10(vL[1], cL, x, y, z), bz = d_poly10(vL[2], cL, x, y, z);
-        const double bx2 = d_poly10(vR[0], cR, x2, y2, z2), by2 = d_poly10(vR[1], cR, x2, y2, z2),
-                     bz2 = d_poly10(vR[2], cR, x2, y2, z2);
-        bq[q] = 0.5 * (nx * (bx + bx2) + ny * (by + by2) + nz * (bz + bz2));
+        const R nx = geoR<R>(g, d, NF, 0 * ns + nq, p, i, j, k), ny = geoR<R>(g, d, NF, 1 * ns + nq, p, i, j, k),
+                nz = geoR<R>(g, d, NF, 2 * ns + nq, p, i, j, k);
+        const R px = geoR<R>(g, d, QP, q, p, i, j, k), py = geoR<R>(g, d, QP, 5 + q, p, i, j, k),
+                pz = geoR<R>(g, d, QP, 10 + q, p, i, j, k);
+        const R x = (px - lcx) * obl0, y = (py - lcy) * obl0, z = (pz - lcz) * obl0;
+        const R x2 = (px - rcx) * obl02, y2 = (py - rcy) * obl02, z2 = (pz - rcz) * obl02;
+        const R bx = d_poly10(vL[0], cL, x, y, z), by = d_poly10(vL[1], cL, x, y, z), bz = d_poly10(vL[2], cL, x, y, z);
+        const R bx2 = d_poly10(vR[0], cR, x2, y2, z2), by2 = d_poly10(vR[1], cR, x2, y2, z2),
+                bz2 = d_poly10(vR[2], cR, x2, y2, z2);
+        bq[q] = R(0.5) * (nx * (bx + bx2) + ny * (by + by2) + nz * (bz + bz2));
       }
     }
     double bd = Bf[d.at(0, p, i, j, k)];
 #pragma unroll
-    for (int q = 0; q < 5; ++q) bd = bd - geo(g, d, BW, q, p, i, j, k) * bq[q];
+    for (int q = 0; q < 5; ++q) bd = bd - geo(g, d, BW, q, p, i, j, k) * (double)bq[q];
 #pragma unroll
-    for (int q = 0; q < 5; ++q) Bq[d.at(q, p, i, j, k)] = bq[q] + bd;
+    for (int q = 0; q < 5; ++q) Bq[d.at(q, p, i, j, k)] = (double)bq[q] + bd;
   }
 }
 
@@ -992,7 +994,11 @@ __global__ void __launch_bounds__(32 * ADP_WARPS) k_adp(Dims d, PhysC ph, DGeom 
       const long long blk = t / zb, z = t % zb;
       for (int e = lane; e < 36 * 36; e += 32) {
         const int pos = zb == ADP6_ZB ? adp6_stream_pos(e / 36, e % 36) : adp_stream_pos(e / 36, e % 36);
-        s.adp_lu[(blk * 1296 + pos) * zb + z] = S.K[e / 36][e % 36];
+        // panel-shared factors in the state's type, per-panel ones in FP64
+        if (zb == ADP6_ZB)
+          ((R*)s.adp_lu)[(blk * 1296 + pos) * zb + z] = (R)S.K[e / 36][e % 36];
+        else
+          ((double*)s.adp_lu)[(blk * 1296 + pos) * zb + z] = S.K[e / 36][e % 36];
       }
       for (int e = lane; e < 36; e += 32) s.adp_piv[(blk * 36 + e) * zb + z] = (int8_t)S.piv[e];
       __syncwarp();
@@ -1075,7 +1081,7 @@ __global__ void __launch_bounds__(ADPR_TPB) k_adp_rhs(Dims d, PhysC ph, DGeom g,
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
     int p, i, j, k;
     r.decode(t, p, i, j, k);
-    double* out = s.adp_rhs + t;
+    double* out = (double*)s.adp_rhs + t;
     if (mask_at(g, d, p, i, j) != 1) {
 #pragma unroll
       for (int a = 0; a < 36; ++a) out[(long long)a * n] = 0.0;
@@ -1137,22 +1143,22 @@ __global__ void __launch_bounds__(ADPR_TPB, 4) k_adp_rhs6(Dims d, PhysC ph, DGeo
        t1 += (long long)gridDim.x * blockDim.x) {
     int p0, i, j, k;
     r.decode(t1, p0, i, j, k);
-    const double obl0 = 1.0 / fmax(geo(g, d, CS_G_V_SCALE, 0, 0, i, j, k), ph.smallnum);
-    const double vc0 = geo(g, d, CS_G_V_CEN, 0, 0, i, j, k), vc1 = geo(g, d, CS_G_V_CEN, 1, 0, i, j, k),
-                 vc2 = geo(g, d, CS_G_V_CEN, 2, 0, i, j, k);
-    double c0[10];
+    const R obl0 = R(1.0) / fmax(geoR<R>(g, d, CS_G_V_SCALE, 0, 0, i, j, k), R(ph.smallnum));
+    const R vc0 = geoR<R>(g, d, CS_G_V_CEN, 0, 0, i, j, k), vc1 = geoR<R>(g, d, CS_G_V_CEN, 1, 0, i, j, k),
+            vc2 = geoR<R>(g, d, CS_G_V_CEN, 2, 0, i, j, k);
+    R c0[10];
     coef10(g, d, 0, i, j, k, c0);
 #pragma unroll 1
     for (int p = 0; p < 6; ++p) {
-      double* out = s.adp_rhs + p * n1 + t1;
+      R* out = (R*)s.adp_rhs + p * n1 + t1;
       if (mask_at(g, d, p, i, j) != 1) {
 #pragma unroll
-        for (int a = 0; a < 36; ++a) out[(long long)a * n] = 0.0;
+        for (int a = 0; a < 36; ++a) out[(long long)a * n] = R(0.0);
         continue;
       }
-      double rhs[30];
+      R rhs[30];
 #pragma unroll
-      for (int a = 0; a < 30; ++a) rhs[a] = 0.0;
+      for (int a = 0; a < 30; ++a) rhs[a] = R(0.0);
 #pragma unroll 1
       for (int f = 0; f < 6; ++f) {
         const int dir = f / 2;
@@ -1161,25 +1167,25 @@ __global__ void __launch_bounds__(ADPR_TPB, 4) k_adp_rhs6(Dims d, PhysC ph, DGeo
         const int BW = dir == 0 ? CS_G_XB_QW : (dir == 1 ? CS_G_YB_QW : CS_G_ZB_QW);
         const int NF = dir == 0 ? CS_G_XF_N : (dir == 1 ? CS_G_YF_N : CS_G_ZF_N);
         const int ns = dir == 2 ? 5 : 1;
-        double dacc = 0.0;
+        R dacc = R(0.0);
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
           const int nq = dir == 2 ? q : 0;
-          const double nx = geo(g, d, NF, nq, 0, fx, fy, fz), ny = geo(g, d, NF, ns + nq, 0, fx, fy, fz),
-                       nz = geo(g, d, NF, 2 * ns + nq, 0, fx, fy, fz);
-          const double x = (geo(g, d, QP, q, 0, fx, fy, fz) - vc0) * obl0;
-          const double y = (geo(g, d, QP, 5 + q, 0, fx, fy, fz) - vc1) * obl0;
-          const double z = (geo(g, d, QP, 10 + q, 0, fx, fy, fz) - vc2) * obl0;
-          const double bfn[10] = {1.0, x, y, z, x * x - c0[4], y * y - c0[5], z * z - c0[6], x * y - c0[7],
-                                  y * z - c0[8], x * z - c0[9]};
-          const double bq = s.Bq[dir][d.at(q, p, fx, fy, fz)];
+          const R nx = geoR<R>(g, d, NF, nq, 0, fx, fy, fz), ny = geoR<R>(g, d, NF, ns + nq, 0, fx, fy, fz),
+                  nz = geoR<R>(g, d, NF, 2 * ns + nq, 0, fx, fy, fz);
+          const R x = (geoR<R>(g, d, QP, q, 0, fx, fy, fz) - vc0) * obl0;
+          const R y = (geoR<R>(g, d, QP, 5 + q, 0, fx, fy, fz) - vc1) * obl0;
+          const R z = (geoR<R>(g, d, QP, 10 + q, 0, fx, fy, fz) - vc2) * obl0;
+          const R bfn[10] = {R(1.0), x, y, z, x * x - c0[4], y * y - c0[5], z * z - c0[6], x * y - c0[7],
+                             y * z - c0[8], x * z - c0[9]};
+          const R bq = (R)s.Bq[dir][d.at(q, p, fx, fy, fz)];
 #pragma unroll
           for (int m = 0; m < 10; ++m) {
             rhs[m] = rhs[m] + (m == 0 ? nx : nx * bfn[m]) * bq;
             rhs[10 + m] = rhs[10 + m] + (m == 0 ? ny : ny * bfn[m]) * bq;
             rhs[20 + m] = rhs[20 + m] + (m == 0 ? nz : nz * bfn[m]) * bq;
           }
-          dacc = dacc + geo(g, d, BW, q, 0, fx, fy, fz) * bq;
+          dacc = dacc + geoR<R>(g, d, BW, q, 0, fx, fy, fz) * bq;
         }
         out[(long long)(30 + f) * n] = dacc;
       }
@@ -1187,7 +1193,7 @@ __global__ void __launch_bounds__(ADPR_TPB, 4) k_adp_rhs6(Dims d, PhysC ph, DGeo
 #pragma unroll
       for (int v = 0; v < 30; ++v) {
         const int u = __ldg(umap + v);
-        out[(long long)u * n] = (double)__ldg(umap + 36 + v) * rhs[v] + Vat(s, d, 5 + u / 10, u % 10, p, i, j, k);
+        out[(long long)u * n] = (R)__ldg(umap + 36 + v) * rhs[v] + Vat(s, d, 5 + u / 10, u % 10, p, i, j, k);
       }
     }
   }
@@ -1241,7 +1247,7 @@ __global__ void __launch_bounds__(ADPS_THREADS, 2) k_adp_solve(Dims d, PhysC ph,
         if (gch >= ADPS_NS) mbar_wait(&S.empty[slot], (uint32_t)(((gch / ADPS_NS) - 1) & 1), s.err_flag);
         const long long it = gch / ADPS_NCH, c = gch % ADPS_NCH;
         const long long blk = blockIdx.x + it * gridDim.x;
-        const double* src = s.adp_lu + (blk * 1296 + c * ADPS_CH) * (long long)ADP_ZB;
+        const double* src = (const double*)s.adp_lu + (blk * 1296 + c * ADPS_CH) * (long long)ADP_ZB;
         mbar_expect_tx(&S.full[slot], ADPS_CH * ADP_ZB * sizeof(double));
         bulk_g2s(&S.stage[slot][0][0], src, ADPS_CH * ADP_ZB * sizeof(double), &S.full[slot]);
       }
@@ -1275,7 +1281,7 @@ __global__ void __launch_bounds__(ADPS_THREADS, 2) k_adp_solve(Dims d, PhysC ph,
     // permuted right-hand side first (36 independent loads), then the
     // substitution in place
 #pragma unroll
-    for (int a = 0; a < 36; ++a) S.y[a][tid] = inr ? s.adp_rhs[(long long)pv[a * ADP_ZB] * n + t] : 0.0;
+    for (int a = 0; a < 36; ++a) S.y[a][tid] = inr ? ((const double*)s.adp_rhs)[(long long)pv[a * ADP_ZB] * n + t] : 0.0;
 #pragma unroll 1
     for (int a = 1; a < 36; ++a) {
       double acc = S.y[a][tid];
@@ -1572,8 +1578,9 @@ constexpr int ADP6_THREADS = ADP6_CONS + 32;
 constexpr int ADP6_CH = 16;
 constexpr int ADP6_NS = 12;
 constexpr int ADP6_NCH = 1296 / ADP6_CH;
-struct Adp6Smem {
-  double stage[ADP6_NS][ADP6_CH][ADP6_ZB];
+template <typename F>
+struct Adp6SmemT {
+  F stage[ADP6_NS][ADP6_CH][ADP6_ZB];
   uint64_t full[ADP6_NS];
   uint64_t empty[ADP6_NS];
 };
@@ -1612,24 +1619,24 @@ static_assert(adp_elem(630).a == 35 && adp_elem(630).b == 35 && adp_elem(631).a 
 // One stream element applied to y in registers (every index a compile-time
 // constant): forward and backward eliminations y[a] -= f y[b], the
 // diagonal y[a] /= f -- the substitution order of the reference.
-template <int E>
-__device__ __forceinline__ void adp6_apply(double (&y)[36], double f) {
+template <int E, typename F>
+__device__ __forceinline__ void adp6_apply(F (&y)[36], F f) {
   constexpr AdpElem x = adp_elem(E);
   if constexpr (x.a == x.b)
     y[x.a] = y[x.a] / f;
   else
     y[x.a] -= f * y[x.b];
 }
-template <int C, int... W>
-__device__ __forceinline__ void adp6_chunk(double (&y)[36], const double* cur, std::integer_sequence<int, W...>) {
+template <int C, typename F, int... W>
+__device__ __forceinline__ void adp6_chunk(F (&y)[36], const F* cur, std::integer_sequence<int, W...>) {
   (adp6_apply<C * ADP6_CH + W>(y, cur[W * ADP6_ZB]), ...);
 }
 // The whole stream of one zone block, chunk by chunk through the ring:
 // release the previous stage, wait for this one, apply its 16 elements.
-template <int... C>
-__device__ __forceinline__ void adp6_substitute(double (&y)[36], Adp6Smem& S, int lane, long long& gch, int* err,
+template <typename F, int... C>
+__device__ __forceinline__ void adp6_substitute(F (&y)[36], Adp6SmemT<F>& S, int lane, long long& gch, int* err,
                                                 std::integer_sequence<int, C...>) {
-  auto acquire = [&]() -> const double* {
+  auto acquire = [&]() -> const F* {
     if (gch > 0) {
       __syncwarp();
       if (lane == 0) mbar_arrive(&S.empty[(int)((gch - 1) % ADP6_NS)]);
@@ -1642,10 +1649,12 @@ __device__ __forceinline__ void adp6_substitute(double (&y)[36], Adp6Smem& S, in
   (adp6_chunk<C>(y, acquire(), std::make_integer_sequence<int, ADP6_CH>{}), ...);
 }
 
+// The factor stream, the right-hand sides and the substitution are in the
+// state's type R (FP32 in the precision form: half the stream's bytes).
 template <typename R>
-__global__ void __launch_bounds__(ADP6_THREADS, 2) k_adp_solve6(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
+__global__ void __launch_bounds__(ADP6_THREADS, sizeof(R) == 4 ? 4 : 2) k_adp_solve6(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
   extern __shared__ __align__(128) unsigned char adp6_raw[];
-  Adp6Smem& S = *reinterpret_cast<Adp6Smem*>(adp6_raw);
+  Adp6SmemT<R>& S = *reinterpret_cast<Adp6SmemT<R>*>(adp6_raw);
   const int tid = threadIdx.x;
   const long long n = r.count(), n1 = n / 6;
   const long long nblk = (n1 + ADP6_ZB - 1) / ADP6_ZB;
@@ -1667,9 +1676,9 @@ __global__ void __launch_bounds__(ADP6_THREADS, 2) k_adp_solve6(Dims d, PhysC ph
         if (gch >= ADP6_NS) mbar_wait(&S.empty[slot], (uint32_t)(((gch / ADP6_NS) - 1) & 1), s.err_flag);
         const long long it = gch / ADP6_NCH, c = gch % ADP6_NCH;
         const long long blk = blockIdx.x + it * gridDim.x;
-        const double* src = s.adp_lu + (blk * 1296 + c * ADP6_CH) * (long long)ADP6_ZB;
-        mbar_expect_tx(&S.full[slot], ADP6_CH * ADP6_ZB * sizeof(double));
-        bulk_g2s(&S.stage[slot][0][0], src, ADP6_CH * ADP6_ZB * sizeof(double), &S.full[slot]);
+        const R* src = (const R*)s.adp_lu + (blk * 1296 + c * ADP6_CH) * (long long)ADP6_ZB;
+        mbar_expect_tx(&S.full[slot], ADP6_CH * ADP6_ZB * sizeof(R));
+        bulk_g2s(&S.stage[slot][0][0], src, ADP6_CH * ADP6_ZB * sizeof(R), &S.full[slot]);
       }
     }
     return;
@@ -1683,12 +1692,12 @@ __global__ void __launch_bounds__(ADP6_THREADS, 2) k_adp_solve6(Dims d, PhysC ph
     const long long t1 = blk * ADP6_ZB + lane, t = p * n1 + t1;
     const bool inr = t1 < n1;
     const int8_t* pv = s.adp_piv + blk * 36 * ADP6_ZB + lane;
-    double y[36];
+    R y[36];
 #pragma unroll
     for (int a = 0; a < 36; ++a) {
       const int v = inr ? pv[a * ADP6_ZB] : 0;
       const int u = __ldg(umap + v);
-      y[a] = inr ? (double)__ldg(smap + v) * s.adp_rhs[(long long)u * n + t] : 0.0;
+      y[a] = inr ? (R)__ldg(smap + v) * ((const R*)s.adp_rhs)[(long long)u * n + t] : R(0.0);
     }
     adp6_substitute(y, S, lane, gch, s.err_flag, std::make_integer_sequence<int, ADP6_NCH>{});
     if (inr) {
@@ -1699,7 +1708,7 @@ __global__ void __launch_bounds__(ADP6_THREADS, 2) k_adp_solve6(Dims d, PhysC ph
 #pragma unroll
         for (int v = 0; v < 30; ++v) {
           const int u = __ldg(umap + v);
-          const double val = (double)__ldg(smap + v) * y[v];
+          const double val = (double)__ldg(smap + v) * (double)y[v];
           Vat(s, d, 5 + u / 10, u % 10, p, i, j, k) = (R)val;
           if (v % 10 == 0) {
             if (u == 0) nb[0] = val;
@@ -1719,6 +1728,88 @@ __global__ void __launch_bounds__(ADP6_THREADS, 2) k_adp_solve6(Dims d, PhysC ph
       }
     }
   }
+}
+
+// STEP 10 (421:9354-9976): min and max over the active interior zones of
+// the 8 primitives (zone values, B from the ADP solve) and of the zone's
+// net face flux of B normalised by the larger of the two sides' |B| and the
+// magnetosonic scale msonic sqrt(4 3.14 rho) (the reference's constant).
+// Min and max do not depend on order: each warp reduces with shuffles and
+// lane 0 folds its 18 values into keys[] by atomicMin / atomicMax on
+// order-preserving integer keys of the doubles.
+__device__ __forceinline__ unsigned long long minmax_key(double v) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+  return (b >> 63) ? ~b : (b | 0x8000000000000000ULL);
+}
+__global__ void k_step10_reset(unsigned long long* keys) {
+  if (threadIdx.x < 18) keys[threadIdx.x] = threadIdx.x < 9 ? ~0ULL : 0ULL;
+}
+template <typename R>
+__global__ void k_step10(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r, unsigned long long* keys) {
+  double mn[9], mx[9];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) {
+    mn[q] = 1.0e30;
+    mx[q] = -1.0e30;
+  }
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
+    int p, i, j, k;
+    r.decode(t, p, i, j, k);
+    if (mask_at(g, d, p, i, j) != 1) continue;
+    double v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      v[q] = (double)Vat(s, d, q, 0, p, i, j, k);
+      mn[q] = fmin(mn[q], v[q]);
+      mx[q] = fmax(mx[q], v[q]);
+    }
+    const double bxp = s.Bxf[d.at(0, p, i, j, k)], bxm = s.Bxf[d.at(0, p, i - 1, j, k)];
+    const double byp = s.Byf[d.at(0, p, i, j, k)], bym = s.Byf[d.at(0, p, i, j - 1, k)];
+    const double bzp = s.Bzf[d.at(0, p, i, j, k)], bzm = s.Bzf[d.at(0, p, i, j, k - 1)];
+    const double a21 = geo(g, d, CS_G_XF_AREA, 0, p, i, j, k) * bxp + geo(g, d, CS_G_YF_AREA, 0, p, i, j, k) * byp +
+                       geo(g, d, CS_G_ZF_AREA, 0, p, i, j, k) * bzp - geo(g, d, CS_G_XF_AREA, 0, p, i - 1, j, k) * bxm -
+                       geo(g, d, CS_G_YF_AREA, 0, p, i, j - 1, k) * bym - geo(g, d, CS_G_ZF_AREA, 0, p, i, j, k - 1) * bzm;
+    const double a11 = v[5] * v[5] + v[6] * v[6] + v[7] * v[7];
+    const double ms = sqrt((ph.gamma * v[4] + ph.ob4pi * a11) / v[0]);
+    const double den = fmax(fmax(sqrt(bxp * bxp + byp * byp + bzp * bzp), sqrt(bxm * bxm + bym * bym + bzm * bzm)),
+                            ms * sqrt(4.0 * 3.14 * v[0]));
+    const double dv = a21 / den;
+    mn[8] = fmin(mn[8], dv);
+    mx[8] = fmax(mx[8], dv);
+  }
+#pragma unroll
+  for (int q = 0; q < 9; ++q) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      mn[q] = fmin(mn[q], __shfl_xor_sync(0xffffffffu, mn[q], o));
+      mx[q] = fmax(mx[q], __shfl_xor_sync(0xffffffffu, mx[q], o));
+    }
+  }
+  if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+      atomicMin(keys + q, minmax_key(mn[q]));
+      atomicMax(keys + 9 + q, minmax_key(mx[q]));
+    }
+  }
+}
+
+template <typename R>
+void launch_step10_t(Solve& sv, DStateT<R>& st) {
+  const Dims& d = sv.d;
+  Range3 z = {1, d.N, 1, d.N, 1, d.nr};
+  k_step10_reset<<<1, 32, 0, sv.stream>>>(sv.step10_keys);
+  mark(sv, "k_step10_reset");
+  k_step10<R><<<blocks_for(z.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, z, sv.step10_keys);
+  mark(sv, "k_step10");
+}
+
+void launch_step10(Solve& sv) {
+  if (!sv.step10_keys) return;
+  if (sv.fp32)
+    launch_step10_t(sv, sv.stF);
+  else
+    launch_step10_t(sv, sv.st);
 }
 
 template <typename R>
@@ -1833,8 +1924,8 @@ void launch_faceB_adp_t(Solve& sv, DStateT<R>& st) {
                                                                                                   a);
     mark(sv, "k_adp_rhs6");
     const long long nblk = (a.count() / 6 + ADP6_ZB - 1) / ADP6_ZB;
-    const int grid = (int)std::min<long long>(nblk, (long long)grid_sms(sv) * 2);
-    k_adp_solve6<R><<<grid, ADP6_THREADS, sizeof(Adp6Smem), sv.stream>>>(d, sv.ph, sv.g, st, a);
+    const int grid = (int)std::min<long long>(nblk, (long long)grid_sms(sv) * (sizeof(R) == 4 ? 4 : 2));
+    k_adp_solve6<R><<<grid, ADP6_THREADS, sizeof(Adp6SmemT<R>), sv.stream>>>(d, sv.ph, sv.g, st, a);
     mark(sv, "k_adp_solve6");
     return;
   }
@@ -1896,8 +1987,9 @@ void set_adp_smem_limits() {
   const int smem = (int)(sizeof(AdpSmem) * ADP_WARPS);
   cudaFuncSetAttribute(k_adp_solve<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(AdpsSmem));
   cudaFuncSetAttribute(k_adp_solve<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(AdpsSmem));
-  cudaFuncSetAttribute(k_adp_solve6<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Adp6Smem));
-  cudaFuncSetAttribute(k_adp_solve6<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Adp6Smem));
+  cudaFuncSetAttribute(k_adp_solve6<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(Adp6SmemT<double>));
+  cudaFuncSetAttribute(k_adp_solve6<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Adp6SmemT<float>));
   cudaFuncSetAttribute(k_adp<false, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   cudaFuncSetAttribute(k_adp<true, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   cudaFuncSetAttribute(k_adp<false, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);

@@ -27,10 +27,9 @@ size_t state_device_bytes(const cs_params& p) {
   const size_t S6 = (size_t)6 * b.size();
   // words per point of the state's type: U 8 + entropy 4, V 80 + E 30 +
   // E snapshot 3, flattener 3, face contributions 48, entropy fluxes 3,
-  // speeds 6, dU/dt 8, U0 8, ent0 1, face states 270 (IMEX: + 11);
-  // FP64 in both forms: face B 3, face-B quadrature 15, EMFs 3, saved
-  // faces 3 (IMEX: + 3)
-  size_t rwords = 12 + 113 + 3 + 48 + 3 + 6 + 8 + 8 + 1 + 270;
+  // speeds 6, dU/dt 8, U0 8, ent0 1 (IMEX: + 11); FP64 in both forms:
+  // face B 3, face-B quadrature 15, EMFs 3, saved faces 3 (IMEX: + 3)
+  size_t rwords = 12 + 113 + 3 + 48 + 3 + 6 + 8 + 8 + 1;
   size_t dwords = 3 + 15 + 3 + 3;
   if (p.rk_scheme == CS_IMEX_RK2) {
     rwords += 11;
@@ -41,7 +40,11 @@ size_t state_device_bytes(const cs_params& p) {
   // ghost staging values (one per map entry, see mesh_device_bytes)
   bytes += (size_t)6 * 4 * (p.nghost + 1) * (p.ntp + 2 * p.nghost + 1) * (p.nr + 2 * p.nghost + 1) * 12 * 8;
   const size_t na = (size_t)6 * (p.ntp + 2 * p.nghost - 2) * (p.ntp + 2 * p.nghost - 2) * (p.nr + 2 * p.nghost - 2);
-  if (!(p.flags & CS_FLAG_NO_ADP_CACHE)) bytes += na * 36 * sizeof(double);  // ADP right-hand sides
+  if (!(p.flags & CS_FLAG_NO_ADP_CACHE)) {
+    // ADP right-hand sides: the state's type with panel-shared factors
+    const size_t esz = (p.flags & CS_FLAG_ADP_PER_PANEL) ? sizeof(double) : rsize;
+    bytes += na * 36 * esz;
+  }
   return bytes + ((size_t)64 << 20);
 }
 
@@ -63,9 +66,12 @@ size_t mesh_device_bytes(const cs_params& p) {
     bytes += (n9 * 162 + n10 * 190) * (f32 ? sizeof(float) : sizeof(double));
   }
   if (!(p.flags & CS_FLAG_NO_ADP_CACHE)) {
-    // factors shared by the six panels unless per-panel ones are asked for
-    const size_t nz = (p.flags & CS_FLAG_ADP_PER_PANEL) ? na : na / 6;
-    bytes += (nz + 128) * (1296 * 8 + 36);
+    // factors shared by the six panels (in the state's type) unless
+    // per-panel ones (FP64) are asked for
+    const bool per = (p.flags & CS_FLAG_ADP_PER_PANEL) != 0;
+    const size_t nz = per ? na : na / 6;
+    const size_t esz = (per || !(p.flags & CS_FLAG_FP32)) ? sizeof(double) : sizeof(float);
+    bytes += (nz + 128) * (1296 * esz + 36);
   }
   return bytes + ((size_t)64 << 20);
 }

@@ -62,7 +62,7 @@ struct MeshRes {
   void* op_m10 = nullptr;
   void* lsq_map = nullptr;  // LsqPanelMap[6] when row weights are panel 1's only
   bool m9_shared = false, m10_shared = false;  // which of op_m9 / op_m10 are panel 1's only
-  double* adp_lu = nullptr;
+  void* adp_lu = nullptr;   // FP64 per panel; panel-shared ones in the state's type
   int8_t* adp_piv = nullptr;
   int8_t* adp_pmap = nullptr;  // ADP factors shared by the panels: per panel [unknown map][sign]
   std::vector<void*> allocs;
@@ -93,6 +93,7 @@ struct Solve {
   unsigned char* init_buf = nullptr;  // seeded harmonic terms of cs_init_problem
   size_t init_buf_bytes = 0;
   double* diag_buf = nullptr;         // cs_diag: result and partial sums
+  unsigned long long* step10_keys = nullptr;  // STEP 10 min (9) and max (9) keys, with CS_FLAG_STEP10
   int device = 0;
   int sm_count = 148;
   bool has_mesh = false, has_state = false;

@@ -109,10 +109,13 @@ typedef struct cs_params {
 #define CS_FLAG_NO_PANEL_SYNC 4
 /* cs_params.flags: the precision form.  The bulk of the stage (conserved
  * state, entropy, primitives and their modes, the flattener, face states and
- * fluxes, dU/dt, the stage copies, the resident least-squares inverses) is
- * stored and computed in FP32; face B, its quadrature values, the ADP
- * system and its factors, the edge EMFs and the geometry stay FP64, so the
- * CT update keeps div B at FP64 round-off.
+ * fluxes, dU/dt, the stage copies, the resident least-squares inverses, the
+ * face-B quadrature evaluations and the ADP constrained least squares:
+ * right-hand sides, panel-shared factors, substitution) is stored and
+ * computed in FP32; the geometry, face B, the shift of the quadrature
+ * values to the FP64 face mean, the ADP factorisation itself (stored
+ * rounded), the edge EMFs, the CT update, the positivity fix and the
+ * global reductions stay FP64, so div B stays at FP64 round-off.
  * The WENO nonlinear weights are formed in FP64.  The reference has no
  * such form (it computes everything in REAL*8); the state read and written
  * through cs_state_get / cs_state_put stays FP64 at the boundary. */
@@ -142,6 +145,15 @@ typedef struct cs_params {
  * results agree with per-panel weights to round-off.  This flag restores
  * per-panel weights; meshes without the symmetry use them anyway. */
 #define CS_FLAG_LSQ_PER_PANEL 32
+
+/* cs_params.flags: evaluate STEP 10 of LIMIT_ALL_SLOPES_P12 (421:9354-9976)
+ * in every stage: the min and max over the active interior zones of the 8
+ * primitives and of the normalised zone divergence of B, read back with
+ * cs_limit_minmax (the V_min_local / V_max_local the reference driver
+ * reduces and prints each step, 1000riemann_geomesh_cs_mhd.f:2442-2448,
+ * 3149-3179).  Off by default: the reference bypasses it on the GPU; on
+ * it costs one reduction over the interior per stage. */
+#define CS_FLAG_STEP10 64
 
 /* Seeded initial-state description (new generator cases of the problem
  * library, built with the reference mechanism of 820init_patch_cube_sphere.f). */
@@ -234,6 +246,22 @@ int cs_state_put(cs_ctx* ctx, const double* U, const double* ent,
                  const double* bxf, const double* byf, const double* bzf);
 int cs_state_get(cs_ctx* ctx, double* U, double* ent,
                  double* bxf, double* byf, double* bzf);
+
+/* The same state in the reference driver's own module arrays, passed
+ * unchanged (300riemann_module_3d.f:495-530, one patch per panel, patch
+ * p+1 = panel p, Fortran column-major with their lower bounds):
+ *   U_amr(1-G:N+G, 1-G:N+G, 1-G:nr+G, n_cc_components, 6)
+ *   entropygr_amr(1-G:N+G, 1-G:N+G, 1-G:nr+G, 6)
+ *   Bxf_amr, Byf_amr, Bzf_amr(0-G:N+G, 0-G:N+G, 0-G:nr+G, 6)
+ * with G = nghost, N = ntp.  n_cc_components >= 8: the 8 ideal-MHD
+ * components are read and written, further ones (passive species) are
+ * ignored by put and left untouched by get.  The face arrays' boxes are the
+ * panel boxes above; the zone arrays lack the panel box's lower layer
+ * (index -G), which put leaves zero. */
+int cs_state_put_amr(cs_ctx* ctx, int32_t n_cc_components, const double* U_amr, const double* entropygr_amr,
+                     const double* Bxf_amr, const double* Byf_amr, const double* Bzf_amr);
+int cs_state_get_amr(cs_ctx* ctx, int32_t n_cc_components, double* U_amr, double* entropygr_amr, double* Bxf_amr,
+                     double* Byf_amr, double* Bzf_amr);
 
 /* Whole-stage and whole-step entry points (device resident, on ctx's stream). */
 int cs_stage(cs_ctx* ctx, int32_t irk, double dtcur);
@@ -392,6 +420,17 @@ int cs_batch_destroy(cs_batch* b);
  * Bneta_2, Bneta_3).  out[n] = ESSz, evaluated on the current device. */
 int cs_twod_rs_ez(int32_t kind, int32_t n, const double* in, double* out);
 
+/* V_min_local / V_max_local of the last LIMIT_ALL_SLOPES_P12 of the context
+ * (STEP 10, 421:9354-9976; needs CS_FLAG_STEP10): v_min[0..7] / v_max[0..7]
+ * the min / max over the active interior zones of the primitives (rho,
+ * v_x, v_y, v_z, p, B_x, B_y, B_z; the zone values the stage reconstructs,
+ * B from the ADP solve), v_min[8] / v_max[8] those of the zone's net face
+ * flux of B divided by max(|B| on its upper faces, |B| on its lower faces,
+ * msonic sqrt(4 x 3.14 x rho)).  After a step these are the last stage's,
+ * the values the reference driver prints for that step.  CS_ERR_STATE
+ * without the flag or before the first stage. */
+int cs_limit_minmax(cs_ctx* ctx, double* v_min, double* v_max);
+
 /* Known-answer access to the pointwise physics of the stage kernels,
  * evaluated on the current device in the state type of the form that
  * p->flags selects (FP64, or FP32 with CS_FLAG_FP32), with the physics
@@ -404,6 +443,13 @@ int cs_twod_rs_ez(int32_t kind, int32_t n, const double* in, double* out);
  * Fluct_R[8], F_L[8], F_R[8], S_L, S_R, entropy flux).  The reference's
  * _T/_660riemann_3d/660pde_3d_test_program.f:58-142 runs kind 0 then 1. */
 int cs_pointwise(const cs_params* p, int32_t kind, int32_t n, const double* in, double* out);
+
+/* Measured FP64 fused multiply-add rate of the current device in TFLOP/s
+ * (2 flops per FMA): 8 blocks per SM of 256 threads, each running 8
+ * independent FMA chains for iters x 16 steps, timed with CUDA events after
+ * a warm-up launch.  The denominator of the FP64 roofline; no counterpart
+ * in the reference. */
+int cs_fp64_fma_rate(int32_t iters, double* tflops);
 
 /* Diagnostics: sums over interior zones of 6 panels of volume-weighted
  * mass, energy and the max |div B| (face-area-weighted, per volume),

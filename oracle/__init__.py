@@ -45,6 +45,7 @@ def load() -> ctypes.CDLL:
         "oracle_get_geometry": ([P, ctypes.c_int, dp], None),
         "oracle_get_mask_stencil": ([P, ip, ip], None),
         "oracle_pointwise": ([P, ctypes.c_int, ctypes.c_int, dp, dp], ctypes.c_int),
+        "oracle_limit_minmax": ([P, dp, dp], ctypes.c_int),
     }
     for n in ("oracle_fill_ghosts", "oracle_limit_all_slopes_p12", "oracle_make_facial_fluxes",
               "oracle_make_edge_efields", "oracle_build_non_stiff_sources", "oracle_cleanup"):
@@ -135,6 +136,12 @@ class Oracle:
         out = np.zeros((a.shape[0], nout))
         assert self.lib.oracle_pointwise(self.h, kind, a.shape[0], _d(a), _d(out)) == 0
         return out
+
+    def limit_minmax(self):
+        """STEP 10 of the last LIMIT_ALL_SLOPES_P12: (v_min[9], v_max[9])."""
+        vmin, vmax = np.zeros(9), np.zeros(9)
+        assert self.lib.oracle_limit_minmax(self.h, _d(vmin), _d(vmax)) == 0
+        return vmin, vmax
 
     def init_problem(self, desc) -> None:
         """The seeded initial state of a ``cubesphere_b200.CsInitDesc``."""

@@ -52,6 +52,9 @@ struct Ctx {
       SUy, SBz, STz, EFx, EFy, EFz, Efx, Efy, Efz, U0, ent0, Bxf0, Byf0, Bzf0;
   // STEP 7.c record per zone: 2 x shrink passes + 1 where the zone gave up
   std::vector<double> pos;
+  // STEP 10 per panel: min and max of the 8 primitives and the divergence
+  double vmin[6][NV + 1], vmax[6][NV + 1];
+  bool step10 = false;
   // IMEX: the first stage's dU/dt, entropy fluxes and EMFs
   std::vector<double> K1, EFx1, EFy1, EFz1, Efx1, Efy1, Efz1;
   double time = 0.0;
@@ -1031,6 +1034,37 @@ void limit_all_slopes_p12(Ctx& c, int pn) {
           for (int t = 0; t < 10; ++t) E(q, t, i, j, k) = e[t];
         }
       }
+  // STEP 10 (:9354-9976): min and max over the active interior zones of the
+  // zone primitives (B from STEP 8.d) and of the zone's net face flux of B
+  // over max(|B| of the upper faces, |B| of the lower faces,
+  // msonic sqrt(4 x 3.14 x rho)), with msonic from these primitives.
+  for (int q = 0; q <= NV; ++q) {
+    c.vmin[pn][q] = 1.0e30;
+    c.vmax[pn][q] = -1.0e30;
+  }
+  for (int k = 1; k <= nr; ++k)
+    for (int j = 1; j <= N; ++j)
+      for (int i = 1; i <= N; ++i) {
+        if (c.m(pn, i, j) != 1) continue;
+        for (int q = 0; q < NV; ++q) {
+          c.vmin[pn][q] = std::min(c.vmin[pn][q], V(q, 0, i, j, k));
+          c.vmax[pn][q] = std::max(c.vmax[pn][q], V(q, 0, i, j, k));
+        }
+        auto B = [&](std::vector<double>& f, int x, int y, int z) { return c.a(f, 0, pn, x, y, z); };
+        double a21 = c.geo(XF_AREA, 0, pn, i, j, k) * B(c.Bxf, i, j, k) + c.geo(YF_AREA, 0, pn, i, j, k) * B(c.Byf, i, j, k) +
+                     c.geo(ZF_AREA, 0, pn, i, j, k) * B(c.Bzf, i, j, k) -
+                     c.geo(XF_AREA, 0, pn, i - 1, j, k) * B(c.Bxf, i - 1, j, k) -
+                     c.geo(YF_AREA, 0, pn, i, j - 1, k) * B(c.Byf, i, j - 1, k) -
+                     c.geo(ZF_AREA, 0, pn, i, j, k - 1) * B(c.Bzf, i, j, k - 1);
+        double a11 = sq(V(5, 0, i, j, k)) + sq(V(6, 0, i, j, k)) + sq(V(7, 0, i, j, k));
+        double ms = std::sqrt((g * V(4, 0, i, j, k) + c.ph.ob4pi * a11) / V(0, 0, i, j, k));
+        a21 = a21 / std::max({std::sqrt(sq(B(c.Bxf, i, j, k)) + sq(B(c.Byf, i, j, k)) + sq(B(c.Bzf, i, j, k))),
+                              std::sqrt(sq(B(c.Bxf, i - 1, j, k)) + sq(B(c.Byf, i, j - 1, k)) + sq(B(c.Bzf, i, j, k - 1))),
+                              ms * std::sqrt(4.0 * 3.14 * V(0, 0, i, j, k))});
+        c.vmin[pn][NV] = std::min(c.vmin[pn][NV], a21);
+        c.vmax[pn][NV] = std::max(c.vmax[pn][NV], a21);
+      }
+  c.step10 = true;
 }
 
 // ------------------------------------------------------------------
@@ -2096,6 +2130,22 @@ double oracle_step(void* h, double dtcur) {
   for (int irk = 1; irk <= ns; ++irk) stage(*c, irk, dtcur);
   c->time += dtcur;
   return evaluate_timestep(*c, dtcur);
+}
+
+// STEP 10 of the last LIMIT_ALL_SLOPES_P12 over the six panels (the
+// driver's reduction over patches, 1000riemann_geomesh_cs_mhd.f:2447-2448).
+int oracle_limit_minmax(void* h, double* vmin, double* vmax) {
+  const Ctx* c = (const Ctx*)h;
+  if (!c->step10) return 1;
+  for (int q = 0; q <= NV; ++q) {
+    vmin[q] = 1.0e32;
+    vmax[q] = -1.0e32;
+    for (int pn = 0; pn < 6; ++pn) {
+      vmin[q] = std::min(vmin[q], c->vmin[pn][q]);
+      vmax[q] = std::max(vmax[q], c->vmax[pn][q]);
+    }
+  }
+  return 0;
 }
 
 // The pointwise physics on n cases, with the solve's constants; the same

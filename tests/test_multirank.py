@@ -50,7 +50,7 @@ def test_reference_arm_under_two_ranks_prints_one_line():
     port = 29700 + os.getpid() % 1000
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
            "--master-addr", "127.0.0.1", "--master-port", str(port), str(ROOT / "bench.py"),
-           "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "0"]
+           "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "0", "--workload", "shell16"]
     r = subprocess.run(cmd, capture_output=True, text=True, timeout=600, cwd=ROOT)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]

@@ -244,3 +244,53 @@ def test_positivity_shrinks_and_gives_up_on_the_blob_state():
     assert counts[0] == (0, 0)
     shrunk, gave_up = counts[1]
     assert shrunk >= 10 and gave_up >= 1, counts
+
+
+def step10_numpy(s, V, st):
+    """STEP 10 (421:9354-9976) restated with numpy from the zone primitives V
+    (mode 0 of the reconstruction) and the face field of the state."""
+    G, N, nr = s.G, s.N, s.nr
+    act = s.interior(s.mask() == 1)
+    v = [s.interior(V[q]) for q in range(8)]
+    vmin = [float(x[act].min()) for x in v]
+    vmax = [float(x[act].max()) for x in v]
+    A = [s.geometry(n)[0] for n in ("XF_AREA", "YF_AREA", "ZF_AREA")]
+    B = [st[k][0] for k in ("bxf", "byf", "bzf")]
+
+    def sl(a, di, dj, dk):
+        return a[:, G + 1 + dk:G + nr + 1 + dk, G + 1 + dj:G + N + 1 + dj, G + 1 + di:G + N + 1 + di]
+
+    up = [sl(B[0], 0, 0, 0), sl(B[1], 0, 0, 0), sl(B[2], 0, 0, 0)]
+    lo = [sl(B[0], -1, 0, 0), sl(B[1], 0, -1, 0), sl(B[2], 0, 0, -1)]
+    a21 = (sl(A[0], 0, 0, 0) * up[0] + sl(A[1], 0, 0, 0) * up[1] + sl(A[2], 0, 0, 0) * up[2] -
+           sl(A[0], -1, 0, 0) * lo[0] - sl(A[1], 0, -1, 0) * lo[1] - sl(A[2], 0, 0, -1) * lo[2])
+    gam = s.params.gamma
+    with np.errstate(invalid="ignore", divide="ignore"):
+        ms = np.sqrt((gam * v[4] + (v[5] ** 2 + v[6] ** 2 + v[7] ** 2) / (4 * np.pi)) / v[0])
+        den = np.maximum(np.maximum(np.sqrt(sum(b * b for b in up)), np.sqrt(sum(b * b for b in lo))),
+                         ms * np.sqrt(4 * 3.14 * v[0]))
+        dv = a21 / den
+    return np.array(vmin + [float(dv[act].min())]), np.array(vmax + [float(dv[act].max())]), float(
+        np.abs(sl(A[0], 0, 0, 0)).max())
+
+
+def test_step10_min_max_of_the_oracle():
+    """The oracle's STEP 10 against the same quantities in numpy, on the
+    reconstruction of the seeded shell (B after the ADP solve)."""
+    pr = cs.preset("shell16")
+    s = cs.Solve(**pr["params"])
+    s.mesh_build(device=False)
+    st = s.init_problem_host(**pr["init"])
+    o = Oracle(s)
+    o.put_state(st)
+    o.fill_ghosts()
+    o.limit_all_slopes_p12()
+    vmin, vmax = o.limit_minmax()
+    wmin, wmax, area = step10_numpy(s, o.debug("V"), o.get_state())
+    scale = np.maximum(np.abs(wmin), np.abs(wmax))
+    np.testing.assert_allclose(vmin[:8], wmin[:8], rtol=0, atol=1e-14 * scale[:8].max())
+    np.testing.assert_allclose(vmax[:8], wmax[:8], rtol=0, atol=1e-14 * scale[:8].max())
+    assert vmin[0] > 0 and vmin[4] > 0  # density and pressure
+    # the divergence entries are round-off of a divergence-free field
+    assert abs(vmin[8]) < 1e-12 * area and abs(vmax[8]) < 1e-12 * area
+    assert abs(vmin[8] - wmin[8]) < 1e-13 * area and abs(vmax[8] - wmax[8]) < 1e-13 * area
