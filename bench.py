@@ -137,6 +137,10 @@ def parse():
                     help="also run the precision form against FP64 over --precision-steps steps of this workload "
                          "(shell256: the 6x256^2x128 statement) and report errors and both forms' times")
     ap.add_argument("--precision-steps", type=int, default=200)
+    ap.add_argument("--stated-batch", action="store_true",
+                    help="the batched form at its stated size: 64 solves, N in {32..128}, depth in {1..64}")
+    ap.add_argument("--stated-serving", action="store_true",
+                    help="the serving form at its stated sizes: N in {32..128}, depth in {1..64}, 20-500 steps")
     return ap.parse_args()
 
 
@@ -271,15 +275,18 @@ def cpu_baseline_sample(name: str, steps: int = 1, warmup: int = 0, budget_s: fl
             "steps_timed": done, "seconds": sec}
 
 
-def serving_sample(seed: int = 7, nreq: int = 24, rate: float = 8.0, max_active: int = 8) -> dict:
-    """Serving form on a bounded sample: Poisson arrivals (seeded rate) of
-    solve requests with panel N from {32, 48, 64}, radial depth from
-    {1, 16, 32} and 20..60 steps, admitted by free device memory into the
-    concurrent server (meshes cached between requests), in the plain FP64
-    form and in the precision form; then the FP64 requests run one at a time
-    (the plain path run sequentially, all submitted at once) for the
-    throughput comparison.  Throughput = zone updates / (last completion -
-    first submission); a fresh server per run, so mesh builds are inside."""
+def serving_sample(seed: int = 7, nreq: int = 24, rate: float = 8.0, max_active: int = 8,
+                   sizes=(32, 48, 64), depths=(1, 16, 32), step_range=(20, 60)) -> dict:
+    """Serving form: Poisson arrivals (seeded rate) of solve requests with
+    panel N from `sizes`, radial depth from `depths` and a step count in
+    `step_range`, admitted by free device memory into the concurrent server
+    (meshes cached between requests), in the plain FP64 form and in the
+    precision form; then the FP64 requests run one at a time (the plain path
+    run sequentially, all submitted at once) for the throughput comparison.
+    Throughput = zone updates / (last completion - first submission); a
+    fresh server per run, so mesh builds are inside.  The defaults are a
+    bounded sample; the stated configuration draws N from {32, 48, 64, 96,
+    128}, depth from {1, 16, 32, 64} and 20..500 steps."""
     import numpy as np
 
     import cubesphere_b200 as cs
@@ -287,9 +294,9 @@ def serving_sample(seed: int = 7, nreq: int = 24, rate: float = 8.0, max_active:
     rng = np.random.default_rng(seed)
     reqs = []
     for _ in range(nreq):
-        ntp = int(rng.choice([32, 48, 64]))
-        nr = int(rng.choice([1, 16, 32]))
-        steps = int(rng.integers(20, 61))
+        ntp = int(rng.choice(list(sizes)))
+        nr = int(rng.choice(list(depths)))
+        steps = int(rng.integers(step_range[0], step_range[1] + 1))
         pr = cs.preset("shell16")
         params = dict(pr["params"])
         init = dict(pr["init"])
@@ -324,35 +331,47 @@ def serving_sample(seed: int = 7, nreq: int = 24, rate: float = 8.0, max_active:
             "zone_updates": int(sum(6 * p["ntp"] ** 2 * p["nr"] * n for n, p, _ in reqs)),
             "f64": f64, "f32_precision_form": f32, "f64_sequential": seq,
             "f32_vs_f64_sequential": f32["zone_updates_per_s"] / max(seq["zone_updates_per_s"], 1e-30),
-            "sizes": "N in {32,48,64}, nr in {1,16,32}, 20-60 steps (IMEX-RK2 shells, SSP-RK3 surfaces); "
-                     "latency = submission to completion, mesh builds included"}
+            "sizes": f"N in {set(sizes)}, nr in {set(depths)}, {step_range[0]}-{step_range[1]} steps "
+                     "(IMEX-RK2 shells, SSP-RK3 surfaces); latency = submission to completion, mesh builds included"}
 
 
-def batch_sample(seed: int = 11, nsol: int = 16, steps: int = 4) -> dict:
-    """Batched form on a bounded sample: nsol independent solves with panel N
-    from {32, 48, 64} and radial depth from {1, 16, 32} (seeded), in the
-    precision form, advanced together (one graph launch per step, launch
-    shapes autotuned per size class) and, for comparison, one after another
+def batch_sample(seed: int = 11, nsol: int = 16, steps: int = 4, sizes=(32, 48, 64), depths=(1, 16, 32),
+                 mem_fraction: float = 0.85, autotune: bool = True) -> dict:
+    """Batched form: nsol independent solves with panel N from `sizes` and
+    radial depth from `depths` (seeded; depth 1 is the surface workload,
+    SSP-RK3, the others the shell, IMEX-RK2), in the precision form, created
+    in draw order while the device's free memory holds them (mem_fraction of
+    what was free at the start; solves on equal meshes share one resident
+    mesh), advanced together (one graph launch per step, launch shapes
+    autotuned per size class) and, for comparison, one after another
     (cs_steps per member), each over `steps` steps, timed by the host clock
-    around calls that return after the device work has finished; solves on
-    equal meshes share one resident mesh."""
+    around calls that return after the device work has finished.  The
+    defaults are a bounded sample; the stated configuration draws 64 solves
+    with N from {32, 48, 64, 96, 128} and depth from {1, 16, 32, 64}."""
     import numpy as np
     import torch
 
     import cubesphere_b200 as cs
 
     rng = np.random.default_rng(seed)
-    sols, meshes = [], {}
-    for q in range(nsol):
-        ntp = int(rng.choice([32, 48, 64]))
-        nr = int(rng.choice([1, 16, 32]))
+    draws = [(int(rng.choice(list(sizes))), int(rng.choice(list(depths))), int(rng.integers(1, 1 << 30)))
+             for _ in range(nsol)]
+    budget = mem_fraction * torch.cuda.mem_get_info()[0]
+    used0 = torch.cuda.mem_get_info()[0]
+    sols, meshes, skipped = [], {}, 0
+    t_setup = time.perf_counter()
+    for ntp, nr, sd in draws:
         pr = cs.preset("shell16")
         params, init = dict(pr["params"]), dict(pr["init"])
         params.update(ntp=ntp, nr=nr, nghost=4 if nr > 1 else 3, flags=cs.CS_FLAG_FP32)
-        init.update(seed=int(rng.integers(1, 1 << 30)))
+        init.update(seed=sd)
         if nr == 1:
             params.update(gm=0.0, rmin=1.0, rmax=1.05, radial_mesh="uniform", rk_scheme=cs.CS_SSPRK3)
             init.update(kind=0, v_amp=0.5, p0=1.0, rho_amp=0.1, a_amp=0.1)
+        need = cs.estimate_device_bytes(**params)
+        if (used0 - torch.cuda.mem_get_info()[0]) + need > budget:
+            skipped += 1  # the device is full: the solve is not admitted to this batch
+            continue
         s = cs.Solve(**params)
         if (ntp, nr) in meshes:
             s.mesh_share(meshes[(ntp, nr)])
@@ -361,13 +380,15 @@ def batch_sample(seed: int = 11, nsol: int = 16, steps: int = 4) -> dict:
             meshes[(ntp, nr)] = s
         s.init_problem(**init)
         sols.append(s)
+    t_setup = time.perf_counter() - t_setup
     zones = sum(6 * s.N * s.N * s.nr for s in sols)
     dts = [s.evaluate_timestep(1e30) for s in sols]
     b = cs.Batch(sols)
     t_tune = time.perf_counter()
-    b.autotune(1)
+    if autotune:
+        b.autotune(1)
     t_tune = time.perf_counter() - t_tune
-    fr = sorted({b.grid_fraction(q) for q in range(nsol)})
+    fr = sorted({b.grid_fraction(q) for q in range(len(sols))})
     dts = b.steps(1, dts)  # warm-up: builds the batch graph
     torch.cuda.synchronize()
     # every call below returns after reading the members' next time steps,
@@ -382,11 +403,13 @@ def batch_sample(seed: int = 11, nsol: int = 16, steps: int = 4) -> dict:
     ok = all(np.isfinite(d) and d > 0 for d in dts)
     for s in sols:
         s.close()
-    return {"solves": nsol, "zones": zones, "steps": steps, "dtype": "f32 bulk (precision form)",
+    return {"solves_drawn": nsol, "solves": len(sols), "not_admitted": skipped, "zones": zones, "steps": steps,
+            "dtype": "f32 bulk (precision form)",
             "batched_zone_updates_per_s": zones * steps / bat_s,
             "sequential_zone_updates_per_s": zones * steps / seq_s,
-            "autotune_s": t_tune, "grid_fractions_chosen": fr, "distinct_meshes": len(meshes), "finite": ok,
-            "sizes": "N in {32,48,64}, nr in {1,16,32}; host wall clock around the device-synchronised runs"}
+            "setup_s": t_setup, "autotune_s": t_tune, "grid_fractions_chosen": fr, "distinct_meshes": len(meshes),
+            "finite": ok,
+            "sizes": f"N in {set(sizes)}, nr in {set(depths)}; host wall clock around the device-synchronised runs"}
 
 
 def precision_sample(pr, dts, steps, ref_state, zones, world, allmax) -> dict:
@@ -719,11 +742,18 @@ def run_gpu(args):
         torch.cuda.synchronize()
         precision_stated = precision_long_sample(args.precision_workload, args.precision_steps, timed=True)
     batch = None
-    if not args.no_batch:
+    if args.stated_batch:
+        torch.cuda.synchronize()
+        batch = batch_sample(seed=11, nsol=64, steps=2, sizes=(32, 48, 64, 96, 128), depths=(1, 16, 32, 64))
+    elif not args.no_batch:
         torch.cuda.synchronize()
         batch = batch_sample()
     serving = None
-    if not args.no_serving:
+    if args.stated_serving:
+        torch.cuda.synchronize()
+        serving = serving_sample(seed=7, nreq=24, rate=2.0, max_active=8, sizes=(32, 48, 64, 96, 128),
+                                 depths=(1, 16, 32, 64), step_range=(20, 500))
+    elif not args.no_serving:
         torch.cuda.synchronize()
         serving = serving_sample()
 

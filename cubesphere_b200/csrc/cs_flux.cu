@@ -250,13 +250,21 @@ __global__ void __launch_bounds__(FLUX_FACES * 5, sizeof(R) == 4 ? 7 : 4) k_flux
                      ec = a == 0 ? Cx : (a == 1 ? Cy : Cz);
         return ea * W[o] + eb * W[o + 1] + ec * W[o + 2];
       };
-      // area / volume once per side (the reference divides every term; the
-      // products differ from it in the last bit only)
+      // the two sides' net contributions (fluctuation + flux) summed in the
+      // face frame and rotated back once, and area / volume once per side
+      // (the reference rotates each term and divides every term; the
+      // results differ from it in the last bits only)
+      R GL[8], GR[8];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        GL[c] = FlL[c] + FL[c];
+        GR[c] = FlR[c] - FR[c];
+      }
       const R aL = area / volL, aR = area / volR;
 #pragma unroll
       for (int c = 0; c < 8; ++c) {
-        red[jq][c][lane] = wt * (back(FlL, c) + back(FL, c)) * aL;
-        red[jq][8 + c][lane] = wt * (back(FlR, c) - back(FR, c)) * aR;
+        red[jq][c][lane] = wt * back(GL, c) * aL;
+        red[jq][8 + c][lane] = wt * back(GR, c) * aR;
       }
     }
     __syncthreads();

@@ -234,105 +234,169 @@ __device__ __forceinline__ Nbr12 load_nbr(const DGeom& g, const Dims& d, int p, 
   return n;
 }
 
-template <typename R>
-__device__ void stencil_inv(const Dims& d, const PhysC& ph, const DGeom& g, int p, int i, int j, int k, const Nbr12& n,
-                            R Ai[8][9]) {
-  const R obl0 = R(1.0) / fmax(geoR<R>(g, d, CS_G_V_SCALE, 0, p, i, j, k), R(ph.smallnum));
-  const R cx = geoR<R>(g, d, CS_G_V_CEN, 0, p, i, j, k), cy = geoR<R>(g, d, CS_G_V_CEN, 1, p, i, j, k),
-               cz = geoR<R>(g, d, CS_G_V_CEN, 2, p, i, j, k);
-#pragma unroll
-  for (int st = 0; st < 8; ++st) {
-    const int w1 = c_st8[st][0], w2 = c_st8[st][1], dz = c_st8[st][2];
-    const R a11 = (geoR<R>(g, d, CS_G_V_CEN, 0, p, n.x[w1], n.y[w1], k) - cx) * obl0;
-    const R a12 = (geoR<R>(g, d, CS_G_V_CEN, 1, p, n.x[w1], n.y[w1], k) - cy) * obl0;
-    const R a13 = (geoR<R>(g, d, CS_G_V_CEN, 2, p, n.x[w1], n.y[w1], k) - cz) * obl0;
-    const R a21 = (geoR<R>(g, d, CS_G_V_CEN, 0, p, n.x[w2], n.y[w2], k) - cx) * obl0;
-    const R a22 = (geoR<R>(g, d, CS_G_V_CEN, 1, p, n.x[w2], n.y[w2], k) - cy) * obl0;
-    const R a23 = (geoR<R>(g, d, CS_G_V_CEN, 2, p, n.x[w2], n.y[w2], k) - cz) * obl0;
-    const R a31 = (geoR<R>(g, d, CS_G_V_CEN, 0, p, i, j, k + dz) - cx) * obl0;
-    const R a32 = (geoR<R>(g, d, CS_G_V_CEN, 1, p, i, j, k + dz) - cy) * obl0;
-    const R a33 = (geoR<R>(g, d, CS_G_V_CEN, 2, p, i, j, k + dz) - cz) * obl0;
-    R ob = (-a13 * a22 * a31 + a12 * a23 * a31 + a13 * a21 * a32 - a11 * a23 * a32 - a12 * a21 * a33 + a11 * a22 * a33);
-    ob = copysign(R(1.0), ob) / fmax(R(1.0e-32), fabs(ob));
-    Ai[st][0] = (-a23 * a32 + a22 * a33) * ob;
-    Ai[st][1] = (a13 * a32 - a12 * a33) * ob;
-    Ai[st][2] = (-a13 * a22 + a12 * a23) * ob;
-    Ai[st][3] = (a23 * a31 - a21 * a33) * ob;
-    Ai[st][4] = (-a13 * a31 + a11 * a33) * ob;
-    Ai[st][5] = (a13 * a21 - a11 * a23) * ob;
-    Ai[st][6] = (-a22 * a31 + a21 * a32) * ob;
-    Ai[st][7] = (a12 * a31 - a11 * a32) * ob;
-    Ai[st][8] = (-a12 * a21 + a11 * a22) * ob;
-  }
+// ---- bulk asynchronous copies (cp.async.bulk) and mbarriers ----
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred P;\n mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n selp.u32 %0, 1, 0, P;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+// Tensor (TMA) load of a 2-D box at element coordinates (x, y) of the map
+// into shared memory, completing on the mbarrier.  x times the element size
+// must be a multiple of 16 bytes (the callers pass multiples of 32 zones).
+__device__ __forceinline__ void tma_g2s_2d(void* dst, const void* map, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          smem_u32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+// Bounded wait on an mbarrier phase: after 2^23 polls (seconds, far beyond
+// any copy) it records an error in *err and returns, so no wait can hang.
+__device__ __noinline__ void mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
+  for (int it = 0; it < (1 << 23); ++it)
+    if (mbar_try_wait(bar, parity)) return;
+  atomicOr(err, 1);
 }
 
-// WENO of the eight linear stencils plus their mean (weight 100).
-template <typename R>
-__device__ void weno8(const Dims& d, const PhysC& ph, int p, int i, int j, int k, const Nbr12& n, const R Ai[8][9],
-                      const R* f, long long cstride_off, R gr[3]) {
-  const R f0 = f[cstride_off + d.idx(i, j, k)];
-  R X[3][9];
-#pragma unroll
-  for (int st = 0; st < 8; ++st) {
-    const int w1 = c_st8[st][0], w2 = c_st8[st][1], dz = c_st8[st][2];
-    const R R0 = f[cstride_off + d.idx(n.x[w1], n.y[w1], k)] - f0;
-    const R R1 = f[cstride_off + d.idx(n.x[w2], n.y[w2], k)] - f0;
-    const R R2 = f[cstride_off + d.idx(i, j, k + dz)] - f0;
-#pragma unroll
-    for (int rr = 0; rr < 3; ++rr) X[rr][st] = Ai[st][rr * 3 + 0] * R0 + Ai[st][rr * 3 + 1] * R1 + Ai[st][rr * 3 + 2] * R2;
-  }
-#pragma unroll
-  for (int rr = 0; rr < 3; ++rr)
-    X[rr][8] = R(0.125) * (X[rr][0] + X[rr][1] + X[rr][2] + X[rr][3] + X[rr][4] + X[rr][5] + X[rr][6] + X[rr][7]);
-  // The nonlinear weights (IS + eps)^-4 span far more than the FP32 range,
-  // so they are formed in FP64 in every form.
-  double W[9];
-#pragma unroll
-  for (int st = 0; st < 9; ++st) {
-    const double x0 = X[0][st], x1 = X[1][st], x2 = X[2][st];
-    const double IS = x0 * x0 + x1 * x1 + x2 * x2;
-    const double t = IS + ph.smallnum;
-    const double t2 = t * t;
-    W[st] = (st < 8 ? 1.0 : 100.0) / (t2 * t2);
-  }
-  const double a11 = 1.0 / (W[0] + W[1] + W[2] + W[3] + W[4] + W[5] + W[6] + W[7] + W[8]);
-#pragma unroll
-  for (int st = 0; st < 9; ++st) W[st] = W[st] * a11;
-#pragma unroll
-  for (int rr = 0; rr < 3; ++rr) {
-    double t = W[0] * (double)X[rr][0];
-#pragma unroll
-    for (int st = 1; st < 9; ++st) t = t + W[st] * (double)X[rr][st];
-    gr[rr] = (R)t;
-  }
-}
-
-// STEP 7.a (421:2515-3804): linear WENO slopes of the 8 primitives and the entropy.
-// Occupancy: 3 blocks per SM suit the FP64 instantiation, 4 the FP32 one
-// (measured on the 6 x 128^2 x 64 shell; the spills cost less than the
-// extra resident warps gain).
-template <typename R>
-__global__ void __launch_bounds__(TPB, sizeof(R) == 4 ? 4 : 3) k_weno7a(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
-    int p, i, j, k;
-    r.decode(t, p, i, j, k);
-    if (mask_at(g, d, p, i, j) != 1) continue;
-    const Nbr12 n = load_nbr(g, d, p, i, j);
-    R Ai[8][9];
-    stencil_inv(d, ph, g, p, i, j, k, n, Ai);
-    for (int q = 0; q < NVAR; ++q) {
-      R gr[3];
-      weno8(d, ph, p, i, j, k, n, Ai, s.V, ((long long)(0 * NVAR + q) * NPANEL + p) * d.S, gr);
-      Vat(s, d, q, 1, p, i, j, k) = gr[0];
-      Vat(s, d, q, 2, p, i, j, k) = gr[1];
-      Vat(s, d, q, 3, p, i, j, k) = gr[2];
+// STEP 7.a (kE false) and STEP 9.b (kE true, the WENO-AO slopes of the
+// three E components, 421:6840-8400) with the work of a zone spread over
+// three threads: a block takes 32 zones; warp w first forms stencils w,
+// w + 3, w + 6 of each zone's eight one-sided 3x3 stencils (two in-plane
+// neighbours and one radial, 421:2561-3110) as closed-form inverses of the
+// scaled centroid offsets into shared memory; then, for variables w, w + 3,
+// w + 6 (STEP 7.a: primitives 0-7, 8 = entropy; STEP 9.b: E component w),
+// it forms the eight stencil gradients and their mean and combines them
+// with the WENO weights (IS + eps)^-4, central weight 100 (421:3116-3432),
+// so no thread keeps the 72 inverse entries in registers.
+constexpr int W7A_ZT = 32;
+template <bool kE, typename R>
+__global__ void __launch_bounds__(W7A_ZT * 3, sizeof(R) == 4 ? 8 : 6) k_weno_ao_split(Dims d, PhysC ph, DGeom g,
+                                                                                        DStateT<R> s, Range3 r) {
+  __shared__ R ai[72][W7A_ZT];  // [stencil * 9 + entry][zone]
+  // c_st8 as a compile-time table, so that the unrolled stencil loop
+  // indexes the neighbour list with constants (registers, not local memory)
+  constexpr int st8[8][3] = {{0, 2, 1}, {0, 2, -1}, {1, 2, 1}, {1, 2, -1}, {0, 3, 1}, {0, 3, -1}, {1, 3, 1}, {1, 3, -1}};
+  const int zl = threadIdx.x % W7A_ZT, w = threadIdx.x / W7A_ZT;
+  const long long nz = r.count(), ntile = (nz + W7A_ZT - 1) / W7A_ZT;
+  for (long long T = blockIdx.x; T < ntile; T += gridDim.x) {
+    const long long t = T * W7A_ZT + zl;
+    int p = 0, i = 0, j = 0, k = 0;
+    bool act = t < nz;
+    if (act) {
+      r.decode(t, p, i, j, k);
+      act = mask_at(g, d, p, i, j) == 1;
     }
-    R gr[3];
-    weno8(d, ph, p, i, j, k, n, Ai, s.ent, (long long)p * d.S, gr);
-    const R om = R(1.0) - s.flatA[d.at(0, p, i, j, k)];
-    s.ent[d.at(1, p, i, j, k)] = gr[0] * om;
-    s.ent[d.at(2, p, i, j, k)] = gr[1] * om;
-    s.ent[d.at(3, p, i, j, k)] = gr[2] * om;
+    Nbr12 n;
+    if (act) {
+      n = load_nbr(g, d, p, i, j);
+      const R obl0 = R(1.0) / fmax(geoR<R>(g, d, CS_G_V_SCALE, 0, p, i, j, k), R(ph.smallnum));
+      const R cx = geoR<R>(g, d, CS_G_V_CEN, 0, p, i, j, k), cy = geoR<R>(g, d, CS_G_V_CEN, 1, p, i, j, k),
+              cz = geoR<R>(g, d, CS_G_V_CEN, 2, p, i, j, k);
+#pragma unroll 1
+      for (int st = w; st < 8; st += 3) {
+        const int w1 = c_st8[st][0], w2 = c_st8[st][1], dz = c_st8[st][2];
+        const R a11 = (geoR<R>(g, d, CS_G_V_CEN, 0, p, n.x[w1], n.y[w1], k) - cx) * obl0;
+        const R a12 = (geoR<R>(g, d, CS_G_V_CEN, 1, p, n.x[w1], n.y[w1], k) - cy) * obl0;
+        const R a13 = (geoR<R>(g, d, CS_G_V_CEN, 2, p, n.x[w1], n.y[w1], k) - cz) * obl0;
+        const R a21 = (geoR<R>(g, d, CS_G_V_CEN, 0, p, n.x[w2], n.y[w2], k) - cx) * obl0;
+        const R a22 = (geoR<R>(g, d, CS_G_V_CEN, 1, p, n.x[w2], n.y[w2], k) - cy) * obl0;
+        const R a23 = (geoR<R>(g, d, CS_G_V_CEN, 2, p, n.x[w2], n.y[w2], k) - cz) * obl0;
+        const R a31 = (geoR<R>(g, d, CS_G_V_CEN, 0, p, i, j, k + dz) - cx) * obl0;
+        const R a32 = (geoR<R>(g, d, CS_G_V_CEN, 1, p, i, j, k + dz) - cy) * obl0;
+        const R a33 = (geoR<R>(g, d, CS_G_V_CEN, 2, p, i, j, k + dz) - cz) * obl0;
+        R ob = (-a13 * a22 * a31 + a12 * a23 * a31 + a13 * a21 * a32 - a11 * a23 * a32 - a12 * a21 * a33 + a11 * a22 * a33);
+        ob = copysign(R(1.0), ob) / fmax(R(1.0e-32), fabs(ob));
+        ai[st * 9 + 0][zl] = (-a23 * a32 + a22 * a33) * ob;
+        ai[st * 9 + 1][zl] = (a13 * a32 - a12 * a33) * ob;
+        ai[st * 9 + 2][zl] = (-a13 * a22 + a12 * a23) * ob;
+        ai[st * 9 + 3][zl] = (a23 * a31 - a21 * a33) * ob;
+        ai[st * 9 + 4][zl] = (-a13 * a31 + a11 * a33) * ob;
+        ai[st * 9 + 5][zl] = (a13 * a21 - a11 * a23) * ob;
+        ai[st * 9 + 6][zl] = (-a22 * a31 + a21 * a32) * ob;
+        ai[st * 9 + 7][zl] = (a12 * a31 - a11 * a32) * ob;
+        ai[st * 9 + 8][zl] = (-a12 * a21 + a11 * a22) * ob;
+      }
+    }
+    __syncthreads();
+    if (act) {
+#pragma unroll 1
+      for (int q = w; q < (kE ? 3 : 9); q += 3) {
+        const R* f = kE ? s.Esnap + ((long long)q * NPANEL + p) * d.S
+                        : (q < 8 ? s.V + ((long long)q * NPANEL + p) * d.S : s.ent + (long long)p * d.S);
+        const R f0 = f[d.idx(i, j, k)];
+        R X[3][9];
+#pragma unroll
+        for (int st = 0; st < 8; ++st) {
+          const int w1 = st8[st][0], w2 = st8[st][1], dz = st8[st][2];
+          const R R0 = f[d.idx(n.x[w1], n.y[w1], k)] - f0;
+          const R R1 = f[d.idx(n.x[w2], n.y[w2], k)] - f0;
+          const R R2 = f[d.idx(i, j, k + dz)] - f0;
+#pragma unroll
+          for (int rr = 0; rr < 3; ++rr)
+            X[rr][st] = ai[st * 9 + rr * 3 + 0][zl] * R0 + ai[st * 9 + rr * 3 + 1][zl] * R1 + ai[st * 9 + rr * 3 + 2][zl] * R2;
+        }
+#pragma unroll
+        for (int rr = 0; rr < 3; ++rr)
+          X[rr][8] = R(0.125) * (X[rr][0] + X[rr][1] + X[rr][2] + X[rr][3] + X[rr][4] + X[rr][5] + X[rr][6] + X[rr][7]);
+        // The nonlinear weights (IS + eps)^-4 span far more than the FP32
+        // range, so they are formed in FP64 in every form.
+        double W[9];
+#pragma unroll
+        for (int st = 0; st < 9; ++st) {
+          const double x0 = X[0][st], x1 = X[1][st], x2 = X[2][st];
+          const double IS = x0 * x0 + x1 * x1 + x2 * x2;
+          const double tt = IS + ph.smallnum;
+          const double t2 = tt * tt;
+          W[st] = (st < 8 ? 1.0 : 100.0) / (t2 * t2);
+        }
+        const double a11 = 1.0 / (W[0] + W[1] + W[2] + W[3] + W[4] + W[5] + W[6] + W[7] + W[8]);
+#pragma unroll
+        for (int st = 0; st < 9; ++st) W[st] = W[st] * a11;
+        R gr[3];
+#pragma unroll
+        for (int rr = 0; rr < 3; ++rr) {
+          double tt = W[0] * (double)X[rr][0];
+#pragma unroll
+          for (int st = 1; st < 9; ++st) tt = tt + W[st] * (double)X[rr][st];
+          gr[rr] = (R)tt;
+        }
+        if (kE) {
+          s.E[d.at(3 + q, p, i, j, k)] = gr[0];
+          s.E[d.at(6 + q, p, i, j, k)] = gr[1];
+          s.E[d.at(9 + q, p, i, j, k)] = gr[2];
+        } else if (q < 8) {
+          Vat(s, d, q, 1, p, i, j, k) = gr[0];
+          Vat(s, d, q, 2, p, i, j, k) = gr[1];
+          Vat(s, d, q, 3, p, i, j, k) = gr[2];
+        } else {
+          const R om = R(1.0) - s.flatA[d.at(0, p, i, j, k)];
+          s.ent[d.at(1, p, i, j, k)] = gr[0] * om;
+          s.ent[d.at(2, p, i, j, k)] = gr[1] * om;
+          s.ent[d.at(3, p, i, j, k)] = gr[2] * om;
+        }
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -496,7 +560,7 @@ __global__ void __launch_bounds__(TPB) k_weno7b(Dims d, PhysC ph, DGeom g, DStat
           const int w = c_n18[rr][0];
           off = d.idx(w < 0 ? i : n.x[w], w < 0 ? j : n.y[w], k + c_n18[rr][1]);
 #pragma unroll
-          for (int a = 0; a < 9; ++a) A[a] = __ldg(wc + (long long)(rr * 9 + a) * ord.nw);
+          for (int a = 0; a < 9; ++a) A[a] = __ldg(wc + (long long)(rr * 9 + a) * m9_stride(ord.nw));
         } else {
           w7b_row(d, ph, g, p, i, j, k, n, rr, cx, cy, cz, l0, obl0, c0, A, off);
         }
@@ -552,6 +616,115 @@ __global__ void __launch_bounds__(TPB) k_weno7b(Dims d, PhysC ph, DGeom g, DStat
   }
 }
 
+// STEP 7.b with the resident row weights, four threads per zone: a block
+// takes 32 zones and warp c the primitives 2c and 2c + 1, so each thread
+// keeps 2 x 9 least-squares sums instead of 8 x 9.  The 162 row weights of
+// the block's 32 zones are one 32 x 162 tile of the weight array (zone
+// fastest, rows m9_stride apart): a tensor (TMA) load stages it into shared
+// memory, completing on an mbarrier whose wait is bounded (a timeout sets
+// err_flag), and the four warps read it there.  The order of the zones
+// (LsqOrder's with 32 zones a tile) and every sum are those of k_weno7b.
+constexpr int W7B_ZT = 32;
+template <bool kShared, typename R>
+__global__ void __launch_bounds__(W7B_ZT * 4, sizeof(R) == 4 ? 8 : 5) k_weno7b_split(
+    Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r, const __grid_constant__ CUtensorMap wmap) {
+  __shared__ alignas(128) R wsm[162][W7B_ZT];
+  __shared__ uint64_t bar;
+  const R ob12 = R(1.0) / R(12.0), ob180 = R(1.0) / R(180.0), ob144 = R(1.0) / R(144.0);
+  const int zl = threadIdx.x % W7B_ZT, q0 = 2 * (threadIdx.x / W7B_ZT);
+  const long long nr = r.count(), npp = nr / 6;
+  const long long ntile = kShared ? 6 * ((npp + W7B_ZT - 1) / W7B_ZT) : (nr + W7B_ZT - 1) / W7B_ZT;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  uint32_t parity = 0;
+  for (long long T = blockIdx.x; T < ntile; T += gridDim.x) {
+    const long long tw0 = kShared ? (T / 6) * W7B_ZT : T * W7B_ZT;
+    if (threadIdx.x == 0) {
+      mbar_expect_tx(&bar, (uint32_t)sizeof(wsm));
+      tma_g2s_2d(&wsm[0][0], &wmap, (int)tw0, 0, &bar);
+    }
+    long long t, tw = tw0 + zl;
+    bool act;
+    if (kShared) {
+      t = (T % 6) * npp + tw;
+      act = tw < npp;
+    } else {
+      t = tw;
+      act = t < nr;
+    }
+    int p = 0, i = 0, j = 0, k = 0;
+    if (act) {
+      r.decode(t, p, i, j, k);
+      act = mask_at(g, d, p, i, j) == 1;
+    }
+    mbar_wait(&bar, parity, s.err_flag);
+    parity ^= 1u;
+    if (act) {
+      const Nbr12 n = load_nbr(g, d, p, i, j);
+      const R f = s.flatA[d.at(0, p, i, j, k)];
+      const R betalo = f + (R(1.0) - f) * R(2.0);
+      const R ghi = f * R(0.6) + (R(1.0) - f) * R(0.95), glo = R(1.0) - ghi, obghi = R(1.0) / ghi, grat = glo / ghi;
+      R v0[2];
+#pragma unroll
+      for (int qq = 0; qq < 2; ++qq) v0[qq] = s.V[((long long)(q0 + qq) * NPANEL + p) * d.S + d.idx(i, j, k)];
+      R Y[2][9];
+#pragma unroll
+      for (int qq = 0; qq < 2; ++qq)
+#pragma unroll
+        for (int a = 0; a < 9; ++a) Y[qq][a] = R(0.0);
+#pragma unroll 2
+      for (int rr = 0; rr < 18; ++rr) {
+        const int w = c_n18[rr][0];
+        const long long off = d.idx(w < 0 ? i : n.x[w], w < 0 ? j : n.y[w], k + c_n18[rr][1]);
+#pragma unroll
+        for (int qq = 0; qq < 2; ++qq) {
+          const R Rv = s.V[((long long)(q0 + qq) * NPANEL + p) * d.S + off] - v0[qq];
+#pragma unroll
+          for (int a = 0; a < 9; ++a) Y[qq][a] = Y[qq][a] + wsm[rr * 9 + a][zl] * Rv;
+        }
+      }
+      const unsigned long long qsrc = kShared ? s.lsq_map9[p].src : LSQ_IDENTITY_SRC;
+      const unsigned int qneg = kShared ? s.lsq_map9[p].neg : 0u;
+      R c0[10];
+      coef10(g, d, p, i, j, k, c0);
+#pragma unroll
+      for (int qq = 0; qq < 2; ++qq) {
+        const int q = q0 + qq;
+        R X[9];
+#pragma unroll
+        for (int a = 0; a < 9; ++a) X[a] = kShared ? lsq_rotated<1>(Y[qq], a + 1, qsrc, qneg) : Y[qq][a];
+        const R v2 = Vat(s, d, q, 1, p, i, j, k), v3 = Vat(s, d, q, 2, p, i, j, k), v4 = Vat(s, d, q, 3, p, i, j, k);
+        const R ISlo = betalo * (v2 * v2 + v3 * v3 + v4 * v4) * ob12;
+        R Phi[9];
+        Phi[0] = X[0] * obghi - v2 * grat;
+        Phi[1] = X[1] * obghi - v3 * grat;
+        Phi[2] = X[2] * obghi - v4 * grat;
+#pragma unroll
+        for (int a = 3; a < 9; ++a) Phi[a] = X[a] * obghi;
+        const R IShi = (Phi[0] * Phi[0] + Phi[1] * Phi[1] + Phi[2] * Phi[2]) * ob12 +
+                       (Phi[3] * Phi[3]) * (sqr(c0[4] - ob12) + ob180) + (Phi[4] * Phi[4]) * (sqr(c0[5] - ob12) + ob180) +
+                       (Phi[5] * Phi[5]) * (sqr(c0[6] - ob12) + ob180) + (Phi[6] * Phi[6]) * (c0[7] * c0[7] + ob144) +
+                       (Phi[7] * Phi[7]) * (c0[8] * c0[8] + ob144) + (Phi[8] * Phi[8]) * (c0[9] * c0[9] + ob144);
+        const R tau = fabs(IShi - ISlo);
+        R Wlo = glo * (R(1.0) + tau / (ISlo + R(ph.smallnum))), Whi = ghi * (R(1.0) + tau / (IShi + R(ph.smallnum)));
+        const R aa = R(1.0) / (Wlo + Whi);
+        Wlo = Wlo * aa;
+        Whi = Whi * aa;
+        const R x = R(1.0) - f;
+        Vat(s, d, q, 1, p, i, j, k) = (Whi * Phi[0] + Wlo * v2) * x;
+        Vat(s, d, q, 2, p, i, j, k) = (Whi * Phi[1] + Wlo * v3) * x;
+        Vat(s, d, q, 3, p, i, j, k) = (Whi * Phi[2] + Wlo * v4) * x;
+#pragma unroll
+        for (int m = 4; m < 10; ++m) Vat(s, d, q, m, p, i, j, k) = (Whi * Phi[m - 1]) * x;
+      }
+    }
+    __syncthreads();  // every warp is done with wsm before the next tile's load
+  }
+}
+
 template <typename R>
 __global__ void k_ops_m9(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
   // shared by the panels: panel 1's zones only (the first sixth of the range)
@@ -576,7 +749,7 @@ __global__ void k_ops_m9(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
       for (int a = 0; a < 9; ++a) {
         double w = 0.0;
         for (int b = 0; b < 9; ++b) w = w + Minv[a * 9 + b] * A[b];
-        s.op_m9[(long long)(rr * 9 + a) * nr_ + t] = (R)w;
+        s.op_m9[(long long)(rr * 9 + a) * m9_stride(nr_) + t] = (R)w;
       }
     }
   }
@@ -735,75 +908,86 @@ __global__ void k_apply_giveup(Dims d, DStateT<R> s, Range3 r) {
 }
 
 // STEP 8.a-c (421:4686-5567): B at the five quadrature points of each face,
-// averaged from both sides and shifted to the facial mean.
+// averaged from both sides and shifted to the facial mean.  A block takes 32
+// faces: thread (w, face) with w = 3 side + component evaluates that side's
+// polynomial of B_component at the five points (in the state's type) into
+// shared memory, then the first warp forms each face's normal component
+// 0.5 (n . B_L + n . B_R) point by point and shifts it in FP64 so the five
+// values average to the FP64 face B exactly.
+constexpr int FB_FACES = 32;
 template <typename R>
-__global__ void __launch_bounds__(TPB) k_faceB(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r, int dir) {
+__global__ void __launch_bounds__(FB_FACES * 6, 4) k_faceB(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r, int dir) {
+  __shared__ R bv[2][3][5][FB_FACES];  // [side][component][point][face]
   const int QP = dir == 0 ? CS_G_XF_QP : (dir == 1 ? CS_G_YF_QP : CS_G_ZF_QP);
   const int BW = dir == 0 ? CS_G_XB_QW : (dir == 1 ? CS_G_YB_QW : CS_G_ZB_QW);
   const int NF = dir == 0 ? CS_G_XF_N : (dir == 1 ? CS_G_YF_N : CS_G_ZF_N);
   double* Bq = s.Bq[dir];
   const double* Bf = dir == 0 ? s.Bxf : (dir == 1 ? s.Byf : s.Bzf);
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
-    int p, i, j, k;
-    r.decode(t, p, i, j, k);
+  const int lane = threadIdx.x % FB_FACES, w = threadIdx.x / FB_FACES;
+  const long long nf = r.count(), ntile = (nf + FB_FACES - 1) / FB_FACES;
+  for (long long tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
+    const long long t = tile * FB_FACES + lane;
+    const bool valid = t < nf;
+    int p = 0, i = 0, j = 0, k = 0;
+    if (valid) r.decode(t, p, i, j, k);
     int lx = i, ly = j, lz = k, rx = i, ry = j, rz = k;
-    bool skip = false;
-    if (dir == 0) {
-      const int mL = mask_at(g, d, p, i, j), mR = mask_at(g, d, p, i + 1, j);
-      rx = i + 1;
-      if (mL == 0 && mR == 1) { lx = sten(g, d, p, rx, ry, 1, 0); ly = sten(g, d, p, rx, ry, 1, 1); }
-      else if (mL == 1 && mR == 0) { rx = sten(g, d, p, lx, ly, 0, 0); ry = sten(g, d, p, lx, ly, 0, 1); }
-      else if (mL == 0 && mR == 0) skip = true;
-    } else if (dir == 1) {
-      const int mL = mask_at(g, d, p, i, j), mR = mask_at(g, d, p, i, j + 1);
-      ry = j + 1;
-      if (mL == 0 && mR == 1) { lx = sten(g, d, p, rx, ry, 3, 0); ly = sten(g, d, p, rx, ry, 3, 1); }
-      else if (mL == 1 && mR == 0) { rx = sten(g, d, p, lx, ly, 2, 0); ry = sten(g, d, p, lx, ly, 2, 1); }
-      else if (mL == 0 && mR == 0) skip = true;
-    } else {
-      if (mask_at(g, d, p, i, j) == 0) skip = true;
-      rz = k + 1;
-    }
-    // the two sides' values in the state's type; the shift to the facial
-    // mean in FP64, so the values average to the FP64 face B exactly
-    R bq[5] = {R(0), R(0), R(0), R(0), R(0)};
-    if (!skip) {
-      const R obl0 = R(1.0) / fmax(geoR<R>(g, d, CS_G_V_SCALE, 0, p, lx, ly, lz), R(ph.smallnum));
-      const R obl02 = R(1.0) / fmax(geoR<R>(g, d, CS_G_V_SCALE, 0, p, rx, ry, rz), R(ph.smallnum));
-      R cL[10], cR[10], vL[3][10], vR[3][10];
-      coef10(g, d, p, lx, ly, lz, cL);
-      coef10(g, d, p, rx, ry, rz, cR);
-#pragma unroll
-      for (int b = 0; b < 3; ++b)
-#pragma unroll
-        for (int m = 0; m < 10; ++m) {
-          vL[b][m] = Vat(s, d, 5 + b, m, p, lx, ly, lz);
-          vR[b][m] = Vat(s, d, 5 + b, m, p, rx, ry, rz);
-        }
-      const R lcx = geoR<R>(g, d, CS_G_V_CEN, 0, p, lx, ly, lz), lcy = geoR<R>(g, d, CS_G_V_CEN, 1, p, lx, ly, lz),
-              lcz = geoR<R>(g, d, CS_G_V_CEN, 2, p, lx, ly, lz);
-      const R rcx = geoR<R>(g, d, CS_G_V_CEN, 0, p, rx, ry, rz), rcy = geoR<R>(g, d, CS_G_V_CEN, 1, p, rx, ry, rz),
-              rcz = geoR<R>(g, d, CS_G_V_CEN, 2, p, rx, ry, rz);
-#pragma unroll
-      for (int q = 0; q < 5; ++q) {
-        const int nq = dir == 2 ? q : 0, ns = dir == 2 ? 5 : 1;
-        const R nx = geoR<R>(g, d, NF, 0 * ns + nq, p, i, j, k), ny = geoR<R>(g, d, NF, 1 * ns + nq, p, i, j, k),
-                nz = geoR<R>(g, d, NF, 2 * ns + nq, p, i, j, k);
-        const R px = geoR<R>(g, d, QP, q, p, i, j, k), py = geoR<R>(g, d, QP, 5 + q, p, i, j, k),
-                pz = geoR<R>(g, d, QP, 10 + q, p, i, j, k);
-        const R x = (px - lcx) * obl0, y = (py - lcy) * obl0, z = (pz - lcz) * obl0;
-        const R x2 = (px - rcx) * obl02, y2 = (py - rcy) * obl02, z2 = (pz - rcz) * obl02;
-        const R bx = d_poly10(vL[0], cL, x, y, z), by = d_poly10(vL[1], cL, x, y, z), bz = d_poly10(vL[2], cL, x, y, z);
-        const R bx2 = d_poly10(vR[0], cR, x2, y2, z2), by2 = d_poly10(vR[1], cR, x2, y2, z2),
-                bz2 = d_poly10(vR[2], cR, x2, y2, z2);
-        bq[q] = R(0.5) * (nx * (bx + bx2) + ny * (by + by2) + nz * (bz + bz2));
+    bool skip = !valid;
+    if (valid) {
+      if (dir == 0) {
+        const int mL = mask_at(g, d, p, i, j), mR = mask_at(g, d, p, i + 1, j);
+        rx = i + 1;
+        if (mL == 0 && mR == 1) { lx = sten(g, d, p, rx, ry, 1, 0); ly = sten(g, d, p, rx, ry, 1, 1); }
+        else if (mL == 1 && mR == 0) { rx = sten(g, d, p, lx, ly, 0, 0); ry = sten(g, d, p, lx, ly, 0, 1); }
+        else if (mL == 0 && mR == 0) skip = true;
+      } else if (dir == 1) {
+        const int mL = mask_at(g, d, p, i, j), mR = mask_at(g, d, p, i, j + 1);
+        ry = j + 1;
+        if (mL == 0 && mR == 1) { lx = sten(g, d, p, rx, ry, 3, 0); ly = sten(g, d, p, rx, ry, 3, 1); }
+        else if (mL == 1 && mR == 0) { rx = sten(g, d, p, lx, ly, 2, 0); ry = sten(g, d, p, lx, ly, 2, 1); }
+        else if (mL == 0 && mR == 0) skip = true;
+      } else {
+        if (mask_at(g, d, p, i, j) == 0) skip = true;
+        rz = k + 1;
       }
     }
-    double bd = Bf[d.at(0, p, i, j, k)];
+    if (!skip) {
+      const int side = w / 3, b = w % 3;
+      const int zx = side ? rx : lx, zy = side ? ry : ly, zz = side ? rz : lz;
+      const R obl = R(1.0) / fmax(geoR<R>(g, d, CS_G_V_SCALE, 0, p, zx, zy, zz), R(ph.smallnum));
+      const R cx = geoR<R>(g, d, CS_G_V_CEN, 0, p, zx, zy, zz), cy = geoR<R>(g, d, CS_G_V_CEN, 1, p, zx, zy, zz),
+              cz = geoR<R>(g, d, CS_G_V_CEN, 2, p, zx, zy, zz);
+      R cc[10], v[10];
+      coef10(g, d, p, zx, zy, zz, cc);
 #pragma unroll
-    for (int q = 0; q < 5; ++q) bd = bd - geo(g, d, BW, q, p, i, j, k) * (double)bq[q];
+      for (int m = 0; m < 10; ++m) v[m] = Vat(s, d, 5 + b, m, p, zx, zy, zz);
 #pragma unroll
-    for (int q = 0; q < 5; ++q) Bq[d.at(q, p, i, j, k)] = (double)bq[q] + bd;
+      for (int q = 0; q < 5; ++q) {
+        const R x = (geoR<R>(g, d, QP, q, p, i, j, k) - cx) * obl;
+        const R y = (geoR<R>(g, d, QP, 5 + q, p, i, j, k) - cy) * obl;
+        const R z = (geoR<R>(g, d, QP, 10 + q, p, i, j, k) - cz) * obl;
+        bv[side][b][q][lane] = d_poly10(v, cc, x, y, z);
+      }
+    }
+    __syncthreads();
+    if (w == 0 && valid) {
+      R bq[5] = {R(0), R(0), R(0), R(0), R(0)};
+      if (!skip) {
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+          const int nq = dir == 2 ? q : 0, ns = dir == 2 ? 5 : 1;
+          const R nx = geoR<R>(g, d, NF, nq, p, i, j, k), ny = geoR<R>(g, d, NF, ns + nq, p, i, j, k),
+                  nz = geoR<R>(g, d, NF, 2 * ns + nq, p, i, j, k);
+          bq[q] = R(0.5) * (nx * (bv[0][0][q][lane] + bv[1][0][q][lane]) + ny * (bv[0][1][q][lane] + bv[1][1][q][lane]) +
+                            nz * (bv[0][2][q][lane] + bv[1][2][q][lane]));
+        }
+      }
+      double bd = Bf[d.at(0, p, i, j, k)];
+#pragma unroll
+      for (int q = 0; q < 5; ++q) bd = bd - geo(g, d, BW, q, p, i, j, k) * (double)bq[q];
+#pragma unroll
+      for (int q = 0; q < 5; ++q) Bq[d.at(q, p, i, j, k)] = (double)bq[q] + bd;
+    }
+    __syncthreads();
   }
 }
 
@@ -1035,40 +1219,6 @@ __global__ void __launch_bounds__(32 * ADP_WARPS) k_adp(Dims d, PhysC ph, DGeom 
     }
     __syncwarp();
   }
-}
-
-// ---- bulk asynchronous copies (cp.async.bulk) and mbarriers ----
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred P;\n mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n selp.u32 %0, 1, 0, P;\n}\n"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   smem_u32(dst)),
-               "l"(src), "r"(bytes), "r"(smem_u32(bar))
-               : "memory");
-}
-// Bounded wait on an mbarrier phase: after 2^23 polls (seconds, far beyond
-// any copy) it records an error in *err and returns, so no wait can hang.
-__device__ __noinline__ void mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
-  for (int it = 0; it < (1 << 23); ++it)
-    if (mbar_try_wait(bar, parity)) return;
-  atomicOr(err, 1);
 }
 
 // STEP 8.d right-hand side with the resident factors: one thread per zone
@@ -1349,25 +1499,6 @@ __global__ void k_efield_a(Dims d, DGeom g, DStateT<R> s, Range3 r) {
 // STEP 9.b (421:6840-8400): linear WENO slopes of the E point values.
 // Three blocks per SM (measured: faster than two at 255 registers, and than
 // four).
-template <typename R>
-__global__ void __launch_bounds__(TPB, 3) k_efield_b(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
-    int p, i, j, k;
-    r.decode(t, p, i, j, k);
-    if (mask_at(g, d, p, i, j) != 1) continue;
-    const Nbr12 n = load_nbr(g, d, p, i, j);
-    R Ai[8][9];
-    stencil_inv(d, ph, g, p, i, j, k, n, Ai);
-    for (int q = 0; q < 3; ++q) {
-      R gr[3];
-      weno8(d, ph, p, i, j, k, n, Ai, s.Esnap, ((long long)q * NPANEL + p) * d.S, gr);
-      s.E[d.at(3 + q, p, i, j, k)] = gr[0];
-      s.E[d.at(6 + q, p, i, j, k)] = gr[1];
-      s.E[d.at(9 + q, p, i, j, k)] = gr[2];
-    }
-  }
-}
-
 // Row rr (0: the zone itself, 1..18: the STEP 7.b neighbours) of the
 // 19 x 10 interpolation least-squares matrix of STEP 9.c (421:8464-8620).
 template <typename R>
@@ -1869,14 +2000,21 @@ template <typename R>
 void launch_weno_t(Solve& sv, DStateT<R>& st) {
   const Dims& d = sv.d;
   Range3 a = shrink(d, 1), b = shrink(d, 2);
-  k_weno7a<R><<<blocks_for(a.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, a);
-  mark(sv, "k_weno7a");
-  if (st.op_m9)
+  {
+    const long long nt = (a.count() + W7A_ZT - 1) / W7A_ZT;
+    const int nb = (int)std::min<long long>(nt, (long long)grid_sms(sv) * 16);
+    k_weno_ao_split<false, R><<<nb, W7A_ZT * 3, 0, sv.stream>>>(d, sv.ph, sv.g, st, a);
+    mark(sv, "k_weno7a");
+  }
+  if (st.op_m9) {
+    const long long nt = (b.count() + W7B_ZT - 1) / W7B_ZT + 6;
+    const int nb = (int)std::min<long long>(nt, (long long)grid_sms(sv) * 16);
+    const CUtensorMap& wm = sv.mesh->m9_map;
     if (st.lsq_map9)
-      k_weno7b<true, true, R><<<blocks_for(b.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
+      k_weno7b_split<true, R><<<nb, W7B_ZT * 4, 0, sv.stream>>>(d, sv.ph, sv.g, st, b, wm);
     else
-      k_weno7b<true, false, R><<<blocks_for(b.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
-  else
+      k_weno7b_split<false, R><<<nb, W7B_ZT * 4, 0, sv.stream>>>(d, sv.ph, sv.g, st, b, wm);
+  } else
     k_weno7b<false, false, R><<<blocks_for(b.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
   mark(sv, "k_weno7b");
 }
@@ -1912,12 +2050,13 @@ void launch_faceB_adp_t(Solve& sv, DStateT<R>& st) {
   Range3 fx = {1 - G, N + G - 1, 2 - G, N + G - 1, 2 - G, nr + G - 1};
   Range3 fy = {2 - G, N + G - 1, 1 - G, N + G - 1, 2 - G, nr + G - 1};
   Range3 fz = {2 - G, N + G - 1, 2 - G, N + G - 1, 1 - G, nr + G - 1};
-  k_faceB<R><<<blocks_for(fx.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, fx, 0);
-  mark(sv, "k_faceB");
-  k_faceB<R><<<blocks_for(fy.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, fy, 1);
-  mark(sv, "k_faceB");
-  k_faceB<R><<<blocks_for(fz.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, fz, 2);
-  mark(sv, "k_faceB");
+  const Range3 fr[3] = {fx, fy, fz};
+  for (int dir = 0; dir < 3; ++dir) {
+    const long long nt = (fr[dir].count() + FB_FACES - 1) / FB_FACES;
+    const int nb = (int)std::min<long long>(nt, (long long)grid_sms(sv) * 16);
+    k_faceB<R><<<nb, FB_FACES * 6, 0, sv.stream>>>(d, sv.ph, sv.g, st, fr[dir], dir);
+    mark(sv, "k_faceB");
+  }
   Range3 a = shrink(d, 1);
   if (st.adp_lu && st.adp_pmap) {
     k_adp_rhs6<R><<<blocks_for(a.count() / 6, ADPR_TPB, grid_sms(sv)), ADPR_TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st,
@@ -2024,8 +2163,12 @@ void launch_efield_t(Solve& sv, DStateT<R>& st) {
   Range3 z = zones_all(d), a = shrink(d, 1), b = shrink(d, 2);
   k_efield_a<R><<<blocks_for(z.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.g, st, z);
   mark(sv, "k_efield_a");
-  k_efield_b<R><<<blocks_for(a.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, a);
-  mark(sv, "k_efield_b");
+  {
+    const long long nt = (a.count() + W7A_ZT - 1) / W7A_ZT;
+    const int nb = (int)std::min<long long>(nt, (long long)grid_sms(sv) * 16);
+    k_weno_ao_split<true, R><<<nb, W7A_ZT * 3, 0, sv.stream>>>(d, sv.ph, sv.g, st, a);
+    mark(sv, "k_efield_b");
+  }
   if (st.op_m10)
     if (st.lsq_map10)
       k_efield_c<true, true, R><<<blocks_for(b.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);

@@ -240,8 +240,12 @@ def test_shared_panel_row_weights_match_per_panel(name, rk, form):
         out.append((s, s.mesh_device_bytes(), V, E1, dt, s.get_state()))
     (s, b0, V0, E0, d0, st0), (_, b1, V1, E1, d1, st1) = out
     nl = 6 * (s.N + 2 * s.G - 4) ** 2 * (s.nr + 2 * s.G - 4)
-    words, size = (352, 4) if form else (190, 8)  # shared: both operators in FP32, STEP 9.c's in FP64
-    assert b1 - b0 == (nl - nl // 6) * words * size - 6 * 16  # the weights, less the six panel maps
+    stride = lambda n: (n + 3) // 4 * 4  # STEP 7.b's rows start on 16-byte boundaries (its tensor map)
+    if form:  # shared: both operators in FP32
+        saved = ((stride(nl) - stride(nl // 6)) * 162 + (nl - nl // 6) * 190) * 4
+    else:  # STEP 9.c's in FP64
+        saved = (nl - nl // 6) * 190 * 8
+    assert b1 - b0 == saved - 6 * 16  # the weights, less the six panel maps
     tw, ts = (1e-5, 1e-5) if form else (1e-11, TOL_STATE)
     for m in range(10):
         for c in range(8):
