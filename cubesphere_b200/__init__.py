@@ -51,7 +51,7 @@ EXPORTS = [
     "cs_serve_wait", "cs_serve_state", "cs_serve_stats", "cs_serve_destroy",
     "cs_batch_create", "cs_batch_steps", "cs_batch_autotune", "cs_batch_grid_fraction", "cs_batch_last_error",
     "cs_batch_destroy", "cs_twod_rs_ez", "cs_pointwise", "cs_fp64_fma_rate", "cs_limit_minmax",
-    "cs_state_put_amr", "cs_state_get_amr",
+    "cs_state_put_amr", "cs_state_get_amr", "cs_debug_set_wait_error",
     "cs_snapshot_save", "cs_snapshot_load", "cs_snapshot_write_host", "cs_snapshot_read_host",
 ]
 
@@ -189,6 +189,7 @@ def load_library() -> ctypes.CDLL:
         "cs_fp64_fma_rate": ([ctypes.c_int32, dp], ctypes.c_int),
         "cs_limit_minmax": ([P, dp, dp], ctypes.c_int),
         "cs_state_put_amr": ([P, ctypes.c_int32, dp, dp, dp, dp, dp], ctypes.c_int),
+        "cs_debug_set_wait_error": ([P, ctypes.c_int32], ctypes.c_int),
         "cs_state_get_amr": ([P, ctypes.c_int32, dp, dp, dp, dp, dp], ctypes.c_int),
         "cs_snapshot_save": ([P, ctypes.c_char_p, D, D, ctypes.c_int64], ctypes.c_int),
         "cs_snapshot_load": ([P, ctypes.c_char_p, dp, dp, ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),

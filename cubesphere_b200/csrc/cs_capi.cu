@@ -442,6 +442,7 @@ PhysC make_phys(const cs_params& p) {
   ph.flatten_coef = p.flatten_coef;
   ph.prs_flatten_coef = p.prs_flatten_coef;
   ph.gm = p.gm;
+  ph.ogm1 = 1.0 / (p.gamma - 1.0);
   return ph;
 }
 
@@ -763,7 +764,7 @@ int mesh_operators(Solve& sv, MeshRes& m, DStateT<R>& s) {
     size_t fr = 0, tot = 0;
     const size_t bytes = (size_t)(m9_stride(n9) * 162 + n10 * 190) * sizeof(R);
     // room left after them as for the ADP factors below
-    if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && bytes + (size_t)8 * S6 * 10 + ((size_t)1 << 30) < fr) {
+    if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && bytes + (size_t)8 * S6 + ((size_t)2 << 30) < fr) {
       m.op_m9 = mdalloc(sv, m, (size_t)m9_stride(n9) * 162 * sizeof(R), e);
       m.op_m10 = m.op_m9 ? mdalloc(sv, m, (size_t)n10 * 190 * sizeof(R), e) : nullptr;
       if (!m.op_m9 || !m.op_m10) return cuda_fail(sv, e, "cudaMalloc(least-squares operators)");
@@ -785,10 +786,12 @@ int mesh_operators(Solve& sv, MeshRes& m, DStateT<R>& s) {
     const size_t esz = shared ? sizeof(R) : sizeof(double);
     const long long nf = adp_factor_doubles(d, shared);
     const size_t lu_bytes = (size_t)nf * esz, pv_bytes = (size_t)nf / 36;
+    const size_t rhs_bytes = (size_t)adp_range_count(d) * 36 * esz;
     size_t fr = 0, tot = 0;
-    // room left after them: the FP32 form's state staging (9 FP64 words
-    // per point, cs_state_put / cs_state_get) and 1 GB
-    if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && lu_bytes + pv_bytes + (size_t)8 * S6 * 10 + ((size_t)1 << 30) < fr) {
+    // room left after them and their right-hand sides: the FP32 form's state
+    // staging (one FP64 word per point, cs_state_put / cs_state_get) and 2 GB
+    if (cudaMemGetInfo(&fr, &tot) == cudaSuccess &&
+        lu_bytes + pv_bytes + rhs_bytes + (size_t)8 * S6 + ((size_t)2 << 30) < fr) {
       m.adp_lu = mdalloc(sv, m, lu_bytes, e);
       m.adp_piv = m.adp_lu ? (int8_t*)mdalloc(sv, m, pv_bytes, e) : nullptr;
       s.adp_rhs = m.adp_piv ? dalloc(sv, (size_t)adp_range_count(d) * 36 * esz, e) : nullptr;
@@ -1263,16 +1266,16 @@ int cs_state_put(cs_ctx* ctx, const double* U, const double* ent, const double* 
   const size_t S6 = (size_t)6 * sv.d.S;
   if (sv.fp32) {
     // The precision form keeps U and the entropy in FP32 on the device: the
-    // FP64 host values go through a stream-ordered staging buffer and are
-    // rounded on the device.
-    const size_t nu = cs::NVAR * S6;
+    // FP64 host values go through a stream-ordered staging buffer of one
+    // component and are rounded on the device, component by component.
     double* stage = nullptr;
-    CS_CUDA(sv, cudaMallocFromPoolAsync((void**)&stage, (nu + S6) * sizeof(double), sv.pool, sv.stream));
-    CS_CUDA(sv, cudaMemcpyAsync(stage, U, nu * sizeof(double), cudaMemcpyHostToDevice, sv.stream));
-    CS_CUDA(sv, cudaMemcpyAsync(stage + nu, ent, S6 * sizeof(double), cudaMemcpyHostToDevice, sv.stream));
-    cs::k_narrow<<<cs::blocks_for((long long)nu, 256, sv.sm_count), 256, 0, sv.stream>>>(stage, sv.stF.U, (long long)nu);
-    cs::k_narrow<<<cs::blocks_for((long long)S6, 256, sv.sm_count), 256, 0, sv.stream>>>(stage + nu, sv.stF.ent,
-                                                                                       (long long)S6);
+    CS_CUDA(sv, cudaMallocFromPoolAsync((void**)&stage, S6 * sizeof(double), sv.pool, sv.stream));
+    for (int c = 0; c <= cs::NVAR; ++c) {
+      const double* src = c < cs::NVAR ? U + (size_t)c * S6 : ent;
+      float* dst = c < cs::NVAR ? sv.stF.U + (size_t)c * S6 : sv.stF.ent;
+      CS_CUDA(sv, cudaMemcpyAsync(stage, src, S6 * sizeof(double), cudaMemcpyHostToDevice, sv.stream));
+      cs::k_narrow<<<cs::blocks_for((long long)S6, 256, sv.sm_count), 256, 0, sv.stream>>>(stage, dst, (long long)S6);
+    }
     CS_CUDA(sv, cudaGetLastError());
     CS_CUDA(sv, cudaFreeAsync(stage, sv.stream));
     CS_CUDA(sv, cudaMemcpyAsync(sv.stF.Bxf, bxf, S6 * sizeof(double), cudaMemcpyHostToDevice, sv.stream));
@@ -1299,16 +1302,17 @@ int cs_state_get(cs_ctx* ctx, double* U, double* ent, double* bxf, double* byf, 
   if (int rc = cs::need(sv, true)) return rc;
   const size_t S6 = (size_t)6 * sv.d.S;
   if (sv.fp32) {
-    // widened to FP64 on the device, through a stream-ordered staging buffer
-    const size_t nu = cs::NVAR * S6;
+    // widened to FP64 on the device, component by component, through a
+    // stream-ordered staging buffer of one component
     double* stage = nullptr;
-    CS_CUDA(sv, cudaMallocFromPoolAsync((void**)&stage, (nu + S6) * sizeof(double), sv.pool, sv.stream));
-    cs::k_widen<<<cs::blocks_for((long long)nu, 256, sv.sm_count), 256, 0, sv.stream>>>(sv.stF.U, stage, (long long)nu);
-    cs::k_widen<<<cs::blocks_for((long long)S6, 256, sv.sm_count), 256, 0, sv.stream>>>(sv.stF.ent, stage + nu,
-                                                                                      (long long)S6);
+    CS_CUDA(sv, cudaMallocFromPoolAsync((void**)&stage, S6 * sizeof(double), sv.pool, sv.stream));
+    for (int c = 0; c <= cs::NVAR; ++c) {
+      const float* src = c < cs::NVAR ? sv.stF.U + (size_t)c * S6 : sv.stF.ent;
+      double* dst = c < cs::NVAR ? U + (size_t)c * S6 : ent;
+      cs::k_widen<<<cs::blocks_for((long long)S6, 256, sv.sm_count), 256, 0, sv.stream>>>(src, stage, (long long)S6);
+      CS_CUDA(sv, cudaMemcpyAsync(dst, stage, S6 * sizeof(double), cudaMemcpyDeviceToHost, sv.stream));
+    }
     CS_CUDA(sv, cudaGetLastError());
-    CS_CUDA(sv, cudaMemcpyAsync(U, stage, nu * sizeof(double), cudaMemcpyDeviceToHost, sv.stream));
-    CS_CUDA(sv, cudaMemcpyAsync(ent, stage + nu, S6 * sizeof(double), cudaMemcpyDeviceToHost, sv.stream));
     CS_CUDA(sv, cudaFreeAsync(stage, sv.stream));
     CS_CUDA(sv, cudaMemcpyAsync(bxf, sv.stF.Bxf, S6 * sizeof(double), cudaMemcpyDeviceToHost, sv.stream));
     CS_CUDA(sv, cudaMemcpyAsync(byf, sv.stF.Byf, S6 * sizeof(double), cudaMemcpyDeviceToHost, sv.stream));
@@ -1559,6 +1563,17 @@ int cs_state_get_amr(cs_ctx* ctx, int32_t n_cc_components, double* U_amr, double
   std::vector<double> U(cs::NVAR * S6), ent(S6);
   if (int rc = cs_state_get(ctx, U.data(), ent.data(), Bxf_amr, Byf_amr, Bzf_amr)) return rc;
   box_to_amr(sv.d, n_cc_components, U.data(), ent.data(), U_amr, entropygr_amr);
+  return CS_OK;
+}
+
+int cs_debug_set_wait_error(cs_ctx* ctx, int32_t value) {
+  if (!ctx) return CS_ERR_ARG;
+  Solve& sv = ctx->sv;
+  if (int rc = cs::need(sv, false)) return rc;
+  int* flag = sv.fp32 ? sv.stF.err_flag : sv.st.err_flag;
+  const int v = value;
+  CS_CUDA(sv, cudaMemcpyAsync(flag, &v, sizeof v, cudaMemcpyHostToDevice, sv.stream));
+  CS_CUDA(sv, cudaStreamSynchronize(sv.stream));
   return CS_OK;
 }
 

@@ -908,86 +908,75 @@ __global__ void k_apply_giveup(Dims d, DStateT<R> s, Range3 r) {
 }
 
 // STEP 8.a-c (421:4686-5567): B at the five quadrature points of each face,
-// averaged from both sides and shifted to the facial mean.  A block takes 32
-// faces: thread (w, face) with w = 3 side + component evaluates that side's
-// polynomial of B_component at the five points (in the state's type) into
-// shared memory, then the first warp forms each face's normal component
-// 0.5 (n . B_L + n . B_R) point by point and shifts it in FP64 so the five
-// values average to the FP64 face B exactly.
-constexpr int FB_FACES = 32;
+// averaged from both sides and shifted to the facial mean.
 template <typename R>
-__global__ void __launch_bounds__(FB_FACES * 6, 4) k_faceB(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r, int dir) {
-  __shared__ R bv[2][3][5][FB_FACES];  // [side][component][point][face]
+__global__ void __launch_bounds__(TPB) k_faceB(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r, int dir) {
   const int QP = dir == 0 ? CS_G_XF_QP : (dir == 1 ? CS_G_YF_QP : CS_G_ZF_QP);
   const int BW = dir == 0 ? CS_G_XB_QW : (dir == 1 ? CS_G_YB_QW : CS_G_ZB_QW);
   const int NF = dir == 0 ? CS_G_XF_N : (dir == 1 ? CS_G_YF_N : CS_G_ZF_N);
   double* Bq = s.Bq[dir];
   const double* Bf = dir == 0 ? s.Bxf : (dir == 1 ? s.Byf : s.Bzf);
-  const int lane = threadIdx.x % FB_FACES, w = threadIdx.x / FB_FACES;
-  const long long nf = r.count(), ntile = (nf + FB_FACES - 1) / FB_FACES;
-  for (long long tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
-    const long long t = tile * FB_FACES + lane;
-    const bool valid = t < nf;
-    int p = 0, i = 0, j = 0, k = 0;
-    if (valid) r.decode(t, p, i, j, k);
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < r.count(); t += (long long)gridDim.x * blockDim.x) {
+    int p, i, j, k;
+    r.decode(t, p, i, j, k);
     int lx = i, ly = j, lz = k, rx = i, ry = j, rz = k;
-    bool skip = !valid;
-    if (valid) {
-      if (dir == 0) {
-        const int mL = mask_at(g, d, p, i, j), mR = mask_at(g, d, p, i + 1, j);
-        rx = i + 1;
-        if (mL == 0 && mR == 1) { lx = sten(g, d, p, rx, ry, 1, 0); ly = sten(g, d, p, rx, ry, 1, 1); }
-        else if (mL == 1 && mR == 0) { rx = sten(g, d, p, lx, ly, 0, 0); ry = sten(g, d, p, lx, ly, 0, 1); }
-        else if (mL == 0 && mR == 0) skip = true;
-      } else if (dir == 1) {
-        const int mL = mask_at(g, d, p, i, j), mR = mask_at(g, d, p, i, j + 1);
-        ry = j + 1;
-        if (mL == 0 && mR == 1) { lx = sten(g, d, p, rx, ry, 3, 0); ly = sten(g, d, p, rx, ry, 3, 1); }
-        else if (mL == 1 && mR == 0) { rx = sten(g, d, p, lx, ly, 2, 0); ry = sten(g, d, p, lx, ly, 2, 1); }
-        else if (mL == 0 && mR == 0) skip = true;
-      } else {
-        if (mask_at(g, d, p, i, j) == 0) skip = true;
-        rz = k + 1;
-      }
+    bool skip = false;
+    if (dir == 0) {
+      const int mL = mask_at(g, d, p, i, j), mR = mask_at(g, d, p, i + 1, j);
+      rx = i + 1;
+      if (mL == 0 && mR == 1) { lx = sten(g, d, p, rx, ry, 1, 0); ly = sten(g, d, p, rx, ry, 1, 1); }
+      else if (mL == 1 && mR == 0) { rx = sten(g, d, p, lx, ly, 0, 0); ry = sten(g, d, p, lx, ly, 0, 1); }
+      else if (mL == 0 && mR == 0) skip = true;
+    } else if (dir == 1) {
+      const int mL = mask_at(g, d, p, i, j), mR = mask_at(g, d, p, i, j + 1);
+      ry = j + 1;
+      if (mL == 0 && mR == 1) { lx = sten(g, d, p, rx, ry, 3, 0); ly = sten(g, d, p, rx, ry, 3, 1); }
+      else if (mL == 1 && mR == 0) { rx = sten(g, d, p, lx, ly, 2, 0); ry = sten(g, d, p, lx, ly, 2, 1); }
+      else if (mL == 0 && mR == 0) skip = true;
+    } else {
+      if (mask_at(g, d, p, i, j) == 0) skip = true;
+      rz = k + 1;
     }
+    // the two sides' values in the state's type; the shift to the facial
+    // mean in FP64, so the values average to the FP64 face B exactly
+    R bq[5] = {R(0), R(0), R(0), R(0), R(0)};
     if (!skip) {
-      const int side = w / 3, b = w % 3;
-      const int zx = side ? rx : lx, zy = side ? ry : ly, zz = side ? rz : lz;
-      const R obl = R(1.0) / fmax(geoR<R>(g, d, CS_G_V_SCALE, 0, p, zx, zy, zz), R(ph.smallnum));
-      const R cx = geoR<R>(g, d, CS_G_V_CEN, 0, p, zx, zy, zz), cy = geoR<R>(g, d, CS_G_V_CEN, 1, p, zx, zy, zz),
-              cz = geoR<R>(g, d, CS_G_V_CEN, 2, p, zx, zy, zz);
-      R cc[10], v[10];
-      coef10(g, d, p, zx, zy, zz, cc);
+      const R obl0 = R(1.0) / fmax(geoR<R>(g, d, CS_G_V_SCALE, 0, p, lx, ly, lz), R(ph.smallnum));
+      const R obl02 = R(1.0) / fmax(geoR<R>(g, d, CS_G_V_SCALE, 0, p, rx, ry, rz), R(ph.smallnum));
+      R cL[10], cR[10], vL[3][10], vR[3][10];
+      coef10(g, d, p, lx, ly, lz, cL);
+      coef10(g, d, p, rx, ry, rz, cR);
 #pragma unroll
-      for (int m = 0; m < 10; ++m) v[m] = Vat(s, d, 5 + b, m, p, zx, zy, zz);
+      for (int b = 0; b < 3; ++b)
+#pragma unroll
+        for (int m = 0; m < 10; ++m) {
+          vL[b][m] = Vat(s, d, 5 + b, m, p, lx, ly, lz);
+          vR[b][m] = Vat(s, d, 5 + b, m, p, rx, ry, rz);
+        }
+      const R lcx = geoR<R>(g, d, CS_G_V_CEN, 0, p, lx, ly, lz), lcy = geoR<R>(g, d, CS_G_V_CEN, 1, p, lx, ly, lz),
+              lcz = geoR<R>(g, d, CS_G_V_CEN, 2, p, lx, ly, lz);
+      const R rcx = geoR<R>(g, d, CS_G_V_CEN, 0, p, rx, ry, rz), rcy = geoR<R>(g, d, CS_G_V_CEN, 1, p, rx, ry, rz),
+              rcz = geoR<R>(g, d, CS_G_V_CEN, 2, p, rx, ry, rz);
 #pragma unroll
       for (int q = 0; q < 5; ++q) {
-        const R x = (geoR<R>(g, d, QP, q, p, i, j, k) - cx) * obl;
-        const R y = (geoR<R>(g, d, QP, 5 + q, p, i, j, k) - cy) * obl;
-        const R z = (geoR<R>(g, d, QP, 10 + q, p, i, j, k) - cz) * obl;
-        bv[side][b][q][lane] = d_poly10(v, cc, x, y, z);
+        const int nq = dir == 2 ? q : 0, ns = dir == 2 ? 5 : 1;
+        const R nx = geoR<R>(g, d, NF, 0 * ns + nq, p, i, j, k), ny = geoR<R>(g, d, NF, 1 * ns + nq, p, i, j, k),
+                nz = geoR<R>(g, d, NF, 2 * ns + nq, p, i, j, k);
+        const R px = geoR<R>(g, d, QP, q, p, i, j, k), py = geoR<R>(g, d, QP, 5 + q, p, i, j, k),
+                pz = geoR<R>(g, d, QP, 10 + q, p, i, j, k);
+        const R x = (px - lcx) * obl0, y = (py - lcy) * obl0, z = (pz - lcz) * obl0;
+        const R x2 = (px - rcx) * obl02, y2 = (py - rcy) * obl02, z2 = (pz - rcz) * obl02;
+        const R bx = d_poly10(vL[0], cL, x, y, z), by = d_poly10(vL[1], cL, x, y, z), bz = d_poly10(vL[2], cL, x, y, z);
+        const R bx2 = d_poly10(vR[0], cR, x2, y2, z2), by2 = d_poly10(vR[1], cR, x2, y2, z2),
+                bz2 = d_poly10(vR[2], cR, x2, y2, z2);
+        bq[q] = R(0.5) * (nx * (bx + bx2) + ny * (by + by2) + nz * (bz + bz2));
       }
     }
-    __syncthreads();
-    if (w == 0 && valid) {
-      R bq[5] = {R(0), R(0), R(0), R(0), R(0)};
-      if (!skip) {
+    double bd = Bf[d.at(0, p, i, j, k)];
 #pragma unroll
-        for (int q = 0; q < 5; ++q) {
-          const int nq = dir == 2 ? q : 0, ns = dir == 2 ? 5 : 1;
-          const R nx = geoR<R>(g, d, NF, nq, p, i, j, k), ny = geoR<R>(g, d, NF, ns + nq, p, i, j, k),
-                  nz = geoR<R>(g, d, NF, 2 * ns + nq, p, i, j, k);
-          bq[q] = R(0.5) * (nx * (bv[0][0][q][lane] + bv[1][0][q][lane]) + ny * (bv[0][1][q][lane] + bv[1][1][q][lane]) +
-                            nz * (bv[0][2][q][lane] + bv[1][2][q][lane]));
-        }
-      }
-      double bd = Bf[d.at(0, p, i, j, k)];
+    for (int q = 0; q < 5; ++q) bd = bd - geo(g, d, BW, q, p, i, j, k) * (double)bq[q];
 #pragma unroll
-      for (int q = 0; q < 5; ++q) bd = bd - geo(g, d, BW, q, p, i, j, k) * (double)bq[q];
-#pragma unroll
-      for (int q = 0; q < 5; ++q) Bq[d.at(q, p, i, j, k)] = (double)bq[q] + bd;
-    }
-    __syncthreads();
+    for (int q = 0; q < 5; ++q) Bq[d.at(q, p, i, j, k)] = (double)bq[q] + bd;
   }
 }
 
@@ -2050,13 +2039,12 @@ void launch_faceB_adp_t(Solve& sv, DStateT<R>& st) {
   Range3 fx = {1 - G, N + G - 1, 2 - G, N + G - 1, 2 - G, nr + G - 1};
   Range3 fy = {2 - G, N + G - 1, 1 - G, N + G - 1, 2 - G, nr + G - 1};
   Range3 fz = {2 - G, N + G - 1, 2 - G, N + G - 1, 1 - G, nr + G - 1};
-  const Range3 fr[3] = {fx, fy, fz};
-  for (int dir = 0; dir < 3; ++dir) {
-    const long long nt = (fr[dir].count() + FB_FACES - 1) / FB_FACES;
-    const int nb = (int)std::min<long long>(nt, (long long)grid_sms(sv) * 16);
-    k_faceB<R><<<nb, FB_FACES * 6, 0, sv.stream>>>(d, sv.ph, sv.g, st, fr[dir], dir);
-    mark(sv, "k_faceB");
-  }
+  k_faceB<R><<<blocks_for(fx.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, fx, 0);
+  mark(sv, "k_faceB");
+  k_faceB<R><<<blocks_for(fy.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, fy, 1);
+  mark(sv, "k_faceB");
+  k_faceB<R><<<blocks_for(fz.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, fz, 2);
+  mark(sv, "k_faceB");
   Range3 a = shrink(d, 1);
   if (st.adp_lu && st.adp_pmap) {
     k_adp_rhs6<R><<<blocks_for(a.count() / 6, ADPR_TPB, grid_sms(sv)), ADPR_TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st,

@@ -296,6 +296,16 @@ int cs_cleanup_after_update(cs_ctx* ctx);
  * applied (0-15) plus 1 where the zone gave up (440:553-830). */
 int cs_debug_get(cs_ctx* ctx, int32_t which, double* host_out, size_t n_doubles);
 
+/* Test hook of the error path of the bounded device waits: the kernels
+ * that wait on an mbarrier for a bulk or tensor copy (the ADP substitution,
+ * STEP 7.b's row weights) give up after a fixed number of polls and set a
+ * per-context device flag, which the next read of the time step turns into
+ * CS_ERR_CUDA ("a bounded device wait gave up").  This sets that flag to
+ * value from the host (nonzero: as if a wait had given up; 0: clears it),
+ * so the path can be tested without making a device wait fail.  No
+ * counterpart in the reference. */
+int cs_debug_set_wait_error(cs_ctx* ctx, int32_t value);
+
 /* Timing and launch accounting.  cs_get_stream returns the context's
  * cudaStream_t (as void*) so a caller can order its own work and events
  * after the library's.  Between cs_profile_begin and cs_profile_end every

@@ -445,3 +445,21 @@ def test_step10_min_max_match_oracle(name, flags):
     plain.mesh_build()
     with pytest.raises(cs.CsError):
         plain.limit_minmax()  # not evaluated without the flag
+
+
+@pytest.mark.parametrize("flags", [0, cs.CS_FLAG_FP32])
+def test_a_bounded_wait_that_gave_up_fails_the_step(flags):
+    """The device flag a bounded mbarrier wait sets when it gives up (here
+    set from the host: no device wait is made to fail) turns the next step
+    into CS_ERR_CUDA with the reason; cleared, the solve steps again."""
+    pr = cs.preset("shell16")
+    s = cs.Solve(**pr["params"], flags=flags)
+    s.mesh_build()
+    s.init_problem(**pr["init"])
+    dt = s.evaluate_timestep(1e30)
+    assert s.lib.cs_debug_set_wait_error(s.h, 1) == 0
+    with pytest.raises(cs.CsError, match="bounded device wait"):
+        s.step(dt)
+    assert s.lib.cs_debug_set_wait_error(s.h, 0) == 0
+    s.init_problem(**pr["init"])
+    assert s.step(s.evaluate_timestep(1e30)) > 0

@@ -57,3 +57,18 @@ def test_reference_arm_under_two_ranks_prints_one_line():
     assert len(lines) == 1
     rec = json.loads(lines[0])
     assert rec["impl"] == "reference" and rec["n_gpus"] == 2 and rec["value"] > 0
+
+
+def test_path_bytes_follow_the_compulsory_state_traffic():
+    """Algorithmic bytes per zone-update of the path: every stage reads and
+    writes the 12-word state (60 B in the precision form), later stages also
+    read the stage-start copy: RK2 / IMEX-RK2 480 B (300 B), SSP-RK3 768 B
+    (480 B)."""
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    assert bench.path_bytes_per_zone_update(2, False) == 480.0
+    assert bench.path_bytes_per_zone_update(4, False) == 480.0
+    assert bench.path_bytes_per_zone_update(4, True) == 300.0
+    assert bench.path_bytes_per_zone_update(3, False) == 768.0
+    assert bench.path_bytes_per_zone_update(3, True) == 480.0
