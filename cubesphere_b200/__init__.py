@@ -89,6 +89,7 @@ CS_FLAG_FP32 = 8
 CS_FLAG_ADP_PER_PANEL = 16
 CS_FLAG_LSQ_PER_PANEL = 32
 CS_FLAG_STEP10 = 64
+CS_FLAG_P2 = 128
 
 
 def make_params(**kw) -> CsParams:

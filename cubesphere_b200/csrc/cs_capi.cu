@@ -425,6 +425,10 @@ bool check_params(const cs_params& p, std::string& why) {
     why = "radial boundary codes must be 2 (outflow) or 0 (none)";
     return false;
   }
+  if ((p.flags & CS_FLAG_P2) && (p.flags & CS_FLAG_NO_OP_CACHE)) {
+    why = "CS_FLAG_P2 needs the resident stencil operators (not CS_FLAG_NO_OP_CACHE)";
+    return false;
+  }
   return true;
 }
 
@@ -479,6 +483,9 @@ int alloc_state(Solve& sv, DStateT<R>& s) {
   s.op_m10 = (R*)m.op_m10;
   s.lsq_map9 = m.m9_shared ? (const LsqPanelMap*)m.lsq_map : nullptr;
   s.lsq_map10 = m.m10_shared ? (const LsqPanelMap*)m.lsq_map : nullptr;
+  s.op_p2v = (R*)m.op_p2v;
+  s.op_p2e = (R*)m.op_p2e;
+  s.p2_map = m.p2_shared ? (const LsqPanelMap*)m.lsq_map : nullptr;
   s.adp_lu = m.adp_lu;
   s.adp_piv = m.adp_piv;
   s.adp_pmap = m.adp_pmap;
@@ -777,6 +784,20 @@ int mesh_operators(Solve& sv, MeshRes& m, DStateT<R>& s) {
         CS_CUDA(sv, cudaStreamSynchronize(sv.stream));  // qmap is a stack array
       }
     }
+    // CS_FLAG_P2: the inverses of the eight one-sided stencils of STEPS 7.a
+    // (9 x 9) and 9.b (10 x 10) of every zone, with the same panel maps as
+    // the row weights.  P2 has no in-stage rebuild, so no room is an error.
+    if (sv.p.flags & CS_FLAG_P2) {
+      if (!m.op_m10) return fail(sv, CS_ERR_NOMEM, "no device room for the least-squares operators CS_FLAG_P2 needs");
+      m.p2_shared = shared;
+      const long long np = shared ? nl / 6 : nl;
+      const size_t pb = (size_t)np * (648 + 800) * sizeof(R);
+      if (cudaMemGetInfo(&fr, &tot) != cudaSuccess || pb + (size_t)8 * S6 + ((size_t)2 << 30) >= fr)
+        return fail(sv, CS_ERR_NOMEM, "no device room for the CS_FLAG_P2 stencil inverses");
+      m.op_p2v = mdalloc(sv, m, (size_t)np * 648 * sizeof(R), e);
+      m.op_p2e = m.op_p2v ? mdalloc(sv, m, (size_t)np * 800 * sizeof(R), e) : nullptr;
+      if (!m.op_p2v || !m.op_p2e) return cuda_fail(sv, e, "cudaMalloc(P2 stencil inverses)");
+    }
   }
   if (!(sv.p.flags & CS_FLAG_NO_ADP_CACHE)) {
     int8_t pmap[6 * 72];
@@ -809,6 +830,9 @@ int mesh_operators(Solve& sv, MeshRes& m, DStateT<R>& s) {
   s.op_m10 = (R*)m.op_m10;
   s.lsq_map9 = m.m9_shared ? (const LsqPanelMap*)m.lsq_map : nullptr;
   s.lsq_map10 = m.m10_shared ? (const LsqPanelMap*)m.lsq_map : nullptr;
+  s.op_p2v = (R*)m.op_p2v;
+  s.op_p2e = (R*)m.op_p2e;
+  s.p2_map = m.p2_shared ? (const LsqPanelMap*)m.lsq_map : nullptr;
   s.adp_lu = m.adp_lu;
   s.adp_piv = m.adp_piv;
   launch_ops_build(sv);
@@ -824,7 +848,7 @@ std::string mesh_key(const cs_params& p) {
   std::snprintf(b, sizeof b, "%d/%d/%d/%d/%.17g/%.17g/%.17g/%.17g/%d", p.ntp, p.nr, p.nghost, p.radial_mesh, p.rmin,
                 p.rmax, p.radial_ratio, p.smallnum,
                 p.flags & (CS_FLAG_NO_ADP_CACHE | CS_FLAG_NO_OP_CACHE | CS_FLAG_NO_PANEL_SYNC | CS_FLAG_FP32 |
-                           CS_FLAG_ADP_PER_PANEL | CS_FLAG_LSQ_PER_PANEL));
+                           CS_FLAG_ADP_PER_PANEL | CS_FLAG_LSQ_PER_PANEL | CS_FLAG_P2));
   return b;
 }
 

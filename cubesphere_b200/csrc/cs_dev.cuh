@@ -72,6 +72,9 @@ struct DStateT {
   R* op_m10;                             // STEP 9.c row weights Minv A_rr^T, [19 x 10][zones of shrink(2)], or null
   const LsqPanelMap* lsq_map9;           // op_m9 shared by the panels (panel 1's zones only), or null
   const LsqPanelMap* lsq_map10;          // op_m10 likewise
+  R* op_p2v;                             // CS_FLAG_P2 STEP 7.a stencil inverses, [8 x 9 x 9][zones of shrink(2)], or null
+  R* op_p2e;                             // CS_FLAG_P2 STEP 9.b stencil inverses, [8 x 10 x 10][zones of shrink(2)], or null
+  const LsqPanelMap* p2_map;             // op_p2v / op_p2e shared by the panels, or null
   void* adp_lu;                          // ADP KKT factors, per block of zones [1296 in use order][block], or null:
                                          // FP64 per panel; panel 1's (adp_pmap set) in the state's type R
   int8_t* adp_piv;                       // their row permutation, per block [36][block]

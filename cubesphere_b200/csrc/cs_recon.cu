@@ -287,9 +287,11 @@ __device__ __noinline__ void mbar_wait(uint64_t* bar, uint32_t parity, int* err)
 // w + 6 (STEP 7.a: primitives 0-7, 8 = entropy; STEP 9.b: E component w),
 // it forms the eight stencil gradients and their mean and combines them
 // with the WENO weights (IS + eps)^-4, central weight 100 (421:3116-3432),
-// so no thread keeps the 72 inverse entries in registers.
+// so no thread keeps the 72 inverse entries in registers.  kEnt: the
+// entropy only (LIMIT_ALL_SLOPES_P2's STEP 7.a limits the entropy this way,
+// 420:5396-6306, and the primitives with k_p2).
 constexpr int W7A_ZT = 32;
-template <bool kE, typename R>
+template <bool kE, typename R, bool kEnt = false>
 __global__ void __launch_bounds__(W7A_ZT * 3, sizeof(R) == 4 ? 8 : 6) k_weno_ao_split(Dims d, PhysC ph, DGeom g,
                                                                                         DStateT<R> s, Range3 r) {
   __shared__ R ai[72][W7A_ZT];  // [stencil * 9 + entry][zone]
@@ -340,7 +342,7 @@ __global__ void __launch_bounds__(W7A_ZT * 3, sizeof(R) == 4 ? 8 : 6) k_weno_ao_
     __syncthreads();
     if (act) {
 #pragma unroll 1
-      for (int q = w; q < (kE ? 3 : 9); q += 3) {
+      for (int q = kEnt ? (w == 2 ? 8 : 9) : w; q < (kE ? 3 : 9); q += 3) {
         const R* f = kE ? s.Esnap + ((long long)q * NPANEL + p) * d.S
                         : (q < 8 ? s.V + ((long long)q * NPANEL + p) * d.S : s.ent + (long long)p * d.S);
         const R f0 = f[d.idx(i, j, k)];
@@ -1673,6 +1675,250 @@ __global__ void k_ops_m10(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
   }
 }
 
+// ---------------------------------------------------------------------
+// LIMIT_ALL_SLOPES_P2 (400riemann_integrate/420limit_all_slopes_p2.f,
+// CS_FLAG_P2): STEP 7.a of the primitives (420:2459-5394) and STEP 9.b of E
+// (420:8553-12285), the two steps where it differs from P12.
+//
+// Row rr (0..8) of one-sided stencil st around (i, j, k).  The stencils, in
+// the reference's order (420:2596-4329): (R,U,+1), (L,U,+1), (L,D,+1),
+// (R,D,+1), then the same with radial offset -1; with a the R / L
+// neighbour, b the U / D neighbour and dz the radial direction, the rows are
+// a, b, the zone at dz, aa, bb, the zone at 2 dz, the corner between a and
+// b, a at dz, b at dz.  With rr a compile-time constant (unrolled loop)
+// each neighbour is a select among registers, whatever st is.
+__device__ __forceinline__ void p2_zone(const Nbr12& n, int st, int rr, int i, int j, int k, int& zx, int& zy,
+                                        int& zz) {
+  const int q = st & 3, dz = st < 4 ? 1 : -1;
+  const bool R_ = q == 0 || q == 3, U_ = q < 2;
+  zx = i;
+  zy = j;
+  zz = k;
+  switch (rr) {
+    case 0: case 7:  // a
+      zx = R_ ? n.x[0] : n.x[1];
+      zy = R_ ? n.y[0] : n.y[1];
+      break;
+    case 1: case 8:  // b
+      zx = U_ ? n.x[2] : n.x[3];
+      zy = U_ ? n.y[2] : n.y[3];
+      break;
+    case 3:  // aa
+      zx = R_ ? n.x[4] : n.x[5];
+      zy = R_ ? n.y[4] : n.y[5];
+      break;
+    case 4:  // bb
+      zx = U_ ? n.x[6] : n.x[7];
+      zy = U_ ? n.y[6] : n.y[7];
+      break;
+    case 6:  // corner RU, LU, LD, RD
+      zx = q == 0 ? n.x[8] : (q == 1 ? n.x[9] : (q == 2 ? n.x[10] : n.x[11]));
+      zy = q == 0 ? n.y[8] : (q == 1 ? n.y[9] : (q == 2 ? n.y[10] : n.y[11]));
+      break;
+    default: break;
+  }
+  if (rr == 2 || rr == 7 || rr == 8) zz = k + dz;
+  if (rr == 5) zz = k + 2 * dz;
+}
+
+// The inverses of every zone's eight one-sided stencil matrices (geometry
+// only), built once per mesh: STEP 7.a's 9 x 9 RECONSTRUCTION_COEFS systems
+// (the modes x .. xz from the zone-average differences) into
+// op_p2v[(st * 9 + m) * 9 + rr][zone] and STEP 9.b's 10 x 10
+// INTERPOLATION_COEFS systems (the zone itself first, modes 1 .. xz from
+// the point values) into op_p2e[(st * 10 + m) * 10 + rr][zone], inverted by
+// MATINV's LU (121matinv.f:8).  Shared by the panels: panel 1's zones only.
+template <typename R>
+__global__ void k_ops_p2(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
+  const long long nr_ = s.p2_map ? r.count() / 6 : r.count();
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nr_; t += (long long)gridDim.x * blockDim.x) {
+    int p, i, j, k;
+    r.decode(t, p, i, j, k);
+    if (mask_at(g, d, p, i, j) != 1) continue;
+    const Nbr12 n = load_nbr(g, d, p, i, j);
+    const double l0 = fmax(geo(g, d, CS_G_V_SCALE, 0, p, i, j, k), ph.smallnum), obl0 = 1.0 / l0;
+    double c0[10];
+    coef10(g, d, p, i, j, k, c0);
+    const double cx = geo(g, d, CS_G_V_CEN, 0, p, i, j, k), cy = geo(g, d, CS_G_V_CEN, 1, p, i, j, k),
+                 cz = geo(g, d, CS_G_V_CEN, 2, p, i, j, k);
+    for (int st = 0; st < 8; ++st) {
+      double A[81], Ai[81], B[100], Bi[100];
+      for (int m = 0; m < 10; ++m) B[m] = m == 0 ? 1.0 : (m < 4 ? 0.0 : 0.0 * 0.0 - c0[m]);
+      for (int rr = 0; rr < 9; ++rr) {
+        int zx, zy, zz;
+        p2_zone(n, st, rr, i, j, k, zx, zy, zz);
+        const double x = (geo(g, d, CS_G_V_CEN, 0, p, zx, zy, zz) - cx) * obl0;
+        const double y = (geo(g, d, CS_G_V_CEN, 1, p, zx, zy, zz) - cy) * obl0;
+        const double z = (geo(g, d, CS_G_V_CEN, 2, p, zx, zy, zz) - cz) * obl0;
+        const double lj = fmax(geo(g, d, CS_G_V_SCALE, 0, p, zx, zy, zz), ph.smallnum);
+        const double rt = lj / l0, r2 = rt * rt;
+        const double sq[6] = {x * x, y * y, z * z, x * y, y * z, x * z};
+        double* a = A + 9 * rr;
+        a[0] = x;
+        a[1] = y;
+        a[2] = z;
+        for (int m = 0; m < 6; ++m) a[3 + m] = sq[m] - c0[4 + m] + geo(g, d, CS_G_COEF, 4 + m, p, zx, zy, zz) * r2;
+        double* e = B + 10 * (rr + 1);
+        e[0] = 1.0;
+        e[1] = x;
+        e[2] = y;
+        e[3] = z;
+        for (int m = 0; m < 6; ++m) e[4 + m] = sq[m] - c0[4 + m];
+      }
+      d_matinv<9>(A, Ai);
+      d_matinv<10>(B, Bi);
+      for (int e = 0; e < 81; ++e) s.op_p2v[(long long)(st * 81 + e) * nr_ + t] = (R)Ai[e];
+      for (int e = 0; e < 100; ++e) s.op_p2e[(long long)(st * 100 + e) * nr_ + t] = (R)Bi[e];
+    }
+  }
+}
+
+// STEP 7.a (kE false) / STEP 9.b (kE true) of LIMIT_ALL_SLOPES_P2.  A block
+// takes 32 zones and one warp per variable (the 8 primitives / the 3 E
+// components), a thread one (zone, variable): the nine stencils' modes
+// (eight one-sided from the resident inverses, the central one from
+// P12's resident row weights: STEP 7.b's 18-zone least squares, STEP 9.c's
+// 19-zone one), their smoothness indicators over the zone's unit cube
+// (420:5245-5257) and WENO weights 1 and 100 over (IS + smallnum)^4 (in
+// FP64 in every form), then the weighted modes, summed stencil by stencil
+// in the reference's order (the one-sided stencils' modes formed again
+// rather than kept: 72 values a thread).  STEP 7.a writes modes 2..10 damped
+// by the flattener; STEP 9.b only the point value, flattened toward the
+// unlimited one (the edge solver consumes nothing else).  With kShared
+// the inverses are panel 1's, rotated per panel like the row weights, and
+// iteration T covers tile T / 6 of panel T % 6 so that the six blocks
+// reading one tile's inverses run together.
+template <bool kE, bool kShared, typename R>
+__global__ void __launch_bounds__(32 * (kE ? 3 : 8)) k_p2(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
+  constexpr int NM = kE ? 10 : 9, NR = kE ? 10 : 9, M0 = kE ? 0 : 1, NO = kE ? 1 : 9;
+  constexpr int n18[18][2] = {{0, 0},  {1, 0},  {2, 0},  {3, 0},  {-1, 1}, {-1, -1}, {8, 0}, {9, 0},  {10, 0},
+                              {11, 0}, {0, 1},  {1, 1},  {0, -1}, {1, -1}, {2, 1},   {3, 1}, {2, -1}, {3, -1}};
+  const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;
+  const long long nz = r.count(), npp = nz / 6, nw = kShared ? npp : nz;
+  const long long ntile = kShared ? 6 * ((npp + 31) / 32) : (nz + 31) / 32;
+  for (long long T = blockIdx.x; T < ntile; T += gridDim.x) {
+    long long t, tw;
+    if (kShared) {
+      tw = (T / 6) * 32 + lane;
+      t = (T % 6) * npp + tw;
+      if (tw >= npp) continue;
+    } else {
+      t = tw = T * 32 + lane;
+      if (t >= nz) continue;
+    }
+    int p, i, j, k;
+    r.decode(t, p, i, j, k);
+    if (mask_at(g, d, p, i, j) != 1) continue;
+    const Nbr12 n = load_nbr(g, d, p, i, j);
+    // smoothness weight of each mode x .. xz over the unit cube
+    double wis[9];
+    {
+      const double ob12 = 1.0 / 12.0, ob180 = 1.0 / 180.0, ob144 = 1.0 / 144.0;
+      wis[0] = wis[1] = wis[2] = ob12;
+#pragma unroll
+      for (int m = 0; m < 3; ++m) {
+        const double cm = geo(g, d, CS_G_COEF, 4 + m, p, i, j, k), cc = geo(g, d, CS_G_COEF, 7 + m, p, i, j, k);
+        wis[3 + m] = (cm - ob12) * (cm - ob12) + ob180;
+        wis[6 + m] = cc * cc + ob144;
+      }
+    }
+    auto smooth = [&](const R* X) {  // X: modes x .. xz
+      return ((double)X[0] * X[0] + (double)X[1] * X[1] + (double)X[2] * X[2]) * wis[0] +
+             ((double)X[3] * X[3]) * wis[3] + ((double)X[4] * X[4]) * wis[4] + ((double)X[5] * X[5]) * wis[5] +
+             ((double)X[6] * X[6]) * wis[6] + ((double)X[7] * X[7]) * wis[7] + ((double)X[8] * X[8]) * wis[8];
+    };
+    const R* f = (kE ? s.Esnap : s.V) + ((long long)q * NPANEL + p) * d.S;
+    const R f0 = f[d.idx(i, j, k)];
+    const unsigned long long qsrc = kShared ? s.p2_map[p].src : LSQ_IDENTITY_SRC;
+    const unsigned int qneg = kShared ? s.p2_map[p].neg : 0u;
+    const R* op = (kE ? s.op_p2e : s.op_p2v) + tw;
+    // modes of one-sided stencil st (rotated to this panel); only the first
+    // nm of them when the caller needs no more
+    auto stencil = [&](int st, int nm, R* X) {
+      R Rv[NR];
+#pragma unroll
+      for (int rr = 0; rr < NR; ++rr) {
+        int zx = i, zy = j, zz = k;
+        if (!kE || rr > 0) p2_zone(n, st, rr - (kE ? 1 : 0), i, j, k, zx, zy, zz);
+        const R v = f[d.idx(zx, zy, zz)];
+        Rv[rr] = kE ? v : v - f0;
+      }
+      R Y[NM];
+#pragma unroll
+      for (int m = 0; m < NM; ++m) {
+        R acc = R(0.0);
+        if (m < nm) {  // the constant mode (E's only one in pass 2) is never permuted
+#pragma unroll
+          for (int rr = 0; rr < NR; ++rr) acc = acc + __ldg(op + (long long)((st * NM + m) * NR + rr) * nw) * Rv[rr];
+        }
+        Y[m] = acc;
+      }
+#pragma unroll
+      for (int m = 0; m < NM; ++m) X[m] = kShared ? lsq_rotated<M0>(Y, m + M0, qsrc, qneg) : Y[m];
+    };
+    double IS[9];
+    R X8[NM];
+    {  // central stencil from the resident row weights
+      R Y[NM];
+#pragma unroll
+      for (int m = 0; m < NM; ++m) Y[m] = R(0.0);
+      const LsqPanelMap* cmap = kE ? s.lsq_map10 : s.lsq_map9;
+      const long long tc = cmap ? t - (long long)p * npp : t, ncw = cmap ? npp : nz;
+      const R* wc = (kE ? s.op_m10 : s.op_m9) + tc;
+      const long long cstride = kE ? ncw : m9_stride(ncw);
+#pragma unroll
+      for (int rr = 0; rr < NR + 9; ++rr) {
+        const int ro = kE ? rr - 1 : rr;  // E: the zone itself first
+        const int w = ro < 0 ? -1 : n18[ro][0], dz = ro < 0 ? 0 : n18[ro][1];
+        const R v = f[d.idx(w < 0 ? i : n.x[w], w < 0 ? j : n.y[w], k + dz)];
+        const R Rv = kE ? v : v - f0;
+#pragma unroll
+        for (int m = 0; m < NM; ++m) Y[m] = Y[m] + __ldg(wc + (long long)(rr * NM + m) * cstride) * Rv;
+      }
+      const unsigned long long csrc = cmap ? cmap[p].src : LSQ_IDENTITY_SRC;
+      const unsigned int cneg = cmap ? cmap[p].neg : 0u;
+#pragma unroll
+      for (int m = 0; m < NM; ++m) X8[m] = cmap ? lsq_rotated<M0>(Y, m + M0, csrc, cneg) : Y[m];
+      IS[8] = smooth(X8 + (kE ? 1 : 0));
+    }
+#pragma unroll 1
+    for (int st = 0; st < 8; ++st) {
+      R X[NM];
+      stencil(st, NM, X);
+      IS[st] = smooth(X + (kE ? 1 : 0));
+    }
+    double W[9];
+#pragma unroll
+    for (int st = 0; st < 9; ++st) {
+      const double tt = IS[st] + ph.smallnum, t2 = tt * tt;
+      W[st] = (st < 8 ? 1.0 : 100.0) / (t2 * t2);
+    }
+    const double wn = 1.0 / (W[0] + W[1] + W[2] + W[3] + W[4] + W[5] + W[6] + W[7] + W[8]);
+#pragma unroll
+    for (int st = 0; st < 9; ++st) W[st] = W[st] * wn;
+    double acc[NO];
+#pragma unroll
+    for (int m = 0; m < NO; ++m) acc[m] = 0.0;
+#pragma unroll 1
+    for (int st = 0; st < 8; ++st) {
+      R X[NM];
+      stencil(st, NO, X);
+      const double ws = W[st];
+#pragma unroll
+      for (int m = 0; m < NO; ++m) acc[m] = st == 0 ? ws * (double)X[m] : acc[m] + ws * (double)X[m];
+    }
+#pragma unroll
+    for (int m = 0; m < NO; ++m) acc[m] = acc[m] + W[8] * (double)X8[m];
+    const R fl = s.flatA[d.at(0, p, i, j, k)], x = R(1.0) - fl;
+    if (kE) {
+      s.E[d.at(q, p, i, j, k)] = fl * f0 + x * (R)acc[0];
+    } else {
+#pragma unroll
+      for (int m = 0; m < NO; ++m) Vat(s, d, q, 1 + m, p, i, j, k) = (R)acc[m] * x;
+    }
+  }
+}
+
 inline Range3 zones_all(const Dims& d) { return {1 - d.G, d.N + d.G, 1 - d.G, d.N + d.G, 1 - d.G, d.nr + d.G}; }
 inline Range3 shrink(const Dims& d, int s) {
   return {1 - d.G + s, d.N + d.G - s, 1 - d.G + s, d.N + d.G - s, 1 - d.G + s, d.nr + d.G - s};
@@ -1985,10 +2231,29 @@ void launch_flattener(Solve& sv) {
     launch_flattener_t(sv, sv.st);
 }
 
+// Grid of k_p2 over range b: 32-zone tiles (panel-interleaved when shared).
+inline int p2_blocks(Solve& sv, const Range3& b, bool shared) {
+  const long long npp = b.count() / 6;
+  const long long nt = shared ? 6 * ((npp + 31) / 32) : (b.count() + 31) / 32;
+  return (int)std::min<long long>(nt, (long long)grid_sms(sv) * 16);
+}
+
 template <typename R>
 void launch_weno_t(Solve& sv, DStateT<R>& st) {
   const Dims& d = sv.d;
   Range3 a = shrink(d, 1), b = shrink(d, 2);
+  if (sv.p.flags & CS_FLAG_P2) {  // LIMIT_ALL_SLOPES_P2's STEP 7.a
+    const long long nt = (b.count() + W7A_ZT - 1) / W7A_ZT;
+    const int nb = (int)std::min<long long>(nt, (long long)grid_sms(sv) * 16);
+    k_weno_ao_split<false, R, true><<<nb, W7A_ZT * 3, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
+    mark(sv, "k_p2_entropy");
+    if (st.p2_map)
+      k_p2<false, true, R><<<p2_blocks(sv, b, true), 256, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
+    else
+      k_p2<false, false, R><<<p2_blocks(sv, b, false), 256, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
+    mark(sv, "k_p2_prim");
+    return;
+  }
   {
     const long long nt = (a.count() + W7A_ZT - 1) / W7A_ZT;
     const int nb = (int)std::min<long long>(nt, (long long)grid_sms(sv) * 16);
@@ -2096,6 +2361,10 @@ void launch_ops_build_t(Solve& sv, DStateT<R>& st) {
     k_ops_m10<R><<<blocks_for(b.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
     mark(sv, "k_ops_m10");
   }
+  if (st.op_p2v) {
+    k_ops_p2<R><<<blocks_for(b.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
+    mark(sv, "k_ops_p2");
+  }
 }
 
 void launch_ops_build(Solve& sv) {
@@ -2151,6 +2420,14 @@ void launch_efield_t(Solve& sv, DStateT<R>& st) {
   Range3 z = zones_all(d), a = shrink(d, 1), b = shrink(d, 2);
   k_efield_a<R><<<blocks_for(z.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.g, st, z);
   mark(sv, "k_efield_a");
+  if (sv.p.flags & CS_FLAG_P2) {  // LIMIT_ALL_SLOPES_P2's STEP 9.b
+    if (st.p2_map)
+      k_p2<true, true, R><<<p2_blocks(sv, b, true), 96, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
+    else
+      k_p2<true, false, R><<<p2_blocks(sv, b, false), 96, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
+    mark(sv, "k_p2_efield");
+    return;
+  }
   {
     const long long nt = (a.count() + W7A_ZT - 1) / W7A_ZT;
     const int nb = (int)std::min<long long>(nt, (long long)grid_sms(sv) * 16);

@@ -64,6 +64,8 @@ size_t mesh_device_bytes(const cs_params& p) {
     const bool f32 = (p.flags & CS_FLAG_FP32) != 0, per = (p.flags & CS_FLAG_LSQ_PER_PANEL) != 0;
     const size_t n9 = (per || !f32) ? nl : nl / 6, n10 = per ? nl : nl / 6;
     bytes += (m9_stride(n9) * 162 + n10 * 190) * (f32 ? sizeof(float) : sizeof(double));
+    // CS_FLAG_P2's one-sided stencil inverses, shared like STEP 9.c's
+    if (p.flags & CS_FLAG_P2) bytes += n10 * (648 + 800) * (f32 ? sizeof(float) : sizeof(double));
   }
   if (!(p.flags & CS_FLAG_NO_ADP_CACHE)) {
     // factors shared by the six panels (in the state's type) unless

@@ -62,6 +62,9 @@ struct MeshRes {
   void* op_m10 = nullptr;
   void* lsq_map = nullptr;  // LsqPanelMap[6] when row weights are panel 1's only
   bool m9_shared = false, m10_shared = false;  // which of op_m9 / op_m10 are panel 1's only
+  void* op_p2v = nullptr;  // CS_FLAG_P2 one-sided stencil inverses (state's type)
+  void* op_p2e = nullptr;
+  bool p2_shared = false;  // op_p2v / op_p2e are panel 1's only
   CUtensorMap m9_map{};  // tensor map of op_m9 as [162 rows][m9_stride zones], 32 x 162 boxes
   void* adp_lu = nullptr;   // FP64 per panel; panel-shared ones in the state's type
   int8_t* adp_piv = nullptr;

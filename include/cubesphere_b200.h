@@ -155,6 +155,23 @@ typedef struct cs_params {
  * it costs one reduction over the interior per stage. */
 #define CS_FLAG_STEP10 64
 
+/* cs_params.flags: reconstruct with LIMIT_ALL_SLOPES_P2
+ * (400riemann_integrate/420limit_all_slopes_p2.f:9), the full third-order
+ * WENO-AO the reference driver calls in place of LIMIT_ALL_SLOPES_P12
+ * (1000riemann_geomesh_cs_mhd.f:2387-2391, same arguments).  It differs in
+ * two steps: STEP 7.a limits the primitives with eight one-sided 9-zone
+ * quadratic stencils and the central 18-zone least squares (420:2459-5394,
+ * replacing P12's STEPS 7.a and 7.b), and STEP 9.b interpolates E with
+ * eight one-sided 10-zone stencils and the central 19-zone least squares
+ * (420:8553-12285, replacing STEPS 9.b and 9.c); the entropy slopes and every
+ * other step are P12's.  The stencil inverses depend on the geometry only
+ * and are resident (built at cs_mesh_build, 5.2 KB (primitives) + 6.4 KB (E)
+ * per zone in FP64, shared by the six panels where they are rotations of one
+ * another): cs_create rejects the flag together with CS_FLAG_NO_OP_CACHE
+ * (CS_ERR_ARG), and cs_mesh_build fails with CS_ERR_NOMEM where the device
+ * has no room for them. */
+#define CS_FLAG_P2 128
+
 /* Seeded initial-state description (new generator cases of the problem
  * library, built with the reference mechanism of 820init_patch_cube_sphere.f). */
 typedef struct cs_init_desc {

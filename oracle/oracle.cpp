@@ -453,6 +453,248 @@ static void coef_at(const Ctx& c, int pn, int i, int j, int k, double* co) {
 }
 
 // ------------------------------------------------------------------
+// LIMIT_ALL_SLOPES_P2 (pkg/inc/cubesphere/400riemann_integrate/420limit_all_slopes_p2.f)
+// differs from P12 in STEP 7.a and STEP 9.b only.  Its eight one-sided
+// quadratic stencils, in the reference's order (R,U,+1), (L,U,+1), (L,D,+1),
+// (R,D,+1), then the same with radial offset -1 (420:2596-4329, 8687-10120):
+// in-plane neighbour a (R = 0 / L = 1), in-plane neighbour b (U = 2 / D = 3),
+// radial direction dz and the corner zone between a and b.
+static const int kP2St[8][4] = {{0, 2, 1, 8},  {1, 2, 1, 9},  {1, 3, 1, 10},  {0, 3, 1, 11},
+                                {0, 2, -1, 8}, {1, 2, -1, 9}, {1, 3, -1, 10}, {0, 3, -1, 11}};
+
+// The nine zones of stencil s around (i, j, k): a, b, the zone at dz, aa,
+// bb, the zone at 2 dz, the corner, a at dz, b at dz.
+static void p2_zones(const Nb& n, int s, int i, int j, int k, int* zx, int* zy, int* zz) {
+  const int a = kP2St[s][0], b = kP2St[s][1], dz = kP2St[s][2], cn = kP2St[s][3];
+  const int w[9] = {a, b, -1, a + 4, b + 4, -1, cn, a, b};
+  const int o[9] = {0, 0, dz, 0, 0, 2 * dz, 0, dz, dz};
+  for (int r = 0; r < 9; ++r) {
+    zx[r] = w[r] < 0 ? i : n.x[w[r]];
+    zy[r] = w[r] < 0 ? j : n.y[w[r]];
+    zz[r] = k + o[r];
+  }
+}
+
+// Smoothness indicator of the nine non-constant modes X (x, y, z, xx, yy,
+// zz, xy, yz, xz) over the zone's unit cube (420:5245-5257, 10990-11002).
+static double p2_smoothness(const double* X, const double* c0) {
+  const double ob12 = 1.0 / 12.0, ob180 = 1.0 / 180.0, ob144 = 1.0 / 144.0;
+  return (X[0] * X[0] + X[1] * X[1] + X[2] * X[2]) * ob12 + (X[3] * X[3]) * (sq(c0[4] - ob12) + ob180) +
+         (X[4] * X[4]) * (sq(c0[5] - ob12) + ob180) + (X[5] * X[5]) * (sq(c0[6] - ob12) + ob180) +
+         (X[6] * X[6]) * (c0[7] * c0[7] + ob144) + (X[7] * X[7]) * (c0[8] * c0[8] + ob144) +
+         (X[8] * X[8]) * (c0[9] * c0[9] + ob144);
+}
+
+// Normalised WENO weights of the nine stencils: linear weights 1 (one-sided)
+// and 100 (central), divided by (IS + smallnum)^4 (420:5264-5277).
+static void p2_weights(const double* IS, double sm, double* W) {
+  for (int s = 0; s < 9; ++s) W[s] = (s < 8 ? 1.0 : 100.0) / pow4(IS[s] + sm);
+  double x = 1.0 / (W[0] + W[1] + W[2] + W[3] + W[4] + W[5] + W[6] + W[7] + W[8]);
+  for (int s = 0; s < 9; ++s) W[s] = W[s] * x;
+}
+
+// Scaled centroid offset of zone (x, y, z) from zone (i, j, k).
+static void p2_offset(const Ctx& c, int pn, int i, int j, int k, int zx, int zy, int zz, double obl0, double* o) {
+  for (int a = 0; a < 3; ++a) o[a] = (c.geo(V_CEN, a, pn, zx, zy, zz) - c.geo(V_CEN, a, pn, i, j, k)) * obl0;
+}
+
+// STEP 7.a of LIMIT_ALL_SLOPES_P2 (420:2459-5394) for the primitives: per
+// zone, the eight one-sided stencils' 9 x 9 reconstruction matrices
+// (RECONSTRUCTION_COEFS rows) inverted by MATINV and the central 18-zone
+// least squares (the STEP 7.b matrix of P12); per primitive, the nine
+// stencils' modes, their smoothness indicators and WENO weights, the
+// weighted modes 2..10 and the flattener.
+static void p2_limit_primitives(Ctx& c, int pn) {
+  const int N = c.N, G = c.G, nr = c.nr;
+  const double sm = c.p.smallnum;
+  auto V = [&](int comp, int mode, int i, int j, int k) -> double& { return c.a(c.V, mode * NV + comp, pn, i, j, k); };
+  OMP_ZONES
+  for (int k = 3 - G; k <= nr + G - 2; ++k)
+    for (int j = 3 - G; j <= N + G - 2; ++j)
+      for (int i = 3 - G; i <= N + G - 2; ++i) {
+        if (c.m(pn, i, j) != 1) continue;
+        Nb n = nbrs(c, pn, i, j);
+        const double l0 = std::max(c.geo(V_SCALE, 0, pn, i, j, k), sm), obl0 = 1.0 / l0;
+        double c0[10];
+        coef_at(c, pn, i, j, k, c0);
+        double Ai[8][81];
+        int zx[8][9], zy[8][9], zz[8][9];
+        for (int s = 0; s < 8; ++s) {
+          p2_zones(n, s, i, j, k, zx[s], zy[s], zz[s]);
+          double A[81];
+          for (int r = 0; r < 9; ++r) {
+            double o[3], cj[10];
+            p2_offset(c, pn, i, j, k, zx[s][r], zy[s][r], zz[s][r], obl0, o);
+            const double lj = std::max(c.geo(V_SCALE, 0, pn, zx[s][r], zy[s][r], zz[s][r]), sm);
+            coef_at(c, pn, zx[s][r], zy[s][r], zz[s][r], cj);
+            recon_row(o[0], o[1], o[2], l0, lj, c0, cj, A + 9 * r);
+          }
+          matinv(9, A, Ai[s]);
+        }
+        double A18[18][9];
+        int cx[18], cy[18], cz[18];
+        for (int r = 0; r < 18; ++r) {
+          const int w = kN18[r][0];
+          cx[r] = (w < 0) ? i : n.x[w];
+          cy[r] = (w < 0) ? j : n.y[w];
+          cz[r] = k + kN18[r][1];
+          double o[3], cj[10];
+          p2_offset(c, pn, i, j, k, cx[r], cy[r], cz[r], obl0, o);
+          const double lj = std::max(c.geo(V_SCALE, 0, pn, cx[r], cy[r], cz[r]), sm);
+          coef_at(c, pn, cx[r], cy[r], cz[r], cj);
+          recon_row(o[0], o[1], o[2], l0, lj, c0, cj, A18[r]);
+        }
+        double M[81], Minv[81];
+        for (int a2 = 0; a2 < 9; ++a2)
+          for (int b2 = 0; b2 < 9; ++b2) {
+            double s = 0.0;
+            for (int r = 0; r < 18; ++r) s = s + A18[r][a2] * A18[r][b2];
+            M[a2 * 9 + b2] = s;
+          }
+        matinv(9, M, Minv);
+        const double x = 1.0 - c.a(c.flat, 0, pn, i, j, k);
+        for (int q = 0; q < NV; ++q) {
+          const double v0 = V(q, 0, i, j, k);
+          double X[9][9], IS[9], W[9];  // X[stencil][mode]
+          for (int s = 0; s < 8; ++s) {
+            double R[9];
+            for (int r = 0; r < 9; ++r) R[r] = V(q, 0, zx[s][r], zy[s][r], zz[s][r]) - v0;
+            for (int a2 = 0; a2 < 9; ++a2) {
+              double t = 0.0;
+              for (int r = 0; r < 9; ++r) t = t + Ai[s][a2 * 9 + r] * R[r];
+              X[s][a2] = t;
+            }
+          }
+          double Y[9];
+          for (int a2 = 0; a2 < 9; ++a2) {
+            double t = 0.0;
+            for (int r = 0; r < 18; ++r) t = t + A18[r][a2] * (V(q, 0, cx[r], cy[r], cz[r]) - v0);
+            Y[a2] = t;
+          }
+          for (int a2 = 0; a2 < 9; ++a2) {
+            double t = 0.0;
+            for (int b2 = 0; b2 < 9; ++b2) t = t + Minv[a2 * 9 + b2] * Y[b2];
+            X[8][a2] = t;
+          }
+          for (int s = 0; s < 9; ++s) IS[s] = p2_smoothness(X[s], c0);
+          p2_weights(IS, sm, W);
+          for (int a2 = 0; a2 < 9; ++a2) {
+            double t = W[0] * X[0][a2];
+            for (int s = 1; s < 9; ++s) t = t + W[s] * X[s][a2];
+            V(q, 1 + a2, i, j, k) = t * x;
+          }
+        }
+        // entropy: P12's eight linear stencils and their mean (420:5396-6306)
+        double Al[8][3][3], gr[3];
+        stencil_inverses(c, pn, i, j, k, n, Al);
+        weno8(c, n, i, j, k, Al, [&](int x2, int y2, int z2) { return c.a(c.ent, 0, pn, x2, y2, z2); }, gr);
+        for (int r = 0; r < 3; ++r) c.a(c.ent, 1 + r, pn, i, j, k) = gr[r] * x;
+      }
+}
+
+// STEP 9.b of LIMIT_ALL_SLOPES_P2 (420:8553-12285): third-order
+// interpolation WENO of the zone-centred E components: the eight one-sided
+// 10-zone stencils (the zone and the nine zones of the primitive stencil,
+// INTERPOLATION_COEFS rows, 10 x 10 MATINV) and the central 19-zone least
+// squares (the STEP 9.c matrix of P12), WENO-weighted; the point value is
+// flattened toward the unlimited one and modes 2..10 damped.  Each zone
+// rewrites its own point value, so neighbours are read from the values
+// before the loop (parallel-loop semantics, order-free).
+static void p2_limit_efield(Ctx& c, int pn) {
+  const int N = c.N, G = c.G, nr = c.nr;
+  const double sm = c.p.smallnum;
+  auto E = [&](int comp, int mode, int i, int j, int k) -> double& { return c.a(c.E, mode * 3 + comp, pn, i, j, k); };
+  std::vector<double> esnap(3 * c.S);
+  for (int q = 0; q < 3; ++q)
+    std::memcpy(&esnap[(size_t)q * c.S], &c.E[((size_t)q * 6 + pn) * c.S], c.S * sizeof(double));
+  auto Es = [&](int q, int x, int y, int z) { return esnap[(size_t)q * c.S + c.idx(x, y, z)]; };
+  OMP_ZONES
+  for (int k = 3 - G; k <= nr + G - 2; ++k)
+    for (int j = 3 - G; j <= N + G - 2; ++j)
+      for (int i = 3 - G; i <= N + G - 2; ++i) {
+        if (c.m(pn, i, j) != 1) continue;
+        Nb n = nbrs(c, pn, i, j);
+        const double obl0 = 1.0 / std::max(c.geo(V_SCALE, 0, pn, i, j, k), sm);
+        double c0[10];
+        coef_at(c, pn, i, j, k, c0);
+        double Ai[8][100];
+        int zx[8][10], zy[8][10], zz[8][10];
+        for (int s = 0; s < 8; ++s) {
+          zx[s][0] = i;
+          zy[s][0] = j;
+          zz[s][0] = k;
+          p2_zones(n, s, i, j, k, zx[s] + 1, zy[s] + 1, zz[s] + 1);
+          double A[100];
+          for (int r = 0; r < 10; ++r) {
+            double o[3];
+            p2_offset(c, pn, i, j, k, zx[s][r], zy[s][r], zz[s][r], obl0, o);
+            if (r == 0) o[0] = o[1] = o[2] = 0.0;
+            interp_row(o[0], o[1], o[2], c0, A + 10 * r);
+          }
+          matinv(10, A, Ai[s]);
+        }
+        double A19[19][10];
+        int cx[19], cy[19], cz[19];
+        cx[0] = i;
+        cy[0] = j;
+        cz[0] = k;
+        interp_row(0.0, 0.0, 0.0, c0, A19[0]);
+        for (int r = 0; r < 18; ++r) {
+          const int w = kN18[r][0];
+          cx[r + 1] = (w < 0) ? i : n.x[w];
+          cy[r + 1] = (w < 0) ? j : n.y[w];
+          cz[r + 1] = k + kN18[r][1];
+          double o[3];
+          p2_offset(c, pn, i, j, k, cx[r + 1], cy[r + 1], cz[r + 1], obl0, o);
+          interp_row(o[0], o[1], o[2], c0, A19[r + 1]);
+        }
+        double M[100], Minv[100];
+        for (int a2 = 0; a2 < 10; ++a2)
+          for (int b2 = 0; b2 < 10; ++b2) {
+            double s = 0.0;
+            for (int r = 0; r < 19; ++r) s = s + A19[r][a2] * A19[r][b2];
+            M[a2 * 10 + b2] = s;
+          }
+        matinv(10, M, Minv);
+        const double f = c.a(c.flat, 0, pn, i, j, k), x = 1.0 - f;
+        for (int q = 0; q < 3; ++q) {
+          double X[9][10], IS[9], W[9];
+          for (int s = 0; s < 8; ++s) {
+            double R[10];
+            for (int r = 0; r < 10; ++r) R[r] = Es(q, zx[s][r], zy[s][r], zz[s][r]);
+            for (int a2 = 0; a2 < 10; ++a2) {
+              double t = 0.0;
+              for (int r = 0; r < 10; ++r) t = t + Ai[s][a2 * 10 + r] * R[r];
+              X[s][a2] = t;
+            }
+          }
+          double Y[10];
+          for (int a2 = 0; a2 < 10; ++a2) {
+            double t = 0.0;
+            for (int r = 0; r < 19; ++r) t = t + A19[r][a2] * Es(q, cx[r], cy[r], cz[r]);
+            Y[a2] = t;
+          }
+          for (int a2 = 0; a2 < 10; ++a2) {
+            double t = 0.0;
+            for (int b2 = 0; b2 < 10; ++b2) t = t + Minv[a2 * 10 + b2] * Y[b2];
+            X[8][a2] = t;
+          }
+          for (int s = 0; s < 9; ++s) IS[s] = p2_smoothness(X[s] + 1, c0);
+          p2_weights(IS, sm, W);
+          const double Ept = Es(q, i, j, k);
+          double e[10];
+          for (int a2 = 0; a2 < 10; ++a2) {
+            double t = W[0] * X[0][a2];
+            for (int s = 1; s < 9; ++s) t = t + W[s] * X[s][a2];
+            e[a2] = t;
+          }
+          E(q, 0, i, j, k) = f * Ept + x * e[0];
+          for (int a2 = 1; a2 < 10; ++a2) E(q, a2, i, j, k) = e[a2] * x;
+        }
+      }
+}
+
+// ------------------------------------------------------------------
 // LIMIT_ALL_SLOPES_P12 (pkg/inc/cubesphere/400riemann_integrate/421limit_all_slopes_p12.f:9-9985)
 // without its STEP 10 diagnostics, for one panel.
 void limit_all_slopes_p12(Ctx& c, int pn) {
@@ -565,6 +807,10 @@ void limit_all_slopes_p12(Ctx& c, int pn) {
           }
         }
   }
+  // CS_FLAG_P2: STEP 7.a of LIMIT_ALL_SLOPES_P2 in place of STEPS 7.a and 7.b
+  const bool p2 = (c.p.flags & CS_FLAG_P2) != 0;
+  if (p2) p2_limit_primitives(c, pn);
+  if (!p2) {  // P12 STEPS 7.a, 7.b
   // STEP 7.a (:2515-3804)
   OMP_ZONES
   for (int k = 2 - G; k <= nr + G - 1; ++k)
@@ -660,6 +906,7 @@ void limit_all_slopes_p12(Ctx& c, int pn) {
           for (int t = 1; t < 10; ++t) V(q, t, i, j, k) = V(q, t, i, j, k) * x;
         }
       }
+  }  // P12 STEPS 7.a, 7.b
   // STEP 7.c ENFORCE_PRESSURE_POSITIVITY_PRIM (440enforce_pressure_positivity_prim.f:204-829).
   // The zone loop is a parallel loop in the reference's GPU path; neighbour
   // entropy is read from the values before the loop (a zone that gives up
@@ -938,6 +1185,9 @@ void limit_all_slopes_p12(Ctx& c, int pn) {
         E(1, 0, i, j, k) = -(vz * Bx - vx * Bz);
         E(2, 0, i, j, k) = -(vx * By - vy * Bx);
       }
+  // CS_FLAG_P2: STEP 9.b of LIMIT_ALL_SLOPES_P2 in place of STEPS 9.b and 9.c
+  if (p2) p2_limit_efield(c, pn);
+  if (!p2) {  // P12 STEPS 9.b, 9.c
   // STEP 9.b WENO gradients of E (:6840-8400)
   OMP_ZONES
   for (int k = 2 - G; k <= nr + G - 1; ++k)
@@ -1034,6 +1284,7 @@ void limit_all_slopes_p12(Ctx& c, int pn) {
           for (int t = 0; t < 10; ++t) E(q, t, i, j, k) = e[t];
         }
       }
+  }  // P12 STEPS 9.b, 9.c
   // STEP 10 (:9354-9976): min and max over the active interior zones of the
   // zone primitives (B from STEP 8.d) and of the zone's net face flux of B
   // over max(|B| of the upper faces, |B| of the lower faces,

@@ -81,6 +81,80 @@ def linear_gradients():
     return g
 
 
+QUAD_A = {0: 2.0, 1: 0.1, 2: -0.2, 3: 0.05, 4: 3.0}
+QUAD_G = {0: (0.1, -0.05, 0.08), 1: (0.02, 0.01, -0.03), 2: (0.01, 0.02, 0.01), 3: (-0.01, 0.01, 0.02),
+          4: (0.2, 0.1, -0.1)}
+QUAD_H = {0: ((0.04, 0.01, -0.02), (0.01, 0.03, 0.005), (-0.02, 0.005, 0.05)),
+          1: ((0.01, 0.002, 0.0), (0.002, -0.01, 0.003), (0.0, 0.003, 0.02)),
+          2: ((-0.02, 0.0, 0.004), (0.0, 0.01, 0.002), (0.004, 0.002, 0.01)),
+          3: ((0.01, -0.003, 0.0), (-0.003, 0.02, 0.001), (0.0, 0.001, -0.01)),
+          4: ((0.06, 0.02, 0.01), (0.02, -0.03, 0.01), (0.01, 0.01, 0.05))}
+
+
+def quadratic_state(s):
+    """rho, v, p quadratic in the global coordinates (QUAD_A + QUAD_G . X +
+    X . QUAD_H . X / 2), each zone holding the exact zone average of its
+    primitive (the centroid value plus the second moments from the zone's
+    Taylor-basis coefficients: avg = q(c) + l^2 (H_xx C5 + H_yy C6 + H_zz C7)
+    / 2 + l^2 (H_xy C8 + H_yz C9 + H_xz C10)), and the linear
+    divergence-free field of linear_state.  Third-order stencils reproduce
+    its modes exactly: slopes l grad q(c), square modes l^2 H_aa / 2, cross
+    modes l^2 H_ab."""
+    x, y, z = s.geometry("V_CEN")
+    l = s.geometry("V_SCALE")[0]
+    C = s.geometry("COEF")
+    act = s.mask() == 1
+    prim = {}
+    for c in range(5):
+        g, H = np.array(QUAD_G[c]), np.array(QUAD_H[c])
+        X = (x, y, z)
+        val = QUAD_A[c] + sum(g[a] * X[a] for a in range(3)) + 0.5 * sum(
+            H[a, b] * X[a] * X[b] for a in range(3) for b in range(3))
+        mom = 0.5 * (H[0, 0] * C[4] + H[1, 1] * C[5] + H[2, 2] * C[6]) + H[0, 1] * C[7] + H[1, 2] * C[8] + H[0, 2] * C[9]
+        prim[c] = val + l * l * mom
+    B = np.stack([LIN_B * x, -2 * LIN_B * y, LIN_B * z])
+    U = cons_from_prims(prim[0], np.stack([prim[1], prim[2], prim[3]]), prim[4], B)
+    return _finish(s, U, prim[4], prim[0], lambda a, b, c: (LIN_B * a, -2 * LIN_B * b, LIN_B * c), act)
+
+
+def quadratic_modes(s):
+    """Per primitive 0..4: the exact modes 2..10 of quadratic_state, shape
+    (9,) + box."""
+    x, y, z = s.geometry("V_CEN")
+    l = s.geometry("V_SCALE")[0]
+    out = {}
+    for c in range(5):
+        g, H = np.array(QUAD_G[c]), np.array(QUAD_H[c])
+        X = (x, y, z)
+        grad = [g[a] + sum(H[a, b] * X[b] for b in range(3)) for a in range(3)]
+        out[c] = np.stack([l * grad[0], l * grad[1], l * grad[2],
+                           0.5 * l * l * H[0, 0] + 0 * x, 0.5 * l * l * H[1, 1] + 0 * x, 0.5 * l * l * H[2, 2] + 0 * x,
+                           l * l * H[0, 1] + 0 * x, l * l * H[1, 2] + 0 * x, l * l * H[0, 2] + 0 * x])
+    return out
+
+
+def linear_state_e_averages(s):
+    """Zone averages of E = -v x B for linear_state, per component (shape
+    box): v and B are linear, so E is quadratic with Hessian -(gv_a gB_b^T +
+    gB_b gv_a^T - gv_b gB_a^T - gB_a gv_b^T), and its zone average is the
+    centroid value plus the second-moment terms (quadratic_state)."""
+    x, y, z = s.geometry("V_CEN")
+    l = s.geometry("V_SCALE")[0]
+    C = s.geometry("COEF")
+    X = np.stack([x, y, z])
+    gv = [np.array(LIN[c][1:]) for c in (1, 2, 3)]
+    v0 = [LIN[c][0] for c in (1, 2, 3)]
+    gB = [np.array([LIN_B, 0.0, 0.0]), np.array([0.0, -2 * LIN_B, 0.0]), np.array([0.0, 0.0, LIN_B])]
+    val = lambda f0, g: f0 + np.tensordot(g, X, 1)
+    out = []
+    for a, b in ((1, 2), (2, 0), (0, 1)):
+        e = -(val(v0[a], gv[a]) * val(0.0, gB[b]) - val(v0[b], gv[b]) * val(0.0, gB[a]))
+        H = -(np.outer(gv[a], gB[b]) + np.outer(gB[b], gv[a]) - np.outer(gv[b], gB[a]) - np.outer(gB[a], gv[b]))
+        mom = 0.5 * (H[0, 0] * C[4] + H[1, 1] * C[5] + H[2, 2] * C[6]) + H[0, 1] * C[7] + H[1, 2] * C[8] + H[0, 2] * C[9]
+        out.append(e + l * l * mom)
+    return out
+
+
 def uniform_state(s, B=(0.0, 0.0, 0.0), rho=1.0, p=1.0):
     act = s.mask() == 1
     shape = act.shape

@@ -35,6 +35,17 @@ def test_params_check_rejects_bad_sizes():
         cs.Solve(ntp=16, nr=4, nghost=4, rk_scheme=7)
 
 
+def test_p2_needs_the_resident_stencil_operators():
+    """CS_FLAG_P2 has no in-stage rebuild of its stencil inverses, so it is
+    refused together with CS_FLAG_NO_OP_CACHE and accepted alone."""
+    lib = cs.load_library()
+    bad = cs.make_params(ntp=16, nr=4, flags=cs.CS_FLAG_P2 | cs.CS_FLAG_NO_OP_CACHE)
+    assert "CS_FLAG_P2" in lib.cs_params_check(ctypes.byref(bad)).decode()
+    with pytest.raises(cs.CsError):
+        cs.Solve(bad)
+    assert lib.cs_params_check(ctypes.byref(cs.make_params(ntp=16, nr=4, flags=cs.CS_FLAG_P2))).decode() == ""
+
+
 def test_calls_out_of_order_return_state_errors():
     s = cs.Solve(ntp=8, nr=2, nghost=3)
     lib = s.lib

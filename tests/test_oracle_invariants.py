@@ -193,6 +193,76 @@ def test_linear_field_is_reproduced_by_steps_7ab_and_the_adp_solve():
         assert slope < 1e-12 and higher < 1e-12, (c, slope, higher)
 
 
+def _quadratic_errors(s, V, m=3):
+    """Max error of modes 2-10 of primitives 0-4 against quadratic_modes,
+    relative to the largest exact mode, in zones m layers clear of the
+    radial padding."""
+    from seeded_states import away_from_radial_padding, quadratic_modes
+
+    ex = quadratic_modes(s)
+    out = {}
+    for c in range(5):
+        err = max(np.abs(away_from_radial_padding(s, V[(t + 1) * 8 + c] - ex[c][t], m)).max() for t in range(9))
+        out[c] = err / max(np.abs(away_from_radial_padding(s, ex[c][t], m)).max() for t in range(9))
+    return out
+
+
+def test_p2_reproduces_quadratic_primitives():
+    """Known answer of LIMIT_ALL_SLOPES_P2 ("at third order, all stencils
+    are third order", 420:2469): each zone holding the exact zone average of
+    quadratic primitives, STEP 7.a's eight one-sided 9-zone stencils and the
+    central least squares all return the quadratic's modes, so the WENO
+    combination does too: slopes l grad q, square modes l^2 H_aa / 2, cross
+    modes l^2 H_ab, to round-off, across panel edges, in zones three layers
+    clear of the radial padding (P2's radial reach is two).  P12's linear
+    stencils do not (its MRWENO blend keeps a truncation-size part of them)."""
+    from seeded_states import quadratic_state
+
+    errs = {}
+    for flags in (cs.CS_FLAG_P2, 0):
+        pr = cs.preset("shell16")
+        pr["params"].update(flatten_coef=1e30, flags=flags)
+        s = cs.Solve(**pr["params"])
+        s.mesh_build(device=False)
+        o = Oracle(s)
+        o.put_state(quadratic_state(s))
+        o.fill_ghosts()
+        o.limit_all_slopes_p12()
+        assert np.abs(s.interior(o.debug("positivity"))).max() == 0
+        assert np.abs(s.interior(o.debug("flatten"))).max() == 0
+        errs[flags] = _quadratic_errors(s, o.debug("V"))
+    for c, e in errs[cs.CS_FLAG_P2].items():
+        assert e < 1e-12, (c, e)
+    assert min(errs[0].values()) > 1e-6, errs[0]
+
+
+def test_p2_interpolates_a_quadratic_electric_field_to_its_zone_averages():
+    """Known answer of P2's STEP 9.b (420:8553-12285): with the linear v and
+    linear divergence-free B of linear_state, the zone-centred E = -v x B
+    (STEP 9.a) is quadratic; the eight one-sided 10-zone interpolation
+    stencils and the central 19-zone least squares all recover it, so the
+    unflattened mode 1 is its zone average (centroid value plus the
+    second-moment terms) to round-off, in zones two clear of the panel edges
+    and five of the radial padding (the ghost zones' face-B constraints make
+    the ADP inexact one and two layers out, which P2's wider stencils reach
+    from the first interior rows)."""
+    from seeded_states import away_from_radial_padding, linear_state, linear_state_e_averages
+
+    pr = cs.preset("shell32")
+    pr["params"].update(flatten_coef=1e30, flags=cs.CS_FLAG_P2)
+    s = cs.Solve(**pr["params"])
+    s.mesh_build(device=False)
+    o = Oracle(s)
+    o.put_state(linear_state(s))
+    o.fill_ghosts()
+    o.limit_all_slopes_p12()
+    E1 = o.debug("E1")
+    core = lambda a: away_from_radial_padding(s, a, m=5)[..., 2:-2, 2:-2]
+    for q, ex in enumerate(linear_state_e_averages(s)):
+        err = np.abs(core(E1[q] - ex)).max() / np.abs(core(ex)).max()
+        assert err < 1e-12, (q, err)
+
+
 def test_uniform_static_gas_stays_uniform_to_the_mesh_closure():
     """A uniform gas at rest (no field, no gravity) changes in one step only
     through the discrete closure of each zone's faces (sum of area x
