@@ -542,6 +542,7 @@ def workload_config(args, zones: int, world: int) -> dict:
     return {"workload": args.workload, "desc": WORKLOAD_DOC.get(args.workload, ""), "flags": args.flags,
             "zones": zones, "parallelism": f"replicas x{world}",
             "precision": "f32 bulk / f64 B" if args.flags & cs.CS_FLAG_FP32 else "f64",
+            "reconstruction": "LIMIT_ALL_SLOPES_P2" if args.flags & cs.CS_FLAG_P2 else "LIMIT_ALL_SLOPES_P12",
             "l2": "inputs larger than L2 (state and work arrays >> 126 MB), no flush"}
 
 

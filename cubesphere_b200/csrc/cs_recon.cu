@@ -1774,28 +1774,31 @@ __global__ void k_ops_p2(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
 }
 
 // STEP 7.a (kE false) / STEP 9.b (kE true) of LIMIT_ALL_SLOPES_P2.  A block
-// takes 32 zones and one warp per variable (the 8 primitives / the 3 E
-// components), a thread one (zone, variable): the nine stencils' modes
-// (eight one-sided from the resident inverses, the central one from
+// takes 32 zones and all the variables (the 8 primitives / the 3 E
+// components), a thread one zone and CPT variables: the nine stencils'
+// modes (eight one-sided from the resident inverses, the central one from
 // P12's resident row weights: STEP 7.b's 18-zone least squares, STEP 9.c's
 // 19-zone one), their smoothness indicators over the zone's unit cube
 // (420:5245-5257) and WENO weights 1 and 100 over (IS + smallnum)^4 (in
 // FP64 in every form), then the weighted modes, summed stencil by stencil
 // in the reference's order (the one-sided stencils' modes formed again
-// rather than kept: 72 values a thread).  STEP 7.a writes modes 2..10 damped
-// by the flattener; STEP 9.b only the point value, flattened toward the
-// unlimited one (the edge solver consumes nothing else).  With kShared
-// the inverses are panel 1's, rotated per panel like the row weights, and
-// iteration T covers tile T / 6 of panel T % 6 so that the six blocks
-// reading one tile's inverses run together.
-template <bool kE, bool kShared, typename R>
-__global__ void __launch_bounds__(32 * (kE ? 3 : 8)) k_p2(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
+// rather than kept: 72 values a variable).  Each operator word is loaded
+// once for the CPT variables of the thread (the sums are the same for any
+// CPT).  STEP 7.a writes modes 2..10 damped by the flattener; STEP 9.b only
+// the point value, flattened toward the unlimited one (the edge solver
+// consumes nothing else).  With kShared the inverses are panel 1's, rotated
+// per panel like the row weights, and iteration T covers tile T / 6 of
+// panel T % 6 so that the six blocks reading one tile's inverses run
+// together.
+template <bool kE, bool kShared, int CPT, typename R>
+__global__ void __launch_bounds__(32 * (kE ? 3 : 8) / CPT) k_p2(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r) {
   constexpr int NM = kE ? 10 : 9, NR = kE ? 10 : 9, M0 = kE ? 0 : 1, NO = kE ? 1 : 9;
   constexpr int n18[18][2] = {{0, 0},  {1, 0},  {2, 0},  {3, 0},  {-1, 1}, {-1, -1}, {8, 0}, {9, 0},  {10, 0},
                               {11, 0}, {0, 1},  {1, 1},  {0, -1}, {1, -1}, {2, 1},   {3, 1}, {2, -1}, {3, -1}};
-  const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31, q0 = (threadIdx.x >> 5) * CPT;
   const long long nz = r.count(), npp = nz / 6, nw = kShared ? npp : nz;
   const long long ntile = kShared ? 6 * ((npp + 31) / 32) : (nz + 31) / 32;
+  const long long cstr = (long long)NPANEL * d.S;  // stride between variables
   for (long long T = blockIdx.x; T < ntile; T += gridDim.x) {
     long long t, tw;
     if (kShared) {
@@ -1827,41 +1830,58 @@ __global__ void __launch_bounds__(32 * (kE ? 3 : 8)) k_p2(Dims d, PhysC ph, DGeo
              ((double)X[3] * X[3]) * wis[3] + ((double)X[4] * X[4]) * wis[4] + ((double)X[5] * X[5]) * wis[5] +
              ((double)X[6] * X[6]) * wis[6] + ((double)X[7] * X[7]) * wis[7] + ((double)X[8] * X[8]) * wis[8];
     };
-    const R* f = (kE ? s.Esnap : s.V) + ((long long)q * NPANEL + p) * d.S;
-    const R f0 = f[d.idx(i, j, k)];
+    const R* fb = (kE ? s.Esnap : s.V) + ((long long)q0 * NPANEL + p) * d.S;
+    const long long o0 = d.idx(i, j, k);
+    R f0[CPT];
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) f0[c] = fb[c * cstr + o0];
     const unsigned long long qsrc = kShared ? s.p2_map[p].src : LSQ_IDENTITY_SRC;
     const unsigned int qneg = kShared ? s.p2_map[p].neg : 0u;
     const R* op = (kE ? s.op_p2e : s.op_p2v) + tw;
-    // modes of one-sided stencil st (rotated to this panel); only the first
-    // nm of them when the caller needs no more
-    auto stencil = [&](int st, int nm, R* X) {
-      R Rv[NR];
+    // modes of one-sided stencil st for the thread's variables (rotated to
+    // this panel); only the first nm of them when the caller needs no more
+    auto stencil = [&](int st, int nm, R (*X)[NM]) {
+      R Rv[CPT][NR];
 #pragma unroll
       for (int rr = 0; rr < NR; ++rr) {
         int zx = i, zy = j, zz = k;
         if (!kE || rr > 0) p2_zone(n, st, rr - (kE ? 1 : 0), i, j, k, zx, zy, zz);
-        const R v = f[d.idx(zx, zy, zz)];
-        Rv[rr] = kE ? v : v - f0;
+        const long long off = d.idx(zx, zy, zz);
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) {
+          const R v = fb[c * cstr + off];
+          Rv[c][rr] = kE ? v : v - f0[c];
+        }
       }
-      R Y[NM];
+      R Y[CPT][NM];
 #pragma unroll
       for (int m = 0; m < NM; ++m) {
-        R acc = R(0.0);
-        if (m < nm) {  // the constant mode (E's only one in pass 2) is never permuted
+        R w[NR];
 #pragma unroll
-          for (int rr = 0; rr < NR; ++rr) acc = acc + __ldg(op + (long long)((st * NM + m) * NR + rr) * nw) * Rv[rr];
+        for (int rr = 0; rr < NR; ++rr)
+          w[rr] = m < nm ? __ldg(op + (long long)((st * NM + m) * NR + rr) * nw) : R(0.0);
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) {
+          R acc = R(0.0);
+#pragma unroll
+          for (int rr = 0; rr < NR; ++rr) acc = acc + w[rr] * Rv[c][rr];
+          Y[c][m] = acc;
         }
-        Y[m] = acc;
       }
+      // the constant mode (E's only one in pass 2) is never permuted
 #pragma unroll
-      for (int m = 0; m < NM; ++m) X[m] = kShared ? lsq_rotated<M0>(Y, m + M0, qsrc, qneg) : Y[m];
+      for (int c = 0; c < CPT; ++c)
+#pragma unroll
+        for (int m = 0; m < NM; ++m) X[c][m] = kShared ? lsq_rotated<M0>(Y[c], m + M0, qsrc, qneg) : Y[c][m];
     };
-    double IS[9];
-    R X8[NM];
+    double IS[CPT][9];
+    R X8[CPT][NM];
     {  // central stencil from the resident row weights
-      R Y[NM];
+      R Y[CPT][NM];
 #pragma unroll
-      for (int m = 0; m < NM; ++m) Y[m] = R(0.0);
+      for (int c = 0; c < CPT; ++c)
+#pragma unroll
+        for (int m = 0; m < NM; ++m) Y[c][m] = R(0.0);
       const LsqPanelMap* cmap = kE ? s.lsq_map10 : s.lsq_map9;
       const long long tc = cmap ? t - (long long)p * npp : t, ncw = cmap ? npp : nz;
       const R* wc = (kE ? s.op_m10 : s.op_m9) + tc;
@@ -1870,51 +1890,76 @@ __global__ void __launch_bounds__(32 * (kE ? 3 : 8)) k_p2(Dims d, PhysC ph, DGeo
       for (int rr = 0; rr < NR + 9; ++rr) {
         const int ro = kE ? rr - 1 : rr;  // E: the zone itself first
         const int w = ro < 0 ? -1 : n18[ro][0], dz = ro < 0 ? 0 : n18[ro][1];
-        const R v = f[d.idx(w < 0 ? i : n.x[w], w < 0 ? j : n.y[w], k + dz)];
-        const R Rv = kE ? v : v - f0;
+        const long long off = d.idx(w < 0 ? i : n.x[w], w < 0 ? j : n.y[w], k + dz);
+        R Rv[CPT];
 #pragma unroll
-        for (int m = 0; m < NM; ++m) Y[m] = Y[m] + __ldg(wc + (long long)(rr * NM + m) * cstride) * Rv;
+        for (int c = 0; c < CPT; ++c) {
+          const R v = fb[c * cstr + off];
+          Rv[c] = kE ? v : v - f0[c];
+        }
+#pragma unroll
+        for (int m = 0; m < NM; ++m) {
+          const R wv = __ldg(wc + (long long)(rr * NM + m) * cstride);
+#pragma unroll
+          for (int c = 0; c < CPT; ++c) Y[c][m] = Y[c][m] + wv * Rv[c];
+        }
       }
       const unsigned long long csrc = cmap ? cmap[p].src : LSQ_IDENTITY_SRC;
       const unsigned int cneg = cmap ? cmap[p].neg : 0u;
 #pragma unroll
-      for (int m = 0; m < NM; ++m) X8[m] = cmap ? lsq_rotated<M0>(Y, m + M0, csrc, cneg) : Y[m];
-      IS[8] = smooth(X8 + (kE ? 1 : 0));
+      for (int c = 0; c < CPT; ++c) {
+#pragma unroll
+        for (int m = 0; m < NM; ++m) X8[c][m] = cmap ? lsq_rotated<M0>(Y[c], m + M0, csrc, cneg) : Y[c][m];
+        IS[c][8] = smooth(X8[c] + (kE ? 1 : 0));
+      }
     }
 #pragma unroll 1
     for (int st = 0; st < 8; ++st) {
-      R X[NM];
+      R X[CPT][NM];
       stencil(st, NM, X);
-      IS[st] = smooth(X + (kE ? 1 : 0));
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) IS[c][st] = smooth(X[c] + (kE ? 1 : 0));
     }
-    double W[9];
+    double W[CPT][9];
 #pragma unroll
-    for (int st = 0; st < 9; ++st) {
-      const double tt = IS[st] + ph.smallnum, t2 = tt * tt;
-      W[st] = (st < 8 ? 1.0 : 100.0) / (t2 * t2);
+    for (int c = 0; c < CPT; ++c) {
+#pragma unroll
+      for (int st = 0; st < 9; ++st) {
+        const double tt = IS[c][st] + ph.smallnum, t2 = tt * tt;
+        W[c][st] = (st < 8 ? 1.0 : 100.0) / (t2 * t2);
+      }
+      const double wn =
+          1.0 / (W[c][0] + W[c][1] + W[c][2] + W[c][3] + W[c][4] + W[c][5] + W[c][6] + W[c][7] + W[c][8]);
+#pragma unroll
+      for (int st = 0; st < 9; ++st) W[c][st] = W[c][st] * wn;
     }
-    const double wn = 1.0 / (W[0] + W[1] + W[2] + W[3] + W[4] + W[5] + W[6] + W[7] + W[8]);
+    double acc[CPT][NO];
 #pragma unroll
-    for (int st = 0; st < 9; ++st) W[st] = W[st] * wn;
-    double acc[NO];
+    for (int c = 0; c < CPT; ++c)
 #pragma unroll
-    for (int m = 0; m < NO; ++m) acc[m] = 0.0;
+      for (int m = 0; m < NO; ++m) acc[c][m] = 0.0;
 #pragma unroll 1
     for (int st = 0; st < 8; ++st) {
-      R X[NM];
+      R X[CPT][NM];
       stencil(st, NO, X);
-      const double ws = W[st];
 #pragma unroll
-      for (int m = 0; m < NO; ++m) acc[m] = st == 0 ? ws * (double)X[m] : acc[m] + ws * (double)X[m];
+      for (int c = 0; c < CPT; ++c) {
+        const double ws = W[c][st];
+#pragma unroll
+        for (int m = 0; m < NO; ++m) acc[c][m] = st == 0 ? ws * (double)X[c][m] : acc[c][m] + ws * (double)X[c][m];
+      }
     }
-#pragma unroll
-    for (int m = 0; m < NO; ++m) acc[m] = acc[m] + W[8] * (double)X8[m];
     const R fl = s.flatA[d.at(0, p, i, j, k)], x = R(1.0) - fl;
-    if (kE) {
-      s.E[d.at(q, p, i, j, k)] = fl * f0 + x * (R)acc[0];
-    } else {
 #pragma unroll
-      for (int m = 0; m < NO; ++m) Vat(s, d, q, 1 + m, p, i, j, k) = (R)acc[m] * x;
+    for (int c = 0; c < CPT; ++c) {
+#pragma unroll
+      for (int m = 0; m < NO; ++m) acc[c][m] = acc[c][m] + W[c][8] * (double)X8[c][m];
+      if (kE) {
+        s.E[d.at(q0 + c, p, i, j, k)] = fl * f0[c] + x * (R)acc[c][0];
+      } else {
+#pragma unroll
+        for (int m = 0; m < NO; ++m) Vat(s, d, q0 + c, 1 + m, p, i, j, k) = (R)acc[c][m] * x;
+      }
     }
   }
 }
@@ -2232,6 +2277,9 @@ void launch_flattener(Solve& sv) {
 }
 
 // Grid of k_p2 over range b: 32-zone tiles (panel-interleaved when shared).
+// Primitives a thread of STEP 7.a's k_p2 takes (each operator word loaded
+// once for all of them).
+constexpr int P2_CPT = 2;
 inline int p2_blocks(Solve& sv, const Range3& b, bool shared) {
   const long long npp = b.count() / 6;
   const long long nt = shared ? 6 * ((npp + 31) / 32) : (b.count() + 31) / 32;
@@ -2248,9 +2296,9 @@ void launch_weno_t(Solve& sv, DStateT<R>& st) {
     k_weno_ao_split<false, R, true><<<nb, W7A_ZT * 3, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
     mark(sv, "k_p2_entropy");
     if (st.p2_map)
-      k_p2<false, true, R><<<p2_blocks(sv, b, true), 256, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
+      k_p2<false, true, P2_CPT, R><<<p2_blocks(sv, b, true), 256 / P2_CPT, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
     else
-      k_p2<false, false, R><<<p2_blocks(sv, b, false), 256, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
+      k_p2<false, false, P2_CPT, R><<<p2_blocks(sv, b, false), 256 / P2_CPT, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
     mark(sv, "k_p2_prim");
     return;
   }
@@ -2422,9 +2470,9 @@ void launch_efield_t(Solve& sv, DStateT<R>& st) {
   mark(sv, "k_efield_a");
   if (sv.p.flags & CS_FLAG_P2) {  // LIMIT_ALL_SLOPES_P2's STEP 9.b
     if (st.p2_map)
-      k_p2<true, true, R><<<p2_blocks(sv, b, true), 96, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
+      k_p2<true, true, 1, R><<<p2_blocks(sv, b, true), 96, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
     else
-      k_p2<true, false, R><<<p2_blocks(sv, b, false), 96, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
+      k_p2<true, false, 1, R><<<p2_blocks(sv, b, false), 96, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
     mark(sv, "k_p2_efield");
     return;
   }
