@@ -446,7 +446,6 @@ PhysC make_phys(const cs_params& p) {
   ph.flatten_coef = p.flatten_coef;
   ph.prs_flatten_coef = p.prs_flatten_coef;
   ph.gm = p.gm;
-  ph.ogm1 = 1.0 / (p.gamma - 1.0);
   return ph;
 }
 

@@ -27,7 +27,6 @@ struct Dims {
 // Physical constants of one solve.
 struct PhysC {
   double gamma, rhofloor, prsfloor, smallnum, ob4pi, ob8pi, fourpi, cfl, flatten_coef, prs_flatten_coef, gm;
-  double ogm1;  // 1 / (gamma - 1): the pointwise physics multiplies by it instead of dividing
 };
 
 // Geometry resident on the device (read only during stages).
@@ -146,7 +145,7 @@ __device__ __forceinline__ int d_cons_to_prim(const PhysC& ph, R& ent, R* U, R* 
     flag = 1;
   }
   ent = V[4] / pow(V[0], R(ph.gamma) - R(1.0));
-  U[4] = V[4] * R(ph.ogm1) + R(0.5) * V[0] * v2 + R(ph.ob8pi) * b2;
+  U[4] = V[4] / (R(ph.gamma) - R(1.0)) + R(0.5) * V[0] * v2 + R(ph.ob8pi) * b2;
   return flag;
 }
 
@@ -161,19 +160,17 @@ __device__ __forceinline__ void d_prim_to_cons(const PhysC& ph, R ent, R* U, R* 
   U[5] = V[5];
   U[6] = V[6];
   U[7] = V[7];
-  U[4] = V[4] * R(ph.ogm1) + R(0.5) * V[0] * (V[1] * V[1] + V[2] * V[2] + V[3] * V[3]) +
+  U[4] = V[4] / (R(ph.gamma) - R(1.0)) + R(0.5) * V[0] * (V[1] * V[1] + V[2] * V[2] + V[3] * V[3]) +
          R(ph.ob8pi) * (V[5] * V[5] + V[6] * V[6] + V[7] * V[7]);
 }
 
 // Fast magnetosonic extremal speeds along the local x axis.
 template <typename R>
 __device__ __forceinline__ void d_wavespeeds(const PhysC& ph, const R* V, R& smin, R& smax) {
-  // one reciprocal of rho and of 4 pi rho instead of three divisions
-  const R orho = R(1.0) / V[0], o4pirho = R(ph.ob4pi) * orho;
-  const R cs2 = R(ph.gamma) * V[4] * orho;
-  const R b2r = (V[5] * V[5] + V[6] * V[6] + V[7] * V[7]) * o4pirho;
+  const R cs2 = R(ph.gamma) * V[4] / V[0];
+  const R b2r = (V[5] * V[5] + V[6] * V[6] + V[7] * V[7]) / (R(ph.fourpi) * V[0]);
   const R bb = -(cs2 + b2r);
-  const R cc = cs2 * V[5] * V[5] * o4pirho;
+  const R cc = cs2 * V[5] * V[5] / (R(ph.fourpi) * V[0]);
   const R mf = sqrt((-bb + sqrt(bb * bb - R(4.0) * cc)) / R(2.0));
   smin = V[1] - mf;
   smax = V[1] + mf;
@@ -181,7 +178,7 @@ __device__ __forceinline__ void d_wavespeeds(const PhysC& ph, const R* V, R& smi
 
 template <typename R>
 __device__ __forceinline__ void d_flux_x(const PhysC& ph, const R* V, R* F) {
-  const R u4 = V[4] * R(ph.ogm1) + R(0.5) * V[0] * (V[1] * V[1] + V[2] * V[2] + V[3] * V[3]) +
+  const R u4 = V[4] / (R(ph.gamma) - R(1.0)) + R(0.5) * V[0] * (V[1] * V[1] + V[2] * V[2] + V[3] * V[3]) +
                     R(ph.ob8pi) * (V[5] * V[5] + V[6] * V[6] + V[7] * V[7]);
   const R b2 = V[5] * V[5] + V[6] * V[6] + V[7] * V[7];
   const R vdb = V[1] * V[5] + V[2] * V[6] + V[3] * V[7];
@@ -235,7 +232,7 @@ __device__ __forceinline__ void d_hll(const PhysC& ph, R* VL, R* VR, R entL, R e
   // The entropy pressure (a pow) is formed only where the floor needs it.
   if (peng <= R(ph.prsfloor)) {
     const R pent = entU * pow(Us[0], R(ph.gamma) - R(1.0));
-    Us[4] = Us[4] + (pent - peng) * R(ph.ogm1);
+    Us[4] = Us[4] + (pent - peng) / (R(ph.gamma) - R(1.0));
   }
   if (SL >= R(0.0)) {
 #pragma unroll

@@ -95,7 +95,6 @@ extern "C" int cs_cfl_timestep_noalloc(const double* U, const double* ent, const
   ph.ob8pi = 1.0 / (8.0 * pi);
   ph.fourpi = 4.0 * pi;
   ph.cfl = cfl_coef;
-  ph.ogm1 = 1.0 / (gamma - 1.0);
   cudaStream_t st = (cudaStream_t)stream;
   const int nparts = 6 * nr;
   cs::k_cfl_layers<<<nparts, 256, 0, st>>>(d, ph, U, ent, v_scale, mask, scratch);

@@ -2279,7 +2279,7 @@ void launch_flattener(Solve& sv) {
 // Grid of k_p2 over range b: 32-zone tiles (panel-interleaved when shared).
 // Primitives a thread of STEP 7.a's k_p2 takes (each operator word loaded
 // once for all of them).
-constexpr int P2_CPT = 2;
+constexpr int P2_CPT = 4;
 inline int p2_blocks(Solve& sv, const Range3& b, bool shared) {
   const long long npp = b.count() / 6;
   const long long nt = shared ? 6 * ((npp + 31) / 32) : (b.count() + 31) / 32;
