@@ -12,7 +12,6 @@
 #include <string>
 #include <vector>
 
-#include <cudaTypedefs.h>
 
 #include "cs_solve.h"
 
@@ -719,30 +718,6 @@ bool lsq_panel_maps(const GeomHost& h, LsqPanelMap* q) {
   return true;
 }
 
-// Tensor (TMA) map of STEP 7.b's row weights: a 2-D array of 162 rows of n
-// zones (row stride m9_stride(n) elements), read in boxes of 32 zones x 162
-// rows; zones past n read as zero.  cuTensorMapEncodeTiled is a driver entry
-// point, fetched through the runtime.
-bool row_weight_map(CUtensorMap& map, void* base, size_t elem, long long n) {
-  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
-  if (!encode) {
-    void* fn = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
-        q != cudaDriverEntryPointSuccess || !fn)
-      return false;
-    encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
-  }
-  const cuuint64_t dims[2] = {(cuuint64_t)n, 162};
-  const cuuint64_t strides[1] = {(cuuint64_t)m9_stride(n) * elem};
-  const cuuint32_t box[2] = {32, 162};
-  const cuuint32_t estr[2] = {1, 1};
-  const CUresult r = encode(&map, elem == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base,
-                            dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  return r == CUDA_SUCCESS;
-}
-
 // Resident geometry-only operators of a new mesh, where the device has room
 // for them after the first solve's state, computed by that solve's stream.
 template <typename R>
@@ -774,8 +749,6 @@ int mesh_operators(Solve& sv, MeshRes& m, DStateT<R>& s) {
       m.op_m9 = mdalloc(sv, m, (size_t)m9_stride(n9) * 162 * sizeof(R), e);
       m.op_m10 = m.op_m9 ? mdalloc(sv, m, (size_t)n10 * 190 * sizeof(R), e) : nullptr;
       if (!m.op_m9 || !m.op_m10) return cuda_fail(sv, e, "cudaMalloc(least-squares operators)");
-      if (!row_weight_map(m.m9_map, m.op_m9, sizeof(R), n9))
-        return fail(sv, CS_ERR_CUDA, "cuTensorMapEncodeTiled(STEP 7.b row weights)");
       if (shared) {
         m.lsq_map = mdalloc(sv, m, sizeof qmap, e);
         if (!m.lsq_map) return cuda_fail(sv, e, "cudaMalloc(least-squares panel maps)");

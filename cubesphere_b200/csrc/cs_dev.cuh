@@ -3,7 +3,6 @@
 // i fastest) so that a warp along i reads 32 consecutive doubles per field.
 #pragma once
 
-#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -432,7 +431,7 @@ __device__ __forceinline__ void d_matinv(const R* A, R* Ainv) {
 
 // Row stride of STEP 7.b's resident row weights [162][stride]: the zone
 // count rounded up to 4 elements, so each row starts on a 16-byte (FP32) or
-// 32-byte (FP64) boundary, as a tensor (TMA) map of the array requires.
+// 32-byte (FP64) boundary.
 __host__ __device__ constexpr long long m9_stride(long long n) { return (n + 3) / 4 * 4; }
 
 // Host-side launch helpers implemented in the .cu files.

@@ -260,16 +260,6 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
                "l"(src), "r"(bytes), "r"(smem_u32(bar))
                : "memory");
 }
-// Tensor (TMA) load of a 2-D box at element coordinates (x, y) of the map
-// into shared memory, completing on the mbarrier.  x times the element size
-// must be a multiple of 16 bytes (the callers pass multiples of 32 zones).
-__device__ __forceinline__ void tma_g2s_2d(void* dst, const void* map, int x, int y, uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
-          smem_u32(dst)),
-      "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
-      : "memory");
-}
 // Bounded wait on an mbarrier phase: after 2^23 polls (seconds, far beyond
 // any copy) it records an error in *err and returns, so no wait can hang.
 __device__ __noinline__ void mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
@@ -615,115 +605,6 @@ __global__ void __launch_bounds__(TPB) k_weno7b(Dims d, PhysC ph, DGeom g, DStat
         for (int m = 4; m < 10; ++m) Vat(s, d, q, m, p, i, j, k) = (Whi * Phi[m - 1]) * x;
       }
     }
-  }
-}
-
-// STEP 7.b with the resident row weights, four threads per zone: a block
-// takes 32 zones and warp c the primitives 2c and 2c + 1, so each thread
-// keeps 2 x 9 least-squares sums instead of 8 x 9.  The 162 row weights of
-// the block's 32 zones are one 32 x 162 tile of the weight array (zone
-// fastest, rows m9_stride apart): a tensor (TMA) load stages it into shared
-// memory, completing on an mbarrier whose wait is bounded (a timeout sets
-// err_flag), and the four warps read it there.  The order of the zones
-// (LsqOrder's with 32 zones a tile) and every sum are those of k_weno7b.
-constexpr int W7B_ZT = 32;
-template <bool kShared, typename R>
-__global__ void __launch_bounds__(W7B_ZT * 4, sizeof(R) == 4 ? 8 : 5) k_weno7b_split(
-    Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 r, const __grid_constant__ CUtensorMap wmap) {
-  __shared__ alignas(128) R wsm[162][W7B_ZT];
-  __shared__ uint64_t bar;
-  const R ob12 = R(1.0) / R(12.0), ob180 = R(1.0) / R(180.0), ob144 = R(1.0) / R(144.0);
-  const int zl = threadIdx.x % W7B_ZT, q0 = 2 * (threadIdx.x / W7B_ZT);
-  const long long nr = r.count(), npp = nr / 6;
-  const long long ntile = kShared ? 6 * ((npp + W7B_ZT - 1) / W7B_ZT) : (nr + W7B_ZT - 1) / W7B_ZT;
-  if (threadIdx.x == 0) {
-    mbar_init(&bar, 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  __syncthreads();
-  uint32_t parity = 0;
-  for (long long T = blockIdx.x; T < ntile; T += gridDim.x) {
-    const long long tw0 = kShared ? (T / 6) * W7B_ZT : T * W7B_ZT;
-    if (threadIdx.x == 0) {
-      mbar_expect_tx(&bar, (uint32_t)sizeof(wsm));
-      tma_g2s_2d(&wsm[0][0], &wmap, (int)tw0, 0, &bar);
-    }
-    long long t, tw = tw0 + zl;
-    bool act;
-    if (kShared) {
-      t = (T % 6) * npp + tw;
-      act = tw < npp;
-    } else {
-      t = tw;
-      act = t < nr;
-    }
-    int p = 0, i = 0, j = 0, k = 0;
-    if (act) {
-      r.decode(t, p, i, j, k);
-      act = mask_at(g, d, p, i, j) == 1;
-    }
-    mbar_wait(&bar, parity, s.err_flag);
-    parity ^= 1u;
-    if (act) {
-      const Nbr12 n = load_nbr(g, d, p, i, j);
-      const R f = s.flatA[d.at(0, p, i, j, k)];
-      const R betalo = f + (R(1.0) - f) * R(2.0);
-      const R ghi = f * R(0.6) + (R(1.0) - f) * R(0.95), glo = R(1.0) - ghi, obghi = R(1.0) / ghi, grat = glo / ghi;
-      R v0[2];
-#pragma unroll
-      for (int qq = 0; qq < 2; ++qq) v0[qq] = s.V[((long long)(q0 + qq) * NPANEL + p) * d.S + d.idx(i, j, k)];
-      R Y[2][9];
-#pragma unroll
-      for (int qq = 0; qq < 2; ++qq)
-#pragma unroll
-        for (int a = 0; a < 9; ++a) Y[qq][a] = R(0.0);
-#pragma unroll 2
-      for (int rr = 0; rr < 18; ++rr) {
-        const int w = c_n18[rr][0];
-        const long long off = d.idx(w < 0 ? i : n.x[w], w < 0 ? j : n.y[w], k + c_n18[rr][1]);
-#pragma unroll
-        for (int qq = 0; qq < 2; ++qq) {
-          const R Rv = s.V[((long long)(q0 + qq) * NPANEL + p) * d.S + off] - v0[qq];
-#pragma unroll
-          for (int a = 0; a < 9; ++a) Y[qq][a] = Y[qq][a] + wsm[rr * 9 + a][zl] * Rv;
-        }
-      }
-      const unsigned long long qsrc = kShared ? s.lsq_map9[p].src : LSQ_IDENTITY_SRC;
-      const unsigned int qneg = kShared ? s.lsq_map9[p].neg : 0u;
-      R c0[10];
-      coef10(g, d, p, i, j, k, c0);
-#pragma unroll
-      for (int qq = 0; qq < 2; ++qq) {
-        const int q = q0 + qq;
-        R X[9];
-#pragma unroll
-        for (int a = 0; a < 9; ++a) X[a] = kShared ? lsq_rotated<1>(Y[qq], a + 1, qsrc, qneg) : Y[qq][a];
-        const R v2 = Vat(s, d, q, 1, p, i, j, k), v3 = Vat(s, d, q, 2, p, i, j, k), v4 = Vat(s, d, q, 3, p, i, j, k);
-        const R ISlo = betalo * (v2 * v2 + v3 * v3 + v4 * v4) * ob12;
-        R Phi[9];
-        Phi[0] = X[0] * obghi - v2 * grat;
-        Phi[1] = X[1] * obghi - v3 * grat;
-        Phi[2] = X[2] * obghi - v4 * grat;
-#pragma unroll
-        for (int a = 3; a < 9; ++a) Phi[a] = X[a] * obghi;
-        const R IShi = (Phi[0] * Phi[0] + Phi[1] * Phi[1] + Phi[2] * Phi[2]) * ob12 +
-                       (Phi[3] * Phi[3]) * (sqr(c0[4] - ob12) + ob180) + (Phi[4] * Phi[4]) * (sqr(c0[5] - ob12) + ob180) +
-                       (Phi[5] * Phi[5]) * (sqr(c0[6] - ob12) + ob180) + (Phi[6] * Phi[6]) * (c0[7] * c0[7] + ob144) +
-                       (Phi[7] * Phi[7]) * (c0[8] * c0[8] + ob144) + (Phi[8] * Phi[8]) * (c0[9] * c0[9] + ob144);
-        const R tau = fabs(IShi - ISlo);
-        R Wlo = glo * (R(1.0) + tau / (ISlo + R(ph.smallnum))), Whi = ghi * (R(1.0) + tau / (IShi + R(ph.smallnum)));
-        const R aa = R(1.0) / (Wlo + Whi);
-        Wlo = Wlo * aa;
-        Whi = Whi * aa;
-        const R x = R(1.0) - f;
-        Vat(s, d, q, 1, p, i, j, k) = (Whi * Phi[0] + Wlo * v2) * x;
-        Vat(s, d, q, 2, p, i, j, k) = (Whi * Phi[1] + Wlo * v3) * x;
-        Vat(s, d, q, 3, p, i, j, k) = (Whi * Phi[2] + Wlo * v4) * x;
-#pragma unroll
-        for (int m = 4; m < 10; ++m) Vat(s, d, q, m, p, i, j, k) = (Whi * Phi[m - 1]) * x;
-      }
-    }
-    __syncthreads();  // every warp is done with wsm before the next tile's load
   }
 }
 
@@ -2308,15 +2189,11 @@ void launch_weno_t(Solve& sv, DStateT<R>& st) {
     k_weno_ao_split<false, R><<<nb, W7A_ZT * 3, 0, sv.stream>>>(d, sv.ph, sv.g, st, a);
     mark(sv, "k_weno7a");
   }
-  if (st.op_m9) {
-    const long long nt = (b.count() + W7B_ZT - 1) / W7B_ZT + 6;
-    const int nb = (int)std::min<long long>(nt, (long long)grid_sms(sv) * 16);
-    const CUtensorMap& wm = sv.mesh->m9_map;
-    if (st.lsq_map9)
-      k_weno7b_split<true, R><<<nb, W7B_ZT * 4, 0, sv.stream>>>(d, sv.ph, sv.g, st, b, wm);
-    else
-      k_weno7b_split<false, R><<<nb, W7B_ZT * 4, 0, sv.stream>>>(d, sv.ph, sv.g, st, b, wm);
-  } else
+  if (st.op_m9 && st.lsq_map9)
+    k_weno7b<true, true, R><<<blocks_for(b.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
+  else if (st.op_m9)
+    k_weno7b<true, false, R><<<blocks_for(b.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
+  else
     k_weno7b<false, false, R><<<blocks_for(b.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
   mark(sv, "k_weno7b");
 }

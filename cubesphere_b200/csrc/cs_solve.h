@@ -65,7 +65,6 @@ struct MeshRes {
   void* op_p2v = nullptr;  // CS_FLAG_P2 one-sided stencil inverses (state's type)
   void* op_p2e = nullptr;
   bool p2_shared = false;  // op_p2v / op_p2e are panel 1's only
-  CUtensorMap m9_map{};  // tensor map of op_m9 as [162 rows][m9_stride zones], 32 x 162 boxes
   void* adp_lu = nullptr;   // FP64 per panel; panel-shared ones in the state's type
   int8_t* adp_piv = nullptr;
   int8_t* adp_pmap = nullptr;  // ADP factors shared by the panels: per panel [unknown map][sign]
