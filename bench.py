@@ -56,13 +56,12 @@ ALGO_WORDS_PER_UNIT = {
     "k_adp_rhs": 30 + 30 + 162 + 14 + 36,
     # the same with panel 1's geometry serving the six panels (1/6 per zone)
     "k_adp_rhs6": 30 + 30 + (162 + 14) / 6 + 36,
-    # 80 modes + 4 entropy modes + 10 moments + scale/centroid in, 30 face
-    # points x 3 coordinates of geometry, 270 face-state values out
-    "k_face_states": 80 + 4 + 14 + 90 + 270,
-    # per face (one launch per direction, units = zones): two face states
-    # (2 x 45), geometry (15 points + 5 weights + normals/centroid 6 + area
-    # + 2 volumes + scale), 16 contributions + 3 speeds/entropy flux out
-    "k_flux": 90 + 30 + 19,
+    # one launch per stage, the three face directions (units = zones): the
+    # zone's 80 modes, 4 entropy modes, 10 moments, centroid and scale in;
+    # per direction the face geometry (15 points, 5 weights, normals /
+    # centroid 6, area, 2 volumes) in and 16 contributions, 2 speeds and the
+    # entropy flux out
+    "k_flux": 80 + 4 + 10 + 4 + 3 * (15 + 5 + 6 + 1 + 2) + 3 * (16 + 3),
     # E snapshot (3) and modes 1-3 (9) in, E mode 0 out (3), flattener,
     # moments, the resident row weights (19 x 10, panel 1's serving the six
     # panels: 1/6 per zone)
@@ -71,28 +70,33 @@ ALGO_WORDS_PER_UNIT = {
     "k_faceB": 80 + 1 + 20 + 5,
 }
 
-# DRAM bytes per unit (read + write) measured by ncu on the shell32 case
-# (units: 190,608 zones of the ADP range, 155,520 of the face-state / flux /
-# least-squares ranges); the full shell128 launches are too large to
-# capture, so roofline.traffic scales these by the units of a full launch.
+# DRAM bytes per unit and launch (read + write) measured by ncu on the
+# shell32 case (units: 190,608 zones of the ADP range, 155,520 of the flux /
+# least-squares ranges; 14 launches each), FP64 and precision form; the full
+# shell128 launches are too large to capture, so roofline.traffic scales
+# these by the units of a full launch.
 MEASURED_TRAFFIC_PER_UNIT = {
-    "k_adp_solve6": (397.223e6 + 36.802e6) / 190608,
-    "k_flux": (150.846e6 + 18.736e6 + 155.063e6 + 19.871e6 + 168.527e6 + 18.285e6) / 3 / 155520,
-    "k_weno7b": (269.9e6 + 124.4e6) / 155520,
-    "k_face_states": (254.736e6 + 308.688e6) / 155520,
-    "k_efield_c": (68.69e6 + 7.622e6) / 155520,
+    "k_adp_solve6": 2274.8,
+    "k_flux": 2085.8,
+    "k_weno7b": 2188.9,
+    "k_efield_c": 486.5,
 }
-# FP64 operations per unit (2 x DFMA + DADD + DMUL thread instructions),
-# from the same ncu captures.  The path is FP64-bound, so the roofline also
-# reports these against the FP64 FMA rate measured on the device in the
-# same run (cs_fp64_fma_rate); the nominal rate, 148 SMs x 64 FP64 FMA per
-# clock x 2 x 1.965 GHz = 37.2 TFLOP/s, is kept for context.
+MEASURED_TRAFFIC_PER_UNIT_FP32 = {
+    "k_adp_solve6": 1117.1,
+    "k_flux": 1489.4,
+    "k_weno7b": 420.0,
+    "k_efield_c": 262.9,
+}
+# FP64 operations per unit and launch (2 x DFMA + DADD + DMUL thread
+# instructions), from the same FP64 capture.  The path is FP64-bound, so the
+# roofline also reports these against the FP64 FMA rate measured on the
+# device in the same run (cs_fp64_fma_rate); the nominal rate, 148 SMs x 64
+# FP64 FMA per clock x 2 x 1.965 GHz = 37.2 TFLOP/s, is kept for context.
 FP64_FLOP_PER_UNIT = {
-    "k_adp_solve6": 6.012e8 / 190608,
-    "k_flux": (5.448e8 + 5.448e8 + 6.120e8) / 3 / 155520,
-    "k_weno7b": 5.79e8 / 155520,
-    "k_face_states": 1.163e9 / 155520,
-    "k_efield_c": 2.367e8 / 155520,
+    "k_adp_solve6": 3154.2,
+    "k_flux": 16485.3,
+    "k_weno7b": 3727.7,
+    "k_efield_c": 1529.2,
 }
 FP64_NOMINAL_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12
 
@@ -484,7 +488,8 @@ def precision_long_sample(name: str = "shell32", nsteps: int = 200, timed: bool 
     `nsteps` steps.  The FP64 run drops the resident operators
     (CS_FLAG_NO_ADP_CACHE | CS_FLAG_NO_OP_CACHE: the same results to
     round-off) when the device cannot hold them, as on the 6 x 256^2 x 128
-    shell.  With `timed`, each run's device time per step (CUDA events
+    shell, where the precision form drops the least-squares row weights
+    (CS_FLAG_NO_OP_CACHE) to keep its ADP factors.  With `timed`, each run's device time per step (CUDA events
     around the step loop, one host read of the time step per step)."""
     import torch
 
@@ -506,10 +511,14 @@ def precision_long_sample(name: str = "shell32", nsteps: int = 200, timed: bool 
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s.synchronize()
         e0.record(stream)
+        t0 = time.time()
         for n in range(nsteps):
             d = dts_in[n] if dts_in is not None else dt
             dts.append(d)
             dt = s.step(d)
+            if nsteps >= 50 and (n + 1) % 25 == 0:
+                print(f"precision run flags={flags}: step {n + 1}/{nsteps}, {time.time() - t0:.0f} s", file=sys.stderr,
+                      flush=True)
         e1.record(stream)
         e1.synchronize()
         ms = e0.elapsed_time(e1) / nsteps
@@ -520,14 +529,19 @@ def precision_long_sample(name: str = "shell32", nsteps: int = 200, timed: bool 
 
     ref, dts, _, ms64 = run(f64_flags, None)
     torch.cuda.synchronize()
-    got, _, divb, ms32 = run(cs.CS_FLAG_FP32, dts)
+    # the precision form keeps its ADP factors (the costly rebuild) and drops
+    # the cheaper least-squares row weights when the device cannot hold both
+    f32_flags = cs.CS_FLAG_FP32
+    if cs.estimate_device_bytes(**dict(pr["params"], flags=f32_flags)) > 0.9 * torch.cuda.mem_get_info()[0]:
+        f32_flags |= cs.CS_FLAG_NO_OP_CACHE
+    got, _, divb, ms32 = run(f32_flags, dts)
     shape = cs.Solve(**pr["params"])
     err, err_inf, divb_rel = state_errors(shape, got, ref, divb)
     shape.close()
     p = pr["params"]
     out = {"workload": name, "zones": 6 * p["ntp"] ** 2 * p["nr"], "steps_compared": nsteps,
            "l1_rel_err_vs_f64": err, "linf_rel_err_vs_f64": err_inf, "max_divb_over_bmax": divb_rel,
-           "f64_flags": f64_flags}
+           "f64_flags": f64_flags, "f32_flags": f32_flags}
     if timed:
         zones = out["zones"]
         out.update({"f64_ms_per_step": ms64, "f32_ms_per_step": ms32,
@@ -692,12 +706,12 @@ def run_gpu(args):
     units = 6 * (N + 2 * G - 2) ** 2 * (nr + 2 * G - 2)  # zones of the shrink-1 range (7.a / 8.d / 9.b)
     if dname in ("k_weno7b", "k_efield_c"):
         units = 6 * (N + 2 * G - 4) ** 2 * (nr + 2 * G - 4)
-    if dname in ("k_flux", "k_face_states"):
+    if dname == "k_flux":
         units = 6 * (N + 4) ** 2 * (nr + 4)
     launch_s = dms / dcount / 1e3
     per_launch = stage_b * units
     achieved = per_launch / launch_s / 1e9
-    tr = MEASURED_TRAFFIC_PER_UNIT.get(dname)
+    tr = (MEASURED_TRAFFIC_PER_UNIT_FP32 if fp32 else MEASURED_TRAFFIC_PER_UNIT).get(dname)
     traffic = tr * units if tr else None
     words = ALGO_WORDS_PER_UNIT.get(dname)
     per_value = value / world  # one GPU's zone-updates/s

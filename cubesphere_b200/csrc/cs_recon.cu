@@ -2347,9 +2347,9 @@ void launch_efield_t(Solve& sv, DStateT<R>& st) {
   mark(sv, "k_efield_a");
   if (sv.p.flags & CS_FLAG_P2) {  // LIMIT_ALL_SLOPES_P2's STEP 9.b
     if (st.p2_map)
-      k_p2<true, true, 1, R><<<p2_blocks(sv, b, true), 96, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
+      k_p2<true, true, 3, R><<<p2_blocks(sv, b, true), 32, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
     else
-      k_p2<true, false, 1, R><<<p2_blocks(sv, b, false), 96, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
+      k_p2<true, false, 3, R><<<p2_blocks(sv, b, false), 32, 0, sv.stream>>>(d, sv.ph, sv.g, st, b);
     mark(sv, "k_p2_efield");
     return;
   }
