@@ -523,7 +523,17 @@ __global__ void __launch_bounds__(TPB) k_weno7b(Dims d, PhysC ph, DGeom g, DStat
     // no neighbour geometry; without the cache the rows are rebuilt and the
     // inverse applied to their sums.
     R Minv[kCached ? 1 : 81];
-    if (!kCached) w7b_minv(d, ph, g, p, i, j, k, n, cx, cy, cz, l0, obl0, c0, Minv);
+    if (!kCached) {
+      // formed in FP64 in every form, like the cached row weights; the
+      // precision form rounds the inverse once
+      double c0d[10], Md[81];
+      coef10(g, d, p, i, j, k, c0d);
+      const double l0d = fmax(geo(g, d, CS_G_V_SCALE, 0, p, i, j, k), ph.smallnum);
+      w7b_minv<double>(d, ph, g, p, i, j, k, n, geo(g, d, CS_G_V_CEN, 0, p, i, j, k), geo(g, d, CS_G_V_CEN, 1, p, i, j, k),
+                       geo(g, d, CS_G_V_CEN, 2, p, i, j, k), l0d, 1.0 / l0d, c0d, Md);
+#pragma unroll
+      for (int e = 0; e < 81; ++e) Minv[e] = (R)Md[e];
+    }
     // kShared: panel 1's row weights; the sums are rotated at the end
     const R* wc = s.op_m9 + tw;
     auto MI = [&](int e) { return Minv[kCached ? 0 : e]; };
@@ -1451,7 +1461,16 @@ __global__ void __launch_bounds__(TPB, sizeof(R) == 4 ? 6 : 4) k_efield_c(Dims d
     // kCached: the solution operator comes from the cache as the row weights
     // W_rr = Minv A_rr^T (geometry only), so X = sum_rr W_rr E_rr directly.
     R Minv[kCached ? 1 : 100];
-    if (!kCached) e9c_minv(d, g, p, i, j, k, n, cx, cy, cz, obl0, c0, Minv);
+    if (!kCached) {
+      // formed in FP64 in every form, like the cached row weights
+      double c0d[10], Md[100];
+      coef10(g, d, p, i, j, k, c0d);
+      e9c_minv<double>(d, g, p, i, j, k, n, geo(g, d, CS_G_V_CEN, 0, p, i, j, k), geo(g, d, CS_G_V_CEN, 1, p, i, j, k),
+                       geo(g, d, CS_G_V_CEN, 2, p, i, j, k), 1.0 / fmax(geo(g, d, CS_G_V_SCALE, 0, p, i, j, k), ph.smallnum),
+                       c0d, Md);
+#pragma unroll
+      for (int e = 0; e < 100; ++e) Minv[e] = (R)Md[e];
+    }
     const R* wc = s.op_m10 + tw;
     auto MI = [&](int e) { return Minv[kCached ? 0 : e]; };
     R Y[3][10];
@@ -1719,9 +1738,13 @@ __global__ void __launch_bounds__(32 * (kE ? 3 : 8) / CPT) k_p2(Dims d, PhysC ph
     const unsigned long long qsrc = kShared ? s.p2_map[p].src : LSQ_IDENTITY_SRC;
     const unsigned int qneg = kShared ? s.p2_map[p].neg : 0u;
     const R* op = (kE ? s.op_p2e : s.op_p2v) + tw;
-    // modes of one-sided stencil st for the thread's variables (rotated to
-    // this panel); only the first nm of them when the caller needs no more
-    auto stencil = [&](int st, int nm, R (*X)[NM]) {
+    // The modes of one-sided stencil st for the thread's variables, group
+    // by group -- the groups the panel rotations permute within (for E the
+    // constant first, then x y z, the squares, the cross terms) -- rotated
+    // to this panel and handed to visit(group, X[variable][0..2]); groups
+    // g0 .. g1 - 1 only.  Three modes a variable are live at a time.
+    constexpr int NG = kE ? 4 : 3;
+    auto stencil = [&](int st, int g0, int g1, auto&& visit) {
       R Rv[CPT][NR];
 #pragma unroll
       for (int rr = 0; rr < NR; ++rr) {
@@ -1734,26 +1757,43 @@ __global__ void __launch_bounds__(32 * (kE ? 3 : 8) / CPT) k_p2(Dims d, PhysC ph
           Rv[c][rr] = kE ? v : v - f0[c];
         }
       }
-      R Y[CPT][NM];
 #pragma unroll
-      for (int m = 0; m < NM; ++m) {
-        R w[NR];
+      for (int gi = 0; gi < NG; ++gi) {
+        if (gi < g0 || gi >= g1) continue;
+        const int mb = kE ? (gi == 0 ? 0 : 3 * gi - 2) : 3 * gi + 1;  // first mode of the group
+        const int gs = (kE && gi == 0) ? 1 : 3;
+        R Y[CPT][3];
 #pragma unroll
-        for (int rr = 0; rr < NR; ++rr)
-          w[rr] = m < nm ? __ldg(op + (long long)((st * NM + m) * NR + rr) * nw) : R(0.0);
+        for (int q = 0; q < 3; ++q) {
+          if (q < gs) {
+            R w[NR];
 #pragma unroll
-        for (int c = 0; c < CPT; ++c) {
-          R acc = R(0.0);
+            for (int rr = 0; rr < NR; ++rr) w[rr] = __ldg(op + (long long)((st * NM + mb - M0 + q) * NR + rr) * nw);
 #pragma unroll
-          for (int rr = 0; rr < NR; ++rr) acc = acc + w[rr] * Rv[c][rr];
-          Y[c][m] = acc;
+            for (int c = 0; c < CPT; ++c) {
+              R acc = R(0.0);
+#pragma unroll
+              for (int rr = 0; rr < NR; ++rr) acc = acc + w[rr] * Rv[c][rr];
+              Y[c][q] = acc;
+            }
+          }
         }
+        R X[CPT][3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          if (q < gs) {
+            const int mm = mb + q;
+            const int mu = kShared ? (int)((qsrc >> (4 * mm)) & 15) - mb : q;
+            const bool ng = kShared && ((qneg >> mm) & 1u);
+#pragma unroll
+            for (int c = 0; c < CPT; ++c) {
+              const R v = mu == 0 ? Y[c][0] : (mu == 1 ? Y[c][1] : Y[c][2]);
+              X[c][q] = ng ? -v : v;
+            }
+          }
+        }
+        visit(gi, X);
       }
-      // the constant mode (E's only one in pass 2) is never permuted
-#pragma unroll
-      for (int c = 0; c < CPT; ++c)
-#pragma unroll
-        for (int m = 0; m < NM; ++m) X[c][m] = kShared ? lsq_rotated<M0>(Y[c], m + M0, qsrc, qneg) : Y[c][m];
     };
     double IS[CPT][9];
     R X8[CPT][NM];
@@ -1796,10 +1836,21 @@ __global__ void __launch_bounds__(32 * (kE ? 3 : 8) / CPT) k_p2(Dims d, PhysC ph
     }
 #pragma unroll 1
     for (int st = 0; st < 8; ++st) {
-      R X[CPT][NM];
-      stencil(st, NM, X);
+      double sm[CPT];
+      stencil(st, 0, NG, [&](int gi, R (*X)[3]) {
+        const int gg = kE ? gi - 1 : gi;  // 0: x y z, 1: the squares, 2: the cross terms
+        if (gg < 0) return;               // E's constant has no indicator term
 #pragma unroll
-      for (int c = 0; c < CPT; ++c) IS[c][st] = smooth(X[c] + (kE ? 1 : 0));
+        for (int c = 0; c < CPT; ++c) {
+          const double a0 = X[c][0], a1 = X[c][1], a2 = X[c][2];
+          if (gg == 0)
+            sm[c] = (a0 * a0 + a1 * a1 + a2 * a2) * wis[0];
+          else
+            sm[c] = sm[c] + (a0 * a0) * wis[3 * gg] + (a1 * a1) * wis[3 * gg + 1] + (a2 * a2) * wis[3 * gg + 2];
+        }
+      });
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) IS[c][st] = sm[c];
     }
     double W[CPT][9];
 #pragma unroll
@@ -1821,14 +1872,17 @@ __global__ void __launch_bounds__(32 * (kE ? 3 : 8) / CPT) k_p2(Dims d, PhysC ph
       for (int m = 0; m < NO; ++m) acc[c][m] = 0.0;
 #pragma unroll 1
     for (int st = 0; st < 8; ++st) {
-      R X[CPT][NM];
-      stencil(st, NO, X);
+      stencil(st, 0, kE ? 1 : NG, [&](int gi, R (*X)[3]) {
 #pragma unroll
-      for (int c = 0; c < CPT; ++c) {
-        const double ws = W[c][st];
+        for (int c = 0; c < CPT; ++c) {
+          const double ws = W[c][st];
 #pragma unroll
-        for (int m = 0; m < NO; ++m) acc[c][m] = st == 0 ? ws * (double)X[c][m] : acc[c][m] + ws * (double)X[c][m];
-      }
+          for (int q = 0; q < (kE ? 1 : 3); ++q) {
+            const int m = kE ? 0 : 3 * gi + q;
+            acc[c][m] = st == 0 ? ws * (double)X[c][q] : acc[c][m] + ws * (double)X[c][q];
+          }
+        }
+      });
     }
     const R fl = s.flatA[d.at(0, p, i, j, k)], x = R(1.0) - fl;
 #pragma unroll
