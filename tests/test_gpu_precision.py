@@ -154,9 +154,11 @@ def test_fp32_form_without_resident_operators_tracks_the_cached_form():
     (CS_FLAG_NO_OP_CACHE, taken on meshes too large for them: every stage
     rebuilds the rows and inverts the normal matrices, in FP64 like the
     cached weights, and rounds the inverse once) stays within FP32 rounding
-    of the cached form: relative L1 <= 1e-6 per field after 3 steps."""
+    of the cached form after 3 steps: relative L1 <= 1e-6 per field, 5e-5
+    for the momentum (the shell starts at rest, so it is small against its
+    own rounding): TOL_L1, the bounds of test_fp32_form_tracks_fp64."""
     s0, dts = run("shell16", cs.CS_FLAG_FP32, 3)
     s1, _ = run("shell16", cs.CS_FLAG_FP32 | cs.CS_FLAG_NO_OP_CACHE, 3, dts=dts)
     err = field_errors(s0, s1.get_state(), s0.get_state())
     for k in ("rho", "mom", "E", "ent", "B"):
-        assert err[k] <= 1e-6, (k, err[k], err)
+        assert err[k] <= TOL_L1[k], (k, err[k], err)
