@@ -132,6 +132,7 @@ def parse():
     ap.add_argument("--workload", default="shell128")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-form sample")
+    ap.add_argument("--no-p2", action="store_true", help="skip the LIMIT_ALL_SLOPES_P2 sample (one GPU only)")
     ap.add_argument("--no-precision", action="store_true", help="skip the FP32 precision-form sample")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-form sample")
     ap.add_argument("--flags", type=int, default=0,
@@ -452,6 +453,35 @@ def precision_sample(pr, dts, steps, ref_state, zones, world, allmax) -> dict:
             "max_divb_over_bmax": divb_rel, "long_run": precision_long_sample()}
 
 
+def p2_sample(pr, steps: int, zones: int) -> dict:
+    """LIMIT_ALL_SLOPES_P2 (CS_FLAG_P2) in place of P12 on the same workload
+    and precision: 3 untimed steps, then `steps` steps replayed from the
+    captured step graph and timed with CUDA events as the headline."""
+    import torch
+
+    import cubesphere_b200 as cs
+
+    f = cs.Solve(**pr["params"], flags=cs.CS_FLAG_P2)
+    f.mesh_build()
+    f.init_problem(**pr["init"])
+    stream = torch.cuda.ExternalStream(f.stream_ptr())
+    dt = f.steps(3, f.evaluate_timestep(1e30))
+    f.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    dt = f.steps(steps, dt)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    _, _, divb = f.diag()
+    f.close()
+    return {"value": zones * steps / (ms / 1e3), "unit": "zone-updates/s", "ms_per_step": ms / steps,
+            "reconstruction": "LIMIT_ALL_SLOPES_P2 (420limit_all_slopes_p2.f): eight one-sided quadratic stencils "
+                              "+ the central least squares, resident stencil inverses",
+            "finite": bool(dt == dt and dt > 0), "max_divb": divb}
+
+
 def state_errors(s, got, ref, divb):
     """Relative L1 and Linf errors of `got` against `ref` per field (interior
     zones; the three face-B components as one field) and max |div B| over
@@ -752,6 +782,13 @@ def run_gpu(args):
     if ref_state is not None:
         torch.cuda.synchronize()
         precision = precision_sample(pr, dts[:PRECISION_STEPS], args.steps, ref_state, zones, world, allmax)
+    p2 = None
+    if world == 1 and not (args.no_p2 or args.flags):
+        torch.cuda.synchronize()
+        try:
+            p2 = p2_sample(pr, args.steps, zones)
+        except Exception as e:  # recorded, not fatal: the headline line still prints
+            p2 = {"error": f"{type(e).__name__}: {e}"}
     precision_stated = None
     if args.precision_workload:
         torch.cuda.synchronize()
@@ -789,7 +826,7 @@ def run_gpu(args):
         "roofline": roof, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches,
         "top_kernels": {k: round(v[0] / prof_steps, 3) for k, v in
                         sorted(prof.items(), key=lambda kv: -kv[1][0])[:8]},
-        "finite": finite, "dt_last": dt, "precision_form": precision, "precision_stated": precision_stated,
+        "finite": finite, "dt_last": dt, "precision_form": precision, "p2_form": p2, "precision_stated": precision_stated,
         "batch": batch, "serving": serving,
     }
     if rank == 0:
