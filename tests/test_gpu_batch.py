@@ -79,6 +79,32 @@ def test_batch_is_reproducible_under_concurrency():
             s.close()
 
 
+def test_batch_of_p2_solves_matches_each_solve_alone():
+    """The same members with LIMIT_ALL_SLOPES_P2 (CS_FLAG_P2: the kernels with
+    the largest per-thread stacks of the library) batched side by side, twice,
+    equal each solve run alone, bit for bit."""
+    members = [(n, o, i, f | cs.CS_FLAG_P2) for (n, o, i, f) in MEMBERS]
+    want = []
+    for m in members:
+        s = make(m)
+        dt = s.steps(3, s.evaluate_timestep(1e30))
+        want.append((dt, s.get_state()))
+        s.close()
+    for rep in range(2):
+        sols = [make(m) for m in members]
+        b = cs.Batch(sols)
+        dts = b.steps(3, [s.evaluate_timestep(1e30) for s in sols])
+        for q, s in enumerate(sols):
+            dt0, st0 = want[q]
+            assert dts[q] == dt0, (rep, q)
+            st = s.get_state()
+            for k in st0:
+                assert np.array_equal(st[k], st0[k]), (rep, q, k)
+        b.close()
+        for s in sols:
+            s.close()
+
+
 def test_autotune_changes_no_result():
     want = alone(2)
     sols = [make(m) for m in MEMBERS]
