@@ -121,7 +121,7 @@ void fill_ghosts(Ctx& c) {
     return c.m(pn, i, std::max(j, 1 - G)) * c.m(pn, i, std::min(j + 1, N + G));
   };
   for (int pn = 0; pn < 6; ++pn) {
-    const int rt = kNbr[pn][0] - 1, lf = kNbr[pn][1] - 1, up = kNbr[pn][2] - 1, dn = kNbr[pn][3] - 1;
+    const int rt = kNbr[pn][0] - 1, lf = kNbr[pn][1] - 1;
     auto inner = [&](int j, int k) { return j >= 1 && j <= N && k >= 1 && k <= nr; };
     // ---- x direction: right strip
     OMP_ZONES
@@ -1321,7 +1321,7 @@ void limit_all_slopes_p12(Ctx& c, int pn) {
 // ------------------------------------------------------------------
 // MAKE_FACIAL_FLUXES (400riemann_integrate/450make_facial_fluxes.f:405-2933), one panel.
 void make_facial_fluxes(Ctx& c, int pn) {
-  const int N = c.N, G = c.G, nr = c.nr;
+  const int N = c.N, nr = c.nr;
   const double sm = c.p.smallnum;
   auto V = [&](int comp, int mode, int i, int j, int k) -> double& { return c.a(c.V, mode * NV + comp, pn, i, j, k); };
   for (int dir = 0; dir < 3; ++dir) {
@@ -1481,7 +1481,7 @@ void scatter_facial_fluxes(Ctx& c, int pn) {
     for (int j = 1 - G; j <= N + G; ++j)
       for (int i = 1 - G; i <= N + G; ++i)
         for (int q = 0; q < NV; ++q) c.a(c.dUdt, q, pn, i, j, k) = 0.0;
-  auto sub = [&](int dir, int jq, size_t fo, long long z, const std::vector<double>& cc) {
+  auto sub = [&](int jq, size_t fo, long long z, const std::vector<double>& cc) {
     for (int q = 0; q < NV; ++q) {
       double& d = c.dUdt[((size_t)q * 6 + pn) * c.S + (size_t)z];
       d = d - cc[((size_t)(jq * NV + q) * 6 + pn) * c.S + fo];
@@ -1498,8 +1498,8 @@ void scatter_facial_fluxes(Ctx& c, int pn) {
             const size_t fo = c.idx(i, j, k);
             const long long l = c.tL[dir][(size_t)pn * c.S + fo], r = c.tR[dir][(size_t)pn * c.S + fo];
             if (l < 0) continue;
-            sub(dir, jq, fo, l, c.cL[dir]);
-            sub(dir, jq, fo, r, c.cR[dir]);
+            sub(jq, fo, l, c.cL[dir]);
+            sub(jq, fo, r, c.cR[dir]);
           }
   }
   // z faces k in [-1, nr + 1] over (i, j) in [0, N + 1]^2: lower side zone
@@ -1516,8 +1516,8 @@ void scatter_facial_fluxes(Ctx& c, int pn) {
         if (ub && c.tR[2][(size_t)pn * c.S + fb] != z) std::abort();
         if (ua && c.tL[2][(size_t)pn * c.S + fa] != z) std::abort();
         for (int jq = 0; jq < 5; ++jq) {
-          if (ub) sub(2, jq, fb, z, c.cR[2]);
-          if (ua) sub(2, jq, fa, z, c.cL[2]);
+          if (ub) sub(jq, fb, z, c.cR[2]);
+          if (ua) sub(jq, fa, z, c.cL[2]);
         }
       }
 }

@@ -38,9 +38,11 @@ def test_initial_field_is_divergence_free():
     assert _divb(s, st) < 1e-12
 
 
-@pytest.mark.parametrize("rk", [cs.CS_RK2, cs.CS_IMEX_RK2])
-def test_panel_edge_ownership_keeps_div_b_at_roundoff(rk):
-    s, o, st = _setup(0, rk_scheme=rk)
+@pytest.mark.parametrize("rk,flags", [(cs.CS_RK2, 0), (cs.CS_IMEX_RK2, 0), (cs.CS_IMEX_RK2, cs.CS_FLAG_P2)])
+def test_panel_edge_ownership_keeps_div_b_at_roundoff(rk, flags):
+    """CT with panel-edge ownership keeps div B at round-off whichever
+    reconstruction (P12 or P2) feeds the EMFs."""
+    s, o, st = _setup(flags, rk_scheme=rk)
     dt = o.evaluate_timestep(1e30)
     for _ in range(2):
         dt = o.step(dt)
@@ -263,7 +265,8 @@ def test_p2_interpolates_a_quadratic_electric_field_to_its_zone_averages():
         assert err < 1e-12, (q, err)
 
 
-def test_uniform_static_gas_stays_uniform_to_the_mesh_closure():
+@pytest.mark.parametrize("flags", [0, cs.CS_FLAG_P2])
+def test_uniform_static_gas_stays_uniform_to_the_mesh_closure(flags):
     """A uniform gas at rest (no field, no gravity) changes in one step only
     through the discrete closure of each zone's faces (sum of area x
     quadrature-weighted normals, 2.5e-8 of the face area on shell16: the
@@ -275,7 +278,7 @@ def test_uniform_static_gas_stays_uniform_to_the_mesh_closure():
     from seeded_states import uniform_state
 
     pr = cs.preset("shell16")
-    pr["params"]["gm"] = 0.0
+    pr["params"].update(gm=0.0, flags=flags)
     s = cs.Solve(**pr["params"])
     s.mesh_build(device=False)
     st = uniform_state(s)
