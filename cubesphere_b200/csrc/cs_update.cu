@@ -249,7 +249,7 @@ __global__ void k_cleanup_zones(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 
       }
       const double Rm[6] = {s.Bxf[d.at(0, p, i, j, k)], s.Bxf[d.at(0, p, i - 1, j, k)], s.Byf[d.at(0, p, i, j, k)],
                             s.Byf[d.at(0, p, i, j - 1, k)], s.Bzf[d.at(0, p, i, j, k)], s.Bzf[d.at(0, p, i, j, k - 1)]};
-      double M[3][3], R[3];
+      double M[3][3], rhs[3];
 #pragma unroll
       for (int a1 = 0; a1 < 3; ++a1) {
 #pragma unroll
@@ -262,7 +262,7 @@ __global__ void k_cleanup_zones(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 
         double sm = 0.0;
 #pragma unroll
         for (int q = 0; q < 6; ++q) sm = sm + Am[q][a1] * Rm[q];
-        R[a1] = sm;
+        rhs[a1] = sm;
       }
       const double a11 = M[0][0], a12 = M[0][1], a13 = M[0][2], a21 = M[1][0], a22 = M[1][1], a23 = M[1][2],
                    a31 = M[2][0], a32 = M[2][1], a33 = M[2][2];
@@ -271,9 +271,9 @@ __global__ void k_cleanup_zones(Dims d, PhysC ph, DGeom g, DStateT<R> s, Range3 
       const double b11 = (a22 * a33 - a23 * a32) * ob, b12 = (a13 * a32 - a12 * a33) * ob, b13 = (a12 * a23 - a22 * a13) * ob;
       const double b21 = (a23 * a31 - a21 * a33) * ob, b22 = (a11 * a33 - a13 * a31) * ob, b23 = (a13 * a21 - a11 * a23) * ob;
       const double b31 = (a21 * a32 - a22 * a31) * ob, b32 = (a12 * a31 - a11 * a32) * ob, b33 = (a11 * a22 - a12 * a21) * ob;
-      const double nb0 = b11 * R[0] + b12 * R[1] + b13 * R[2];
-      const double nb1 = b21 * R[0] + b22 * R[1] + b23 * R[2];
-      const double nb2 = b31 * R[0] + b32 * R[1] + b33 * R[2];
+      const double nb0 = b11 * rhs[0] + b12 * rhs[1] + b13 * rhs[2];
+      const double nb1 = b21 * rhs[0] + b22 * rhs[1] + b23 * rhs[2];
+      const double nb2 = b31 * rhs[0] + b32 * rhs[1] + b33 * rhs[2];
       const double Bx = U[5], By = U[6], Bz = U[7];
       U[5] = nb0;
       U[6] = nb1;
