@@ -78,3 +78,16 @@ def test_device_estimate_counts_panel_shared_row_weights():
     f32 = cs.estimate_device_bytes(**kw, flags=cs.CS_FLAG_FP32)
     f32_pp = cs.estimate_device_bytes(**kw, flags=cs.CS_FLAG_FP32 | cs.CS_FLAG_LSQ_PER_PANEL)
     assert f32_pp - f32 == (nl - nl // 6) * 352 * 4
+
+
+def test_device_estimate_counts_the_p2_stencil_inverses():
+    """With CS_FLAG_P2 the estimate adds the eight one-sided 9 x 9 (STEP 7.a)
+    and 10 x 10 (STEP 9.b) inverses per zone of the least-squares range,
+    panel 1's serving the six panels, one set per panel with
+    CS_FLAG_LSQ_PER_PANEL, in the state's type."""
+    kw = dict(ntp=32, nr=16, nghost=4)
+    nl = 6 * (32 + 2 * 4 - 4) ** 2 * (16 + 2 * 4 - 4)
+    for flags, n, size in ((0, nl // 6, 8), (cs.CS_FLAG_LSQ_PER_PANEL, nl, 8), (cs.CS_FLAG_FP32, nl // 6, 4)):
+        base = cs.estimate_device_bytes(**kw, flags=flags)
+        p2 = cs.estimate_device_bytes(**kw, flags=flags | cs.CS_FLAG_P2)
+        assert p2 - base == n * (8 * 81 + 8 * 100) * size, flags
