@@ -797,7 +797,7 @@ def run_gpu(args):
     if args.stated_batch:
         torch.cuda.synchronize()
         batch = batch_sample(seed=11, nsol=64, steps=2, sizes=(32, 48, 64, 96, 128), depths=(1, 16, 32, 64))
-    elif not args.no_batch:
+    elif not args.no_batch and world == 1:  # single-GPU characterisations: not repeated on every rank
         torch.cuda.synchronize()
         batch = batch_sample()
     serving = None
@@ -805,7 +805,7 @@ def run_gpu(args):
         torch.cuda.synchronize()
         serving = serving_sample(seed=7, nreq=24, rate=2.0, max_active=8, sizes=(32, 48, 64, 96, 128),
                                  depths=(1, 16, 32, 64), step_range=(20, 500))
-    elif not args.no_serving:
+    elif not args.no_serving and world == 1:
         torch.cuda.synchronize()
         serving = serving_sample()
 
