@@ -42,6 +42,7 @@ CS_RK2, CS_SSPRK3, CS_IMEX_RK2 = 2, 3, 4
 EXPORTS = [
     "cs_geom_ncomp", "cs_create", "cs_destroy", "cs_last_error", "cs_box_dims", "cs_params_check",
     "cs_mesh_build", "cs_mesh_share", "cs_mesh_device_bytes", "cs_mesh_build_host", "cs_geometry_get", "cs_mask_get", "cs_stencil_get",
+    "cs_fill_map_get",
     "cs_geometry_single_zone", "cs_init_problem", "cs_init_problem_host", "cs_state_put", "cs_state_get",
     "cs_stage", "cs_step", "cs_steps", "cs_evaluate_timestep", "cs_synchronize", "cs_fill_ghosts",
     "cs_limit_all_slopes_p12", "cs_make_facial_fluxes", "cs_make_edge_efields_p1",
@@ -152,6 +153,7 @@ def load_library() -> ctypes.CDLL:
         "cs_geometry_get": ([P, ctypes.c_int, dp, S], ctypes.c_int),
         "cs_mask_get": ([P, ip, S], ctypes.c_int),
         "cs_stencil_get": ([P, ip, S], ctypes.c_int),
+        "cs_fill_map_get": ([P, ip, ip, ctypes.POINTER(ctypes.c_uint8), ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
         "cs_geometry_single_zone": ([I, I, I, I, D, D, I, I, dp, S], ctypes.c_int),
         "cs_init_problem": ([P, ctypes.POINTER(CsInitDesc)], ctypes.c_int),
         "cs_init_problem_host": ([P, ctypes.POINTER(CsInitDesc), dp, dp, dp, dp, dp], ctypes.c_int),
@@ -295,6 +297,21 @@ class Solve:
         out = np.zeros((6, self.NK, self.NJ, self.NI), dtype=np.int32)
         self._check(self.lib.cs_mask_get(self.h, _iptr(out), out.size), "cs_mask_get")
         return out
+
+    def fill_map(self):
+        """The ghost-exchange map cs_fill_ghosts applies (cs_fill_map_get):
+        arrays src, dst (int32 element offsets into the field arrays) and meta
+        (uint8: destination field bits 0-2, source field bits 5-7, negate bit
+        3, average bit 4)."""
+        n = ctypes.c_int64(0)
+        self._check(self.lib.cs_fill_map_get(self.h, None, None, None, ctypes.byref(n)), "cs_fill_map_get")
+        src = np.zeros(n.value, dtype=np.int32)
+        dst = np.zeros(n.value, dtype=np.int32)
+        meta = np.zeros(n.value, dtype=np.uint8)
+        self._check(self.lib.cs_fill_map_get(self.h, _iptr(src), _iptr(dst),
+                                             meta.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), ctypes.byref(n)),
+                    "cs_fill_map_get")
+        return src, dst, meta
 
     def stencil(self) -> np.ndarray:
         out = np.zeros((6, 12, 2, self.NJ, self.NI), dtype=np.int32)

@@ -134,6 +134,16 @@ struct MapEntry {
   uint8_t meta;
 };
 
+// The order the device applies the map in: by destination field, then by
+// destination offset (all sources are read before any write, so the order
+// changes no value; it keeps the scatter's writes coalesced).
+void sort_fill_map(std::vector<MapEntry>& map) {
+  std::sort(map.begin(), map.end(), [](const MapEntry& a, const MapEntry& b2) {
+    if ((a.meta & 7) != (b2.meta & 7)) return (a.meta & 7) < (b2.meta & 7);
+    return a.dst < b2.dst;
+  });
+}
+
 std::string build_fill_map(const Solve& sv, std::vector<MapEntry>& out) {
   const GeomHost& g = sv.mesh->host;
   const Box& b = g.box;
@@ -548,10 +558,7 @@ int mesh_upload(Solve& sv, MeshRes& m) {
   std::vector<MapEntry> map;
   std::string why = build_fill_map(sv, map);
   if (!why.empty()) return fail(sv, CS_ERR_ARG, why);
-  std::sort(map.begin(), map.end(), [](const MapEntry& a, const MapEntry& b2) {
-    if ((a.meta & 7) != (b2.meta & 7)) return (a.meta & 7) < (b2.meta & 7);
-    return a.dst < b2.dst;
-  });
+  sort_fill_map(map);
   const size_t n = map.size();
   std::vector<int32_t> hs(n), hd(n);
   std::vector<uint8_t> hm(n);
@@ -1208,6 +1215,27 @@ int cs_geometry_get(cs_ctx* ctx, int field, double* host_out, size_t n) {
   const std::vector<double>& v = sv.mesh->host.f[field];
   if (n != v.size()) return cs::fail(sv, CS_ERR_ARG, "geometry buffer size mismatch");
   std::memcpy(host_out, v.data(), n * sizeof(double));
+  return CS_OK;
+}
+
+int cs_fill_map_get(cs_ctx* ctx, int32_t* src, int32_t* dst, uint8_t* meta, int64_t* n) {
+  if (!ctx || !n) return CS_ERR_ARG;
+  Solve& sv = ctx->sv;
+  if (int rc = cs::ensure_host_mesh(sv)) return rc;
+  std::vector<cs::MapEntry> map;
+  const std::string why = cs::build_fill_map(sv, map);
+  if (!why.empty()) return cs::fail(sv, CS_ERR_ARG, why);
+  cs::sort_fill_map(map);
+  if (src || dst || meta) {
+    if (!src || !dst || !meta) return cs::fail(sv, CS_ERR_ARG, "src, dst and meta are all given or all null");
+    if (*n != (int64_t)map.size()) return cs::fail(sv, CS_ERR_ARG, "fill map buffer size mismatch");
+    for (size_t t = 0; t < map.size(); ++t) {
+      src[t] = map[t].src;
+      dst[t] = map[t].dst;
+      meta[t] = map[t].meta;
+    }
+  }
+  *n = (int64_t)map.size();
   return CS_OK;
 }
 

@@ -243,6 +243,20 @@ int cs_mesh_device_bytes(cs_ctx* ctx, uint64_t* bytes);
 int cs_mesh_build_host(cs_ctx* ctx);
 int cs_geometry_get(cs_ctx* ctx, int field, double* host_out, size_t n_doubles);
 int cs_mask_get(cs_ctx* ctx, int32_t* host_out, size_t n);            /* imask_active, per box */
+/* Host copy of the ghost-exchange map cs_fill_ghosts applies on the device
+ * (the panel-edge exchange of the reference's LOAD_LOCAL_BUFFERS_* /
+ * FETCH_BUFFERS_FILL_IN_* routines, 300riemann_module/320-333, written as
+ * one list): entry t sets element dst[t] from element src[t], both offsets
+ * into a field array of the panel-box layout (for U they include the
+ * component), and meta[t] holds the destination field in bits 0-2, the
+ * source field in bits 5-7 (0 U, 1 entropy mode 1, 2 Bxf, 3 Byf, 4 Bzf), a
+ * negation in bit 3 and, in bit 4, averaging with the destination's value
+ * before the exchange.  Every source is read before any destination is
+ * written.  Built from the host mesh (cs_mesh_build_host is enough: no
+ * device).  With all three arrays null only *n is set; otherwise *n must be
+ * the entry count.  A panel split across ranks exchanges the entries whose
+ * source and destination panels sit on different ranks. */
+int cs_fill_map_get(cs_ctx* ctx, int32_t* src, int32_t* dst, uint8_t* meta, int64_t* n);
 int cs_stencil_get(cs_ctx* ctx, int32_t* host_out, size_t n);         /* istencil, [6][12][2][NJ][NI] */
 
 /* Geometry of one coarse zone cut with stride iscale out of sector isector
