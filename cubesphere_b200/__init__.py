@@ -42,7 +42,7 @@ CS_RK2, CS_SSPRK3, CS_IMEX_RK2 = 2, 3, 4
 EXPORTS = [
     "cs_geom_ncomp", "cs_create", "cs_destroy", "cs_last_error", "cs_box_dims", "cs_params_check",
     "cs_mesh_build", "cs_mesh_share", "cs_mesh_device_bytes", "cs_mesh_build_host", "cs_geometry_get", "cs_mask_get", "cs_stencil_get",
-    "cs_fill_map_get",
+    "cs_fill_map_get", "cs_sync_map_get",
     "cs_geometry_single_zone", "cs_init_problem", "cs_init_problem_host", "cs_state_put", "cs_state_get",
     "cs_stage", "cs_step", "cs_steps", "cs_evaluate_timestep", "cs_synchronize", "cs_fill_ghosts",
     "cs_limit_all_slopes_p12", "cs_make_facial_fluxes", "cs_make_edge_efields_p1",
@@ -154,6 +154,8 @@ def load_library() -> ctypes.CDLL:
         "cs_mask_get": ([P, ip, S], ctypes.c_int),
         "cs_stencil_get": ([P, ip, S], ctypes.c_int),
         "cs_fill_map_get": ([P, ip, ip, ctypes.POINTER(ctypes.c_uint8), ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
+        "cs_sync_map_get": ([P, I, ip, ip, ctypes.POINTER(ctypes.c_int8), ctypes.POINTER(ctypes.c_int8),
+                             ctypes.POINTER(ctypes.c_int8), ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
         "cs_geometry_single_zone": ([I, I, I, I, D, D, I, I, dp, S], ctypes.c_int),
         "cs_init_problem": ([P, ctypes.POINTER(CsInitDesc)], ctypes.c_int),
         "cs_init_problem_host": ([P, ctypes.POINTER(CsInitDesc), dp, dp, dp, dp, dp], ctypes.c_int),
@@ -312,6 +314,20 @@ class Solve:
                                              meta.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), ctypes.byref(n)),
                     "cs_fill_map_get")
         return src, dst, meta
+
+    def sync_map(self, which: int):
+        """The panel-edge ownership list cs_stage applies (cs_sync_map_get):
+        which 0 faces, 1 edges.  Arrays dst, src (int32 offsets), dst_kind,
+        src_kind (int8 face direction or EMF component) and sign (int8)."""
+        n = ctypes.c_int64(0)
+        self._check(self.lib.cs_sync_map_get(self.h, which, None, None, None, None, None, ctypes.byref(n)),
+                    "cs_sync_map_get")
+        dst, src = np.zeros(n.value, dtype=np.int32), np.zeros(n.value, dtype=np.int32)
+        dk, sk, sg = (np.zeros(n.value, dtype=np.int8) for _ in range(3))
+        i8 = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_int8))
+        self._check(self.lib.cs_sync_map_get(self.h, which, _iptr(dst), _iptr(src), i8(dk), i8(sk), i8(sg),
+                                             ctypes.byref(n)), "cs_sync_map_get")
+        return dst, src, dk, sk, sg
 
     def stencil(self) -> np.ndarray:
         out = np.zeros((6, 12, 2, self.NJ, self.NI), dtype=np.int32)

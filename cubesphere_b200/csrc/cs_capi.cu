@@ -1239,6 +1239,31 @@ int cs_fill_map_get(cs_ctx* ctx, int32_t* src, int32_t* dst, uint8_t* meta, int6
   return CS_OK;
 }
 
+int cs_sync_map_get(cs_ctx* ctx, int32_t which, int32_t* dst, int32_t* src, int8_t* dst_kind, int8_t* src_kind,
+                    int8_t* sign, int64_t* n) {
+  if (!ctx || !n || (which != 0 && which != 1)) return CS_ERR_ARG;
+  Solve& sv = ctx->sv;
+  if (int rc = cs::ensure_host_mesh(sv)) return rc;
+  cs::SyncMaps m;
+  const std::string why = cs::build_sync_maps(sv, m);
+  if (!why.empty()) return cs::fail(sv, CS_ERR_ARG, why);
+  const size_t cnt = which == 0 ? m.f_dst.size() : m.e_dst.size();
+  if (dst || src || dst_kind || src_kind || sign) {
+    if (!dst || !src || !dst_kind || !src_kind || !sign)
+      return cs::fail(sv, CS_ERR_ARG, "dst, src, dst_kind, src_kind and sign are all given or all null");
+    if (*n != (int64_t)cnt) return cs::fail(sv, CS_ERR_ARG, "sync map buffer size mismatch");
+    for (size_t t = 0; t < cnt; ++t) {
+      dst[t] = which == 0 ? m.f_dst[t] : m.e_dst[t];
+      src[t] = which == 0 ? m.f_src[t] : m.e_src[t];
+      dst_kind[t] = which == 0 ? m.f_ddir[t] : m.e_df[t];
+      src_kind[t] = which == 0 ? m.f_sdir[t] : m.e_sf[t];
+      sign[t] = which == 0 ? (int8_t)-1 : m.e_sign[t];
+    }
+  }
+  *n = (int64_t)cnt;
+  return CS_OK;
+}
+
 int cs_mask_get(cs_ctx* ctx, int32_t* host_out, size_t n) {
   if (!ctx || !host_out) return CS_ERR_ARG;
   Solve& sv = ctx->sv;

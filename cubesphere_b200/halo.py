@@ -1,19 +1,25 @@
-"""Ghost exchange of a solve whose panels are split across ranks.
+"""Exchanges of a solve whose panels are split across ranks.
 
-The device fill (cs_fill_ghosts) applies one list of entries, each setting
-one ghost value from one source value (cs_fill_map_get: source and
-destination offsets into the field arrays, the fields, a sign, and whether
-the value is averaged with the destination's own).  This is the exchange of
-the reference's LOAD_LOCAL_BUFFERS_* / FETCH_BUFFERS_FILL_IN_* routines
-(300riemann_module/320-333), which run it between MPI ranks that each own
-panels.  With the panels assigned to ranks, the entries whose destination
-panel a rank owns split into those it can apply from its own panels and
-those whose source panel another rank owns; every rank derives both its
-receive lists and the matching send lists from the same global list, so the
-two sides agree on order without exchanging any index.
+Two lists move values between panels during a stage, and both are explicit:
 
-Host arrays or torch tensors (CPU with gloo, CUDA with NCCL) hold the
-fields; `exchange` is one grouped point-to-point round per call.
+* the ghost fill (cs_fill_ghosts; cs_fill_map_get): each entry sets one
+  ghost value from one source value (source and destination offsets into
+  the field arrays, the fields, a sign, and whether the value is averaged
+  with the destination's own).  This is the exchange of the reference's
+  LOAD_LOCAL_BUFFERS_* / FETCH_BUFFERS_FILL_IN_* routines
+  (300riemann_module/320-333), which run it between MPI ranks that each own
+  panels;
+* panel-edge ownership (cs_sync_map_get): the face fluxes and edge EMFs that
+  two or three panels compute take the lowest-numbered panel's value, the
+  single-device form of the reference's defect exchange (DRV:3200-3461).
+
+With the panels assigned to ranks, the entries whose destination panel a
+rank owns split into those it can apply from its own panels and those whose
+source panel another rank owns; every rank derives both its receive lists
+and the matching send lists from the same global list, so the two sides
+agree on order without exchanging any index.  Host arrays (numpy) hold the
+fields for the single-process forms; torch tensors (CPU with gloo, CUDA with
+NCCL) for the split ones, one grouped point-to-point round per exchange.
 """
 from __future__ import annotations
 
@@ -64,17 +70,41 @@ def apply_fill_map(st: dict, src, dst, meta) -> None:
         flat[f][dst[sel]] = vals[sel]
 
 
-class PanelSplit:
-    """Exchange lists of one rank: `panel_rank[p]` is the rank owning panel
-    p; `box` the points of one panel box.  Entries whose destination panel
-    this rank owns are applied here: `local` ones from its own panels, the
-    `recv[q]` ones from values rank q sends, in the global list's order;
-    `send[q]` lists the entries rank q applies from this rank's panels, in
-    the same order."""
+def apply_face_sync(fcon, EF, dst, src, dk, sk) -> None:
+    """Face ownership on host arrays, in place: fcon[d] (16, 6 * box) holds
+    a direction's two one-sided contributions (components 0-7 and 8-15) and
+    EF[d] (6 * box) its entropy flux; each listed copy takes its owner's
+    contributions with the sides exchanged and the negated entropy flux."""
+    for d in range(len(fcon)):
+        for s in range(len(fcon)):
+            sel = np.flatnonzero((dk == d) & (sk == s))
+            if len(sel):
+                fcon[d][:, dst[sel]] = np.roll(fcon[s][:, src[sel]], 8, axis=0)
+                EF[d][dst[sel]] = -EF[s][src[sel]]
 
-    def __init__(self, src, dst, meta, box: int, panel_rank, rank: int):
+
+def apply_edge_sync(Ef, dst, src, dk, sk, sign) -> None:
+    """Edge ownership on host arrays, in place: Ef[c] (6 * box) is EMF
+    component c; each listed copy takes its owner's value times sign."""
+    vals = np.array([sign[t] * Ef[sk[t]][src[t]] for t in range(len(dst))])
+    for c in range(len(Ef)):
+        sel = dk == c
+        Ef[c][dst[sel]] = vals[sel]
+
+
+class PanelSplit:
+    """Entries of one exchange list as one rank sees them: `panel_rank[p]`
+    is the rank owning panel p, `box` the points of one panel box, and src /
+    dst the entries' offsets (for multi-component fields, any offset whose
+    panel is (offset // box) % 6).  `mine` are the entries whose destination
+    panel this rank owns: `local` ones from its own panels, the `recv[q]`
+    ones from values rank q sends, in the global list's order; `send[q]`
+    lists the entries rank q applies from this rank's panels, in the same
+    order."""
+
+    def __init__(self, src, dst, box: int, panel_rank, rank: int):
         panel_rank = np.asarray(panel_rank)
-        self.src, self.dst, self.meta = np.asarray(src), np.asarray(dst), np.asarray(meta)
+        self.src, self.dst = np.asarray(src), np.asarray(dst)
         sp = panel_rank[(self.src // box) % 6]
         dp = panel_rank[(self.dst // box) % 6]
         self.rank = rank
@@ -84,53 +114,143 @@ class PanelSplit:
         self.recv = {q: np.flatnonzero((dp == rank) & (sp == q)) for q in self.peers}
         self.send = {q: np.flatnonzero((dp == q) & (sp == rank)) for q in self.peers}
 
-    def values_bytes(self) -> int:
-        """Bytes this rank sends per exchange (FP64 values)."""
-        return 8 * sum(len(v) for v in self.send.values())
+    def values_bytes(self, width: int = 1) -> int:
+        """Bytes this rank sends per exchange (`width` FP64 values an entry)."""
+        return 8 * width * sum(len(v) for v in self.send.values())
 
-    def exchange(self, st: dict, dist) -> None:
-        """Fills this rank's ghost values in `st` (torch tensors; the other
-        ranks' panels may hold anything) from its own panels and its peers'
-        messages; every rank of the split calls it together."""
+    def route(self, gather, dist, width: int, device):
+        """Source values of every entry in `mine` (a (len(mine), width) FP64
+        tensor, in `mine`'s order): `gather(entries)` reads the values of
+        the given entries from this rank's panels; every source value is
+        read before the caller writes any destination.  Every rank of the
+        split calls it together."""
         import torch
 
-        flat = _fields(st)
-        dev = flat[0].device
-        idx = lambda a: torch.as_tensor(a, device=dev, dtype=torch.long)
-
-        def gather(entries):
-            s, f = self.src[entries], self.meta[entries] >> 5
-            out = torch.empty(len(entries), dtype=torch.float64, device=dev)
-            for k in range(5):
-                sel = np.flatnonzero(f == k)
-                if len(sel):
-                    out[idx(sel)] = flat[k][idx(s[sel])].to(torch.float64)
-            return out
-
-        # every source value read before any destination is written
         bufs = {q: gather(self.send[q]) for q in self.peers}
-        incoming = {q: torch.empty(len(self.recv[q]), dtype=torch.float64, device=dev) for q in self.peers}
+        incoming = {q: torch.empty((len(self.recv[q]), width), dtype=torch.float64, device=device) for q in self.peers}
         ops = []
         for q in self.peers:
             if len(self.send[q]):
-                ops.append(dist.P2POp(dist.isend, bufs[q], q))
+                ops.append(dist.P2POp(dist.isend, bufs[q].contiguous(), q))
             if len(self.recv[q]):
                 ops.append(dist.P2POp(dist.irecv, incoming[q], q))
         for w in (dist.batch_isend_irecv(ops) if ops else []):
             w.wait()
-        vals = torch.empty(len(self.src), dtype=torch.float64, device=dev)
-        vals[idx(self.local)] = gather(self.local)
+        vals = torch.empty((len(self.src), width), dtype=torch.float64, device=device)
+        vals[torch.as_tensor(self.local, device=device, dtype=torch.long)] = gather(self.local)
         for q in self.peers:
-            vals[idx(self.recv[q])] = incoming[q]
-        mine = self.mine
-        d, m = self.dst[mine], self.meta[mine]
-        old = torch.empty(len(mine), dtype=torch.float64, device=dev)
+            vals[torch.as_tensor(self.recv[q], device=device, dtype=torch.long)] = incoming[q]
+        return vals[torch.as_tensor(self.mine, device=device, dtype=torch.long)]
+
+
+def _idx(a, dev):
+    import torch
+
+    return torch.as_tensor(a, device=dev, dtype=torch.long)
+
+
+class GhostExchange(PanelSplit):
+    """The ghost fill split across ranks (cs_fill_map_get's src, dst, meta)."""
+
+    def __init__(self, src, dst, meta, box: int, panel_rank, rank: int):
+        super().__init__(src, dst, box, panel_rank, rank)
+        self.meta = np.asarray(meta)
+
+    def exchange(self, st: dict, dist) -> None:
+        """Fills this rank's ghost values in `st` (torch tensors U, ent,
+        bxf, byf, bzf; the other ranks' panels may hold anything) from its
+        own panels and its peers' messages."""
+        import torch
+
+        flat = _fields(st)
+        dev = flat[0].device
+
+        def gather(entries):
+            s, f = self.src[entries], self.meta[entries] >> 5
+            out = torch.empty((len(entries), 1), dtype=torch.float64, device=dev)
+            for k in range(5):
+                sel = np.flatnonzero(f == k)
+                if len(sel):
+                    out[_idx(sel, dev), 0] = flat[k][_idx(s[sel], dev)].to(torch.float64)
+            return out
+
+        v = self.route(gather, dist, 1, dev)[:, 0]
+        d, m = self.dst[self.mine], self.meta[self.mine]
+        old = torch.empty(len(d), dtype=torch.float64, device=dev)
         for k in range(5):
             sel = np.flatnonzero((m & 7) == k)
             if len(sel):
-                old[idx(sel)] = flat[k][idx(d[sel])].to(torch.float64)
-        v = _finish(vals[idx(mine)], m, old)
+                old[_idx(sel, dev)] = flat[k][_idx(d[sel], dev)].to(torch.float64)
+        v = _finish(v, m, old)
         for k in range(5):
             sel = np.flatnonzero((m & 7) == k)
             if len(sel):
-                flat[k][idx(d[sel])] = v[idx(sel)].to(flat[k].dtype)
+                flat[k][_idx(d[sel], dev)] = v[_idx(sel, dev)].to(flat[k].dtype)
+
+
+class FaceSync(PanelSplit):
+    """Face ownership split across ranks (cs_sync_map_get(0)): 17 values an
+    entry, the owner's 16 one-sided contributions and its entropy flux."""
+
+    def __init__(self, dst, src, dk, sk, box: int, panel_rank, rank: int):
+        super().__init__(src, dst, box, panel_rank, rank)
+        self.dk, self.sk = np.asarray(dk), np.asarray(sk)
+
+    def exchange(self, fcon, EF, dist) -> None:
+        """fcon[d]: (16, 6 * box) torch tensors, EF[d]: (6 * box), d the
+        face direction; this rank's listed copies take their owners'
+        values (sides exchanged, entropy flux negated)."""
+        import torch
+
+        dev = EF[0].device
+
+        def gather(entries):
+            out = torch.empty((len(entries), 17), dtype=torch.float64, device=dev)
+            s, k = self.src[entries], self.sk[entries]
+            for d in range(len(fcon)):
+                sel = np.flatnonzero(k == d)
+                if len(sel):
+                    out[_idx(sel, dev), :16] = fcon[d][:, _idx(s[sel], dev)].T.to(torch.float64)
+                    out[_idx(sel, dev), 16] = EF[d][_idx(s[sel], dev)].to(torch.float64)
+            return out
+
+        v = self.route(gather, dist, 17, dev)
+        d, k = self.dst[self.mine], self.dk[self.mine]
+        for q in range(len(fcon)):
+            sel = np.flatnonzero(k == q)
+            if len(sel):
+                rows = v[_idx(sel, dev)]
+                fcon[q][:, _idx(d[sel], dev)] = torch.roll(rows[:, :16], 8, dims=1).T.to(fcon[q].dtype)
+                EF[q][_idx(d[sel], dev)] = (-rows[:, 16]).to(EF[q].dtype)
+
+
+class EdgeSync(PanelSplit):
+    """Edge ownership split across ranks (cs_sync_map_get(1))."""
+
+    def __init__(self, dst, src, dk, sk, sign, box: int, panel_rank, rank: int):
+        super().__init__(src, dst, box, panel_rank, rank)
+        self.dk, self.sk, self.sign = np.asarray(dk), np.asarray(sk), np.asarray(sign)
+
+    def exchange(self, Ef, dist) -> None:
+        """Ef[c]: (6 * box) torch tensors, c the EMF component; this rank's
+        listed copies take their owners' values times the sign."""
+        import torch
+
+        dev = Ef[0].device
+
+        def gather(entries):
+            out = torch.empty((len(entries), 1), dtype=torch.float64, device=dev)
+            s, k = self.src[entries], self.sk[entries]
+            for c in range(len(Ef)):
+                sel = np.flatnonzero(k == c)
+                if len(sel):
+                    out[_idx(sel, dev), 0] = Ef[c][_idx(s[sel], dev)].to(torch.float64)
+            return out
+
+        v = self.route(gather, dist, 1, dev)[:, 0]
+        v = v * torch.as_tensor(self.sign[self.mine], device=dev, dtype=torch.float64)
+        d, k = self.dst[self.mine], self.dk[self.mine]
+        for c in range(len(Ef)):
+            sel = np.flatnonzero(k == c)
+            if len(sel):
+                Ef[c][_idx(d[sel], dev)] = v[_idx(sel, dev)].to(Ef[c].dtype)

@@ -257,6 +257,21 @@ int cs_mask_get(cs_ctx* ctx, int32_t* host_out, size_t n);            /* imask_a
  * the entry count.  A panel split across ranks exchanges the entries whose
  * source and destination panels sit on different ranks. */
 int cs_fill_map_get(cs_ctx* ctx, int32_t* src, int32_t* dst, uint8_t* meta, int64_t* n);
+/* Host copy of the panel-edge ownership lists the stage applies unless
+ * CS_FLAG_NO_PANEL_SYNC is set (the single-device form of the reference's
+ * defect exchange, DRV:3200-3461 with 485update_defect_imex_rk.f): every
+ * copy of a face or edge that two or three panels compute takes the value
+ * of the copy on the lowest-numbered panel.  which = 0: faces on panel
+ * edges; dst[t] / src[t] are face offsets (panel * box + point) and
+ * dst_kind / src_kind their directions (0 x, 1 y), the copy taking the
+ * source's two one-sided flux contributions with the sides exchanged and
+ * the negated entropy flux (sign = -1).  which = 1: edges on panel
+ * boundaries; offsets as for faces, dst_kind / src_kind the EMF component
+ * (0 Ex, 1 Ey, 2 Ez) and sign the factor (+1 or -1, where the two panels
+ * run the edge in opposite directions).  No source is a destination.  Built
+ * from the host mesh; null arrays and *n as for cs_fill_map_get. */
+int cs_sync_map_get(cs_ctx* ctx, int32_t which, int32_t* dst, int32_t* src, int8_t* dst_kind, int8_t* src_kind,
+                    int8_t* sign, int64_t* n);
 int cs_stencil_get(cs_ctx* ctx, int32_t* host_out, size_t n);         /* istencil, [6][12][2][NJ][NI] */
 
 /* Geometry of one coarse zone cut with stride iscale out of sector isector

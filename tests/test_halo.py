@@ -1,8 +1,10 @@
-"""The ghost exchange as an explicit list (cs_fill_map_get) and its split
+"""The stage's two cross-panel exchanges as explicit lists and their split
 across ranks that each own whole panels (cubesphere_b200.halo), on the CPU:
-the list applied on the host reproduces the oracle's ghost fill, and ranks
-that hold only their own panels (gloo, 2 and 3 ranks) fill their ghost
-values from their peers exactly as the single-process fill does."""
+the ghost fill (cs_fill_map_get) and the panel-edge ownership of face
+fluxes and edge EMFs (cs_sync_map_get), each applied on the host, reproduce
+the oracle's; ranks that hold only their own panels (gloo, 2 and 3 ranks)
+fill their ghost values and owned copies from their peers exactly as the
+single-process application does."""
 import os
 import sys
 from pathlib import Path
@@ -12,7 +14,7 @@ import pytest
 import torch.multiprocessing as mp
 
 import cubesphere_b200 as cs
-from cubesphere_b200.halo import FIELDS, apply_fill_map
+from cubesphere_b200.halo import FIELDS, apply_edge_sync, apply_face_sync, apply_fill_map
 from oracle import Oracle
 
 ROOT = Path(__file__).resolve().parents[1]
@@ -45,6 +47,49 @@ def test_fill_map_reproduces_the_oracle_ghost_fill(name):
         assert np.array_equal(mine[k].reshape(-1)[d], ref[k].reshape(-1)[d]), k
 
 
+def _oracle_fluxes_and_emfs(pr, flags):
+    s = cs.Solve(**pr["params"], flags=flags)
+    s.mesh_build(device=False)
+    st = s.init_problem_host(**pr["init"])
+    o = Oracle(s)
+    o.put_state(st)
+    o.fill_ghosts()
+    o.limit_all_slopes_p12()
+    o.make_facial_fluxes()
+    o.make_edge_efields_p1()
+    return s, o.debug("entflux"), [o.debug(k) for k in ("Efx", "Efy", "Efz")]
+
+
+@pytest.mark.parametrize("name", ["shell16", "surface32"])
+def test_sync_maps_reproduce_the_oracle_ownership(name):
+    """The ownership lists applied on the host to the oracle's per-panel
+    values (CS_FLAG_NO_PANEL_SYNC) give its synchronised entropy fluxes and
+    edge EMFs bit for bit; no (offset, kind) pair is both a source and a
+    destination, so the lists need no ordering."""
+    pr = cs.preset(name)
+    s, ef_on, e_on = _oracle_fluxes_and_emfs(pr, 0)
+    _, ef_off, e_off = _oracle_fluxes_and_emfs(pr, cs.CS_FLAG_NO_PANEL_SYNC)
+    for which in (0, 1):
+        dst, src, dk, sk, sg = s.sync_map(which)
+        assert len(dst) > 0
+        d = set((dk.astype(np.int64) << 40 | dst).tolist())
+        assert len(d) == len(dst)
+        assert not d & set((sk.astype(np.int64) << 40 | src).tolist())
+    dst, src, dk, sk, sg = s.sync_map(0)
+    assert set(dk.tolist()) <= {0, 1} and (sg == -1).all()
+    EF = [a.reshape(-1).copy() for a in ef_off]
+    fcon = [np.zeros((16, EF[0].size)) for _ in range(3)]
+    apply_face_sync(fcon, EF, dst, src, dk, sk)
+    for q in range(3):
+        assert np.array_equal(EF[q], ef_on[q].reshape(-1)), q
+    dst, src, dk, sk, sg = s.sync_map(1)
+    assert set(sg.tolist()) == {-1, 1}
+    Ef = [a.reshape(-1).copy() for a in e_off]
+    apply_edge_sync(Ef, dst, src, dk, sk, sg)
+    for q in range(3):
+        assert np.array_equal(Ef[q], e_on[q].reshape(-1)), q
+
+
 def _rank(rank, world, port, panel_rank, q):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     sys.path.insert(0, str(ROOT))
@@ -52,7 +97,8 @@ def _rank(rank, world, port, panel_rank, q):
     import torch.distributed as dist
 
     import cubesphere_b200 as cs
-    from cubesphere_b200.halo import PanelSplit, apply_fill_map
+    from cubesphere_b200.halo import (EdgeSync, FaceSync, GhostExchange, apply_edge_sync, apply_face_sync,
+                                      apply_fill_map)
 
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
@@ -68,16 +114,46 @@ def _rank(rank, world, port, panel_rank, q):
         held = {k: torch.from_numpy(v.copy()) for k, v in st.items()}
         for v in held.values():
             v[:, other] = float("nan")  # this rank holds only its own panels
-        plan = PanelSplit(src, dst, meta, s.NI * s.NJ * s.NK, panel_rank, rank)
+        box = s.NI * s.NJ * s.NK
+        plan = GhostExchange(src, dst, meta, box, panel_rank, rank)
         plan.exchange(held, dist)
         ok = all(np.array_equal(held[k].numpy()[:, owned], want[k][:, owned]) for k in want)
-        q.put((rank, ok, plan.values_bytes(), sum(len(v) for v in plan.recv.values())))
+        sent, received = plan.values_bytes(), 8 * sum(len(v) for v in plan.recv.values())
+
+        # ownership copies of seeded face contributions and edge EMFs
+        rng = np.random.default_rng(7)
+        fcon = [rng.standard_normal((16, 6 * box)) for _ in range(3)]
+        EF = [rng.standard_normal(6 * box) for _ in range(3)]
+        Ef = [rng.standard_normal(6 * box) for _ in range(3)]
+        dst_f, src_f, dk_f, sk_f, _ = s.sync_map(0)
+        dst_e, src_e, dk_e, sk_e, sg_e = s.sync_map(1)
+        w_fcon, w_EF, w_Ef = [a.copy() for a in fcon], [a.copy() for a in EF], [a.copy() for a in Ef]
+        apply_face_sync(w_fcon, w_EF, dst_f, src_f, dk_f, sk_f)
+        apply_edge_sync(w_Ef, dst_e, src_e, dk_e, sk_e, sg_e)
+
+        def hold(a):
+            t = torch.from_numpy(a.copy())
+            v = t.view(-1, 6, box)
+            v[:, other] = float("nan")
+            return t
+
+        h_fcon, h_EF, h_Ef = [hold(a) for a in fcon], [hold(a) for a in EF], [hold(a) for a in Ef]
+        fs = FaceSync(dst_f, src_f, dk_f, sk_f, box, panel_rank, rank)
+        fs.exchange(h_fcon, h_EF, dist)
+        es = EdgeSync(dst_e, src_e, dk_e, sk_e, sg_e, box, panel_rank, rank)
+        es.exchange(h_Ef, dist)
+        mine = lambda a: a.reshape(-1, 6, box)[:, owned]
+        for got, ref in zip(h_fcon + h_EF + h_Ef, w_fcon + w_EF + w_Ef):
+            ok = ok and np.array_equal(mine(got.numpy()), mine(ref))
+        sent += fs.values_bytes(17) + es.values_bytes()
+        received += 8 * (17 * sum(len(v) for v in fs.recv.values()) + sum(len(v) for v in es.recv.values()))
+        q.put((rank, ok, sent, received))
     finally:
         dist.destroy_process_group()
 
 
 @pytest.mark.parametrize("panel_rank", [[0, 0, 0, 1, 1, 1], [0, 0, 1, 1, 2, 2]])
-def test_panel_split_exchange_matches_the_single_process_fill(panel_rank):
+def test_panel_split_exchanges_match_the_single_process_application(panel_rank):
     world = max(panel_rank) + 1
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
@@ -93,4 +169,4 @@ def test_panel_split_exchange_matches_the_single_process_fill(panel_rank):
         assert ok, rank
         assert sent > 0 and received > 0, rank
     # every value one rank sends, another receives
-    assert sum(o[2] for o in out) == 8 * sum(o[3] for o in out)
+    assert sum(o[2] for o in out) == sum(o[3] for o in out)
