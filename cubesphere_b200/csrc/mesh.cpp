@@ -659,6 +659,9 @@ std::string build_from_unit_vertices(const cs_params& p, const std::vector<V3> s
   const Box b(p.ntp, p.nr, p.nghost);
   g.box = b;
   const size_t S = b.size();
+  // The fields hold ≈126 words a point (6 GB at 6 x 128^2 x 64): their first
+  // touch (page faults and zeroing) runs one field a thread.
+#pragma omp parallel for schedule(dynamic, 1)
   for (int f = 0; f < CS_G_NFIELDS; ++f) g.f[f].assign((size_t)geom_ncomp(f) * NPANEL * S, 0.0);
   g.mask.assign((size_t)NPANEL * S, 0);
   g.stencil.assign((size_t)NPANEL * 24 * b.plane(), 0);
