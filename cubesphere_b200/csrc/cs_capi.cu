@@ -134,16 +134,6 @@ struct MapEntry {
   uint8_t meta;
 };
 
-// The order the device applies the map in: by destination field, then by
-// destination offset (all sources are read before any write, so the order
-// changes no value; it keeps the scatter's writes coalesced).
-void sort_fill_map(std::vector<MapEntry>& map) {
-  std::sort(map.begin(), map.end(), [](const MapEntry& a, const MapEntry& b2) {
-    if ((a.meta & 7) != (b2.meta & 7)) return (a.meta & 7) < (b2.meta & 7);
-    return a.dst < b2.dst;
-  });
-}
-
 std::string build_fill_map(const Solve& sv, std::vector<MapEntry>& out) {
   const GeomHost& g = sv.mesh->host;
   const Box& b = g.box;
@@ -243,7 +233,16 @@ std::string build_fill_map(const Solve& sv, std::vector<MapEntry>& out) {
         for (int i = 1 - G; i <= N + G; ++i) emit(4, 4, pn, i, j, k, up, 2 * N + 1 - j, i, k, false, false);
   }
   if (!err.empty()) return err;
-  out.swap(e);
+  // The entries in the order the device applies them: by destination field,
+  // then by destination offset (all sources are read before any write, so
+  // the order changes no value; it keeps the scatter's writes coalesced).
+  // Each (field, point) has one slot, so a scan of the slots gives the order.
+  out.clear();
+  out.reserve(e.size());
+  for (int f = 0; f < 5; ++f)
+    for (int c = 0; c < (f == 0 ? NVAR : 1); ++c)
+      for (long long d = 0; d < S6; ++d)
+        if (slot[f][(size_t)d] >= 0) out.push_back(e[(size_t)slot[f][(size_t)d] + c]);
   return "";
 }
 
@@ -558,7 +557,6 @@ int mesh_upload(Solve& sv, MeshRes& m) {
   std::vector<MapEntry> map;
   std::string why = build_fill_map(sv, map);
   if (!why.empty()) return fail(sv, CS_ERR_ARG, why);
-  sort_fill_map(map);
   const size_t n = map.size();
   std::vector<int32_t> hs(n), hd(n);
   std::vector<uint8_t> hm(n);
@@ -1225,7 +1223,6 @@ int cs_fill_map_get(cs_ctx* ctx, int32_t* src, int32_t* dst, uint8_t* meta, int6
   std::vector<cs::MapEntry> map;
   const std::string why = cs::build_fill_map(sv, map);
   if (!why.empty()) return cs::fail(sv, CS_ERR_ARG, why);
-  cs::sort_fill_map(map);
   if (src || dst || meta) {
     if (!src || !dst || !meta) return cs::fail(sv, CS_ERR_ARG, "src, dst and meta are all given or all null");
     if (*n != (int64_t)map.size()) return cs::fail(sv, CS_ERR_ARG, "fill map buffer size mismatch");
