@@ -71,15 +71,16 @@ def apply_fill_map(st: dict, src, dst, meta) -> None:
 
 
 def apply_face_sync(fcon, EF, dst, src, dk, sk) -> None:
-    """Face ownership on host arrays, in place: fcon[d] (16, 6 * box) holds
-    a direction's two one-sided contributions (components 0-7 and 8-15) and
-    EF[d] (6 * box) its entropy flux; each listed copy takes its owner's
-    contributions with the sides exchanged and the negated entropy flux."""
+    """Face ownership on host arrays, in place: fcon[d] (2m, 6 * box) holds
+    a direction's two one-sided contributions (rows 0..m-1 and m..2m-1; m = 8
+    on the device) and EF[d] (6 * box) its entropy flux; each listed copy
+    takes its owner's contributions with the sides exchanged and the negated
+    entropy flux."""
     for d in range(len(fcon)):
         for s in range(len(fcon)):
             sel = np.flatnonzero((dk == d) & (sk == s))
             if len(sel):
-                fcon[d][:, dst[sel]] = np.roll(fcon[s][:, src[sel]], 8, axis=0)
+                fcon[d][:, dst[sel]] = np.roll(fcon[s][:, src[sel]], fcon[s].shape[0] // 2, axis=0)
                 EF[d][dst[sel]] = -EF[s][src[sel]]
 
 
@@ -189,39 +190,44 @@ class GhostExchange(PanelSplit):
 
 
 class FaceSync(PanelSplit):
-    """Face ownership split across ranks (cs_sync_map_get(0)): 17 values an
-    entry, the owner's 16 one-sided contributions and its entropy flux."""
+    """Face ownership split across ranks (cs_sync_map_get(0)): ncomp + 1
+    values an entry, the owner's one-sided contributions (ncomp / 2 a side:
+    8 on the device, whose face arrays hold one value a variable and side)
+    and its entropy flux."""
 
-    def __init__(self, dst, src, dk, sk, box: int, panel_rank, rank: int):
+    def __init__(self, dst, src, dk, sk, box: int, panel_rank, rank: int, ncomp: int = 16):
         super().__init__(src, dst, box, panel_rank, rank)
         self.dk, self.sk = np.asarray(dk), np.asarray(sk)
+        self.ncomp = ncomp
 
     def exchange(self, fcon, EF, dist) -> None:
-        """fcon[d]: (16, 6 * box) torch tensors, EF[d]: (6 * box), d the
-        face direction; this rank's listed copies take their owners'
-        values (sides exchanged, entropy flux negated)."""
+        """fcon[d]: (ncomp, 6 * box) torch tensors (one side's rows, then the
+        other's), EF[d]: (6 * box), d the face direction; this rank's listed
+        copies take their owners' values (sides exchanged, entropy flux
+        negated)."""
         import torch
 
         dev = EF[0].device
+        m = self.ncomp
 
         def gather(entries):
-            out = torch.empty((len(entries), 17), dtype=torch.float64, device=dev)
+            out = torch.empty((len(entries), m + 1), dtype=torch.float64, device=dev)
             s, k = self.src[entries], self.sk[entries]
             for d in range(len(fcon)):
                 sel = np.flatnonzero(k == d)
                 if len(sel):
-                    out[_idx(sel, dev), :16] = fcon[d][:, _idx(s[sel], dev)].T.to(torch.float64)
-                    out[_idx(sel, dev), 16] = EF[d][_idx(s[sel], dev)].to(torch.float64)
+                    out[_idx(sel, dev), :m] = fcon[d][:, _idx(s[sel], dev)].T.to(torch.float64)
+                    out[_idx(sel, dev), m] = EF[d][_idx(s[sel], dev)].to(torch.float64)
             return out
 
-        v = self.route(gather, dist, 17, dev)
+        v = self.route(gather, dist, m + 1, dev)
         d, k = self.dst[self.mine], self.dk[self.mine]
         for q in range(len(fcon)):
             sel = np.flatnonzero(k == q)
             if len(sel):
                 rows = v[_idx(sel, dev)]
-                fcon[q][:, _idx(d[sel], dev)] = torch.roll(rows[:, :16], 8, dims=1).T.to(fcon[q].dtype)
-                EF[q][_idx(d[sel], dev)] = (-rows[:, 16]).to(EF[q].dtype)
+                fcon[q][:, _idx(d[sel], dev)] = torch.roll(rows[:, :m], m // 2, dims=1).T.to(fcon[q].dtype)
+                EF[q][_idx(d[sel], dev)] = (-rows[:, m]).to(EF[q].dtype)
 
 
 class EdgeSync(PanelSplit):

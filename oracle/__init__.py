@@ -46,6 +46,9 @@ def load() -> ctypes.CDLL:
         "oracle_get_mask_stencil": ([P, ip, ip], None),
         "oracle_pointwise": ([P, ctypes.c_int, ctypes.c_int, dp, dp], ctypes.c_int),
         "oracle_limit_minmax": ([P, dp, dp], ctypes.c_int),
+        "oracle_stage_phase": ([P, ctypes.c_int, ctypes.c_int, D, ctypes.c_uint], ctypes.c_int),
+        "oracle_evaluate_timestep_panels": ([P, D, ctypes.c_uint], D),
+        "oracle_stage_array": ([P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)], dp),
     }
     for n in ("oracle_fill_ghosts", "oracle_limit_all_slopes_p12", "oracle_make_facial_fluxes",
               "oracle_make_edge_efields", "oracle_build_non_stiff_sources", "oracle_cleanup"):
@@ -215,6 +218,26 @@ class Oracle:
 
     def step(self, dtcur: float) -> float:
         return self.lib.oracle_step(self.h, dtcur)
+
+    # A stage in phases over a set of panels (bit p of `panels` = panel p),
+    # for runs in which ranks hold some of the panels and exchange between
+    # the phases: 0 radial padding, 1 reconstruction + face fluxes, 2 flux
+    # scatter + edge EMFs, 3 the rest of the stage.
+    def stage_phase(self, phase: int, irk: int = 1, dtcur: float = 0.0, panels: int = 63):
+        assert self.lib.oracle_stage_phase(self.h, phase, irk, dtcur, panels) == 0
+
+    def evaluate_timestep_panels(self, dtcur: float, panels: int) -> float:
+        return self.lib.oracle_evaluate_timestep_panels(self.h, dtcur, panels)
+
+    def stage_array(self, which: str, d: int) -> np.ndarray:
+        """In-place view of a stage array: "cL" / "cR" (direction d's one-sided
+        face contributions, (5 * 8, 6 * box)), "EF" (entropy flux) or "Ef"
+        (EMF component d), (6 * box)."""
+        n = ctypes.c_size_t(0)
+        ptr = self.lib.oracle_stage_array(self.h, ("cL", "cR", "EF", "Ef").index(which), d, ctypes.byref(n))
+        assert ptr
+        a = np.ctypeslib.as_array(ptr, shape=(n.value,))
+        return a.reshape(40, -1) if which in ("cL", "cR") else a
 
 
 def twod_rs_ez_4state(S_R, S_L, S_U, S_D, cos_t, sin_t, Ez_RU, Ez_LU, Ez_LD, Ez_RD, Bneta_U, Bneta_D, By_R, By_L):

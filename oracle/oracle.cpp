@@ -98,6 +98,8 @@ static inline double poly10(const double* v, const double* c, double x, double y
          v[6] * (z * z - c[6]) + v[7] * (x * y - c[7]) + v[8] * (y * z - c[8]) + v[9] * (x * z - c[9]);
 }
 
+void pad_radial(Ctx& c, int pn);
+
 // ------------------------------------------------------------------
 // Ghost fill across panel edges plus the radial outflow padding.
 // Follows FETCH_BUFFERS_FILL_IN_UX / _UY / _UY_TOP
@@ -228,44 +230,48 @@ void fill_ghosts(Ctx& c) {
       for (int j = N + 1; j <= N + G; ++j)
         for (int i = 1 - G; i <= N + G; ++i) c.a(c.Bzf, 0, pn, i, j, k) = src(Bz, 0, up, 2 * N + 1 - j, i, k);
   }
-  // ---- radial padding
-  for (int pn = 0; pn < 6; ++pn) {
-    for (int kk = 1; kk <= G; ++kk)
-      for (int j = 1 - G; j <= N + G; ++j)
-        for (int i = 1 - G; i <= N + G; ++i) {
-          if (c.m(pn, i, j) != 1) continue;
-          if (c.p.bc_lower == 2) {
-            int l = 1 - kk, r = 1;
-            for (int q = 0; q < NV; ++q) c.a(c.U, q, pn, i, j, l) = c.a(c.U, q, pn, i, j, r);
-            c.a(c.Bxf, 0, pn, i, j, l) = c.a(c.Bxf, 0, pn, i, j, r);
-            c.a(c.Bxf, 0, pn, i - 1, j, l) = c.a(c.Bxf, 0, pn, i - 1, j, r);
-            c.a(c.Byf, 0, pn, i, j, l) = c.a(c.Byf, 0, pn, i, j, r);
-            c.a(c.Byf, 0, pn, i, j - 1, l) = c.a(c.Byf, 0, pn, i, j - 1, r);
-            c.a(c.Bzf, 0, pn, i, j, l - 1) = c.a(c.Bzf, 0, pn, i, j, r - 1);
-          }
+  for (int pn = 0; pn < 6; ++pn) pad_radial(c, pn);
+}
+
+// PAD_BOUNDARY_R of one panel (826pad_boundary_r.f:190-420, outflow code 2):
+// the radial ghost layers of the active columns from the first / last zone.
+void pad_radial(Ctx& c, int pn) {
+  const int N = c.N, G = c.G, nr = c.nr;
+  for (int kk = 1; kk <= G; ++kk)
+    for (int j = 1 - G; j <= N + G; ++j)
+      for (int i = 1 - G; i <= N + G; ++i) {
+        if (c.m(pn, i, j) != 1) continue;
+        if (c.p.bc_lower == 2) {
+          int l = 1 - kk, r = 1;
+          for (int q = 0; q < NV; ++q) c.a(c.U, q, pn, i, j, l) = c.a(c.U, q, pn, i, j, r);
+          c.a(c.Bxf, 0, pn, i, j, l) = c.a(c.Bxf, 0, pn, i, j, r);
+          c.a(c.Bxf, 0, pn, i - 1, j, l) = c.a(c.Bxf, 0, pn, i - 1, j, r);
+          c.a(c.Byf, 0, pn, i, j, l) = c.a(c.Byf, 0, pn, i, j, r);
+          c.a(c.Byf, 0, pn, i, j - 1, l) = c.a(c.Byf, 0, pn, i, j - 1, r);
+          c.a(c.Bzf, 0, pn, i, j, l - 1) = c.a(c.Bzf, 0, pn, i, j, r - 1);
         }
-    for (int kk = 1; kk <= G; ++kk)
-      for (int j = 1 - G; j <= N + G; ++j)
-        for (int i = 1 - G; i <= N + G; ++i) {
-          if (c.m(pn, i, j) != 1) continue;
-          if (c.p.bc_upper == 2) {
-            int l = nr + kk, r = nr;
-            for (int q = 0; q < NV; ++q)
-              c.a(c.U, q, pn, i, j, l) =
-                  c.a(c.U, q, pn, i, j, r) * c.geo(V_VOL, 0, pn, i, j, r) / c.geo(V_VOL, 0, pn, i, j, l);
-            c.a(c.Bzf, 0, pn, i, j, l) =
-                c.a(c.Bzf, 0, pn, i, j, r) * c.geo(ZF_AREA, 0, pn, i, j, r) / c.geo(ZF_AREA, 0, pn, i, j, l);
-            c.a(c.Bxf, 0, pn, i, j, l) =
-                c.a(c.Bxf, 0, pn, i, j, r) * c.geo(XF_AREA, 0, pn, i, j, r) / c.geo(XF_AREA, 0, pn, i, j, l);
-            c.a(c.Byf, 0, pn, i, j, l) =
-                c.a(c.Byf, 0, pn, i, j, r) * c.geo(YF_AREA, 0, pn, i, j, r) / c.geo(YF_AREA, 0, pn, i, j, l);
-            c.a(c.Bxf, 0, pn, i - 1, j, l) = c.a(c.Bxf, 0, pn, i - 1, j, r) * c.geo(XF_AREA, 0, pn, i - 1, j, r) /
-                                              c.geo(XF_AREA, 0, pn, i - 1, j, l);
-            c.a(c.Byf, 0, pn, i, j - 1, l) = c.a(c.Byf, 0, pn, i, j - 1, r) * c.geo(YF_AREA, 0, pn, i, j - 1, r) /
-                                              c.geo(YF_AREA, 0, pn, i, j - 1, l);
-          }
+      }
+  for (int kk = 1; kk <= G; ++kk)
+    for (int j = 1 - G; j <= N + G; ++j)
+      for (int i = 1 - G; i <= N + G; ++i) {
+        if (c.m(pn, i, j) != 1) continue;
+        if (c.p.bc_upper == 2) {
+          int l = nr + kk, r = nr;
+          for (int q = 0; q < NV; ++q)
+            c.a(c.U, q, pn, i, j, l) =
+                c.a(c.U, q, pn, i, j, r) * c.geo(V_VOL, 0, pn, i, j, r) / c.geo(V_VOL, 0, pn, i, j, l);
+          c.a(c.Bzf, 0, pn, i, j, l) =
+              c.a(c.Bzf, 0, pn, i, j, r) * c.geo(ZF_AREA, 0, pn, i, j, r) / c.geo(ZF_AREA, 0, pn, i, j, l);
+          c.a(c.Bxf, 0, pn, i, j, l) =
+              c.a(c.Bxf, 0, pn, i, j, r) * c.geo(XF_AREA, 0, pn, i, j, r) / c.geo(XF_AREA, 0, pn, i, j, l);
+          c.a(c.Byf, 0, pn, i, j, l) =
+              c.a(c.Byf, 0, pn, i, j, r) * c.geo(YF_AREA, 0, pn, i, j, r) / c.geo(YF_AREA, 0, pn, i, j, l);
+          c.a(c.Bxf, 0, pn, i - 1, j, l) = c.a(c.Bxf, 0, pn, i - 1, j, r) * c.geo(XF_AREA, 0, pn, i - 1, j, r) /
+                                            c.geo(XF_AREA, 0, pn, i - 1, j, l);
+          c.a(c.Byf, 0, pn, i, j - 1, l) = c.a(c.Byf, 0, pn, i, j - 1, r) * c.geo(YF_AREA, 0, pn, i, j - 1, r) /
+                                            c.geo(YF_AREA, 0, pn, i, j - 1, l);
         }
-  }
+      }
 }
 
 // Tri-corner face-B synchronisation at the four panel corners
@@ -1998,7 +2004,7 @@ void cleanup(Ctx& c, int pn) {
 }
 
 // EVALUATE_TIMESTEP (400riemann_integrate/490evaluate_timestep.f:121-286), all panels.
-double evaluate_timestep(Ctx& c, double dtcur) {
+double evaluate_timestep(Ctx& c, double dtcur, unsigned panels = 63u) {
   double dt = 1.1 * dtcur;
   const int N = c.N, nr = c.nr;
 #pragma omp parallel for collapse(3) schedule(static) reduction(min : dt)
@@ -2006,7 +2012,7 @@ double evaluate_timestep(Ctx& c, double dtcur) {
     for (int k = 1; k <= nr; ++k)
       for (int j = 1; j <= N; ++j)
         for (int i = 1; i <= N; ++i) {
-          if (c.m(pn, i, j) == 0) continue;
+          if (((panels >> pn) & 1u) == 0 || c.m(pn, i, j) == 0) continue;
           double Up[NV], Vp[NV];
           for (int q = 0; q < NV; ++q) Up[q] = c.a(c.U, q, pn, i, j, k);
           double en = c.a(c.ent, 0, pn, i, j, k);
@@ -2072,24 +2078,37 @@ static void add_gravity(Ctx& c, int pn, double cc) {
       }
 }
 
-// One ARS(2,2,2) stage: fluxes, entropy transport and CT explicit, gravity
-// implicit; gamma = 1 - 1/sqrt(2), delta = 1 - 1/(2 gamma).
+static bool owns(unsigned panels, int pn) { return (panels >> pn) & 1u; }
+
+// A stage in phases over a set of panels (bit p of `panels` = panel p), so
+// that ranks holding some of the panels can run them with the exchanges
+// between: the ghost fill before stage_fluxes, the face-flux ownership
+// before stage_emfs, the EMF ownership before stage_finish.  Reconstruction
+// and face fluxes:
+void stage_fluxes(Ctx& c, unsigned panels) {
+  for (int pn = 0; pn < 6; ++pn)
+    if (owns(panels, pn)) {
+      limit_all_slopes_p12(c, pn);
+      make_facial_fluxes(c, pn);
+    }
+}
+
+// The face-flux scatter into the zones and the edge EMFs.
+void stage_emfs(Ctx& c, unsigned panels) {
+  for (int pn = 0; pn < 6; ++pn)
+    if (owns(panels, pn)) {
+      scatter_facial_fluxes(c, pn);
+      make_edge_efields(c, pn);
+    }
+}
+
+// The rest of one ARS(2,2,2) stage: fluxes, entropy transport and CT
+// explicit, gravity implicit; gamma = 1 - 1/sqrt(2), delta = 1 - 1/(2 gamma).
 //   stage 1: U* = U^n + gamma dt F(U^n);  U2 = U* + gamma dt S(U2)
 //   stage 2: U* = U^n + delta dt F(U^n) + (1-delta) dt F(U2) + (1-gamma) dt S(U2)
 //            U^{n+1} = U* + gamma dt S(U^{n+1})
-static void stage_imex(Ctx& c, int irk, double dtcur) {
+static void stage_imex_finish(Ctx& c, int irk, double dtcur, unsigned panels) {
   const double gam = 1.0 - 1.0 / std::sqrt(2.0), del = 1.0 - 1.0 / (2.0 * gam);
-  fill_ghosts(c);
-  for (int pn = 0; pn < 6; ++pn) {
-    limit_all_slopes_p12(c, pn);
-    make_facial_fluxes(c, pn);
-  }
-  sync_facial_fluxes(c);
-  for (int pn = 0; pn < 6; ++pn) {
-    scatter_facial_fluxes(c, pn);
-    make_edge_efields(c, pn);
-  }
-  sync_edge_efields(c);
   if (irk == 1) {
     c.U0 = c.U;
     std::memcpy(c.ent0.data(), c.ent.data(), 6 * c.S * sizeof(double));
@@ -2099,9 +2118,11 @@ static void stage_imex(Ctx& c, int irk, double dtcur) {
     c.K1 = c.dUdt;
     c.EFx1 = c.EFx; c.EFy1 = c.EFy; c.EFz1 = c.EFz;
     c.Efx1 = c.Efx; c.Efy1 = c.Efy; c.Efz1 = c.Efz;
-    for (int pn = 0; pn < 6; ++pn) update(c, pn, gam * dtcur);
+    for (int pn = 0; pn < 6; ++pn)
+      if (owns(panels, pn)) update(c, pn, gam * dtcur);
   } else {
-    for (int pn = 0; pn < 6; ++pn) add_gravity(c, pn, (1.0 - gam) / (1.0 - del));
+    for (int pn = 0; pn < 6; ++pn)
+      if (owns(panels, pn)) add_gravity(c, pn, (1.0 - gam) / (1.0 - del));
     c.U = c.U0;
     std::memcpy(c.ent.data(), c.ent0.data(), 6 * c.S * sizeof(double));
     c.Bxf = c.Bxf0;
@@ -2113,26 +2134,22 @@ static void stage_imex(Ctx& c, int irk, double dtcur) {
       std::swap(c.Efx, c.Efx1); std::swap(c.Efy, c.Efy1); std::swap(c.Efz, c.Efz1);
     };
     swap1();
-    for (int pn = 0; pn < 6; ++pn) update(c, pn, del * dtcur);
+    for (int pn = 0; pn < 6; ++pn)
+      if (owns(panels, pn)) update(c, pn, del * dtcur);
     swap1();
-    for (int pn = 0; pn < 6; ++pn) update(c, pn, (1.0 - del) * dtcur);
+    for (int pn = 0; pn < 6; ++pn)
+      if (owns(panels, pn)) update(c, pn, (1.0 - del) * dtcur);
   }
-  for (int pn = 0; pn < 6; ++pn) {
-    gravity_implicit(c, pn, gam * dtcur);
-    cleanup(c, pn);
-  }
+  for (int pn = 0; pn < 6; ++pn)
+    if (owns(panels, pn)) {
+      gravity_implicit(c, pn, gam * dtcur);
+      cleanup(c, pn);
+    }
 }
 
-// One RK stage in the driver's order (1000riemann_geomesh_cs_mhd.f:1746-2887):
-// ghost fill, then per panel reconstruction, fluxes, EMFs, sources, the
-// stage combine, the update and the clean-up, with the panel-edge
-// ownership applied to the fluxes and EMFs before they are used.
-void stage(Ctx& c, int irk, double dtcur) {
-  if (c.p.rk_scheme == 4) {
-    stage_imex(c, irk, dtcur);
-    return;
-  }
-  fill_ghosts(c);
+// The rest of an RK2 / SSP-RK3 stage: sources, the stage combine, the
+// update and the clean-up.
+static void stage_rk_finish(Ctx& c, int irk, double dtcur, unsigned panels) {
   double dtmove = dtcur;
   double a0 = 0.0;  // weight of the saved state in the combine
   int scheme = c.p.rk_scheme;
@@ -2142,20 +2159,8 @@ void stage(Ctx& c, int irk, double dtcur) {
     if (irk == 2) { a0 = 0.75; dtmove = 0.25 * dtcur; }
     if (irk == 3) { a0 = 1.0 / 3.0; dtmove = (2.0 / 3.0) * dtcur; }
   }
-  // Panels are independent within a stage (each reads only its own,
-  // ghost-filled arrays); the zone loops inside every routine run on all
-  // host threads.
   for (int pn = 0; pn < 6; ++pn) {
-    limit_all_slopes_p12(c, pn);
-    make_facial_fluxes(c, pn);
-  }
-  sync_facial_fluxes(c);
-  for (int pn = 0; pn < 6; ++pn) {
-    scatter_facial_fluxes(c, pn);
-    make_edge_efields(c, pn);
-  }
-  sync_edge_efields(c);
-  for (int pn = 0; pn < 6; ++pn) {
+    if (!owns(panels, pn)) continue;
     build_non_stiff_sources(c, pn);
     const size_t S = c.S;
     if (irk == 1) {
@@ -2183,6 +2188,29 @@ void stage(Ctx& c, int irk, double dtcur) {
     update(c, pn, dtmove);
     cleanup(c, pn);
   }
+}
+
+void stage_finish(Ctx& c, int irk, double dtcur, unsigned panels) {
+  if (c.p.rk_scheme == 4)
+    stage_imex_finish(c, irk, dtcur, panels);
+  else
+    stage_rk_finish(c, irk, dtcur, panels);
+}
+
+// One RK stage in the driver's order (1000riemann_geomesh_cs_mhd.f:1746-2887):
+// ghost fill, then per panel reconstruction, fluxes, EMFs, sources, the
+// stage combine, the update and the clean-up, with the panel-edge
+// ownership applied to the fluxes and EMFs before they are used.  Panels
+// are independent between the exchanges (each reads only its own,
+// ghost-filled arrays); the zone loops inside every routine run on all host
+// threads.
+void stage(Ctx& c, int irk, double dtcur) {
+  fill_ghosts(c);
+  stage_fluxes(c, 63u);
+  sync_facial_fluxes(c);
+  stage_emfs(c, 63u);
+  sync_edge_efields(c);
+  stage_finish(c, irk, dtcur, 63u);
 }
 
 }  // namespace oracle
@@ -2374,6 +2402,42 @@ void oracle_cleanup(void* h) {
 }
 double oracle_evaluate_timestep(void* h, double dtcur) { return evaluate_timestep(*(Ctx*)h, dtcur); }
 void oracle_stage(void* h, int irk, double dtcur) { stage(*(Ctx*)h, irk, dtcur); }
+// One phase of a stage over the panels in the bit set `panels`: 0 the radial
+// padding (after the ghost fill), 1 reconstruction and face fluxes, 2 the
+// flux scatter and the edge EMFs, 3 the rest of the stage; the exchanges go
+// between them (pad_radial / stage_fluxes / stage_emfs / stage_finish).
+int oracle_stage_phase(void* h, int phase, int irk, double dtcur, unsigned panels) {
+  Ctx& c = *(Ctx*)h;
+  switch (phase) {
+    case 0:
+      for (int pn = 0; pn < 6; ++pn)
+        if ((panels >> pn) & 1u) pad_radial(c, pn);
+      return 0;
+    case 1: stage_fluxes(c, panels); return 0;
+    case 2: stage_emfs(c, panels); return 0;
+    case 3: stage_finish(c, irk, dtcur, panels); return 0;
+    default: return 1;
+  }
+}
+double oracle_evaluate_timestep_panels(void* h, double dtcur, unsigned panels) {
+  return evaluate_timestep(*(Ctx*)h, dtcur, panels);
+}
+// The stage arrays the panel-edge ownership acts on, in place: which 0 / 1
+// the two one-sided face contributions cL / cR of direction `dir` (5
+// quadrature points x NV per face, [point * NV + var][panel][box]), 2 the
+// entropy flux of direction `dir`, 3 EMF component `dir`.  Null for any
+// other request; *n is the array's length.
+double* oracle_stage_array(void* h, int which, int dir, size_t* n) {
+  Ctx& c = *(Ctx*)h;
+  if (dir < 0 || dir > 2) return nullptr;
+  std::vector<double>* EF[3] = {&c.EFx, &c.EFy, &c.EFz};
+  std::vector<double>* Ef[3] = {&c.Efx, &c.Efy, &c.Efz};
+  std::vector<double>* v = which == 0 ? &c.cL[dir] : which == 1 ? &c.cR[dir] : which == 2 ? EF[dir]
+                         : which == 3 ? Ef[dir] : nullptr;
+  if (!v) return nullptr;
+  *n = v->size();
+  return v->data();
+}
 // One full time step; returns the next dt (min over panels, grown at most 10%).
 double oracle_step(void* h, double dtcur) {
   Ctx* c = (Ctx*)h;

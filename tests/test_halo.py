@@ -170,3 +170,99 @@ def test_panel_split_exchanges_match_the_single_process_application(panel_rank):
         assert sent > 0 and received > 0, rank
     # every value one rank sends, another receives
     assert sum(o[2] for o in out) == sum(o[3] for o in out)
+
+
+def _sharded_rank(rank, world, port, name, panel_rank, nsteps, q):
+    """Whole steps of the oracle on a rank that holds only its own panels:
+    each stage runs over them alone, with the ghost fill, the face-flux and
+    the EMF ownership exchanged between its phases and the time step's
+    minimum all-reduced; the single-process oracle runs beside it."""
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), OMP_NUM_THREADS="2")
+    sys.path.insert(0, str(ROOT))
+    import torch
+    import torch.distributed as dist
+
+    import cubesphere_b200 as cs
+    from cubesphere_b200.halo import EdgeSync, FaceSync, GhostExchange
+    from oracle import Oracle
+
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        pr = cs.preset(name)
+        s = cs.Solve(**pr["params"])
+        s.mesh_build(device=False)
+        st = s.init_problem_host(**pr["init"])
+        box = s.NI * s.NJ * s.NK
+        owned = [p for p in range(6) if panel_rank[p] == rank]
+        other = [p for p in range(6) if panel_rank[p] != rank]
+        mask = sum(1 << p for p in owned)
+        fill = GhostExchange(*s.fill_map(), box, panel_rank, rank)
+        dst, src, dk, sk, _ = s.sync_map(0)
+        face = FaceSync(dst, src, dk, sk, box, panel_rank, rank, ncomp=80)
+        edge = EdgeSync(*s.sync_map(1), box, panel_rank, rank)
+
+        ref = Oracle(s)
+        ref.put_state(st)
+        dt_ref = ref.evaluate_timestep(1e30)
+        o = Oracle(s)
+        held = {k: v.copy() for k, v in st.items()}
+        for v in held.values():
+            v[:, other] = np.nan
+        o.put_state(held)
+
+        def all_min(x):
+            t = torch.tensor([x], dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MIN)
+            return float(t[0])
+
+        dt = all_min(o.evaluate_timestep_panels(1e30, mask))
+        ok = dt == dt_ref
+        nst = 3 if s.params.rk_scheme == cs.CS_SSPRK3 else 2
+        for _ in range(nsteps):
+            for irk in range(1, nst + 1):
+                cur = o.get_state()
+                fill.exchange({k: torch.from_numpy(v) for k, v in cur.items()}, dist)
+                o.put_state(cur)
+                o.stage_phase(0, panels=mask)
+                o.stage_phase(1, panels=mask)
+                cL = [o.stage_array("cL", d) for d in range(2)]
+                cR = [o.stage_array("cR", d) for d in range(2)]
+                fcon = [torch.from_numpy(np.concatenate([cL[d], cR[d]])) for d in range(2)]
+                face.exchange(fcon, [torch.from_numpy(o.stage_array("EF", d)) for d in range(2)], dist)
+                for d in range(2):
+                    cL[d][:] = fcon[d][:40].numpy()
+                    cR[d][:] = fcon[d][40:].numpy()
+                o.stage_phase(2, panels=mask)
+                edge.exchange([torch.from_numpy(o.stage_array("Ef", c)) for c in range(3)], dist)
+                o.stage_phase(3, irk, dt, panels=mask)
+            dt = all_min(o.evaluate_timestep_panels(dt, mask))
+            dt_ref = ref.step(dt_ref)
+            ok = ok and dt == dt_ref
+        got, want = o.get_state(), ref.get_state()
+        for k in want:
+            ok = ok and np.array_equal(got[k][:, owned], want[k][:, owned])
+        q.put((rank, ok, dt, dt_ref))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("name,panel_rank", [("shell16", [0, 0, 0, 1, 1, 1]), ("surface32", [0, 0, 1, 1, 2, 2])])
+def test_panel_sharded_steps_match_the_single_process_solve(name, panel_rank):
+    """The two exchange lists (plus the time step's all-reduce) are all a
+    panel-sharded stage needs: ranks that hold only their own panels and run
+    every stage phase over them alone end two whole steps (IMEX-RK2 with
+    gravity on shell16, SSP-RK3 on surface32) with the single-process
+    oracle's state on their panels and its time step, bit for bit."""
+    world = max(panel_rank) + 1
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = 29500 + os.getpid() % 1000 + 7 * world
+    procs = [ctx.Process(target=_sharded_rank, args=(r, world, port, name, panel_rank, 2, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = sorted(q.get(timeout=600) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, ok, dt, dt_ref in out:
+        assert ok, (rank, dt, dt_ref)
