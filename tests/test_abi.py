@@ -65,6 +65,38 @@ def test_geometry_getter_checks_buffer_size():
     assert rc == 1
 
 
+def test_exchange_list_getters_check_their_arguments():
+    """cs_fill_map_get / cs_sync_map_get: counts with null arrays, refusal
+    of a wrong count, of partly null arrays and of an unknown list."""
+    import numpy as np
+    s = cs.Solve(ntp=8, nr=2, nghost=3)
+    s.mesh_build(device=False)
+    lib, n = s.lib, ctypes.c_int64(0)
+    assert lib.cs_fill_map_get(s.h, None, None, None, ctypes.byref(n)) == 0 and n.value > 0
+    a, b = np.zeros(n.value + 1, dtype=np.int32), np.zeros(n.value + 1, dtype=np.int32)
+    m = np.zeros(n.value + 1, dtype=np.uint8)
+    ip = lambda x: x.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+    u8 = m.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))
+    n1 = ctypes.c_int64(n.value + 1)
+    assert lib.cs_fill_map_get(s.h, ip(a), ip(b), u8, ctypes.byref(n1)) == 1
+    assert "size" in lib.cs_last_error(s.h).decode()
+    assert lib.cs_fill_map_get(s.h, ip(a), None, u8, ctypes.byref(n)) == 1
+    for which, expect in ((0, 4 * 8 * 2 * 6 // 2), (1, None)):
+        k = ctypes.c_int64(0)
+        assert lib.cs_sync_map_get(s.h, which, None, None, None, None, None, ctypes.byref(k)) == 0
+        if expect is not None:  # 4 panel edges x N faces x nr layers a panel, one copy of each pair
+            assert k.value == expect
+        assert k.value > 0
+    assert lib.cs_sync_map_get(s.h, 2, None, None, None, None, None, ctypes.byref(n)) == 1
+    i8 = ctypes.POINTER(ctypes.c_int8)
+    k = ctypes.c_int64(0)
+    lib.cs_sync_map_get(s.h, 1, None, None, None, None, None, ctypes.byref(k))
+    d, sr = np.zeros(k.value, dtype=np.int32), np.zeros(k.value, dtype=np.int32)
+    assert lib.cs_sync_map_get(s.h, 1, ip(d), ip(sr), None, None, None, ctypes.byref(k)) == 1
+    dst, src, dk, sk, sg = s.sync_map(1)
+    assert set(np.unique(sg)) <= {-1, 1} and set(np.unique(dk)) <= {0, 1, 2}
+
+
 def test_device_estimate_counts_panel_shared_row_weights():
     """The planning estimate counts the least-squares row weights the mesh
     build keeps: panel 1's serving the six panels by default (STEP 9.c's in
