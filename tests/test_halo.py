@@ -172,7 +172,7 @@ def test_panel_split_exchanges_match_the_single_process_application(panel_rank):
     assert sum(o[2] for o in out) == sum(o[3] for o in out)
 
 
-def _sharded_rank(rank, world, port, name, panel_rank, nsteps, q):
+def _sharded_rank(rank, world, port, name, flags, panel_rank, nsteps, q):
     """Whole steps of the oracle on a rank that holds only its own panels:
     each stage runs over them alone, with the ghost fill, the face-flux and
     the EMF ownership exchanged between its phases and the time step's
@@ -189,7 +189,7 @@ def _sharded_rank(rank, world, port, name, panel_rank, nsteps, q):
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
         pr = cs.preset(name)
-        s = cs.Solve(**pr["params"])
+        s = cs.Solve(**pr["params"], flags=flags)
         s.mesh_build(device=False)
         st = s.init_problem_host(**pr["init"])
         box = s.NI * s.NJ * s.NK
@@ -237,19 +237,22 @@ def _sharded_rank(rank, world, port, name, panel_rank, nsteps, q):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("name,panel_rank", [("shell16", [0, 0, 0, 1, 1, 1]), ("surface32", [0, 0, 1, 1, 2, 2])])
-def test_panel_sharded_steps_match_the_single_process_solve(name, panel_rank):
+@pytest.mark.parametrize("name,flags,panel_rank", [("shell16", 0, [0, 0, 0, 1, 1, 1]),
+                                                   ("surface32", 0, [0, 0, 1, 1, 2, 2]),
+                                                   ("shell16", cs.CS_FLAG_P2, [0, 1, 0, 1, 0, 1])])
+def test_panel_sharded_steps_match_the_single_process_solve(name, flags, panel_rank):
     """The two exchange lists (plus the time step's all-reduce) are all a
     panel-sharded stage needs: ranks that hold only their own panels and run
     every stage phase over them alone end two whole steps (IMEX-RK2 with
-    gravity on shell16, SSP-RK3 on surface32) with the single-process
-    oracle's state on their panels and its time steps, bit for bit."""
+    gravity on shell16, also with LIMIT_ALL_SLOPES_P2 and interleaved
+    panels; SSP-RK3 on surface32) with the single-process oracle's state on
+    their panels and its time steps, bit for bit."""
     world = max(panel_rank) + 1
     nsteps = 2
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = 29500 + os.getpid() % 1000 + 7 * world
-    procs = [ctx.Process(target=_sharded_rank, args=(r, world, port, name, panel_rank, nsteps, q)) for r in range(world)]
+    procs = [ctx.Process(target=_sharded_rank, args=(r, world, port, name, flags, panel_rank, nsteps, q)) for r in range(world)]
     for p in procs:
         p.start()
     out = sorted((q.get(timeout=600) for _ in procs), key=lambda o: o[0])
@@ -257,7 +260,7 @@ def test_panel_sharded_steps_match_the_single_process_solve(name, panel_rank):
         p.join(timeout=60)
         assert p.exitcode == 0
     pr = cs.preset(name)
-    s = cs.Solve(**pr["params"])
+    s = cs.Solve(**pr["params"], flags=flags)
     s.mesh_build(device=False)
     o = Oracle(s)
     o.put_state(s.init_problem_host(**pr["init"]))
