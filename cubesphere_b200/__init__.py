@@ -91,6 +91,7 @@ CS_FLAG_ADP_PER_PANEL = 16
 CS_FLAG_LSQ_PER_PANEL = 32
 CS_FLAG_STEP10 = 64
 CS_FLAG_P2 = 128
+CS_FLAG_PANEL_AVERAGE = 256
 
 
 def make_params(**kw) -> CsParams:

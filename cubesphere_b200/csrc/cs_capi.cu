@@ -313,6 +313,7 @@ struct SyncMaps {
   std::vector<int8_t> f_ddir, f_sdir;
   std::vector<int32_t> e_dst, e_src;  // edge offsets
   std::vector<int8_t> e_df, e_sf, e_sign;
+  std::vector<int32_t> e_cls;  // where each edge's entries start (one or two), then the entry count
 };
 
 std::string build_sync_maps(const Solve& sv, SyncMaps& m) {
@@ -403,6 +404,7 @@ std::string build_sync_maps(const Solve& sv, SyncMaps& m) {
     if (v.size() < 2) return "a panel-boundary edge belongs to one panel only";
     std::sort(v.begin(), v.end(), [](const Copy& x, const Copy& y) { return x.p < y.p; });
     const Copy& o = v[0];
+    m.e_cls.push_back((int32_t)m.e_dst.size());
     for (size_t q = 1; q < v.size(); ++q) {
       const Copy& x = v[q];
       m.e_df.push_back((int8_t)x.f);
@@ -412,6 +414,7 @@ std::string build_sync_maps(const Solve& sv, SyncMaps& m) {
       m.e_sign.push_back((int8_t)((x.a == o.a && x.c == o.c) ? 1 : -1));
     }
   }
+  m.e_cls.push_back((int32_t)m.e_dst.size());
   return "";
 }
 
@@ -431,6 +434,10 @@ bool check_params(const cs_params& p, std::string& why) {
   }
   if ((p.bc_lower != 2 && p.bc_lower != 0) || (p.bc_upper != 2 && p.bc_upper != 0)) {
     why = "radial boundary codes must be 2 (outflow) or 0 (none)";
+    return false;
+  }
+  if ((p.flags & CS_FLAG_PANEL_AVERAGE) && (p.flags & CS_FLAG_NO_PANEL_SYNC)) {
+    why = "CS_FLAG_PANEL_AVERAGE is a rule for the shared copies, which CS_FLAG_NO_PANEL_SYNC leaves alone";
     return false;
   }
   if ((p.flags & CS_FLAG_P2) && (p.flags & CS_FLAG_NO_OP_CACHE)) {
@@ -578,6 +585,7 @@ int mesh_upload(Solve& sv, MeshRes& m) {
     PanelSync& ps = m.psync;
     ps.nf = (long long)sm.f_dst.size();
     ps.ne = (long long)sm.e_dst.size();
+    ps.ncls = (long long)sm.e_cls.size() - 1;
     auto up32 = [&](const std::vector<int32_t>& v, int32_t*& dptr) -> cudaError_t {
       dptr = (int32_t*)mdalloc(sv, m, v.size() * sizeof(int32_t) + 16, e);
       if (!dptr) return e;
@@ -597,6 +605,7 @@ int mesh_upload(Solve& sv, MeshRes& m) {
     CS_CUDA(sv, up8(sm.e_df, ps.e_df));
     CS_CUDA(sv, up8(sm.e_sf, ps.e_sf));
     CS_CUDA(sv, up8(sm.e_sign, ps.e_sign));
+    CS_CUDA(sv, up32(sm.e_cls, ps.e_cls));
     CS_CUDA(sv, cudaStreamSynchronize(sv.stream));
   }
   return CS_OK;

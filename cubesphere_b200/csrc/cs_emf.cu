@@ -236,6 +236,25 @@ __global__ void k_sync_emf(DStateT<R> s, PanelSync ps) {
     s.Ef[ps.e_df[t]][ps.e_dst[t]] = (double)ps.e_sign[t] * s.Ef[ps.e_sf[t]][ps.e_src[t]];
 }
 
+// The reference's rule for a shared edge (CS_FLAG_PANEL_AVERAGE): all
+// copies take the average of the panels' EMFs, signed where a panel runs the
+// edge the other way; two copies (own + other) * 0.5, the three of a
+// cube-corner radial edge their sum / 3 (334fetch_buffers_fill_in_flux_x.f:
+// 341-395, 335fetch_buffers_fill_in_flux_y.f:761-795).  One thread an edge:
+// its owner's copy, then the one or two entries from e_cls[q].
+template <typename R>
+__global__ void k_avg_emf(DStateT<R> s, PanelSync ps) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < ps.ncls; q += (long long)gridDim.x * blockDim.x) {
+    const int h = ps.e_cls[q], n = ps.e_cls[q + 1] - h;
+    double* own = s.Ef[ps.e_sf[h]] + ps.e_src[h];
+    double sum = *own;
+    for (int m = h; m < h + n; ++m) sum += (double)ps.e_sign[m] * s.Ef[ps.e_df[m]][ps.e_dst[m]];
+    const double avg = n == 1 ? sum * 0.5 : sum / 3.0;
+    *own = avg;
+    for (int m = h; m < h + n; ++m) s.Ef[ps.e_df[m]][ps.e_dst[m]] = (double)ps.e_sign[m] * avg;
+  }
+}
+
 }  // namespace
 
 template <typename R>
@@ -251,7 +270,10 @@ void launch_edges_t(Solve& sv, DStateT<R>& st) {
   mark(sv, "k_edges_y");
   k_edges_z<R><<<blocks_for(ez.count(), TPB, grid_sms(sv)), TPB, 0, sv.stream>>>(d, sv.g, st, ez);
   mark(sv, "k_edges_z");
-  if (sv.psync.ne > 0) {
+  if (sv.psync.ncls > 0 && (sv.p.flags & CS_FLAG_PANEL_AVERAGE)) {
+    k_avg_emf<R><<<blocks_for(sv.psync.ncls, 128, grid_sms(sv)), 128, 0, sv.stream>>>(st, sv.psync);
+    mark(sv, "k_avg_emf");
+  } else if (sv.psync.ne > 0) {
     k_sync_emf<R><<<blocks_for(sv.psync.ne, 128, grid_sms(sv)), 128, 0, sv.stream>>>(st, sv.psync);
     mark(sv, "k_sync_emf");
   }

@@ -302,6 +302,38 @@ __global__ void k_sync_flux(Dims d, DStateT<R> s, PanelSync ps) {
   }
 }
 
+// The reference's rule for a shared face (CS_FLAG_PANEL_AVERAGE): both
+// copies take the average of the two panels' one-sided contributions (the
+// sides exchanged between them) and of their entropy fluxes (negated), as
+// its defect correction does (FETCH_BUFFERS_FILL_IN_FLUX_X / _Y,
+// 334fetch_buffers_fill_in_flux_x.f:295-309).  Each face is in one entry.
+template <typename R>
+__global__ void k_avg_flux(Dims d, DStateT<R> s, PanelSync ps) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < ps.nf; t += (long long)gridDim.x * blockDim.x) {
+    const long long dst = ps.f_dst[t], src = ps.f_src[t];
+    const int dd = ps.f_ddir[t], sd = ps.f_sdir[t];
+    const int dp = (int)(dst / d.S), sp = (int)(src / d.S);
+    const long long dof = dst % d.S, sof = src % d.S;
+    R* Fd = s.fcon[dd];
+    R* Fs = s.fcon[sd];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      R& dl = Fd[((long long)c * NPANEL + dp) * d.S + dof];
+      R& dr = Fd[((long long)(8 + c) * NPANEL + dp) * d.S + dof];
+      R& sl = Fs[((long long)c * NPANEL + sp) * d.S + sof];
+      R& sr = Fs[((long long)(8 + c) * NPANEL + sp) * d.S + sof];
+      const R a = (dl + sr) * R(0.5), b = (dr + sl) * R(0.5);
+      dl = a;
+      sr = a;
+      dr = b;
+      sl = b;
+    }
+    const R e = (s.EF[dd][dst] - s.EF[sd][src]) * R(0.5);
+    s.EF[dd][dst] = e;
+    s.EF[sd][src] = -e;
+  }
+}
+
 // dU/dt of each zone from its six faces (x, then y, then z; lower face,
 // upper face) for the zones whose faces were all computed.
 template <typename R>
@@ -368,7 +400,10 @@ void launch_fluxes_t(Solve& sv, DStateT<R>& st) {
     k_flux<R><<<nb, FLUX_FACES * 5, 0, sv.stream>>>(d, sv.ph, sv.g, st, fx, fy, fz);
     mark(sv, "k_flux");
   }
-  if (sv.psync.nf > 0) {
+  if (sv.psync.nf > 0 && (sv.p.flags & CS_FLAG_PANEL_AVERAGE)) {
+    k_avg_flux<R><<<blocks_for(sv.psync.nf, 128, grid_sms(sv)), 128, 0, sv.stream>>>(d, st, sv.psync);
+    mark(sv, "k_avg_flux");
+  } else if (sv.psync.nf > 0) {
     k_sync_flux<R><<<blocks_for(sv.psync.nf, 128, grid_sms(sv)), 128, 0, sv.stream>>>(d, st, sv.psync);
     mark(sv, "k_sync_flux");
   }

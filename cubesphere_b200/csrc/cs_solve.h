@@ -33,7 +33,8 @@ struct PanelSync {
   int8_t *f_ddir = nullptr, *f_sdir = nullptr;
   int32_t *e_dst = nullptr, *e_src = nullptr;
   int8_t *e_df = nullptr, *e_sf = nullptr, *e_sign = nullptr;
-  long long nf = 0, ne = 0;
+  int32_t* e_cls = nullptr;  // ncls + 1 starts: the entries of one edge (its copies but the owner's)
+  long long nf = 0, ne = 0, ncls = 0;
 };
 
 // Per-kernel device timing with CUDA events recorded on the solve's

@@ -93,6 +93,50 @@ def apply_edge_sync(Ef, dst, src, dk, sk, sign) -> None:
         Ef[c][dst[sel]] = vals[sel]
 
 
+def apply_face_average(fcon, EF, dst, src, dk, sk) -> None:
+    """The reference's rule for shared faces (CS_FLAG_PANEL_AVERAGE) on host
+    arrays laid out as for apply_face_sync, in place: both copies of each
+    listed face take the average of the two panels' contributions (sides
+    exchanged) and of their entropy fluxes (negated), as k_avg_flux does."""
+    for d in range(len(fcon)):
+        for s in range(len(fcon)):
+            sel = np.flatnonzero((dk == d) & (sk == s))
+            if len(sel):
+                m = fcon[d].shape[0] // 2
+                own, other = fcon[d][:, dst[sel]], np.roll(fcon[s][:, src[sel]], m, axis=0)
+                avg = (own + other) * 0.5
+                fcon[d][:, dst[sel]] = avg
+                fcon[s][:, src[sel]] = np.roll(avg, m, axis=0)
+                e = (EF[d][dst[sel]] - EF[s][src[sel]]) * 0.5
+                EF[d][dst[sel]] = e
+                EF[s][src[sel]] = -e
+
+
+def edge_classes(src, sk):
+    """Starts of the runs of entries that share an owner copy (one run an
+    edge: one entry for an edge of two panels, two at a cube corner), then
+    the entry count; the device builds the same starts with the list."""
+    key = sk.astype(np.int64) << 40 | src.astype(np.int64)
+    return np.concatenate([[0], np.flatnonzero(key[1:] != key[:-1]) + 1, [len(src)]])
+
+
+def apply_edge_average(Ef, dst, src, dk, sk, sign) -> None:
+    """The reference's rule for shared edges (CS_FLAG_PANEL_AVERAGE) on host
+    arrays Ef[c] (6 * box), in place: every copy takes the signed average of
+    the copies, (own + other) * 0.5 for two and their sum / 3 for the three of
+    a cube-corner radial edge, as k_avg_emf does."""
+    cls = edge_classes(src, sk)
+    for q in range(len(cls) - 1):
+        h, n = cls[q], cls[q + 1] - cls[q]
+        total = Ef[sk[h]][src[h]]
+        for m in range(h, h + n):
+            total = total + float(sign[m]) * Ef[dk[m]][dst[m]]
+        avg = total * 0.5 if n == 1 else total / 3.0
+        Ef[sk[h]][src[h]] = avg
+        for m in range(h, h + n):
+            Ef[dk[m]][dst[m]] = float(sign[m]) * avg
+
+
 class PanelSplit:
     """Entries of one exchange list as one rank sees them: `panel_rank[p]`
     is the rank owning panel p, `box` the points of one panel box, and src /

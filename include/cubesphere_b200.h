@@ -104,9 +104,19 @@ typedef struct cs_params {
  * edges it shares with other panels instead of giving every shared face and
  * edge the value of its owner (the lowest-numbered panel holding it).  The
  * default ownership is this library's single-device form of the reference's
- * defect correction (DRV:3200-3461): conservative, and div B stays at
- * round-off across panel edges; without it div B grows at the cube corners. */
+ * defect correction (DRV:3200-3461), whose values are the copies' average
+ * instead (CS_FLAG_PANEL_AVERAGE): conservative, and div B stays at round-off
+ * across panel edges; without it div B grows at the cube corners. */
 #define CS_FLAG_NO_PANEL_SYNC 4
+/* cs_params.flags: the reference's rule for the shared copies instead of
+ * ownership: every copy of a face or edge that two panels compute takes
+ * their average, the three copies of a cube-corner radial edge their sum / 3
+ * (the values its defect correction applies: FETCH_BUFFERS_FILL_IN_FLUX_X /
+ * _Y, 334fetch_buffers_fill_in_flux_x.f:295-395, 335:761-795, through
+ * UPDATE_DEFECT_IMEX_RK with the stage's dtmove, DRV:2777, 3200-3470).
+ * Conservative, div B at round-off, and unlike ownership it keeps the cube's
+ * rotation symmetry.  Not with CS_FLAG_NO_PANEL_SYNC (CS_ERR_ARG). */
+#define CS_FLAG_PANEL_AVERAGE 256
 /* cs_params.flags: the precision form.  The bulk of the stage (conserved
  * state, entropy, primitives and their modes, the flattener, face states and
  * fluxes, dU/dt, the stage copies, the resident least-squares inverses, the

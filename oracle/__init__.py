@@ -48,6 +48,7 @@ def load() -> ctypes.CDLL:
         "oracle_limit_minmax": ([P, dp, dp], ctypes.c_int),
         "oracle_stage_phase": ([P, ctypes.c_int, ctypes.c_int, D, ctypes.c_uint], ctypes.c_int),
         "oracle_evaluate_timestep_panels": ([P, D, ctypes.c_uint], D),
+        "oracle_set_panel_rule": ([P, ctypes.c_int], None),
         "oracle_stage_array": ([P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)], dp),
     }
     for n in ("oracle_fill_ghosts", "oracle_limit_all_slopes_p12", "oracle_make_facial_fluxes",
@@ -225,6 +226,12 @@ class Oracle:
     # scatter + edge EMFs, 3 the rest of the stage.
     def stage_phase(self, phase: int, irk: int = 1, dtcur: float = 0.0, panels: int = 63):
         assert self.lib.oracle_stage_phase(self.h, phase, irk, dtcur, panels) == 0
+
+    def set_panel_rule(self, rule: int):
+        """Value of the copies of a shared face or edge: 0 the lowest-numbered
+        panel's (the library's default), 1 their average (the reference's
+        defect correction; what CS_FLAG_PANEL_AVERAGE selects)."""
+        self.lib.oracle_set_panel_rule(self.h, rule)
 
     def evaluate_timestep_panels(self, dtcur: float, panels: int) -> float:
         return self.lib.oracle_evaluate_timestep_panels(self.h, dtcur, panels)

@@ -68,6 +68,11 @@ struct Ctx {
   bool maps_built = false;
   std::vector<FaceSync> fsync;
   std::vector<EdgeSync> esync;
+  std::vector<size_t> eclass;  // esync index where each edge's copies start, then esync.size()
+  // which value the copies of a shared face or edge take: 0 the
+  // lowest-numbered panel's (the library's default), 1 their average (the
+  // reference's defect correction; CS_FLAG_PANEL_AVERAGE)
+  int panel_rule = 0;
 
   size_t idx(int i, int j, int k) const { return ((size_t)(k + G) * NJ + (size_t)(j + G)) * NI + (size_t)(i + G); }
   double& a(std::vector<double>& v, int c, int pn, int i, int j, int k) { return v[((size_t)c * 6 + pn) * S + idx(i, j, k)]; }
@@ -1621,6 +1626,7 @@ static void build_sync_maps(Ctx& c) {
     }
   }
   c.esync.clear();
+  c.eclass.clear();
   for (auto& kv : cls) {
     auto& v = kv.second;
     if (v.size() < 2) {
@@ -1629,23 +1635,55 @@ static void build_sync_maps(Ctx& c) {
     }
     std::sort(v.begin(), v.end(), [](const Copy& x, const Copy& y) { return x.p < y.p; });
     const Copy& o = v[0];
+    c.eclass.push_back(c.esync.size());
     for (size_t m = 1; m < v.size(); ++m) {
       const Copy& x = v[m];
       const int sign = (x.a == o.a && x.b == o.b) ? 1 : -1;
       c.esync.push_back({x.f, x.p, x.i, x.j, x.k, o.f, o.p, o.i, o.j, o.k, sign});
     }
   }
+  c.eclass.push_back(c.esync.size());
   c.maps_built = true;
 }
 
-static bool sync_on(const Ctx& c) { return !(c.p.flags & 4); }
+static bool sync_on(const Ctx& c) { return !(c.p.flags & CS_FLAG_NO_PANEL_SYNC); }
 
 // Non-owner copies of panel-edge faces take the owner's contributions with
 // the two sides exchanged (the normals are opposite) and the negated
 // entropy flux.
+//
+// With panel_rule 1 the copies take their average instead, as in the
+// reference's defect correction: FETCH_BUFFERS_FILL_IN_FLUX_X / _Y set each
+// coinciding face's fluctuations and entropy flux and each coinciding edge's
+// EMF to (own + neighbour's) * 0.5 (334fetch_buffers_fill_in_flux_x.f:295-309,
+// :341-350, :384-395, 335 likewise), the three copies of a cube-corner radial
+// edge to their sum / 3 (335:761-795), and UPDATE_DEFECT_IMEX_RK applies the
+// differences from the per-panel values with the stage's dtmove
+// (1000riemann_geomesh_cs_mhd.f:2777, :3200-3470), which is the update with
+// the averages up to round-off.
 void sync_facial_fluxes(Ctx& c) {
   if (!sync_on(c)) return;
   if (!c.maps_built) build_sync_maps(c);
+  if (c.panel_rule == 1) {
+    for (const auto& f : c.fsync) {
+      const size_t d = c.idx(f.i, f.j, f.k), o = c.idx(f.oi, f.oj, f.ok);
+      for (int t = 0; t < 5 * NV; ++t) {
+        double& Ld = c.cL[f.dir][((size_t)t * 6 + f.pn) * c.S + d];
+        double& Rd = c.cR[f.dir][((size_t)t * 6 + f.pn) * c.S + d];
+        double& Lo = c.cL[f.odir][((size_t)t * 6 + f.opn) * c.S + o];
+        double& Ro = c.cR[f.odir][((size_t)t * 6 + f.opn) * c.S + o];
+        const double a = (Ld + Ro) * 0.5, b = (Rd + Lo) * 0.5;
+        Ld = Ro = a;
+        Rd = Lo = b;
+      }
+      std::vector<double>& EFd = f.dir == 0 ? c.EFx : (f.dir == 1 ? c.EFy : c.EFz);
+      std::vector<double>& EFo = f.odir == 0 ? c.EFx : (f.odir == 1 ? c.EFy : c.EFz);
+      const double a = (EFd[(size_t)f.pn * c.S + d] - EFo[(size_t)f.opn * c.S + o]) * 0.5;
+      EFd[(size_t)f.pn * c.S + d] = a;
+      EFo[(size_t)f.opn * c.S + o] = -a;
+    }
+    return;
+  }
   for (const auto& f : c.fsync) {
     const size_t d = c.idx(f.i, f.j, f.k), o = c.idx(f.oi, f.oj, f.ok);
     for (int t = 0; t < 5 * NV; ++t) {
@@ -1661,6 +1699,25 @@ void sync_facial_fluxes(Ctx& c) {
 void sync_edge_efields(Ctx& c) {
   if (!sync_on(c)) return;
   if (!c.maps_built) build_sync_maps(c);
+  auto E = [&](int f) -> std::vector<double>& { return f == 0 ? c.Efx : (f == 1 ? c.Efy : c.Efz); };
+  if (c.panel_rule == 1) {
+    for (size_t q = 0; q + 1 < c.eclass.size(); ++q) {
+      const Ctx::EdgeSync& h = c.esync[c.eclass[q]];
+      double& Eo = E(h.of)[(size_t)h.opn * c.S + c.idx(h.oi, h.oj, h.ok)];
+      double sum = Eo;
+      for (size_t m = c.eclass[q]; m < c.eclass[q + 1]; ++m) {
+        const Ctx::EdgeSync& e = c.esync[m];
+        sum += e.sign * E(e.f)[(size_t)e.pn * c.S + c.idx(e.i, e.j, e.k)];
+      }
+      const double avg = c.eclass[q + 1] - c.eclass[q] == 1 ? sum * 0.5 : sum / 3.0;
+      Eo = avg;
+      for (size_t m = c.eclass[q]; m < c.eclass[q + 1]; ++m) {
+        const Ctx::EdgeSync& e = c.esync[m];
+        E(e.f)[(size_t)e.pn * c.S + c.idx(e.i, e.j, e.k)] = e.sign * avg;
+      }
+    }
+    return;
+  }
   for (const auto& e : c.esync) {
     std::vector<double>& Ed = e.f == 0 ? c.Efx : (e.f == 1 ? c.Efy : c.Efz);
     const std::vector<double>& Eo = e.of == 0 ? c.Efx : (e.of == 1 ? c.Efy : c.Efz);
@@ -2222,6 +2279,7 @@ extern "C" {
 void* oracle_create(const void* params) {
   Ctx* c = new Ctx();
   std::memcpy(&c->p, params, sizeof(Params));
+  c->panel_rule = (c->p.flags & CS_FLAG_PANEL_AVERAGE) ? 1 : 0;
   c->N = c->p.ntp;
   c->nr = c->p.nr;
   c->G = c->p.nghost;
@@ -2419,6 +2477,9 @@ int oracle_stage_phase(void* h, int phase, int irk, double dtcur, unsigned panel
     default: return 1;
   }
 }
+// Rule for the copies of shared faces and edges: 0 the lowest-numbered
+// panel's (the library's), 1 their average (the reference's).
+void oracle_set_panel_rule(void* h, int rule) { ((Ctx*)h)->panel_rule = rule; }
 double oracle_evaluate_timestep_panels(void* h, double dtcur, unsigned panels) {
   return evaluate_timestep(*(Ctx*)h, dtcur, panels);
 }

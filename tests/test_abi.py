@@ -46,6 +46,18 @@ def test_p2_needs_the_resident_stencil_operators():
     assert lib.cs_params_check(ctypes.byref(cs.make_params(ntp=16, nr=4, flags=cs.CS_FLAG_P2))).decode() == ""
 
 
+def test_panel_average_needs_the_shared_copies():
+    """CS_FLAG_PANEL_AVERAGE is a rule for the shared copies: refused with
+    CS_FLAG_NO_PANEL_SYNC, which leaves them alone, and accepted alone."""
+    lib = cs.load_library()
+    bad = cs.make_params(ntp=16, nr=4, flags=cs.CS_FLAG_PANEL_AVERAGE | cs.CS_FLAG_NO_PANEL_SYNC)
+    assert "CS_FLAG_PANEL_AVERAGE" in lib.cs_params_check(ctypes.byref(bad)).decode()
+    with pytest.raises(cs.CsError):
+        cs.Solve(bad)
+    ok = cs.make_params(ntp=16, nr=4, flags=cs.CS_FLAG_PANEL_AVERAGE)
+    assert lib.cs_params_check(ctypes.byref(ok)).decode() == ""
+
+
 def test_calls_out_of_order_return_state_errors():
     s = cs.Solve(ntp=8, nr=2, nghost=3)
     lib = s.lib

@@ -14,7 +14,8 @@ import pytest
 import torch.multiprocessing as mp
 
 import cubesphere_b200 as cs
-from cubesphere_b200.halo import FIELDS, apply_edge_sync, apply_face_sync, apply_fill_map
+from cubesphere_b200.halo import (FIELDS, apply_edge_average, apply_edge_sync, apply_face_average, apply_face_sync,
+                                  apply_fill_map, edge_classes)
 from oracle import Oracle
 
 ROOT = Path(__file__).resolve().parents[1]
@@ -73,8 +74,15 @@ def test_sync_maps_reproduce_the_oracle_ownership(name):
         dst, src, dk, sk, sg = s.sync_map(which)
         assert len(dst) > 0
         d = set((dk.astype(np.int64) << 40 | dst).tolist())
+        owners = (sk.astype(np.int64) << 40 | src).tolist()
         assert len(d) == len(dst)
-        assert not d & set((sk.astype(np.int64) << 40 | src).tolist())
+        assert not d & set(owners)
+        # one entry a face, one run of one or two entries an edge (its
+        # owner's copy shared by the run only): the averaging kernels' threads
+        # touch disjoint copies
+        cls = edge_classes(src, sk)
+        assert len(set(owners)) == len(cls) - 1
+        assert set(np.diff(cls).tolist()) <= ({1} if which == 0 else {1, 2})
     dst, src, dk, sk, sg = s.sync_map(0)
     assert set(dk.tolist()) <= {0, 1} and (sg == -1).all()
     EF = [a.reshape(-1).copy() for a in ef_off]
@@ -88,6 +96,42 @@ def test_sync_maps_reproduce_the_oracle_ownership(name):
     apply_edge_sync(Ef, dst, src, dk, sk, sg)
     for q in range(3):
         assert np.array_equal(Ef[q], e_on[q].reshape(-1)), q
+
+
+def _oracle_stage_arrays(pr, flags):
+    s = cs.Solve(**pr["params"], flags=flags)
+    s.mesh_build(device=False)
+    o = Oracle(s)
+    o.put_state(s.init_problem_host(**pr["init"]))
+    o.fill_ghosts()
+    o.limit_all_slopes_p12()
+    o.make_facial_fluxes()
+    o.make_edge_efields_p1()
+    fcon = [np.concatenate([o.stage_array("cL", d), o.stage_array("cR", d)]) for d in range(2)]
+    return s, fcon, [o.stage_array("EF", d).copy() for d in range(3)], [o.stage_array("Ef", c).copy() for c in range(3)]
+
+
+@pytest.mark.parametrize("name", ["shell16", "surface32"])
+def test_average_rule_through_the_lists_reproduces_the_oracle(name):
+    """CS_FLAG_PANEL_AVERAGE (the reference's rule): the averages formed
+    through the exported ownership lists, in the order and grouping the
+    device kernels use (each face entry on its own, each edge's entries as
+    one run from its owner copy), turn the oracle's per-panel contributions,
+    entropy fluxes and EMFs into its averaged ones bit for bit."""
+    pr = cs.preset(name)
+    s, fcon, EF, Ef = _oracle_stage_arrays(pr, cs.CS_FLAG_NO_PANEL_SYNC)
+    _, fcon_avg, EF_avg, Ef_avg = _oracle_stage_arrays(pr, cs.CS_FLAG_PANEL_AVERAGE)
+    dst, src, dk, sk, _ = s.sync_map(0)
+    apply_face_average(fcon, EF, dst, src, dk, sk)
+    for d in range(2):
+        assert np.array_equal(fcon[d], fcon_avg[d]), d
+    for d in range(3):
+        assert np.array_equal(EF[d], EF_avg[d]), d
+    dst, src, dk, sk, sg = s.sync_map(1)
+    apply_edge_average(Ef, dst, src, dk, sk, sg)
+    for c in range(3):
+        assert np.array_equal(Ef[c], Ef_avg[c]), c
+    assert not np.array_equal(Ef_avg[2], _oracle_stage_arrays(pr, 0)[3][2])  # the rules differ
 
 
 def _rank(rank, world, port, panel_rank, q):

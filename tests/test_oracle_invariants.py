@@ -38,10 +38,12 @@ def test_initial_field_is_divergence_free():
     assert _divb(s, st) < 1e-12
 
 
-@pytest.mark.parametrize("rk,flags", [(cs.CS_RK2, 0), (cs.CS_IMEX_RK2, 0), (cs.CS_IMEX_RK2, cs.CS_FLAG_P2)])
+@pytest.mark.parametrize("rk,flags", [(cs.CS_RK2, 0), (cs.CS_IMEX_RK2, 0), (cs.CS_IMEX_RK2, cs.CS_FLAG_P2),
+                                     (cs.CS_IMEX_RK2, cs.CS_FLAG_PANEL_AVERAGE)])
 def test_panel_edge_ownership_keeps_div_b_at_roundoff(rk, flags):
-    """CT with panel-edge ownership keeps div B at round-off whichever
-    reconstruction (P12 or P2) feeds the EMFs."""
+    """CT with one value on every shared face and edge (ownership, or the
+    reference's averages) keeps div B at round-off whichever reconstruction
+    (P12 or P2) feeds the EMFs."""
     s, o, st = _setup(flags, rk_scheme=rk)
     dt = o.evaluate_timestep(1e30)
     for _ in range(2):
@@ -367,3 +369,29 @@ def test_step10_min_max_of_the_oracle():
     # the divergence entries are round-off of a divergence-free field
     assert abs(vmin[8]) < 1e-12 * area and abs(vmax[8]) < 1e-12 * area
     assert abs(vmin[8] - wmin[8]) < 1e-13 * area and abs(vmax[8] - wmax[8]) < 1e-13 * area
+
+
+@pytest.mark.parametrize("flags", [cs.CS_FLAG_PANEL_AVERAGE, cs.CS_FLAG_NO_PANEL_SYNC, 0])
+def test_shared_copies_and_the_cube_symmetry(flags):
+    """A spherically symmetric state (the hydrostatic shell without its
+    perturbations) on panels that are exact rotations of one another stays
+    the same on all six panels, to round-off, when the shared copies take
+    their average (the reference's rule) or keep their own values; giving
+    them the lowest-numbered panel's value breaks the symmetry near the cube
+    corners by the copies' difference (truncation size)."""
+    pr = cs.preset("shell16")
+    s = cs.Solve(**pr["params"], flags=flags)
+    s.mesh_build(device=False)
+    init = dict(pr["init"], rho_amp=0.0, a_amp=0.0)
+    o = Oracle(s)
+    o.put_state(s.init_problem_host(**init))
+    dt = o.evaluate_timestep(1e30)
+    for _ in range(3):
+        dt = o.step(dt)
+    G, N, nr = s.G, s.N, s.nr
+    rho = o.get_state()["U"][0][:, G + 1:G + nr + 1, G + 1:G + N + 1, G + 1:G + N + 1]
+    asym = np.abs(rho - rho[0]).max() / np.abs(rho).max()
+    if flags:
+        assert asym < 1e-13
+    else:
+        assert asym > 1e-7
